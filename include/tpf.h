@@ -1,0 +1,182 @@
+/*
+ * tpf.h -- C ABI of the B200 (sm_100a) implementation of TwoPhaseFlow's hot path:
+ * the 6th-order combined compact difference (CCD) operator and the
+ * variable-density FVM pressure-Poisson (PPE) solve.
+ *
+ * Plain C: opaque handles, device pointers, sizes, an explicit CUDA stream
+ * (cudaStream_t passed as void*), int status codes.  No torch or C++ types.
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   CCD: src/twophase/ccd/ccd_solver.py:79-281 (CCDSolver)
+ *   PPE: src/twophase/ppe/interfaces.py:28-86 (IPPESolver.solve),
+ *        src/twophase/ppe/fvm_matrixfree.py:46-363 (PPESolverFVMMatrixFree)
+ *
+ * Status codes mirror the reference's error conventions: the Python layer maps
+ * TPF_EINVAL -> ValueError, TPF_ESINGULAR -> numpy.linalg.LinAlgError,
+ * TPF_ENOCONV -> RuntimeError("did not converge ... info=<iters>"),
+ * TPF_ECUDA / TPF_EABORT -> RuntimeError.
+ *
+ * Threading: calls on one handle are not thread safe; distinct handles are
+ * independent.  All compute calls are asynchronous on `stream` unless stated.
+ */
+#ifndef TPF_H_
+#define TPF_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum tpf_status {
+  TPF_OK = 0,
+  TPF_EINVAL = 1,     /* invalid argument (reference: ValueError)            */
+  TPF_ENOCONV = 2,    /* Krylov did not converge (reference: RuntimeError)    */
+  TPF_ECUDA = 3,      /* CUDA runtime error                                   */
+  TPF_EABORT = 4,     /* a bounded device wait gave up (barrier timeout)      */
+  TPF_ESINGULAR = 5   /* singular pivot in a factorization (LinAlgError)      */
+};
+
+enum tpf_dtype { TPF_F64 = 0, TPF_F32 = 1 };
+enum tpf_bc { TPF_BC_WALL = 0, TPF_BC_PERIODIC = 1 };
+
+/* flags for tpf_ccd_apply */
+enum tpf_ccd_flags {
+  TPF_CCD_APPLY_METRIC = 1   /* map xi-space derivatives to x (non-uniform grid) */
+};
+
+/* Library version (major*10000 + minor*100 + patch). */
+int tpf_version(void);
+/* Message of the last failing call on this host thread ("" if none). */
+const char* tpf_last_error(void);
+
+/* ------------------------------------------------------------------------ */
+/* CCD operator                                                              */
+/* ------------------------------------------------------------------------ */
+typedef struct tpf_ccd_plan tpf_ccd_plan;
+
+/* One axis of a CCD operator: n_pts nodes (N+1), spacing h (the stencil
+ * spacing: L/N on uniform grids, 1/N in xi-space), boundary TPF_BC_WALL or
+ * TPF_BC_PERIODIC, data type TPF_F64 or TPF_F32.
+ * Replaces CCDSolver._get_axis_solver / build_ccd_axis_solver /
+ * build_ccd_axis_solver_periodic (ccd_solver.py:99-130,294-299;
+ * ccd_solver_helpers.py:227-314,406-423).  Wall requires n_pts >= 6
+ * (ccd_solver.py:459-465) -> TPF_EINVAL; periodic requires n_pts >= 4.
+ * Blocking (host-side factorization + one host->device copy). */
+int tpf_ccd_plan_create(tpf_ccd_plan** plan, int64_t n_pts, double h, int bc,
+                        int dtype);
+int tpf_ccd_plan_destroy(tpf_ccd_plan* plan);
+
+/* Metric of a non-uniform axis (host arrays of n_pts doubles: J = dxi/dx and
+ * dJ/dxi).  Replaces the grid metric used by apply_ccd_metric
+ * (ccd_solver_helpers.py:509-533).  Blocking. */
+int tpf_ccd_plan_set_metric(tpf_ccd_plan* plan, const double* J,
+                            const double* dJ);
+
+/* d1/d2 of f along the plan's axis for an array viewed as C-order
+ * [outer, n_pts, inner] (the axis in the middle).  f, d1, d2 are device
+ * pointers of the plan's dtype; d1 or d2 may be NULL (first_derivative /
+ * second_derivative).  bc_left / bc_right: optional host pointers to
+ * (f'_b, f''_b) overrides of the wall closure (testing hook of the reference),
+ * NULL for the compact closure.  flags: TPF_CCD_APPLY_METRIC.
+ * Replaces CCDSolver.differentiate / first_derivative / second_derivative /
+ * differentiate_raw (ccd_solver.py:134-237; ccd_solver_helpers.py:38-224,
+ * 426-506). */
+int tpf_ccd_apply(const tpf_ccd_plan* plan, int64_t outer, int64_t inner,
+                  const void* f, void* d1, void* d2, const double* bc_left,
+                  const double* bc_right, int flags, void* stream);
+
+/* Zero grad at index 0 and n_pts-1 along the axis of a [outer, n, inner]
+ * array (wall axes only; no-op for periodic plans).  Replaces
+ * CCDSolver.enforce_wall_neumann (ccd_solver.py:264-281;
+ * ccd_boundary_helpers.py:52-61). */
+int tpf_ccd_enforce_wall_neumann(const tpf_ccd_plan* plan, int64_t outer,
+                                 int64_t inner, void* grad, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Variable-density FVM PPE                                                   */
+/* ------------------------------------------------------------------------ */
+typedef struct tpf_ppe tpf_ppe;
+
+enum tpf_ppe_method {
+  TPF_PPE_CG = 0,        /* CG on the control-volume-weighted SPD system       */
+  TPF_PPE_GMRES = 1      /* restarted GMRES, left preconditioned               */
+};
+enum tpf_ppe_precond {
+  TPF_PRECOND_NONE = 0,
+  TPF_PRECOND_JACOBI = 1,
+  TPF_PRECOND_LINE = 2,       /* shifted additive line solves, exact Thomas   */
+  TPF_PRECOND_LINE_PCR = 3    /* same, truncated PCR with pcr_stages stages    */
+};
+enum tpf_precision {
+  TPF_PREC_F64 = 0,      /* FP64 Krylov                                          */
+  TPF_PREC_MIXED = 1     /* FP32 inner CG under FP64 iterative refinement       */
+};
+
+typedef struct tpf_ppe_options {
+  int method;            /* tpf_ppe_method                                      */
+  int precond;           /* tpf_ppe_precond                                     */
+  int precision;         /* tpf_precision                                       */
+  double tol;            /* relative residual tolerance (pseudo_tol)             */
+  int64_t maxiter;       /* CG: iterations; GMRES: restart cycles (pseudo_maxiter)*/
+  int restart;           /* GMRES restart length (ppe_restart)                   */
+  double c_tau;          /* line-preconditioner shift factor (pseudo_c_tau)      */
+  int pcr_stages;        /* TPF_PRECOND_LINE_PCR stages (ppe_pcr_stages)         */
+  double inner_tol;      /* MIXED: relative tolerance of each FP32 inner solve   */
+  int64_t max_refine;    /* MIXED: maximum refinement sweeps                     */
+} tpf_ppe_options;
+
+typedef struct tpf_ppe_result {
+  int64_t iterations;    /* CG iterations / GMRES inner iterations (all sweeps)  */
+  int64_t applies;       /* operator applications                                */
+  int64_t refinements;   /* MIXED: outer refinement sweeps                       */
+  double rel_residual;   /* ||b - A x|| / ||b|| of the solved system             */
+  int info;              /* 0 converged, >0 iteration budget exhausted           */
+} tpf_ppe_result;
+
+/* Fill `opts` with the reference defaults: GMRES, line preconditioner,
+ * tol 1e-8, maxiter 500, restart 80, c_tau 2, pcr_stages 4
+ * (fvm_matrixfree.py:90-127; config.py:331-333). */
+void tpf_ppe_default_options(tpf_ppe_options* opts);
+
+/* Handle for one wall-bounded grid: ndim in {2,3}, N[a] cells per axis,
+ * coords[a] = host array of N[a]+1 node coordinates, pin = flat index of the
+ * gauge-pinned node (BoundarySpec.pin_dof).  Allocates the device workspace.
+ * Replaces PPESolverFVMMatrixFree.__init__ / _refresh_grid_metrics
+ * (fvm_matrixfree.py:66-138,338-343; fvm_matrixfree_helpers.py:23-43). */
+int tpf_ppe_create(tpf_ppe** h, int ndim, const int64_t* N,
+                   const double* const* coords, int64_t pin,
+                   const tpf_ppe_options* opts);
+int tpf_ppe_destroy(tpf_ppe* h);
+int tpf_ppe_set_options(tpf_ppe* h, const tpf_ppe_options* opts);
+
+/* Build face coefficients, Jacobi diagonal and line-preconditioner state
+ * from rho (device, grid shape, FP64).  Replaces prepare_operator /
+ * _prepare_preconditioner_state (fvm_matrixfree.py:262-279,352-363;
+ * fvm_matrixfree_helpers.py:46-104). */
+int tpf_ppe_prepare(tpf_ppe* h, const double* rho, void* stream);
+
+/* out = L p with the pinned row (out[pin] = p[pin]).  Replaces
+ * PPESolverFVMMatrixFree.apply (fvm_matrixfree.py:281-300). */
+int tpf_ppe_apply(tpf_ppe* h, const double* p, double* out, void* stream);
+
+/* z = M^-1 r for the handle's preconditioner on the unweighted system.
+ * Replaces apply_line_preconditioner / apply_jacobi_preconditioner
+ * (fvm_matrixfree.py:302-331). */
+int tpf_ppe_precondition(tpf_ppe* h, const double* r, double* z, void* stream);
+
+/* Solve L p = rhs for the density given to the last tpf_ppe_prepare (or
+ * prepare from `rho` first when rho != NULL).  p_init may be NULL.  p is
+ * written with p[pin] = 0.  Synchronizes `stream` (the result is read back).
+ * Returns TPF_ENOCONV when the iteration budget ends before tol (p holds the
+ * last iterate).  Replaces PPESolverFVMMatrixFree.solve
+ * (fvm_matrixfree.py:150-260) and the SciPy Krylov loops it calls
+ * (gmres_helpers.py:16-80). */
+int tpf_ppe_solve(tpf_ppe* h, const double* rhs, const double* rho, double* p,
+                  const double* p_init, void* stream, tpf_ppe_result* result);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TPF_H_ */

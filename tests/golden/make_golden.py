@@ -1,0 +1,233 @@
+"""Generate the golden fixtures by running the reference itself.
+
+Run in a container that has the reference source tree (not needed at test time):
+
+    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py /root/reference/src
+
+It imports the reference's ``twophase`` package read-only, runs its own CPU
+functions (``CCDSolver.differentiate``, ``PPESolverFVMMatrixFree``,
+``PPESolverFVMSpsolve``, the batched tridiagonal helpers and the CCD
+variable-density Laplacian) on small seeded inputs and stores inputs and
+outputs in ``ccd_golden.npz`` / ``ppe_golden.npz`` next to this script.
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _ref_import(src):
+    sys.path.insert(0, src)
+    os.environ.setdefault("PYTHONDONTWRITEBYTECODE", "1")
+    sys.dont_write_bytecode = True
+    import twophase  # noqa: F401
+    return twophase
+
+
+def make_ccd(out):
+    from twophase.backend import Backend
+    from twophase.config import GridConfig
+    from twophase.core.grid import Grid
+    from twophase.ccd.ccd_solver import CCDSolver
+    from twophase.levelset.heaviside import heaviside
+
+    be = Backend(use_gpu=False)
+    rng = np.random.default_rng(2024)
+    cases = [
+        ("wall2d", (16, 12), "wall"),
+        ("wall3d", (8, 10, 6), "wall"),
+        ("per2d", (16, 10), "periodic"),
+        ("per3d", (8, 6, 10), "periodic"),
+        ("wall2d_big", (64, 40), "wall"),
+    ]
+    for name, N, bc in cases:
+        grid = Grid(GridConfig(ndim=len(N), N=N, L=tuple(1.0 + 0.25 * a for a in range(len(N)))), be)
+        ccd = CCDSolver(grid, be, bc_type=bc)
+        f = rng.standard_normal(grid.shape)
+        out[f"{name}/N"] = np.array(N)
+        out[f"{name}/L"] = np.array(grid.L, dtype=np.float64)
+        out[f"{name}/f"] = f
+        for ax in range(len(N)):
+            d1, d2 = ccd.differentiate(f, ax)
+            out[f"{name}/d1_ax{ax}"] = np.asarray(d1)
+            out[f"{name}/d2_ax{ax}"] = np.asarray(d2)
+            out[f"{name}/first_ax{ax}"] = np.asarray(ccd.first_derivative(f, ax))
+            out[f"{name}/second_ax{ax}"] = np.asarray(ccd.second_derivative(f, ax))
+        if bc == "wall":
+            d1, d2 = ccd.differentiate(f, 0, bc_left=(0.3, -1.2), bc_right=(0.0, 2.5))
+            out[f"{name}/bcov_d1"] = np.asarray(d1)
+            out[f"{name}/bcov_d2"] = np.asarray(d2)
+    # analytic case of the reference test suite: sin(2 pi x) on N=32, periodic and wall
+    for bc in ("wall", "periodic"):
+        grid = Grid(GridConfig(ndim=2, N=(32, 4), L=(1.0, 1.0)), be)
+        ccd = CCDSolver(grid, be, bc_type=bc)
+        x = np.asarray(grid.coords[0])
+        f = np.broadcast_to(np.sin(2 * np.pi * x)[:, None], grid.shape).copy()
+        d1, d2 = ccd.differentiate(f, 0)
+        out[f"sin_{bc}/f"] = f
+        out[f"sin_{bc}/d1"] = np.asarray(d1)
+        out[f"sin_{bc}/d2"] = np.asarray(d2)
+    # non-uniform (interface-fitted) grid: metric path
+    N = 32
+    grid = Grid(GridConfig(ndim=2, N=(N, N), L=(1.0, 1.0), alpha_grid=2.0, eps_g_factor=2.0), be)
+    ccd = CCDSolver(grid, be, bc_type="wall")
+    X, Y = grid.meshgrid()
+    psi = heaviside(np, X - 0.5, 0.5 / N)
+    grid.update_from_levelset(psi, 0.5 / N, ccd=ccd)
+    ccd = CCDSolver(grid, be, bc_type="wall")
+    X, Y = np.meshgrid(grid.coords[0], grid.coords[1], indexing="ij")
+    f = np.sin(np.pi * X) * np.cos(np.pi * Y)
+    out["nonuni/f"] = f
+    for ax in range(2):
+        out[f"nonuni/J{ax}"] = np.asarray(grid.J[ax], dtype=np.float64)
+        out[f"nonuni/dJ{ax}"] = np.asarray(grid.dJ_dxi[ax], dtype=np.float64)
+        out[f"nonuni/coords{ax}"] = np.asarray(grid.coords[ax])
+        d1, d2 = ccd.differentiate(f, ax)
+        out[f"nonuni/d1_ax{ax}"] = np.asarray(d1)
+        out[f"nonuni/d2_ax{ax}"] = np.asarray(d2)
+        out[f"nonuni/first_ax{ax}"] = np.asarray(ccd.first_derivative(f, ax))
+        out[f"nonuni/second_ax{ax}"] = np.asarray(ccd.second_derivative(f, ax))
+        r1, r2 = ccd.differentiate(f, ax, apply_metric=False)
+        out[f"nonuni/raw_d1_ax{ax}"] = np.asarray(r1)
+        out[f"nonuni/raw_d2_ax{ax}"] = np.asarray(r2)
+
+
+def make_ppe(out):
+    from twophase.backend import Backend
+    from twophase.config import SimulationConfig, GridConfig, SolverConfig
+    from twophase.core.grid import Grid
+    from twophase.ccd.ccd_solver import CCDSolver
+    from twophase.ppe.fvm_matrixfree import PPESolverFVMMatrixFree
+    from twophase.ppe.fvm_spsolve import PPESolverFVMSpsolve
+    from twophase.ppe.ccd_ppe_utils import compute_ccd_laplacian, precompute_density_gradients
+    from twophase.linalg_backend import tridiag_variable_batched, _pcr_solve_variable_batched
+
+    sys.path.insert(0, os.path.abspath(os.path.join(HERE, "..", "..")))
+    from twophaseflow_b200.workloads import droplet_density, divergence_rhs
+
+    be = Backend(use_gpu=False)
+
+    def cfg_for(N, **solver):
+        base = dict(ppe_solver_type="fvm_iterative", pseudo_tol=1e-10,
+                    pseudo_maxiter=200, pseudo_c_tau=2.0)
+        base.update(solver)
+        cfg = SimulationConfig(grid=GridConfig(ndim=len(N), N=N, L=(1.0,) * len(N)),
+                               solver=SolverConfig(**{k: v for k, v in base.items()
+                                                      if k in ("ppe_solver_type", "pseudo_tol",
+                                                               "pseudo_maxiter", "pseudo_c_tau")}))
+        for k, v in base.items():
+            if k not in ("ppe_solver_type", "pseudo_tol", "pseudo_maxiter", "pseudo_c_tau"):
+                setattr(cfg.solver, k, v)
+        return cfg
+
+    # (name, N, seed, solver options, density kind)
+    cases = [
+        ("apply2d", (8, 8), 123, {}, "rand"),
+        ("gmres_line2d", (8, 8), 456, {}, "rand"),
+        ("gmres_jac2d", (8, 8), 789, {"ppe_preconditioner": "jacobi"}, "rand"),
+        ("cg_jac2d", (8, 8), 987, {"ppe_iteration_method": "cg", "ppe_preconditioner": "jacobi"}, "rand"),
+        ("cg_jac3d", (6, 7, 5), 11, {"ppe_iteration_method": "cg", "ppe_preconditioner": "jacobi"}, "rand"),
+        ("gmres_line3d", (6, 5, 7), 12, {}, "rand"),
+        ("cg_drop32", (32, 32), 0,
+         {"ppe_iteration_method": "cg", "ppe_preconditioner": "jacobi", "pseudo_tol": 1e-8,
+          "pseudo_maxiter": 20000}, "drop"),
+        ("gmres_drop16", (16, 16), 0,
+         {"pseudo_tol": 1e-8, "pseudo_maxiter": 500}, "drop"),
+        ("cg_rect", (12, 20), 5, {"ppe_iteration_method": "cg", "ppe_preconditioner": "jacobi"}, "rand"),
+    ]
+    for name, N, seed, opts, kind in cases:
+        cfg = cfg_for(N, **opts)
+        grid = Grid(cfg.grid, be)
+        rng = np.random.default_rng(seed)
+        if kind == "rand":
+            rho = 1.0 + rng.uniform(0.0, 1.0, grid.shape)
+            rhs = rng.standard_normal(grid.shape)
+        else:
+            rho = droplet_density(N, seed=seed)
+            rhs = divergence_rhs(N, seed=seed + 1)
+        solver = PPESolverFVMMatrixFree(be, cfg, grid, bc_type="wall")
+        out[f"{name}/N"] = np.array(N)
+        out[f"{name}/rho"] = rho
+        out[f"{name}/rhs"] = rhs
+        out[f"{name}/tol"] = np.array(solver.tol)
+        out[f"{name}/maxiter"] = np.array(solver.maxiter)
+        out[f"{name}/restart"] = np.array(solver.restart)
+        out[f"{name}/method"] = np.array(solver.iteration_method)
+        out[f"{name}/precond"] = np.array(solver.preconditioner)
+        out[f"{name}/pin"] = np.array(solver._pin_dof)
+        # operator apply
+        solver.prepare_operator(rho)
+        p_rand = rng.standard_normal(grid.shape)
+        out[f"{name}/p_rand"] = p_rand
+        out[f"{name}/apply"] = np.asarray(solver.apply(p_rand))
+        # count operator applies inside the reference solve
+        counter = {"n": 0}
+        orig_apply = solver.apply
+
+        def counting_apply(p, _orig=orig_apply):
+            counter["n"] += 1
+            return _orig(p)
+
+        solver.apply = counting_apply
+        p = solver.solve(rhs, rho, dt=1e-3)
+        solver.apply = orig_apply
+        out[f"{name}/p"] = np.asarray(p)
+        out[f"{name}/applies"] = np.array(counter["n"])
+        # preconditioner outputs on a random residual
+        solver._prepare_preconditioner_state(rho)
+        r_rand = rng.standard_normal(grid.shape)
+        out[f"{name}/r_rand"] = r_rand
+        if solver.preconditioner == "line_pcr":
+            out[f"{name}/line_thomas"] = np.asarray(solver.apply_line_preconditioner(r_rand))
+            # the GPU branch (truncated PCR, 4 stages) run through NumPy
+            rw = r_rand.copy()
+            rw.ravel()[solver._pin_dof] = 0.0
+            z = np.zeros_like(rw)
+            for ax, (lo, d, up) in enumerate(solver._precond_coeffs):
+                z += tridiag_variable_batched(np, lo, d, up, rw, ax) * 0.0  # shape check
+                n = rw.shape[ax]
+                mv = lambda a: np.moveaxis(a, ax, 0).reshape(n, -1)
+                x2 = _pcr_solve_variable_batched(np, mv(lo), mv(d), mv(up), mv(rw), max_stages=4)
+                moved = np.moveaxis(rw, ax, 0)
+                z += np.moveaxis(x2.reshape(moved.shape), 0, ax)
+            z /= float(rw.ndim)
+            z.ravel()[solver._pin_dof] = 0.0
+            out[f"{name}/line_pcr4"] = z
+        else:
+            out[f"{name}/jacobi"] = np.asarray(solver.apply_jacobi_preconditioner(r_rand))
+        # exact direct solution
+        direct = PPESolverFVMSpsolve(be, grid, bc_type="wall")
+        out[f"{name}/p_direct"] = np.asarray(direct.solve(rhs, rho, dt=1e-3))
+
+    # CCD variable-density Laplacian L_H (ccd_ppe_utils.compute_ccd_laplacian)
+    for name, N in (("lh2d", (16, 12)), ("lh3d", (8, 9, 10))):
+        grid = Grid(GridConfig(ndim=len(N), N=N, L=(1.0,) * len(N)), be)
+        ccd = CCDSolver(grid, be, bc_type="wall")
+        rng = np.random.default_rng(77)
+        rho = 1.0 + rng.uniform(0.0, 1.0, grid.shape)
+        p = rng.standard_normal(grid.shape)
+        drho = precompute_density_gradients(rho, ccd, be)
+        out[f"{name}/N"] = np.array(N)
+        out[f"{name}/rho"] = rho
+        out[f"{name}/p"] = p
+        out[f"{name}/Lp"] = np.asarray(compute_ccd_laplacian(p, rho, drho, ccd, be))
+
+
+def main():
+    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
+    _ref_import(src)
+    ccd_out, ppe_out = {}, {}
+    make_ccd(ccd_out)
+    make_ppe(ppe_out)
+    np.savez_compressed(os.path.join(HERE, "ccd_golden.npz"), **ccd_out)
+    np.savez_compressed(os.path.join(HERE, "ppe_golden.npz"), **ppe_out)
+    print("wrote", len(ccd_out), "ccd and", len(ppe_out), "ppe arrays")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,230 @@
+"""CCD parity on the GPU: the CUDA line kernels against the reference's own
+outputs (golden fixtures) and the CPU oracle.
+
+Tolerances: FP64 results within 1e-12 of the oracle relative to the field's
+max magnitude (the reference's pivoted dense LU and the block-Thomas chunked
+solve differ only by round-off); FP32 within 2e-5 relative.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import ccd as occd
+from twophaseflow_b200.workloads import fourier_field
+
+pytestmark = pytest.mark.gpu
+
+FP64_RTOL = 1e-12
+FP32_RTOL = 2e-5
+
+
+class _Grid:
+    def __init__(self, N, L, uniform=True, J=None, dJ=None, coords=None):
+        self.N = tuple(int(n) for n in N)
+        self.ndim = len(self.N)
+        self.L = tuple(float(v) for v in L)
+        self.shape = tuple(n + 1 for n in self.N)
+        self.uniform = uniform
+        self.J = J
+        self.dJ_dxi = dJ
+        self.coords = coords if coords is not None else [np.linspace(0, l, n + 1) for n, l in zip(self.N, self.L)]
+
+
+def _close(a, b, rtol):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    scale = max(np.abs(b).max(), 1e-300)
+    err = np.abs(a - b).max() / scale
+    assert err <= rtol, f"max rel err {err:.3e} > {rtol:.1e}"
+
+
+CASES = [("wall2d", "wall"), ("wall3d", "wall"), ("wall2d_big", "wall"), ("per2d", "periodic"),
+         ("per3d", "periodic")]
+
+
+@pytest.mark.parametrize("name,bc", CASES)
+def test_ccd_matches_reference_golden(cuda_device, ccd_golden, name, bc):
+    import torch
+    from twophaseflow_b200 import CCDSolver
+    g = ccd_golden
+    grid = _Grid(g[f"{name}/N"], g[f"{name}/L"])
+    ccd = CCDSolver(grid, None, bc_type=bc)
+    f = torch.from_numpy(g[f"{name}/f"]).to(cuda_device)
+    for ax in range(grid.ndim):
+        d1, d2 = ccd.differentiate(f, ax)
+        _close(d1.cpu().numpy(), g[f"{name}/d1_ax{ax}"], FP64_RTOL)
+        _close(d2.cpu().numpy(), g[f"{name}/d2_ax{ax}"], FP64_RTOL)
+        _close(ccd.first_derivative(f, ax).cpu().numpy(), g[f"{name}/first_ax{ax}"], FP64_RTOL)
+        _close(ccd.second_derivative(f, ax).cpu().numpy(), g[f"{name}/second_ax{ax}"], FP64_RTOL)
+
+
+@pytest.mark.parametrize("name", ["wall2d", "wall3d", "wall2d_big"])
+def test_ccd_bc_override(cuda_device, ccd_golden, name):
+    from twophaseflow_b200 import CCDSolver
+    g = ccd_golden
+    grid = _Grid(g[f"{name}/N"], g[f"{name}/L"])
+    ccd = CCDSolver(grid, None, bc_type="wall")
+    d1, d2 = ccd.differentiate(g[f"{name}/f"], 0, bc_left=(0.3, -1.2), bc_right=(0.0, 2.5))
+    assert isinstance(d1, np.ndarray)   # NumPy in -> NumPy out
+    _close(d1, g[f"{name}/bcov_d1"], FP64_RTOL)
+    _close(d2, g[f"{name}/bcov_d2"], FP64_RTOL)
+    # one-sided override: the other side keeps the compact closure
+    h = float(g[f"{name}/L"][0]) / float(g[f"{name}/N"][0])
+    o1, o2 = occd.differentiate(g[f"{name}/f"], 0, h, bc_left=(0.3, -1.2))
+    d1, d2 = ccd.differentiate(g[f"{name}/f"], 0, bc_left=(0.3, -1.2))
+    _close(d1, o1, FP64_RTOL)
+    _close(d2, o2, FP64_RTOL)
+
+
+@pytest.mark.parametrize("bc", ["wall", "periodic"])
+def test_ccd_sin_reference_case(cuda_device, ccd_golden, bc):
+    from twophaseflow_b200 import CCDSolver
+    g = ccd_golden
+    grid = _Grid((32, 4), (1.0, 1.0))
+    ccd = CCDSolver(grid, None, bc_type=bc)
+    d1, d2 = ccd.differentiate(g[f"sin_{bc}/f"], 0)
+    _close(d1, g[f"sin_{bc}/d1"], FP64_RTOL)
+    _close(d2, g[f"sin_{bc}/d2"], FP64_RTOL)
+    if bc == "periodic":
+        # image node equals node 0 (test_ccd.py:65-81)
+        np.testing.assert_allclose(d1[-1], d1[0], atol=1e-12)
+
+
+def test_ccd_nonuniform_metric(cuda_device, ccd_golden):
+    from twophaseflow_b200 import CCDSolver
+    g = ccd_golden
+    J = [g["nonuni/J0"], g["nonuni/J1"]]
+    dJ = [g["nonuni/dJ0"], g["nonuni/dJ1"]]
+    grid = _Grid((32, 32), (1.0, 1.0), uniform=False, J=J, dJ=dJ,
+                 coords=[g["nonuni/coords0"], g["nonuni/coords1"]])
+    ccd = CCDSolver(grid, None, bc_type="wall")
+    f = g["nonuni/f"]
+    for ax in range(2):
+        d1, d2 = ccd.differentiate(f, ax)
+        _close(d1, g[f"nonuni/d1_ax{ax}"], 1e-11)
+        _close(d2, g[f"nonuni/d2_ax{ax}"], 1e-11)
+        _close(ccd.first_derivative(f, ax), g[f"nonuni/first_ax{ax}"], 1e-11)
+        _close(ccd.second_derivative(f, ax), g[f"nonuni/second_ax{ax}"], 1e-11)
+        r1, r2 = ccd.differentiate(f, ax, apply_metric=False)
+        _close(r1, g[f"nonuni/raw_d1_ax{ax}"], FP64_RTOL)
+        _close(r2, g[f"nonuni/raw_d2_ax{ax}"], FP64_RTOL)
+
+
+@pytest.mark.parametrize("n", [6, 7, 9, 17, 33, 34, 65, 100, 129, 257, 300, 1025, 1500])
+@pytest.mark.parametrize("bc", ["wall", "periodic"])
+def test_ccd_line_lengths(cuda_device, n, bc):
+    """Ragged lengths around the chunk size, single-chunk and many-chunk lines,
+    batches that are not a multiple of the CTA's line count."""
+    import torch
+    from twophaseflow_b200 import CCDSolver
+    rng = np.random.default_rng(n)
+    for shape, ax in [((n, 3), 0), ((5, n), 1), ((3, n, 7), 1), ((2, 3, n), 2)]:
+        N = tuple(s - 1 for s in shape)
+        grid = _Grid(N, tuple(1.0 + 0.1 * i for i in range(len(N))))
+        ccd = CCDSolver(grid, None, bc_type=bc)
+        f = rng.standard_normal(shape)
+        h = grid.L[ax] / N[ax]
+        o1, o2 = occd.differentiate(f, ax, h, bc=bc)
+        d1, d2 = ccd.differentiate(torch.from_numpy(f).to(cuda_device), ax)
+        _close(d1.cpu().numpy(), o1, FP64_RTOL)
+        _close(d2.cpu().numpy(), o2, FP64_RTOL)
+
+
+@pytest.mark.parametrize("bc", ["wall", "periodic"])
+def test_ccd_fp32(cuda_device, bc):
+    import torch
+    from twophaseflow_b200 import CCDSolver
+    N = (256, 200)
+    grid = _Grid(N, (1.0, 1.0))
+    f = fourier_field(N, n_modes=8, kmax=8, seed=3)
+    ccd32 = CCDSolver(grid, None, bc_type=bc, dtype=torch.float32)
+    for ax in range(2):
+        h = 1.0 / N[ax]
+        o1, o2 = occd.differentiate(f, ax, h, bc=bc)
+        d1, d2 = ccd32.differentiate(torch.from_numpy(f).to(cuda_device), ax)
+        assert d1.dtype == torch.float32
+        _close(d1.double().cpu().numpy(), o1, FP32_RTOL)
+        _close(d2.double().cpu().numpy(), o2, 10 * FP32_RTOL)
+
+
+def test_ccd_full_size_2d_against_oracle(cuda_device):
+    """Workload size: 2-D 1025^2 Fourier field, wall and periodic, both axes."""
+    import torch
+    from twophaseflow_b200 import CCDSolver
+    N = (1024, 1024)
+    grid = _Grid(N, (1.0, 1.0))
+    f = fourier_field(N, seed=0)
+    ft = torch.from_numpy(f).to(cuda_device)
+    for bc in ("wall", "periodic"):
+        ccd = CCDSolver(grid, None, bc_type=bc)
+        for ax in range(2):
+            o1, o2 = occd.differentiate(f, ax, 1.0 / 1024, bc=bc)
+            d1, d2 = ccd.differentiate(ft, ax)
+            _close(d1.cpu().numpy(), o1, FP64_RTOL)
+            _close(d2.cpu().numpy(), o2, FP64_RTOL)
+
+
+def test_ccd_full_size_3d_properties(cuda_device):
+    """3-D 257^3: exact derivatives of a low-degree polynomial (the scheme is
+    exact for cubics, test_ccd.py:201-252) and axis consistency."""
+    import torch
+    from twophaseflow_b200 import CCDSolver
+    N = (256, 256, 256)
+    grid = _Grid(N, (1.0, 1.0, 1.0))
+    x = torch.linspace(0, 1, 257, dtype=torch.float64, device=cuda_device)
+    X = x.view(-1, 1, 1)
+    Y = x.view(1, -1, 1)
+    Z = x.view(1, 1, -1)
+    f = (X ** 3 * Y ** 2 + Z ** 3).expand(257, 257, 257).contiguous()
+    ccd = CCDSolver(grid, None, bc_type="wall")
+    d1, d2 = ccd.differentiate(f, 0)
+    assert torch.max(torch.abs(d1 - 3 * X ** 2 * Y ** 2)).item() < 1e-9
+    assert torch.max(torch.abs(d2 - 6 * X * Y ** 2)).item() < 1e-7
+    d1, d2 = ccd.differentiate(f, 2)
+    assert torch.max(torch.abs(d1 - 3 * Z ** 2)).item() < 1e-9
+    d1, _ = ccd.differentiate(f, 1)
+    assert torch.max(torch.abs(d1 - 2 * X ** 3 * Y)).item() < 1e-9
+
+
+def test_ccd_oracle_3d_slab(cuda_device):
+    """3-D wall/periodic against the oracle on a 257 x 40 x 257 slab (all axes)."""
+    import torch
+    from twophaseflow_b200 import CCDSolver
+    N = (256, 39, 256)
+    grid = _Grid(N, (1.0, 0.5, 2.0))
+    f = fourier_field(N, L=grid.L, n_modes=8, kmax=16, seed=5)
+    ft = torch.from_numpy(f).to(cuda_device)
+    for bc in ("wall", "periodic"):
+        ccd = CCDSolver(grid, None, bc_type=bc)
+        for ax in range(3):
+            o1, o2 = occd.differentiate(f, ax, grid.L[ax] / N[ax], bc=bc)
+            d1, d2 = ccd.differentiate(ft, ax)
+            _close(d1.cpu().numpy(), o1, FP64_RTOL)
+            _close(d2.cpu().numpy(), o2, FP64_RTOL)
+
+
+def test_differentiate_raw_and_neumann(cuda_device):
+    import torch
+    from twophaseflow_b200 import CCDSolver
+    N = (40, 24)
+    grid = _Grid(N, (1.0, 1.0))
+    ccd = CCDSolver(grid, None, bc_type="wall")
+    x = np.linspace(0.0, 1.0, 41) ** 1.3
+    d1, d2 = ccd.differentiate_raw(x, 0)
+    o1, o2 = occd.differentiate_wall(x[:, None], 0, 1.0 / 40)
+    _close(d1, o1[:, 0], FP64_RTOL)
+    _close(d2, o2[:, 0], FP64_RTOL)
+    gt = torch.ones((41, 25), dtype=torch.float64, device=cuda_device)
+    ccd.enforce_wall_neumann(gt, 1)
+    assert gt[:, 0].abs().max().item() == 0 and gt[:, -1].abs().max().item() == 0
+    assert gt[:, 1:-1].min().item() == 1.0
+
+
+def test_ccd_rejects_short_wall_axis(cuda_device):
+    from twophaseflow_b200 import CCDSolver
+    grid = _Grid((4, 4), (1.0, 1.0))
+    ccd = CCDSolver(grid, None, bc_type="wall")
+    with pytest.raises(ValueError, match="n_pts >= 6"):
+        ccd.differentiate(np.zeros(grid.shape), axis=0)

@@ -1,0 +1,25 @@
+"""twophaseflow_b200: B200 (sm_100a) implementation of TwoPhaseFlow's hot path.
+
+* ``CCDSolver`` -- drop-in for ``twophase.ccd.ccd_solver.CCDSolver``
+* ``PPESolverFVMMatrixFree`` -- drop-in for
+  ``twophase.ppe.fvm_matrixfree.PPESolverFVMMatrixFree`` (an ``IPPESolver``)
+* ``register_with_reference`` -- installs the PPE solver in the reference's
+  ``register_ppe_solver`` registry.
+
+All arithmetic runs in the in-tree CUDA library ``libtpf.so`` (C ABI:
+``include/tpf.h``); build it with ``python -m twophaseflow_b200.build``.
+"""
+
+from .ccd import CCDSolver
+from .grid import BoundarySpec, UniformGrid
+from .ppe import MatrixAssemblyUnavailable, PPESolverFVMMatrixFree, create_fvm_matrixfree, register_with_reference
+
+__all__ = [
+    "CCDSolver",
+    "PPESolverFVMMatrixFree",
+    "MatrixAssemblyUnavailable",
+    "create_fvm_matrixfree",
+    "register_with_reference",
+    "UniformGrid",
+    "BoundarySpec",
+]

@@ -1,0 +1,125 @@
+"""ctypes binding of the in-tree CUDA library ``libtpf.so`` (C ABI in include/tpf.h).
+
+The library is the only compute path: if it is missing or no CUDA device is
+visible, every entry point raises.  There is no CPU fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtpf.so")
+
+TPF_OK, TPF_EINVAL, TPF_ENOCONV, TPF_ECUDA, TPF_EABORT, TPF_ESINGULAR = range(6)
+TPF_F64, TPF_F32 = 0, 1
+TPF_BC_WALL, TPF_BC_PERIODIC = 0, 1
+TPF_CCD_APPLY_METRIC = 1
+TPF_PPE_CG, TPF_PPE_GMRES = 0, 1
+TPF_PRECOND_NONE, TPF_PRECOND_JACOBI, TPF_PRECOND_LINE, TPF_PRECOND_LINE_PCR = range(4)
+TPF_PREC_F64, TPF_PREC_MIXED = 0, 1
+
+
+class tpf_ppe_options(C.Structure):
+    _fields_ = [
+        ("method", C.c_int),
+        ("precond", C.c_int),
+        ("precision", C.c_int),
+        ("tol", C.c_double),
+        ("maxiter", C.c_int64),
+        ("restart", C.c_int),
+        ("c_tau", C.c_double),
+        ("pcr_stages", C.c_int),
+        ("inner_tol", C.c_double),
+        ("max_refine", C.c_int64),
+    ]
+
+
+class tpf_ppe_result(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int64),
+        ("applies", C.c_int64),
+        ("refinements", C.c_int64),
+        ("rel_residual", C.c_double),
+        ("info", C.c_int),
+    ]
+
+
+# name -> (restype, argtypes); every function declared in include/tpf.h
+SIGNATURES = {
+    "tpf_version": (C.c_int, []),
+    "tpf_last_error": (C.c_char_p, []),
+    "tpf_ccd_plan_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int64, C.c_double, C.c_int, C.c_int]),
+    "tpf_ccd_plan_destroy": (C.c_int, [C.c_void_p]),
+    "tpf_ccd_plan_set_metric": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "tpf_ccd_apply": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int, C.c_void_p]),
+    "tpf_ccd_enforce_wall_neumann": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]),
+    "tpf_ppe_default_options": (None, [C.POINTER(tpf_ppe_options)]),
+    "tpf_ppe_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_int64),
+                                 C.POINTER(C.POINTER(C.c_double)), C.c_int64, C.POINTER(tpf_ppe_options)]),
+    "tpf_ppe_destroy": (C.c_int, [C.c_void_p]),
+    "tpf_ppe_set_options": (C.c_int, [C.c_void_p, C.POINTER(tpf_ppe_options)]),
+    "tpf_ppe_prepare": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tpf_ppe_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tpf_ppe_precondition": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tpf_ppe_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                C.POINTER(tpf_ppe_result)]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+class LibraryNotBuilt(RuntimeError):
+    pass
+
+
+def load(path: str | None = None):
+    """Load libtpf.so (once) and attach prototypes.  Raises if it is missing."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        p = path or LIB_PATH
+        if not os.path.exists(p):
+            raise LibraryNotBuilt(
+                f"{p} is missing: build it with `python -m twophaseflow_b200.build` "
+                "(the CUDA library is the only compute path; there is no CPU fallback)")
+        lib = C.CDLL(p)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def last_error() -> str:
+    msg = load().tpf_last_error()
+    return msg.decode() if msg else ""
+
+
+def check(status: int, what: str = ""):
+    """Map a tpf status code to the reference's exception types."""
+    if status == TPF_OK:
+        return
+    msg = last_error() or what
+    if status == TPF_EINVAL:
+        raise ValueError(msg)
+    if status == TPF_ESINGULAR:
+        raise np.linalg.LinAlgError(msg)
+    raise RuntimeError(msg)
+
+
+def dptr(t) -> C.c_void_p:
+    return C.c_void_p(int(t.data_ptr()))
+
+
+def current_stream_handle():
+    import torch
+    return C.c_void_p(int(torch.cuda.current_stream().cuda_stream))

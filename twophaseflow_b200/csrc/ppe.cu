@@ -1,0 +1,1243 @@
+// Variable-density FVM pressure-Poisson solve for sm_100a.
+//
+// Operator (reference src/twophase/ppe/fvm_matrixfree.py:281-300,
+// fvm_matrixfree_helpers.py:46-73): harmonic face coefficient
+// cf = 2/(rho_L + rho_R)/d_face, L p = sum_a [cf(i-e_a)(p_{i-e_a}-p_i) +
+// cf(i)(p_{i+e_a}-p_i)] / dv_a, pinned row out[pin] = p[pin].
+// The CG route solves the control-volume-weighted SPD system S p = -W rhs,
+// S = -W L with column/row pin (fvm_matrixfree.py:167-215), whose symmetric
+// face couplings s_a = cf * prod_{b != a} dv_b are stored per face.
+//
+// Kernels:
+//  * prepare: face couplings (FP64 + FP32 copies), Jacobi diagonals, shifted
+//    line-preconditioner coefficients and their Thomas factors.
+//  * persistent cooperative PCG: the whole Jacobi-PCG loop of SciPy's cg
+//    (restated: stop when ||r|| < tol ||b|| at the top of an iteration) runs in
+//    ONE launch; two grid-wide reductions per iteration through a bounded grid
+//    barrier, the p-update is fused into the stencil (neighbour p_new values
+//    are recomputed from z and p_old), scalars never leave the device.
+//  * mixed precision: the same loop in FP32 (dots in FP64) as the inner solve
+//    of an FP64 iterative-refinement loop, also one launch.
+//  * GMRES (SciPy's left-preconditioned restarted GMRES with its gh-8400
+//    inner tolerance control) driven from the host with the Hessenberg /
+//    Givens state on the device; classical Gram-Schmidt with
+//    re-orthogonalization replaces modified Gram-Schmidt.
+#include "tpf_common.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+namespace {
+
+constexpr int kThreads = 512;
+constexpr long long kSpinLimit = 4000000;  // polls per barrier wait (~seconds)
+
+struct Grid3 {
+  int n0, n1, n2;   // nodes per axis (n2 = 1 in 2-D)
+  int N0, N1, N2;   // cells per axis (N2 = 0 in 2-D)
+  int st0;          // n1 * n2
+  int ndof;
+  int pin;
+};
+
+__device__ __forceinline__ void coords3(const Grid3& g, int idx, int& i0, int& i1, int& i2) {
+  i0 = idx / g.st0;
+  int r = idx - i0 * g.st0;
+  i1 = r / g.n2;
+  i2 = r - i1 * g.n2;
+}
+
+struct Geo {
+  const double* dv[3];     // node control-volume widths
+  const double* dface[3];  // face widths
+};
+
+// S p at node idx (pin column treated as zero when ZERO_PIN, pin row identity
+// handled by the caller).  s[a] are the symmetric face couplings.
+template <typename T, typename PF>
+__device__ __forceinline__ void s_row(const Grid3& g, int idx, int i0, int i1, int i2,
+                                      const T* __restrict__ s0, const T* __restrict__ s1,
+                                      const T* __restrict__ s2, PF pv, T& diag, T& off) {
+  T d = T(0), acc = T(0);
+  if (i0 > 0) { T s = s0[idx - g.st0]; d += s; acc += s * pv(idx - g.st0); }
+  if (i0 < g.N0) { T s = s0[idx]; d += s; acc += s * pv(idx + g.st0); }
+  if (i1 > 0) { T s = s1[idx - g.n2]; d += s; acc += s * pv(idx - g.n2); }
+  if (i1 < g.N1) { T s = s1[idx]; d += s; acc += s * pv(idx + g.n2); }
+  if (g.N2 > 0) {
+    if (i2 > 0) { T s = s2[idx - 1]; d += s; acc += s * pv(idx - 1); }
+    if (i2 < g.N2) { T s = s2[idx]; d += s; acc += s * pv(idx + 1); }
+  }
+  diag = d;
+  off = acc;
+}
+
+// ---- prepare ---------------------------------------------------------------
+
+struct PrepArgs {
+  Grid3 g;
+  Geo geo;
+  const double* rho;
+  double* s[3];
+  float* s32[3];
+  double* dinvS;       // 1/diag(S), pin -> 1
+  float* dinvS32;
+  double* dinvL;       // reference Jacobi diag_inv of the unweighted operator
+  double* tlo[3];      // shifted line system: lower coefficient
+  double* tdg[3];      // diagonal (later overwritten by Thomas denominators)
+  double* tup[3];      // upper (later overwritten by Thomas c')
+  double shift_scale;  // 2/(c_tau h_min^2)
+  int ndim;
+  int want_line;
+};
+
+__global__ void prep_faces_kernel(PrepArgs a) {
+  const Grid3& g = a.g;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < g.ndof; idx += gridDim.x * blockDim.x) {
+    int i0, i1, i2;
+    coords3(g, idx, i0, i1, i2);
+    const int iv[3] = {i0, i1, i2};
+    const int Nv[3] = {g.N0, g.N1, g.N2};
+    const int stv[3] = {g.st0, g.n2, 1};
+    const double rho_i = a.rho[idx];
+    double dvv[3] = {a.geo.dv[0][i0], a.geo.dv[1][i1], g.N2 > 0 ? a.geo.dv[2][i2] : 1.0};
+    double diagS = 0.0, diagL = 0.0;
+    for (int ax = 0; ax < 3; ++ax) {
+      if (Nv[ax] == 0) continue;
+      double other = 1.0;
+      for (int b = 0; b < 3; ++b)
+        if (b != ax) other *= dvv[b];
+      double lower = 0.0, upper = 0.0, cf_lo = 0.0, cf_hi = 0.0;
+      if (iv[ax] > 0) {
+        double rl = a.rho[idx - stv[ax]];
+        cf_lo = 2.0 / (rl + rho_i) / a.geo.dface[ax][iv[ax] - 1];
+        lower = cf_lo / dvv[ax];
+      }
+      if (iv[ax] < Nv[ax]) {
+        double rr = a.rho[idx + stv[ax]];
+        cf_hi = 2.0 / (rho_i + rr) / a.geo.dface[ax][iv[ax]];
+        upper = cf_hi / dvv[ax];
+        double sv = cf_hi * other;
+        a.s[ax][idx] = sv;
+        a.s32[ax][idx] = (float)sv;
+      } else {
+        a.s[ax][idx] = 0.0;
+        a.s32[ax][idx] = 0.0f;
+      }
+      diagS += cf_lo * other + cf_hi * other;
+      double main = -(lower + upper);
+      diagL += main;
+      if (a.want_line) {
+        double shift = a.shift_scale / rho_i;
+        a.tlo[ax][idx] = -lower;
+        a.tdg[ax][idx] = shift - main;
+        a.tup[ax][idx] = -upper;
+      }
+    }
+    if (idx == g.pin) {
+      diagS = 1.0;
+      diagL = 1.0;
+    }
+    a.dinvS[idx] = 1.0 / diagS;
+    a.dinvS32[idx] = (float)(1.0 / diagS);
+    a.dinvL[idx] = 1.0 / (fabs(diagL) > 1e-30 ? diagL : 1.0);
+  }
+}
+
+struct LineArgs {
+  int lines, n;              // number of lines, points per line
+  int stride;                // element stride along the line
+  int lstride_hi, lmod;      // line -> base: (l / lmod) * lstride_hi + (l % lmod) * lstride_lo
+  int lstride_lo;
+};
+
+__device__ __forceinline__ int line_base(const LineArgs& L, int l) {
+  return (l / L.lmod) * L.lstride_hi + (l % L.lmod) * L.lstride_lo;
+}
+
+// Thomas factors along lines: tdg -> denominators, tup -> c' (the reference's
+// CPU recurrence, linalg_backend.py:496-507, with the coefficient part hoisted).
+__global__ void thomas_factor_kernel(LineArgs L, const double* lo, double* dg, double* up) {
+  int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= L.lines) return;
+  int b = line_base(L, l);
+  double den = dg[b];
+  double cp = (L.n > 1) ? up[b] / den : 0.0;
+  up[b] = cp;
+  for (int i = 1; i < L.n; ++i) {
+    int e = b + i * L.stride;
+    den = dg[e] - lo[e] * cp;
+    dg[e] = den;
+    cp = (i < L.n - 1) ? up[e] / den : 0.0;
+    up[e] = cp;
+  }
+}
+
+// x = T^-1 r along lines, with r[pin] read as 0.  ACC: out = (out + x) * scale.
+template <bool ACC>
+__global__ void thomas_solve_kernel(LineArgs L, const double* __restrict__ lo, const double* __restrict__ den,
+                                    const double* __restrict__ cp, const double* __restrict__ r, double* out,
+                                    double* tmp, int pin, double scale, const int* done) {
+  if (done && *done) return;
+  int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= L.lines) return;
+  int b = line_base(L, l);
+  // forward: dp_i = (r_i - lo_i dp_{i-1}) / den_i   (stored in tmp)
+  double dp = 0.0;
+  for (int i = 0; i < L.n; ++i) {
+    int e = b + i * L.stride;
+    double ri = (e == pin) ? 0.0 : r[e];
+    dp = (i == 0) ? ri / den[e] : (ri - lo[e] * dp) / den[e];
+    tmp[e] = dp;
+  }
+  double x = 0.0;
+  for (int i = L.n - 1; i >= 0; --i) {
+    int e = b + i * L.stride;
+    x = (i == L.n - 1) ? tmp[e] : tmp[e] - cp[e] * x;
+    if (ACC) {
+      double v = (out[e] + x) * scale;
+      out[e] = (e == pin) ? 0.0 : v;
+    } else {
+      out[e] = x;
+    }
+  }
+}
+
+// ---- elementwise helpers ------------------------------------------------------
+
+// L p (reference apply): -(S p)/W for rows != pin (pin column kept), pin row identity.
+__global__ void apply_L_kernel(Grid3 g, Geo geo, const double* s0, const double* s1, const double* s2,
+                               const double* __restrict__ p, double* out, const double* bsub,
+                               const int* done) {
+  if (done && *done) return;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < g.ndof; idx += gridDim.x * blockDim.x) {
+    int i0, i1, i2;
+    coords3(g, idx, i0, i1, i2);
+    double v;
+    if (idx == g.pin) {
+      v = p[idx];
+    } else {
+      double d, off;
+      s_row<double>(g, idx, i0, i1, i2, s0, s1, s2, [&](int j) { return p[j]; }, d, off);
+      double W = geo.dv[0][i0] * geo.dv[1][i1] * (g.N2 > 0 ? geo.dv[2][i2] : 1.0);
+      v = (off - d * p[idx]) / W;
+    }
+    out[idx] = bsub ? bsub[idx] - v : v;   // optional residual b - L p
+  }
+}
+
+// weighted rhs of the CG system: b = -W rhs, b[pin] = 0; x0 from p_init (pin -> 0)
+__global__ void cg_rhs_kernel(Grid3 g, Geo geo, const double* rhs, double* b, const double* p_init,
+                              double* x) {
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < g.ndof; idx += gridDim.x * blockDim.x) {
+    int i0, i1, i2;
+    coords3(g, idx, i0, i1, i2);
+    double W = geo.dv[0][i0] * geo.dv[1][i1] * (g.N2 > 0 ? geo.dv[2][i2] : 1.0);
+    b[idx] = (idx == g.pin) ? 0.0 : -(rhs[idx] * W);
+    x[idx] = (p_init && idx != g.pin) ? p_init[idx] : 0.0;
+  }
+}
+
+__global__ void jacobi_L_kernel(int ndof, int pin, const double* dinvL, const double* r, double* z,
+                                const int* done) {
+  if (done && *done) return;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += gridDim.x * blockDim.x)
+    z[idx] = (idx == pin) ? 0.0 : r[idx] * dinvL[idx];
+}
+
+__global__ void copy_pin0_kernel(int ndof, int pin, const double* src, double* dst) {
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += gridDim.x * blockDim.x)
+    dst[idx] = (idx == pin) ? 0.0 : src[idx];
+}
+
+// ---- persistent PCG --------------------------------------------------------------
+
+struct SolveStatus {
+  long long iters;
+  long long applies;
+  long long refinements;
+  double rr;          // final ||r||^2 of the solved system
+  double bb;          // ||b||^2
+  int converged;
+  int pad;
+};
+
+template <typename T>
+struct PcgVecs {
+  const T* s0; const T* s1; const T* s2;
+  const T* dinv;
+  T* x; T* r; T* z; T* p0; T* p1; T* q;
+};
+
+struct PcgArgs {
+  Grid3 g;
+  PcgVecs<double> v64;
+  PcgVecs<float> v32;
+  const double* b;        // SPD-system rhs (FP64)
+  double* x64;            // FP64 solution (mixed) / unused
+  double* r64;
+  long long maxiter;      // CG iterations (plain) / inner iterations per sweep (mixed)
+  long long max_refine;
+  double tol;             // relative tolerance on ||r||/||b||
+  double inner_tol;       // mixed: relative tolerance of each FP32 inner solve
+  int x_nonzero;
+  double* part;           // [4][nblocks] partial sums
+  unsigned int* bar;
+  int* err;
+  SolveStatus* st;
+};
+
+struct GridCtx {
+  tpf::GridBarrier gb;
+  double* part;
+  unsigned nb;
+  __device__ __forceinline__ bool reduce(double (&v)[2], int site, double* scratch) {
+    tpf::block_sum<2>(v, scratch);
+    if (threadIdx.x == 0) {
+      part[(site * 2 + 0) * nb + blockIdx.x] = v[0];
+      part[(site * 2 + 1) * nb + blockIdx.x] = v[1];
+    }
+    if (!gb.sync(nb)) return false;
+    // every block sums the partials in the same order -> identical scalars
+    double a0 = 0.0, a1 = 0.0;
+    if (threadIdx.x < 32) {
+      for (unsigned k = threadIdx.x; k < nb; k += 32) {
+        a0 += ((volatile double*)part)[(site * 2 + 0) * nb + k];
+        a1 += ((volatile double*)part)[(site * 2 + 1) * nb + k];
+      }
+      a0 = tpf::warp_sum(a0);
+      a1 = tpf::warp_sum(a1);
+      if (threadIdx.x == 0) { scratch[128] = a0; scratch[129] = a1; }
+    }
+    __syncthreads();
+    v[0] = scratch[128];
+    v[1] = scratch[129];
+    __syncthreads();
+    return true;
+  }
+};
+
+// One PCG solve on S x = r_in (the vectors of `v`), SciPy cg semantics.
+// On entry r holds the residual of the current x and z = dinv r has NOT been
+// formed.  Returns iterations; sets *conv.  atol2 = (tol * ||b||)^2.
+template <typename T>
+__device__ long long pcg_loop(const Grid3& g, const PcgVecs<T>& v, long long maxiter, double atol2,
+                              GridCtx& ctx, double* scratch, int site_base, bool& conv, bool& ok,
+                              double& rr_out) {
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int G = gridDim.x * blockDim.x;
+  // phase A0: z = dinv r, rr, rz
+  double red[2] = {0.0, 0.0};
+  for (int idx = gtid; idx < g.ndof; idx += G) {
+    T r = v.r[idx];
+    T z = v.dinv[idx] * r;
+    v.z[idx] = z;
+    v.p0[idx] = T(0);
+    red[0] += (double)r * (double)r;
+    red[1] += (double)r * (double)z;
+  }
+  ok = ctx.reduce(red, site_base, scratch);
+  double rr = red[0], rz = red[1], rz_prev = 1.0;
+  T* pc = v.p0;
+  T* pn = v.p1;
+  long long it = 0;
+  conv = false;
+  while (ok) {
+    if (rr < atol2) { conv = true; break; }
+    if (it >= maxiter) break;
+    const T beta = (it > 0) ? (T)(rz / rz_prev) : T(0);
+    // phase B: p_new = z + beta p ; q = S p_new ; pq
+    double pq[2] = {0.0, 0.0};
+    for (int idx = gtid; idx < g.ndof; idx += G) {
+      int i0, i1, i2;
+      coords3(g, idx, i0, i1, i2);
+      auto pnew = [&](int j) -> T { return (j == g.pin) ? T(0) : v.z[j] + beta * pc[j]; };
+      T pi = v.z[idx] + beta * pc[idx];
+      T qi;
+      if (idx == g.pin) {
+        qi = pi;
+      } else {
+        T d, off;
+        s_row<T>(g, idx, i0, i1, i2, v.s0, v.s1, v.s2, pnew, d, off);
+        qi = d * pi - off;
+      }
+      pn[idx] = pi;
+      v.q[idx] = qi;
+      pq[0] += (double)pi * (double)qi;
+    }
+    ok = ctx.reduce(pq, site_base + 1, scratch);
+    if (!ok) break;
+    const double alpha_d = rz / pq[0];
+    const T alpha = (T)alpha_d;
+    // phase A: x += alpha p ; r -= alpha q ; z = dinv r ; rr, rz
+    red[0] = red[1] = 0.0;
+    for (int idx = gtid; idx < g.ndof; idx += G) {
+      T pi = pn[idx];
+      v.x[idx] += alpha * pi;
+      T r = v.r[idx] - alpha * v.q[idx];
+      v.r[idx] = r;
+      T z = v.dinv[idx] * r;
+      v.z[idx] = z;
+      red[0] += (double)r * (double)r;
+      red[1] += (double)r * (double)z;
+    }
+    ok = ctx.reduce(red, site_base, scratch);
+    rz_prev = rz;
+    rr = red[0];
+    rz = red[1];
+    T* t = pc; pc = pn; pn = t;
+    ++it;
+  }
+  rr_out = rr;
+  return it;
+}
+
+// Plain FP64 PCG: the whole SciPy-cg loop in one cooperative launch.
+__global__ void __launch_bounds__(kThreads) pcg64_kernel(PcgArgs a) {
+  __shared__ double scratch[160];
+  GridCtx ctx{tpf::GridBarrier{a.bar, a.err, kSpinLimit}, a.part, gridDim.x};
+  const Grid3& g = a.g;
+  const PcgVecs<double>& v = a.v64;
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int G = gridDim.x * blockDim.x;
+  // r = b - S x  (x read-only here; S with the pin column zeroed, pin row identity)
+  double bbv[2] = {0.0, 0.0};
+  for (int idx = gtid; idx < g.ndof; idx += G) {
+    double bi = a.b[idx];
+    double r = bi;
+    if (a.x_nonzero) {
+      double sx;
+      if (idx == g.pin) sx = v.x[idx];
+      else {
+        int i0, i1, i2;
+        coords3(g, idx, i0, i1, i2);
+        double d, off;
+        s_row<double>(g, idx, i0, i1, i2, v.s0, v.s1, v.s2,
+                      [&](int j) { return (j == g.pin) ? 0.0 : v.x[j]; }, d, off);
+        sx = d * v.x[idx] - off;
+      }
+      r = bi - sx;
+    }
+    v.r[idx] = r;
+    bbv[0] += bi * bi;
+  }
+  bool ok = ctx.reduce(bbv, 2, scratch);
+  if (!ok) return;
+  const double bb = bbv[0];
+  if (bb == 0.0) {
+    for (int idx = gtid; idx < g.ndof; idx += G) v.x[idx] = 0.0;
+    if (gtid == 0) { a.st->iters = 0; a.st->applies = 0; a.st->rr = 0.0; a.st->bb = 0.0; a.st->converged = 1; }
+    return;
+  }
+  const double atol2 = (a.tol * sqrt(bb)) * (a.tol * sqrt(bb));
+  bool conv = false;
+  double rr = 0.0;
+  long long it = pcg_loop<double>(g, v, a.maxiter, atol2, ctx, scratch, 0, conv, ok, rr);
+  if (gtid == 0) {
+    a.st->iters = it;
+    a.st->applies = it + (a.x_nonzero ? 1 : 0);
+    a.st->refinements = 0;
+    a.st->rr = rr;
+    a.st->bb = bb;
+    a.st->converged = conv ? 1 : 0;
+  }
+}
+
+// Mixed precision: FP64 residual / update, FP32 inner PCG (dots in FP64).
+__global__ void __launch_bounds__(kThreads) pcg_mixed_kernel(PcgArgs a) {
+  __shared__ double scratch[160];
+  GridCtx ctx{tpf::GridBarrier{a.bar, a.err, kSpinLimit}, a.part, gridDim.x};
+  const Grid3& g = a.g;
+  const PcgVecs<double>& v = a.v64;
+  const PcgVecs<float>& w = a.v32;
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int G = gridDim.x * blockDim.x;
+  double bb = -1.0, rr = 0.0;
+  long long inner_total = 0, sweeps = 0;
+  bool conv = false, ok = true;
+  double atol2 = 0.0;
+  for (;;) {
+    // FP64 residual of the current x64: r64 = b - S x64
+    double red[2] = {0.0, 0.0};
+    for (int idx = gtid; idx < g.ndof; idx += G) {
+      double bi = a.b[idx];
+      double sx;
+      if (idx == g.pin) sx = v.x[idx];
+      else {
+        int i0, i1, i2;
+        coords3(g, idx, i0, i1, i2);
+        double d, off;
+        s_row<double>(g, idx, i0, i1, i2, v.s0, v.s1, v.s2,
+                      [&](int j) { return (j == g.pin) ? 0.0 : v.x[j]; }, d, off);
+        sx = d * v.x[idx] - off;
+      }
+      double r = bi - sx;
+      v.r[idx] = r;
+      red[0] += r * r;
+      red[1] += bi * bi;
+    }
+    ok = ctx.reduce(red, 2, scratch);
+    if (!ok) break;
+    rr = red[0];
+    if (bb < 0.0) {
+      bb = red[1];
+      atol2 = (a.tol * sqrt(bb)) * (a.tol * sqrt(bb));
+      if (bb == 0.0) { conv = true; break; }
+    }
+    if (rr < atol2) { conv = true; break; }
+    if (sweeps >= a.max_refine) break;
+    // FP32 inner solve on the normalized residual
+    const double scale = 1.0 / sqrt(rr);
+    for (int idx = gtid; idx < g.ndof; idx += G) {
+      w.r[idx] = (float)(v.r[idx] * scale);
+      w.x[idx] = 0.0f;
+    }
+    // pcg_loop starts with a reduction barrier, which orders these writes
+    bool iconv = false;
+    double irr = 0.0;
+    long long it = pcg_loop<float>(g, w, a.maxiter, a.inner_tol * a.inner_tol, ctx, scratch, 0, iconv, ok, irr);
+    inner_total += it;
+    ++sweeps;
+    if (!ok) break;
+    for (int idx = gtid; idx < g.ndof; idx += G) v.x[idx] += (double)w.x[idx] / scale;
+    // the residual pass reads x64 at neighbours: order the updates
+    if (!ctx.gb.sync(ctx.nb)) { ok = false; break; }
+  }
+  if (gtid == 0) {
+    a.st->iters = inner_total;
+    a.st->applies = inner_total + sweeps + 1;
+    a.st->refinements = sweeps;
+    a.st->rr = rr;
+    a.st->bb = bb < 0.0 ? 0.0 : bb;
+    a.st->converged = conv ? 1 : 0;
+  }
+}
+
+// ---- GMRES building blocks ---------------------------------------------------------
+
+struct GmState {
+  int done;          // inner loop finished (presid <= ptol or breakdown)
+  int breakdown;
+  int ncols;         // columns completed in this cycle
+  int reorth;        // second Gram-Schmidt pass requested
+  double presid;
+  double ptol;
+  double h0;         // ||w|| before orthogonalization
+  double wn2;        // ||w||^2 scratch
+  double rnorm;      // true residual norm (end of cycle)
+  double scal;       // scale factor for the new basis vector
+};
+
+// partial dots: part[k*nb + block] = <V_k, w> for k < ncols, part[ncols*nb+block] = <w,w>
+__global__ void mdot_kernel(int ndof, const double* __restrict__ V, int ncols, const double* __restrict__ w,
+                            double* part, const int* done) {
+  if (done && *done) return;
+  extern __shared__ double sh[];
+  const int nb = gridDim.x;
+  for (int k = 0; k <= ncols; ++k) {
+    const double* vk = (k < ncols) ? V + (size_t)k * ndof : w;
+    double acc = 0.0;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += gridDim.x * blockDim.x)
+      acc += vk[idx] * w[idx];
+    acc = tpf::warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      double s = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
+      s = tpf::warp_sum(s);
+      if (threadIdx.x == 0) part[(size_t)k * nb + blockIdx.x] = s;
+    }
+    __syncthreads();
+  }
+}
+
+// sum partials -> out[k] (k <= ncols); mode selects how the state uses them.
+// mode 0: first GS pass (h column = dots, h0 = sqrt(<w,w>)), decide re-orth
+// mode 1: second pass (h column += dots)
+// mode 2: plain norm -> out[0] = sqrt(<w,w>)
+__global__ void mdot_finalize_kernel(const double* part, int nb, int ncols, double* hcol, GmState* st,
+                                     int mode, double* out_norm) {
+  if (mode != 2 && st->done) return;
+  if (mode == 1 && !st->reorth) return;
+  __shared__ double sh[32];
+  for (int k = 0; k <= ncols; ++k) {
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) acc += part[(size_t)k * nb + b];
+    acc = tpf::warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int q = 0; q < (int)(blockDim.x >> 5); ++q) s += sh[q];
+      if (mode == 2) {
+        *out_norm = sqrt(s);
+      } else if (k < ncols) {
+        if (mode == 0) hcol[k] = s; else { hcol[k] += s; st->wn2 = 0.0; }
+      } else if (mode == 0) {
+        st->h0 = sqrt(s);
+        double proj = 0.0;
+        for (int q = 0; q < ncols; ++q) proj += hcol[q] * hcol[q];
+        st->reorth = (s - proj < 0.5 * s) ? 1 : 0;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// w -= sum_k c_k V_k  (c = hcol, or the second-pass dots in part-summed form)
+__global__ void maxpy_kernel(int ndof, const double* __restrict__ V, int ncols, const double* coef, double* w,
+                             const GmState* st, int pass) {
+  if (st->done) return;
+  if (pass == 1 && !st->reorth) return;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += gridDim.x * blockDim.x) {
+    double acc = w[idx];
+    for (int k = 0; k < ncols; ++k) acc -= coef[k] * V[(size_t)k * ndof + idx];
+    w[idx] = acc;
+  }
+}
+
+// Givens rotation generator for real (f, g): c f + s g = r, -s f + c g = 0,
+// r carries the sign of f (the convention of LAPACK's lartg).
+__device__ void givens_rot(double f, double g, double& c, double& s, double& r) {
+  if (g == 0.0) { c = 1.0; s = 0.0; r = f; return; }
+  if (f == 0.0) { c = 0.0; s = (g > 0.0) ? 1.0 : -1.0; r = fabs(g); return; }
+  double d = hypot(f, g);
+  c = fabs(f) / d;
+  r = copysign(d, f);
+  s = g / r;
+}
+
+// Finish Arnoldi column `col`: h1, breakdown, rotations, S, presid, done flag.
+// H is stored like SciPy's h[col, k] (row col = column of the Hessenberg matrix).
+__global__ void gm_column_kernel(double* H, int ldh, double* givens, double* S, GmState* st, int col,
+                                 const double* w_norm, const double* hcol2) {
+  if (st->done) return;
+  double* hc = H + (size_t)col * ldh;
+  if (st->reorth) {
+    // second-pass coefficients were accumulated into hcol2; fold them in
+    for (int k = 0; k <= col; ++k) hc[k] += hcol2[k];
+  }
+  const double eps = 2.220446049250313e-16;
+  double h1 = *w_norm;
+  hc[col + 1] = h1;
+  int breakdown = 0;
+  if (h1 <= eps * st->h0) {
+    hc[col + 1] = 0.0;
+    breakdown = 1;
+    st->scal = 1.0;
+  } else {
+    st->scal = 1.0 / h1;
+  }
+  for (int k = 0; k < col; ++k) {
+    double c = givens[2 * k], s = givens[2 * k + 1];
+    double n0 = hc[k], n1 = hc[k + 1];
+    hc[k] = c * n0 + s * n1;
+    hc[k + 1] = -s * n0 + c * n1;
+  }
+  double c, s, mag;
+  givens_rot(hc[col], hc[col + 1], c, s, mag);
+  givens[2 * col] = c;
+  givens[2 * col + 1] = s;
+  hc[col] = mag;
+  hc[col + 1] = 0.0;
+  double t = -s * S[col];
+  S[col] = c * S[col];
+  S[col + 1] = t;
+  st->presid = fabs(t);
+  st->ncols = col + 1;
+  st->breakdown = breakdown;
+  if (st->presid <= st->ptol || breakdown) st->done = 1;
+}
+
+__global__ void gm_scale_kernel(int ndof, const double* w, double* vout, const GmState* st) {
+  if (st->done && st->scal == 0.0) return;
+  // executed even when this column set done (the vector is then unused)
+  const double sc = st->scal;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += gridDim.x * blockDim.x)
+    vout[idx] = w[idx] * sc;
+}
+
+// y = H(:ncols,:ncols)^-1 S (SciPy's trsv loop), then coef = y
+__global__ void gm_backsolve_kernel(const double* H, int ldh, double* S, double* y, const GmState* st) {
+  int col = st->ncols - 1;
+  if (col < 0) return;
+  if (H[(size_t)col * ldh + col] == 0.0) S[col] = 0.0;
+  for (int k = 0; k <= col; ++k) y[k] = S[k];
+  for (int k = col; k > 0; --k) {
+    if (y[k] != 0.0) {
+      y[k] /= H[(size_t)k * ldh + k];
+      double t = y[k];
+      for (int q = 0; q < k; ++q) y[q] -= t * H[(size_t)k * ldh + q];
+    }
+  }
+  if (y[0] != 0.0) y[0] /= H[0];
+}
+
+__global__ void gm_update_x_kernel(int ndof, const double* __restrict__ V, const double* y, double* x,
+                                   const GmState* st) {
+  int ncols = st->ncols;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int k = 0; k < ncols; ++k) acc += y[k] * V[(size_t)k * ndof + idx];
+    x[idx] += acc;
+  }
+}
+
+__global__ void gm_start_kernel(int ndof, const double* w, double* v0, double* S, int m1, GmState* st,
+                                double vnorm, double ptol) {
+  const double inv = 1.0 / vnorm;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += gridDim.x * blockDim.x)
+    v0[idx] = w[idx] * inv;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    for (int k = 0; k < m1; ++k) S[k] = 0.0;
+    S[0] = vnorm;
+    st->done = 0;
+    st->breakdown = 0;
+    st->ncols = 0;
+    st->reorth = 0;
+    st->ptol = ptol;
+    st->presid = 0.0;
+  }
+}
+
+}  // namespace
+
+// ---- handle -------------------------------------------------------------------------
+
+struct tpf_ppe {
+  int ndim = 2;
+  Grid3 g{};
+  tpf_ppe_options o{};
+  double h_min = 0.0;
+  std::vector<std::vector<double>> coords;
+  // geometry
+  double* dv[3] = {nullptr, nullptr, nullptr};
+  double* dface[3] = {nullptr, nullptr, nullptr};
+  // operator state
+  double* s[3] = {nullptr, nullptr, nullptr};
+  float* s32[3] = {nullptr, nullptr, nullptr};
+  double* dinvS = nullptr;
+  float* dinvS32 = nullptr;
+  double* dinvL = nullptr;
+  double* tlo[3] = {nullptr, nullptr, nullptr};
+  double* tden[3] = {nullptr, nullptr, nullptr};
+  double* tcp[3] = {nullptr, nullptr, nullptr};
+  bool prepared = false;
+  // Krylov workspace
+  double* x = nullptr; double* r = nullptr; double* z = nullptr; double* p0 = nullptr; double* p1 = nullptr;
+  double* q = nullptr; double* b = nullptr; double* t1 = nullptr; double* t2 = nullptr;
+  float* x32 = nullptr; float* r32 = nullptr; float* z32 = nullptr; float* p032 = nullptr; float* p132 = nullptr;
+  float* q32 = nullptr;
+  double* ones64 = nullptr;
+  float* ones32 = nullptr;
+  double* V = nullptr;            // GMRES basis (restart+1) x ndof
+  int V_cols = 0;
+  double* gm = nullptr;           // H | givens | S | y | hcol | hcol2 | norm
+  GmState* gst = nullptr;
+  double* part = nullptr;
+  int part_len = 0;
+  unsigned int* bar = nullptr;
+  int* err = nullptr;
+  SolveStatus* st = nullptr;
+  int coop_blocks = 0;
+  int ew_blocks = 0;
+  std::vector<void*> allocs;
+};
+
+namespace {
+
+template <typename T>
+int dalloc(tpf_ppe* h, T** p, size_t n) {
+  if (cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) {
+    tpf::set_error("cudaMalloc of %zu bytes failed", n * sizeof(T));
+    return TPF_ECUDA;
+  }
+  h->allocs.push_back(*p);
+  return TPF_OK;
+}
+
+int validate_options(const tpf_ppe_options* o) {
+  TPF_CHECK_ARG(o->method == TPF_PPE_CG || o->method == TPF_PPE_GMRES,
+                "PPESolverFVMMatrixFree supports ppe_iteration_method='gmres' or 'cg' today");
+  TPF_CHECK_ARG(o->precond >= TPF_PRECOND_NONE && o->precond <= TPF_PRECOND_LINE_PCR,
+                "ppe_preconditioner must be 'jacobi', 'line_pcr', or 'none'");
+  TPF_CHECK_ARG(!(o->method == TPF_PPE_CG && (o->precond == TPF_PRECOND_LINE || o->precond == TPF_PRECOND_LINE_PCR)),
+                "ppe_iteration_method='cg' supports preconditioner='jacobi' or 'none'; line_pcr is a "
+                "nonsymmetric GMRES preconditioner.");
+  TPF_CHECK_ARG(o->precision == TPF_PREC_F64 || o->precision == TPF_PREC_MIXED, "unknown precision mode");
+  TPF_CHECK_ARG(!(o->precision == TPF_PREC_MIXED && o->method != TPF_PPE_CG),
+                "mixed precision is implemented for the CG route");
+  TPF_CHECK_ARG(o->tol > 0.0 && std::isfinite(o->tol), "tolerance must be > 0");
+  TPF_CHECK_ARG(o->maxiter >= 0, "maxiter must be >= 0");
+  TPF_CHECK_ARG(o->restart >= 1 && o->restart <= 1024, "restart must be in [1, 1024]");
+  TPF_CHECK_ARG(o->c_tau > 0.0, "c_tau must be > 0");
+  return TPF_OK;
+}
+
+LineArgs line_args(const Grid3& g, int axis) {
+  LineArgs L{};
+  if (axis == 0) {
+    L.lines = g.n1 * g.n2; L.n = g.n0; L.stride = g.st0; L.lmod = 1 << 30; L.lstride_hi = 0; L.lstride_lo = 1;
+  } else if (axis == 1) {
+    L.lines = g.n0 * g.n2; L.n = g.n1; L.stride = g.n2; L.lmod = g.n2; L.lstride_hi = g.st0; L.lstride_lo = 1;
+  } else {
+    L.lines = g.n0 * g.n1; L.n = g.n2; L.stride = 1; L.lmod = 1 << 30; L.lstride_hi = 0; L.lstride_lo = g.n2;
+  }
+  return L;
+}
+
+int ensure_gmres(tpf_ppe* h) {
+  int m = h->o.restart;
+  if (h->V && h->V_cols >= m + 1) return TPF_OK;
+  if (h->V) {
+    cudaFree(h->V);
+    cudaFree(h->gm);
+    h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void*)h->V), h->allocs.end());
+    h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void*)h->gm), h->allocs.end());
+  }
+  int st;
+  if ((st = dalloc(h, &h->V, (size_t)(m + 1) * h->g.ndof))) return st;
+  size_t gm_len = (size_t)m * (m + 2) + 2 * m + (m + 1) * 4 + 8;
+  if ((st = dalloc(h, &h->gm, gm_len))) return st;
+  h->V_cols = m + 1;
+  return TPF_OK;
+}
+
+int ew_grid(const tpf_ppe* h) { return h->ew_blocks; }
+
+// z = M^-1 r on the unweighted system (reference preconditioners), done-guarded
+int precond_L(tpf_ppe* h, const double* r, double* z, cudaStream_t s, const int* done) {
+  const Grid3& g = h->g;
+  switch (h->o.precond) {
+    case TPF_PRECOND_NONE:
+      TPF_CUDA_TRY(cudaMemcpyAsync(z, r, sizeof(double) * g.ndof, cudaMemcpyDeviceToDevice, s));
+      break;
+    case TPF_PRECOND_JACOBI:
+      jacobi_L_kernel<<<ew_grid(h), 256, 0, s>>>(g.ndof, g.pin, h->dinvL, r, z, done);
+      break;
+    default: {
+      // additive shifted line solves: z = (sum_a T_a^-1 r) / ndim, r[pin] = 0, z[pin] = 0
+      for (int ax = 0; ax < h->ndim; ++ax) {
+        LineArgs L = line_args(g, ax);
+        int blocks = (L.lines + 127) / 128;
+        if (ax == 0)
+          thomas_solve_kernel<false><<<blocks, 128, 0, s>>>(L, h->tlo[ax], h->tden[ax], h->tcp[ax], r, z, h->t2,
+                                                            g.pin, 1.0, done);
+        else
+          thomas_solve_kernel<true><<<blocks, 128, 0, s>>>(L, h->tlo[ax], h->tden[ax], h->tcp[ax], r, z, h->t2,
+                                                           g.pin, ax == h->ndim - 1 ? 1.0 / h->ndim : 1.0, done);
+      }
+      if (h->ndim == 1) { /* unreachable: ndim >= 2 */ }
+    }
+  }
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
+int norm2_dev(tpf_ppe* h, const double* w, double* out, cudaStream_t s) {
+  int nb = std::min(h->ew_blocks, h->part_len / 2);
+  mdot_kernel<<<nb, 256, 8 * 32 * sizeof(double), s>>>(h->g.ndof, nullptr, 0, w, h->part, nullptr);
+  mdot_finalize_kernel<<<1, 256, 0, s>>>(h->part, nb, 0, nullptr, h->gst, 2, out);
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
+int read_scalar(double* dev, double* host, cudaStream_t s) {
+  TPF_CUDA_TRY(cudaMemcpyAsync(host, dev, sizeof(double), cudaMemcpyDeviceToHost, s));
+  TPF_CUDA_TRY(cudaStreamSynchronize(s));
+  return TPF_OK;
+}
+
+// SciPy 1.18.1 gmres restated on the device (see the file header).
+int solve_gmres(tpf_ppe* h, const double* rhs, double* p, const double* p_init, cudaStream_t s,
+                tpf_ppe_result* res) {
+  const Grid3& g = h->g;
+  const int n = g.ndof;
+  int st;
+  if ((st = ensure_gmres(h))) return st;
+  const int m = std::min(h->o.restart, n);
+  const int ldh = h->o.restart + 2;
+  double* H = h->gm;
+  double* givens = H + (size_t)h->o.restart * ldh;
+  double* S = givens + 2 * h->o.restart;
+  double* y = S + (h->o.restart + 1);
+  double* hcol = y + (h->o.restart + 1);
+  double* hcol2 = hcol + (h->o.restart + 1);
+  double* wnorm = hcol2 + (h->o.restart + 1);
+  double* bnorm_d = wnorm + 1;
+  double* b = h->b;
+  double* x = h->x;
+  double* r = h->r;
+  double* w = h->z;
+  double* t = h->q;
+  // b = rhs with b[pin] = 0 ; x0 = p_init with pin = 0
+  copy_pin0_kernel<<<ew_grid(h), 256, 0, s>>>(n, g.pin, rhs, b);
+  if (p_init) copy_pin0_kernel<<<ew_grid(h), 256, 0, s>>>(n, g.pin, p_init, x);
+  else TPF_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(double) * n, s));
+  TPF_CUDA_TRY(cudaMemsetAsync(H, 0, sizeof(double) * (size_t)h->o.restart * ldh, s));
+  TPF_CUDA_TRY(cudaMemsetAsync(h->gst, 0, sizeof(GmState), s));
+  if ((st = norm2_dev(h, b, bnorm_d, s))) return st;
+  double bnrm2 = 0.0;
+  if ((st = read_scalar(bnorm_d, &bnrm2, s))) return st;
+  long long applies = 0, inner = 0;
+  res->refinements = 0;
+  if (bnrm2 == 0.0) {
+    TPF_CUDA_TRY(cudaMemsetAsync(p, 0, sizeof(double) * n, s));
+    TPF_CUDA_TRY(cudaStreamSynchronize(s));
+    res->iterations = 0; res->applies = 0; res->rel_residual = 0.0; res->info = 0;
+    return TPF_OK;
+  }
+  const double atol = h->o.tol * bnrm2;
+  const double eps = 2.220446049250313e-16;
+  // Mb_nrm2 = ||M b||
+  if ((st = precond_L(h, b, w, s, nullptr))) return st;
+  if ((st = norm2_dev(h, w, wnorm, s))) return st;
+  double Mb_nrm2 = 0.0;
+  if ((st = read_scalar(wnorm, &Mb_nrm2, s))) return st;
+  double ptol_max_factor = 1.0;
+  double ptol = Mb_nrm2 * std::min(ptol_max_factor, atol / bnrm2);
+  double presid = 0.0, rnorm = INFINITY;
+  const bool x_nonzero = p_init != nullptr;
+  const int nb_dot = std::min(h->ew_blocks, h->part_len / (m + 2));
+  const int* done = &h->gst->done;
+  bool converged = false;
+  for (long long iteration = 0; iteration < h->o.maxiter; ++iteration) {
+    if (iteration == 0) {
+      if (x_nonzero) {
+        apply_L_kernel<<<ew_grid(h), 256, 0, s>>>(g, Geo{{h->dv[0], h->dv[1], h->dv[2]}, {h->dface[0], h->dface[1], h->dface[2]}},
+                                                  h->s[0], h->s[1], h->s[2], x, r, b, nullptr);
+        ++applies;
+      } else {
+        TPF_CUDA_TRY(cudaMemcpyAsync(r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+      }
+      if ((st = norm2_dev(h, r, wnorm, s))) return st;
+      double r0 = 0.0;
+      if ((st = read_scalar(wnorm, &r0, s))) return st;
+      if (r0 < atol) { rnorm = r0; converged = true; break; }
+    }
+    // v0 = M r / ||M r||
+    TPF_CUDA_TRY(cudaMemsetAsync(h->gst, 0, sizeof(int), s));  // done = 0 for the precond call
+    if ((st = precond_L(h, r, w, s, nullptr))) return st;
+    if ((st = norm2_dev(h, w, wnorm, s))) return st;
+    double v0n = 0.0;
+    if ((st = read_scalar(wnorm, &v0n, s))) return st;
+    gm_start_kernel<<<ew_grid(h), 256, 0, s>>>(n, w, h->V, S, m + 1, h->gst, v0n, ptol);
+    const Geo geo{{h->dv[0], h->dv[1], h->dv[2]}, {h->dface[0], h->dface[1], h->dface[2]}};
+    for (int col = 0; col < m; ++col) {
+      const double* vc = h->V + (size_t)col * n;
+      apply_L_kernel<<<ew_grid(h), 256, 0, s>>>(g, geo, h->s[0], h->s[1], h->s[2], vc, t, nullptr, done);
+      if ((st = precond_L(h, t, w, s, done))) return st;
+      double* hc = H + (size_t)col * ldh;
+      mdot_kernel<<<nb_dot, 256, 8 * 32 * sizeof(double), s>>>(n, h->V, col + 1, w, h->part, done);
+      mdot_finalize_kernel<<<1, 256, 0, s>>>(h->part, nb_dot, col + 1, hc, h->gst, 0, nullptr);
+      maxpy_kernel<<<ew_grid(h), 256, 0, s>>>(n, h->V, col + 1, hc, w, h->gst, 0);
+      // conditional re-orthogonalization pass (hcol2 accumulates its coefficients)
+      TPF_CUDA_TRY(cudaMemsetAsync(hcol2, 0, sizeof(double) * (col + 1), s));
+      mdot_kernel<<<nb_dot, 256, 8 * 32 * sizeof(double), s>>>(n, h->V, col + 1, w, h->part, done);
+      mdot_finalize_kernel<<<1, 256, 0, s>>>(h->part, nb_dot, col + 1, hcol2, h->gst, 1, nullptr);
+      maxpy_kernel<<<ew_grid(h), 256, 0, s>>>(n, h->V, col + 1, hcol2, w, h->gst, 1);
+      if ((st = norm2_dev(h, w, wnorm, s))) return st;
+      gm_column_kernel<<<1, 1, 0, s>>>(H, ldh, givens, S, h->gst, col, wnorm, hcol2);
+      gm_scale_kernel<<<ew_grid(h), 256, 0, s>>>(n, w, h->V + (size_t)(col + 1) * n, h->gst);
+      TPF_CUDA_TRY(cudaGetLastError());
+    }
+    GmState hs{};
+    TPF_CUDA_TRY(cudaMemcpyAsync(&hs, h->gst, sizeof(GmState), cudaMemcpyDeviceToHost, s));
+    TPF_CUDA_TRY(cudaStreamSynchronize(s));
+    inner += hs.ncols;
+    applies += hs.ncols;
+    presid = hs.presid;
+    gm_backsolve_kernel<<<1, 1, 0, s>>>(H, ldh, S, y, h->gst);
+    gm_update_x_kernel<<<ew_grid(h), 256, 0, s>>>(n, h->V, y, x, h->gst);
+    apply_L_kernel<<<ew_grid(h), 256, 0, s>>>(g, geo, h->s[0], h->s[1], h->s[2], x, r, b, nullptr);
+    ++applies;
+    if ((st = norm2_dev(h, r, wnorm, s))) return st;
+    if ((st = read_scalar(wnorm, &rnorm, s))) return st;
+    if (rnorm <= atol) { converged = true; break; }
+    if (hs.breakdown) break;
+    if (presid <= ptol) ptol_max_factor = std::max(eps, 0.25 * ptol_max_factor);
+    else ptol_max_factor = std::min(1.0, 1.5 * ptol_max_factor);
+    ptol = presid * std::min(ptol_max_factor, atol / rnorm);
+  }
+  copy_pin0_kernel<<<ew_grid(h), 256, 0, s>>>(n, g.pin, x, p);
+  TPF_CUDA_TRY(cudaGetLastError());
+  TPF_CUDA_TRY(cudaStreamSynchronize(s));
+  res->iterations = inner;
+  res->applies = applies;
+  res->rel_residual = rnorm / bnrm2;
+  res->info = converged ? 0 : (int)std::min<long long>(h->o.maxiter, 0x7fffffff);
+  if (!converged) {
+    tpf::set_error("PPESolverFVMMatrixFree did not converge cleanly (info=%d); no alternate PPE solver was applied.",
+                   res->info);
+    return TPF_ENOCONV;
+  }
+  return TPF_OK;
+}
+
+int solve_cg(tpf_ppe* h, const double* rhs, double* p, const double* p_init, cudaStream_t s,
+             tpf_ppe_result* res) {
+  const Grid3& g = h->g;
+  const int n = g.ndof;
+  const Geo geo{{h->dv[0], h->dv[1], h->dv[2]}, {h->dface[0], h->dface[1], h->dface[2]}};
+  cg_rhs_kernel<<<ew_grid(h), 256, 0, s>>>(g, geo, rhs, h->b, p_init, h->x);
+  TPF_CUDA_TRY(cudaMemsetAsync(h->bar, 0, 2 * sizeof(unsigned int), s));
+  TPF_CUDA_TRY(cudaMemsetAsync(h->err, 0, sizeof(int), s));
+  TPF_CUDA_TRY(cudaMemsetAsync(h->st, 0, sizeof(SolveStatus), s));
+  const bool none = (h->o.precond == TPF_PRECOND_NONE);
+  PcgArgs a{};
+  a.g = g;
+  a.v64 = PcgVecs<double>{h->s[0], h->s[1], h->s[2], none ? h->ones64 : h->dinvS, h->x, h->r, h->z, h->p0, h->p1, h->q};
+  a.v32 = PcgVecs<float>{h->s32[0], h->s32[1], h->s32[2], none ? h->ones32 : h->dinvS32,
+                         h->x32, h->r32, h->z32, h->p032, h->p132, h->q32};
+  a.b = h->b;
+  a.tol = h->o.tol;
+  a.x_nonzero = p_init ? 1 : 0;
+  a.part = h->part;
+  a.bar = h->bar;
+  a.err = h->err;
+  a.st = h->st;
+  const bool mixed = (h->o.precision == TPF_PREC_MIXED);
+  if (mixed) {
+    a.maxiter = h->o.maxiter;
+    a.max_refine = h->o.max_refine;
+    a.inner_tol = h->o.inner_tol;
+  } else {
+    a.maxiter = h->o.maxiter;
+  }
+  void* args[] = {&a};
+  void* fn = mixed ? (void*)pcg_mixed_kernel : (void*)pcg64_kernel;
+  TPF_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(h->coop_blocks), dim3(kThreads), args, 0, s));
+  copy_pin0_kernel<<<ew_grid(h), 256, 0, s>>>(n, g.pin, h->x, p);
+  SolveStatus hs{};
+  int herr = 0;
+  TPF_CUDA_TRY(cudaMemcpyAsync(&hs, h->st, sizeof(SolveStatus), cudaMemcpyDeviceToHost, s));
+  TPF_CUDA_TRY(cudaMemcpyAsync(&herr, h->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  TPF_CUDA_TRY(cudaStreamSynchronize(s));
+  if (herr) {
+    tpf::set_error("PCG grid barrier timed out; the solve was aborted");
+    return TPF_EABORT;
+  }
+  res->iterations = hs.iters;
+  res->applies = hs.applies;
+  res->refinements = hs.refinements;
+  res->rel_residual = hs.bb > 0.0 ? std::sqrt(hs.rr / hs.bb) : 0.0;
+  res->info = hs.converged ? 0 : (int)std::min<long long>(mixed ? h->o.max_refine : h->o.maxiter, 0x7fffffff);
+  if (!hs.converged) {
+    tpf::set_error("PPESolverFVMMatrixFree did not converge cleanly (info=%d); no alternate PPE solver was applied.",
+                   res->info);
+    return TPF_ENOCONV;
+  }
+  return TPF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void tpf_ppe_default_options(tpf_ppe_options* o) {
+  if (!o) return;
+  o->method = TPF_PPE_GMRES;
+  o->precond = TPF_PRECOND_LINE;
+  o->precision = TPF_PREC_F64;
+  o->tol = 1e-8;
+  o->maxiter = 500;
+  o->restart = 80;
+  o->c_tau = 2.0;
+  o->pcr_stages = 4;
+  o->inner_tol = 1e-4;
+  o->max_refine = 50;
+}
+
+int tpf_ppe_create(tpf_ppe** out, int ndim, const int64_t* N, const double* const* coords, int64_t pin,
+                   const tpf_ppe_options* opts) {
+  TPF_CHECK_ARG(out && N && coords, "NULL argument");
+  *out = nullptr;
+  TPF_CHECK_ARG(ndim == 2 || ndim == 3, "ndim must be 2 or 3");
+  tpf_ppe_options o;
+  tpf_ppe_default_options(&o);
+  if (opts) o = *opts;
+  int st = validate_options(&o);
+  if (st) return st;
+  int64_t nn[3] = {1, 1, 1}, ndof = 1;
+  for (int a = 0; a < ndim; ++a) {
+    TPF_CHECK_ARG(N[a] >= 1, "N must be >= 1");
+    nn[a] = N[a] + 1;
+    ndof *= nn[a];
+  }
+  TPF_CHECK_ARG(ndof < (int64_t)1 << 31, "grid too large for 32-bit indexing");
+  TPF_CHECK_ARG(pin >= 0 && pin < ndof, "pin DOF out of range");
+  auto* h = new tpf_ppe();
+  h->ndim = ndim;
+  h->o = o;
+  Grid3& g = h->g;
+  g.n0 = (int)nn[0]; g.n1 = (int)nn[1]; g.n2 = (int)nn[2];
+  g.N0 = (int)N[0]; g.N1 = (int)N[1]; g.N2 = ndim == 3 ? (int)N[2] : 0;
+  g.st0 = g.n1 * g.n2;
+  g.ndof = (int)ndof;
+  g.pin = (int)pin;
+  // grid metrics (fvm_matrixfree_helpers.py:23-43)
+  h->h_min = INFINITY;
+  std::vector<std::vector<double>> dvh(3), dfh(3);
+  for (int a = 0; a < ndim; ++a) {
+    std::vector<double> c(coords[a], coords[a] + nn[a]);
+    std::vector<double> d(nn[a] - 1);
+    for (int64_t i = 0; i + 1 < nn[a]; ++i) {
+      d[i] = c[i + 1] - c[i];
+      h->h_min = std::min(h->h_min, d[i]);
+    }
+    std::vector<double> dv(nn[a]);
+    dv[0] = d[0] / 2.0;
+    dv[nn[a] - 1] = d[nn[a] - 2] / 2.0;
+    for (int64_t i = 1; i + 1 < nn[a]; ++i) dv[i] = (c[i + 1] - c[i - 1]) / 2.0;
+    dvh[a] = dv;
+    dfh[a] = d;
+    h->coords.push_back(c);
+  }
+  auto fail = [&](int code) { tpf_ppe_destroy(h); return code; };
+  for (int a = 0; a < ndim; ++a) {
+    if ((st = dalloc(h, &h->dv[a], nn[a]))) return fail(st);
+    if ((st = dalloc(h, &h->dface[a], nn[a] - 1))) return fail(st);
+    if (cudaMemcpy(h->dv[a], dvh[a].data(), nn[a] * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(h->dface[a], dfh[a].data(), (nn[a] - 1) * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+      tpf::set_error("copy of grid metrics failed");
+      return fail(TPF_ECUDA);
+    }
+  }
+  const size_t n = (size_t)ndof;
+  for (int a = 0; a < ndim; ++a) {
+    if ((st = dalloc(h, &h->s[a], n))) return fail(st);
+    if ((st = dalloc(h, &h->s32[a], n))) return fail(st);
+    if ((st = dalloc(h, &h->tlo[a], n))) return fail(st);
+    if ((st = dalloc(h, &h->tden[a], n))) return fail(st);
+    if ((st = dalloc(h, &h->tcp[a], n))) return fail(st);
+  }
+  if (ndim == 2) { h->s[2] = h->s[1]; h->s32[2] = h->s32[1]; }  // never read (N2 = 0)
+  double** d64[] = {&h->dinvS, &h->dinvL, &h->x, &h->r, &h->z, &h->p0, &h->p1, &h->q, &h->b, &h->t1, &h->t2,
+                      &h->ones64};
+  for (double** pp : d64)
+    if ((st = dalloc(h, pp, n))) return fail(st);
+  float** d32[] = {&h->dinvS32, &h->x32, &h->r32, &h->z32, &h->p032, &h->p132, &h->q32, &h->ones32};
+  for (float** pp : d32)
+    if ((st = dalloc(h, pp, n))) return fail(st);
+  // ones: the identity preconditioner of the CG route ('none')
+  {
+    std::vector<double> ones(n, 1.0);
+    std::vector<float> onesf(n, 1.0f);
+    if (cudaMemcpy(h->ones64, ones.data(), n * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(h->ones32, onesf.data(), n * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
+      tpf::set_error("workspace init failed");
+      return fail(TPF_ECUDA);
+    }
+  }
+  // cooperative grid for the persistent PCG kernels
+  int dev = 0, nsm = tpf::sm_count(), occ64 = 0, occmx = 0;
+  cudaGetDevice(&dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ64, pcg64_kernel, kThreads, 0) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occmx, pcg_mixed_kernel, kThreads, 0) != cudaSuccess) {
+    tpf::set_error("occupancy query failed");
+    return fail(TPF_ECUDA);
+  }
+  int per_sm = std::max(1, std::min(std::min(occ64, occmx), 1));
+  int need = (int)((n + kThreads - 1) / kThreads);
+  h->coop_blocks = std::max(1, std::min(nsm * per_sm, need));
+  h->ew_blocks = std::max(1, std::min(nsm * 8, (int)((n + 255) / 256)));
+  h->part_len = std::max(8 * h->coop_blocks, (o.restart + 2) * h->ew_blocks);
+  if ((st = dalloc(h, &h->part, (size_t)h->part_len))) return fail(st);
+  if ((st = dalloc(h, &h->bar, 4))) return fail(st);
+  if ((st = dalloc(h, &h->err, 1))) return fail(st);
+  if ((st = dalloc(h, &h->st, 1))) return fail(st);
+  if ((st = dalloc(h, &h->gst, 1))) return fail(st);
+  *out = h;
+  return TPF_OK;
+}
+
+int tpf_ppe_destroy(tpf_ppe* h) {
+  if (!h) return TPF_OK;
+  for (void* p : h->allocs) cudaFree(p);
+  delete h;
+  return TPF_OK;
+}
+
+int tpf_ppe_set_options(tpf_ppe* h, const tpf_ppe_options* o) {
+  TPF_CHECK_ARG(h && o, "NULL argument");
+  int st = validate_options(o);
+  if (st) return st;
+  bool line_changed = (o->precond != h->o.precond) || (o->c_tau != h->o.c_tau);
+  bool grow = o->restart > h->o.restart;
+  h->o = *o;
+  if (grow) {
+    cudaFree(h->part);
+    h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void*)h->part), h->allocs.end());
+    h->part_len = std::max(8 * h->coop_blocks, (o->restart + 2) * h->ew_blocks);
+    if ((st = dalloc(h, &h->part, (size_t)h->part_len))) return st;
+  }
+  if (line_changed) h->prepared = false;
+  return TPF_OK;
+}
+
+int tpf_ppe_prepare(tpf_ppe* h, const double* rho, void* stream) {
+  TPF_CHECK_ARG(h && rho, "NULL argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  PrepArgs a{};
+  a.g = h->g;
+  a.geo = Geo{{h->dv[0], h->dv[1], h->dv[2]}, {h->dface[0], h->dface[1], h->dface[2]}};
+  a.rho = rho;
+  for (int ax = 0; ax < 3; ++ax) {
+    a.s[ax] = (ax < h->ndim) ? h->s[ax] : nullptr;
+    a.s32[ax] = (ax < h->ndim) ? h->s32[ax] : nullptr;
+    a.tlo[ax] = (ax < h->ndim) ? h->tlo[ax] : nullptr;
+    a.tdg[ax] = (ax < h->ndim) ? h->tden[ax] : nullptr;
+    a.tup[ax] = (ax < h->ndim) ? h->tcp[ax] : nullptr;
+  }
+  a.dinvS = h->dinvS;
+  a.dinvS32 = h->dinvS32;
+  a.dinvL = h->dinvL;
+  a.shift_scale = 2.0 / (h->o.c_tau * h->h_min * h->h_min);
+  a.ndim = h->ndim;
+  a.want_line = 1;
+  prep_faces_kernel<<<h->ew_blocks, 256, 0, s>>>(a);
+  TPF_CUDA_TRY(cudaGetLastError());
+  for (int ax = 0; ax < h->ndim; ++ax) {
+    LineArgs L = line_args(h->g, ax);
+    thomas_factor_kernel<<<(L.lines + 127) / 128, 128, 0, s>>>(L, h->tlo[ax], h->tden[ax], h->tcp[ax]);
+  }
+  TPF_CUDA_TRY(cudaGetLastError());
+  h->prepared = true;
+  return TPF_OK;
+}
+
+int tpf_ppe_apply(tpf_ppe* h, const double* p, double* out, void* stream) {
+  TPF_CHECK_ARG(h && p && out, "NULL argument");
+  TPF_CHECK_ARG(h->prepared, "operator coefficients are not initialised (call prepare first)");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const Geo geo{{h->dv[0], h->dv[1], h->dv[2]}, {h->dface[0], h->dface[1], h->dface[2]}};
+  apply_L_kernel<<<h->ew_blocks, 256, 0, s>>>(h->g, geo, h->s[0], h->s[1], h->s[2], p, out, nullptr, nullptr);
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
+int tpf_ppe_precondition(tpf_ppe* h, const double* r, double* z, void* stream) {
+  TPF_CHECK_ARG(h && r && z, "NULL argument");
+  TPF_CHECK_ARG(h->prepared, "preconditioner state is not initialised (call prepare first)");
+  TPF_CHECK_ARG(h->o.precond != TPF_PRECOND_LINE_PCR, "truncated-PCR line preconditioner is not built");
+  return precond_L(h, r, z, static_cast<cudaStream_t>(stream), nullptr);
+}
+
+int tpf_ppe_solve(tpf_ppe* h, const double* rhs, const double* rho, double* p, const double* p_init, void* stream,
+                  tpf_ppe_result* result) {
+  TPF_CHECK_ARG(h && rhs && p, "NULL argument");
+  TPF_CHECK_ARG(h->o.precond != TPF_PRECOND_LINE_PCR, "truncated-PCR line preconditioner is not built");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int st;
+  if (rho) {
+    if ((st = tpf_ppe_prepare(h, rho, stream))) return st;
+  }
+  TPF_CHECK_ARG(h->prepared, "operator coefficients are not initialised (call prepare first)");
+  tpf_ppe_result local{};
+  tpf_ppe_result* res = result ? result : &local;
+  *res = tpf_ppe_result{};
+  if (h->o.method == TPF_PPE_CG) return solve_cg(h, rhs, p, p_init, s, res);
+  return solve_gmres(h, rhs, p, p_init, s, res);
+}
+
+}  // extern "C"
