@@ -138,7 +138,7 @@ def make_inputs():
 def _solver(precision):
     from twophaseflow_b200 import PPESolverFVMMatrixFree, UniformGrid
     cfg = _Cfg(pseudo_tol=TOL, pseudo_maxiter=1_000_000, ppe_iteration_method="cg", ppe_preconditioner="jacobi",
-               ppe_precision=precision, ppe_inner_tol=1e-4, ppe_max_refine=100)
+               ppe_precision=precision, ppe_inner_tol=1e-3)
     return PPESolverFVMMatrixFree(None, cfg, UniformGrid(N_PPE))
 
 

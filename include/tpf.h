@@ -86,6 +86,16 @@ int tpf_ccd_apply(const tpf_ccd_plan* plan, int64_t outer, int64_t inner,
                   const void* f, void* d1, void* d2, const double* bc_left,
                   const double* bc_right, int flags, void* stream);
 
+/* Variable-density CCD term along the plan's axis, fused into the line
+ * solve's output stage: out (+)= D2 f / rho - (drho / rho^2) D1 f, where drho
+ * is d(rho)/dx along this axis (accumulate != 0 adds to out).  Summed over
+ * the axes this is the CCD operator L_H p = sum_a [D2_a p / rho -
+ * (D1_a rho / rho^2) D1_a p].  Replaces compute_ccd_laplacian
+ * (ppe/ccd_ppe_utils.py:51-82). */
+int tpf_ccd_apply_vd(const tpf_ccd_plan* plan, int64_t outer, int64_t inner,
+                     const void* f, const void* rho, const void* drho,
+                     void* out, int accumulate, int flags, void* stream);
+
 /* Zero grad at index 0 and n_pts-1 along the axis of a [outer, n, inner]
  * array (wall axes only; no-op for periodic plans).  Replaces
  * CCDSolver.enforce_wall_neumann (ccd_solver.py:264-281;
@@ -122,14 +132,15 @@ typedef struct tpf_ppe_options {
   int restart;           /* GMRES restart length (ppe_restart)                   */
   double c_tau;          /* line-preconditioner shift factor (pseudo_c_tau)      */
   int pcr_stages;        /* TPF_PRECOND_LINE_PCR stages (ppe_pcr_stages)         */
-  double inner_tol;      /* MIXED: relative tolerance of each FP32 inner solve   */
-  int64_t max_refine;    /* MIXED: maximum refinement sweeps                     */
+  double inner_tol;      /* MIXED: FP64 residual replacement + FP32 CG restart     
+                          * whenever ||r|| fell by this factor (default 1e-3)   */
+  int64_t max_refine;    /* reserved                                             */
 } tpf_ppe_options;
 
 typedef struct tpf_ppe_result {
   int64_t iterations;    /* CG iterations / GMRES inner iterations (all sweeps)  */
   int64_t applies;       /* operator applications                                */
-  int64_t refinements;   /* MIXED: outer refinement sweeps                       */
+  int64_t refinements;   /* MIXED: FP64 residual replacements                    */
   double rel_residual;   /* ||b - A x|| / ||b|| of the solved system             */
   int info;              /* 0 converged, >0 iteration budget exhausted           */
 } tpf_ppe_result;

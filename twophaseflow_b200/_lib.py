@@ -58,6 +58,8 @@ SIGNATURES = {
     "tpf_ccd_plan_set_metric": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "tpf_ccd_apply": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                 C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int, C.c_void_p]),
+    "tpf_ccd_apply_vd": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "tpf_ccd_enforce_wall_neumann": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]),
     "tpf_ppe_default_options": (None, [C.POINTER(tpf_ppe_options)]),
     "tpf_ppe_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_int64),

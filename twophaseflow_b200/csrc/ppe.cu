@@ -250,265 +250,301 @@ __global__ void copy_pin0_kernel(int ndof, int pin, const double* src, double* d
     dst[idx] = (idx == pin) ? 0.0 : src[idx];
 }
 
-// ---- persistent PCG --------------------------------------------------------------
+// ---- persistent PCG ----------------------------------------------------------------
+//
+// Chronopoulos-Gear preconditioned CG: mathematically the CG iteration SciPy's
+// cg performs (stop when ||r|| < tol ||b|| at the top of an iteration), with
+// the two inner products of an iteration fused into ONE grid-wide reduction:
+//   gamma = (r,u), delta = (w,u), u = M r, w = S u,
+//   beta = gamma/gamma_old, alpha = gamma / (delta - beta gamma / alpha_old),
+//   p = u + beta p, s = w + beta s, x += alpha p, r -= alpha s.
+// The next stencil w_new = S M r_new is fused into the same pass: neighbour
+// values of u_new are recomputed from (r, w, s) of the previous pass, which
+// are double-buffered, so each iteration needs one barrier.
 
 struct SolveStatus {
   long long iters;
   long long applies;
-  long long refinements;
-  double rr;          // final ||r||^2 of the solved system
-  double bb;          // ||b||^2
+  long long refinements;   // FP64 residual replacements (mixed)
+  double rr;               // final ||r||^2 of the solved system
+  double bb;               // ||b||^2
   int converged;
   int pad;
 };
 
 template <typename T>
-struct PcgVecs {
-  const T* s0; const T* s1; const T* s2;
-  const T* dinv;
-  T* x; T* r; T* z; T* p0; T* p1; T* q;
+struct Cg1Vecs {
+  const T* s0; const T* s1; const T* s2;   // face couplings
+  const T* dinv;                           // Jacobi (1/diag S; pin -> 1)
+  T* r[2]; T* w[2]; T* s[2];
+  T* p;
 };
 
-struct PcgArgs {
+struct Cg1Args {
   Grid3 g;
-  PcgVecs<double> v64;
-  PcgVecs<float> v32;
-  const double* b;        // SPD-system rhs (FP64)
-  double* x64;            // FP64 solution (mixed) / unused
-  double* r64;
-  long long maxiter;      // CG iterations (plain) / inner iterations per sweep (mixed)
-  long long max_refine;
-  double tol;             // relative tolerance on ||r||/||b||
-  double inner_tol;       // mixed: relative tolerance of each FP32 inner solve
+  Cg1Vecs<double> v64;
+  Cg1Vecs<float> v32;
+  const double* s64[3];    // FP64 couplings for the residual replacement (mixed)
+  const double* b;         // SPD-system rhs
+  double* x;               // solution (FP64 in both modes)
+  long long maxiter;
+  double tol;
+  double replace_drop;     // mixed: replace the residual when ||r|| fell by this factor
   int x_nonzero;
-  double* part;           // [4][nblocks] partial sums
-  unsigned int* bar;
+  double* part;            // [2 slots][8][nblocks]
+  unsigned int* count;     // monotonic arrival counter
   int* err;
   SolveStatus* st;
 };
 
-struct GridCtx {
-  tpf::GridBarrier gb;
+__device__ __forceinline__ void red_release_add(unsigned int* p, unsigned int v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid-wide sum of NV doubles through a bounded barrier on a monotonic counter.
+struct GridSum {
   double* part;
-  unsigned nb;
-  __device__ __forceinline__ bool reduce(double (&v)[2], int site, double* scratch) {
-    tpf::block_sum<2>(v, scratch);
+  unsigned int* count;
+  int* err;
+  unsigned int nb;
+  unsigned int epoch;
+
+  template <int NV>
+  __device__ __forceinline__ bool sum(double (&v)[NV], double* scratch) {
+    tpf::block_sum<NV>(v, scratch);
+    const int slot = epoch & 1;
+    __shared__ int s_ok;
     if (threadIdx.x == 0) {
-      part[(site * 2 + 0) * nb + blockIdx.x] = v[0];
-      part[(site * 2 + 1) * nb + blockIdx.x] = v[1];
-    }
-    if (!gb.sync(nb)) return false;
-    // every block sums the partials in the same order -> identical scalars
-    double a0 = 0.0, a1 = 0.0;
-    if (threadIdx.x < 32) {
-      for (unsigned k = threadIdx.x; k < nb; k += 32) {
-        a0 += ((volatile double*)part)[(site * 2 + 0) * nb + k];
-        a1 += ((volatile double*)part)[(site * 2 + 1) * nb + k];
+#pragma unroll
+      for (int k = 0; k < NV; ++k) part[(slot * 8 + k) * nb + blockIdx.x] = v[k];
+      red_release_add(count, 1u);
+      const unsigned int target = (epoch + 1) * nb;
+      int ok = 1;
+      long long spins = 0;
+      while (ld_acquire(count) < target) {
+        if (++spins > kSpinLimit * 8) { atomicExch(err, 1); ok = 0; break; }
+        if ((spins & 1023) == 0 && *(volatile int*)err) { ok = 0; break; }
       }
-      a0 = tpf::warp_sum(a0);
-      a1 = tpf::warp_sum(a1);
-      if (threadIdx.x == 0) { scratch[128] = a0; scratch[129] = a1; }
+      __threadfence();
+      s_ok = ok;
     }
     __syncthreads();
-    v[0] = scratch[128];
-    v[1] = scratch[129];
+    const bool ok = s_ok != 0;
+    if (threadIdx.x < 32) {
+      double acc[NV];
+#pragma unroll
+      for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+      for (unsigned int j = threadIdx.x; j < nb; j += 32) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) acc[k] += __ldcg(part + (slot * 8 + k) * nb + j);
+      }
+#pragma unroll
+      for (int k = 0; k < NV; ++k) {
+        acc[k] = tpf::warp_sum(acc[k]);
+        if (threadIdx.x == 0) scratch[224 + k] = acc[k];
+      }
+    }
     __syncthreads();
-    return true;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = scratch[224 + k];
+    __syncthreads();
+    ++epoch;
+    return ok;
+  }
+
+  __device__ __forceinline__ bool sync(double* scratch) {
+    double d[1] = {0.0};
+    return sum<1>(d, scratch);
   }
 };
 
-// One PCG solve on S x = r_in (the vectors of `v`), SciPy cg semantics.
-// On entry r holds the residual of the current x and z = dinv r has NOT been
-// formed.  Returns iterations; sets *conv.  atol2 = (tol * ||b||)^2.
+// r = b - S x for own nodes (x FP64, pin column zero / pin row identity)
 template <typename T>
-__device__ long long pcg_loop(const Grid3& g, const PcgVecs<T>& v, long long maxiter, double atol2,
-                              GridCtx& ctx, double* scratch, int site_base, bool& conv, bool& ok,
-                              double& rr_out) {
+__device__ __forceinline__ void residual_pass(const Grid3& g, const double* s0, const double* s1,
+                                              const double* s2, const double* b, const double* x, T* r,
+                                              bool x_nonzero, double& bb, double& rr) {
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const int G = gridDim.x * blockDim.x;
-  // phase A0: z = dinv r, rr, rz
-  double red[2] = {0.0, 0.0};
   for (int idx = gtid; idx < g.ndof; idx += G) {
-    T r = v.r[idx];
-    T z = v.dinv[idx] * r;
-    v.z[idx] = z;
-    v.p0[idx] = T(0);
-    red[0] += (double)r * (double)r;
-    red[1] += (double)r * (double)z;
-  }
-  ok = ctx.reduce(red, site_base, scratch);
-  double rr = red[0], rz = red[1], rz_prev = 1.0;
-  T* pc = v.p0;
-  T* pn = v.p1;
-  long long it = 0;
-  conv = false;
-  while (ok) {
-    if (rr < atol2) { conv = true; break; }
-    if (it >= maxiter) break;
-    const T beta = (it > 0) ? (T)(rz / rz_prev) : T(0);
-    // phase B: p_new = z + beta p ; q = S p_new ; pq
-    double pq[2] = {0.0, 0.0};
-    for (int idx = gtid; idx < g.ndof; idx += G) {
-      int i0, i1, i2;
-      coords3(g, idx, i0, i1, i2);
-      auto pnew = [&](int j) -> T { return (j == g.pin) ? T(0) : v.z[j] + beta * pc[j]; };
-      T pi = v.z[idx] + beta * pc[idx];
-      T qi;
-      if (idx == g.pin) {
-        qi = pi;
-      } else {
-        T d, off;
-        s_row<T>(g, idx, i0, i1, i2, v.s0, v.s1, v.s2, pnew, d, off);
-        qi = d * pi - off;
-      }
-      pn[idx] = pi;
-      v.q[idx] = qi;
-      pq[0] += (double)pi * (double)qi;
-    }
-    ok = ctx.reduce(pq, site_base + 1, scratch);
-    if (!ok) break;
-    const double alpha_d = rz / pq[0];
-    const T alpha = (T)alpha_d;
-    // phase A: x += alpha p ; r -= alpha q ; z = dinv r ; rr, rz
-    red[0] = red[1] = 0.0;
-    for (int idx = gtid; idx < g.ndof; idx += G) {
-      T pi = pn[idx];
-      v.x[idx] += alpha * pi;
-      T r = v.r[idx] - alpha * v.q[idx];
-      v.r[idx] = r;
-      T z = v.dinv[idx] * r;
-      v.z[idx] = z;
-      red[0] += (double)r * (double)r;
-      red[1] += (double)r * (double)z;
-    }
-    ok = ctx.reduce(red, site_base, scratch);
-    rz_prev = rz;
-    rr = red[0];
-    rz = red[1];
-    T* t = pc; pc = pn; pn = t;
-    ++it;
-  }
-  rr_out = rr;
-  return it;
-}
-
-// Plain FP64 PCG: the whole SciPy-cg loop in one cooperative launch.
-__global__ void __launch_bounds__(kThreads) pcg64_kernel(PcgArgs a) {
-  __shared__ double scratch[160];
-  GridCtx ctx{tpf::GridBarrier{a.bar, a.err, kSpinLimit}, a.part, gridDim.x};
-  const Grid3& g = a.g;
-  const PcgVecs<double>& v = a.v64;
-  const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int G = gridDim.x * blockDim.x;
-  // r = b - S x  (x read-only here; S with the pin column zeroed, pin row identity)
-  double bbv[2] = {0.0, 0.0};
-  for (int idx = gtid; idx < g.ndof; idx += G) {
-    double bi = a.b[idx];
-    double r = bi;
-    if (a.x_nonzero) {
+    double bi = b[idx];
+    double ri = bi;
+    if (x_nonzero) {
       double sx;
-      if (idx == g.pin) sx = v.x[idx];
+      if (idx == g.pin) sx = x[idx];
       else {
         int i0, i1, i2;
         coords3(g, idx, i0, i1, i2);
         double d, off;
-        s_row<double>(g, idx, i0, i1, i2, v.s0, v.s1, v.s2,
-                      [&](int j) { return (j == g.pin) ? 0.0 : v.x[j]; }, d, off);
-        sx = d * v.x[idx] - off;
+        s_row<double>(g, idx, i0, i1, i2, s0, s1, s2, [&](int j) { return (j == g.pin) ? 0.0 : x[j]; }, d, off);
+        sx = d * x[idx] - off;
       }
-      r = bi - sx;
+      ri = bi - sx;
     }
-    v.r[idx] = r;
-    bbv[0] += bi * bi;
+    r[idx] = (T)ri;
+    bb += bi * bi;
+    rr += ri * ri;
   }
-  bool ok = ctx.reduce(bbv, 2, scratch);
-  if (!ok) return;
-  const double bb = bbv[0];
+}
+
+// u = M r, w = S u for own nodes (r read at neighbours) and the six inner
+// products of the single reduction with the current search directions p, s:
+// red = {(r,u), (w,u), (u,s), (p,w), (p,s), (r,r)}.  init: p = s = 0.
+template <typename T>
+__device__ __forceinline__ void w_pass(const Grid3& g, const Cg1Vecs<T>& v, int cur, bool init, double (&red)[6]) {
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int G = gridDim.x * blockDim.x;
+  const T* r = v.r[cur];
+  for (int idx = gtid; idx < g.ndof; idx += G) {
+    int i0, i1, i2;
+    coords3(g, idx, i0, i1, i2);
+    const T ri = r[idx];
+    const T ui = v.dinv[idx] * ri;
+    T wi;
+    if (idx == g.pin) {
+      wi = ui;
+    } else {
+      T d, off;
+      s_row<T>(g, idx, i0, i1, i2, v.s0, v.s1, v.s2,
+               [&](int j) -> T { return (j == g.pin) ? T(0) : v.dinv[j] * r[j]; }, d, off);
+      wi = d * ui - off;
+    }
+    v.w[cur][idx] = wi;
+    T si = T(0), pi = T(0);
+    if (init) {
+      v.s[cur][idx] = T(0);
+      v.p[idx] = T(0);
+    } else {
+      si = v.s[cur][idx];
+      pi = v.p[idx];
+    }
+    red[0] += (double)ri * (double)ui;
+    red[1] += (double)wi * (double)ui;
+    red[2] += (double)ui * (double)si;
+    red[3] += (double)pi * (double)wi;
+    red[4] += (double)pi * (double)si;
+    red[5] += (double)ri * (double)ri;
+  }
+}
+
+template <typename T, bool MIXED>
+__global__ void __launch_bounds__(kThreads, 1) cg1_kernel(Cg1Args a) {
+  __shared__ double scratch[256];
+  GridSum gs{a.part, a.count, a.err, gridDim.x, 0u};
+  const Grid3& g = a.g;
+  const Cg1Vecs<T>& v = *reinterpret_cast<const Cg1Vecs<T>*>(MIXED ? (const void*)&a.v32 : (const void*)&a.v64);
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int G = gridDim.x * blockDim.x;
+  int cur = 0;
+  // r0 = b - S x0
+  double red0[2] = {0.0, 0.0};
+  residual_pass<T>(g, a.s64[0], a.s64[1], a.s64[2], a.b, a.x, v.r[cur], a.x_nonzero != 0, red0[0], red0[1]);
+  if (!gs.sum<2>(red0, scratch)) return;
+  const double bb = red0[0];
   if (bb == 0.0) {
-    for (int idx = gtid; idx < g.ndof; idx += G) v.x[idx] = 0.0;
+    for (int idx = gtid; idx < g.ndof; idx += G) a.x[idx] = 0.0;
     if (gtid == 0) { a.st->iters = 0; a.st->applies = 0; a.st->rr = 0.0; a.st->bb = 0.0; a.st->converged = 1; }
     return;
   }
-  const double atol2 = (a.tol * sqrt(bb)) * (a.tol * sqrt(bb));
+  const double atol = a.tol * sqrt(bb);
+  const double atol2 = atol * atol;
+  double red[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  w_pass<T>(g, v, cur, true, red);
+  bool ok = gs.sum<6>(red, scratch);
+  // loop state: gamma_i, rr_i and the denominator (p_i, S p_i) of alpha_i
+  double gamma = red[0], rr = red[5];
+  double beta = 0.0, denom = red[1];
+  double rr_ref = rr;            // ||r||^2 at the last FP64 residual replacement
+  long long it = 0, replacements = 0, applies = a.x_nonzero ? 2 : 1;
   bool conv = false;
-  double rr = 0.0;
-  long long it = pcg_loop<double>(g, v, a.maxiter, atol2, ctx, scratch, 0, conv, ok, rr);
+  while (ok) {
+    const bool small = rr < atol2;
+    if (small && !MIXED) { conv = true; break; }
+    if (!small && it >= a.maxiter) break;
+    if (MIXED && (small || rr < a.replace_drop * a.replace_drop * rr_ref)) {
+      // FP64 residual replacement r = b - S x (x is FP64) followed by a CG
+      // restart: in FP32 the recurrences r, s drift from b - S x and S p
+      // (the true residual stalls near eps32 * kappa), so each replacement
+      // starts a fresh Krylov cycle from the FP64 iterate
+      double rb[2] = {0.0, 0.0};
+      residual_pass<T>(g, a.s64[0], a.s64[1], a.s64[2], a.b, a.x, v.r[cur], true, rb[0], rb[1]);
+      ++replacements;
+      ++applies;
+      if (!(ok = gs.sum<2>(rb, scratch))) break;
+      if (rb[1] < atol2) { rr = rb[1]; conv = true; break; }
+      if (it >= a.maxiter) { rr = rb[1]; break; }
+      double rd[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+      w_pass<T>(g, v, cur, true, rd);
+      ++applies;
+      if (!(ok = gs.sum<6>(rd, scratch))) break;
+      beta = 0.0;
+      denom = rd[1];
+      gamma = rd[0];
+      rr = rd[5];
+      rr_ref = rr;
+      continue;
+    }
+    const double alpha_d = gamma / denom;
+    const T b_t = (T)beta, alpha = (T)alpha_d;
+    const int nxt = cur ^ 1;
+    const T* rc = v.r[cur];
+    const T* wc = v.w[cur];
+    const T* sc = v.s[cur];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) red[k] = 0.0;
+    for (int idx = gtid; idx < g.ndof; idx += G) {
+      int i0, i1, i2;
+      coords3(g, idx, i0, i1, i2);
+      const T ri = rc[idx];
+      const T ui = v.dinv[idx] * ri;
+      const T si = wc[idx] + b_t * sc[idx];
+      const T pi = ui + b_t * v.p[idx];
+      v.p[idx] = pi;
+      a.x[idx] += alpha_d * (double)pi;
+      const T rn = ri - alpha * si;
+      const T un = v.dinv[idx] * rn;
+      T wn;
+      if (idx == g.pin) {
+        wn = un;
+      } else {
+        auto unb = [&](int j) -> T {
+          if (j == g.pin) return T(0);
+          return v.dinv[j] * (rc[j] - alpha * (wc[j] + b_t * sc[j]));
+        };
+        T d, off;
+        s_row<T>(g, idx, i0, i1, i2, v.s0, v.s1, v.s2, unb, d, off);
+        wn = d * un - off;
+      }
+      v.r[nxt][idx] = rn;
+      v.s[nxt][idx] = si;
+      v.w[nxt][idx] = wn;
+      red[0] += (double)rn * (double)un;
+      red[1] += (double)wn * (double)un;
+      red[2] += (double)un * (double)si;
+      red[3] += (double)pi * (double)wn;
+      red[4] += (double)pi * (double)si;
+      red[5] += (double)rn * (double)rn;
+    }
+    ok = gs.sum<6>(red, scratch);
+    const double gnew = red[0];
+    beta = gnew / gamma;
+    denom = red[1] + beta * (red[2] + red[3]) + beta * beta * red[4];
+    gamma = gnew;
+    rr = red[5];
+    cur = nxt;
+    ++it;
+    ++applies;
+  }
   if (gtid == 0) {
     a.st->iters = it;
-    a.st->applies = it + (a.x_nonzero ? 1 : 0);
-    a.st->refinements = 0;
+    a.st->applies = applies;
+    a.st->refinements = replacements;
     a.st->rr = rr;
     a.st->bb = bb;
-    a.st->converged = conv ? 1 : 0;
-  }
-}
-
-// Mixed precision: FP64 residual / update, FP32 inner PCG (dots in FP64).
-__global__ void __launch_bounds__(kThreads) pcg_mixed_kernel(PcgArgs a) {
-  __shared__ double scratch[160];
-  GridCtx ctx{tpf::GridBarrier{a.bar, a.err, kSpinLimit}, a.part, gridDim.x};
-  const Grid3& g = a.g;
-  const PcgVecs<double>& v = a.v64;
-  const PcgVecs<float>& w = a.v32;
-  const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int G = gridDim.x * blockDim.x;
-  double bb = -1.0, rr = 0.0;
-  long long inner_total = 0, sweeps = 0;
-  bool conv = false, ok = true;
-  double atol2 = 0.0;
-  for (;;) {
-    // FP64 residual of the current x64: r64 = b - S x64
-    double red[2] = {0.0, 0.0};
-    for (int idx = gtid; idx < g.ndof; idx += G) {
-      double bi = a.b[idx];
-      double sx;
-      if (idx == g.pin) sx = v.x[idx];
-      else {
-        int i0, i1, i2;
-        coords3(g, idx, i0, i1, i2);
-        double d, off;
-        s_row<double>(g, idx, i0, i1, i2, v.s0, v.s1, v.s2,
-                      [&](int j) { return (j == g.pin) ? 0.0 : v.x[j]; }, d, off);
-        sx = d * v.x[idx] - off;
-      }
-      double r = bi - sx;
-      v.r[idx] = r;
-      red[0] += r * r;
-      red[1] += bi * bi;
-    }
-    ok = ctx.reduce(red, 2, scratch);
-    if (!ok) break;
-    rr = red[0];
-    if (bb < 0.0) {
-      bb = red[1];
-      atol2 = (a.tol * sqrt(bb)) * (a.tol * sqrt(bb));
-      if (bb == 0.0) { conv = true; break; }
-    }
-    if (rr < atol2) { conv = true; break; }
-    if (sweeps >= a.max_refine) break;
-    // FP32 inner solve on the normalized residual
-    const double scale = 1.0 / sqrt(rr);
-    for (int idx = gtid; idx < g.ndof; idx += G) {
-      w.r[idx] = (float)(v.r[idx] * scale);
-      w.x[idx] = 0.0f;
-    }
-    // pcg_loop starts with a reduction barrier, which orders these writes
-    bool iconv = false;
-    double irr = 0.0;
-    long long it = pcg_loop<float>(g, w, a.maxiter, a.inner_tol * a.inner_tol, ctx, scratch, 0, iconv, ok, irr);
-    inner_total += it;
-    ++sweeps;
-    if (!ok) break;
-    for (int idx = gtid; idx < g.ndof; idx += G) v.x[idx] += (double)w.x[idx] / scale;
-    // the residual pass reads x64 at neighbours: order the updates
-    if (!ctx.gb.sync(ctx.nb)) { ok = false; break; }
-  }
-  if (gtid == 0) {
-    a.st->iters = inner_total;
-    a.st->applies = inner_total + sweeps + 1;
-    a.st->refinements = sweeps;
-    a.st->rr = rr;
-    a.st->bb = bb < 0.0 ? 0.0 : bb;
     a.st->converged = conv ? 1 : 0;
   }
 }
@@ -726,8 +762,8 @@ struct tpf_ppe {
   // Krylov workspace
   double* x = nullptr; double* r = nullptr; double* z = nullptr; double* p0 = nullptr; double* p1 = nullptr;
   double* q = nullptr; double* b = nullptr; double* t1 = nullptr; double* t2 = nullptr;
-  float* x32 = nullptr; float* r32 = nullptr; float* z32 = nullptr; float* p032 = nullptr; float* p132 = nullptr;
-  float* q32 = nullptr;
+  double* c64[7] = {};            // CG: r[2], w[2], s[2], p (FP64)
+  float* c32[7] = {};             // CG: r[2], w[2], s[2], p (FP32, mixed)
   double* ones64 = nullptr;
   float* ones32 = nullptr;
   double* V = nullptr;            // GMRES basis (restart+1) x ndof
@@ -984,28 +1020,32 @@ int solve_cg(tpf_ppe* h, const double* rhs, double* p, const double* p_init, cud
   TPF_CUDA_TRY(cudaMemsetAsync(h->err, 0, sizeof(int), s));
   TPF_CUDA_TRY(cudaMemsetAsync(h->st, 0, sizeof(SolveStatus), s));
   const bool none = (h->o.precond == TPF_PRECOND_NONE);
-  PcgArgs a{};
+  Cg1Args a{};
   a.g = g;
-  a.v64 = PcgVecs<double>{h->s[0], h->s[1], h->s[2], none ? h->ones64 : h->dinvS, h->x, h->r, h->z, h->p0, h->p1, h->q};
-  a.v32 = PcgVecs<float>{h->s32[0], h->s32[1], h->s32[2], none ? h->ones32 : h->dinvS32,
-                         h->x32, h->r32, h->z32, h->p032, h->p132, h->q32};
+  a.v64.s0 = h->s[0]; a.v64.s1 = h->s[1]; a.v64.s2 = h->s[2];
+  a.v64.dinv = none ? h->ones64 : h->dinvS;
+  a.v32.s0 = h->s32[0]; a.v32.s1 = h->s32[1]; a.v32.s2 = h->s32[2];
+  a.v32.dinv = none ? h->ones32 : h->dinvS32;
+  for (int k = 0; k < 2; ++k) {
+    a.v64.r[k] = h->c64[k]; a.v64.w[k] = h->c64[2 + k]; a.v64.s[k] = h->c64[4 + k];
+    a.v32.r[k] = h->c32[k]; a.v32.w[k] = h->c32[2 + k]; a.v32.s[k] = h->c32[4 + k];
+  }
+  a.v64.p = h->c64[6];
+  a.v32.p = h->c32[6];
+  a.s64[0] = h->s[0]; a.s64[1] = h->s[1]; a.s64[2] = h->s[2];
   a.b = h->b;
+  a.x = h->x;
   a.tol = h->o.tol;
   a.x_nonzero = p_init ? 1 : 0;
   a.part = h->part;
-  a.bar = h->bar;
+  a.count = h->bar;
   a.err = h->err;
   a.st = h->st;
   const bool mixed = (h->o.precision == TPF_PREC_MIXED);
-  if (mixed) {
-    a.maxiter = h->o.maxiter;
-    a.max_refine = h->o.max_refine;
-    a.inner_tol = h->o.inner_tol;
-  } else {
-    a.maxiter = h->o.maxiter;
-  }
+  a.maxiter = h->o.maxiter;
+  a.replace_drop = h->o.inner_tol > 0.0 ? h->o.inner_tol : 1e-3;
   void* args[] = {&a};
-  void* fn = mixed ? (void*)pcg_mixed_kernel : (void*)pcg64_kernel;
+  void* fn = mixed ? (void*)cg1_kernel<float, true> : (void*)cg1_kernel<double, false>;
   TPF_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(h->coop_blocks), dim3(kThreads), args, 0, s));
   copy_pin0_kernel<<<ew_grid(h), 256, 0, s>>>(n, g.pin, h->x, p);
   SolveStatus hs{};
@@ -1021,7 +1061,7 @@ int solve_cg(tpf_ppe* h, const double* rhs, double* p, const double* p_init, cud
   res->applies = hs.applies;
   res->refinements = hs.refinements;
   res->rel_residual = hs.bb > 0.0 ? std::sqrt(hs.rr / hs.bb) : 0.0;
-  res->info = hs.converged ? 0 : (int)std::min<long long>(mixed ? h->o.max_refine : h->o.maxiter, 0x7fffffff);
+  res->info = hs.converged ? 0 : (int)std::min<long long>(h->o.maxiter, 0x7fffffff);
   if (!hs.converged) {
     tpf::set_error("PPESolverFVMMatrixFree did not converge cleanly (info=%d); no alternate PPE solver was applied.",
                    res->info);
@@ -1044,7 +1084,7 @@ void tpf_ppe_default_options(tpf_ppe_options* o) {
   o->restart = 80;
   o->c_tau = 2.0;
   o->pcr_stages = 4;
-  o->inner_tol = 1e-4;
+  o->inner_tol = 1e-3;
   o->max_refine = 50;
 }
 
@@ -1116,9 +1156,13 @@ int tpf_ppe_create(tpf_ppe** out, int ndim, const int64_t* N, const double* cons
                       &h->ones64};
   for (double** pp : d64)
     if ((st = dalloc(h, pp, n))) return fail(st);
-  float** d32[] = {&h->dinvS32, &h->x32, &h->r32, &h->z32, &h->p032, &h->p132, &h->q32, &h->ones32};
+  float** d32[] = {&h->dinvS32, &h->ones32};
   for (float** pp : d32)
     if ((st = dalloc(h, pp, n))) return fail(st);
+  for (int k = 0; k < 7; ++k) {
+    if ((st = dalloc(h, &h->c64[k], n))) return fail(st);
+    if ((st = dalloc(h, &h->c32[k], n))) return fail(st);
+  }
   // ones: the identity preconditioner of the CG route ('none')
   {
     std::vector<double> ones(n, 1.0);
@@ -1132,8 +1176,8 @@ int tpf_ppe_create(tpf_ppe** out, int ndim, const int64_t* N, const double* cons
   // cooperative grid for the persistent PCG kernels
   int dev = 0, nsm = tpf::sm_count(), occ64 = 0, occmx = 0;
   cudaGetDevice(&dev);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ64, pcg64_kernel, kThreads, 0) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occmx, pcg_mixed_kernel, kThreads, 0) != cudaSuccess) {
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ64, cg1_kernel<double, false>, kThreads, 0) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occmx, cg1_kernel<float, true>, kThreads, 0) != cudaSuccess) {
     tpf::set_error("occupancy query failed");
     return fail(TPF_ECUDA);
   }
@@ -1141,7 +1185,7 @@ int tpf_ppe_create(tpf_ppe** out, int ndim, const int64_t* N, const double* cons
   int need = (int)((n + kThreads - 1) / kThreads);
   h->coop_blocks = std::max(1, std::min(nsm * per_sm, need));
   h->ew_blocks = std::max(1, std::min(nsm * 8, (int)((n + 255) / 256)));
-  h->part_len = std::max(8 * h->coop_blocks, (o.restart + 2) * h->ew_blocks);
+  h->part_len = std::max(16 * h->coop_blocks, (o.restart + 2) * h->ew_blocks);
   if ((st = dalloc(h, &h->part, (size_t)h->part_len))) return fail(st);
   if ((st = dalloc(h, &h->bar, 4))) return fail(st);
   if ((st = dalloc(h, &h->err, 1))) return fail(st);
@@ -1168,7 +1212,7 @@ int tpf_ppe_set_options(tpf_ppe* h, const tpf_ppe_options* o) {
   if (grow) {
     cudaFree(h->part);
     h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void*)h->part), h->allocs.end());
-    h->part_len = std::max(8 * h->coop_blocks, (o->restart + 2) * h->ew_blocks);
+    h->part_len = std::max(16 * h->coop_blocks, (o->restart + 2) * h->ew_blocks);
     if ((st = dalloc(h, &h->part, (size_t)h->part_len))) return st;
   }
   if (line_changed) h->prepared = false;

@@ -48,8 +48,8 @@ __device__ __forceinline__ T warp_sum(T v) {
   return v;
 }
 
-// Block-wide sum of up to 4 values; every thread receives the totals.
-// scratch must hold 4 * 32 doubles.
+// Block-wide sum of NV values; every thread receives the totals.
+// scratch must hold NV * 32 doubles.
 template <int NV>
 __device__ __forceinline__ void block_sum(double (&v)[NV], double* scratch) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;

@@ -1,0 +1,106 @@
+"""Run single hot-path kernels on synthetic inputs for timing and profiling.
+
+    python -m twophaseflow_b200.kernel_cases ccd --N 256 256 256 --axis 0 --bc wall [--dtype f64] [--reps 5]
+    python -m twophaseflow_b200.kernel_cases ppe --N 512 512 [--precision fp64] [--reps 2]
+
+``ccd`` captures ``reps`` CCDSolver.differentiate calls in one CUDA graph and
+replays it, so the reported time is device time per call (no Python launch
+overhead), and prints achieved GB/s over the algorithmic 3 x field bytes.
+``ppe`` runs full CG+Jacobi solves (one persistent kernel each).
+Used for the ncu captures summarised under profiles/.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import sys
+
+
+def ccd_case(N, axis, bc, dtype, reps, warmup=3):
+    import torch
+    from . import CCDSolver, UniformGrid
+    from .workloads import fourier_field
+    dt = torch.float64 if dtype == "f64" else torch.float32
+    f = torch.from_numpy(fourier_field(N, seed=0)).to("cuda").to(dt)
+    ccd = CCDSolver(UniformGrid(N), None, bc_type=bc, dtype=dt)
+    for _ in range(warmup):
+        ccd.differentiate(f, axis)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        outs = []
+        with torch.cuda.graph(g, stream=s):
+            for _ in range(reps):
+                outs.append(ccd.differentiate(f, axis))
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    g.replay()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    g.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    nbytes = 3 * f.numel() * f.element_size()
+    return {"case": "ccd", "N": list(N), "axis": axis, "bc": bc, "dtype": dtype, "us_per_call": round(ms * 1e3, 2),
+            "GBps": round(nbytes / (ms * 1e-3) / 1e9, 1), "alg_bytes": nbytes}
+
+
+def ppe_case(N, precision, reps, tol=1e-8):
+    import torch
+    from . import PPESolverFVMMatrixFree, UniformGrid
+    from .workloads import divergence_rhs, droplet_density
+
+    class Cfg:
+        pseudo_tol = tol
+        pseudo_maxiter = 1_000_000
+        ppe_iteration_method = "cg"
+        ppe_preconditioner = "jacobi"
+        ppe_precision = precision
+
+    rho = torch.from_numpy(droplet_density(N, seed=0)).cuda()
+    rhs = torch.from_numpy(divergence_rhs(N, seed=1)).cuda()
+    s = PPESolverFVMMatrixFree(None, Cfg(), UniformGrid(N))
+    s.solve(rhs, rho)
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        s.solve(rhs, rho)
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    d = s.last_diagnostics
+    it = d["ppe_low_order_cg_iterations"]
+    ms = min(ts)
+    return {"case": "ppe", "N": list(N), "precision": precision, "ms": round(ms, 3), "iterations": it,
+            "us_per_iteration": round(ms * 1e3 / max(it, 1), 2)}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("case", choices=["ccd", "ppe"])
+    ap.add_argument("--N", type=int, nargs="+", required=True)
+    ap.add_argument("--axis", type=int, default=0)
+    ap.add_argument("--bc", default="wall")
+    ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--reps", type=int, default=5)
+    a = ap.parse_args(argv)
+    if a.case == "ccd":
+        r = ccd_case(tuple(a.N), a.axis, a.bc, a.dtype, a.reps)
+    else:
+        r = ppe_case(tuple(a.N), a.precision, a.reps)
+    print(json.dumps(r), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

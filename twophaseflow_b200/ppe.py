@@ -79,7 +79,7 @@ class PPESolverFVMMatrixFree:
             raise ValueError(f"ppe_precision must be 'fp64' or 'mixed', got {self.precision!r}")
         if self.precision == "mixed" and method != "cg":
             raise ValueError("ppe_precision='mixed' runs the CG route (ppe_iteration_method='cg')")
-        self.inner_tol = float(getattr(solver_cfg, "ppe_inner_tol", 1e-4))
+        self.inner_tol = float(getattr(solver_cfg, "ppe_inner_tol", 1e-3))
         self.max_refine = int(getattr(solver_cfg, "ppe_max_refine", 60))
         if bc_spec is not None:
             self._pin_dof = int(bc_spec.pin_dof)
