@@ -520,6 +520,379 @@ __global__ void __launch_bounds__(512, 1) ccd_line_kernel(CcdArgs a) {
   cp_async_wait<0>();
 }
 
+// ---- warp-per-line fast path ------------------------------------------------------
+//
+// One warp solves one line: lane q owns rows [qR, qR+R) in registers.  The
+// chunk carries of the two block-Thomas sweeps are affine maps (M, v) that
+// compose as (M2, v2) o (M1, v1) = (M2 M1, v2 + M2 v1); a Kogge-Stone scan of
+// them over the 32 lanes (shuffles, no block barrier) gives every lane its
+// exact carry.  The tile of W lines is staged in shared memory by cp.async
+// (double-buffered) with one padding element per R rows, so lanes reading
+// rows R apart hit distinct banks; results are staged back for coalesced stores.
+
+template <typename T>
+struct Aff { T m0, m1, m2, m3, v0, v1; };
+
+template <typename T>
+__device__ __forceinline__ Aff<T> aff_compose(const Aff<T>& hi, const Aff<T>& lo) {
+  Aff<T> r;
+  r.m0 = hi.m0 * lo.m0 + hi.m1 * lo.m2;
+  r.m1 = hi.m0 * lo.m1 + hi.m1 * lo.m3;
+  r.m2 = hi.m2 * lo.m0 + hi.m3 * lo.m2;
+  r.m3 = hi.m2 * lo.m1 + hi.m3 * lo.m3;
+  r.v0 = hi.v0 + hi.m0 * lo.v0 + hi.m1 * lo.v1;
+  r.v1 = hi.v1 + hi.m2 * lo.v0 + hi.m3 * lo.v1;
+  return r;
+}
+
+template <typename T>
+__device__ __forceinline__ Aff<T> aff_shfl_up(const Aff<T>& a, int d) {
+  Aff<T> r;
+  r.m0 = __shfl_up_sync(0xffffffffu, a.m0, d); r.m1 = __shfl_up_sync(0xffffffffu, a.m1, d);
+  r.m2 = __shfl_up_sync(0xffffffffu, a.m2, d); r.m3 = __shfl_up_sync(0xffffffffu, a.m3, d);
+  r.v0 = __shfl_up_sync(0xffffffffu, a.v0, d); r.v1 = __shfl_up_sync(0xffffffffu, a.v1, d);
+  return r;
+}
+
+template <typename T>
+__device__ __forceinline__ Aff<T> aff_shfl_down(const Aff<T>& a, int d) {
+  Aff<T> r;
+  r.m0 = __shfl_down_sync(0xffffffffu, a.m0, d); r.m1 = __shfl_down_sync(0xffffffffu, a.m1, d);
+  r.m2 = __shfl_down_sync(0xffffffffu, a.m2, d); r.m3 = __shfl_down_sync(0xffffffffu, a.m3, d);
+  r.v0 = __shfl_down_sync(0xffffffffu, a.v0, d); r.v1 = __shfl_down_sync(0xffffffffu, a.v1, d);
+  return r;
+}
+
+template <typename T>
+__device__ __forceinline__ Aff<T> aff_identity() { return {T(1), T(0), T(0), T(1), T(0), T(0)}; }
+
+// copy tile t (TL lines) into fb[l*FSP + k + k/R]
+template <typename T, bool CONTIG, int R>
+__device__ __forceinline__ void issue_tile_padded(const CcdArgs& a, const T* __restrict__ f, T* fb, long long* lb,
+                                                  int t) {
+  const int TL = a.TL, n = a.n, FSP = a.FS;
+  const int64_t line0 = (int64_t)t * TL;
+  if (threadIdx.x < TL) {
+    const int64_t line = line0 + threadIdx.x;
+    long long b = -1;
+    if (line < a.n_lines) {
+      if (CONTIG) b = line * n;
+      else {
+        const int64_t o = line / a.inner, i = line - o * a.inner;
+        b = o * (int64_t)n * a.inner + i;
+      }
+    }
+    lb[threadIdx.x] = b;
+  }
+  __syncthreads();
+  const int total = TL * n;
+  if (CONTIG) {
+    // consecutive threads -> consecutive k of one line (coalesced)
+    int l = threadIdx.x / n, k = threadIdx.x - (threadIdx.x / n) * n;
+    const int step_l = blockDim.x / n, step_k = blockDim.x - step_l * n;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      const long long b = lb[l];
+      cp_async<sizeof(T)>(fb + l * FSP + k + k / R, b >= 0 ? f + b + k : f, b >= 0);
+      l += step_l;
+      k += step_k;
+      if (k >= n) { k -= n; ++l; }
+    }
+  } else {
+    // consecutive threads -> consecutive lines at one k (coalesced)
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      const int k = e >> a.tl_shift, l = e & (TL - 1);
+      const long long b = lb[l];
+      cp_async<sizeof(T)>(fb + l * FSP + k + k / R, b >= 0 ? f + b + (int64_t)k * a.inner : f, b >= 0);
+    }
+  }
+  cp_async_commit();
+}
+
+template <typename T, bool PERIODIC, bool CONTIG, int R>
+__global__ void __launch_bounds__(256) ccd_warp_kernel(CcdArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int TL = a.TL, n = a.n, n_rows = a.n_rows, H0 = a.H0, FSP = a.FS;
+  const TabLayout lay{R, H0};
+  const int fsz = TL * FSP;
+  // shared: lbase(2 x TL) | tab | fbuf[nbuf] | sbuf
+  long long* lbase = reinterpret_cast<long long*>(smem_raw);
+  T* tab = reinterpret_cast<T*>(lbase + 2 * TL);
+  T* fbuf = tab + ((a.tab_total + 1) & ~1);
+  T* sbuf = fbuf + (size_t)a.nbuf * fsz;
+
+  const T* __restrict__ f = static_cast<const T*>(a.f);
+  const T* tabT = static_cast<const T*>(a.tabT);
+  for (int i = threadIdx.x; i < a.tab_total; i += blockDim.x) tab[i] = tabT[i];
+  __syncthreads();
+
+  const int lane = threadIdx.x & 31;
+  const int wl = threadIdx.x >> 5;              // line of the tile owned by this warp
+  const int j0 = lane * R;
+  const int cnt = max(0, min(R, n_rows - j0));  // rows of this lane
+  const T c1 = tab[lay.bc() + 30], c2 = tab[lay.bc() + 31];
+  const T* Lfi = tab + lay.cst();
+  const T Lf0 = Lfi[0], Lf1 = Lfi[1], Lf2 = Lfi[2], Lf3 = Lfi[3];
+  const T P0 = Lfi[4], P1 = Lfi[5], P2 = Lfi[6], P3 = Lfi[7];
+  const T H0m = Lfi[8], H1m = Lfi[9], H2m = Lfi[10], H3m = Lfi[11];
+  const T* Plast = Lfi + 12;
+  const T* Phi = tab + lay.phi();
+  const T* Psi = tab + lay.psi();
+  const T* head = tab + lay.head();
+  const double* tb = a.tab + lay.bc();
+  const double* J = a.J;
+  const bool in_head = !PERIODIC && j0 < H0;
+
+  int t = blockIdx.x;
+  int buf = 0;
+  if (t < a.n_tiles) issue_tile_padded<T, CONTIG, R>(a, f, fbuf, lbase, t);
+  for (; t < a.n_tiles; t += gridDim.x) {
+    const int tn = t + gridDim.x;
+    if (a.nbuf == 2 && tn < a.n_tiles) {
+      issue_tile_padded<T, CONTIG, R>(a, f, fbuf + (size_t)(buf ^ 1) * fsz, lbase + (buf ^ 1) * TL, tn);
+      cp_async_wait<1>();
+    } else {
+      if (a.nbuf == 1 && t != (int)blockIdx.x) issue_tile_padded<T, CONTIG, R>(a, f, fbuf, lbase, t);
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    T* fl = fbuf + (size_t)buf * fsz + wl * FSP;   // this warp's line (padded)
+    T* sl = sbuf + wl * FSP;
+    const long long* lb = lbase + buf * TL;
+    const bool valid = wl < TL && lb[wl] >= 0;
+    auto F = [&](int k) -> T { return fl[k + k / R]; };
+
+    if (wl < TL) {
+      // ---- closures (FP64, lanes 0 and last) --------------------------------
+      const int last = (n_rows - 1) / R;
+      double bl0 = 0.0, bl1 = 0.0, br0 = 0.0, br1 = 0.0;
+      if (!PERIODIC) {
+        if (lane == 0) {
+          if (a.ovl) { bl0 = a.bcl0; bl1 = a.bcl1; }
+          else {
+            double fv[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) fv[k] = (double)F(k);
+            bl0 = tb[16] * fv[0] + tb[17] * fv[1] + tb[18] * fv[2] + tb[19] * fv[3];
+            bl1 = tb[24] * fv[0] + tb[25] * fv[1] + tb[26] * fv[2] + tb[27] * fv[3] + tb[28] * fv[4] + tb[29] * fv[5];
+          }
+        }
+        if (lane == last) {
+          if (a.ovr) { br0 = a.bcr0; br1 = a.bcr1; }
+          else {
+            double fv[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) fv[k] = (double)F(n - 1 - k);
+            br0 = tb[20] * fv[0] + tb[21] * fv[1] + tb[22] * fv[2] + tb[23] * fv[3];
+            br1 = tb[24] * fv[0] + tb[25] * fv[1] + tb[26] * fv[2] + tb[27] * fv[3] + tb[28] * fv[4] + tb[29] * fv[5];
+          }
+        }
+      }
+      // ---- forward local sweep ------------------------------------------------
+      V2<T> y[R];
+      const int Nn = n - 1;
+      const int off = PERIODIC ? 0 : 1;
+      auto node = [&](int k) -> int {
+        if (PERIODIC) { if (k < 0) return k + Nn; if (k >= Nn) return k - Nn; }
+        return k;
+      };
+      V2<T> prev{T(0), T(0)};
+      if (cnt > 0) {
+        T fm = F(node(j0 + off - 1));
+        T f0 = F(node(j0 + off));
+#pragma unroll R
+        for (int r = 0; r < R; ++r) {
+          const int j = j0 + r;
+          if (r < cnt) {
+            const T fp = F(node(j + off + 1));
+            V2<T> b{c1 * (fp - fm), c2 * ((fm - T(2) * f0) + fp)};
+            if (!PERIODIC) {
+              if (j == 0) {
+                b.a = (T)((double)b.a - (tb[0] * bl0 + tb[1] * bl1));
+                b.b = (T)((double)b.b - (tb[2] * bl0 + tb[3] * bl1));
+              }
+              if (j == n_rows - 1) {
+                b.a = (T)((double)b.a - (tb[4] * br0 + tb[5] * br1));
+                b.b = (T)((double)b.b - (tb[6] * br0 + tb[7] * br1));
+              }
+            }
+            if (r == 0) {
+              prev = b;
+            } else if (in_head && j < H0) {
+              const V2<T> q = mv(head + 20 * j, prev);
+              prev = {b.a - q.a, b.b - q.b};
+            } else {
+              prev = {b.a - (Lf0 * prev.a + Lf1 * prev.b), b.b - (Lf2 * prev.a + Lf3 * prev.b)};
+            }
+            y[r] = prev;
+            fm = f0;
+            f0 = fp;
+          }
+        }
+      }
+      // ---- forward carry scan over lanes ---------------------------------------
+      {
+        Aff<T> m = aff_identity<T>();
+        if (cnt > 0) {
+          const int e = j0 + cnt;
+          const T* Tm = (in_head && e - 1 < H0) ? head + 20 * (e - 1) + 12 : Phi + 4 * (cnt - 1);
+          m = {Tm[0], Tm[1], Tm[2], Tm[3], prev.a, prev.b};
+        }
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const Aff<T> o = aff_shfl_up(m, d);
+          if (lane >= d) m = aff_compose(m, o);
+        }
+        Aff<T> ex = aff_shfl_up(m, 1);
+        if (lane == 0) ex = aff_identity<T>();
+        V2<T> Yin{ex.v0, ex.v1};
+        if (PERIODIC) {
+          // ring closure: Y_{-1} = Gf * (scan result of the last lane)
+          const T l0 = __shfl_sync(0xffffffffu, m.v0, 31), l1 = __shfl_sync(0xffffffffu, m.v1, 31);
+          const V2<T> ring = mv(Lfi + 16, V2<T>{l0, l1});
+          Yin = {ex.v0 + ex.m0 * ring.a + ex.m1 * ring.b, ex.v1 + ex.m2 * ring.a + ex.m3 * ring.b};
+        }
+        if ((PERIODIC || lane > 0) && cnt > 0) {
+#pragma unroll R
+          for (int r = 0; r < R; ++r) {
+            const int j = j0 + r;
+            if (r < cnt) {
+              const T* mm = (in_head && j < H0) ? head + 20 * j + 12 : Phi + 4 * r;
+              y[r].a += mm[0] * Yin.a + mm[1] * Yin.b;
+              y[r].b += mm[2] * Yin.a + mm[3] * Yin.b;
+            }
+          }
+        }
+      }
+      // ---- backward local sweep -----------------------------------------------
+      V2<T> xn{T(0), T(0)};
+#pragma unroll R
+      for (int r = R - 1; r >= 0; --r) {
+        const int j = j0 + r;
+        if (r < cnt) {
+          V2<T> x;
+          if (in_head && j < H0) {
+            const V2<T> pp = mv(head + 20 * j + 4, y[r]);
+            const V2<T> qq = mv(head + 20 * j + 8, xn);
+            x = {pp.a - qq.a, pp.b - qq.b};
+          } else if (!PERIODIC && j == n_rows - 1) {
+            x = mv(Plast, y[r]);
+          } else {
+            x = {(P0 * y[r].a + P1 * y[r].b) - (H0m * xn.a + H1m * xn.b),
+                 (P2 * y[r].a + P3 * y[r].b) - (H2m * xn.a + H3m * xn.b)};
+          }
+          y[r] = x;
+          xn = x;
+        }
+      }
+      // ---- backward carry scan over lanes (suffix) -----------------------------------
+      {
+        Aff<T> m = aff_identity<T>();
+        if (cnt > 0) {
+          const T* Rm = (in_head && j0 < H0) ? head + 20 * j0 + 16 : Psi + 4 * cnt;
+          m = {Rm[0], Rm[1], Rm[2], Rm[3], xn.a, xn.b};
+        }
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const Aff<T> o = aff_shfl_down(m, d);
+          if (lane + d < 32) m = aff_compose(m, o);
+        }
+        Aff<T> ex = aff_shfl_down(m, 1);
+        if (lane == 31) ex = aff_identity<T>();
+        V2<T> Xin{ex.v0, ex.v1};
+        if (PERIODIC) {
+          const T l0 = __shfl_sync(0xffffffffu, m.v0, 0), l1 = __shfl_sync(0xffffffffu, m.v1, 0);
+          const V2<T> ring = mv(Lfi + 20, V2<T>{l0, l1});
+          Xin = {ex.v0 + ex.m0 * ring.a + ex.m1 * ring.b, ex.v1 + ex.m2 * ring.a + ex.m3 * ring.b};
+        }
+        if ((PERIODIC || lane < last) && cnt > 0) {
+#pragma unroll R
+          for (int r = 0; r < R; ++r) {
+            const int j = j0 + r;
+            if (r < cnt) {
+              const T* mm = (in_head && j < H0) ? head + 20 * j + 16 : Psi + 4 * (cnt - r);
+              y[r].a += mm[0] * Xin.a + mm[1] * Xin.b;
+              y[r].b += mm[2] * Xin.a + mm[3] * Xin.b;
+            }
+          }
+        }
+      }
+      // ---- stage (d1, d2) in (own f line, sbuf line) --------------------------------------
+      __syncwarp();
+#pragma unroll R
+      for (int r = 0; r < R; ++r) {
+        if (r < cnt) {
+          const int k = PERIODIC ? j0 + r : j0 + r + 1;
+          fl[k + k / R] = y[r].a;
+          sl[k + k / R] = y[r].b;
+        }
+      }
+      if (!PERIODIC) {
+        if (lane == 0 && cnt > 0) {
+          const double x0 = (double)y[0].a, x1 = (double)y[0].b;
+          fl[0] = (T)((tb[8] * x0 + tb[9] * x1) + bl0);
+          sl[0] = (T)((tb[10] * x0 + tb[11] * x1) + bl1);
+        }
+        if (lane == last) {
+#pragma unroll R
+          for (int r = 0; r < R; ++r)
+            if (r == cnt - 1) {
+              const double x0 = (double)y[r].a, x1 = (double)y[r].b;
+              const int k = n - 1;
+              fl[k + k / R] = (T)((tb[12] * x0 + tb[13] * x1) + br0);
+              sl[k + k / R] = (T)((tb[14] * x0 + tb[15] * x1) + br1);
+            }
+        }
+      } else if (lane == 0) {
+        const int k = n - 1;
+        fl[k + k / R] = y[0].a;
+        sl[k + k / R] = y[0].b;
+      }
+      (void)valid;
+    }
+    __syncthreads();
+    // ---- coalesced stores of the tile ---------------------------------------------------
+    {
+      const T* f1 = fbuf + (size_t)buf * fsz;
+      auto metric = [&](int k, double& o1, double& o2) {
+        if (J) {
+          const double Jk = J[k], dJk = J[n + k];
+          o2 = Jk * Jk * o2 + Jk * dJk * o1;
+          o1 = Jk * o1;
+        }
+      };
+      const int total = TL * n;
+      if (CONTIG) {
+        int l = threadIdx.x / n, k = threadIdx.x - (threadIdx.x / n) * n;
+        const int step_l = blockDim.x / n, step_k = blockDim.x - step_l * n;
+        for (int e = threadIdx.x; e < total; e += blockDim.x) {
+          const long long b = lb[l];
+          if (b >= 0) {
+            double o1 = (double)f1[l * FSP + k + k / R], o2 = (double)sbuf[l * FSP + k + k / R];
+            metric(k, o1, o2);
+            store_out<T>(a, b + k, o1, o2);
+          }
+          l += step_l;
+          k += step_k;
+          if (k >= n) { k -= n; ++l; }
+        }
+      } else {
+        for (int e = threadIdx.x; e < total; e += blockDim.x) {
+          const int k = e >> a.tl_shift, l = e & (TL - 1);
+          const long long b = lb[l];
+          if (b >= 0) {
+            double o1 = (double)f1[l * FSP + k + k / R], o2 = (double)sbuf[l * FSP + k + k / R];
+            metric(k, o1, o2);
+            store_out<T>(a, b + (int64_t)k * a.inner, o1, o2);
+          }
+        }
+      }
+    }
+    __syncthreads();
+    buf ^= (a.nbuf == 2) ? 1 : 0;
+  }
+  cp_async_wait<0>();
+}
+
 template <typename T>
 __global__ void wall_zero_kernel(T* g, int64_t outer, int64_t n, int64_t inner) {
   int64_t tot = outer * inner * 2;
@@ -575,11 +948,13 @@ int build_tables(tpf_ccd_plan* p, std::vector<double>& tab) {
     // smallest head (a multiple of C) beyond which the factors sit at the fixed point
     H0 = n_rows;
     for (int hh = C; hh < n_rows; hh += C) {
+      // rows >= hh use the fixed-point Lf (all rows, the last included) and
+      // the fixed-point P, H (all but the last, which carries the closure)
       bool conv = true;
-      for (int j = hh; j < n_rows - 1 && conv; ++j) {
-        const double e = std::max(maxabs(sub(Lf[j], Lfinf)) / maxabs(Lfinf),
-                                  std::max(maxabs(sub(Pm[j], Pinf)) / maxabs(Pinf),
-                                           maxabs(sub(Hm[j], Hinf)) / maxabs(Hinf)));
+      for (int j = hh; j < n_rows && conv; ++j) {
+        double e = maxabs(sub(Lf[j], Lfinf)) / maxabs(Lfinf);
+        if (j < n_rows - 1)
+          e = std::max(e, std::max(maxabs(sub(Pm[j], Pinf)) / maxabs(Pinf), maxabs(sub(Hm[j], Hinf)) / maxabs(Hinf)));
         conv = e < 1e-15;
       }
       if (conv) { H0 = hh; break; }
@@ -716,6 +1091,43 @@ LaunchShape pick_shape(const tpf_ccd_plan* p, bool contig, int64_t n_lines) {
   return best;
 }
 
+template <typename T, int R>
+LaunchShape pick_warp_shape(const tpf_ccd_plan* p, int64_t n_lines) {
+  const int n = (int)p->n_pts;
+  int FSP = n + (n - 1) / R + 1;
+  if (FSP % 2 == 0) ++FSP;
+  const int nsm = tpf::sm_count();
+  const int regs = R == 8 ? 128 : (R == 16 ? 168 : 255);
+  TabLayout lay{R, p->H0};
+  LaunchShape best{};
+  best.TL = 0;
+  double best_score = -1e30;
+  const int tl_opts[4] = {8, 4, 2, 1};
+  for (int t = 0; t < 4; ++t) {
+    const int TL = tl_opts[t];
+    const int threads = 32 * TL;
+    const int64_t tiles = (n_lines + TL - 1) / TL;
+    const size_t fsz = (size_t)TL * FSP;
+    for (int nbuf = 2; nbuf >= 1; --nbuf) {
+      const size_t sm = sizeof(long long) * 2 * TL + sizeof(T) * (((size_t)lay.total() + 1) & ~(size_t)1) +
+                        sizeof(T) * (nbuf + 1) * fsz + 64;
+      if (sm > 225 * 1024) continue;
+      const int by_smem = (int)((228 * 1024) / (sm + 1024));
+      const int by_regs = 65536 / (regs * threads);
+      const int per_sm = std::max(1, std::min(std::min(by_smem, by_regs), 16));
+      const int64_t grid = std::min<int64_t>(tiles, (int64_t)nsm * per_sm);
+      const double waves = (double)tiles / (double)grid;
+      double score = 400.0 * std::min(1.0, (double)grid / nsm) + 0.25 * std::min(per_sm * threads, 2048) +
+                     (nbuf == 2 && waves > 1.5 ? 150.0 : 0.0) - (nbuf == 2 && waves <= 1.0 ? 300.0 : 0.0);
+      if (score > best_score) {
+        best_score = score;
+        best = {TL, 0, FSP, nbuf, (int)grid, sm};
+      }
+    }
+  }
+  return best;
+}
+
 template <typename T>
 int launch_ccd(const tpf_ccd_plan* p, int64_t outer, int64_t inner, const void* f, void* d1, void* d2,
                const double* bcl, const double* bcr, int flags, cudaStream_t stream,
@@ -724,8 +1136,12 @@ int launch_ccd(const tpf_ccd_plan* p, int64_t outer, int64_t inner, const void* 
   const bool contig = (inner == 1);
   const int64_t n_lines = outer * inner;
   if (n_lines == 0) return TPF_OK;
-  TPF_CHECK_ARG(n_lines < ((int64_t)1 << 31) * 1, "too many lines");
-  LaunchShape s = pick_shape<T>(p, contig, n_lines);
+  TPF_CHECK_ARG(n_lines < ((int64_t)1 << 31), "too many lines");
+  const bool warp = (p->C == 8 || p->C == 16 || p->C == 32) && p->n_rows <= 32 * p->C;
+  LaunchShape s = !warp ? pick_shape<T>(p, contig, n_lines)
+                        : (p->C == 8 ? pick_warp_shape<T, 8>(p, n_lines)
+                                     : (p->C == 16 ? pick_warp_shape<T, 16>(p, n_lines)
+                                                   : pick_warp_shape<T, 32>(p, n_lines)));
   TPF_CHECK_ARG(s.TL > 0, "CCD axis of %lld points does not fit the line kernel's shared memory",
                 (long long)p->n_pts);
   CcdArgs a{};
@@ -734,7 +1150,7 @@ int launch_ccd(const tpf_ccd_plan* p, int64_t outer, int64_t inner, const void* 
   a.n = (int)p->n_pts; a.n_rows = p->n_rows; a.C = p->C; a.P = p->P; a.H0 = p->H0; a.TL = s.TL;
   a.tl_shift = 0;
   while ((1 << a.tl_shift) < s.TL) ++a.tl_shift;
-  a.LS = s.LS; a.FS = contig ? s.FS : 0; a.nbuf = s.nbuf;
+  a.LS = s.LS; a.FS = (contig || warp) ? s.FS : 0; a.nbuf = s.nbuf;
   a.n_tiles = (int)((n_lines + s.TL - 1) / s.TL);
   a.tab_total = TabLayout{p->C, p->H0}.total();
   a.tab = p->d_tab;
@@ -750,10 +1166,21 @@ int launch_ccd(const tpf_ccd_plan* p, int64_t outer, int64_t inner, const void* 
   a.vd_accumulate = vd_accumulate;
   const bool per = (p->bc == TPF_BC_PERIODIC) && !a.ovl && !a.ovr;
   void (*kern)(CcdArgs);
-  if (per) kern = contig ? ccd_line_kernel<T, true, true> : ccd_line_kernel<T, true, false>;
-  else kern = contig ? ccd_line_kernel<T, false, true> : ccd_line_kernel<T, false, false>;
+  if (!warp) {
+    if (per) kern = contig ? ccd_line_kernel<T, true, true> : ccd_line_kernel<T, true, false>;
+    else kern = contig ? ccd_line_kernel<T, false, true> : ccd_line_kernel<T, false, false>;
+  } else if (p->C == 8) {
+    if (per) kern = contig ? ccd_warp_kernel<T, true, true, 8> : ccd_warp_kernel<T, true, false, 8>;
+    else kern = contig ? ccd_warp_kernel<T, false, true, 8> : ccd_warp_kernel<T, false, false, 8>;
+  } else if (p->C == 16) {
+    if (per) kern = contig ? ccd_warp_kernel<T, true, true, 16> : ccd_warp_kernel<T, true, false, 16>;
+    else kern = contig ? ccd_warp_kernel<T, false, true, 16> : ccd_warp_kernel<T, false, false, 16>;
+  } else {
+    if (per) kern = contig ? ccd_warp_kernel<T, true, true, 32> : ccd_warp_kernel<T, true, false, 32>;
+    else kern = contig ? ccd_warp_kernel<T, false, true, 32> : ccd_warp_kernel<T, false, false, 32>;
+  }
   TPF_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem));
-  kern<<<s.grid, s.TL * p->P, s.smem, stream>>>(a);
+  kern<<<s.grid, warp ? 32 * s.TL : s.TL * p->P, s.smem, stream>>>(a);
   TPF_CUDA_TRY(cudaGetLastError());
   return TPF_OK;
 }
@@ -781,7 +1208,9 @@ int tpf_ccd_plan_create(tpf_ccd_plan** out, int64_t n_pts, double h, int bc, int
   p->bc = bc;
   p->dtype = dtype;
   p->n_rows = (bc == TPF_BC_WALL) ? (int)(n_pts - 2) : (int)(n_pts - 1);
-  p->C = std::max(16, (p->n_rows + 31) / 32);   // P = ceil(n_rows / C) <= 32 lines of chunks
+  // chunk length = rows per lane of the warp-per-line kernel (8, 16, 32); longer
+  // lines use the shared-memory chunk kernel with C = ceil(n_rows / 32)
+  p->C = p->n_rows <= 256 ? 8 : (p->n_rows <= 512 ? 16 : (p->n_rows <= 1024 ? 32 : (p->n_rows + 31) / 32));
   std::vector<double> tab;
   int st = build_tables(p, tab);
   if (st != TPF_OK) { delete p; return st; }
