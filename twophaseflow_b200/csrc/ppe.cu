@@ -48,6 +48,33 @@ __device__ __forceinline__ void coords3(const Grid3& g, int idx, int& i0, int& i
   i2 = r - i1 * g.n2;
 }
 
+// Block-contiguous node ownership for the persistent kernels: block b owns
+// [b*chunk, (b+1)*chunk), thread t visits start+t, start+t+blockDim, ...; the
+// (i0, i1, i2) coordinates advance incrementally (no division per node).
+struct NodeIter {
+  int idx, end, i0, i1, i2, d0, d1, d2;
+  __device__ __forceinline__ NodeIter(const Grid3& g) {
+    const int chunk = (g.ndof + gridDim.x - 1) / gridDim.x;
+    const int start = blockIdx.x * chunk;
+    end = min(start + chunk, g.ndof);
+    idx = start + threadIdx.x;
+    coords3(g, idx, i0, i1, i2);
+    const int step = blockDim.x;
+    d2 = step % g.n2;
+    d1 = (step / g.n2) % g.n1;
+    d0 = step / g.st0;
+  }
+  __device__ __forceinline__ bool ok() const { return idx < end; }
+  __device__ __forceinline__ void next(const Grid3& g) {
+    idx += blockDim.x;
+    i2 += d2;
+    if (i2 >= g.n2) { i2 -= g.n2; ++i1; }
+    i1 += d1;
+    if (i1 >= g.n1) { i1 -= g.n1; ++i0; }
+    i0 += d0;
+  }
+};
+
 struct Geo {
   const double* dv[3];     // node control-volume widths
   const double* dface[3];  // face widths
@@ -59,14 +86,19 @@ template <typename T, typename PF>
 __device__ __forceinline__ void s_row(const Grid3& g, int idx, int i0, int i1, int i2,
                                       const T* __restrict__ s0, const T* __restrict__ s1,
                                       const T* __restrict__ s2, PF pv, T& diag, T& off) {
-  T d = T(0), acc = T(0);
-  if (i0 > 0) { T s = s0[idx - g.st0]; d += s; acc += s * pv(idx - g.st0); }
-  if (i0 < g.N0) { T s = s0[idx]; d += s; acc += s * pv(idx + g.st0); }
-  if (i1 > 0) { T s = s1[idx - g.n2]; d += s; acc += s * pv(idx - g.n2); }
-  if (i1 < g.N1) { T s = s1[idx]; d += s; acc += s * pv(idx + g.n2); }
+  // branch-free: clamp the neighbour indices, load unconditionally, mask the
+  // couplings of faces that do not exist (upper faces already store 0)
+  const int m0 = (i0 > 0) ? idx - g.st0 : idx, p0 = (i0 < g.N0) ? idx + g.st0 : idx;
+  const int m1 = (i1 > 0) ? idx - g.n2 : idx, p1 = (i1 < g.N1) ? idx + g.n2 : idx;
+  const T sm0 = (i0 > 0) ? s0[m0] : T(0), sp0 = s0[idx];
+  const T sm1 = (i1 > 0) ? s1[m1] : T(0), sp1 = s1[idx];
+  T d = (sm0 + sp0) + (sm1 + sp1);
+  T acc = sm0 * pv(m0) + sp0 * pv(p0) + sm1 * pv(m1) + sp1 * pv(p1);
   if (g.N2 > 0) {
-    if (i2 > 0) { T s = s2[idx - 1]; d += s; acc += s * pv(idx - 1); }
-    if (i2 < g.N2) { T s = s2[idx]; d += s; acc += s * pv(idx + 1); }
+    const int m2 = (i2 > 0) ? idx - 1 : idx, p2 = (i2 < g.N2) ? idx + 1 : idx;
+    const T sm2 = (i2 > 0) ? s2[m2] : T(0), sp2 = s2[idx];
+    d += sm2 + sp2;
+    acc += sm2 * pv(m2) + sp2 * pv(p2);
   }
   diag = d;
   off = acc;
@@ -306,10 +338,12 @@ __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
   return v;
 }
 
-// Grid-wide sum of NV doubles through a bounded barrier on a monotonic counter.
+// Grid-wide sum of NV doubles through a bounded barrier on a monotonic
+// arrival counter (release add / acquire poll by one thread per block); the
+// partials are summed in block order by every block (identical totals).
 struct GridSum {
-  double* part;
-  unsigned int* count;
+  double* part;            // [2 slots][8][nblocks]
+  unsigned int* count;     // monotonic arrival counter, zeroed before the launch
   int* err;
   unsigned int nb;
   unsigned int epoch;
@@ -330,7 +364,6 @@ struct GridSum {
         if (++spins > kSpinLimit * 8) { atomicExch(err, 1); ok = 0; break; }
         if ((spins & 1023) == 0 && *(volatile int*)err) { ok = 0; break; }
       }
-      __threadfence();
       s_ok = ok;
     }
     __syncthreads();
@@ -356,11 +389,6 @@ struct GridSum {
     ++epoch;
     return ok;
   }
-
-  __device__ __forceinline__ bool sync(double* scratch) {
-    double d[1] = {0.0};
-    return sum<1>(d, scratch);
-  }
 };
 
 // r = b - S x for own nodes (x FP64, pin column zero / pin row identity)
@@ -368,17 +396,15 @@ template <typename T>
 __device__ __forceinline__ void residual_pass(const Grid3& g, const double* s0, const double* s1,
                                               const double* s2, const double* b, const double* x, T* r,
                                               bool x_nonzero, double& bb, double& rr) {
-  const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int G = gridDim.x * blockDim.x;
-  for (int idx = gtid; idx < g.ndof; idx += G) {
+  for (NodeIter it(g); it.ok(); it.next(g)) {
+    const int idx = it.idx;
     double bi = b[idx];
     double ri = bi;
     if (x_nonzero) {
       double sx;
       if (idx == g.pin) sx = x[idx];
       else {
-        int i0, i1, i2;
-        coords3(g, idx, i0, i1, i2);
+        const int i0 = it.i0, i1 = it.i1, i2 = it.i2;
         double d, off;
         s_row<double>(g, idx, i0, i1, i2, s0, s1, s2, [&](int j) { return (j == g.pin) ? 0.0 : x[j]; }, d, off);
         sx = d * x[idx] - off;
@@ -396,12 +422,10 @@ __device__ __forceinline__ void residual_pass(const Grid3& g, const double* s0, 
 // red = {(r,u), (w,u), (u,s), (p,w), (p,s), (r,r)}.  init: p = s = 0.
 template <typename T>
 __device__ __forceinline__ void w_pass(const Grid3& g, const Cg1Vecs<T>& v, int cur, bool init, double (&red)[6]) {
-  const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int G = gridDim.x * blockDim.x;
-  const T* r = v.r[cur];
-  for (int idx = gtid; idx < g.ndof; idx += G) {
-    int i0, i1, i2;
-    coords3(g, idx, i0, i1, i2);
+  const T* __restrict__ r = v.r[cur];
+  for (NodeIter it(g); it.ok(); it.next(g)) {
+    const int idx = it.idx;
+    const int i0 = it.i0, i1 = it.i1, i2 = it.i2;
     const T ri = r[idx];
     const T ui = v.dinv[idx] * ri;
     T wi;
@@ -446,7 +470,7 @@ __global__ void __launch_bounds__(kThreads, 1) cg1_kernel(Cg1Args a) {
   if (!gs.sum<2>(red0, scratch)) return;
   const double bb = red0[0];
   if (bb == 0.0) {
-    for (int idx = gtid; idx < g.ndof; idx += G) a.x[idx] = 0.0;
+    for (NodeIter it(g); it.ok(); it.next(g)) a.x[it.idx] = 0.0;
     if (gtid == 0) { a.st->iters = 0; a.st->applies = 0; a.st->rr = 0.0; a.st->bb = 0.0; a.st->converged = 1; }
     return;
   }
@@ -491,37 +515,44 @@ __global__ void __launch_bounds__(kThreads, 1) cg1_kernel(Cg1Args a) {
     const double alpha_d = gamma / denom;
     const T b_t = (T)beta, alpha = (T)alpha_d;
     const int nxt = cur ^ 1;
-    const T* rc = v.r[cur];
-    const T* wc = v.w[cur];
-    const T* sc = v.s[cur];
+    const T* __restrict__ rc = v.r[cur];
+    const T* __restrict__ wc = v.w[cur];
+    const T* __restrict__ sc = v.s[cur];
+    const T* __restrict__ dinv = v.dinv;
+    T* __restrict__ pv = v.p;
+    double* __restrict__ xv = a.x;
+    T* __restrict__ rn_out = v.r[nxt];
+    T* __restrict__ sn_out = v.s[nxt];
+    T* __restrict__ wn_out = v.w[nxt];
 #pragma unroll
     for (int k = 0; k < 6; ++k) red[k] = 0.0;
-    for (int idx = gtid; idx < g.ndof; idx += G) {
-      int i0, i1, i2;
-      coords3(g, idx, i0, i1, i2);
+#pragma unroll 2
+    for (NodeIter it(g); it.ok(); it.next(g)) {
+      const int idx = it.idx;
+      const int i0 = it.i0, i1 = it.i1, i2 = it.i2;
       const T ri = rc[idx];
-      const T ui = v.dinv[idx] * ri;
+      const T ui = dinv[idx] * ri;
       const T si = wc[idx] + b_t * sc[idx];
-      const T pi = ui + b_t * v.p[idx];
-      v.p[idx] = pi;
-      a.x[idx] += alpha_d * (double)pi;
+      const T pi = ui + b_t * pv[idx];
+      pv[idx] = pi;
+      xv[idx] += alpha_d * (double)pi;
       const T rn = ri - alpha * si;
-      const T un = v.dinv[idx] * rn;
+      const T un = dinv[idx] * rn;
       T wn;
       if (idx == g.pin) {
         wn = un;
       } else {
         auto unb = [&](int j) -> T {
           if (j == g.pin) return T(0);
-          return v.dinv[j] * (rc[j] - alpha * (wc[j] + b_t * sc[j]));
+          return dinv[j] * (rc[j] - alpha * (wc[j] + b_t * sc[j]));
         };
         T d, off;
         s_row<T>(g, idx, i0, i1, i2, v.s0, v.s1, v.s2, unb, d, off);
         wn = d * un - off;
       }
-      v.r[nxt][idx] = rn;
-      v.s[nxt][idx] = si;
-      v.w[nxt][idx] = wn;
+      rn_out[idx] = rn;
+      sn_out[idx] = si;
+      wn_out[idx] = wn;
       red[0] += (double)rn * (double)un;
       red[1] += (double)wn * (double)un;
       red[2] += (double)un * (double)si;
