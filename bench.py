@@ -181,32 +181,12 @@ def time_ppe_e2e(precision, rho_h, rhs_h, steps, warmup):
     return e0.elapsed_time(e1) / steps, wall, p
 
 
-def time_ccd(N, bc, axis, steps, flush, dtype=None):
-    import torch
-    from twophaseflow_b200 import CCDSolver, UniformGrid
-    from twophaseflow_b200.workloads import fourier_field
-    dtype = dtype or torch.float64
-    f = torch.from_numpy(fourier_field(N, seed=0)).to("cuda").to(dtype)
-    ccd = CCDSolver(UniformGrid(N), None, bc_type=bc, dtype=dtype)
-    d1 = torch.empty_like(f)
-    d2 = torch.empty_like(f)
-    for _ in range(3):
-        ccd.differentiate(f, axis)
-    torch.cuda.synchronize()
-    ts = []
-    for _ in range(steps):
-        flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        ccd.differentiate(f, axis)
-        e1.record()
-        torch.cuda.synchronize()
-        ts.append(e0.elapsed_time(e1))
-    ms = float(np.median(ts))
-    nbytes = f.numel() * f.element_size() * 3
-    return {"N": list(N), "bc": bc, "axis": axis, "dtype": str(dtype).replace("torch.", ""),
-            "ms": round(ms, 4), "GBps": round(nbytes / (ms * 1e-3) / 1e9, 1)}
+def time_ccd(N, bc, axis, dtype="f64", reps=10):
+    """CCD line-kernel device time per call: `reps` calls captured in one CUDA
+    graph and replayed (inputs 136 MB / 8 MB; a 3-D field exceeds L2)."""
+    from twophaseflow_b200.kernel_cases import ccd_case
+    r = ccd_case(tuple(N), axis, bc, dtype, reps)
+    return {"N": list(N), "bc": bc, "axis": axis, "dtype": dtype, "us": r["us_per_call"], "GBps": r["GBps"]}
 
 
 def cpu_baseline_sample(rho, rhs, iters_full, max_iters=300):
@@ -287,40 +267,48 @@ def main(argv=None):
     rho_d = torch.from_numpy(rho).to(dev)
     rhs_d = torch.from_numpy(rhs).to(dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > L2 (126 MB)
+    # per solve: prepare (face couplings + ndim Thomas factorizations), rhs
+    # weighting, the persistent CG kernel and the pin/copy-out = 5 launches
 
-    # plain FP64 PCG (the comparator) and the B200 method
-    _barrier(ws)
-    s64, p64, t64 = time_ppe("fp64", rho_d, rhs_d, max(2, args.steps // 2), 1, flush)
-    it64 = s64.last_diagnostics["ppe_low_order_cg_iterations"]
+    # plain FP64 PCG (the timed headline method) and the mixed-precision variant
     _barrier(ws)
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
-        smx, pmx, tmx = time_ppe("mixed", rho_d, rhs_d, args.steps, args.warmup, flush)
+        s64, p64, t64 = time_ppe("fp64", rho_d, rhs_d, args.steps, args.warmup, flush)
         torch.cuda.synchronize()
+    _barrier(ws)
+    it64 = s64.last_diagnostics["ppe_low_order_cg_iterations"]
+    smx, pmx, tmx = time_ppe("mixed", rho_d, rhs_d, max(2, args.steps // 2), 1, flush)
     _barrier(ws)
     dmx = smx.last_diagnostics
     ms_mx = _max_over_ranks(float(np.mean(tmx)), ws)
     ms_64 = _max_over_ranks(float(np.mean(t64)), ws)
     err = float(torch.max(torch.abs(pmx - p64)).item() / torch.max(torch.abs(p64)).item())
+    best = "fp64" if ms_64 <= ms_mx else "mixed"
+    ms_best = min(ms_64, ms_mx)
 
-    # e2e through the public API with host buffers
-    e2e_ms, e2e_wall, _ = time_ppe_e2e("mixed", rho, rhs, max(2, args.steps // 2), 1)
+    # e2e through the public API with host buffers (same method as the headline)
+    e2e_ms, e2e_wall, _ = time_ppe_e2e(best, rho, rhs, max(2, args.steps // 2), 1)
     e2e_ms = _max_over_ranks(e2e_ms, ws)
 
-    # roofline of the dominant kernel (persistent PCG): algorithmic bytes per
-    # FP64 PCG iteration = 112 B/DOF; per FP32 inner iteration = 56 B/DOF
+    # roofline of the dominant kernel (persistent PCG, one launch per solve):
+    # algorithmic bytes per FP64 iteration = 112 B/DOF (survey's fused 3-kernel
+    # count); the 512^2 working set (~13 MB) is L2-resident, so this is a
+    # latency-bound kernel measured against the HBM copy peak
     ndof = (N_PPE[0] + 1) * (N_PPE[1] + 1)
     peak, peak_kind = _peaks()
     alg64 = it64 * 112 * ndof
     ach64 = alg64 / (np.mean(t64) * 1e-3) / 1e9
 
-    # CCD bandwidth (2-D 1024^2 and 3-D 256^3, FP64 and FP32)
+    # CCD line kernels (2-D 1024^2 and 3-D 256^3, FP64 and FP32), graph-timed
     ccd = []
     for N in ((1024, 1024), (256, 256, 256)):
         for axis in range(len(N)):
-            ccd.append(time_ccd(N, "wall", axis, 10, flush))
-        ccd.append(time_ccd(N, "periodic", 0, 10, flush))
-        ccd.append(time_ccd(N, "wall", len(N) - 1, 10, flush, dtype=torch.float32))
+            ccd.append(time_ccd(N, "wall", axis))
+        ccd.append(time_ccd(N, "periodic", 0))
+        ccd.append(time_ccd(N, "wall", len(N) - 1, dtype="f32"))
+    ccd3 = [c for c in ccd if len(c["N"]) == 3 and c["dtype"] == "f64"]
+    ccd_best = max(ccd3, key=lambda c: c["GBps"])
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -329,19 +317,20 @@ def main(argv=None):
     clocks = clk.summary()
     if rank == 0:
         line = {
-            "metric": METRIC, "value": round(ms_mx, 3), "unit": "ms", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(ms_mx, 3), "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 outer",
+            "metric": METRIC, "value": round(ms_best, 3), "unit": "ms", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_best, 3), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if best == "fp64" else "f32 inner / f64 outer",
             "data": "synthetic (seeded droplets, seeded velocity divergence)",
             "config": {"workload": "ppe_512x512_rho1000_12drops", "grid": list(N_PPE), "tol": TOL,
-                       "method": "mixed: FP32 Jacobi-PCG inner, FP64 iterative refinement",
+                       "method": ("FP64 Jacobi-PCG, persistent single-reduction kernel" if best == "fp64"
+                                  else "mixed: FP32 Jacobi-PCG with FP64 residual replacement"),
                        "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{ws}"},
             "plain_fp64_pcg": {"ms": round(ms_64, 3), "iterations": it64},
             "mixed": {"ms": round(ms_mx, 3), "inner_iterations": dmx["ppe_low_order_cg_iterations"],
-                      "refinements": dmx["ppe_low_order_cg_refinements"],
+                      "replacements": dmx["ppe_low_order_cg_refinements"],
                       "rel_residual": dmx["ppe_low_order_cg_relative_residual"],
                       "max_rel_diff_vs_fp64": err},
-            "speedup_vs_plain_fp64": round(ms_64 / ms_mx, 3),
+            "mixed_speedup_vs_plain_fp64": round(ms_64 / ms_mx, 3),
             "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": 2 * ndof * 8,
                     "d2h_bytes_per_step": ndof * 8, "wall_ms": round(e2e_wall, 3)},
             "roofline": {"kernel": "pcg64_kernel (plain FP64 PCG, persistent)", "bound": "hbm",
@@ -349,7 +338,11 @@ def main(argv=None):
                          "frac": round(ach64 / peak, 3), "traffic": None,
                          "note": "112 B/DOF/iteration algorithmic; the 512^2 working set (~13 MB) is L2-resident"},
             "ccd": ccd,
-            "gpu_launches": None,
+            "ccd_roofline": {"kernel": "ccd_warp_kernel (3-D 257^3 FP64)", "bound": "hbm",
+                             "achieved": ccd_best["GBps"], "peak": peak, "unit": "GB/s",
+                             "frac": round(ccd_best["GBps"] / peak, 3),
+                             "note": "24 B/point/axis call algorithmic; graph-replayed device time"},
+            "gpu_launches": 5 * args.steps,
             "clocks": clocks,
         }
         if cpu is not None:
