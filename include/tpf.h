@@ -186,6 +186,35 @@ int tpf_ppe_precondition(tpf_ppe* h, const double* r, double* z, void* stream);
 int tpf_ppe_solve(tpf_ppe* h, const double* rhs, const double* rho, double* p,
                   const double* p_init, void* stream, tpf_ppe_result* result);
 
+/* ---- allocation-free CG solve (no counterpart in the reference) ----------
+ *
+ * For callers that cannot allocate device memory while they run: a host whose
+ * caching allocator (PyTorch's, a memory pool) already holds the device
+ * memory, so a cudaMalloc inside a time step may fail or stall, or a solver
+ * loop whose memory budget is fixed at start-up.  Same solve as tpf_ppe_solve
+ * with method TPF_PPE_CG, precision TPF_PREC_F64 and precond TPF_PRECOND_JACOBI
+ * or TPF_PRECOND_NONE (identical iterates), but no handle: the workspace is a
+ * fixed file-scope device array of about 9.3 MB inside the library, and the
+ * call issues no cudaMalloc / cudaFree and calls no allocating library.
+ *
+ * Limits: at most TPF_PPE_STATIC_MAX_DOF nodes in total (e.g. 256 x 256 cells
+ * in 2-D, 40 x 40 x 40 in 3-D) and TPF_PPE_STATIC_MAX_AXIS nodes per axis;
+ * larger grids are rejected with TPF_EINVAL (use tpf_ppe_create /
+ * tpf_ppe_solve).  coords[a] are HOST arrays of N[a]+1 node coordinates (as
+ * for tpf_ppe_create); rhs, rho, p, p_init are device arrays of the grid's
+ * nodes.  The first call on a device looks up the workspace address for that
+ * device; a caller that will capture work into a stream should make one call
+ * on each device beforehand.  All calls on one device share the workspace:
+ * calls that overlap in time on the same device (two host threads, or two
+ * streams without ordering between them) race and must be serialised by the
+ * caller.  Synchronizes `stream`; returns TPF_ENOCONV like tpf_ppe_solve. */
+#define TPF_PPE_STATIC_MAX_DOF 66049
+#define TPF_PPE_STATIC_MAX_AXIS 4097
+int tpf_ppe_solve_cg_static(int ndim, const int64_t* N, const double* const* coords,
+                            int64_t pin, const double* rhs, const double* rho, double* p,
+                            const double* p_init, int precond, double tol,
+                            int64_t maxiter, void* stream, tpf_ppe_result* result);
+
 #ifdef __cplusplus
 }
 #endif

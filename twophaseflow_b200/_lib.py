@@ -22,6 +22,7 @@ TPF_CCD_APPLY_METRIC = 1
 TPF_PPE_CG, TPF_PPE_GMRES = 0, 1
 TPF_PRECOND_NONE, TPF_PRECOND_JACOBI, TPF_PRECOND_LINE, TPF_PRECOND_LINE_PCR = range(4)
 TPF_PREC_F64, TPF_PREC_MIXED = 0, 1
+TPF_PPE_STATIC_MAX_DOF, TPF_PPE_STATIC_MAX_AXIS = 66049, 4097
 
 
 class tpf_ppe_options(C.Structure):
@@ -71,6 +72,9 @@ SIGNATURES = {
     "tpf_ppe_precondition": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tpf_ppe_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                 C.POINTER(tpf_ppe_result)]),
+    "tpf_ppe_solve_cg_static": (C.c_int, [C.c_int, C.POINTER(C.c_int64), C.POINTER(C.POINTER(C.c_double)),
+                                          C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                          C.c_double, C.c_int64, C.c_void_p, C.POINTER(tpf_ppe_result)]),
 }
 
 _lib = None

@@ -26,6 +26,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 namespace {
@@ -1316,3 +1317,217 @@ int tpf_ppe_solve(tpf_ppe* h, const double* rhs, const double* rho, double* p, c
 }
 
 }  // extern "C"
+
+// ---- allocation-free CG solve ----------------------------------------------------
+//
+// For callers that must not allocate device memory while they run: a host
+// whose caching allocator (PyTorch's, or a memory pool) already holds the
+// device memory, so that a cudaMalloc inside a time step can fail or stall;
+// solver loops with a fixed memory budget checked at start-up.  The whole
+// workspace lives in one file-scope device array of fixed size; the entry
+// point issues no cudaMalloc / cudaFree and calls no allocating library.
+// Every call on a device uses the same array: calls that overlap in time on
+// one device (two host threads, or two streams without ordering) race on it.
+
+namespace {
+
+constexpr int kStaticMaxDof = TPF_PPE_STATIC_MAX_DOF;
+constexpr int kStaticMaxAxis = TPF_PPE_STATIC_MAX_AXIS;
+constexpr int kStaticMaxBlocks = 256;
+// layout in doubles: coords | dv | dface (3 x kStaticMaxAxis each), s0..s2,
+// dinvS, dinvL, b, x, ones, c64[7] (kStaticMaxDof each), s32[3] + dinvS32
+// (4 x kStaticMaxDof floats), partial sums, then 32 doubles for counter /
+// error flag / status
+constexpr size_t kStaticAxisDoubles = (size_t)9 * kStaticMaxAxis;
+constexpr size_t kStaticVecDoubles = (size_t)15 * kStaticMaxDof;
+constexpr size_t kStaticF32Doubles = (size_t)2 * kStaticMaxDof;
+constexpr size_t kStaticPartDoubles = (size_t)16 * kStaticMaxBlocks;
+constexpr size_t kStaticDoubles = kStaticAxisDoubles + kStaticVecDoubles + kStaticF32Doubles + kStaticPartDoubles + 32;
+static_assert(sizeof(SolveStatus) <= 16 * sizeof(double), "status slot too small");
+
+static __device__ __align__(256) double g_static_ws[kStaticDoubles];
+
+constexpr int kStaticMaxDevices = 64;
+std::mutex g_static_mu;
+double* g_static_ptr[kStaticMaxDevices] = {};
+
+// Device address of g_static_ws for the current device, looked up once per
+// device (the first call on a device does the lookup; later calls reuse it).
+int static_workspace(double** out) {
+  int dev = -1;
+  TPF_CUDA_TRY(cudaGetDevice(&dev));
+  TPF_CHECK_ARG(dev >= 0 && dev < kStaticMaxDevices, "device ordinal out of range for the static workspace");
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (!g_static_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_static_ws);
+    if (e != cudaSuccess || p == nullptr) {
+      tpf::set_error("cudaGetSymbolAddress of the static PPE workspace failed: %s", cudaGetErrorString(e));
+      return TPF_ECUDA;
+    }
+    g_static_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_static_ptr[dev];
+  return TPF_OK;
+}
+
+// node control-volume widths and face widths from node coordinates
+// (fvm_matrixfree_helpers.py:23-43), same arithmetic as tpf_ppe_create
+__global__ void static_metrics_kernel(const double* c, double* dv, double* dface, int nn) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
+    if (i + 1 < nn) dface[i] = c[i + 1] - c[i];
+    double v;
+    if (i == 0) v = (c[1] - c[0]) / 2.0;
+    else if (i == nn - 1) v = (c[nn - 1] - c[nn - 2]) / 2.0;
+    else v = (c[i + 1] - c[i - 1]) / 2.0;
+    dv[i] = v;
+  }
+}
+
+__global__ void static_fill_kernel(double* x, int n, double v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = v;
+}
+
+}  // namespace
+
+extern "C" int tpf_ppe_solve_cg_static(int ndim, const int64_t* N, const double* const* coords, int64_t pin,
+                                       const double* rhs, const double* rho, double* p, const double* p_init,
+                                       int precond, double tol, int64_t maxiter, void* stream,
+                                       tpf_ppe_result* result) {
+  TPF_CHECK_ARG(N && coords && rhs && rho && p, "NULL argument");
+  TPF_CHECK_ARG(ndim == 2 || ndim == 3, "ndim must be 2 or 3");
+  TPF_CHECK_ARG(precond == TPF_PRECOND_JACOBI || precond == TPF_PRECOND_NONE,
+                "the static-workspace CG solve supports preconditioner 'jacobi' or 'none'");
+  TPF_CHECK_ARG(tol > 0.0 && std::isfinite(tol), "tolerance must be > 0");
+  TPF_CHECK_ARG(maxiter >= 0, "maxiter must be >= 0");
+  int64_t nn[3] = {1, 1, 1}, ndof = 1;
+  for (int a = 0; a < ndim; ++a) {
+    TPF_CHECK_ARG(N[a] >= 1, "N must be >= 1");
+    TPF_CHECK_ARG(coords[a] != nullptr, "NULL coordinate array");
+    nn[a] = N[a] + 1;
+    if (nn[a] > kStaticMaxAxis) {
+      tpf::set_error("static-workspace CG solve: %lld nodes on axis %d exceeds the maximum of %d",
+                     (long long)nn[a], a, kStaticMaxAxis);
+      return TPF_EINVAL;
+    }
+    ndof *= nn[a];
+  }
+  if (ndof > kStaticMaxDof) {
+    tpf::set_error("static-workspace CG solve: %lld nodes exceed the maximum of %d (use tpf_ppe_create/tpf_ppe_solve)",
+                   (long long)ndof, kStaticMaxDof);
+    return TPF_EINVAL;
+  }
+  TPF_CHECK_ARG(pin >= 0 && pin < ndof, "pin DOF out of range");
+  double* ws = nullptr;
+  int st = static_workspace(&ws);
+  if (st) return st;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int n = (int)ndof;
+  Grid3 g{};
+  g.n0 = (int)nn[0]; g.n1 = (int)nn[1]; g.n2 = (int)nn[2];
+  g.N0 = (int)N[0]; g.N1 = (int)N[1]; g.N2 = ndim == 3 ? (int)N[2] : 0;
+  g.st0 = g.n1 * g.n2;
+  g.ndof = n;
+  g.pin = (int)pin;
+  // carve the workspace
+  double* cur = ws;
+  double *cst[3], *dv[3], *dface[3];
+  for (int a = 0; a < 3; ++a) { cst[a] = cur; cur += kStaticMaxAxis; }
+  for (int a = 0; a < 3; ++a) { dv[a] = cur; cur += kStaticMaxAxis; }
+  for (int a = 0; a < 3; ++a) { dface[a] = cur; cur += kStaticMaxAxis; }
+  double* sv[3];
+  for (int a = 0; a < 3; ++a) { sv[a] = cur; cur += kStaticMaxDof; }
+  double* dinvS = cur; cur += kStaticMaxDof;
+  double* dinvL = cur; cur += kStaticMaxDof;
+  double* b = cur; cur += kStaticMaxDof;
+  double* x = cur; cur += kStaticMaxDof;
+  double* ones = cur; cur += kStaticMaxDof;
+  double* c64[7];
+  for (int k = 0; k < 7; ++k) { c64[k] = cur; cur += kStaticMaxDof; }
+  float* f32 = reinterpret_cast<float*>(cur);
+  float* s32[3] = {f32, f32 + kStaticMaxDof, f32 + 2 * (size_t)kStaticMaxDof};
+  float* dinvS32 = f32 + 3 * (size_t)kStaticMaxDof;
+  cur += kStaticF32Doubles;
+  double* part = cur; cur += kStaticPartDoubles;
+  unsigned int* bar = reinterpret_cast<unsigned int*>(cur);        // 4 counters (2 doubles)
+  int* err = reinterpret_cast<int*>(cur + 2);                       // 1 flag (1 double)
+  SolveStatus* stp = reinterpret_cast<SolveStatus*>(cur + 4);       // 16 doubles
+  const int nsm = tpf::sm_count();
+  const int ew_blocks = std::max(1, std::min(nsm * 8, (n + 255) / 256));
+  const int coop_blocks = std::max(1, std::min(nsm, (n + kThreads - 1) / kThreads));
+  TPF_CHECK_ARG(coop_blocks <= kStaticMaxBlocks, "cooperative grid larger than the static partial-sum area");
+  // grid metrics from the host coordinates
+  for (int a = 0; a < ndim; ++a) {
+    TPF_CUDA_TRY(cudaMemcpyAsync(cst[a], coords[a], nn[a] * sizeof(double), cudaMemcpyHostToDevice, s));
+    static_metrics_kernel<<<(int)((nn[a] + 255) / 256), 256, 0, s>>>(cst[a], dv[a], dface[a], (int)nn[a]);
+  }
+  const Geo geo{{dv[0], dv[1], dv[2]}, {dface[0], dface[1], dface[2]}};
+  // face couplings and Jacobi diagonal (the FP32 copies are written too; unused here)
+  PrepArgs pa{};
+  pa.g = g;
+  pa.geo = geo;
+  pa.rho = rho;
+  for (int a = 0; a < 3; ++a) {
+    pa.s[a] = (a < ndim) ? sv[a] : nullptr;
+    pa.s32[a] = (a < ndim) ? s32[a] : nullptr;
+  }
+  pa.dinvS = dinvS;
+  pa.dinvS32 = dinvS32;
+  pa.dinvL = dinvL;
+  pa.shift_scale = 0.0;
+  pa.ndim = ndim;
+  pa.want_line = 0;
+  prep_faces_kernel<<<ew_blocks, 256, 0, s>>>(pa);
+  if (precond == TPF_PRECOND_NONE) static_fill_kernel<<<ew_blocks, 256, 0, s>>>(ones, n, 1.0);
+  cg_rhs_kernel<<<ew_blocks, 256, 0, s>>>(g, geo, rhs, b, p_init, x);
+  TPF_CUDA_TRY(cudaGetLastError());
+  // the grid-barrier counter, the error flag and the status start at zero
+  TPF_CUDA_TRY(cudaMemsetAsync(bar, 0, 4 * sizeof(unsigned int), s));
+  TPF_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), s));
+  TPF_CUDA_TRY(cudaMemsetAsync(stp, 0, sizeof(SolveStatus), s));
+  Cg1Args a{};
+  a.g = g;
+  a.v64.s0 = sv[0]; a.v64.s1 = sv[1]; a.v64.s2 = (ndim == 3) ? sv[2] : sv[1];
+  a.v64.dinv = (precond == TPF_PRECOND_NONE) ? ones : dinvS;
+  for (int k = 0; k < 2; ++k) { a.v64.r[k] = c64[k]; a.v64.w[k] = c64[2 + k]; a.v64.s[k] = c64[4 + k]; }
+  a.v64.p = c64[6];
+  a.s64[0] = sv[0]; a.s64[1] = sv[1]; a.s64[2] = (ndim == 3) ? sv[2] : sv[1];
+  a.b = b;
+  a.x = x;
+  a.tol = tol;
+  a.maxiter = maxiter;
+  a.replace_drop = 1e-3;
+  a.x_nonzero = p_init ? 1 : 0;
+  a.part = part;
+  a.count = bar;
+  a.err = err;
+  a.st = stp;
+  void* args[] = {&a};
+  TPF_CUDA_TRY(cudaLaunchCooperativeKernel((void*)cg1_kernel<double, false>, dim3(coop_blocks), dim3(kThreads), args,
+                                           0, s));
+  copy_pin0_kernel<<<ew_blocks, 256, 0, s>>>(n, g.pin, x, p);
+  TPF_CUDA_TRY(cudaGetLastError());
+  SolveStatus hs{};
+  int herr = 0;
+  TPF_CUDA_TRY(cudaMemcpyAsync(&hs, stp, sizeof(SolveStatus), cudaMemcpyDeviceToHost, s));
+  TPF_CUDA_TRY(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  TPF_CUDA_TRY(cudaStreamSynchronize(s));
+  if (herr) {
+    tpf::set_error("PCG grid barrier timed out; the solve was aborted");
+    return TPF_EABORT;
+  }
+  tpf_ppe_result local{};
+  tpf_ppe_result* res = result ? result : &local;
+  *res = tpf_ppe_result{};
+  res->iterations = hs.iters;
+  res->applies = hs.applies;
+  res->refinements = 0;
+  res->rel_residual = hs.bb > 0.0 ? std::sqrt(hs.rr / hs.bb) : 0.0;
+  res->info = hs.converged ? 0 : (int)std::min<long long>(maxiter, 0x7fffffff);
+  if (!hs.converged) {
+    tpf::set_error("PPESolverFVMMatrixFree did not converge cleanly (info=%d); no alternate PPE solver was applied.",
+                   res->info);
+    return TPF_ENOCONV;
+  }
+  return TPF_OK;
+}
