@@ -215,6 +215,78 @@ int tpf_ppe_solve_cg_static(int ndim, const int64_t* N, const double* const* coo
                             const double* p_init, int precond, double tol,
                             int64_t maxiter, void* stream, tpf_ppe_result* result);
 
+/* ------------------------------------------------------------------------ */
+/* Learned PPE preconditioner (no counterpart in the reference, which has no  */
+/* learned component; its PPE Krylov loops are SciPy cg / gmres,              */
+/* src/twophase/ppe/gmres_helpers.py:16-80)                                   */
+/* ------------------------------------------------------------------------ */
+typedef struct tpf_unet tpf_unet;
+
+/* Number of FP32 parameters of the U-Net (4 levels, 3x3 convolutions,
+ * channels 16-32-64-128, 1x1 output).  Flat layout: for each of the 14
+ * convolutions W[cout][cin][3][3] then b[cout]; then w_out[16], b_out. */
+int64_t tpf_unet_num_params(void);
+
+/* Network workspace for images of H x W nodes (multiples of 8) and batches
+ * up to max_batch.  Parameters start at zero. */
+int tpf_unet_create(tpf_unet** net, int H, int W, int max_batch);
+int tpf_unet_destroy(tpf_unet* net);
+/* Copy the FP32 master parameters in / out (host or device pointer). */
+int tpf_unet_set_params(tpf_unet* net, const float* params, int on_device);
+int tpf_unet_get_params(tpf_unet* net, float* params, int on_device);
+
+/* y[B][H][W] = UNet(in2[B][H][W][2]) (device FP32; BF16 inside).  Synchronizes. */
+int tpf_unet_forward(tpf_unet* net, int B, const float* in2, float* y, void* stream);
+/* Parameter gradients (FP32, num_params, device) of sum(dy * y) for the
+ * activations of the last tpf_unet_forward with the same B.  Synchronizes. */
+int tpf_unet_backward(tpf_unet* net, int B, const float* dy, float* grads, void* stream);
+/* One Adam step on the mean over the batch of the relative squared error
+ * sum (y - target)^2 / sum target^2; *loss (may be NULL) is that mean before
+ * the step.  Synchronizes when loss != NULL. */
+int tpf_unet_train_step(tpf_unet* net, int B, const float* in2, const float* target, float lr,
+                        float weight_decay, double* loss, void* stream);
+
+typedef struct tpf_learned_options {
+  double tol;           /* relative residual tolerance of the weighted system   */
+  int64_t maxiter;      /* flexible-CG iterations before the fallback           */
+  int smooth;           /* damped-Jacobi sweeps after the network (0..8)         */
+  double omega;         /* their damping                                         */
+  int check_every;      /* iterations between host checks of the residual        */
+  int stall_checks;     /* fallback when the best ||r|| has not fallen by         */
+  double stall_factor;  /* stall_factor within stall_checks x check_every iters  */
+  int fallback;         /* 1: finish with plain Jacobi PCG after a stall          */
+  int use_graph;        /* 1: replay one iteration as a CUDA graph                */
+} tpf_learned_options;
+
+typedef struct tpf_lppe_result {
+  int64_t iterations;           /* flexible-CG iterations (network applications)  */
+  int64_t fallback_iterations;  /* plain PCG iterations after a stall             */
+  int64_t restarts;             /* restarts from the true residual                */
+  double rel_residual;          /* ||b - S p|| / ||b|| at exit                     */
+  int info;                     /* 0 converged                                     */
+  int fell_back;                /* 1 when the plain PCG fallback ran               */
+} tpf_lppe_result;
+
+typedef struct tpf_lppe tpf_lppe;
+
+void tpf_lppe_default_options(tpf_learned_options* opts);
+/* Learned solver on a 2-D PPE handle; the network image must be the node
+ * counts rounded up to multiples of 8. */
+int tpf_lppe_create(tpf_lppe** lp, tpf_ppe* ppe, tpf_unet* net);
+int tpf_lppe_destroy(tpf_lppe* lp);
+/* tpf_ppe_prepare plus the density feature of the network input. */
+int tpf_lppe_prepare(tpf_lppe* lp, const double* rho, void* stream);
+/* Same contract as tpf_ppe_solve (p[pin] = 0, TPF_ENOCONV when the budget
+ * ends), flexible CG preconditioned by the network. */
+int tpf_lppe_solve(tpf_lppe* lp, const double* rhs, const double* rho, double* p, const double* p_init,
+                   const tpf_learned_options* opts, void* stream, tpf_lppe_result* result);
+/* z = B(r), the preconditioner alone (r, z device vectors of the grid). */
+int tpf_lppe_precondition(tpf_lppe* lp, const double* r, double* z, int smooth, double omega, void* stream);
+/* Training pair from an error field e of the weighted system (pin 0):
+ * in2 = (D^-1/2 S e / s, density feature), target = D^1/2 e / s on the
+ * network image (s = rms of D^-1/2 S e); in2 and target are device FP32. */
+int tpf_lppe_pair(tpf_lppe* lp, const double* e, float* in2, float* target, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,169 @@
+"""GPU tests of the learned preconditioner: the tcgen05 U-Net forward/backward
+against the NumPy oracle, training, and the network-preconditioned flexible CG
+against the direct solution of the same PPE."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import ppe as oppe
+from oracle import unet as ou
+
+pytestmark = pytest.mark.gpu
+
+# BF16 activations are rounded at every layer; GPU (FP32 sums) and oracle
+# (float64 sums) round a few values to neighbouring BF16 numbers, so outputs
+# and gradients agree to about 1e-2 of their magnitude.
+FWD_TOL = 3e-2
+
+
+def _net(H, W, B, params):
+    from twophaseflow_b200.learned import UNet
+    return UNet(H, W, B, params=params)
+
+
+@pytest.mark.parametrize("H,W,B", [(16, 16, 2), (24, 40, 1)])
+def test_unet_forward_matches_oracle(cuda_device, H, W, B):
+    import torch
+    rng = np.random.default_rng(7)
+    p = ou.init_params(seed=2)
+    p[ou.param_layout()[0][3][1]:ou.param_layout()[0][3][1] + 32] = 0.05  # nonzero biases somewhere
+    x = rng.standard_normal((B, H, W, 2)).astype(np.float32)
+    net = _net(H, W, B, p)
+    y = net.forward(torch.from_numpy(x).to(cuda_device)).cpu().numpy()
+    yo, _ = ou.forward(p, x, precision="bf16")
+    scale = np.abs(yo).max()
+    assert scale > 0
+    err = np.abs(y - yo).max() / scale
+    assert err < FWD_TOL, err
+    assert np.abs(y - yo).mean() / np.abs(yo).mean() < 1e-2
+
+
+def _layer_rel(g, ref):
+    offs, wo, bo, _ = ou.param_layout()
+    segs = [(w, b + ou.LAYERS[l][1]) for l, (w, b) in enumerate(offs)] + [(wo, bo + 1)]
+    out = []
+    for a, b in segs:
+        nrm = np.linalg.norm(ref[a:b])
+        out.append(np.linalg.norm(g[a:b] - ref[a:b]) / nrm if nrm > 0 else np.linalg.norm(g[a:b]))
+    return np.array(out)
+
+
+def test_unet_backward_matches_oracle(cuda_device):
+    """GPU gradients vs the BF16 oracle, judged against the oracle's own
+    sensitivity: BF16 storage makes the gradients chaotic (a 1e-6 relative
+    change of the parameters already moves them by several percent), so the
+    bar per layer is a multiple of that measured sensitivity, plus a cosine
+    check that catches any systematic error."""
+    import torch
+    rng = np.random.default_rng(11)
+    H, W, B = 16, 24, 2
+    p = ou.init_params(seed=5)
+    x = rng.standard_normal((B, H, W, 2)).astype(np.float32)
+    dy = rng.standard_normal((B, H, W)).astype(np.float32)
+    net = _net(H, W, B, p)
+    net.forward(torch.from_numpy(x).to(cuda_device))
+    g = net.backward(torch.from_numpy(dy).to(cuda_device)).cpu().numpy().astype(np.float64)
+    _, A = ou.forward(p, x, precision="bf16")
+    go = ou.backward(p, A, dy, precision="bf16")
+    p2 = (p * (1.0 + 1e-6 * rng.standard_normal(p.shape))).astype(np.float32)
+    _, A2 = ou.forward(p2, x, precision="bf16")
+    sens = _layer_rel(ou.backward(p2, A2, dy, precision="bf16"), go)
+    rels = _layer_rel(g, go)
+    assert np.all(rels <= 3.0 * np.maximum(sens, 2e-2)), (rels, sens)
+    offs, wo, bo, _ = ou.param_layout()
+    cos = g @ go / (np.linalg.norm(g) * np.linalg.norm(go))
+    assert cos > 0.995, cos
+
+
+def test_train_step_reduces_loss(cuda_device):
+    import torch
+    from twophaseflow_b200.learned import UNet
+    rng = np.random.default_rng(0)
+    H = W = 32
+    B = 4
+    x = rng.standard_normal((B, H, W, 2)).astype(np.float32)
+    # target: a smooth function of the first input channel
+    t = np.cumsum(np.cumsum(x[..., 0], axis=1), axis=2) / 32.0
+    net = UNet(H, W, B, seed=3)
+    xt = torch.from_numpy(x).to(cuda_device)
+    tt = torch.from_numpy(t.astype(np.float32)).to(cuda_device)
+    losses = [net.train_step(xt, tt, 1e-3) for _ in range(60)]
+    assert np.isfinite(losses).all()
+    assert losses[-1] < 0.5 * losses[0], (losses[0], losses[-1])
+    # the loss matches the oracle's on the updated parameters
+    p = net.get_params()
+    y = net.forward(xt).cpu().numpy()
+    L_gpu, _ = ou.loss(y, t)
+    yo, _ = ou.forward(p, x, precision="bf16")
+    L_or, _ = ou.loss(yo, t)
+    assert abs(L_gpu - L_or) < 0.05 * L_or + 1e-3
+
+
+class _Cfg:
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+
+
+def _case(N, seed, ratio=1000.0):
+    from twophaseflow_b200.workloads import divergence_rhs, droplet_density
+    rho = droplet_density(N, n_drops=6, rho_l=1.0, rho_g=1.0 / ratio, seed=seed)
+    rhs = divergence_rhs(N, seed=seed + 1)
+    return rho, rhs
+
+
+@pytest.mark.parametrize("smooth", [1, 2])
+def test_flexible_cg_matches_direct_solution(cuda_device, smooth):
+    """With all-zero network parameters the preconditioner reduces to damped
+    Jacobi sweeps (a fixed SPD map), so the flexible CG must converge like
+    PCG: this checks the FCG recurrences, the pinning and the true-residual
+    exit independently of training."""
+    import torch
+    from twophaseflow_b200 import UniformGrid
+    from twophaseflow_b200.learned import PPESolverLearned, num_params
+    N = (64, 64)
+    rho, rhs = _case(N, seed=3)
+    cfg = _Cfg(pseudo_tol=1e-10, pseudo_maxiter=4000, ppe_learned_smooth=smooth, ppe_learned_fallback=False)
+    s = PPESolverLearned(None, cfg, UniformGrid(N), params=np.zeros(num_params(), np.float32))
+    p = s.solve(torch.from_numpy(rhs).to(cuda_device), torch.from_numpy(rho).to(cuda_device)).cpu().numpy()
+    d = s.last_diagnostics
+    assert d["ppe_learned_info"] == 0 and not d["ppe_learned_fell_back"]
+    assert d["ppe_learned_relative_residual"] <= 1e-10
+    pd = oppe.spsolve_fvm(rhs, rho, oppe.uniform_coords(N, (1.0, 1.0)))
+    assert np.abs(p - pd).max() <= 1e-7 * np.abs(pd).max()
+    pin = s._pin_dof
+    assert p.ravel()[pin] == 0.0
+
+
+def test_learned_solve_falls_back_to_pcg_on_stall(cuda_device):
+    import torch
+    from twophaseflow_b200 import UniformGrid
+    from twophaseflow_b200.learned import PPESolverLearned
+    N = (48, 48)
+    rho, rhs = _case(N, seed=5)
+    # an all-zero network without smoothing gives z = 0: no progress -> fallback
+    from twophaseflow_b200.learned import num_params
+    cfg = _Cfg(pseudo_tol=1e-9, pseudo_maxiter=400, ppe_learned_smooth=0, ppe_learned_maxiter=400)
+    s = PPESolverLearned(None, cfg, UniformGrid(N), params=np.zeros(num_params(), np.float32))
+    p = s.solve(torch.from_numpy(rhs).to(cuda_device), torch.from_numpy(rho).to(cuda_device)).cpu().numpy()
+    d = s.last_diagnostics
+    assert d["ppe_learned_fell_back"] and d["ppe_learned_info"] == 0
+    pd = oppe.spsolve_fvm(rhs, rho, oppe.uniform_coords(N, (1.0, 1.0)))
+    assert np.abs(p - pd).max() <= 1e-6 * np.abs(pd).max()
+
+
+def test_pairs_are_consistent(cuda_device):
+    """in2 channel 0 is D^-1/2 S e / s and target is D^1/2 e / s for the same s."""
+    import torch
+    from twophaseflow_b200.learned import generate_pairs
+    in2, tgt = generate_pairs(N=(32, 32), n_cases=2, snapshots=(0, 5), seed=1)
+    assert in2.shape == (4, 40, 40, 2) and tgt.shape == (4, 40, 40)
+    a = in2.cpu().numpy()
+    t = tgt.cpu().numpy()
+    assert np.isfinite(a).all() and np.isfinite(t).all()
+    # scaled residual has unit RMS over the grid nodes; padding is zero
+    rms = np.sqrt((a[:, :33, :33, 0] ** 2).mean(axis=(1, 2)))
+    assert np.allclose(rms, 1.0, rtol=1e-4)
+    assert np.all(a[:, 33:, :, :] == 0) and np.all(t[:, :, 33:] == 0)
+    assert np.all((a[..., 1] >= 0) & (a[..., 1] <= 1))

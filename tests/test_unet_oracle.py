@@ -1,0 +1,52 @@
+"""CPU checks of the U-Net oracle: its backward pass against finite differences
+(FP64 mode) and the BF16 rounding helper."""
+
+from __future__ import annotations
+
+import numpy as np
+
+from oracle import unet as ou
+
+
+def test_bf16_rounding_ties_to_even():
+    x = np.array([1.0, 1.0 + 2**-8, 1.0 + 3 * 2**-8, -2.5, 3.140625], np.float32)
+    r = ou.bf16(x)
+    assert r[0] == 1.0
+    assert r[1] == 1.0                  # tie -> even mantissa
+    assert r[2] == np.float32(1.0 + 4 * 2**-8)
+    assert r[3] == -2.5 and r[4] == np.float32(3.140625)
+
+
+def test_backward_matches_finite_differences():
+    rng = np.random.default_rng(3)
+    p = ou.init_params(seed=1)
+    B, H, W = 2, 16, 16
+    x = rng.standard_normal((B, H, W, 2))
+    dy = rng.standard_normal((B, H, W))
+    y, A = ou.forward(p, x, precision="fp64")
+    g = ou.backward(p, A, dy, precision="fp64")
+    offs, wo, bo, total = ou.param_layout()
+    picks = [wo + 3, bo]
+    for (w, b) in offs:
+        picks += [w + 5, w + 17, b]
+    h = 1e-6  # ReLU kinks make larger steps inexact
+    for i in picks:
+        pp, pm = p.astype(np.float64).copy(), p.astype(np.float64).copy()
+        pp[i] += h
+        pm[i] -= h
+        fp = float(np.sum(dy * ou.forward(pp, x, precision="fp64")[0]))
+        fm = float(np.sum(dy * ou.forward(pm, x, precision="fp64")[0]))
+        num = (fp - fm) / (2 * h)
+        assert abs(num - g[i]) <= 1e-5 * max(1.0, abs(num)), (i, num, g[i])
+
+
+def test_loss_gradient():
+    rng = np.random.default_rng(0)
+    y = rng.standard_normal((2, 4, 4))
+    t = rng.standard_normal((2, 4, 4))
+    L, dy = ou.loss(y, t)
+    h = 1e-6
+    y2 = y.copy()
+    y2[1, 2, 3] += h
+    L2, _ = ou.loss(y2, t)
+    assert abs((L2 - L) / h - dy[1, 2, 3]) < 1e-4

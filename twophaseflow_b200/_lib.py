@@ -50,6 +50,31 @@ class tpf_ppe_result(C.Structure):
     ]
 
 
+class tpf_learned_options(C.Structure):
+    _fields_ = [
+        ("tol", C.c_double),
+        ("maxiter", C.c_int64),
+        ("smooth", C.c_int),
+        ("omega", C.c_double),
+        ("check_every", C.c_int),
+        ("stall_checks", C.c_int),
+        ("stall_factor", C.c_double),
+        ("fallback", C.c_int),
+        ("use_graph", C.c_int),
+    ]
+
+
+class tpf_lppe_result(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int64),
+        ("fallback_iterations", C.c_int64),
+        ("restarts", C.c_int64),
+        ("rel_residual", C.c_double),
+        ("info", C.c_int),
+        ("fell_back", C.c_int),
+    ]
+
+
 # name -> (restype, argtypes); every function declared in include/tpf.h
 SIGNATURES = {
     "tpf_version": (C.c_int, []),
@@ -75,6 +100,23 @@ SIGNATURES = {
     "tpf_ppe_solve_cg_static": (C.c_int, [C.c_int, C.POINTER(C.c_int64), C.POINTER(C.POINTER(C.c_double)),
                                           C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                           C.c_double, C.c_int64, C.c_void_p, C.POINTER(tpf_ppe_result)]),
+    "tpf_unet_num_params": (C.c_int64, []),
+    "tpf_unet_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int]),
+    "tpf_unet_destroy": (C.c_int, [C.c_void_p]),
+    "tpf_unet_set_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "tpf_unet_get_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "tpf_unet_forward": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tpf_unet_backward": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tpf_unet_train_step": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_float, C.c_float,
+                                      C.POINTER(C.c_double), C.c_void_p]),
+    "tpf_lppe_default_options": (None, [C.POINTER(tpf_learned_options)]),
+    "tpf_lppe_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_void_p, C.c_void_p]),
+    "tpf_lppe_destroy": (C.c_int, [C.c_void_p]),
+    "tpf_lppe_prepare": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tpf_lppe_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.POINTER(tpf_learned_options), C.c_void_p, C.POINTER(tpf_lppe_result)]),
+    "tpf_lppe_precondition": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_void_p]),
+    "tpf_lppe_pair": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 _lib = None

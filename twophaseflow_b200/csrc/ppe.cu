@@ -23,6 +23,7 @@
 //    Givens state on the device; classical Gram-Schmidt with
 //    re-orthogonalization replaces modified Gram-Schmidt.
 #include "tpf_common.cuh"
+#include "ppe_view.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -1238,7 +1239,8 @@ int tpf_ppe_set_options(tpf_ppe* h, const tpf_ppe_options* o) {
   TPF_CHECK_ARG(h && o, "NULL argument");
   int st = validate_options(o);
   if (st) return st;
-  bool line_changed = (o->precond != h->o.precond) || (o->c_tau != h->o.c_tau);
+  // prepare builds every preconditioner's state; only the line shift depends on an option
+  bool line_changed = (o->c_tau != h->o.c_tau);
   bool grow = o->restart > h->o.restart;
   h->o = *o;
   if (grow) {
@@ -1317,6 +1319,32 @@ int tpf_ppe_solve(tpf_ppe* h, const double* rhs, const double* rho, double* p, c
 }
 
 }  // extern "C"
+
+namespace tpf {
+
+int ppe_view(tpf_ppe* h, PpeView* v) {
+  TPF_CHECK_ARG(h && v, "NULL argument");
+  v->ndim = h->ndim;
+  v->n0 = h->g.n0; v->n1 = h->g.n1; v->n2 = h->g.n2;
+  v->N0 = h->g.N0; v->N1 = h->g.N1; v->N2 = h->g.N2;
+  v->ndof = h->g.ndof;
+  v->pin = h->g.pin;
+  for (int a = 0; a < 3; ++a) {
+    v->s[a] = h->s[a];
+    v->dv[a] = h->dv[a];
+  }
+  v->dinvS = h->dinvS;
+  v->prepared = h->prepared;
+  return TPF_OK;
+}
+
+int ppe_options(tpf_ppe* h, tpf_ppe_options* o) {
+  TPF_CHECK_ARG(h && o, "NULL argument");
+  *o = h->o;
+  return TPF_OK;
+}
+
+}  // namespace tpf
 
 // ---- allocation-free CG solve ----------------------------------------------------
 //
