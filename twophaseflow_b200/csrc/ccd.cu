@@ -78,6 +78,11 @@ struct tpf_ccd_plan {
   float* d_tabf = nullptr;   // float copy (interior factors for F32)
   double* d_J = nullptr;     // metric J, dJ (n_pts each)
   bool has_metric = false;
+  // lane-per-line kernel table (factors, ring closures, head rows)
+  double* d_ltab = nullptr;
+  float* d_ltabf = nullptr;
+  int ltab_total = 0;
+  std::vector<double> ltab_host;
 };
 
 namespace {
@@ -907,6 +912,324 @@ __global__ void wall_zero_kernel(T* g, int64_t outer, int64_t n, int64_t inner) 
 
 // ---- host: factor tables ---------------------------------------------------
 
+// ---- lane-per-line kernel ---------------------------------------------------------
+//
+// For many lines (3-D grids): lane l of a warp owns line 32g + l and runs the
+// block-Thomas recurrences serially along it, so no scan, shuffle or carry
+// fix-up is needed.  A line is cut into chunks of kLaneCR rows and visited
+// twice:
+//   pass 1: forward sweep y_r = b_r - Lf_r y_{r-1}; the carry at the end of
+//           every chunk is kept in shared memory;
+//   pass 2: chunks in reverse order: the forward sweep of the chunk is redone
+//           from the stored carry (y in registers), then back substitution
+//           x_r = P_r y_r - H_r x_{r+1} from the carry of the chunk after it.
+// Each chunk's nodes (plus one halo node either side) are staged through a
+// [rows][lanes] shared tile so global loads and stores are coalesced for the
+// strided axes (lanes = adjacent lines) and the contiguous axis (lanes = nodes
+// of one line).  Periodic axes close the forward recurrence exactly on the
+// ring (Gf = (I - (-Lf)^N)^-1) and the backward one with the carry
+// X = Gb x_0, where x_0 of the zero-carry sweep is the sum over the first
+// kLaneK rows of (-H)^k P y_k (the neglected tail is below 0.46^64 of x_0).
+constexpr int kLaneCR = 16;
+constexpr int kLaneK = 64;
+
+struct LaneTab {
+  static constexpr int Lf = 0, P = 4, H = 8, Plast = 12, Gf = 16, Gb = 20, PhiC = 24, Q = 28, M = 32;
+  static constexpr int head = M + 4 * kLaneK;   // per head row: Lf, P, H (12)
+};
+
+template <typename T>
+__device__ __forceinline__ V2<T> mvs(const T* m, T a0, T a1) {
+  return {m[0] * a0 + m[1] * a1, m[2] * a0 + m[3] * a1};
+}
+
+// The lane table holds the factors in a scaled form: with D = diag(a1/h, a2/h^2)
+// the forward recurrence runs on y~ = D^-1 y, whose right-hand side is the
+// plain differences (f+ - f-, f- - 2 f0 + f+); every factor that touches y is
+// rescaled on the host (Lf~ = D^-1 Lf D, P~ = P D, ...), so no row pays for
+// the RHS constants.
+template <int N>
+__device__ __forceinline__ void cp_async_wait_dyn(int pending) {
+  // cp.async.wait_group takes an immediate: dispatch on the (small) count
+  if (pending <= 0) cp_async_wait<0>();
+  else if (pending == 1 || N <= 2) cp_async_wait<1>();
+  else cp_async_wait<2>();
+}
+
+template <typename T, bool PERIODIC, bool PLAIN, int NBUF>
+__global__ void __launch_bounds__(128) ccd_lane_kernel(CcdArgs a, const T* __restrict__ ltab_g, int ltab_total) {
+  constexpr int CR = kLaneCR, TR = CR + 2;
+  static_assert(NBUF == 2 || NBUF == 3, "f tile ring of 2 or 3 buffers");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* lt = reinterpret_cast<T*>(smem_raw);
+  const int lt_pad = (ltab_total + 1) & ~1;
+  const int n = a.n, n_rows = a.n_rows, H0 = PERIODIC ? 0 : a.H0;
+  const int P = (n_rows + CR - 1) / CR;
+  const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  T* fb0 = lt + lt_pad + (size_t)wid * (NBUF * TR * 32 + 64 * P);   // ring of f tiles [TR][32]
+  T* cy = fb0 + NBUF * TR * 32;                                         // chunk-end carries [P][2][32]
+  for (int i = threadIdx.x; i < ltab_total; i += blockDim.x) lt[i] = ltab_g[i];
+  __syncthreads();
+
+  const T* __restrict__ f = static_cast<const T*>(a.f);
+  const TabLayout lay{a.C, a.H0};
+  const double* tb = a.tab + lay.bc();
+  const double c1d = tb[30], c2d = tb[31];
+  const T lf0 = lt[LaneTab::Lf], lf1 = lt[LaneTab::Lf + 1], lf2 = lt[LaneTab::Lf + 2], lf3 = lt[LaneTab::Lf + 3];
+  const T p0 = lt[LaneTab::P], p1 = lt[LaneTab::P + 1], p2 = lt[LaneTab::P + 2], p3 = lt[LaneTab::P + 3];
+  const T h0 = lt[LaneTab::H], h1 = lt[LaneTab::H + 1], h2 = lt[LaneTab::H + 2], h3 = lt[LaneTab::H + 3];
+  const int Nn = n - 1;   // periodic: unique nodes
+  const int64_t inner = a.inner;
+  const int64_t n_groups = (a.n_lines + 31) / 32;
+  const double* J = a.J;
+
+  for (int64_t g = blockIdx.x * (int64_t)warps + wid; g < n_groups; g += (int64_t)gridDim.x * warps) {
+    const int64_t L = g * 32 + lane;
+    const bool act = L < a.n_lines;
+    int64_t base = 0;
+    if (act) {
+      const int64_t o = L / inner, i = L - o * inner;
+      base = o * (int64_t)n * inner + i;
+    }
+    const T* __restrict__ fl = f + base;
+    // asynchronous copy of nodes k0 + t, t in [0, KN), into tile[t][lane]
+    auto stage = [&](T* tile, int k0, int KN) {
+      if (act) {
+        if (PERIODIC && (k0 < 0 || k0 + KN > Nn)) {
+          for (int t = 0; t < KN; ++t) {
+            int k = k0 + t;
+            k = (k < 0) ? k + Nn : (k >= Nn ? k - Nn : k);
+            cp_async<sizeof(T)>(tile + t * 32 + lane, fl + (int64_t)k * inner, true);
+          }
+        } else {
+          const T* src = fl + (int64_t)k0 * inner;
+          for (int t = 0; t < KN; ++t) {
+            cp_async<sizeof(T)>(tile + t * 32 + lane, src, true);
+            src += inner;
+          }
+        }
+      }
+      cp_async_commit();
+    };
+    auto put = [&](int k, double o1, double o2) {
+      if (!act) return;
+      if (J) {
+        const double Jk = J[k], dJk = J[n + k];
+        o2 = Jk * Jk * o2 + Jk * dJk * o1;
+        o1 = Jk * o1;
+      }
+      store_out<T>(a, base + (int64_t)k * inner, o1, o2);
+    };
+    auto k0_of = [&](int c) { return PERIODIC ? c * CR - 1 : c * CR; };
+    auto cnt_of = [&](int c) { return min(CR, n_rows - c * CR); };
+
+    // chunk loads in visiting order: 0 .. P-1 (pass 1), then P-2 .. 0 (pass 2;
+    // chunk P-1 is reused from pass 1); load l lives in ring buffer l % NBUF
+    const int n_loads = 2 * P - 1;
+    auto chunk_of_load = [&](int l) { return l < P ? l : 2 * P - 2 - l; };
+    int issued = 0;
+    // make load `need` resident, keeping up to NBUF - 1 loads ahead in flight
+    auto acquire = [&](int need) -> const T* {
+      const int want = min(n_loads, need + NBUF);
+      while (issued < want) {
+        const int c = chunk_of_load(issued);
+        stage(fb0 + (issued % NBUF) * TR * 32, k0_of(c), cnt_of(c) + 2);
+        ++issued;
+      }
+      cp_async_wait_dyn<NBUF>(issued - need - 1);
+      __syncwarp();
+      return fb0 + (need % NBUF) * TR * 32;
+    };
+
+    // wall closures (FP64): boundary pieces bl, br and their (scaled) RHS corrections
+    double bl0 = 0.0, bl1 = 0.0, br0 = 0.0, br1 = 0.0;
+    T cl0 = T(0), cl1 = T(0), cr0 = T(0), cr1 = T(0);
+    if (!PERIODIC && act) {
+      if (a.ovl) { bl0 = a.bcl0; bl1 = a.bcl1; }
+      else {
+        double fv[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) fv[k] = (double)fl[(int64_t)k * inner];
+        bl0 = tb[16] * fv[0] + tb[17] * fv[1] + tb[18] * fv[2] + tb[19] * fv[3];
+        bl1 = tb[24] * fv[0] + tb[25] * fv[1] + tb[26] * fv[2] + tb[27] * fv[3] + tb[28] * fv[4] + tb[29] * fv[5];
+      }
+      if (a.ovr) { br0 = a.bcr0; br1 = a.bcr1; }
+      else {
+        double fv[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) fv[k] = (double)fl[(int64_t)(n - 1 - k) * inner];
+        br0 = tb[20] * fv[0] + tb[21] * fv[1] + tb[22] * fv[2] + tb[23] * fv[3];
+        br1 = tb[24] * fv[0] + tb[25] * fv[1] + tb[26] * fv[2] + tb[27] * fv[3] + tb[28] * fv[4] + tb[29] * fv[5];
+      }
+      cl0 = (T)((tb[0] * bl0 + tb[1] * bl1) / c1d);
+      cl1 = (T)((tb[2] * bl0 + tb[3] * bl1) / c2d);
+      cr0 = (T)((tb[4] * br0 + tb[5] * br1) / c1d);
+      cr1 = (T)((tb[6] * br0 + tb[7] * br1) / c2d);
+    }
+    // one forward row; SPECIAL rows carry closures / head factors / ring sums
+    auto row_fwd = [&](int r, T fm, T f0, T fp, V2<T> yp, bool special) -> V2<T> {
+      T ba = fp - fm, bb = (fm + fp) - T(2) * f0;
+      if (special) {
+        if (!PERIODIC) {
+          if (r == 0) { ba -= cl0; bb -= cl1; }
+          if (r == n_rows - 1) { ba -= cr0; bb -= cr1; }
+          if (r < H0) {
+            const T* m = lt + LaneTab::head + 12 * r;
+            return {ba - (m[0] * yp.a + m[1] * yp.b), bb - (m[2] * yp.a + m[3] * yp.b)};
+          }
+        }
+      }
+      return {ba - (lf0 * yp.a + lf1 * yp.b), bb - (lf2 * yp.a + lf3 * yp.b)};
+    };
+
+    // ---- pass 1: forward sweep, chunk-end carries -------------------------------------
+    V2<T> y{T(0), T(0)};
+    V2<T> acc{T(0), T(0)};   // periodic: sum_{k < K} (-H)^k P~ y~_k of the zero-carry sweep
+    for (int c = 0; c < P; ++c) {
+      const T* tile = acquire(c);
+      const int r0 = c * CR, cnt = cnt_of(c);
+      T fm = tile[lane], f0 = tile[32 + lane];
+      const bool special = PERIODIC ? (r0 < kLaneK) : (c == 0 || c == P - 1 || r0 < H0);
+      if (!special) {
+#pragma unroll
+        for (int q = 0; q < CR; ++q) {
+          const T fp = tile[(q + 2) * 32 + lane];
+          y = row_fwd(r0 + q, fm, f0, fp, y, false);
+          fm = f0;
+          f0 = fp;
+        }
+      } else {
+        for (int q = 0; q < cnt; ++q) {
+          const int r = r0 + q;
+          const T fp = tile[(q + 2) * 32 + lane];
+          y = row_fwd(r, fm, f0, fp, y, true);
+          if (PERIODIC && r < kLaneK) {
+            const V2<T> u = mvs(lt + LaneTab::M + 4 * r, y.a, y.b);
+            acc.a += u.a;
+            acc.b += u.b;
+          }
+          fm = f0;
+          f0 = fp;
+        }
+      }
+      cy[(c * 2) * 32 + lane] = y.a;
+      cy[(c * 2 + 1) * 32 + lane] = y.b;
+      __syncwarp();
+    }
+    // ---- ring closures -------------------------------------------------------------
+    V2<T> yin{T(0), T(0)}, xc{T(0), T(0)};
+    if (PERIODIC) {
+      yin = mvs(lt + LaneTab::Gf, y.a, y.b);
+      V2<T> corr = yin;
+      for (int c = 0; c + 1 < P; ++c) {
+        corr = mvs(lt + LaneTab::PhiC, corr.a, corr.b);
+        cy[(c * 2) * 32 + lane] += corr.a;
+        cy[(c * 2 + 1) * 32 + lane] += corr.b;
+      }
+      const V2<T> qy = mvs(lt + LaneTab::Q, yin.a, yin.b);
+      xc = mvs(lt + LaneTab::Gb, acc.a + qy.a, acc.b + qy.b);
+      __syncwarp();
+    }
+    // ---- pass 2: chunks in reverse order ------------------------------------------------
+    const int noff = PERIODIC ? 0 : 1;   // node of row r
+    for (int c = P - 1; c >= 0; --c) {
+      const T* tile = acquire(c == P - 1 ? P - 1 : 2 * P - 2 - c);
+      const int r0 = c * CR, cnt = cnt_of(c);
+      const bool special = !PERIODIC && (c == 0 || c == P - 1 || r0 < H0);
+      V2<T> yr[CR];
+      V2<T> xlast{T(0), T(0)};
+      V2<T> yp = (c == 0) ? yin : V2<T>{cy[((c - 1) * 2) * 32 + lane], cy[((c - 1) * 2 + 1) * 32 + lane]};
+      T fm = tile[lane], f0 = tile[32 + lane];
+      if (!special && cnt == CR) {
+#pragma unroll
+        for (int q = 0; q < CR; ++q) {
+          const T fp = tile[(q + 2) * 32 + lane];
+          yp = row_fwd(r0 + q, fm, f0, fp, yp, false);
+          yr[q] = yp;
+          fm = f0;
+          f0 = fp;
+        }
+        __syncwarp();   // the tile is refilled by the prefetch after next
+#pragma unroll
+        for (int q = CR - 1; q >= 0; --q) {
+          const V2<T> x{(p0 * yr[q].a + p1 * yr[q].b) - (h0 * xc.a + h1 * xc.b),
+                        (p2 * yr[q].a + p3 * yr[q].b) - (h2 * xc.a + h3 * xc.b)};
+          xc = x;
+          yr[q] = x;
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < CR; ++q) {
+          if (q < cnt) {
+            const T fp = tile[(q + 2) * 32 + lane];
+            yp = row_fwd(r0 + q, fm, f0, fp, yp, true);
+            yr[q] = yp;
+            fm = f0;
+            f0 = fp;
+          }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int q = CR - 1; q >= 0; --q) {
+          if (q < cnt) {
+            const int r = r0 + q;
+            V2<T> x;
+            if (!PERIODIC && r == n_rows - 1) {
+              x = mvs(lt + LaneTab::Plast, yr[q].a, yr[q].b);
+              xlast = x;
+            } else if (r < H0) {
+              const T* pm = lt + LaneTab::head + 12 * r + 4;
+              const T* hm = pm + 4;
+              x = {(pm[0] * yr[q].a + pm[1] * yr[q].b) - (hm[0] * xc.a + hm[1] * xc.b),
+                   (pm[2] * yr[q].a + pm[3] * yr[q].b) - (hm[2] * xc.a + hm[3] * xc.b)};
+            } else {
+              x = {(p0 * yr[q].a + p1 * yr[q].b) - (h0 * xc.a + h1 * xc.b),
+                   (p2 * yr[q].a + p3 * yr[q].b) - (h2 * xc.a + h3 * xc.b)};
+            }
+            xc = x;
+            yr[q] = x;
+          }
+        }
+      }
+      // ascending burst of coalesced stores (lanes = adjacent lines)
+      if (PLAIN) {
+        if (act) {
+          T* o1 = static_cast<T*>(a.d1) + base + (int64_t)(r0 + noff) * inner;
+          T* o2 = static_cast<T*>(a.d2) + base + (int64_t)(r0 + noff) * inner;
+#pragma unroll
+          for (int q = 0; q < CR; ++q) {
+            if (q < cnt) {
+              *o1 = yr[q].a;
+              *o2 = yr[q].b;
+              o1 += inner;
+              o2 += inner;
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < CR; ++q)
+          if (q < cnt) put(r0 + q + noff, (double)yr[q].a, (double)yr[q].b);
+      }
+      if (!PERIODIC && c == P - 1) {
+        const double x0 = (double)xlast.a, x1 = (double)xlast.b;
+        put(n - 1, (tb[12] * x0 + tb[13] * x1) + br0, (tb[14] * x0 + tb[15] * x1) + br1);
+      }
+      if (c == 0) {
+        if (!PERIODIC) {
+          const double x0 = (double)xc.a, x1 = (double)xc.b;
+          put(0, (tb[8] * x0 + tb[9] * x1) + bl0, (tb[10] * x0 + tb[11] * x1) + bl1);
+        } else {
+          put(Nn, (double)xc.a, (double)xc.b);   // image node N = node 0
+        }
+      }
+      __syncwarp();   // this tile may be refilled by the next acquire
+    }
+    cp_async_wait<0>();
+    __syncwarp();
+  }
+}
+
 int build_tables(tpf_ccd_plan* p, std::vector<double>& tab) {
   const double h = p->h;
   const int n_rows = p->n_rows;
@@ -1039,6 +1362,63 @@ int build_tables(tpf_ccd_plan* p, std::vector<double>& tab) {
   tab[b + 31] = kA2 / (h * h);
   p->P = P;
   p->H0 = H0;
+  // lane-per-line kernel table, scaled by D = diag(a1/h, a2/h^2) (see ccd_lane_kernel)
+  {
+    const double d[2] = {kA1 / h, kA2 / (h * h)};
+    auto sim = [&](const M2& m) {   // D^-1 m D
+      return M2{m[0], m[1] * d[1] / d[0], m[2] * d[0] / d[1], m[3]};
+    };
+    auto rmul = [&](const M2& m) {  // m D
+      return M2{m[0] * d[0], m[1] * d[1], m[2] * d[0], m[3] * d[1]};
+    };
+    const int tot = LaneTab::head + 12 * H0;
+    std::vector<double>& lt = p->ltab_host;
+    lt.assign(tot, 0.0);
+    const M2 Lfs = sim(Lfinf), Ps = rmul(Pinf);
+    for (int q = 0; q < 4; ++q) {
+      lt[LaneTab::Lf + q] = Lfs[q];
+      lt[LaneTab::P + q] = Ps[q];
+      lt[LaneTab::H + q] = Hinf[q];
+    }
+    if (p->bc == TPF_BC_WALL) {
+      const M2 Pl = rmul(Pm[n_rows - 1]);
+      for (int q = 0; q < 4; ++q) lt[LaneTab::Plast + q] = Pl[q];
+      for (int j = 0; j < H0; ++j) {
+        const M2 lj = sim(Lf[j]), pj = rmul(Pm[j]);
+        for (int q = 0; q < 4; ++q) {
+          lt[LaneTab::head + 12 * j + q] = lj[q];
+          lt[LaneTab::head + 12 * j + 4 + q] = pj[q];
+          lt[LaneTab::head + 12 * j + 8 + q] = Hm[j][q];
+        }
+      }
+    } else {
+      // ring: Tr = (-Lf)^N, Rr = (-H)^N; PhiC = (-Lf)^CR; M_k = (-H)^k P; Q = sum_k M_k (-Lf)^(k+1)
+      M2 Tr = eye(), Rr = eye(), PhiC = eye();
+      for (int k = 0; k < n_rows; ++k) {
+        Tr = mul(neg(Lfinf), Tr);
+        Rr = mul(neg(Hinf), Rr);
+      }
+      for (int k = 0; k < kLaneCR; ++k) PhiC = mul(neg(Lfinf), PhiC);
+      const M2 Gf = inv(sub(eye(), Tr)), Gb = inv(sub(eye(), Rr));
+      M2 Hk = eye(), Phk = eye(), Q = {0, 0, 0, 0};
+      const int K = std::min(kLaneK, n_rows);
+      for (int k = 0; k < K; ++k) {
+        const M2 Mk = mul(Hk, Pinf);
+        Phk = mul(neg(Lfinf), Phk);
+        Q = add(Q, mul(Mk, Phk));
+        const M2 Mks = rmul(Mk);
+        for (int q = 0; q < 4; ++q) lt[LaneTab::M + 4 * k + q] = Mks[q];
+        Hk = mul(neg(Hinf), Hk);
+      }
+      const M2 Gfs = sim(Gf), PhiCs = sim(PhiC), Qs = rmul(Q);
+      for (int q = 0; q < 4; ++q) {
+        lt[LaneTab::Gf + q] = Gfs[q];
+        lt[LaneTab::Gb + q] = Gb[q];
+        lt[LaneTab::PhiC + q] = PhiCs[q];
+        lt[LaneTab::Q + q] = Qs[q];
+      }
+    }
+  }
   return TPF_OK;
 }
 
@@ -1128,6 +1508,55 @@ LaunchShape pick_warp_shape(const tpf_ccd_plan* p, int64_t n_lines) {
   return best;
 }
 
+// many lines (3-D grids) and long enough lines: the lane-per-line kernel
+bool use_lane_kernel(const tpf_ccd_plan* p, int64_t n_lines, bool periodic, bool contig) {
+  if (contig) return false;   // the contiguous axis keeps the warp-per-line kernel (faster there)
+  if (p->n_rows < 128 || p->n_rows > 2048) return false;
+  if (periodic != (p->bc == TPF_BC_PERIODIC)) return false;   // closure overrides on a periodic plan
+  return n_lines >= 148LL * 4 * 32;
+}
+
+#ifndef TPF_LANE_WARPS
+#define TPF_LANE_WARPS 4
+#endif
+#ifndef TPF_LANE_MAX_BLOCKS_PER_SM
+#define TPF_LANE_MAX_BLOCKS_PER_SM 64
+#endif
+// f tile ring depth: FP64 keeps two chunks in flight (3 buffers); FP32 gets
+// more resident warps from the smaller 2-buffer ring (measured on B200)
+#ifndef TPF_LANE_NBUF64
+#define TPF_LANE_NBUF64 3
+#endif
+#ifndef TPF_LANE_NBUF32
+#define TPF_LANE_NBUF32 2
+#endif
+
+template <typename T>
+int launch_lane(const tpf_ccd_plan* p, const CcdArgs& a, bool periodic, cudaStream_t stream) {
+  constexpr int W = TPF_LANE_WARPS;
+  const int P = (p->n_rows + kLaneCR - 1) / kLaneCR;
+  constexpr int NB = std::is_same<T, double>::value ? TPF_LANE_NBUF64 : TPF_LANE_NBUF32;
+  const size_t per_warp = (size_t)NB * (kLaneCR + 2) * 32 + 64 * (size_t)P;
+  const size_t smem = sizeof(T) * ((((size_t)p->ltab_total + 1) & ~(size_t)1) + W * per_warp);
+  TPF_CHECK_ARG(smem <= 225 * 1024, "CCD lane kernel: axis of %lld points needs too much shared memory",
+                (long long)p->n_pts);
+  const bool plain = a.d1 && a.d2 && !a.vd_out && !a.J;
+  void (*kern)(CcdArgs, const T*, int) =
+      periodic ? (plain ? ccd_lane_kernel<T, true, true, NB> : ccd_lane_kernel<T, true, false, NB>)
+               : (plain ? ccd_lane_kernel<T, false, true, NB> : ccd_lane_kernel<T, false, false, NB>);
+  TPF_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  TPF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * W, smem));
+  per_sm = std::max(1, std::min(per_sm, TPF_LANE_MAX_BLOCKS_PER_SM));
+  const int64_t groups = (a.n_lines + 31) / 32;
+  const int64_t blocks = std::min<int64_t>((groups + W - 1) / W, (int64_t)tpf::sm_count() * per_sm);
+  const T* lt = std::is_same<T, double>::value ? reinterpret_cast<const T*>(p->d_ltab)
+                                               : reinterpret_cast<const T*>(p->d_ltabf);
+  kern<<<(unsigned)blocks, 32 * W, smem, stream>>>(a, lt, p->ltab_total);
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
 template <typename T>
 int launch_ccd(const tpf_ccd_plan* p, int64_t outer, int64_t inner, const void* f, void* d1, void* d2,
                const double* bcl, const double* bcr, int flags, cudaStream_t stream,
@@ -1165,6 +1594,7 @@ int launch_ccd(const tpf_ccd_plan* p, int64_t outer, int64_t inner, const void* 
   a.vd_out = vd_out;
   a.vd_accumulate = vd_accumulate;
   const bool per = (p->bc == TPF_BC_PERIODIC) && !a.ovl && !a.ovr;
+  if (use_lane_kernel(p, n_lines, per, contig)) return launch_lane<T>(p, a, per, stream);
   void (*kern)(CcdArgs);
   if (!warp) {
     if (per) kern = contig ? ccd_line_kernel<T, true, true> : ccd_line_kernel<T, true, false>;
@@ -1230,6 +1660,23 @@ int tpf_ccd_plan_create(tpf_ccd_plan** out, int64_t n_pts, double h, int bc, int
     delete p;
     return TPF_ECUDA;
   }
+  {
+    const std::vector<double>& lt = p->ltab_host;
+    std::vector<float> ltf(lt.begin(), lt.end());
+    p->ltab_total = (int)lt.size();
+    if (cudaMalloc(&p->d_ltab, lt.size() * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&p->d_ltabf, lt.size() * sizeof(float)) != cudaSuccess ||
+        cudaMemcpy(p->d_ltab, lt.data(), lt.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(p->d_ltabf, ltf.data(), ltf.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
+      tpf::set_error("allocation / copy of the CCD lane table failed");
+      cudaFree(p->d_tab);
+      cudaFree(p->d_tabf);
+      cudaFree(p->d_ltab);
+      cudaFree(p->d_ltabf);
+      delete p;
+      return TPF_ECUDA;
+    }
+  }
   *out = p;
   return TPF_OK;
 }
@@ -1238,6 +1685,8 @@ int tpf_ccd_plan_destroy(tpf_ccd_plan* p) {
   if (!p) return TPF_OK;
   cudaFree(p->d_tab);
   cudaFree(p->d_tabf);
+  cudaFree(p->d_ltab);
+  cudaFree(p->d_ltabf);
   cudaFree(p->d_J);
   delete p;
   return TPF_OK;
