@@ -245,3 +245,89 @@ def test_ccd_rejects_short_wall_axis(cuda_device):
     ccd = CCDSolver(grid, None, bc_type="wall")
     with pytest.raises(ValueError, match="n_pts >= 6"):
         ccd.differentiate(np.zeros(grid.shape), axis=0)
+
+
+# shapes whose differentiated axis has 131 nodes and >= 19 200 lines, so every
+# axis runs on the lane-per-line kernel (strided axes and the contiguous one)
+_LANE_SHAPES = {0: (131, 150, 128), 1: (150, 131, 128), 2: (150, 128, 131)}
+
+
+@pytest.mark.parametrize("bc", ["wall", "periodic"])
+@pytest.mark.parametrize("ax", [0, 1, 2])
+def test_ccd_lane_kernel_against_oracle(cuda_device, bc, ax):
+    """Many-line 3-D fields: d1/d2 and the single-output calls against the oracle."""
+    import torch
+    from twophaseflow_b200 import CCDSolver
+    shape = _LANE_SHAPES[ax]
+    N = tuple(s - 1 for s in shape)
+    grid = _Grid(N, (1.0, 1.3, 0.7))
+    f = fourier_field(N, L=grid.L, n_modes=6, kmax=6, seed=11 + ax)
+    ft = torch.from_numpy(f).to(cuda_device)
+    ccd = CCDSolver(grid, None, bc_type=bc)
+    h = grid.L[ax] / N[ax]
+    o1, o2 = occd.differentiate(f, ax, h, bc=bc)
+    cl = bc == "wall"
+    a1 = _closure_atol(f, h, 1) if cl else 0.0
+    a2 = _closure_atol(f, h, 2) if cl else 0.0
+    d1, d2 = ccd.differentiate(ft, ax)
+    _close(d1.cpu().numpy(), o1, FP64_RTOL, a1)
+    _close(d2.cpu().numpy(), o2, FP64_RTOL, a2)
+    _close(ccd.first_derivative(ft, ax).cpu().numpy(), o1, FP64_RTOL, a1)
+    _close(ccd.second_derivative(ft, ax).cpu().numpy(), o2, FP64_RTOL, a2)
+
+
+@pytest.mark.parametrize("bc", ["wall", "periodic"])
+@pytest.mark.parametrize("ax", [0, 2])
+def test_ccd_lane_kernel_fp32(cuda_device, bc, ax):
+    import torch
+    from twophaseflow_b200 import CCDSolver
+    shape = _LANE_SHAPES[ax]
+    N = tuple(s - 1 for s in shape)
+    grid = _Grid(N, (1.0, 1.0, 1.0))
+    f = fourier_field(N, n_modes=6, kmax=6, seed=21 + ax).astype(np.float32).astype(np.float64)
+    ccd32 = CCDSolver(grid, None, bc_type=bc, dtype=torch.float32)
+    h = 1.0 / N[ax]
+    o1, o2 = occd.differentiate(f, ax, h, bc=bc)
+    d1, d2 = ccd32.differentiate(torch.from_numpy(f).to(cuda_device), ax)
+    _close(d1.double().cpu().numpy(), o1, FP32_RTOL)
+    _close(d2.double().cpu().numpy(), o2, 5 * FP32_RTOL)
+
+
+@pytest.mark.parametrize("ax", [0, 2])
+def test_ccd_lane_kernel_metric_and_vd(cuda_device, ax):
+    """Non-uniform metric epilogue and the variable-density (L_H) epilogue on
+    the lane kernel: against J d1_xi, J^2 d2_xi + J J' d1_xi and against
+    d2/rho - (drho/rho^2) d1 built from the raw derivatives."""
+    import torch
+    from twophaseflow_b200 import CCDSolver
+    from twophaseflow_b200.arrays import line_split
+    from twophaseflow_b200 import _lib
+    shape = _LANE_SHAPES[ax]
+    N = tuple(s - 1 for s in shape)
+    xi = [np.linspace(0, 1, n + 1) for n in N]
+    J = [1.0 + 0.3 * np.cos(2 * np.pi * x) for x in xi]
+    dJ = [-0.6 * np.pi * np.sin(2 * np.pi * x) for x in xi]
+    grid = _Grid(N, (1.0, 1.0, 1.0), uniform=False, J=J, dJ=dJ)
+    f = fourier_field(N, n_modes=5, kmax=5, seed=31 + ax)
+    ft = torch.from_numpy(f).to(cuda_device)
+    ccd = CCDSolver(grid, None, bc_type="wall")
+    r1, r2 = ccd.differentiate(ft, ax, apply_metric=False)
+    m1, m2 = ccd.differentiate(ft, ax)
+    bshape = [1, 1, 1]
+    bshape[ax] = -1
+    Jt = torch.from_numpy(J[ax]).to(cuda_device).view(bshape)
+    dJt = torch.from_numpy(dJ[ax]).to(cuda_device).view(bshape)
+    _close(m1.cpu().numpy(), (Jt * r1).cpu().numpy(), 1e-13)
+    _close(m2.cpu().numpy(), (Jt * Jt * r2 + Jt * dJt * r1).cpu().numpy(), 1e-13)
+    # variable-density epilogue on the uniform plan
+    ccdu = CCDSolver(_Grid(N, (1.0, 1.0, 1.0)), None, bc_type="wall")
+    rho = torch.from_numpy(1.5 + np.cos(np.linspace(0, 3, f.size)).reshape(f.shape)).to(cuda_device)
+    drho = torch.from_numpy(0.2 * np.sin(np.linspace(0, 5, f.size)).reshape(f.shape)).to(cuda_device)
+    u1, u2 = ccdu.differentiate(ft, ax)
+    out = torch.empty_like(ft)
+    outer, n, inner = line_split(ft.shape, ax)
+    plan = ccdu._plan(ax, False)
+    _lib.check(ccdu.lib.tpf_ccd_apply_vd(plan, outer, inner, _lib.dptr(ft), _lib.dptr(rho), _lib.dptr(drho),
+                                         _lib.dptr(out), 0, 0, _lib.current_stream_handle()))
+    ref = u2 / rho - (drho / (rho * rho)) * u1
+    _close(out.cpu().numpy(), ref.cpu().numpy(), 1e-13)

@@ -956,9 +956,11 @@ __device__ __forceinline__ void cp_async_wait_dyn(int pending) {
   else cp_async_wait<2>();
 }
 
-template <typename T, bool PERIODIC, bool PLAIN, int NBUF>
+template <typename T, bool PERIODIC, bool PLAIN, int NBUF, bool CONTIG>
 __global__ void __launch_bounds__(128) ccd_lane_kernel(CcdArgs a, const T* __restrict__ ltab_g, int ltab_total) {
   constexpr int CR = kLaneCR, TR = CR + 2;
+  constexpr int TS = CONTIG ? 33 : 32;   // tile row stride (padded for the transposing copies)
+  constexpr int NT = NBUF + (CONTIG ? 1 : 0);   // + the d2 output tile
   static_assert(NBUF == 2 || NBUF == 3, "f tile ring of 2 or 3 buffers");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* lt = reinterpret_cast<T*>(smem_raw);
@@ -966,8 +968,9 @@ __global__ void __launch_bounds__(128) ccd_lane_kernel(CcdArgs a, const T* __res
   const int n = a.n, n_rows = a.n_rows, H0 = PERIODIC ? 0 : a.H0;
   const int P = (n_rows + CR - 1) / CR;
   const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  T* fb0 = lt + lt_pad + (size_t)wid * (NBUF * TR * 32 + 64 * P);   // ring of f tiles [TR][32]
-  T* cy = fb0 + NBUF * TR * 32;                                         // chunk-end carries [P][2][32]
+  T* fb0 = lt + lt_pad + (size_t)wid * (NT * TR * TS + 64 * P);   // ring of f tiles [TR][TS]
+  T* dt = fb0 + NBUF * TR * TS;                                       // contiguous axis: d2 tile
+  T* cy = fb0 + NT * TR * TS;                                         // chunk-end carries [P][2][32]
   for (int i = threadIdx.x; i < ltab_total; i += blockDim.x) lt[i] = ltab_g[i];
   __syncthreads();
 
@@ -994,17 +997,38 @@ __global__ void __launch_bounds__(128) ccd_lane_kernel(CcdArgs a, const T* __res
     const T* __restrict__ fl = f + base;
     // asynchronous copy of nodes k0 + t, t in [0, KN), into tile[t][lane]
     auto stage = [&](T* tile, int k0, int KN) {
+      if (CONTIG) {
+        // element e = (line ll, node t) of the chunk, e = lane + 32 i: runs of KN
+        // contiguous nodes per line, so each warp copy reads ~2 contiguous runs
+        int ll = lane / KN, t = lane - (lane / KN) * KN;
+        const int dl = 32 / KN, dt_ = 32 - dl * KN;
+        const T* fg = f + g * 32 * (int64_t)n;   // first line of the group
+        const int nl = (a.n_lines - g * 32 < 32) ? (int)(a.n_lines - g * 32) : 32;
+        const bool wrap = PERIODIC && (k0 < 0 || k0 + KN > Nn);
+        for (int i = 0; i < KN; ++i) {
+          if (ll < nl) {
+            int kk = k0 + t;
+            if (wrap) kk = (kk < 0) ? kk + Nn : (kk >= Nn ? kk - Nn : kk);
+            cp_async<sizeof(T)>(tile + t * TS + ll, fg + (ll * n + kk), true);
+          }
+          ll += dl;
+          t += dt_;
+          if (t >= KN) { t -= KN; ++ll; }
+        }
+        cp_async_commit();
+        return;
+      }
       if (act) {
         if (PERIODIC && (k0 < 0 || k0 + KN > Nn)) {
           for (int t = 0; t < KN; ++t) {
             int k = k0 + t;
             k = (k < 0) ? k + Nn : (k >= Nn ? k - Nn : k);
-            cp_async<sizeof(T)>(tile + t * 32 + lane, fl + (int64_t)k * inner, true);
+            cp_async<sizeof(T)>(tile + t * TS + lane, fl + (int64_t)k * inner, true);
           }
         } else {
           const T* src = fl + (int64_t)k0 * inner;
           for (int t = 0; t < KN; ++t) {
-            cp_async<sizeof(T)>(tile + t * 32 + lane, src, true);
+            cp_async<sizeof(T)>(tile + t * TS + lane, src, true);
             src += inner;
           }
         }
@@ -1033,12 +1057,12 @@ __global__ void __launch_bounds__(128) ccd_lane_kernel(CcdArgs a, const T* __res
       const int want = min(n_loads, need + NBUF);
       while (issued < want) {
         const int c = chunk_of_load(issued);
-        stage(fb0 + (issued % NBUF) * TR * 32, k0_of(c), cnt_of(c) + 2);
+        stage(fb0 + (issued % NBUF) * TR * TS, k0_of(c), cnt_of(c) + 2);
         ++issued;
       }
       cp_async_wait_dyn<NBUF>(issued - need - 1);
       __syncwarp();
-      return fb0 + (need % NBUF) * TR * 32;
+      return fb0 + (need % NBUF) * TR * TS;
     };
 
     // wall closures (FP64): boundary pieces bl, br and their (scaled) RHS corrections
@@ -1088,12 +1112,12 @@ __global__ void __launch_bounds__(128) ccd_lane_kernel(CcdArgs a, const T* __res
     for (int c = 0; c < P; ++c) {
       const T* tile = acquire(c);
       const int r0 = c * CR, cnt = cnt_of(c);
-      T fm = tile[lane], f0 = tile[32 + lane];
-      const bool special = PERIODIC ? (r0 < kLaneK) : (c == 0 || c == P - 1 || r0 < H0);
+      T fm = tile[lane], f0 = tile[TS + lane];
+      const bool special = cnt != CR || (PERIODIC ? (r0 < kLaneK) : (c == 0 || c == P - 1 || r0 < H0));
       if (!special) {
 #pragma unroll
         for (int q = 0; q < CR; ++q) {
-          const T fp = tile[(q + 2) * 32 + lane];
+          const T fp = tile[(q + 2) * TS + lane];
           y = row_fwd(r0 + q, fm, f0, fp, y, false);
           fm = f0;
           f0 = fp;
@@ -1101,7 +1125,7 @@ __global__ void __launch_bounds__(128) ccd_lane_kernel(CcdArgs a, const T* __res
       } else {
         for (int q = 0; q < cnt; ++q) {
           const int r = r0 + q;
-          const T fp = tile[(q + 2) * 32 + lane];
+          const T fp = tile[(q + 2) * TS + lane];
           y = row_fwd(r, fm, f0, fp, y, true);
           if (PERIODIC && r < kLaneK) {
             const V2<T> u = mvs(lt + LaneTab::M + 4 * r, y.a, y.b);
@@ -1139,11 +1163,11 @@ __global__ void __launch_bounds__(128) ccd_lane_kernel(CcdArgs a, const T* __res
       V2<T> yr[CR];
       V2<T> xlast{T(0), T(0)};
       V2<T> yp = (c == 0) ? yin : V2<T>{cy[((c - 1) * 2) * 32 + lane], cy[((c - 1) * 2 + 1) * 32 + lane]};
-      T fm = tile[lane], f0 = tile[32 + lane];
+      T fm = tile[lane], f0 = tile[TS + lane];
       if (!special && cnt == CR) {
 #pragma unroll
         for (int q = 0; q < CR; ++q) {
-          const T fp = tile[(q + 2) * 32 + lane];
+          const T fp = tile[(q + 2) * TS + lane];
           yp = row_fwd(r0 + q, fm, f0, fp, yp, false);
           yr[q] = yp;
           fm = f0;
@@ -1161,7 +1185,7 @@ __global__ void __launch_bounds__(128) ccd_lane_kernel(CcdArgs a, const T* __res
 #pragma unroll
         for (int q = 0; q < CR; ++q) {
           if (q < cnt) {
-            const T fp = tile[(q + 2) * 32 + lane];
+            const T fp = tile[(q + 2) * TS + lane];
             yp = row_fwd(r0 + q, fm, f0, fp, yp, true);
             yr[q] = yp;
             fm = f0;
@@ -1190,6 +1214,65 @@ __global__ void __launch_bounds__(128) ccd_lane_kernel(CcdArgs a, const T* __res
             yr[q] = x;
           }
         }
+      }
+      if (CONTIG) {
+        // results through the (consumed) f tile and the d2 tile, then runs of
+        // contiguous nodes per line
+        T* ot = const_cast<T*>(tile);
+#pragma unroll
+        for (int q = 0; q < CR; ++q) {
+          if (q < cnt) {
+            ot[(q + 1) * TS + lane] = yr[q].a;
+            dt[(q + 1) * TS + lane] = yr[q].b;
+          }
+        }
+        int t0 = 1, t1 = cnt + 1;
+        if (!PERIODIC && c == P - 1) {
+          const double x0 = (double)xlast.a, x1 = (double)xlast.b;
+          ot[(cnt + 1) * TS + lane] = (T)((tb[12] * x0 + tb[13] * x1) + br0);
+          dt[(cnt + 1) * TS + lane] = (T)((tb[14] * x0 + tb[15] * x1) + br1);
+          t1 = cnt + 2;
+        }
+        if (!PERIODIC && c == 0) {
+          const double x0 = (double)xc.a, x1 = (double)xc.b;
+          ot[lane] = (T)((tb[8] * x0 + tb[9] * x1) + bl0);
+          dt[lane] = (T)((tb[10] * x0 + tb[11] * x1) + bl1);
+          t0 = 0;
+        }
+        __syncwarp();
+        const int KN = t1 - t0;
+        const int k0 = k0_of(c) + t0;
+        int ll = lane / KN, t = lane - (lane / KN) * KN;
+        const int dl = 32 / KN, dt_ = 32 - dl * KN;
+        const int64_t g0 = g * 32 * (int64_t)n;
+        const int nl = (a.n_lines - g * 32 < 32) ? (int)(a.n_lines - g * 32) : 32;
+        const bool plain_c = a.d1 && a.d2 && !a.vd_out && !J;
+        T* o1p = static_cast<T*>(a.d1) + g0;
+        T* o2p = static_cast<T*>(a.d2) + g0;
+        for (int i = 0; i < KN; ++i) {
+          if (ll < nl) {
+            const int node = k0 + t;
+            const T v1 = ot[(t0 + t) * TS + ll], v2 = dt[(t0 + t) * TS + ll];
+            if (plain_c) {
+              o1p[ll * n + node] = v1;
+              o2p[ll * n + node] = v2;
+            } else {
+              double o1 = (double)v1, o2 = (double)v2;
+              if (J) {
+                const double Jk = J[node], dJk = J[n + node];
+                o2 = Jk * Jk * o2 + Jk * dJk * o1;
+                o1 = Jk * o1;
+              }
+              store_out<T>(a, g0 + (int64_t)ll * n + node, o1, o2);
+            }
+          }
+          ll += dl;
+          t += dt_;
+          if (t >= KN) { t -= KN; ++ll; }
+        }
+        if (PERIODIC && c == 0) put(Nn, (double)xc.a, (double)xc.b);   // image node N = node 0 (own line)
+        __syncwarp();
+        continue;
       }
       // ascending burst of coalesced stores (lanes = adjacent lines)
       if (PLAIN) {
@@ -1510,7 +1593,6 @@ LaunchShape pick_warp_shape(const tpf_ccd_plan* p, int64_t n_lines) {
 
 // many lines (3-D grids) and long enough lines: the lane-per-line kernel
 bool use_lane_kernel(const tpf_ccd_plan* p, int64_t n_lines, bool periodic, bool contig) {
-  if (contig) return false;   // the contiguous axis keeps the warp-per-line kernel (faster there)
   if (p->n_rows < 128 || p->n_rows > 2048) return false;
   if (periodic != (p->bc == TPF_BC_PERIODIC)) return false;   // closure overrides on a periodic plan
   return n_lines >= 148LL * 4 * 32;
@@ -1532,18 +1614,22 @@ bool use_lane_kernel(const tpf_ccd_plan* p, int64_t n_lines, bool periodic, bool
 #endif
 
 template <typename T>
-int launch_lane(const tpf_ccd_plan* p, const CcdArgs& a, bool periodic, cudaStream_t stream) {
+int launch_lane(const tpf_ccd_plan* p, const CcdArgs& a, bool periodic, bool contig, cudaStream_t stream) {
   constexpr int W = TPF_LANE_WARPS;
   const int P = (p->n_rows + kLaneCR - 1) / kLaneCR;
   constexpr int NB = std::is_same<T, double>::value ? TPF_LANE_NBUF64 : TPF_LANE_NBUF32;
-  const size_t per_warp = (size_t)NB * (kLaneCR + 2) * 32 + 64 * (size_t)P;
+  const size_t per_warp = (size_t)(NB + (contig ? 1 : 0)) * (kLaneCR + 2) * (contig ? 33 : 32) + 64 * (size_t)P;
   const size_t smem = sizeof(T) * ((((size_t)p->ltab_total + 1) & ~(size_t)1) + W * per_warp);
   TPF_CHECK_ARG(smem <= 225 * 1024, "CCD lane kernel: axis of %lld points needs too much shared memory",
                 (long long)p->n_pts);
   const bool plain = a.d1 && a.d2 && !a.vd_out && !a.J;
-  void (*kern)(CcdArgs, const T*, int) =
-      periodic ? (plain ? ccd_lane_kernel<T, true, true, NB> : ccd_lane_kernel<T, true, false, NB>)
-               : (plain ? ccd_lane_kernel<T, false, true, NB> : ccd_lane_kernel<T, false, false, NB>);
+  void (*kern)(CcdArgs, const T*, int);
+  if (contig)
+    kern = periodic ? ccd_lane_kernel<T, true, false, NB, true> : ccd_lane_kernel<T, false, false, NB, true>;
+  else if (periodic)
+    kern = plain ? ccd_lane_kernel<T, true, true, NB, false> : ccd_lane_kernel<T, true, false, NB, false>;
+  else
+    kern = plain ? ccd_lane_kernel<T, false, true, NB, false> : ccd_lane_kernel<T, false, false, NB, false>;
   TPF_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   TPF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * W, smem));
@@ -1594,7 +1680,7 @@ int launch_ccd(const tpf_ccd_plan* p, int64_t outer, int64_t inner, const void* 
   a.vd_out = vd_out;
   a.vd_accumulate = vd_accumulate;
   const bool per = (p->bc == TPF_BC_PERIODIC) && !a.ovl && !a.ovr;
-  if (use_lane_kernel(p, n_lines, per, contig)) return launch_lane<T>(p, a, per, stream);
+  if (use_lane_kernel(p, n_lines, per, contig)) return launch_lane<T>(p, a, per, contig, stream);
   void (*kern)(CcdArgs);
   if (!warp) {
     if (per) kern = contig ? ccd_line_kernel<T, true, true> : ccd_line_kernel<T, true, false>;
