@@ -246,6 +246,15 @@ int tpf_unet_backward(tpf_unet* net, int B, const float* dy, float* grads, void*
 int tpf_unet_train_step(tpf_unet* net, int B, const float* in2, const float* target, float lr,
                         float weight_decay, double* loss, void* stream);
 
+/* One Adam step on the energy loss of a coarse-grid correction (two-level
+ * training): per sample, with y the network output, x = in2[..,0] and
+ * A~ = I - couplings (coupl[q][0] to the next row, coupl[q][1] to the next
+ * column, inside the nc0 x nc1 coarse grid),
+ * L = (y.A~y - 2 y.x) / escale + 1, the relative A-norm error left after the
+ * correction; *loss (may be NULL) is the batch mean before the step. */
+int tpf_unet_train_step_energy(tpf_unet* net, int B, const float* in2, const float* coupl, const double* escale,
+                               int nc0, int nc1, float lr, float weight_decay, double* loss, void* stream);
+
 typedef struct tpf_learned_options {
   double tol;           /* relative residual tolerance of the weighted system   */
   int64_t maxiter;      /* flexible-CG iterations before the fallback           */
@@ -256,6 +265,7 @@ typedef struct tpf_learned_options {
   double stall_factor;  /* stall_factor within stall_checks x check_every iters  */
   int fallback;         /* 1: finish with plain Jacobi PCG after a stall          */
   int use_graph;        /* 1: replay one iteration as a CUDA graph                */
+  int window;           /* stored directions of the truncated flexible CG (1..8) */
 } tpf_learned_options;
 
 typedef struct tpf_lppe_result {
@@ -270,9 +280,12 @@ typedef struct tpf_lppe_result {
 typedef struct tpf_lppe tpf_lppe;
 
 void tpf_lppe_default_options(tpf_learned_options* opts);
-/* Learned solver on a 2-D PPE handle; the network image must be the node
- * counts rounded up to multiples of 8. */
-int tpf_lppe_create(tpf_lppe** lp, tpf_ppe* ppe, tpf_unet* net);
+/* Learned solver on a 2-D PPE handle.  coarsen = 1: the network reads the
+ * fine residual (image = node counts rounded up to multiples of 8);
+ * coarsen = b in {2, 4, 8}: two-level mode, the network solves the problem
+ * aggregated over b x b node blocks (image = ceil(n / b) rounded up to 8)
+ * inside a V(1, smooth) cycle with damped-Jacobi sweeps on the fine grid. */
+int tpf_lppe_create(tpf_lppe** lp, tpf_ppe* ppe, tpf_unet* net, int coarsen);
 int tpf_lppe_destroy(tpf_lppe* lp);
 /* tpf_ppe_prepare plus the density feature of the network input. */
 int tpf_lppe_prepare(tpf_lppe* lp, const double* rho, void* stream);
@@ -282,10 +295,19 @@ int tpf_lppe_solve(tpf_lppe* lp, const double* rhs, const double* rho, double* p
                    const tpf_learned_options* opts, void* stream, tpf_lppe_result* result);
 /* z = B(r), the preconditioner alone (r, z device vectors of the grid). */
 int tpf_lppe_precondition(tpf_lppe* lp, const double* r, double* z, int smooth, double omega, void* stream);
-/* Training pair from an error field e of the weighted system (pin 0):
- * in2 = (D^-1/2 S e / s, density feature), target = D^1/2 e / s on the
- * network image (s = rms of D^-1/2 S e); in2 and target are device FP32. */
-int tpf_lppe_pair(tpf_lppe* lp, const double* e, float* in2, float* target, void* stream);
+/* Training pair from an error field e of the weighted system (pin 0), in the
+ * form the network reads (in2, target: device FP32 on the network image).
+ * coarsen = 1: in2 = (D^-1/2 S e / s, density feature), target = D^1/2 e / s
+ * (s = rms of D^-1/2 S e).  Two-level mode: with r = S e, the pre-smoothing
+ * sweep z1 = omega D^-1 r, r1 = r - S z1 and e1 = e - z1,
+ * in2 = (D_c^-1/2 R r1 / s_c, aggregate density feature) and
+ * target = D_c^1/2 mean_aggregate(e1) / s_c. */
+int tpf_lppe_pair(tpf_lppe* lp, const double* e, float* in2, float* target, double omega, void* stream);
+/* Two-level mode: the data of the energy loss for an error field e: in2 as
+ * tpf_lppe_pair, coupl [H][W][2] = scaled Galerkin couplings of the coarse
+ * operator, *escale (device) = (e1 . S e1) / s_c^2. */
+int tpf_lppe_pair_energy(tpf_lppe* lp, const double* e, float* in2, float* coupl, double* escale, double omega,
+                         void* stream);
 
 #ifdef __cplusplus
 }

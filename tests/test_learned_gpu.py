@@ -113,8 +113,8 @@ def _case(N, seed, ratio=1000.0):
     return rho, rhs
 
 
-@pytest.mark.parametrize("smooth", [1, 2])
-def test_flexible_cg_matches_direct_solution(cuda_device, smooth):
+@pytest.mark.parametrize("smooth,coarsen", [(1, 1), (2, 1), (1, 4)])
+def test_flexible_cg_matches_direct_solution(cuda_device, smooth, coarsen):
     """With all-zero network parameters the preconditioner reduces to damped
     Jacobi sweeps (a fixed SPD map), so the flexible CG must converge like
     PCG: this checks the FCG recurrences, the pinning and the true-residual
@@ -124,7 +124,8 @@ def test_flexible_cg_matches_direct_solution(cuda_device, smooth):
     from twophaseflow_b200.learned import PPESolverLearned, num_params
     N = (64, 64)
     rho, rhs = _case(N, seed=3)
-    cfg = _Cfg(pseudo_tol=1e-10, pseudo_maxiter=4000, ppe_learned_smooth=smooth, ppe_learned_fallback=False)
+    cfg = _Cfg(pseudo_tol=1e-10, pseudo_maxiter=4000, ppe_learned_smooth=smooth, ppe_learned_fallback=False,
+               ppe_learned_coarsen=coarsen)
     s = PPESolverLearned(None, cfg, UniformGrid(N), params=np.zeros(num_params(), np.float32))
     p = s.solve(torch.from_numpy(rhs).to(cuda_device), torch.from_numpy(rho).to(cuda_device)).cpu().numpy()
     d = s.last_diagnostics
@@ -144,7 +145,8 @@ def test_learned_solve_falls_back_to_pcg_on_stall(cuda_device):
     rho, rhs = _case(N, seed=5)
     # an all-zero network without smoothing gives z = 0: no progress -> fallback
     from twophaseflow_b200.learned import num_params
-    cfg = _Cfg(pseudo_tol=1e-9, pseudo_maxiter=400, ppe_learned_smooth=0, ppe_learned_maxiter=400)
+    cfg = _Cfg(pseudo_tol=1e-9, pseudo_maxiter=400, ppe_learned_smooth=0, ppe_learned_maxiter=400,
+               ppe_learned_coarsen=1)
     s = PPESolverLearned(None, cfg, UniformGrid(N), params=np.zeros(num_params(), np.float32))
     p = s.solve(torch.from_numpy(rhs).to(cuda_device), torch.from_numpy(rho).to(cuda_device)).cpu().numpy()
     d = s.last_diagnostics
@@ -157,7 +159,7 @@ def test_pairs_are_consistent(cuda_device):
     """in2 channel 0 is D^-1/2 S e / s and target is D^1/2 e / s for the same s."""
     import torch
     from twophaseflow_b200.learned import generate_pairs
-    in2, tgt = generate_pairs(N=(32, 32), n_cases=2, snapshots=(0, 5), seed=1)
+    in2, tgt = generate_pairs(N=(32, 32), n_cases=2, snapshots=(0, 5), seed=1, coarsen=1)
     assert in2.shape == (4, 40, 40, 2) and tgt.shape == (4, 40, 40)
     a = in2.cpu().numpy()
     t = tgt.cpu().numpy()
@@ -167,3 +169,63 @@ def test_pairs_are_consistent(cuda_device):
     assert np.allclose(rms, 1.0, rtol=1e-4)
     assert np.all(a[:, 33:, :, :] == 0) and np.all(t[:, :, 33:] == 0)
     assert np.all((a[..., 1] >= 0) & (a[..., 1] <= 1))
+
+
+def test_two_level_pairs(cuda_device):
+    """Two-level pairs: coarse image of ceil(33/4) = 9 aggregates (padded to 16),
+    unit-RMS scaled restricted residual, zero padding."""
+    from twophaseflow_b200.learned import generate_pairs
+    in2, tgt = generate_pairs(N=(32, 32), n_cases=2, snapshots=(0, 5), seed=1, coarsen=4)
+    assert in2.shape == (4, 16, 16, 2) and tgt.shape == (4, 16, 16)
+    a = in2.cpu().numpy()
+    t = tgt.cpu().numpy()
+    assert np.isfinite(a).all() and np.isfinite(t).all()
+    rms = np.sqrt((a[:, :9, :9, 0] ** 2).mean(axis=(1, 2)))
+    assert np.allclose(rms, 1.0, rtol=1e-4)
+    assert np.all(a[:, 9:, :, :] == 0) and np.all(t[:, :, 9:] == 0)
+
+
+def test_energy_pairs_and_loss(cuda_device):
+    """Energy-loss data: a zero network leaves the whole error (loss exactly 1);
+    a few training steps reduce the A-norm error left by the coarse correction."""
+    import torch
+    from twophaseflow_b200.learned import UNet, generate_pairs, net_image, num_params
+    N = (64, 64)
+    in2, coupl, esc = generate_pairs(N=N, n_cases=3, snapshots=(0, 20, 80), seed=2, coarsen=4, energy=True)
+    H, W = net_image((65, 65), 4)
+    assert in2.shape == (9, H, W, 2) and coupl.shape == (9, H, W, 2) and esc.shape == (9,)
+    assert torch.all(esc > 0)
+    c = coupl.cpu().numpy()
+    assert np.all(c >= 0) and np.all(c[:, 17:, :, :] == 0)
+    net = UNet(H, W, 9, params=np.zeros(num_params(), np.float32))
+    l0 = net.train_step_energy(in2, coupl, esc, 17, 17, 0.0)
+    assert abs(l0 - 1.0) < 1e-6, l0
+    net = UNet(H, W, 9, seed=4)
+    losses = [net.train_step_energy(in2, coupl, esc, 17, 17, 1e-3) for _ in range(40)]
+    assert np.isfinite(losses).all() and losses[-1] < min(1.0, losses[0]), (losses[0], losses[-1])
+
+
+def test_trained_network_gain(cuda_device):
+    """The shipped network (trained on 512^2 solver pairs, energy loss) against
+    the same two-level flexible CG without it (all-zero network: the Jacobi
+    two-grid cycle with no coarse correction) on a held-out 256^2 density at
+    ratio 1000: far fewer iterations, same solution."""
+    import torch
+    from twophaseflow_b200 import UniformGrid
+    from twophaseflow_b200.learned import PPESolverLearned, load_params, num_params
+    from twophaseflow_b200.workloads import divergence_rhs, droplet_density
+    N = (256, 256)
+    rho = torch.from_numpy(droplet_density(N, seed=101)).to(cuda_device)
+    rhs = torch.from_numpy(divergence_rhs(N, seed=102)).to(cuda_device)
+    cfg = _Cfg(pseudo_tol=1e-8, pseudo_maxiter=5000, ppe_learned_maxiter=5000, ppe_learned_fallback=False)
+    its = {}
+    sol = {}
+    for name, params in (("trained", load_params()), ("none", np.zeros(num_params(), np.float32))):
+        s = PPESolverLearned(None, cfg, UniformGrid(N), params=params)
+        sol[name] = s.solve(rhs, rho).cpu().numpy()
+        d = s.last_diagnostics
+        assert d["ppe_learned_info"] == 0 and not d["ppe_learned_fell_back"]
+        its[name] = d["ppe_learned_iterations"]
+    assert its["trained"] * 3 <= its["none"], its
+    scale = np.abs(sol["none"]).max()
+    assert np.abs(sol["trained"] - sol["none"]).max() <= 1e-6 * scale

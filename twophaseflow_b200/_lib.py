@@ -61,6 +61,7 @@ class tpf_learned_options(C.Structure):
         ("stall_factor", C.c_double),
         ("fallback", C.c_int),
         ("use_graph", C.c_int),
+        ("window", C.c_int),
     ]
 
 
@@ -109,14 +110,18 @@ SIGNATURES = {
     "tpf_unet_backward": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tpf_unet_train_step": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_float, C.c_float,
                                       C.POINTER(C.c_double), C.c_void_p]),
+    "tpf_unet_train_step_energy": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                             C.c_int, C.c_float, C.c_float, C.POINTER(C.c_double), C.c_void_p]),
     "tpf_lppe_default_options": (None, [C.POINTER(tpf_learned_options)]),
-    "tpf_lppe_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_void_p, C.c_void_p]),
+    "tpf_lppe_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_void_p, C.c_void_p, C.c_int]),
     "tpf_lppe_destroy": (C.c_int, [C.c_void_p]),
     "tpf_lppe_prepare": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "tpf_lppe_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.POINTER(tpf_learned_options), C.c_void_p, C.POINTER(tpf_lppe_result)]),
     "tpf_lppe_precondition": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_void_p]),
-    "tpf_lppe_pair": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tpf_lppe_pair": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]),
+    "tpf_lppe_pair_energy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                       C.c_void_p]),
 }
 
 _lib = None

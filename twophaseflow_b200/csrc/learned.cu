@@ -39,20 +39,32 @@ constexpr int kRedThreads = 256;
 
 struct LGrid {
   int n0, n1, ndof, pin;
-  int H, W;            // network image (>= n0 x n1, multiple of 8)
+  int H, W;            // network image (multiple of 8): fine nodes, or aggregates when b > 1
+  int b, nc0, nc1;     // aggregate size and coarse grid (b = 1: the network runs on the fine grid)
   const double* s0;
   const double* s1;
   const double* dinvS;
   const double* dv0;
   const double* dv1;
+  const double* dcis;  // coarse D_c^-1/2 (b > 1)
+  const float* featc;  // coarse density feature (b > 1)
 };
+
+constexpr int kMaxWin = 8;   // stored directions of the truncated flexible CG
 
 struct FcgState {
   double bb, rr, rdr;
   double s, inv_s;       // network input scale
-  double delta;          // (p', S p') of the stored direction; 0 = none
-  double beta, alpha;
+  double delta[kMaxWin]; // (p_j, S p_j) of the stored directions
+  double beta[kMaxWin];  // projections of the new preconditioned residual
+  double alpha;
+  int count;             // stored directions in use (0 after a restart)
+  int head;              // ring slot of the newest direction
+  int used;              // directions projected out this iteration
+  int slot;              // ring slot receiving this iteration's direction
+  int win;               // window length m
   double tol2;
+  double sc, inv_sc;      // coarse network input scale (two-level mode)
   long long iters;
   int done;
   int restarts;
@@ -129,7 +141,7 @@ __global__ void __launch_bounds__(kRedThreads) fcg_residual_kernel(LGrid g, cons
 
 // first == 1: start of a solve (sets ||b||, the tolerance, the counters);
 // first == 0: true-residual check / restart.
-__global__ void fcg_start_kernel(const double* part, int nb, int ndof, FcgState* st, double tol, int first) {
+__global__ void fcg_start_kernel(const double* part, int nb, int ndof, FcgState* st, double tol, int first, int win) {
   double v[3];
   reduce_partials<3>(part, nb, v);
   if (threadIdx.x == 0) {
@@ -138,14 +150,16 @@ __global__ void fcg_start_kernel(const double* part, int nb, int ndof, FcgState*
       st->tol2 = tol * tol * v[2];
       st->iters = 0;
       st->restarts = 0;
+      st->win = win;
     } else {
       st->restarts += 1;
     }
     st->rr = v[0];
     st->rdr = v[1];
     set_scale(st, v[1], ndof);
-    st->delta = 0.0;
-    st->beta = 0.0;
+    st->count = 0;
+    st->head = -1;
+    st->used = 0;
     st->alpha = 0.0;
     st->done = (v[0] <= st->tol2) ? 1 : 0;
   }
@@ -196,58 +210,100 @@ __global__ void fcg_smooth_kernel(LGrid g, const double* zin, const double* r, d
   }
 }
 
-// w = S z (pin 0); partials (z, q'), (z, r), (p', r), (z, w)
+// w = S z (pin 0); partials (z, Q_j) and (P_j, r) for the stored directions,
+// (z, r), (z, w): everything the step needs in one pass (S is symmetric, so
+// (P_j, S z) = (Q_j, z) and A-orthogonality gives (p, S p) without a second pass)
+template <int M>
 __global__ void __launch_bounds__(kRedThreads) fcg_sdot_kernel(LGrid g, const double* z, const double* r,
-                                                               const double* pp, const double* qp, double* w,
+                                                               const double* P, const double* Q, double* w,
                                                                const FcgState* st, double* part) {
   if (st->done) return;
-  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  constexpr int NV = 2 * M + 2;
+  double v[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) v[k] = 0.0;
+  const int cnt = st->count;
+  const size_t nd = (size_t)g.ndof;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.ndof; i += gridDim.x * blockDim.x) {
     const int i0 = i / g.n1, i1 = i - i0 * g.n1;
     const double wi = (i == g.pin) ? 0.0 : s_apply(g, z, i, i0, i1);
     w[i] = wi;
     const double zi = z[i], ri = r[i];
-    v[0] += zi * qp[i];
-    v[1] += zi * ri;
-    v[2] += pp[i] * ri;
-    v[3] += zi * wi;
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      if (j < cnt) {
+        v[j] += zi * Q[j * nd + i];
+        v[M + j] += P[j * nd + i] * ri;
+      }
+    }
+    v[2 * M] += zi * ri;
+    v[2 * M + 1] += zi * wi;
   }
-  block_partials<4>(v, part);
+  block_partials<NV>(v, part);
 }
 
-// beta, alpha of the flexible CG step
+// beta_j, alpha and the ring bookkeeping of the truncated flexible CG step
+template <int M>
 __global__ void fcg_coef_kernel(const double* part, int nb, FcgState* st) {
   if (st->done) return;
-  double v[4];
-  reduce_partials<4>(part, nb, v);
+  constexpr int NV = 2 * M + 2;
+  double v[NV];
+  reduce_partials<NV>(part, nb, v);
   if (threadIdx.x == 0) {
-    const double zq = v[0], zr = v[1], pr_old = v[2], zw = v[3];
-    double beta = (st->delta > 0.0) ? zq / st->delta : 0.0;
-    double pq = zw - 2.0 * beta * zq + beta * beta * st->delta;
-    double pr = zr - beta * pr_old;
-    if (!(pq > 1e-14 * zw) || !(pq > 0.0)) {  // lost A-orthogonality: restart the direction
-      beta = 0.0;
+    const int cnt = st->count;
+    const double zr = v[2 * M], zw = v[2 * M + 1];
+    double pq = zw, pr = zr;
+    for (int j = 0; j < M; ++j) {
+      const double b = (j < cnt && st->delta[j] > 0.0) ? v[j] / st->delta[j] : 0.0;
+      st->beta[j] = b;
+      pq -= b * v[j];
+      pr -= b * v[M + j];
+    }
+    int used = cnt;
+    if (!(pq > 1e-12 * zw) || !(pq > 0.0)) {   // lost A-orthogonality: restart the window
+      used = 0;
       pq = zw;
       pr = zr;
+      for (int j = 0; j < M; ++j) st->beta[j] = 0.0;
     }
-    st->beta = beta;
+    const int win = st->win < 1 ? 1 : (st->win > M ? M : st->win);
+    // new direction: slot 0 after a restart, else the next ring slot (a full
+    // window overwrites its oldest direction)
+    const int slot = (used == 0) ? 0 : (st->head + 1) % win;
+    st->used = used;
+    st->slot = slot;
     st->alpha = (pq > 0.0) ? pr / pq : 0.0;
-    st->delta = pq;
+    st->delta[slot] = pq;
+    st->head = slot;
+    st->count = (used + 1 < win) ? used + 1 : win;
   }
 }
 
-// p' <- z - beta p', q' <- w - beta q', x += alpha p', r -= alpha q'; partials r.r, r.r dinvS
+// p = z - sum_j beta_j P_j, q = w - sum_j beta_j Q_j -> ring slot; x += alpha p,
+// r -= alpha q; partials r.r, r.r dinvS
+template <int M>
 __global__ void __launch_bounds__(kRedThreads) fcg_update_kernel(LGrid g, const double* z, const double* w,
-                                                                 double* pp, double* qp, double* x, double* r,
+                                                                 double* P, double* Q, double* x, double* r,
                                                                  const FcgState* st, double* part) {
   if (st->done) return;
-  const double beta = st->beta, alpha = st->alpha;
+  const double alpha = st->alpha;
+  const int used = st->used, slot = st->slot;
+  double beta[M];
+#pragma unroll
+  for (int j = 0; j < M; ++j) beta[j] = st->beta[j];
+  const size_t nd = (size_t)g.ndof;
   double v[2] = {0.0, 0.0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.ndof; i += gridDim.x * blockDim.x) {
-    const double pi = z[i] - beta * pp[i];
-    const double qi = w[i] - beta * qp[i];
-    pp[i] = pi;
-    qp[i] = qi;
+    double pi = z[i], qi = w[i];
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      if (j < used) {
+        pi -= beta[j] * P[j * nd + i];
+        qi -= beta[j] * Q[j * nd + i];
+      }
+    }
+    P[slot * nd + i] = pi;
+    Q[slot * nd + i] = qi;
     x[i] += alpha * pi;
     const double ri = r[i] - alpha * qi;
     r[i] = ri;
@@ -355,6 +411,266 @@ __global__ void rscale_finish_kernel(const double* part, int nb, int ndof, FcgSt
   }
 }
 
+// ---- two-level mode: the network solves the aggregated coarse problem ---------------
+//
+// Aggregates are b x b blocks of fine nodes; R sums a block, P copies the coarse
+// value back to its nodes.  The coarse operator A_c = R S P is a 5-point stencil
+// whose couplings are the fine couplings crossing aggregate boundaries; only its
+// diagonal D_c is formed (for the Jacobi-type scaling of the network input).
+// One preconditioner application is a two-grid V(1, smooth) cycle:
+//   z1 = w D^-1 r,  r1 = r - S z1,  z2 = z1 + P (s_c D_c^-1/2 UNet(D_c^-1/2 R r1 / s_c, c~_c)),
+//   z  = z2 + w D^-1 (r - S z2)  (smooth times)
+
+__device__ __forceinline__ int agg_of(const LGrid& g, int i0, int i1) { return (i0 / g.b) * g.nc1 + i1 / g.b; }
+
+__global__ void coarse_diag_kernel(LGrid g, double* dc) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.ndof; i += gridDim.x * blockDim.x) {
+    const int i0 = i / g.n1, i1 = i - i0 * g.n1;
+    const int I = agg_of(g, i0, i1);
+    if (i0 + 1 < g.n0) {
+      const int J = agg_of(g, i0 + 1, i1);
+      if (J != I) {
+        const double v = g.s0[i];
+        atomicAdd(dc + I, v);
+        atomicAdd(dc + J, v);
+      }
+    }
+    if (i1 + 1 < g.n1) {
+      const int J = agg_of(g, i0, i1 + 1);
+      if (J != I) {
+        const double v = g.s1[i];
+        atomicAdd(dc + I, v);
+        atomicAdd(dc + J, v);
+      }
+    }
+  }
+}
+
+// D_c^-1/2 and the aggregate-mean density feature
+__global__ void coarse_setup_kernel(LGrid g, const double* dc, const float* feat, double* dcis, float* featc) {
+  const int nc = g.nc0 * g.nc1;
+  for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += gridDim.x * blockDim.x) {
+    dcis[I] = dc[I] > 0.0 ? 1.0 / sqrt(dc[I]) : 0.0;
+    const int I0 = I / g.nc1, I1 = I - I0 * g.nc1;
+    float acc = 0.f;
+    int cnt = 0;
+    for (int a0 = I0 * g.b; a0 < min(g.n0, (I0 + 1) * g.b); ++a0)
+      for (int a1 = I1 * g.b; a1 < min(g.n1, (I1 + 1) * g.b); ++a1) {
+        acc += feat[a0 * g.n1 + a1];
+        ++cnt;
+      }
+    featc[I] = cnt ? acc / cnt : 0.f;
+  }
+}
+
+// r1 = r - S (w D^-1 r), pin 0 (the pre-smoothing sweep from a zero start)
+__global__ void vc_pre_kernel(LGrid g, const double* r, double omega, const FcgState* st, double* r1) {
+  if (st && st->done) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.ndof; i += gridDim.x * blockDim.x) {
+    const int i0 = i / g.n1, i1 = i - i0 * g.n1;
+    auto zf = [&](int j) -> double { return (j == g.pin) ? 0.0 : omega * g.dinvS[j] * r[j]; };
+    double v = 0.0;
+    if (i != g.pin) {
+      const double sm0 = (i0 > 0) ? g.s0[i - g.n1] : 0.0, sp0 = g.s0[i];
+      const double sm1 = (i1 > 0) ? g.s1[i - 1] : 0.0, sp1 = g.s1[i];
+      double off = 0.0;
+      if (i0 > 0) off += sm0 * zf(i - g.n1);
+      if (i0 < g.n0 - 1) off += sp0 * zf(i + g.n1);
+      if (i1 > 0) off += sm1 * zf(i - 1);
+      if (i1 < g.n1 - 1) off += sp1 * zf(i + 1);
+      v = r[i] - ((sm0 + sp0 + sm1 + sp1) * zf(i) - off);
+    }
+    r1[i] = v;
+  }
+}
+
+// rc = R r1 (block sums); partials of rc^2 / D_c
+__global__ void __launch_bounds__(kRedThreads) restrict_kernel(LGrid g, const double* r1, double* rc,
+                                                               const FcgState* st, double* part) {
+  double v[1] = {0.0};
+  if (!(st && st->done)) {
+    const int nc = g.nc0 * g.nc1;
+    for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += gridDim.x * blockDim.x) {
+      const int I0 = I / g.nc1, I1 = I - I0 * g.nc1;
+      double acc = 0.0;
+      for (int a0 = I0 * g.b; a0 < min(g.n0, (I0 + 1) * g.b); ++a0)
+        for (int a1 = I1 * g.b; a1 < min(g.n1, (I1 + 1) * g.b); ++a1) acc += r1[a0 * g.n1 + a1];
+      rc[I] = acc;
+      const double q = acc * g.dcis[I];
+      v[0] += q * q;
+    }
+  }
+  block_partials<1>(v, part);
+}
+
+__global__ void coarse_scale_kernel(const double* part, int nb, int nc, FcgState* st) {
+  if (st->done) return;
+  double v[1];
+  reduce_partials<1>(part, nb, v);
+  if (threadIdx.x == 0) {
+    const double sc = sqrt(v[0] / nc);
+    st->sc = sc;
+    st->inv_sc = sc > 0.0 ? 1.0 / sc : 0.0;
+  }
+}
+
+// network input on the coarse image: (D_c^-1/2 rc / s_c, c~_c)
+__global__ void pack_coarse_kernel(LGrid g, const double* rc, const FcgState* st, bf16* xin) {
+  if (st->done) return;
+  const int Wp = g.W + 2;
+  const long long P = (long long)(g.H + 2) * Wp;
+  const double inv = st->inv_sc;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < P; q += (long long)gridDim.x * blockDim.x) {
+    const int yy = (int)(q / Wp), xx = (int)(q - (long long)yy * Wp);
+    const int y = yy - 1, x = xx - 1;
+    float c0 = 0.f, c1 = 0.f;
+    if (y >= 0 && y < g.nc0 && x >= 0 && x < g.nc1) {
+      const int I = y * g.nc1 + x;
+      c0 = (float)(rc[I] * g.dcis[I] * inv);
+      c1 = g.featc[I];
+    }
+    uint4 v0, v1 = make_uint4(0, 0, 0, 0);
+    __nv_bfloat162 h = __floats2bfloat162_rn(c0, c1);
+    v0.x = *reinterpret_cast<uint32_t*>(&h);
+    v0.y = v0.z = v0.w = 0;
+    uint4* o = reinterpret_cast<uint4*>(xin + q * 16);
+    o[0] = v0;
+    o[1] = v1;
+  }
+}
+
+// z2 = w D^-1 r + P (s_c D_c^-1/2 y), pin 0
+__global__ void prolong_kernel(LGrid g, const float* y, const double* r, double omega, const FcgState* st,
+                               double* z2) {
+  if (st->done) return;
+  const double sc = st->sc;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.ndof; i += gridDim.x * blockDim.x) {
+    const int i0 = i / g.n1, i1 = i - i0 * g.n1;
+    const int I0 = i0 / g.b, I1 = i1 / g.b, I = I0 * g.nc1 + I1;
+    z2[i] = (i == g.pin) ? 0.0 : omega * g.dinvS[i] * r[i] + sc * g.dcis[I] * (double)y[(size_t)I0 * g.W + I1];
+  }
+}
+
+// prolongation fused with the first post-smoothing sweep:
+// z2 = w D^-1 r + P (s_c D_c^-1/2 y) evaluated on the fly at the node and its
+// neighbours, z = z2 + w D^-1 (r - S z2), pin 0
+__global__ void prolong_smooth_kernel(LGrid g, const float* y, const double* r, double omega, const FcgState* st,
+                                      double* z) {
+  if (st->done) return;
+  const double sc = st->sc;
+  auto z2 = [&](int j, int j0, int j1) -> double {
+    if (j == g.pin) return 0.0;
+    const int J0 = j0 / g.b, J1 = j1 / g.b;
+    return omega * g.dinvS[j] * r[j] + sc * g.dcis[J0 * g.nc1 + J1] * (double)y[(size_t)J0 * g.W + J1];
+  };
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.ndof; i += gridDim.x * blockDim.x) {
+    const int i0 = i / g.n1, i1 = i - i0 * g.n1;
+    if (i == g.pin) {
+      z[i] = 0.0;
+      continue;
+    }
+    const double sm0 = (i0 > 0) ? g.s0[i - g.n1] : 0.0, sp0 = g.s0[i];
+    const double sm1 = (i1 > 0) ? g.s1[i - 1] : 0.0, sp1 = g.s1[i];
+    const double zc = z2(i, i0, i1);
+    double off = 0.0;
+    if (i0 > 0) off += sm0 * z2(i - g.n1, i0 - 1, i1);
+    if (i0 < g.n0 - 1) off += sp0 * z2(i + g.n1, i0 + 1, i1);
+    if (i1 > 0) off += sm1 * z2(i - 1, i0, i1 - 1);
+    if (i1 < g.n1 - 1) off += sp1 * z2(i + 1, i0, i1 + 1);
+    const double sz = (sm0 + sp0 + sm1 + sp1) * zc - off;
+    z[i] = zc + omega * g.dinvS[i] * (r[i] - sz);
+  }
+}
+
+// training pair of the coarse problem: e1 = e - w D^-1 r (error after the
+// pre-smoothing sweep), target = D_c^1/2 mean_I(e1) / s_c on the coarse image
+__global__ void pair_coarse_write_kernel(LGrid g, const double* e, const double* r, const double* rc, double omega,
+                                         const double* part, int nb, float* in2, float* target) {
+  __shared__ double s_inv;
+  if (threadIdx.x == 0) {
+    double a = 0.0;
+    for (int i = 0; i < nb; ++i) a += part[i];
+    const double sc = sqrt(a / (g.nc0 * g.nc1));
+    s_inv = (sc > 0.0) ? 1.0 / sc : 0.0;
+  }
+  __syncthreads();
+  const double inv = s_inv;
+  const long long n = (long long)g.H * g.W;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(q / g.W), x = (int)(q - (long long)y * g.W);
+    float a0 = 0.f, a1 = 0.f, t = 0.f;
+    if (y < g.nc0 && x < g.nc1) {
+      const int I = y * g.nc1 + x;
+      double acc = 0.0;
+      int cnt = 0;
+      for (int i0 = y * g.b; i0 < min(g.n0, (y + 1) * g.b); ++i0)
+        for (int i1 = x * g.b; i1 < min(g.n1, (x + 1) * g.b); ++i1) {
+          const int i = i0 * g.n1 + i1;
+          acc += (i == g.pin) ? 0.0 : e[i] - omega * g.dinvS[i] * r[i];
+          ++cnt;
+        }
+      const double d = g.dcis[I];
+      a0 = (float)(rc[I] * d * inv);
+      a1 = g.featc[I];
+      t = (d > 0.0) ? (float)((acc / cnt) / d * inv) : 0.f;
+    }
+    in2[2 * q] = a0;
+    in2[2 * q + 1] = a1;
+    target[q] = t;
+  }
+}
+
+// energy-loss data of a coarse training pair: scaled Galerkin couplings of the
+// coarse operator on the network image (coupl[q][0]: to the next row,
+// coupl[q][1]: to the next column; A~ = D_c^-1/2 A_c D_c^-1/2 = I - couplings)
+// and E~ = (e1 . S e1) / s_c^2 = (e1 . r1) / s_c^2
+__global__ void coarse_coupl_kernel(LGrid g, double* c0, double* c1) {
+  // c0[I]: sum of fine couplings between aggregate I and the one below; c1: to the right
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.ndof; i += gridDim.x * blockDim.x) {
+    const int i0 = i / g.n1, i1 = i - i0 * g.n1;
+    const int I = agg_of(g, i0, i1);
+    if (i0 + 1 < g.n0 && agg_of(g, i0 + 1, i1) != I) atomicAdd(c0 + I, g.s0[i]);
+    if (i1 + 1 < g.n1 && agg_of(g, i0, i1 + 1) != I) atomicAdd(c1 + I, g.s1[i]);
+  }
+}
+
+__global__ void coarse_coupl_write_kernel(LGrid g, const double* c0, const double* c1, float* coupl) {
+  const long long n = (long long)g.H * g.W;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(q / g.W), x = (int)(q - (long long)y * g.W);
+    float a = 0.f, b = 0.f;
+    if (y < g.nc0 && x < g.nc1) {
+      const int I = y * g.nc1 + x;
+      if (y + 1 < g.nc0) a = (float)(c0[I] * g.dcis[I] * g.dcis[I + g.nc1]);
+      if (x + 1 < g.nc1) b = (float)(c1[I] * g.dcis[I] * g.dcis[I + 1]);
+    }
+    coupl[2 * q] = a;
+    coupl[2 * q + 1] = b;
+  }
+}
+
+// partial sums of e1 . r1 with e1 = e - w D^-1 r (pin 0)
+__global__ void __launch_bounds__(kRedThreads) energy_partials_kernel(LGrid g, const double* e, const double* r,
+                                                                      const double* r1, double omega, double* part) {
+  double v[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.ndof; i += gridDim.x * blockDim.x) {
+    if (i == g.pin) continue;
+    v[0] += (e[i] - omega * g.dinvS[i] * r[i]) * r1[i];
+  }
+  block_partials<1>(v, part);
+}
+
+// E~ = (e1 . r1) / s_c^2, s_c from the restriction partials
+__global__ void energy_scale_kernel(LGrid g, const double* part_e, const double* part_r, int nb, double* escale) {
+  double v[1], w[1];
+  reduce_partials<1>(part_e, nb, v);
+  reduce_partials<1>(part_r, nb, w);
+  if (threadIdx.x == 0) {
+    const double sc2 = w[0] / (g.nc0 * g.nc1);
+    escale[0] = (sc2 > 0.0) ? v[0] / sc2 : 1.0;
+  }
+}
+
 inline int ew_blocks(int n) { return std::max(1, std::min((n + 255) / 256, 148 * 8)); }
 
 }  // namespace
@@ -365,15 +681,22 @@ struct tpf_lppe {
   tpf::PpeView v{};
   LGrid g{};
   double *b = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *z2 = nullptr, *w = nullptr, *pp = nullptr,
-         *qp = nullptr, *part = nullptr;
+         *qp = nullptr, *part = nullptr;   // pp / qp: kMaxWin stored directions P_j, S P_j
   float* feat = nullptr;
   unsigned long long* rmax = nullptr;
+  // two-level mode
+  double *r1 = nullptr, *rc = nullptr, *dc = nullptr, *dcis = nullptr, *cc0 = nullptr, *cc1 = nullptr,
+         *part2 = nullptr;
+  float* featc = nullptr;
+  double graph_pre_omega = 0.0;
   FcgState* st = nullptr;
   FcgState* st_host = nullptr;   // pinned
   cudaStream_t cap = nullptr;
   cudaGraphExec_t exec = nullptr;
   int graph_smooth = -1;
   double graph_omega = 0.0;
+  int win = 1;            // window of the current solve
+  int graph_win = -1;
   bool have_feat = false;
   std::vector<void*> allocs;
 };
@@ -406,6 +729,15 @@ int features(tpf_lppe* lp, const double* rho, cudaStream_t s) {
   TPF_CUDA_TRY(cudaMemsetAsync(lp->rmax, 0, sizeof(unsigned long long), s));
   rho_max_kernel<<<ew_blocks(lp->g.ndof), 256, 0, s>>>(lp->g.ndof, rho, lp->rmax);
   feature_kernel<<<ew_blocks(lp->g.ndof), 256, 0, s>>>(lp->g.ndof, rho, lp->rmax, lp->feat);
+  if (lp->g.b > 1) {
+    const int nc = lp->g.nc0 * lp->g.nc1;
+    TPF_CUDA_TRY(cudaMemsetAsync(lp->dc, 0, sizeof(double) * nc, s));
+    TPF_CUDA_TRY(cudaMemsetAsync(lp->cc0, 0, sizeof(double) * nc, s));
+    TPF_CUDA_TRY(cudaMemsetAsync(lp->cc1, 0, sizeof(double) * nc, s));
+    coarse_diag_kernel<<<ew_blocks(lp->g.ndof), 256, 0, s>>>(lp->g, lp->dc);
+    coarse_coupl_kernel<<<ew_blocks(lp->g.ndof), 256, 0, s>>>(lp->g, lp->cc0, lp->cc1);
+    coarse_setup_kernel<<<ew_blocks(nc), 256, 0, s>>>(lp->g, lp->dc, lp->feat, lp->dcis, lp->featc);
+  }
   TPF_CUDA_TRY(cudaGetLastError());
   lp->have_feat = true;
   return TPF_OK;
@@ -414,6 +746,31 @@ int features(tpf_lppe* lp, const double* rho, cudaStream_t s) {
 // z = B(r): network (+ smoothing); result in lp->z (smooth even) or lp->z2
 int enqueue_precond(tpf_lppe* lp, int smooth, double omega, cudaStream_t s, double** zout) {
   const LGrid& g = lp->g;
+  if (g.b > 1) {
+    const int nc = g.nc0 * g.nc1;
+    vc_pre_kernel<<<ew_blocks(g.ndof), 256, 0, s>>>(g, lp->r, omega, lp->st, lp->r1);
+    restrict_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(g, lp->r1, lp->rc, lp->st, lp->part);
+    coarse_scale_kernel<<<1, 256, 0, s>>>(lp->part, kRedBlocks, nc, lp->st);
+    pack_coarse_kernel<<<ew_blocks((g.H + 2) * (g.W + 2)), 256, 0, s>>>(g, lp->rc, lp->st, tpf::unet_input(lp->net));
+    TPF_CUDA_TRY(cudaGetLastError());
+    int st = tpf::unet_forward_packed(lp->net, 1, s);
+    if (st) return st;
+    double* cur = lp->z;
+    double* other = lp->z2;
+    if (smooth > 0) {
+      prolong_smooth_kernel<<<ew_blocks(g.ndof), 256, 0, s>>>(g, tpf::unet_output(lp->net), lp->r, omega, lp->st,
+                                                               lp->z);
+    } else {
+      prolong_kernel<<<ew_blocks(g.ndof), 256, 0, s>>>(g, tpf::unet_output(lp->net), lp->r, omega, lp->st, lp->z);
+    }
+    for (int k = 1; k < smooth; ++k) {
+      fcg_smooth_kernel<<<ew_blocks(g.ndof), 256, 0, s>>>(g, cur, lp->r, omega, lp->st, other);
+      std::swap(cur, other);
+    }
+    TPF_CUDA_TRY(cudaGetLastError());
+    *zout = cur;
+    return TPF_OK;
+  }
   fcg_pack_kernel<<<ew_blocks((g.H + 2) * (g.W + 2)), 256, 0, s>>>(g, lp->r, lp->feat, lp->st,
                                                                     tpf::unet_input(lp->net));
   TPF_CUDA_TRY(cudaGetLastError());
@@ -436,17 +793,24 @@ int enqueue_iteration(tpf_lppe* lp, int smooth, double omega, cudaStream_t s) {
   int st = enqueue_precond(lp, smooth, omega, s, &z);
   if (st) return st;
   const LGrid& g = lp->g;
-  fcg_sdot_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(g, z, lp->r, lp->pp, lp->qp, lp->w, lp->st, lp->part);
-  fcg_coef_kernel<<<1, 256, 0, s>>>(lp->part, kRedBlocks, lp->st);
-  fcg_update_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(g, z, lp->w, lp->pp, lp->qp, lp->x, lp->r, lp->st,
+  if (lp->win <= 1) {
+    fcg_sdot_kernel<1><<<kRedBlocks, kRedThreads, 0, s>>>(g, z, lp->r, lp->pp, lp->qp, lp->w, lp->st, lp->part);
+    fcg_coef_kernel<1><<<1, 256, 0, s>>>(lp->part, kRedBlocks, lp->st);
+    fcg_update_kernel<1><<<kRedBlocks, kRedThreads, 0, s>>>(g, z, lp->w, lp->pp, lp->qp, lp->x, lp->r, lp->st,
+                                                            lp->part);
+  } else {
+    fcg_sdot_kernel<kMaxWin><<<kRedBlocks, kRedThreads, 0, s>>>(g, z, lp->r, lp->pp, lp->qp, lp->w, lp->st, lp->part);
+    fcg_coef_kernel<kMaxWin><<<1, 256, 0, s>>>(lp->part, kRedBlocks, lp->st);
+    fcg_update_kernel<kMaxWin><<<kRedBlocks, kRedThreads, 0, s>>>(g, z, lp->w, lp->pp, lp->qp, lp->x, lp->r, lp->st,
                                                        lp->part);
+  }
   fcg_finish_iter_kernel<<<1, 256, 0, s>>>(lp->part, kRedBlocks, g.ndof, lp->st);
   TPF_CUDA_TRY(cudaGetLastError());
   return TPF_OK;
 }
 
 int build_graph(tpf_lppe* lp, int smooth, double omega) {
-  if (lp->exec && lp->graph_smooth == smooth && lp->graph_omega == omega) return TPF_OK;
+  if (lp->exec && lp->graph_smooth == smooth && lp->graph_omega == omega && lp->graph_win == lp->win) return TPF_OK;
   if (lp->exec) {
     cudaGraphExecDestroy(lp->exec);
     lp->exec = nullptr;
@@ -472,6 +836,7 @@ int build_graph(tpf_lppe* lp, int smooth, double omega) {
   }
   lp->graph_smooth = smooth;
   lp->graph_omega = omega;
+  lp->graph_win = lp->win;
   return TPF_OK;
 }
 
@@ -481,9 +846,9 @@ int read_state(tpf_lppe* lp, cudaStream_t s) {
   return tpf::unet_check(lp->net, s);
 }
 
-int true_residual(tpf_lppe* lp, cudaStream_t s, double tol, int first) {
+int true_residual(tpf_lppe* lp, cudaStream_t s, double tol, int first, int win) {
   fcg_residual_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(lp->g, lp->b, lp->x, lp->r, lp->part);
-  fcg_start_kernel<<<1, 256, 0, s>>>(lp->part, kRedBlocks, lp->g.ndof, lp->st, tol, first);
+  fcg_start_kernel<<<1, 256, 0, s>>>(lp->part, kRedBlocks, lp->g.ndof, lp->st, tol, first, win);
   TPF_CUDA_TRY(cudaGetLastError());
   return TPF_OK;
 }
@@ -503,10 +868,12 @@ void tpf_lppe_default_options(tpf_learned_options* o) {
   o->stall_factor = 0.5;
   o->fallback = 1;
   o->use_graph = 1;
+  o->window = 1;
 }
 
-int tpf_lppe_create(tpf_lppe** out, tpf_ppe* ppe, tpf_unet* net) {
+int tpf_lppe_create(tpf_lppe** out, tpf_ppe* ppe, tpf_unet* net, int coarsen) {
   TPF_CHECK_ARG(out && ppe && net, "NULL argument");
+  TPF_CHECK_ARG(coarsen == 1 || coarsen == 2 || coarsen == 4 || coarsen == 8, "coarsen must be 1, 2, 4 or 8");
   auto* lp = new tpf_lppe();
   lp->ppe = ppe;
   lp->net = net;
@@ -525,11 +892,16 @@ int tpf_lppe_create(tpf_lppe** out, tpf_ppe* ppe, tpf_unet* net) {
   }
   int H = 0, W = 0, mb = 0;
   tpf::unet_dims(net, &H, &W, &mb);
-  const int Hn = (lp->v.n0 + 7) / 8 * 8, Wn = (lp->v.n1 + 7) / 8 * 8;
+  const int nc0 = (lp->v.n0 + coarsen - 1) / coarsen, nc1 = (lp->v.n1 + coarsen - 1) / coarsen;
+  const int Hn = (nc0 + 7) / 8 * 8, Wn = (nc1 + 7) / 8 * 8;
   if (H != Hn || W != Wn) {
-    tpf::set_error("U-Net image %dx%d does not match the grid: need %dx%d (nodes rounded up to 8)", H, W, Hn, Wn);
+    tpf::set_error("U-Net image %dx%d does not match the grid: need %dx%d (%s rounded up to 8)", H, W, Hn, Wn,
+                   coarsen > 1 ? "aggregates" : "nodes");
     return fail(TPF_EINVAL);
   }
+  lp->g.b = coarsen;
+  lp->g.nc0 = nc0;
+  lp->g.nc1 = nc1;
   lp->g.n0 = lp->v.n0;
   lp->g.n1 = lp->v.n1;
   lp->g.ndof = lp->v.ndof;
@@ -539,9 +911,19 @@ int tpf_lppe_create(tpf_lppe** out, tpf_ppe* ppe, tpf_unet* net) {
   const size_t n = lp->v.ndof;
   if ((st = lalloc(lp, &lp->b, n)) || (st = lalloc(lp, &lp->x, n)) || (st = lalloc(lp, &lp->r, n)) ||
       (st = lalloc(lp, &lp->z, n)) || (st = lalloc(lp, &lp->z2, n)) || (st = lalloc(lp, &lp->w, n)) ||
-      (st = lalloc(lp, &lp->pp, n)) || (st = lalloc(lp, &lp->qp, n)) || (st = lalloc(lp, &lp->part, 8 * kRedBlocks)) ||
+      (st = lalloc(lp, &lp->pp, kMaxWin * n)) || (st = lalloc(lp, &lp->qp, kMaxWin * n)) ||
+      (st = lalloc(lp, &lp->part, (2 * kMaxWin + 4) * kRedBlocks)) ||
       (st = lalloc(lp, &lp->feat, n)) || (st = lalloc(lp, &lp->rmax, 1)) || (st = lalloc(lp, &lp->st, 1)))
     return fail(st);
+  if (coarsen > 1) {
+    const size_t nc = (size_t)nc0 * nc1;
+    if ((st = lalloc(lp, &lp->r1, n)) || (st = lalloc(lp, &lp->rc, nc)) || (st = lalloc(lp, &lp->dc, nc)) ||
+        (st = lalloc(lp, &lp->dcis, nc)) || (st = lalloc(lp, &lp->featc, nc)) || (st = lalloc(lp, &lp->cc0, nc)) ||
+        (st = lalloc(lp, &lp->cc1, nc)) || (st = lalloc(lp, &lp->part2, kRedBlocks)))
+      return fail(st);
+    lp->g.dcis = lp->dcis;
+    lp->g.featc = lp->featc;
+  }
   if (cudaMallocHost(reinterpret_cast<void**>(&lp->st_host), sizeof(FcgState)) != cudaSuccess) {
     cudaGetLastError();
     lp->st_host = nullptr;
@@ -578,13 +960,42 @@ int tpf_lppe_prepare(tpf_lppe* lp, const double* rho, void* stream) {
   return features(lp, rho, s);
 }
 
-int tpf_lppe_pair(tpf_lppe* lp, const double* e, float* in2, float* target, void* stream) {
+int tpf_lppe_pair(tpf_lppe* lp, const double* e, float* in2, float* target, double omega, void* stream) {
   TPF_CHECK_ARG(lp && e && in2 && target, "NULL argument");
   TPF_CHECK_ARG(lp->have_feat, "call tpf_lppe_prepare first");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (lp->g.b > 1) {
+    pair_residual_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(lp->g, e, lp->r, lp->part);
+    vc_pre_kernel<<<ew_blocks(lp->g.ndof), 256, 0, s>>>(lp->g, lp->r, omega, nullptr, lp->r1);
+    restrict_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(lp->g, lp->r1, lp->rc, nullptr, lp->part);
+    pair_coarse_write_kernel<<<ew_blocks(lp->g.H * lp->g.W), 256, 0, s>>>(lp->g, e, lp->r, lp->rc, omega, lp->part,
+                                                                         kRedBlocks, in2, target);
+    TPF_CUDA_TRY(cudaGetLastError());
+    return TPF_OK;
+  }
   pair_residual_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(lp->g, e, lp->r, lp->part);
   pair_write_kernel<<<ew_blocks(lp->g.H * lp->g.W), 256, 0, s>>>(lp->g, e, lp->r, lp->feat, lp->part, kRedBlocks,
                                                                  in2, target);
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
+int tpf_lppe_pair_energy(tpf_lppe* lp, const double* e, float* in2, float* coupl, double* escale, double omega,
+                         void* stream) {
+  TPF_CHECK_ARG(lp && e && in2 && coupl && escale, "NULL argument");
+  TPF_CHECK_ARG(lp->have_feat, "call tpf_lppe_prepare first");
+  TPF_CHECK_ARG(lp->g.b > 1, "energy pairs need the two-level mode (coarsen > 1)");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const LGrid& g = lp->g;
+  pair_residual_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(g, e, lp->r, lp->part);
+  vc_pre_kernel<<<ew_blocks(g.ndof), 256, 0, s>>>(g, lp->r, omega, nullptr, lp->r1);
+  restrict_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(g, lp->r1, lp->rc, nullptr, lp->part);
+  // in2 (channel 0 = scaled restricted residual, channel 1 = feature); the target is unused
+  pair_coarse_write_kernel<<<ew_blocks(g.H * g.W), 256, 0, s>>>(g, e, lp->r, lp->rc, omega, lp->part, kRedBlocks,
+                                                                in2, reinterpret_cast<float*>(lp->z2));
+  energy_partials_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(g, e, lp->r, lp->r1, omega, lp->part2);
+  energy_scale_kernel<<<1, 256, 0, s>>>(g, lp->part2, lp->part, kRedBlocks, escale);
+  coarse_coupl_write_kernel<<<ew_blocks(g.H * g.W), 256, 0, s>>>(g, lp->cc0, lp->cc1, coupl);
   TPF_CUDA_TRY(cudaGetLastError());
   return TPF_OK;
 }
@@ -615,6 +1026,7 @@ int tpf_lppe_solve(tpf_lppe* lp, const double* rhs, const double* rho, double* p
   TPF_CHECK_ARG(o.maxiter >= 0, "maxiter must be >= 0");
   TPF_CHECK_ARG(o.smooth >= 0 && o.smooth <= 8, "smooth must be in [0, 8]");
   TPF_CHECK_ARG(o.check_every >= 1 && o.check_every <= 1024, "check_every must be in [1, 1024]");
+  TPF_CHECK_ARG(o.window >= 1 && o.window <= kMaxWin, "window must be in [1, %d]", kMaxWin);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int st;
   if (rho && (st = tpf_lppe_prepare(lp, rho, stream))) return st;
@@ -624,11 +1036,11 @@ int tpf_lppe_solve(tpf_lppe* lp, const double* rhs, const double* rho, double* p
   tpf_lppe_result* res = result ? result : &local;
   *res = tpf_lppe_result{};
   if ((st = tpf::unet_prepare_weights(lp->net, s))) return st;
+  lp->win = o.window;
   const LGrid& g = lp->g;
   fcg_init_kernel<<<ew_blocks(g.ndof), 256, 0, s>>>(g, rhs, p_init, lp->b, lp->x);
-  TPF_CUDA_TRY(cudaMemsetAsync(lp->pp, 0, sizeof(double) * g.ndof, s));
-  TPF_CUDA_TRY(cudaMemsetAsync(lp->qp, 0, sizeof(double) * g.ndof, s));
-  if ((st = true_residual(lp, s, o.tol, 1))) return st;
+
+  if ((st = true_residual(lp, s, o.tol, 1, o.window))) return st;
   if ((st = read_state(lp, s))) return st;
   bool converged = lp->st_host->done != 0;
   bool graph_ready = false;
@@ -655,7 +1067,7 @@ int tpf_lppe_solve(tpf_lppe* lp, const double* rhs, const double* rho, double* p
     }
     if (lp->st_host->done) {
       // judge convergence on the true residual; restart the recurrence from it otherwise
-      if ((st = true_residual(lp, s, o.tol, 0))) return st;
+      if ((st = true_residual(lp, s, o.tol, 0, o.window))) return st;
       if ((st = read_state(lp, s))) return st;
       converged = lp->st_host->done != 0;
       rr_ref = lp->st_host->rr;

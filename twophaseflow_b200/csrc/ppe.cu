@@ -792,6 +792,7 @@ struct tpf_ppe {
   double* tden[3] = {nullptr, nullptr, nullptr};
   double* tcp[3] = {nullptr, nullptr, nullptr};
   bool prepared = false;
+  bool line_ready = false;   // line-preconditioner factors built by the last prepare
   // Krylov workspace
   double* x = nullptr; double* r = nullptr; double* z = nullptr; double* p0 = nullptr; double* p1 = nullptr;
   double* q = nullptr; double* b = nullptr; double* t1 = nullptr; double* t2 = nullptr;
@@ -1239,8 +1240,9 @@ int tpf_ppe_set_options(tpf_ppe* h, const tpf_ppe_options* o) {
   TPF_CHECK_ARG(h && o, "NULL argument");
   int st = validate_options(o);
   if (st) return st;
-  // prepare builds every preconditioner's state; only the line shift depends on an option
-  bool line_changed = (o->c_tau != h->o.c_tau);
+  // the line preconditioner's state depends on c_tau and is only built when it is selected
+  const bool to_line = (o->precond == TPF_PRECOND_LINE || o->precond == TPF_PRECOND_LINE_PCR);
+  bool line_changed = to_line && (!h->line_ready || o->c_tau != h->o.c_tau);
   bool grow = o->restart > h->o.restart;
   h->o = *o;
   if (grow) {
@@ -1272,14 +1274,19 @@ int tpf_ppe_prepare(tpf_ppe* h, const double* rho, void* stream) {
   a.dinvL = h->dinvL;
   a.shift_scale = 2.0 / (h->o.c_tau * h->h_min * h->h_min);
   a.ndim = h->ndim;
-  a.want_line = 1;
+  // the shifted line systems and their Thomas factors only for the line preconditioner
+  const bool line = (h->o.precond == TPF_PRECOND_LINE || h->o.precond == TPF_PRECOND_LINE_PCR);
+  a.want_line = line ? 1 : 0;
   prep_faces_kernel<<<h->ew_blocks, 256, 0, s>>>(a);
   TPF_CUDA_TRY(cudaGetLastError());
-  for (int ax = 0; ax < h->ndim; ++ax) {
-    LineArgs L = line_args(h->g, ax);
-    thomas_factor_kernel<<<(L.lines + 127) / 128, 128, 0, s>>>(L, h->tlo[ax], h->tden[ax], h->tcp[ax]);
+  if (line) {
+    for (int ax = 0; ax < h->ndim; ++ax) {
+      LineArgs L = line_args(h->g, ax);
+      thomas_factor_kernel<<<(L.lines + 127) / 128, 128, 0, s>>>(L, h->tlo[ax], h->tden[ax], h->tcp[ax]);
+    }
+    TPF_CUDA_TRY(cudaGetLastError());
   }
-  TPF_CUDA_TRY(cudaGetLastError());
+  h->line_ready = line;
   h->prepared = true;
   return TPF_OK;
 }

@@ -572,6 +572,43 @@ __global__ void loss_grad_kernel(int B, long long npix, const float* y, const fl
   }
 }
 
+// Energy loss of a coarse-grid correction (two-level preconditioner training):
+// per sample b, with y the network output on the coarse image, x = in2[..,0]
+// the scaled coarse residual and A~ = I - (couplings c0 to the next row, c1 to
+// the next column; unit diagonal inside the nc0 x nc1 coarse grid),
+//   L_b = (y.A~y - 2 y.x) / E_b + 1  = ||e1 - P y^||_A^2 / ||e1||_A^2,
+// dL/dy = 2 (A~y - x) / (B E_b).  Pixels outside the coarse grid carry no term.
+__global__ void energy_terms_kernel(int B, int H, int W, int nc0, int nc1, const float* y, const float* in2,
+                                    const float* coupl, double* sums, float* dy, const double* escale,
+                                    int want_grad) {
+  const int b = blockIdx.y;
+  const long long npix = (long long)H * W;
+  const float* yb = y + b * npix;
+  const float* xb = in2 + b * npix * 2;
+  const float* cb = coupl + b * npix * 2;
+  double acc = 0.0;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < npix; q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q / W), j = (int)(q - (long long)i * W);
+    float g = 0.f;
+    if (i < nc0 && j < nc1) {
+      const float yv = yb[q];
+      float ay = yv;
+      if (i + 1 < nc0) ay -= cb[2 * q] * yb[q + W];
+      if (i > 0) ay -= cb[2 * (q - W)] * yb[q - W];
+      if (j + 1 < nc1) ay -= cb[2 * q + 1] * yb[q + 1];
+      if (j > 0) ay -= cb[2 * (q - 1) + 1] * yb[q - 1];
+      const float xv = xb[2 * q];
+      acc += (double)yv * ((double)ay - 2.0 * (double)xv);
+      g = ay - xv;
+    }
+    if (want_grad) dy[b * npix + q] = (float)(2.0 * g / (B * escale[b]));
+  }
+  double v[1] = {acc};
+  __shared__ double scratch[32];
+  tpf::block_sum<1>(v, scratch);
+  if (threadIdx.x == 0) atomicAdd(sums + b, v[0]);
+}
+
 __global__ void adam_kernel(float* p, float* g, float* m, float* v, long long n, float lr, float b1, float b2,
                             float eps, float c1, float c2, float wd) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -1022,6 +1059,41 @@ int tpf_unet_train_step(tpf_unet* n, int B, const float* in2, const float* targe
     for (int b = 0; b < B; ++b) L += hs[2 * b] / (hs[2 * b + 1] > 0 ? hs[2 * b + 1] : 1.0);
     *loss = L / B;
     return TPF_OK;
+  }
+  return TPF_OK;
+}
+
+int tpf_unet_train_step_energy(tpf_unet* n, int B, const float* in2, const float* coupl, const double* escale,
+                               int nc0, int nc1, float lr, float weight_decay, double* loss, void* stream) {
+  TPF_CHECK_ARG(n && in2 && coupl && escale, "null argument");
+  TPF_CHECK_ARG(B >= 1 && B <= n->max_batch, "batch %d outside [1, %d]", B, n->max_batch);
+  TPF_CHECK_ARG(nc0 >= 1 && nc1 >= 1 && nc0 <= n->H && nc1 <= n->W, "coarse grid %dx%d outside the image", nc0, nc1);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int st = ensure_training(n);
+  if (st) return st;
+  const LevelGeom g0 = n->geom(0, B);
+  pack_input_kernel<<<grid_for(g0.P()), 256, 0, s>>>(g0, in2, n->xin);
+  if ((st = forward(n, B, s))) return st;
+  TPF_CUDA_TRY(cudaMemsetAsync(n->sums, 0, sizeof(double) * B, s));
+  energy_terms_kernel<<<dim3(64, B), 256, 0, s>>>(B, n->H, n->W, nc0, nc1, n->out, in2, coupl, n->sums, n->dy,
+                                                  escale, 1);
+  TPF_CUDA_TRY(cudaGetLastError());
+  if ((st = backward(n, B, n->dy, s))) return st;
+  n->adam_t += 1;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.f - std::pow(b1, (float)n->adam_t), c2 = 1.f - std::pow(b2, (float)n->adam_t);
+  adam_kernel<<<grid_for(layout().total), 256, 0, s>>>(n->params, n->grads, n->m, n->v, layout().total, lr, b1, b2,
+                                                        1e-8f, c1, c2, weight_decay);
+  TPF_CUDA_TRY(cudaGetLastError());
+  n->arranged = false;
+  if (loss) {
+    std::vector<double> hs(B), he(B);
+    TPF_CUDA_TRY(cudaMemcpyAsync(hs.data(), n->sums, sizeof(double) * B, cudaMemcpyDeviceToHost, s));
+    TPF_CUDA_TRY(cudaMemcpyAsync(he.data(), escale, sizeof(double) * B, cudaMemcpyDeviceToHost, s));
+    if ((st = check_err(n, s))) return st;
+    double L = 0.0;
+    for (int b = 0; b < B; ++b) L += hs[b] / (he[b] > 0 ? he[b] : 1.0) + 1.0;
+    *loss = L / B;
   }
   return TPF_OK;
 }

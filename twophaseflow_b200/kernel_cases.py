@@ -2,6 +2,7 @@
 
     python -m twophaseflow_b200.kernel_cases ccd --N 256 256 256 --axis 0 --bc wall [--dtype f64] [--reps 5]
     python -m twophaseflow_b200.kernel_cases ppe --N 512 512 [--precision fp64] [--reps 2]
+    python -m twophaseflow_b200.kernel_cases learned --N 512 512 [--maxiter 16] [--reps 2]
 
 ``ccd`` captures ``reps`` CCDSolver.differentiate calls in one CUDA graph and
 replays it, so the reported time is device time per call (no Python launch
@@ -84,20 +85,66 @@ def ppe_case(N, precision, reps, tol=1e-8):
             "us_per_iteration": round(ms * 1e3 / max(it, 1), 2)}
 
 
+def learned_case(N, reps, maxiter=None, tol=1e-8):
+    """Network-preconditioned flexible CG (shipped weights, two-level mode) on
+    the droplet PPE; ``maxiter`` bounds the iterations (no fallback) for
+    profiling a fixed amount of work."""
+    import torch
+    from . import UniformGrid
+    from .learned import PPESolverLearned
+    from .workloads import divergence_rhs, droplet_density
+
+    class Cfg:
+        pseudo_tol = tol
+        pseudo_maxiter = 20000
+        ppe_learned_maxiter = maxiter if maxiter else 20000
+        ppe_learned_fallback = False
+
+    rho = torch.from_numpy(droplet_density(N, seed=0)).cuda()
+    rhs = torch.from_numpy(divergence_rhs(N, seed=1)).cuda()
+    s = PPESolverLearned(None, Cfg(), UniformGrid(N))
+
+    def run():
+        try:
+            s.solve(rhs, rho)
+        except RuntimeError:
+            if not maxiter:
+                raise
+
+    run()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        run()
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    it = s.last_diagnostics["ppe_learned_iterations"]
+    ms = min(ts)
+    return {"case": "learned", "N": list(N), "ms": round(ms, 3), "iterations": it,
+            "us_per_iteration": round(ms * 1e3 / max(it, 1), 2)}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["ccd", "ppe"])
+    ap.add_argument("case", choices=["ccd", "ppe", "learned"])
     ap.add_argument("--N", type=int, nargs="+", required=True)
     ap.add_argument("--axis", type=int, default=0)
     ap.add_argument("--bc", default="wall")
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--maxiter", type=int, default=0, help="learned: stop after this many iterations")
     a = ap.parse_args(argv)
     if a.case == "ccd":
         r = ccd_case(tuple(a.N), a.axis, a.bc, a.dtype, a.reps)
-    else:
+    elif a.case == "ppe":
         r = ppe_case(tuple(a.N), a.precision, a.reps)
+    else:
+        r = learned_case(tuple(a.N), a.reps, a.maxiter or None)
     print(json.dumps(r), flush=True)
     return 0
 

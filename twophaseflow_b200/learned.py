@@ -52,6 +52,13 @@ def round8(n: int) -> int:
     return (int(n) + 7) // 8 * 8
 
 
+def net_image(shape, coarsen: int):
+    """Network image for a 2-D node grid: nodes (coarsen = 1) or b x b aggregates,
+    rounded up to multiples of 8."""
+    b = int(coarsen)
+    return round8((int(shape[0]) + b - 1) // b), round8((int(shape[1]) + b - 1) // b)
+
+
 def num_params() -> int:
     return int(_lib.load().tpf_unet_num_params())
 
@@ -132,6 +139,15 @@ class UNet:
                                                 _lib.current_stream_handle()))
         return float(loss.value)
 
+    def train_step_energy(self, in2, coupl, escale, nc0: int, nc1: int, lr: float, weight_decay: float = 0.0) -> float:
+        """Adam step on the energy loss of a coarse-grid correction (tpf_unet_train_step_energy)."""
+        loss = C.c_double()
+        _lib.check(self.lib.tpf_unet_train_step_energy(self.handle, int(in2.shape[0]), _lib.dptr(in2), _lib.dptr(coupl),
+                                                       _lib.dptr(escale), int(nc0), int(nc1), float(lr),
+                                                       float(weight_decay), C.byref(loss),
+                                                       _lib.current_stream_handle()))
+        return float(loss.value)
+
     def save(self, path: str, **meta):
         os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
         np.savez(path, params=self.get_params(), **meta)
@@ -152,10 +168,13 @@ class PPESolverLearned(PPESolverFVMMatrixFree):
     """IPPESolver: flexible CG preconditioned by the trained U-Net (2-D, wall).
 
     Options are read from the solver config like the reference's own
-    (``pseudo_tol``, ``pseudo_maxiter``) plus ``ppe_learned_smooth`` (damped
-    Jacobi sweeps after the network, default 1), ``ppe_learned_omega`` (0.8),
-    ``ppe_learned_weights`` (path of the trained parameters) and
-    ``ppe_learned_fallback`` (finish with plain Jacobi PCG on a stall, True).
+    (``pseudo_tol``, ``pseudo_maxiter``) plus ``ppe_learned_coarsen`` (4: the
+    network solves the problem aggregated over 4 x 4 node blocks inside a
+    two-grid cycle; 1: the network reads the fine residual),
+    ``ppe_learned_smooth`` (damped Jacobi sweeps after the network, default 1),
+    ``ppe_learned_omega`` (0.8), ``ppe_learned_weights`` (path of the trained
+    parameters) and ``ppe_learned_fallback`` (finish with plain Jacobi PCG on a
+    stall, True).
     """
 
     scheme_names = ("fvm_learned",)
@@ -174,9 +193,11 @@ class PPESolverLearned(PPESolverFVMMatrixFree):
         self.omega = float(getattr(solver_cfg, "ppe_learned_omega", 0.8))
         self.fallback = bool(getattr(solver_cfg, "ppe_learned_fallback", True))
         self.learned_maxiter = int(getattr(solver_cfg, "ppe_learned_maxiter", max(self.maxiter, 2000)))
+        self.coarsen = int(getattr(solver_cfg, "ppe_learned_coarsen", 4))
+        self.window = int(getattr(solver_cfg, "ppe_learned_window", 1))
         if params is None:
             params = load_params(str(getattr(solver_cfg, "ppe_learned_weights", DEFAULT_WEIGHTS)))
-        H, W = round8(self.grid.shape[0]), round8(self.grid.shape[1])
+        H, W = net_image(self.grid.shape, self.coarsen)
         self.net = UNet(H, W, 1, params=params)
         self._lp = None
         self._make_lp()
@@ -186,7 +207,7 @@ class PPESolverLearned(PPESolverFVMMatrixFree):
             self.lib.tpf_lppe_destroy(self._lp)
             self._lp = None
         h = C.c_void_p()
-        _lib.check(self.lib.tpf_lppe_create(C.byref(h), self._handle, self.net.handle))
+        _lib.check(self.lib.tpf_lppe_create(C.byref(h), self._handle, self.net.handle, self.coarsen))
         self._lp = h
 
     def __del__(self):
@@ -210,6 +231,7 @@ class PPESolverLearned(PPESolverFVMMatrixFree):
         o.smooth = self.smooth
         o.omega = self.omega
         o.fallback = 1 if self.fallback else 0
+        o.window = self.window
         return o
 
     def prepare_operator(self, rho) -> None:
@@ -285,9 +307,12 @@ class _Cfg:
 
 
 def generate_pairs(N=(256, 256), n_cases: int = 64, snapshots=(0, 3, 10, 30, 80, 200, 500, 1000),
-                   seed: int = 0, log=None):
-    """(in2, target) training pairs from plain-PCG runs: device tensors
-    [M, H, W, 2] and [M, H, W] (M = n_cases x len(snapshots))."""
+                   seed: int = 0, coarsen: int = 4, omega: float = 0.8, energy: bool = False, log=None):
+    """Training pairs from plain-PCG runs on the network image of ``coarsen``
+    (M = n_cases x len(snapshots)):
+    energy=False: (in2 [M,H,W,2], target [M,H,W]) (tpf_lppe_pair);
+    energy=True (two-level mode): (in2, coupl [M,H,W,2], escale [M]) for the
+    energy loss (tpf_lppe_pair_energy)."""
     torch = _torch()
     from .grid import UniformGrid
     rng = np.random.default_rng(seed)
@@ -295,14 +320,18 @@ def generate_pairs(N=(256, 256), n_cases: int = 64, snapshots=(0, 3, 10, 30, 80,
     cfg = _Cfg(pseudo_tol=1e-12, pseudo_maxiter=100000, ppe_iteration_method="cg", ppe_preconditioner="jacobi")
     ppe = PPESolverFVMMatrixFree(None, cfg, grid)
     lib = ppe.lib
-    H, W = round8(grid.shape[0]), round8(grid.shape[1])
+    H, W = net_image(grid.shape, coarsen)
     net = UNet(H, W, 1)
     lp = C.c_void_p()
-    _lib.check(lib.tpf_lppe_create(C.byref(lp), ppe._handle, net.handle))
+    _lib.check(lib.tpf_lppe_create(C.byref(lp), ppe._handle, net.handle, int(coarsen)))
     M = n_cases * len(snapshots)
     dev = torch.device("cuda")
     in2 = torch.empty((M, H, W, 2), dtype=torch.float32, device=dev)
-    tgt = torch.empty((M, H, W), dtype=torch.float32, device=dev)
+    if energy:
+        tgt = torch.empty((M, H, W, 2), dtype=torch.float32, device=dev)
+        esc = torch.empty((M,), dtype=torch.float64, device=dev)
+    else:
+        tgt = torch.empty((M, H, W), dtype=torch.float32, device=dev)
     s = _lib.current_stream_handle()
     m = 0
     try:
@@ -327,7 +356,12 @@ def generate_pairs(N=(256, 256), n_cases: int = 64, snapshots=(0, 3, 10, 30, 80,
                     if st not in (_lib.TPF_OK, _lib.TPF_ENOCONV):
                         _lib.check(st)
                 e = (xs - xk).contiguous()
-                _lib.check(lib.tpf_lppe_pair(lp, _lib.dptr(e), _lib.dptr(in2[m]), _lib.dptr(tgt[m]), s))
+                if energy:
+                    _lib.check(lib.tpf_lppe_pair_energy(lp, _lib.dptr(e), _lib.dptr(in2[m]), _lib.dptr(tgt[m]),
+                                                        _lib.dptr(esc[m:m + 1]), float(omega), s))
+                else:
+                    _lib.check(lib.tpf_lppe_pair(lp, _lib.dptr(e), _lib.dptr(in2[m]), _lib.dptr(tgt[m]), float(omega),
+                                                 s))
                 m += 1
             o.maxiter = 100000
             _lib.check(lib.tpf_ppe_set_options(ppe._handle, C.byref(o)))
@@ -336,12 +370,16 @@ def generate_pairs(N=(256, 256), n_cases: int = 64, snapshots=(0, 3, 10, 30, 80,
     finally:
         lib.tpf_lppe_destroy(lp)
     torch.cuda.synchronize()
+    if energy:
+        return in2[:m], tgt[:m], esc[:m]
     return in2[:m], tgt[:m]
 
 
 def train(net: UNet, in2, target, epochs: int = 10, batch: int = 16, lr: float = 1e-3, weight_decay: float = 0.0,
-          seed: int = 0, log=None):
-    """Adam over shuffled mini-batches with a cosine learning-rate decay; returns per-epoch mean losses."""
+          seed: int = 0, log=None, escale=None, coarse=None):
+    """Adam over shuffled mini-batches with a cosine learning-rate decay; returns per-epoch mean losses.
+    With ``escale`` (and ``coarse`` = (nc0, nc1)) ``target`` holds the coarse
+    couplings and the energy loss is used."""
     torch = _torch()
     M = int(in2.shape[0])
     g = torch.Generator(device="cpu")
@@ -357,7 +395,11 @@ def train(net: UNet, in2, target, epochs: int = 10, batch: int = 16, lr: float =
             xb = in2.index_select(0, idx).contiguous()
             tb = target.index_select(0, idx).contiguous()
             cur = lr * 0.5 * (1.0 + np.cos(np.pi * step / max(1, steps)))
-            losses.append(net.train_step(xb, tb, cur, weight_decay))
+            if escale is not None:
+                eb = escale.index_select(0, idx).contiguous()
+                losses.append(net.train_step_energy(xb, tb, eb, coarse[0], coarse[1], cur, weight_decay))
+            else:
+                losses.append(net.train_step(xb, tb, cur, weight_decay))
             step += 1
         history.append(float(np.mean(losses)) if losses else float("nan"))
         if log:
