@@ -339,6 +339,11 @@ def main(argv=None):
     ccd3_gbps = float(np.mean([c["GBps"] for c in ccd3]))
     ccd3_best = max(ccd3, key=lambda c: c["GBps"])
 
+    # many independent cases in one persistent launch (32 seeded grids, 128..512 per axis)
+    from twophaseflow_b200.kernel_cases import batched_case
+    bat = batched_case(n_cases=32, reps=2)
+    bat.pop("grids", None)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(rho, rhs, it64)
@@ -366,6 +371,7 @@ def main(argv=None):
                         "us_per_iteration": round(ms_lr * 1e3 / max(1, dlr["ppe_learned_iterations"]), 1)},
             "learned_speedup_vs_plain_fp64": round(ms_64 / ms_lr, 3),
             "mixed_speedup_vs_plain_fp64": round(ms_64 / ms_mx, 3),
+            "batched_32_cases": bat,
             "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": 2 * ndof * 8,
                     "d2h_bytes_per_step": ndof * 8, "wall_ms": round(e2e_wall, 3)},
             "roofline": {"kernel": "pcg64_kernel (plain FP64 PCG, persistent)", "bound": "hbm",

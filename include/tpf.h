@@ -116,7 +116,9 @@ enum tpf_ppe_precond {
   TPF_PRECOND_NONE = 0,
   TPF_PRECOND_JACOBI = 1,
   TPF_PRECOND_LINE = 2,       /* shifted additive line solves, exact Thomas   */
-  TPF_PRECOND_LINE_PCR = 3    /* same, truncated PCR with pcr_stages stages    */
+  TPF_PRECOND_LINE_PCR = 3    /* same, PCR truncated to pcr_stages stages: the
+                               * reference's GPU line solver
+                               * (linalg_backend.py:77-163)                      */
 };
 enum tpf_precision {
   TPF_PREC_F64 = 0,      /* FP64 Krylov                                          */
@@ -185,6 +187,17 @@ int tpf_ppe_precondition(tpf_ppe* h, const double* r, double* z, void* stream);
  * (gmres_helpers.py:16-80). */
 int tpf_ppe_solve(tpf_ppe* h, const double* rhs, const double* rho, double* p,
                   const double* p_init, void* stream, tpf_ppe_result* result);
+
+/* Batched solve (no counterpart in the reference, which solves one system
+ * per call): n independent systems (n <= 64, each its own handle and grid,
+ * all with method TPF_PPE_CG and one precision) in ONE cooperative launch;
+ * every system runs the persistent PCG of tpf_ppe_solve on a share of the
+ * SMs proportional to its node count, with its own grid barrier.  rho may be
+ * NULL (or hold NULL entries) for handles prepared beforehand.  results[c]
+ * as tpf_ppe_solve; returns the first failure (TPF_ENOCONV / TPF_EABORT)
+ * after all systems finished.  Synchronizes `stream`. */
+int tpf_ppe_solve_batched(tpf_ppe* const* handles, int n, const double* const* rhs, const double* const* rho,
+                          double* const* p, void* stream, tpf_ppe_result* results);
 
 /* ---- allocation-free CG solve (no counterpart in the reference) ----------
  *

@@ -169,3 +169,56 @@ def test_config3_workload_512(cuda_device):
         p = s.solve(rhs, rho)
         assert s.last_diagnostics["ppe_low_order_cg_relative_residual"] < 1e-10
         assert np.abs(p - pd).max() <= 1e-6 * np.abs(pd).max()
+
+
+@pytest.mark.parametrize("name", ["gmres_line2d", "gmres_line3d", "gmres_drop16"])
+def test_truncated_pcr_line_preconditioner(cuda_device, ppe_golden, name):
+    """ppe_line_solver='pcr': the reference's GPU line solver (PCR truncated to
+    ppe_pcr_stages = 4, linalg_backend.py:77-163) against its own output."""
+    g = ppe_golden
+    key = f"{name}/line_pcr4"
+    if key not in g:
+        pytest.skip("no truncated-PCR golden for this case")
+    s, grid = _solver(g, name, ppe_line_solver="pcr", ppe_pcr_stages=4)
+    s.prepare_operator(g[f"{name}/rho"])
+    z = s.apply_line_preconditioner(g[f"{name}/r_rand"])
+    ref = g[key]
+    np.testing.assert_allclose(z, ref, rtol=1e-12, atol=1e-13 * np.abs(ref).max())
+
+
+def test_gmres_with_truncated_pcr_converges(cuda_device):
+    """GMRES(80) preconditioned by the truncated-PCR line solves reaches the
+    direct solution (density ratio 10: the reference's own GMRES + line
+    preconditioner stalls on ratio-1000 droplets at this size, with either line solver)."""
+    from twophaseflow_b200 import PPESolverFVMMatrixFree, UniformGrid
+    N = (48, 40)
+    rho = droplet_density(N, n_drops=4, seed=7, rho_g=0.1)
+    rhs = divergence_rhs(N, seed=8)
+    cfg = _Cfg(pseudo_tol=1e-8, pseudo_maxiter=200, ppe_iteration_method="gmres", ppe_preconditioner="line_pcr",
+               ppe_line_solver="pcr", ppe_pcr_stages=4, ppe_restart=80)
+    s = PPESolverFVMMatrixFree(None, cfg, UniformGrid(N))
+    p = s.solve(rhs, rho)
+    pd = oppe.spsolve_fvm(rhs, rho, oppe.uniform_coords(N, (1.0, 1.0)))
+    np.testing.assert_allclose(p, pd, rtol=1e-5, atol=1e-6 * np.abs(pd).max())
+
+
+def test_batched_solve_matches_individual_solves(cuda_device):
+    """Uneven grids in one persistent launch: same solutions (and iteration
+    counts within one) as solving each system on its own."""
+    import torch
+    from twophaseflow_b200 import PPESolverFVMMatrixFree, UniformGrid, solve_batched
+    shapes = [(32, 32), (48, 40), (64, 64), (17, 25), (80, 64), (128, 128)]
+    solvers, rhs, rho = [], [], []
+    for k, N in enumerate(shapes):
+        cfg = _Cfg(pseudo_tol=1e-10, pseudo_maxiter=50000, ppe_iteration_method="cg", ppe_preconditioner="jacobi")
+        solvers.append(PPESolverFVMMatrixFree(None, cfg, UniformGrid(N)))
+        rho.append(torch.from_numpy(droplet_density(N, n_drops=3, seed=40 + k)).to(cuda_device))
+        rhs.append(torch.from_numpy(divergence_rhs(N, seed=60 + k)).to(cuda_device))
+    pb = solve_batched(solvers, rhs, rho)
+    its_b = [s.last_diagnostics["ppe_low_order_cg_iterations"] for s in solvers]
+    for k, s in enumerate(solvers):
+        p1 = s.solve(rhs[k], rho[k])
+        it1 = s.last_diagnostics["ppe_low_order_cg_iterations"]
+        assert abs(it1 - its_b[k]) <= 1, (k, it1, its_b[k])
+        scale = float(torch.max(torch.abs(p1)))
+        assert float(torch.max(torch.abs(pb[k] - p1))) <= 1e-8 * scale

@@ -15,7 +15,8 @@ All arithmetic runs in the in-tree CUDA library ``libtpf.so`` (C ABI:
 from .ccd import CCDSolver
 from .ccd_ppe import CCDVariableDensityOperator, PPESolverDefectCorrection
 from .grid import BoundarySpec, UniformGrid
-from .ppe import MatrixAssemblyUnavailable, PPESolverFVMMatrixFree, create_fvm_matrixfree, register_with_reference
+from .ppe import (MatrixAssemblyUnavailable, PPESolverFVMMatrixFree, create_fvm_matrixfree, register_with_reference,
+                  solve_batched)
 
 __all__ = [
     "CCDSolver",
@@ -25,6 +26,7 @@ __all__ = [
     "MatrixAssemblyUnavailable",
     "create_fvm_matrixfree",
     "register_with_reference",
+    "solve_batched",
     "UniformGrid",
     "BoundarySpec",
 ]

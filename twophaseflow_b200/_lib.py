@@ -98,6 +98,9 @@ SIGNATURES = {
     "tpf_ppe_precondition": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tpf_ppe_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                 C.POINTER(tpf_ppe_result)]),
+    "tpf_ppe_solve_batched": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p),
+                                        C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_void_p,
+                                        C.POINTER(tpf_ppe_result)]),
     "tpf_ppe_solve_cg_static": (C.c_int, [C.c_int, C.POINTER(C.c_int64), C.POINTER(C.POINTER(C.c_double)),
                                           C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                           C.c_double, C.c_int64, C.c_void_p, C.POINTER(tpf_ppe_result)]),

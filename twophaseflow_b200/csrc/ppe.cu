@@ -55,9 +55,11 @@ __device__ __forceinline__ void coords3(const Grid3& g, int idx, int& i0, int& i
 // (i0, i1, i2) coordinates advance incrementally (no division per node).
 struct NodeIter {
   int idx, end, i0, i1, i2, d0, d1, d2;
-  __device__ __forceinline__ NodeIter(const Grid3& g) {
-    const int chunk = (g.ndof + gridDim.x - 1) / gridDim.x;
-    const int start = blockIdx.x * chunk;
+  __device__ __forceinline__ NodeIter(const Grid3& g) : NodeIter(g, blockIdx.x, gridDim.x) {}
+  // vb / nvb: this block's index and the block count of its (sub-)grid
+  __device__ __forceinline__ NodeIter(const Grid3& g, int vb, int nvb) {
+    const int chunk = (g.ndof + nvb - 1) / nvb;
+    const int start = vb * chunk;
     end = min(start + chunk, g.ndof);
     idx = start + threadIdx.x;
     coords3(g, idx, i0, i1, i2);
@@ -237,6 +239,83 @@ __global__ void thomas_solve_kernel(LineArgs L, const double* __restrict__ lo, c
   }
 }
 
+// Truncated parallel cyclic reduction along lines (the reference's GPU line
+// solver, linalg_backend.py:77-115): `stages` reduction steps of
+//   alpha = -a_i / d_{i-s}, beta = -c_i / d_{i+s} (0 beyond the line ends),
+//   a_i <- alpha a_{i-s}, c_i <- beta c_{i+s},
+//   d_i <- d_i + alpha c_{i-s} + beta a_{i+s}, b_i <- b_i + alpha b_{i-s} + beta b_{i+s},
+// with the stride s doubling, then x = b / d (exact when 2^stages >= n).
+// One block per line; the four coefficient arrays live in shared memory,
+// double-buffered.  r is read as 0 at the pin.  ACC: out = (out + x) * scale.
+template <bool ACC>
+__global__ void pcr_solve_kernel(LineArgs L, const double* __restrict__ lo, const double* __restrict__ dg,
+                                 const double* __restrict__ up, const double* __restrict__ r, double* out, int pin,
+                                 int stages, double scale, const int* done) {
+  if (done && *done) return;
+  extern __shared__ double sm[];
+  const int n = L.n;
+  double* A0 = sm;
+  double* D0 = A0 + n;
+  double* C0 = D0 + n;
+  double* B0 = C0 + n;
+  double* A1 = B0 + n;
+  double* D1 = A1 + n;
+  double* C1 = D1 + n;
+  double* B1 = C1 + n;
+  const int l = blockIdx.x;
+  const int base = line_base(L, l);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int e = base + i * L.stride;
+    A0[i] = lo[e];
+    D0[i] = dg[e];
+    C0[i] = up[e];
+    B0[i] = (e == pin) ? 0.0 : r[e];
+  }
+  __syncthreads();
+  int s = 1;
+  for (int st = 0; st < stages; ++st) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      double alpha = 0.0, beta = 0.0;
+      double al = 0.0, cl = 0.0, bl = 0.0, ar = 0.0, cr = 0.0, br = 0.0;
+      if (i >= s) {
+        const double dl = D0[i - s];
+        alpha = -A0[i] / (fabs(dl) > 0.0 ? dl : 1.0);
+        al = A0[i - s];
+        cl = C0[i - s];
+        bl = B0[i - s];
+      }
+      if (i < n - s) {
+        const double dr = D0[i + s];
+        beta = -C0[i] / (fabs(dr) > 0.0 ? dr : 1.0);
+        ar = A0[i + s];
+        cr = C0[i + s];
+        br = B0[i + s];
+      }
+      A1[i] = alpha * al;
+      D1[i] = D0[i] + alpha * cl + beta * ar;
+      C1[i] = beta * cr;
+      B1[i] = B0[i] + alpha * bl + beta * br;
+    }
+    __syncthreads();
+    double* t;
+    t = A0; A0 = A1; A1 = t;
+    t = D0; D0 = D1; D1 = t;
+    t = C0; C0 = C1; C1 = t;
+    t = B0; B0 = B1; B1 = t;
+    s *= 2;
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int e = base + i * L.stride;
+    const double x = B0[i] / D0[i];
+    if (ACC) {
+      const double v = (out[e] + x) * scale;
+      out[e] = (e == pin) ? 0.0 : v;
+    } else {
+      out[e] = x;
+    }
+  }
+}
+
 // ---- elementwise helpers ------------------------------------------------------
 
 // L p (reference apply): -(S p)/W for rows != pin (pin column kept), pin row identity.
@@ -347,8 +426,9 @@ struct GridSum {
   double* part;            // [2 slots][8][nblocks]
   unsigned int* count;     // monotonic arrival counter, zeroed before the launch
   int* err;
-  unsigned int nb;
+  unsigned int nb;         // blocks taking part (the whole grid, or one case's blocks)
   unsigned int epoch;
+  unsigned int bid;        // this block's index among them
 
   template <int NV>
   __device__ __forceinline__ bool sum(double (&v)[NV], double* scratch) {
@@ -357,7 +437,7 @@ struct GridSum {
     __shared__ int s_ok;
     if (threadIdx.x == 0) {
 #pragma unroll
-      for (int k = 0; k < NV; ++k) part[(slot * 8 + k) * nb + blockIdx.x] = v[k];
+      for (int k = 0; k < NV; ++k) part[(slot * 8 + k) * nb + bid] = v[k];
       red_release_add(count, 1u);
       const unsigned int target = (epoch + 1) * nb;
       int ok = 1;
@@ -397,8 +477,8 @@ struct GridSum {
 template <typename T>
 __device__ __forceinline__ void residual_pass(const Grid3& g, const double* s0, const double* s1,
                                               const double* s2, const double* b, const double* x, T* r,
-                                              bool x_nonzero, double& bb, double& rr) {
-  for (NodeIter it(g); it.ok(); it.next(g)) {
+                                              bool x_nonzero, double& bb, double& rr, int vb, int nvb) {
+  for (NodeIter it(g, vb, nvb); it.ok(); it.next(g)) {
     const int idx = it.idx;
     double bi = b[idx];
     double ri = bi;
@@ -423,9 +503,10 @@ __device__ __forceinline__ void residual_pass(const Grid3& g, const double* s0, 
 // products of the single reduction with the current search directions p, s:
 // red = {(r,u), (w,u), (u,s), (p,w), (p,s), (r,r)}.  init: p = s = 0.
 template <typename T>
-__device__ __forceinline__ void w_pass(const Grid3& g, const Cg1Vecs<T>& v, int cur, bool init, double (&red)[6]) {
+__device__ __forceinline__ void w_pass(const Grid3& g, const Cg1Vecs<T>& v, int cur, bool init, double (&red)[6],
+                                       int vb, int nvb) {
   const T* __restrict__ r = v.r[cur];
-  for (NodeIter it(g); it.ok(); it.next(g)) {
+  for (NodeIter it(g, vb, nvb); it.ok(); it.next(g)) {
     const int idx = it.idx;
     const int i0 = it.i0, i1 = it.i1, i2 = it.i2;
     const T ri = r[idx];
@@ -457,29 +538,31 @@ __device__ __forceinline__ void w_pass(const Grid3& g, const Cg1Vecs<T>& v, int 
   }
 }
 
+// The whole PCG solve of one system, run by blocks [0, nvb) of a grid (vb =
+// this block's index): the full grid for a single solve, or one case's share
+// of a batched launch.
 template <typename T, bool MIXED>
-__global__ void __launch_bounds__(kThreads, 1) cg1_kernel(Cg1Args a) {
+__device__ __forceinline__ void cg1_body(const Cg1Args& a, int vb, int nvb) {
   __shared__ double scratch[256];
-  GridSum gs{a.part, a.count, a.err, gridDim.x, 0u};
+  GridSum gs{a.part, a.count, a.err, (unsigned int)nvb, 0u, (unsigned int)vb};
   const Grid3& g = a.g;
   const Cg1Vecs<T>& v = *reinterpret_cast<const Cg1Vecs<T>*>(MIXED ? (const void*)&a.v32 : (const void*)&a.v64);
-  const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int G = gridDim.x * blockDim.x;
+  const int gtid = vb * blockDim.x + threadIdx.x;
   int cur = 0;
   // r0 = b - S x0
   double red0[2] = {0.0, 0.0};
-  residual_pass<T>(g, a.s64[0], a.s64[1], a.s64[2], a.b, a.x, v.r[cur], a.x_nonzero != 0, red0[0], red0[1]);
+  residual_pass<T>(g, a.s64[0], a.s64[1], a.s64[2], a.b, a.x, v.r[cur], a.x_nonzero != 0, red0[0], red0[1], vb, nvb);
   if (!gs.sum<2>(red0, scratch)) return;
   const double bb = red0[0];
   if (bb == 0.0) {
-    for (NodeIter it(g); it.ok(); it.next(g)) a.x[it.idx] = 0.0;
+    for (NodeIter it(g, vb, nvb); it.ok(); it.next(g)) a.x[it.idx] = 0.0;
     if (gtid == 0) { a.st->iters = 0; a.st->applies = 0; a.st->rr = 0.0; a.st->bb = 0.0; a.st->converged = 1; }
     return;
   }
   const double atol = a.tol * sqrt(bb);
   const double atol2 = atol * atol;
   double red[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  w_pass<T>(g, v, cur, true, red);
+  w_pass<T>(g, v, cur, true, red, vb, nvb);
   bool ok = gs.sum<6>(red, scratch);
   // loop state: gamma_i, rr_i and the denominator (p_i, S p_i) of alpha_i
   double gamma = red[0], rr = red[5];
@@ -497,14 +580,14 @@ __global__ void __launch_bounds__(kThreads, 1) cg1_kernel(Cg1Args a) {
       // (the true residual stalls near eps32 * kappa), so each replacement
       // starts a fresh Krylov cycle from the FP64 iterate
       double rb[2] = {0.0, 0.0};
-      residual_pass<T>(g, a.s64[0], a.s64[1], a.s64[2], a.b, a.x, v.r[cur], true, rb[0], rb[1]);
+      residual_pass<T>(g, a.s64[0], a.s64[1], a.s64[2], a.b, a.x, v.r[cur], true, rb[0], rb[1], vb, nvb);
       ++replacements;
       ++applies;
       if (!(ok = gs.sum<2>(rb, scratch))) break;
       if (rb[1] < atol2) { rr = rb[1]; conv = true; break; }
       if (it >= a.maxiter) { rr = rb[1]; break; }
       double rd[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-      w_pass<T>(g, v, cur, true, rd);
+      w_pass<T>(g, v, cur, true, rd, vb, nvb);
       ++applies;
       if (!(ok = gs.sum<6>(rd, scratch))) break;
       beta = 0.0;
@@ -529,7 +612,7 @@ __global__ void __launch_bounds__(kThreads, 1) cg1_kernel(Cg1Args a) {
 #pragma unroll
     for (int k = 0; k < 6; ++k) red[k] = 0.0;
 #pragma unroll 2
-    for (NodeIter it(g); it.ok(); it.next(g)) {
+    for (NodeIter it(g, vb, nvb); it.ok(); it.next(g)) {
       const int idx = it.idx;
       const int i0 = it.i0, i1 = it.i1, i2 = it.i2;
       const T ri = rc[idx];
@@ -580,6 +663,27 @@ __global__ void __launch_bounds__(kThreads, 1) cg1_kernel(Cg1Args a) {
     a.st->bb = bb;
     a.st->converged = conv ? 1 : 0;
   }
+}
+
+template <typename T, bool MIXED>
+__global__ void __launch_bounds__(kThreads, 1) cg1_kernel(Cg1Args a) {
+  cg1_body<T, MIXED>(a, blockIdx.x, gridDim.x);
+}
+
+// Many independent systems in one cooperative launch: case c owns blocks
+// [first[c], first[c + 1]) and runs its own PCG with its own barrier counter.
+constexpr int kBatchMax = 64;
+struct Cg1Batch {
+  Cg1Args c[kBatchMax];
+  int first[kBatchMax + 1];
+  int n;
+};
+
+template <typename T, bool MIXED>
+__global__ void __launch_bounds__(kThreads, 1) cg1_batch_kernel(const __grid_constant__ Cg1Batch b) {
+  int c = 0;
+  while (c + 1 < b.n && (int)blockIdx.x >= b.first[c + 1]) ++c;
+  cg1_body<T, MIXED>(b.c[c], blockIdx.x - b.first[c], b.first[c + 1] - b.first[c]);
 }
 
 // ---- GMRES building blocks ---------------------------------------------------------
@@ -792,7 +896,7 @@ struct tpf_ppe {
   double* tden[3] = {nullptr, nullptr, nullptr};
   double* tcp[3] = {nullptr, nullptr, nullptr};
   bool prepared = false;
-  bool line_ready = false;   // line-preconditioner factors built by the last prepare
+  int line_ready = 0;   // line-preconditioner state of the last prepare (0 none, else the precond kind)
   // Krylov workspace
   double* x = nullptr; double* r = nullptr; double* z = nullptr; double* p0 = nullptr; double* p1 = nullptr;
   double* q = nullptr; double* b = nullptr; double* t1 = nullptr; double* t2 = nullptr;
@@ -841,6 +945,7 @@ int validate_options(const tpf_ppe_options* o) {
   TPF_CHECK_ARG(o->maxiter >= 0, "maxiter must be >= 0");
   TPF_CHECK_ARG(o->restart >= 1 && o->restart <= 1024, "restart must be in [1, 1024]");
   TPF_CHECK_ARG(o->c_tau > 0.0, "c_tau must be > 0");
+  TPF_CHECK_ARG(o->precond != TPF_PRECOND_LINE_PCR || o->pcr_stages >= 1, "ppe_pcr_stages must be >= 1");
   return TPF_OK;
 }
 
@@ -885,6 +990,28 @@ int precond_L(tpf_ppe* h, const double* r, double* z, cudaStream_t s, const int*
     case TPF_PRECOND_JACOBI:
       jacobi_L_kernel<<<ew_grid(h), 256, 0, s>>>(g.ndof, g.pin, h->dinvL, r, z, done);
       break;
+    case TPF_PRECOND_LINE_PCR: {
+      // additive shifted line solves by truncated PCR (the reference's GPU variant)
+      for (int ax = 0; ax < h->ndim; ++ax) {
+        LineArgs L = line_args(g, ax);
+        const int nstage = std::min(h->o.pcr_stages, (int)std::ceil(std::log2((double)std::max(L.n, 2))));
+        const size_t smem = sizeof(double) * 8 * (size_t)L.n;
+        TPF_CHECK_ARG(smem <= 227 * 1024, "truncated-PCR line solve: lines of %d nodes exceed shared memory", L.n);
+        const double sc = (ax == h->ndim - 1) ? 1.0 / h->ndim : 1.0;
+        if (ax == 0) {
+          TPF_CUDA_TRY(cudaFuncSetAttribute(pcr_solve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem));
+          pcr_solve_kernel<false><<<L.lines, 256, smem, s>>>(L, h->tlo[ax], h->tden[ax], h->tcp[ax], r, z, g.pin,
+                                                              nstage, 1.0, done);
+        } else {
+          TPF_CUDA_TRY(cudaFuncSetAttribute(pcr_solve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem));
+          pcr_solve_kernel<true><<<L.lines, 256, smem, s>>>(L, h->tlo[ax], h->tden[ax], h->tcp[ax], r, z, g.pin,
+                                                             nstage, sc, done);
+        }
+      }
+      break;
+    }
     default: {
       // additive shifted line solves: z = (sum_a T_a^-1 r) / ndim, r[pin] = 0, z[pin] = 0
       for (int ax = 0; ax < h->ndim; ++ax) {
@@ -1242,7 +1369,7 @@ int tpf_ppe_set_options(tpf_ppe* h, const tpf_ppe_options* o) {
   if (st) return st;
   // the line preconditioner's state depends on c_tau and is only built when it is selected
   const bool to_line = (o->precond == TPF_PRECOND_LINE || o->precond == TPF_PRECOND_LINE_PCR);
-  bool line_changed = to_line && (!h->line_ready || o->c_tau != h->o.c_tau);
+  bool line_changed = to_line && (h->line_ready != o->precond || o->c_tau != h->o.c_tau);
   bool grow = o->restart > h->o.restart;
   h->o = *o;
   if (grow) {
@@ -1279,14 +1406,15 @@ int tpf_ppe_prepare(tpf_ppe* h, const double* rho, void* stream) {
   a.want_line = line ? 1 : 0;
   prep_faces_kernel<<<h->ew_blocks, 256, 0, s>>>(a);
   TPF_CUDA_TRY(cudaGetLastError());
-  if (line) {
+  // Thomas factors for the exact line solve; truncated PCR works on the raw coefficients
+  if (h->o.precond == TPF_PRECOND_LINE) {
     for (int ax = 0; ax < h->ndim; ++ax) {
       LineArgs L = line_args(h->g, ax);
       thomas_factor_kernel<<<(L.lines + 127) / 128, 128, 0, s>>>(L, h->tlo[ax], h->tden[ax], h->tcp[ax]);
     }
     TPF_CUDA_TRY(cudaGetLastError());
   }
-  h->line_ready = line;
+  h->line_ready = line ? h->o.precond : 0;
   h->prepared = true;
   return TPF_OK;
 }
@@ -1304,14 +1432,12 @@ int tpf_ppe_apply(tpf_ppe* h, const double* p, double* out, void* stream) {
 int tpf_ppe_precondition(tpf_ppe* h, const double* r, double* z, void* stream) {
   TPF_CHECK_ARG(h && r && z, "NULL argument");
   TPF_CHECK_ARG(h->prepared, "preconditioner state is not initialised (call prepare first)");
-  TPF_CHECK_ARG(h->o.precond != TPF_PRECOND_LINE_PCR, "truncated-PCR line preconditioner is not built");
   return precond_L(h, r, z, static_cast<cudaStream_t>(stream), nullptr);
 }
 
 int tpf_ppe_solve(tpf_ppe* h, const double* rhs, const double* rho, double* p, const double* p_init, void* stream,
                   tpf_ppe_result* result) {
   TPF_CHECK_ARG(h && rhs && p, "NULL argument");
-  TPF_CHECK_ARG(h->o.precond != TPF_PRECOND_LINE_PCR, "truncated-PCR line preconditioner is not built");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int st;
   if (rho) {
@@ -1323,6 +1449,115 @@ int tpf_ppe_solve(tpf_ppe* h, const double* rhs, const double* rho, double* p, c
   *res = tpf_ppe_result{};
   if (h->o.method == TPF_PPE_CG) return solve_cg(h, rhs, p, p_init, s, res);
   return solve_gmres(h, rhs, p, p_init, s, res);
+}
+
+int tpf_ppe_solve_batched(tpf_ppe* const* hs, int n, const double* const* rhs, const double* const* rho,
+                          double* const* p, void* stream, tpf_ppe_result* results) {
+  TPF_CHECK_ARG(hs && rhs && p && n >= 1, "NULL argument or empty batch");
+  TPF_CHECK_ARG(n <= kBatchMax, "at most %d systems per batched solve (got %d)", kBatchMax, n);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int st;
+  const bool mixed = hs[0]->o.precision == TPF_PREC_MIXED;
+  for (int c = 0; c < n; ++c) {
+    tpf_ppe* h = hs[c];
+    TPF_CHECK_ARG(h && rhs[c] && p[c], "NULL handle or array for system %d", c);
+    TPF_CHECK_ARG(h->o.method == TPF_PPE_CG, "batched solves run the CG route (system %d)", c);
+    TPF_CHECK_ARG((h->o.precision == TPF_PREC_MIXED) == mixed, "all systems of a batch share one precision");
+    if (rho && rho[c] && (st = tpf_ppe_prepare(h, rho[c], stream))) return st;
+    TPF_CHECK_ARG(h->prepared, "operator coefficients of system %d are not initialised", c);
+  }
+  double wsum = 0.0;
+  for (int c = 0; c < n; ++c) wsum += std::pow((double)hs[c]->g.ndof, 1.5);
+  // blocks: one per SM (the kernel's occupancy), shared in proportion to the
+  // expected work, nodes x iterations ~ ndof^1.5 (Jacobi-PCG iteration counts
+  // grow like the grid's linear size)
+  void* fn = mixed ? (void*)cg1_batch_kernel<float, true> : (void*)cg1_batch_kernel<double, false>;
+  int per_sm = 0;
+  TPF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, 0));
+  const int cap = tpf::sm_count() * std::max(1, per_sm);
+  TPF_CHECK_ARG(n <= cap, "batch of %d systems exceeds the %d co-resident blocks", n, cap);
+  std::vector<int> nb(n);
+  int used = 0;
+  for (int c = 0; c < n; ++c) {
+    const double share = (double)cap * std::pow((double)hs[c]->g.ndof, 1.5) / wsum;
+    nb[c] = std::max(1, std::min(hs[c]->coop_blocks, (int)share));
+    used += nb[c];
+  }
+  while (used > cap) {   // trim the largest shares
+    int m = 0;
+    for (int c = 1; c < n; ++c)
+      if (nb[c] > nb[m]) m = c;
+    --nb[m];
+    --used;
+  }
+  auto* b = new Cg1Batch();
+  b->n = n;
+  b->first[0] = 0;
+  for (int c = 0; c < n; ++c) {
+    tpf_ppe* h = hs[c];
+    const Geo geo{{h->dv[0], h->dv[1], h->dv[2]}, {h->dface[0], h->dface[1], h->dface[2]}};
+    cg_rhs_kernel<<<ew_grid(h), 256, 0, s>>>(h->g, geo, rhs[c], h->b, nullptr, h->x);
+    TPF_CUDA_TRY(cudaMemsetAsync(h->bar, 0, 2 * sizeof(unsigned int), s));
+    TPF_CUDA_TRY(cudaMemsetAsync(h->err, 0, sizeof(int), s));
+    TPF_CUDA_TRY(cudaMemsetAsync(h->st, 0, sizeof(SolveStatus), s));
+    Cg1Args& a = b->c[c];
+    a = Cg1Args{};
+    a.g = h->g;
+    const bool none = (h->o.precond == TPF_PRECOND_NONE);
+    a.v64.s0 = h->s[0]; a.v64.s1 = h->s[1]; a.v64.s2 = h->s[2];
+    a.v64.dinv = none ? h->ones64 : h->dinvS;
+    a.v32.s0 = h->s32[0]; a.v32.s1 = h->s32[1]; a.v32.s2 = h->s32[2];
+    a.v32.dinv = none ? h->ones32 : h->dinvS32;
+    for (int k = 0; k < 2; ++k) {
+      a.v64.r[k] = h->c64[k]; a.v64.w[k] = h->c64[2 + k]; a.v64.s[k] = h->c64[4 + k];
+      a.v32.r[k] = h->c32[k]; a.v32.w[k] = h->c32[2 + k]; a.v32.s[k] = h->c32[4 + k];
+    }
+    a.v64.p = h->c64[6];
+    a.v32.p = h->c32[6];
+    a.s64[0] = h->s[0]; a.s64[1] = h->s[1]; a.s64[2] = h->s[2];
+    a.b = h->b;
+    a.x = h->x;
+    a.tol = h->o.tol;
+    a.x_nonzero = 0;
+    a.part = h->part;
+    a.count = h->bar;
+    a.err = h->err;
+    a.st = h->st;
+    a.maxiter = h->o.maxiter;
+    a.replace_drop = h->o.inner_tol > 0.0 ? h->o.inner_tol : 1e-3;
+    b->first[c + 1] = b->first[c] + nb[c];
+  }
+  void* args[] = {b};
+  cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(b->first[n]), dim3(kThreads), args, 0, s);
+  delete b;
+  TPF_CUDA_TRY(e);
+  std::vector<SolveStatus> hst(n);
+  std::vector<int> herr(n);
+  for (int c = 0; c < n; ++c) {
+    tpf_ppe* h = hs[c];
+    copy_pin0_kernel<<<ew_grid(h), 256, 0, s>>>(h->g.ndof, h->g.pin, h->x, p[c]);
+    TPF_CUDA_TRY(cudaMemcpyAsync(&hst[c], h->st, sizeof(SolveStatus), cudaMemcpyDeviceToHost, s));
+    TPF_CUDA_TRY(cudaMemcpyAsync(&herr[c], h->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  }
+  TPF_CUDA_TRY(cudaStreamSynchronize(s));
+  int status = TPF_OK;
+  for (int c = 0; c < n; ++c) {
+    tpf_ppe_result r{};
+    r.iterations = hst[c].iters;
+    r.applies = hst[c].applies;
+    r.refinements = hst[c].refinements;
+    r.rel_residual = hst[c].bb > 0.0 ? std::sqrt(hst[c].rr / hst[c].bb) : 0.0;
+    r.info = hst[c].converged ? 0 : (int)std::min<long long>(hs[c]->o.maxiter, 0x7fffffff);
+    if (results) results[c] = r;
+    if (herr[c]) {
+      tpf::set_error("PCG barrier of batched system %d timed out; the solve was aborted", c);
+      status = TPF_EABORT;
+    } else if (!hst[c].converged && status == TPF_OK) {
+      tpf::set_error("batched PCG system %d did not converge (info=%d)", c, r.info);
+      status = TPF_ENOCONV;
+    }
+  }
+  return status;
 }
 
 }  // extern "C"

@@ -3,6 +3,7 @@
     python -m twophaseflow_b200.kernel_cases ccd --N 256 256 256 --axis 0 --bc wall [--dtype f64] [--reps 5]
     python -m twophaseflow_b200.kernel_cases ppe --N 512 512 [--precision fp64] [--reps 2]
     python -m twophaseflow_b200.kernel_cases learned --N 512 512 [--maxiter 16] [--reps 2]
+    python -m twophaseflow_b200.kernel_cases batched --N 32 [--reps 3]     (32 cases, grids 128..512)
 
 ``ccd`` captures ``reps`` CCDSolver.differentiate calls in one CUDA graph and
 replays it, so the reported time is device time per call (no Python launch
@@ -128,9 +129,55 @@ def learned_case(N, reps, maxiter=None, tol=1e-8):
             "us_per_iteration": round(ms * 1e3 / max(it, 1), 2)}
 
 
+def batched_case(n_cases=32, nmin=128, nmax=512, reps=3, seed=0, tol=1e-8):
+    """``n_cases`` independent 2-D droplet PPEs with seeded uneven grids
+    (N_x, N_y uniform in [nmin, nmax]) solved in ONE persistent launch
+    (solve_batched) against one solve after the other with the same kernels."""
+    import numpy as np
+    import torch
+    from . import PPESolverFVMMatrixFree, UniformGrid, solve_batched
+    from .workloads import divergence_rhs, droplet_density
+
+    class Cfg:
+        pseudo_tol = tol
+        pseudo_maxiter = 1_000_000
+        ppe_iteration_method = "cg"
+        ppe_preconditioner = "jacobi"
+
+    rng = np.random.default_rng(seed)
+    shapes = [tuple(int(v) for v in rng.integers(nmin, nmax + 1, size=2)) for _ in range(n_cases)]
+    solvers, rhs, rho = [], [], []
+    for k, N in enumerate(shapes):
+        solvers.append(PPESolverFVMMatrixFree(None, Cfg(), UniformGrid(N)))
+        rho.append(torch.from_numpy(droplet_density(N, n_drops=8, seed=100 + k)).cuda())
+        rhs.append(torch.from_numpy(divergence_rhs(N, seed=200 + k)).cuda())
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return min(ts)
+
+    ms_b = timed(lambda: solve_batched(solvers, rhs, rho))
+    its = [s.last_diagnostics["ppe_low_order_cg_iterations"] for s in solvers]
+    ms_s = timed(lambda: [s.solve(rhs[k], rho[k]) for k, s in enumerate(solvers)])
+    return {"case": "batched", "n_cases": n_cases, "grids": [list(g) for g in shapes], "ms_batched": round(ms_b, 3),
+            "ms_sequential": round(ms_s, 3), "cases_per_s_batched": round(n_cases / (ms_b * 1e-3), 1),
+            "cases_per_s_sequential": round(n_cases / (ms_s * 1e-3), 1), "iterations_max": int(max(its)),
+            "iterations_total": int(sum(its))}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["ccd", "ppe", "learned"])
+    ap.add_argument("case", choices=["ccd", "ppe", "learned", "batched"])
     ap.add_argument("--N", type=int, nargs="+", required=True)
     ap.add_argument("--axis", type=int, default=0)
     ap.add_argument("--bc", default="wall")
@@ -143,8 +190,10 @@ def main(argv=None):
         r = ccd_case(tuple(a.N), a.axis, a.bc, a.dtype, a.reps)
     elif a.case == "ppe":
         r = ppe_case(tuple(a.N), a.precision, a.reps)
-    else:
+    elif a.case == "learned":
         r = learned_case(tuple(a.N), a.reps, a.maxiter or None)
+    else:
+        r = batched_case(n_cases=a.N[0], reps=a.reps)
     print(json.dumps(r), flush=True)
     return 0
 

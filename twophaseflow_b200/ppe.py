@@ -11,7 +11,9 @@ non-convergence).  All arithmetic runs in ``libtpf.so`` (tpf_ppe_*).
 
 B200 additions, read the same way from the solver config:
 ``ppe_precision`` ('fp64' | 'mixed': FP32 inner CG under FP64 iterative
-refinement), ``ppe_inner_tol`` and ``ppe_max_refine``.
+refinement), ``ppe_inner_tol``, ``ppe_max_refine`` and ``ppe_line_solver``
+('thomas': exact line solves as the reference's CPU backend; 'pcr': PCR
+truncated to ``ppe_pcr_stages`` as the reference's GPU backend).
 """
 
 from __future__ import annotations
@@ -74,6 +76,11 @@ class PPESolverFVMMatrixFree:
                              "line_pcr is a nonsymmetric GMRES preconditioner.")
         pcr = getattr(solver_cfg, "ppe_pcr_stages", 4)
         self.precond_pcr_stages = int(pcr if pcr is not None else 4)
+        # the reference solves the shifted line systems exactly (Thomas) on the
+        # CPU backend and by PCR truncated to ppe_pcr_stages on its GPU backend
+        self.line_solver = str(getattr(solver_cfg, "ppe_line_solver", "thomas")).strip().lower()
+        if self.line_solver not in ("thomas", "pcr"):
+            raise ValueError(f"ppe_line_solver must be 'thomas' or 'pcr', got {self.line_solver!r}")
         self.precision = str(getattr(solver_cfg, "ppe_precision", "fp64")).strip().lower()
         if self.precision not in ("fp64", "mixed"):
             raise ValueError(f"ppe_precision must be 'fp64' or 'mixed', got {self.precision!r}")
@@ -96,6 +103,8 @@ class PPESolverFVMMatrixFree:
         self.lib.tpf_ppe_default_options(C.byref(o))
         o.method = _METHOD[self.iteration_method]
         o.precond = _PRECOND[self.preconditioner]
+        if o.precond == _lib.TPF_PRECOND_LINE and self.line_solver == "pcr":
+            o.precond = _lib.TPF_PRECOND_LINE_PCR
         o.precision = _lib.TPF_PREC_MIXED if self.precision == "mixed" else _lib.TPF_PREC_F64
         o.tol = self.tol
         o.maxiter = self.maxiter
@@ -251,3 +260,55 @@ def register_with_reference(register_ppe_solver, names=("fvm_iterative", "fvm_ma
     ``register_with_reference(twophase.ppe.factory.register_ppe_solver)``."""
     for n in names:
         register_ppe_solver(n, create_fvm_matrixfree)
+
+
+def solve_batched(solvers, rhs_list, rho_list=None):
+    """Solve many independent PPE systems in ONE persistent launch
+    (tpf_ppe_solve_batched): ``solvers`` are CG-route PPESolverFVMMatrixFree
+    instances (each with its own grid), ``rhs_list`` / ``rho_list`` their
+    fields.  Returns the list of pressures (p[pin] = 0); each solver's
+    ``last_diagnostics`` is filled as by its own solve."""
+    torch = _torch()
+    n = len(solvers)
+    if n == 0:
+        return []
+    if len(rhs_list) != n or (rho_list is not None and len(rho_list) != n):
+        raise ValueError("one rhs (and rho) per solver")
+    lib = solvers[0].lib
+    keep, outs, views = [], [], []
+    for k, s in enumerate(solvers):
+        if s.iteration_method != "cg":
+            raise ValueError("batched solves run the CG route (ppe_iteration_method='cg')")
+        s._sync_options()
+        vr = to_device(rhs_list[k], dtype=torch.float64)
+        s._check_shape(vr.tensor)
+        views.append(vr)
+        keep.append(vr.tensor)
+        if rho_list is not None:
+            vrho = to_device(rho_list[k], dtype=torch.float64)
+            s._check_shape(vrho.tensor)
+            keep.append(vrho.tensor)
+            s._rho_keep = vrho.tensor
+        outs.append(torch.empty_like(vr.tensor))
+    H = (C.c_void_p * n)(*[s._handle.value for s in solvers])
+    R = (C.c_void_p * n)(*[int(v.tensor.data_ptr()) for v in views])
+    P = (C.c_void_p * n)(*[int(o.data_ptr()) for o in outs])
+    RHO = None
+    if rho_list is not None:
+        RHO = (C.c_void_p * n)(*[int(t.data_ptr()) for t in keep[1::2]])
+    res = (_lib.tpf_ppe_result * n)()
+    st = lib.tpf_ppe_solve_batched(H, n, R, RHO, P, _lib.current_stream_handle(), res)
+    for k, s in enumerate(solvers):
+        s._prepared = True
+        key = "ppe_low_order_cg"
+        s.last_diagnostics = {
+            f"{key}_info": int(res[k].info),
+            f"{key}_iterations": int(res[k].iterations),
+            f"{key}_applies": int(res[k].applies),
+            f"{key}_refinements": int(res[k].refinements),
+            f"{key}_relative_residual": float(res[k].rel_residual),
+        }
+    if st == _lib.TPF_ENOCONV:
+        raise RuntimeError(_lib.last_error())
+    _lib.check(st)
+    return [v.out(o) for v, o in zip(views, outs)]
