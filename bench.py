@@ -113,11 +113,13 @@ def _dist():
 
 
 def _max_over_ranks(x, ws):
+    """Max of a per-rank device time over the replicas (NCCL on GPUs, gloo on CPU)."""
     if ws == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 

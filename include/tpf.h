@@ -67,6 +67,15 @@ int tpf_ccd_plan_create(tpf_ccd_plan** plan, int64_t n_pts, double h, int bc,
                         int dtype);
 int tpf_ccd_plan_destroy(tpf_ccd_plan* plan);
 
+/* Launch-shape autotuning of the many-line kernel (default on; no counterpart
+ * in the reference): the first tpf_ccd_apply of each (line count, axis kind,
+ * boundary, outputs, dtype) combination times a few launch shapes on the
+ * caller's stream and keeps the fastest (results are identical for every
+ * shape).  That first call synchronizes the stream; it is skipped while the
+ * stream is being captured.  enable = 0 switches tuning off and forgets the
+ * choices. */
+int tpf_ccd_plan_set_autotune(tpf_ccd_plan* plan, int enable);
+
 /* Metric of a non-uniform axis (host arrays of n_pts doubles: J = dxi/dx and
  * dJ/dxi).  Replaces the grid metric used by apply_ccd_metric
  * (ccd_solver_helpers.py:509-533).  Blocking. */
@@ -75,7 +84,8 @@ int tpf_ccd_plan_set_metric(tpf_ccd_plan* plan, const double* J,
 
 /* d1/d2 of f along the plan's axis for an array viewed as C-order
  * [outer, n_pts, inner] (the axis in the middle).  f, d1, d2 are device
- * pointers of the plan's dtype; d1 or d2 may be NULL (first_derivative /
+ * pointers of the plan's dtype (f must not alias d1 or d2 -> TPF_EINVAL);
+ * d1 or d2 may be NULL (first_derivative /
  * second_derivative).  bc_left / bc_right: optional host pointers to
  * (f'_b, f''_b) overrides of the wall closure (testing hook of the reference),
  * NULL for the compact closure.  flags: TPF_CCD_APPLY_METRIC.

@@ -331,3 +331,24 @@ def test_ccd_lane_kernel_metric_and_vd(cuda_device, ax):
                                          _lib.dptr(out), 0, 0, _lib.current_stream_handle()))
     ref = u2 / rho - (drho / (rho * rho)) * u1
     _close(out.cpu().numpy(), ref.cpu().numpy(), 1e-13)
+
+
+@pytest.mark.parametrize("bc", ["wall", "periodic"])
+def test_ccd_autotune_is_bitwise_neutral(cuda_device, bc):
+    """The launch-shape autotuner (first call per shape) changes only the
+    speed: tuned, cached and untuned results are bitwise identical."""
+    import torch
+    from twophaseflow_b200 import CCDSolver, _lib
+    shape = _LANE_SHAPES[0]
+    N = tuple(s - 1 for s in shape)
+    grid = _Grid(N, (1.0, 1.0, 1.0))
+    f = torch.from_numpy(fourier_field(N, n_modes=4, kmax=4, seed=5)).to(cuda_device)
+    tuned = CCDSolver(grid, None, bc_type=bc)
+    plain = CCDSolver(grid, None, bc_type=bc)
+    plan = plain._plan(0, bc == "periodic")
+    _lib.check(plain.lib.tpf_ccd_plan_set_autotune(plan, 0))
+    a1, a2 = tuned.differentiate(f, 0)      # tunes
+    b1, b2 = tuned.differentiate(f, 0)      # cached shape
+    c1, c2 = plain.differentiate(f, 0)      # default shape
+    assert torch.equal(a1, c1) and torch.equal(a2, c2)
+    assert torch.equal(b1, c1) and torch.equal(b2, c2)

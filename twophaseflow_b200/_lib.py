@@ -82,6 +82,7 @@ SIGNATURES = {
     "tpf_last_error": (C.c_char_p, []),
     "tpf_ccd_plan_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int64, C.c_double, C.c_int, C.c_int]),
     "tpf_ccd_plan_destroy": (C.c_int, [C.c_void_p]),
+    "tpf_ccd_plan_set_autotune": (C.c_int, [C.c_void_p, C.c_int]),
     "tpf_ccd_plan_set_metric": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "tpf_ccd_apply": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                 C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int, C.c_void_p]),

@@ -29,6 +29,11 @@
 #include <vector>
 #include <array>
 #include <algorithm>
+#include <map>
+
+struct LaneShape_ {
+  int warps, nbuf, max_bps;
+};
 
 namespace {
 
@@ -83,6 +88,9 @@ struct tpf_ccd_plan {
   float* d_ltabf = nullptr;
   int ltab_total = 0;
   std::vector<double> ltab_host;
+  // lane-kernel launch shapes picked by the autotuner, per call signature
+  mutable std::map<uint64_t, LaneShape_> lane_tuned;
+  bool autotune = true;
 };
 
 namespace {
@@ -1598,48 +1606,92 @@ bool use_lane_kernel(const tpf_ccd_plan* p, int64_t n_lines, bool periodic, bool
   return n_lines >= 148LL * 4 * 32;
 }
 
-#ifndef TPF_LANE_WARPS
-#define TPF_LANE_WARPS 4
-#endif
-#ifndef TPF_LANE_MAX_BLOCKS_PER_SM
-#define TPF_LANE_MAX_BLOCKS_PER_SM 64
-#endif
-// f tile ring depth: FP64 keeps two chunks in flight (3 buffers); FP32 gets
-// more resident warps from the smaller 2-buffer ring (measured on B200)
-#ifndef TPF_LANE_NBUF64
-#define TPF_LANE_NBUF64 3
-#endif
-#ifndef TPF_LANE_NBUF32
-#define TPF_LANE_NBUF32 2
-#endif
+// Launch shape of the lane kernel: warps per block, f-tile ring depth, cap on
+// resident blocks per SM.  Every shape computes each line with the same
+// arithmetic, so the results are bitwise identical; only the speed differs.
+using LaneShape = LaneShape_;
 
 template <typename T>
-int launch_lane(const tpf_ccd_plan* p, const CcdArgs& a, bool periodic, bool contig, cudaStream_t stream) {
-  constexpr int W = TPF_LANE_WARPS;
+using LaneFn = void (*)(CcdArgs, const T*, int);
+
+template <typename T, int NB>
+LaneFn<T> lane_fn_nb(bool periodic, bool plain, bool contig) {
+  if (contig)
+    return periodic ? ccd_lane_kernel<T, true, false, NB, true> : ccd_lane_kernel<T, false, false, NB, true>;
+  if (periodic) return plain ? ccd_lane_kernel<T, true, true, NB, false> : ccd_lane_kernel<T, true, false, NB, false>;
+  return plain ? ccd_lane_kernel<T, false, true, NB, false> : ccd_lane_kernel<T, false, false, NB, false>;
+}
+
+template <typename T>
+int run_lane(const tpf_ccd_plan* p, const CcdArgs& a, bool periodic, bool contig, const LaneShape& sh,
+             cudaStream_t stream) {
+  const int W = sh.warps;
   const int P = (p->n_rows + kLaneCR - 1) / kLaneCR;
-  constexpr int NB = std::is_same<T, double>::value ? TPF_LANE_NBUF64 : TPF_LANE_NBUF32;
-  const size_t per_warp = (size_t)(NB + (contig ? 1 : 0)) * (kLaneCR + 2) * (contig ? 33 : 32) + 64 * (size_t)P;
+  const size_t per_warp = (size_t)(sh.nbuf + (contig ? 1 : 0)) * (kLaneCR + 2) * (contig ? 33 : 32) + 64 * (size_t)P;
   const size_t smem = sizeof(T) * ((((size_t)p->ltab_total + 1) & ~(size_t)1) + W * per_warp);
   TPF_CHECK_ARG(smem <= 225 * 1024, "CCD lane kernel: axis of %lld points needs too much shared memory",
                 (long long)p->n_pts);
   const bool plain = a.d1 && a.d2 && !a.vd_out && !a.J;
-  void (*kern)(CcdArgs, const T*, int);
-  if (contig)
-    kern = periodic ? ccd_lane_kernel<T, true, false, NB, true> : ccd_lane_kernel<T, false, false, NB, true>;
-  else if (periodic)
-    kern = plain ? ccd_lane_kernel<T, true, true, NB, false> : ccd_lane_kernel<T, true, false, NB, false>;
-  else
-    kern = plain ? ccd_lane_kernel<T, false, true, NB, false> : ccd_lane_kernel<T, false, false, NB, false>;
+  LaneFn<T> kern = sh.nbuf == 2 ? lane_fn_nb<T, 2>(periodic, plain, contig) : lane_fn_nb<T, 3>(periodic, plain, contig);
   TPF_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   TPF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * W, smem));
-  per_sm = std::max(1, std::min(per_sm, TPF_LANE_MAX_BLOCKS_PER_SM));
+  per_sm = std::max(1, std::min(per_sm, sh.max_bps));
   const int64_t groups = (a.n_lines + 31) / 32;
   const int64_t blocks = std::min<int64_t>((groups + W - 1) / W, (int64_t)tpf::sm_count() * per_sm);
   const T* lt = std::is_same<T, double>::value ? reinterpret_cast<const T*>(p->d_ltab)
                                                : reinterpret_cast<const T*>(p->d_ltabf);
   kern<<<(unsigned)blocks, 32 * W, smem, stream>>>(a, lt, p->ltab_total);
   TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
+// Autotuner: on the first call of a (lines, axis kind, boundary, epilogue,
+// dtype) combination, time the candidate shapes with CUDA events (one warm-up
+// and two timed launches each) and keep the fastest in the plan.  Skipped while
+// the stream is being captured into a graph (the default shape runs).
+template <typename T>
+int launch_lane(const tpf_ccd_plan* p, const CcdArgs& a, bool periodic, bool contig, cudaStream_t stream) {
+  const bool plain = a.d1 && a.d2 && !a.vd_out && !a.J;
+  const uint64_t key = ((uint64_t)a.n_lines << 8) | ((uint64_t)contig << 0) | ((uint64_t)periodic << 1) |
+                       ((uint64_t)plain << 2) | ((uint64_t)(sizeof(T) == 8) << 3);
+  auto it = p->lane_tuned.find(key);
+  if (it != p->lane_tuned.end()) return run_lane<T>(p, a, periodic, contig, it->second, stream);
+  const LaneShape def{4, std::is_same<T, double>::value ? 3 : 2, 64};
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  TPF_CUDA_TRY(cudaStreamIsCapturing(stream, &cs));
+  // an accumulating epilogue must run exactly once: no tuning runs for it
+  if (!p->autotune || cs != cudaStreamCaptureStatusNone || (a.vd_out && a.vd_accumulate))
+    return run_lane<T>(p, a, periodic, contig, def, stream);
+  const LaneShape cand[] = {{4, 3, 64}, {4, 2, 64}, {4, 3, 2}, {4, 2, 3}, {2, 3, 64}, {2, 2, 64}, {4, 2, 2}};
+  cudaEvent_t e0, e1;
+  TPF_CUDA_TRY(cudaEventCreate(&e0));
+  TPF_CUDA_TRY(cudaEventCreate(&e1));
+  float best = 1e30f;
+  LaneShape bs = def;
+  int st = TPF_OK;
+  for (const LaneShape& c : cand) {
+    if ((st = run_lane<T>(p, a, periodic, contig, c, stream))) {
+      if (st != TPF_EINVAL) break;
+      st = TPF_OK;   // a shape that does not fit in shared memory is skipped
+      continue;
+    }
+    cudaEventRecord(e0, stream);
+    for (int r = 0; r < 2 && !st; ++r) st = run_lane<T>(p, a, periodic, contig, c, stream);
+    cudaEventRecord(e1, stream);
+    if (cudaEventSynchronize(e1) != cudaSuccess || st) break;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best) {
+      best = ms;
+      bs = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st) return st;
+  p->lane_tuned[key] = bs;
+  // the results of the last candidate are already in place and identical for every shape
   return TPF_OK;
 }
 
@@ -1651,6 +1703,7 @@ int launch_ccd(const tpf_ccd_plan* p, int64_t outer, int64_t inner, const void* 
   const bool contig = (inner == 1);
   const int64_t n_lines = outer * inner;
   if (n_lines == 0) return TPF_OK;
+  TPF_CHECK_ARG(f != d1 && f != d2 && f != vd_out, "the CCD input must not alias an output array");
   TPF_CHECK_ARG(n_lines < ((int64_t)1 << 31), "too many lines");
   const bool warp = (p->C == 8 || p->C == 16 || p->C == 32) && p->n_rows <= 32 * p->C;
   LaunchShape s = !warp ? pick_shape<T>(p, contig, n_lines)
@@ -1764,6 +1817,13 @@ int tpf_ccd_plan_create(tpf_ccd_plan** out, int64_t n_pts, double h, int bc, int
     }
   }
   *out = p;
+  return TPF_OK;
+}
+
+int tpf_ccd_plan_set_autotune(tpf_ccd_plan* p, int enable) {
+  TPF_CHECK_ARG(p != nullptr, "plan is NULL");
+  p->autotune = enable != 0;
+  if (!enable) p->lane_tuned.clear();
   return TPF_OK;
 }
 

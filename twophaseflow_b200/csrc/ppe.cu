@@ -450,18 +450,28 @@ struct GridSum {
     }
     __syncthreads();
     const bool ok = s_ok != 0;
-    if (threadIdx.x < 32) {
+    // every thread of the block loads partials (one L2 round trip for up to
+    // blockDim.x / 32 blocks per warp), then a fixed-order reduction: warp
+    // sums, then the warp totals in warp order (deterministic)
+    {
+      const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
       double acc[NV];
 #pragma unroll
       for (int k = 0; k < NV; ++k) acc[k] = 0.0;
-      for (unsigned int j = threadIdx.x; j < nb; j += 32) {
+      for (unsigned int j = threadIdx.x; j < nb; j += blockDim.x) {
 #pragma unroll
         for (int k = 0; k < NV; ++k) acc[k] += __ldcg(part + (slot * 8 + k) * nb + j);
       }
 #pragma unroll
       for (int k = 0; k < NV; ++k) {
         acc[k] = tpf::warp_sum(acc[k]);
-        if (threadIdx.x == 0) scratch[224 + k] = acc[k];
+        if (lane == 0) scratch[k * 16 + wid] = acc[k];
+      }
+      __syncthreads();
+      if (threadIdx.x < NV) {
+        double t = 0.0;
+        for (int w = 0; w < nw; ++w) t += scratch[threadIdx.x * 16 + w];
+        scratch[224 + threadIdx.x] = t;
       }
     }
     __syncthreads();
