@@ -258,7 +258,9 @@ int tpf_unet_destroy(tpf_unet* net);
 int tpf_unet_set_params(tpf_unet* net, const float* params, int on_device);
 int tpf_unet_get_params(tpf_unet* net, float* params, int on_device);
 
-/* y[B][H][W] = UNet(in2[B][H][W][2]) (device FP32; BF16 inside).  Synchronizes. */
+/* y[B][H][W] = UNet(in2[B][H][W][4]) (device FP32; BF16 inside).  The four
+ * input channels: scaled residual, density feature, and the scaled couplings
+ * of the operator to the next row / column.  Synchronizes. */
 int tpf_unet_forward(tpf_unet* net, int B, const float* in2, float* y, void* stream);
 /* Parameter gradients (FP32, num_params, device) of sum(dy * y) for the
  * activations of the last tpf_unet_forward with the same B.  Synchronizes. */
@@ -320,10 +322,12 @@ int tpf_lppe_solve(tpf_lppe* lp, const double* rhs, const double* rho, double* p
 int tpf_lppe_precondition(tpf_lppe* lp, const double* r, double* z, int smooth, double omega, void* stream);
 /* Training pair from an error field e of the weighted system (pin 0), in the
  * form the network reads (in2, target: device FP32 on the network image).
- * coarsen = 1: in2 = (D^-1/2 S e / s, density feature), target = D^1/2 e / s
+ * coarsen = 1: in2 = (D^-1/2 S e / s, density feature, couplings of
+ * D^-1/2 S D^-1/2 to the next row / column), target = D^1/2 e / s
  * (s = rms of D^-1/2 S e).  Two-level mode: with r = S e, the pre-smoothing
  * sweep z1 = omega D^-1 r, r1 = r - S z1 and e1 = e - z1,
- * in2 = (D_c^-1/2 R r1 / s_c, aggregate density feature) and
+ * in2 = (D_c^-1/2 R r1 / s_c, aggregate density feature, scaled Galerkin
+ * couplings to the next row / column) and
  * target = D_c^1/2 mean_aggregate(e1) / s_c. */
 int tpf_lppe_pair(tpf_lppe* lp, const double* e, float* in2, float* target, double omega, void* stream);
 /* Two-level mode: the data of the energy loss for an error field e: in2 as

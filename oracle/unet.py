@@ -22,7 +22,7 @@ from __future__ import annotations
 
 import numpy as np
 
-LAYERS = [(2, 16, 0, 1), (16, 16, 0, 1), (16, 32, 1, 1), (32, 32, 1, 1),
+LAYERS = [(4, 16, 0, 1), (16, 16, 0, 1), (16, 32, 1, 1), (32, 32, 1, 1),
           (32, 64, 2, 1), (64, 64, 2, 1), (64, 128, 3, 1), (128, 128, 3, 1),
           (128, 64, 3, 0), (64, 64, 2, 1), (64, 32, 2, 0), (32, 32, 1, 1),
           (32, 16, 1, 0), (16, 16, 0, 1)]
@@ -140,7 +140,7 @@ def downsum(x):
 
 
 def forward(params, in2, precision="bf16"):
-    """y[B,H,W] of the network for in2[B,H,W,2]; returns (y, activations)."""
+    """y[B,H,W] of the network for in2[B,H,W,4]; returns (y, activations)."""
     n = _Net(params, precision)
     x = np.asarray(in2, np.float64)
     x = n.r(x)

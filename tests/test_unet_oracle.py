@@ -21,7 +21,7 @@ def test_backward_matches_finite_differences():
     rng = np.random.default_rng(3)
     p = ou.init_params(seed=1)
     B, H, W = 2, 16, 16
-    x = rng.standard_normal((B, H, W, 2))
+    x = rng.standard_normal((B, H, W, 4))
     dy = rng.standard_normal((B, H, W))
     y, A = ou.forward(p, x, precision="fp64")
     g = ou.backward(p, A, dy, precision="fp64")

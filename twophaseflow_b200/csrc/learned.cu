@@ -23,6 +23,7 @@
 // solution of the same system within the stated tolerance".
 #include "tpf_common.cuh"
 #include "ppe_view.cuh"
+#include "tc_sm100.cuh"
 
 #include <cuda_bf16.h>
 
@@ -165,8 +166,23 @@ __global__ void fcg_start_kernel(const double* part, int nb, int ndof, FcgState*
   }
 }
 
-// network input: channel 0 = D^-1/2 r / s, channel 1 = c~, channels 2..15 = 0
+// network input: channel 0 = D^-1/2 r / s, 1 = c~, 2 / 3 = the Jacobi-scaled
+// couplings to the next row / column (D^-1/2 S D^-1/2 = I - couplings), 4..15 = 0
+__device__ __forceinline__ void fine_coupl(const LGrid& g, int i, int i0, int i1, float& a0, float& a1) {
+  a0 = (i0 + 1 < g.n0) ? (float)(g.s0[i] * sqrt(g.dinvS[i] * g.dinvS[i + g.n1])) : 0.f;
+  a1 = (i1 + 1 < g.n1) ? (float)(g.s1[i] * sqrt(g.dinvS[i] * g.dinvS[i + 1])) : 0.f;
+}
+
+__device__ __forceinline__ uint4 pack4bf(float c0, float c1, float c2, float c3) {
+  uint4 v = make_uint4(0, 0, 0, 0);
+  __nv_bfloat162 h0 = __floats2bfloat162_rn(c0, c1), h1 = __floats2bfloat162_rn(c2, c3);
+  v.x = *reinterpret_cast<uint32_t*>(&h0);
+  v.y = *reinterpret_cast<uint32_t*>(&h1);
+  return v;
+}
+
 __global__ void fcg_pack_kernel(LGrid g, const double* r, const float* feat, const FcgState* st, bf16* xin) {
+  tpf::tc::pdl_trigger();
   if (st->done) return;
   const int Wp = g.W + 2;
   const long long P = (long long)(g.H + 2) * Wp;
@@ -174,19 +190,16 @@ __global__ void fcg_pack_kernel(LGrid g, const double* r, const float* feat, con
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < P; q += (long long)gridDim.x * blockDim.x) {
     const int yy = (int)(q / Wp), xx = (int)(q - (long long)yy * Wp);
     const int y = yy - 1, x = xx - 1;
-    float c0 = 0.f, c1 = 0.f;
+    float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f;
     if (y >= 0 && y < g.n0 && x >= 0 && x < g.n1) {
       const int i = y * g.n1 + x;
       c0 = (float)(r[i] * sqrt(g.dinvS[i])) * inv_s;
       c1 = feat[i];
+      fine_coupl(g, i, y, x, c2, c3);
     }
-    uint4 v0, v1 = make_uint4(0, 0, 0, 0);
-    __nv_bfloat162 h = __floats2bfloat162_rn(c0, c1);
-    v0.x = *reinterpret_cast<uint32_t*>(&h);
-    v0.y = v0.z = v0.w = 0;
     uint4* o = reinterpret_cast<uint4*>(xin + q * 16);
-    o[0] = v0;
-    o[1] = v1;
+    o[0] = pack4bf(c0, c1, c2, c3);
+    o[1] = make_uint4(0, 0, 0, 0);
   }
 }
 
@@ -362,7 +375,7 @@ __global__ void __launch_bounds__(kRedThreads) pair_residual_kernel(LGrid g, con
 }
 
 __global__ void pair_write_kernel(LGrid g, const double* e, const double* r, const float* feat, const double* part,
-                                  int nb, float* in2, float* target) {
+                                  int nb, float* in, float* target) {
   __shared__ double s_inv;
   if (threadIdx.x == 0) {
     double a = 0.0;
@@ -375,16 +388,19 @@ __global__ void pair_write_kernel(LGrid g, const double* e, const double* r, con
   const long long n = (long long)g.H * g.W;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
     const int y = (int)(q / g.W), x = (int)(q - (long long)y * g.W);
-    float a0 = 0.f, a1 = 0.f, t = 0.f;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f, t = 0.f;
     if (y < g.n0 && x < g.n1) {
       const int i = y * g.n1 + x;
       const double d = sqrt(g.dinvS[i]);
       a0 = (float)(r[i] * d * inv_s);
       a1 = feat[i];
+      fine_coupl(g, i, y, x, a2, a3);
       t = (i == g.pin) ? 0.f : (float)(e[i] / d * inv_s);
     }
-    in2[2 * q] = a0;
-    in2[2 * q + 1] = a1;
+    in[4 * q] = a0;
+    in[4 * q + 1] = a1;
+    in[4 * q + 2] = a2;
+    in[4 * q + 3] = a3;
     target[q] = t;
   }
 }
@@ -423,26 +439,33 @@ __global__ void rscale_finish_kernel(const double* part, int nb, int ndof, FcgSt
 
 __device__ __forceinline__ int agg_of(const LGrid& g, int i0, int i1) { return (i0 / g.b) * g.nc1 + i1 / g.b; }
 
-__global__ void coarse_diag_kernel(LGrid g, double* dc) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.ndof; i += gridDim.x * blockDim.x) {
-    const int i0 = i / g.n1, i1 = i - i0 * g.n1;
-    const int I = agg_of(g, i0, i1);
-    if (i0 + 1 < g.n0) {
-      const int J = agg_of(g, i0 + 1, i1);
-      if (J != I) {
-        const double v = g.s0[i];
-        atomicAdd(dc + I, v);
-        atomicAdd(dc + J, v);
+// D_c (sum of the fine couplings crossing the aggregate's boundary) and the
+// Galerkin couplings to the aggregate below / to the right, gathered per
+// aggregate in a fixed order (deterministic, no atomics)
+__global__ void coarse_operator_kernel(LGrid g, double* dc, double* c0, double* c1) {
+  const int nc = g.nc0 * g.nc1;
+  for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += gridDim.x * blockDim.x) {
+    const int I0 = I / g.nc1, I1 = I - I0 * g.nc1;
+    const int a0 = I0 * g.b, a1 = I1 * g.b;
+    const int e0 = min(g.n0, a0 + g.b), e1 = min(g.n1, a1 + g.b);
+    double d = 0.0, down = 0.0, right = 0.0;
+    for (int i0 = a0; i0 < e0; ++i0)
+      for (int i1 = a1; i1 < e1; ++i1) {
+        const int i = i0 * g.n1 + i1;
+        if (i0 == a0 && i0 > 0) d += g.s0[i - g.n1];
+        if (i0 == e0 - 1 && i0 + 1 < g.n0) {
+          d += g.s0[i];
+          down += g.s0[i];
+        }
+        if (i1 == a1 && i1 > 0) d += g.s1[i - 1];
+        if (i1 == e1 - 1 && i1 + 1 < g.n1) {
+          d += g.s1[i];
+          right += g.s1[i];
+        }
       }
-    }
-    if (i1 + 1 < g.n1) {
-      const int J = agg_of(g, i0, i1 + 1);
-      if (J != I) {
-        const double v = g.s1[i];
-        atomicAdd(dc + I, v);
-        atomicAdd(dc + J, v);
-      }
-    }
+    dc[I] = d;
+    c0[I] = down;
+    c1[I] = right;
   }
 }
 
@@ -514,8 +537,17 @@ __global__ void coarse_scale_kernel(const double* part, int nb, int nc, FcgState
   }
 }
 
-// network input on the coarse image: (D_c^-1/2 rc / s_c, c~_c)
-__global__ void pack_coarse_kernel(LGrid g, const double* rc, const FcgState* st, bf16* xin) {
+// scaled Galerkin couplings of aggregate I to the next row / column
+__device__ __forceinline__ void coarse_coupl(const LGrid& g, const double* cc0, const double* cc1, int I, int y,
+                                             int x, float& a0, float& a1) {
+  a0 = (y + 1 < g.nc0) ? (float)(cc0[I] * g.dcis[I] * g.dcis[I + g.nc1]) : 0.f;
+  a1 = (x + 1 < g.nc1) ? (float)(cc1[I] * g.dcis[I] * g.dcis[I + 1]) : 0.f;
+}
+
+// network input on the coarse image: (D_c^-1/2 rc / s_c, c~_c, coarse couplings)
+__global__ void pack_coarse_kernel(LGrid g, const double* rc, const double* cc0, const double* cc1,
+                                   const FcgState* st, bf16* xin) {
+  tpf::tc::pdl_trigger();
   if (st->done) return;
   const int Wp = g.W + 2;
   const long long P = (long long)(g.H + 2) * Wp;
@@ -523,19 +555,16 @@ __global__ void pack_coarse_kernel(LGrid g, const double* rc, const FcgState* st
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < P; q += (long long)gridDim.x * blockDim.x) {
     const int yy = (int)(q / Wp), xx = (int)(q - (long long)yy * Wp);
     const int y = yy - 1, x = xx - 1;
-    float c0 = 0.f, c1 = 0.f;
+    float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f;
     if (y >= 0 && y < g.nc0 && x >= 0 && x < g.nc1) {
       const int I = y * g.nc1 + x;
       c0 = (float)(rc[I] * g.dcis[I] * inv);
       c1 = g.featc[I];
+      coarse_coupl(g, cc0, cc1, I, y, x, c2, c3);
     }
-    uint4 v0, v1 = make_uint4(0, 0, 0, 0);
-    __nv_bfloat162 h = __floats2bfloat162_rn(c0, c1);
-    v0.x = *reinterpret_cast<uint32_t*>(&h);
-    v0.y = v0.z = v0.w = 0;
     uint4* o = reinterpret_cast<uint4*>(xin + q * 16);
-    o[0] = v0;
-    o[1] = v1;
+    o[0] = pack4bf(c0, c1, c2, c3);
+    o[1] = make_uint4(0, 0, 0, 0);
   }
 }
 
@@ -584,8 +613,9 @@ __global__ void prolong_smooth_kernel(LGrid g, const float* y, const double* r, 
 
 // training pair of the coarse problem: e1 = e - w D^-1 r (error after the
 // pre-smoothing sweep), target = D_c^1/2 mean_I(e1) / s_c on the coarse image
-__global__ void pair_coarse_write_kernel(LGrid g, const double* e, const double* r, const double* rc, double omega,
-                                         const double* part, int nb, float* in2, float* target) {
+__global__ void pair_coarse_write_kernel(LGrid g, const double* e, const double* r, const double* rc,
+                                         const double* cc0, const double* cc1, double omega, const double* part,
+                                         int nb, float* in, float* target) {
   __shared__ double s_inv;
   if (threadIdx.x == 0) {
     double a = 0.0;
@@ -598,7 +628,7 @@ __global__ void pair_coarse_write_kernel(LGrid g, const double* e, const double*
   const long long n = (long long)g.H * g.W;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
     const int y = (int)(q / g.W), x = (int)(q - (long long)y * g.W);
-    float a0 = 0.f, a1 = 0.f, t = 0.f;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f, t = 0.f;
     if (y < g.nc0 && x < g.nc1) {
       const int I = y * g.nc1 + x;
       double acc = 0.0;
@@ -612,10 +642,13 @@ __global__ void pair_coarse_write_kernel(LGrid g, const double* e, const double*
       const double d = g.dcis[I];
       a0 = (float)(rc[I] * d * inv);
       a1 = g.featc[I];
+      coarse_coupl(g, cc0, cc1, I, y, x, a2, a3);
       t = (d > 0.0) ? (float)((acc / cnt) / d * inv) : 0.f;
     }
-    in2[2 * q] = a0;
-    in2[2 * q + 1] = a1;
+    in[4 * q] = a0;
+    in[4 * q + 1] = a1;
+    in[4 * q + 2] = a2;
+    in[4 * q + 3] = a3;
     target[q] = t;
   }
 }
@@ -624,16 +657,6 @@ __global__ void pair_coarse_write_kernel(LGrid g, const double* e, const double*
 // coarse operator on the network image (coupl[q][0]: to the next row,
 // coupl[q][1]: to the next column; A~ = D_c^-1/2 A_c D_c^-1/2 = I - couplings)
 // and E~ = (e1 . S e1) / s_c^2 = (e1 . r1) / s_c^2
-__global__ void coarse_coupl_kernel(LGrid g, double* c0, double* c1) {
-  // c0[I]: sum of fine couplings between aggregate I and the one below; c1: to the right
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.ndof; i += gridDim.x * blockDim.x) {
-    const int i0 = i / g.n1, i1 = i - i0 * g.n1;
-    const int I = agg_of(g, i0, i1);
-    if (i0 + 1 < g.n0 && agg_of(g, i0 + 1, i1) != I) atomicAdd(c0 + I, g.s0[i]);
-    if (i1 + 1 < g.n1 && agg_of(g, i0, i1 + 1) != I) atomicAdd(c1 + I, g.s1[i]);
-  }
-}
-
 __global__ void coarse_coupl_write_kernel(LGrid g, const double* c0, const double* c1, float* coupl) {
   const long long n = (long long)g.H * g.W;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
@@ -731,11 +754,7 @@ int features(tpf_lppe* lp, const double* rho, cudaStream_t s) {
   feature_kernel<<<ew_blocks(lp->g.ndof), 256, 0, s>>>(lp->g.ndof, rho, lp->rmax, lp->feat);
   if (lp->g.b > 1) {
     const int nc = lp->g.nc0 * lp->g.nc1;
-    TPF_CUDA_TRY(cudaMemsetAsync(lp->dc, 0, sizeof(double) * nc, s));
-    TPF_CUDA_TRY(cudaMemsetAsync(lp->cc0, 0, sizeof(double) * nc, s));
-    TPF_CUDA_TRY(cudaMemsetAsync(lp->cc1, 0, sizeof(double) * nc, s));
-    coarse_diag_kernel<<<ew_blocks(lp->g.ndof), 256, 0, s>>>(lp->g, lp->dc);
-    coarse_coupl_kernel<<<ew_blocks(lp->g.ndof), 256, 0, s>>>(lp->g, lp->cc0, lp->cc1);
+    coarse_operator_kernel<<<ew_blocks(nc), 256, 0, s>>>(lp->g, lp->dc, lp->cc0, lp->cc1);
     coarse_setup_kernel<<<ew_blocks(nc), 256, 0, s>>>(lp->g, lp->dc, lp->feat, lp->dcis, lp->featc);
   }
   TPF_CUDA_TRY(cudaGetLastError());
@@ -751,7 +770,8 @@ int enqueue_precond(tpf_lppe* lp, int smooth, double omega, cudaStream_t s, doub
     vc_pre_kernel<<<ew_blocks(g.ndof), 256, 0, s>>>(g, lp->r, omega, lp->st, lp->r1);
     restrict_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(g, lp->r1, lp->rc, lp->st, lp->part);
     coarse_scale_kernel<<<1, 256, 0, s>>>(lp->part, kRedBlocks, nc, lp->st);
-    pack_coarse_kernel<<<ew_blocks((g.H + 2) * (g.W + 2)), 256, 0, s>>>(g, lp->rc, lp->st, tpf::unet_input(lp->net));
+    pack_coarse_kernel<<<ew_blocks((g.H + 2) * (g.W + 2)), 256, 0, s>>>(g, lp->rc, lp->cc0, lp->cc1, lp->st,
+                                                                         tpf::unet_input(lp->net));
     TPF_CUDA_TRY(cudaGetLastError());
     int st = tpf::unet_forward_packed(lp->net, 1, s);
     if (st) return st;
@@ -788,21 +808,29 @@ int enqueue_precond(tpf_lppe* lp, int smooth, double omega, cudaStream_t s, doub
   return TPF_OK;
 }
 
+// one flexible-CG step with M stored directions (the window length picks the instance)
+template <int M>
+void enqueue_fcg_step(tpf_lppe* lp, const double* z, cudaStream_t s) {
+  const LGrid& g = lp->g;
+  fcg_sdot_kernel<M><<<kRedBlocks, kRedThreads, 0, s>>>(g, z, lp->r, lp->pp, lp->qp, lp->w, lp->st, lp->part);
+  fcg_coef_kernel<M><<<1, 256, 0, s>>>(lp->part, kRedBlocks, lp->st);
+  fcg_update_kernel<M><<<kRedBlocks, kRedThreads, 0, s>>>(g, z, lp->w, lp->pp, lp->qp, lp->x, lp->r, lp->st,
+                                                          lp->part);
+}
+
 int enqueue_iteration(tpf_lppe* lp, int smooth, double omega, cudaStream_t s) {
   double* z = nullptr;
   int st = enqueue_precond(lp, smooth, omega, s, &z);
   if (st) return st;
   const LGrid& g = lp->g;
   if (lp->win <= 1) {
-    fcg_sdot_kernel<1><<<kRedBlocks, kRedThreads, 0, s>>>(g, z, lp->r, lp->pp, lp->qp, lp->w, lp->st, lp->part);
-    fcg_coef_kernel<1><<<1, 256, 0, s>>>(lp->part, kRedBlocks, lp->st);
-    fcg_update_kernel<1><<<kRedBlocks, kRedThreads, 0, s>>>(g, z, lp->w, lp->pp, lp->qp, lp->x, lp->r, lp->st,
-                                                            lp->part);
+    enqueue_fcg_step<1>(lp, z, s);
+  } else if (lp->win <= 2) {
+    enqueue_fcg_step<2>(lp, z, s);
+  } else if (lp->win <= 4) {
+    enqueue_fcg_step<4>(lp, z, s);
   } else {
-    fcg_sdot_kernel<kMaxWin><<<kRedBlocks, kRedThreads, 0, s>>>(g, z, lp->r, lp->pp, lp->qp, lp->w, lp->st, lp->part);
-    fcg_coef_kernel<kMaxWin><<<1, 256, 0, s>>>(lp->part, kRedBlocks, lp->st);
-    fcg_update_kernel<kMaxWin><<<kRedBlocks, kRedThreads, 0, s>>>(g, z, lp->w, lp->pp, lp->qp, lp->x, lp->r, lp->st,
-                                                       lp->part);
+    enqueue_fcg_step<kMaxWin>(lp, z, s);
   }
   fcg_finish_iter_kernel<<<1, 256, 0, s>>>(lp->part, kRedBlocks, g.ndof, lp->st);
   TPF_CUDA_TRY(cudaGetLastError());
@@ -868,7 +896,7 @@ void tpf_lppe_default_options(tpf_learned_options* o) {
   o->stall_factor = 0.5;
   o->fallback = 1;
   o->use_graph = 1;
-  o->window = 1;
+  o->window = 8;
 }
 
 int tpf_lppe_create(tpf_lppe** out, tpf_ppe* ppe, tpf_unet* net, int coarsen) {
@@ -968,8 +996,8 @@ int tpf_lppe_pair(tpf_lppe* lp, const double* e, float* in2, float* target, doub
     pair_residual_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(lp->g, e, lp->r, lp->part);
     vc_pre_kernel<<<ew_blocks(lp->g.ndof), 256, 0, s>>>(lp->g, lp->r, omega, nullptr, lp->r1);
     restrict_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(lp->g, lp->r1, lp->rc, nullptr, lp->part);
-    pair_coarse_write_kernel<<<ew_blocks(lp->g.H * lp->g.W), 256, 0, s>>>(lp->g, e, lp->r, lp->rc, omega, lp->part,
-                                                                         kRedBlocks, in2, target);
+    pair_coarse_write_kernel<<<ew_blocks(lp->g.H * lp->g.W), 256, 0, s>>>(lp->g, e, lp->r, lp->rc, lp->cc0, lp->cc1,
+                                                                         omega, lp->part, kRedBlocks, in2, target);
     TPF_CUDA_TRY(cudaGetLastError());
     return TPF_OK;
   }
@@ -991,8 +1019,9 @@ int tpf_lppe_pair_energy(tpf_lppe* lp, const double* e, float* in2, float* coupl
   vc_pre_kernel<<<ew_blocks(g.ndof), 256, 0, s>>>(g, lp->r, omega, nullptr, lp->r1);
   restrict_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(g, lp->r1, lp->rc, nullptr, lp->part);
   // in2 (channel 0 = scaled restricted residual, channel 1 = feature); the target is unused
-  pair_coarse_write_kernel<<<ew_blocks(g.H * g.W), 256, 0, s>>>(g, e, lp->r, lp->rc, omega, lp->part, kRedBlocks,
-                                                                in2, reinterpret_cast<float*>(lp->z2));
+  pair_coarse_write_kernel<<<ew_blocks(g.H * g.W), 256, 0, s>>>(g, e, lp->r, lp->rc, lp->cc0, lp->cc1, omega,
+                                                                lp->part, kRedBlocks, in2,
+                                                                reinterpret_cast<float*>(lp->z2));
   energy_partials_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(g, e, lp->r, lp->r1, omega, lp->part2);
   energy_scale_kernel<<<1, 256, 0, s>>>(g, lp->part2, lp->part, kRedBlocks, escale);
   coarse_coupl_write_kernel<<<ew_blocks(g.H * g.W), 256, 0, s>>>(g, lp->cc0, lp->cc1, coupl);

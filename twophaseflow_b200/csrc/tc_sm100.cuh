@@ -13,6 +13,12 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
+// ---- programmatic dependent launch ----------------------------------------------
+// wait until the preceding grid has completed and its memory is visible
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+// let the next grid (launched with programmatic stream serialization) start
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
 // ---- cp.async (16-byte, zero-filled when !valid) -------------------------------
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
   const int n = valid ? 16 : 0;

@@ -7,7 +7,7 @@
 // The reference has no learned component (its PPE is SciPy CG/GMRES), so the
 // network is this library's own design:
 //
-//   encoder  e0 = R(c1(R(c0(x))))            level 0  16 ch   (x = [r~, c~])
+//   encoder  e0 = R(c1(R(c0(x))))            level 0  16 ch   (x = [r~, c~, a~0, a~1])
 //            e1 = R(c3(R(c2(pool e0))))      level 1  32 ch
 //            e2 = R(c5(R(c4(pool e1))))      level 2  64 ch
 //            e3 = R(c7(R(c6(pool e2))))      level 3 128 ch
@@ -46,8 +46,9 @@ constexpr int kConvs = 14;
 struct LayerSpec {
   int cin, cout, level, relu;
 };
-// cin of layer 0 is the 2 logical input channels; its kernel input is padded to 16
-constexpr LayerSpec kLayers[kConvs] = {{2, 16, 0, 1},   {16, 16, 0, 1},  {16, 32, 1, 1}, {32, 32, 1, 1},
+// cin of layer 0 is the 4 logical input channels; its kernel input is padded to 16
+constexpr int kIn = 4;
+constexpr LayerSpec kLayers[kConvs] = {{4, 16, 0, 1},   {16, 16, 0, 1},  {16, 32, 1, 1}, {32, 32, 1, 1},
                                        {32, 64, 2, 1},  {64, 64, 2, 1},  {64, 128, 3, 1}, {128, 128, 3, 1},
                                        {128, 64, 3, 0}, {64, 64, 2, 1},  {64, 32, 2, 0}, {32, 32, 1, 1},
                                        {32, 16, 1, 0},  {16, 16, 0, 1}};
@@ -134,6 +135,7 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(ConvArgs a) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const long long q0 = (long long)blockIdx.x * kTile;
 
+  pdl_trigger();   // the next layer may start its prologue
   if (warp == 0) tmem_alloc(&tmem_slot, NCOLS);
   if (tid == 0) {
     mbar_init(&mbar, 1);
@@ -143,6 +145,15 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(ConvArgs a) {
   __syncthreads();
   fence_after_sync();
   const uint32_t tmem = tmem_slot;
+
+  // the first tap group's weights do not depend on the previous layer: load
+  // them before waiting for it
+  {
+    const unsigned char* wsrc = reinterpret_cast<const unsigned char*>(a.w);
+    for (int i = tid; i < TG * TAP_W / 16; i += 128) cp_async16(sB + i * 16, wsrc + i * 16, true);
+    cp_async_commit();
+  }
+  pdl_wait();
 
   // three input windows (rows dy = -1, 0, +1), 130 pixels each, channel-plane layout
   for (int i = tid; i < 3 * kWin * KCH; i += 128) {
@@ -159,9 +170,11 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(ConvArgs a) {
   bool ok = true;
   uint32_t phase = 0;
   for (int t0 = 0; t0 < 9; t0 += TG) {
-    const unsigned char* wsrc = reinterpret_cast<const unsigned char*>(a.w) + (size_t)t0 * TAP_W;
-    for (int i = tid; i < TG * TAP_W / 16; i += 128) cp_async16(sB + i * 16, wsrc + i * 16, true);
-    cp_async_commit();
+    if (t0 > 0) {
+      const unsigned char* wsrc = reinterpret_cast<const unsigned char*>(a.w) + (size_t)t0 * TAP_W;
+      for (int i = tid; i < TG * TAP_W / 16; i += 128) cp_async16(sB + i * 16, wsrc + i * 16, true);
+      cp_async_commit();
+    }
     cp_async_wait_all();
     fence_proxy_async_smem();
     __syncthreads();
@@ -267,6 +280,7 @@ __device__ __forceinline__ bool pix(const LevelGeom& g, long long q, int& b, int
 // out(level l+1) = 2x2 average of in(level l); C channels; one thread per 8 channels
 template <int C>
 __global__ void pool_kernel(LevelGeom gi, LevelGeom go, const bf16* in, bf16* out) {
+  tpf::tc::pdl_trigger();
   constexpr int K = C / 8;
   const long long n = go.P() * K;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -292,6 +306,7 @@ __global__ void pool_kernel(LevelGeom gi, LevelGeom go, const bf16* in, bf16* ou
 // out(level l) = relu(up(t)(level l+1 -> l) + skip)
 template <int C>
 __global__ void upadd_relu_kernel(LevelGeom gf, LevelGeom gc, const bf16* t, const bf16* skip, bf16* out) {
+  tpf::tc::pdl_trigger();
   constexpr int K = C / 8;
   const long long n = gf.P() * K;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -359,17 +374,18 @@ __global__ void pool_bwd_kernel(LevelGeom gf, LevelGeom gc, const bf16* dP, cons
   }
 }
 
-// input [B][H][W][2] FP32 -> xin (16 channels, 0..1 used)
-__global__ void pack_input_kernel(LevelGeom g, const float* in2, bf16* xin) {
+// input [B][H][W][kIn] FP32 -> xin (16 channels, 0..kIn-1 used)
+__global__ void pack_input_kernel(LevelGeom g, const float* in, bf16* xin) {
+  tpf::tc::pdl_trigger();
   const long long n = g.P();
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
     int b, y, x;
     float f0[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     float f1[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     if (pix(g, q, b, y, x)) {
-      const long long s = (((long long)b * g.H + y) * g.W + x) * 2;
-      f0[0] = in2[s];
-      f0[1] = in2[s + 1];
+      const long long s = (((long long)b * g.H + y) * g.W + x) * kIn;
+#pragma unroll
+      for (int c = 0; c < kIn; ++c) f0[c] = in[s + c];
     }
     uint4* o = reinterpret_cast<uint4*>(xin + q * kInPad);
     o[0] = pack8(f0);
@@ -573,7 +589,7 @@ __global__ void loss_grad_kernel(int B, long long npix, const float* y, const fl
 }
 
 // Energy loss of a coarse-grid correction (two-level preconditioner training):
-// per sample b, with y the network output on the coarse image, x = in2[..,0]
+// per sample b, with y the network output on the coarse image, x = in[..,0]
 // the scaled coarse residual and A~ = I - (couplings c0 to the next row, c1 to
 // the next column; unit diagonal inside the nc0 x nc1 coarse grid),
 //   L_b = (y.A~y - 2 y.x) / E_b + 1  = ||e1 - P y^||_A^2 / ||e1||_A^2,
@@ -584,7 +600,7 @@ __global__ void energy_terms_kernel(int B, int H, int W, int nc0, int nc1, const
   const int b = blockIdx.y;
   const long long npix = (long long)H * W;
   const float* yb = y + b * npix;
-  const float* xb = in2 + b * npix * 2;
+  const float* xb = in2 + b * npix * kIn;
   const float* cb = coupl + b * npix * 2;
   double acc = 0.0;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < npix; q += (long long)gridDim.x * blockDim.x) {
@@ -597,7 +613,7 @@ __global__ void energy_terms_kernel(int B, int H, int W, int nc0, int nc1, const
       if (i > 0) ay -= cb[2 * (q - W)] * yb[q - W];
       if (j + 1 < nc1) ay -= cb[2 * q + 1] * yb[q + 1];
       if (j > 0) ay -= cb[2 * (q - 1) + 1] * yb[q - 1];
-      const float xv = xb[2 * q];
+      const float xv = xb[kIn * q];
       acc += (double)yv * ((double)ay - 2.0 * (double)xv);
       g = ay - xv;
     }
@@ -638,8 +654,19 @@ int launch_conv_t(const ConvArgs& a, cudaStream_t s) {
     attr = true;
   }
   const long long tiles = (a.P + kTile - 1) / kTile;
-  conv3x3_tc_kernel<CIN, COUT><<<(unsigned)tiles, 128, smem, s>>>(a);
-  TPF_CUDA_TRY(cudaGetLastError());
+  // programmatic dependent launch: the prologue overlaps the previous kernel,
+  // whose outputs are read only after griddepcontrol.wait
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)tiles);
+  cfg.blockDim = dim3(128);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute pdl[1];
+  pdl[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  pdl[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = pdl;
+  cfg.numAttrs = 1;
+  TPF_CUDA_TRY(cudaLaunchKernelEx(&cfg, conv3x3_tc_kernel<CIN, COUT>, a));
   return TPF_OK;
 }
 

@@ -36,8 +36,11 @@ from .ppe import PPESolverFVMMatrixFree
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_WEIGHTS = os.path.join(HERE, "weights", "unet_ppe.npz")
 
-# (cin, cout) of the 14 convolutions, then the 16 -> 1 output layer
-LAYERS = [(2, 16), (16, 16), (16, 32), (32, 32), (32, 64), (64, 64), (64, 128), (128, 128),
+# (cin, cout) of the 14 convolutions, then the 16 -> 1 output layer; the 4 input
+# channels are the scaled residual, the density feature and the two scaled
+# couplings of the (fine or coarse) operator to the next row / column
+IN_CHANNELS = 4
+LAYERS = [(4, 16), (16, 16), (16, 32), (32, 32), (32, 64), (64, 64), (64, 128), (128, 128),
           (128, 64), (64, 64), (64, 32), (32, 32), (32, 16), (16, 16)]
 
 
@@ -114,7 +117,7 @@ class UNet:
         return a
 
     def forward(self, in2):
-        """y[B,H,W] for in2[B,H,W,2] (FP32 CUDA tensor)."""
+        """y[B,H,W] for in2[B,H,W,IN_CHANNELS] (FP32 CUDA tensor)."""
         torch = _torch()
         x = in2.to(torch.float32).contiguous()
         B = int(x.shape[0])
@@ -194,7 +197,7 @@ class PPESolverLearned(PPESolverFVMMatrixFree):
         self.fallback = bool(getattr(solver_cfg, "ppe_learned_fallback", True))
         self.learned_maxiter = int(getattr(solver_cfg, "ppe_learned_maxiter", max(self.maxiter, 2000)))
         self.coarsen = int(getattr(solver_cfg, "ppe_learned_coarsen", 4))
-        self.window = int(getattr(solver_cfg, "ppe_learned_window", 1))
+        self.window = int(getattr(solver_cfg, "ppe_learned_window", 8))
         if params is None:
             params = load_params(str(getattr(solver_cfg, "ppe_learned_weights", DEFAULT_WEIGHTS)))
         H, W = net_image(self.grid.shape, self.coarsen)
@@ -326,7 +329,7 @@ def generate_pairs(N=(256, 256), n_cases: int = 64, snapshots=(0, 3, 10, 30, 80,
     _lib.check(lib.tpf_lppe_create(C.byref(lp), ppe._handle, net.handle, int(coarsen)))
     M = n_cases * len(snapshots)
     dev = torch.device("cuda")
-    in2 = torch.empty((M, H, W, 2), dtype=torch.float32, device=dev)
+    in2 = torch.empty((M, H, W, IN_CHANNELS), dtype=torch.float32, device=dev)
     if energy:
         tgt = torch.empty((M, H, W, 2), dtype=torch.float32, device=dev)
         esc = torch.empty((M,), dtype=torch.float64, device=dev)
