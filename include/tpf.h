@@ -257,6 +257,13 @@ int tpf_unet_destroy(tpf_unet* net);
 /* Copy the FP32 master parameters in / out (host or device pointer). */
 int tpf_unet_set_params(tpf_unet* net, const float* params, int on_device);
 int tpf_unet_get_params(tpf_unet* net, float* params, int on_device);
+/* How the forward pass is launched: 0 (default; -1 restores it) = one launch
+ * per layer, programmatic dependent launch between them; 1 = the whole
+ * network in one persistent cooperative launch (one CTA per SM, grid
+ * barriers between layers, deep layers' output channels split over CTAs).
+ * Both give the same outputs bit for bit; the persistent launch is faster
+ * for a stand-alone call, the layered one inside a CUDA graph. */
+int tpf_unet_set_forward_mode(tpf_unet* net, int mode);
 
 /* y[B][H][W] = UNet(in2[B][H][W][4]) (device FP32; BF16 inside).  The four
  * input channels: scaled residual, density feature, and the scaled couplings

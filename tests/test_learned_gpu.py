@@ -40,6 +40,38 @@ def test_unet_forward_matches_oracle(cuda_device, H, W, B):
     assert np.abs(y - yo).mean() / np.abs(yo).mean() < 1e-2
 
 
+@pytest.mark.parametrize("H,W,B", [(136, 136, 1), (64, 48, 3), (16, 16, 2), (8, 8, 1)])
+def test_persistent_forward_matches_layered(cuda_device, H, W, B):
+    """The one-launch forward (grid barriers, output channels split over
+    CTAs, fused 1x1 output) gives the layered forward's outputs bit for bit:
+    every output element sees the same MMA sequence, only the MMA width
+    differs."""
+    import torch
+    rng = np.random.default_rng(5)
+    p = ou.init_params(seed=4)
+    offs = ou.param_layout()[0]
+    for l in (0, 6, 8, 13):
+        p[offs[l][1]:offs[l][1] + ou.LAYERS[l][1]] = rng.uniform(-0.1, 0.1, ou.LAYERS[l][1])
+    x = torch.from_numpy(rng.standard_normal((B, H, W, 4)).astype(np.float32)).to(cuda_device)
+    net = _net(H, W, B, p)
+    net.set_forward_mode(0)
+    y0 = net.forward(x)
+    net.set_forward_mode(1)
+    y1 = net.forward(x)
+    y1b = net.forward(x)
+    assert torch.equal(y1, y1b)
+    assert float(y0.abs().max()) > 0
+    assert torch.equal(y0, y1), float((y0 - y1).abs().max())
+    # backward after a persistent forward uses the activations it stored
+    dy = torch.from_numpy(rng.standard_normal((B, H, W)).astype(np.float32)).to(cuda_device)
+    g1 = net.backward(dy).clone()
+    net.set_forward_mode(0)
+    net.forward(x)
+    g0 = net.backward(dy)
+    # weight gradients accumulate with atomics: equal up to summation order
+    assert float((g0 - g1).norm() / g0.norm()) < 1e-5
+
+
 def _layer_rel(g, ref):
     offs, wo, bo, _ = ou.param_layout()
     segs = [(w, b + ou.LAYERS[l][1]) for l, (w, b) in enumerate(offs)] + [(wo, bo + 1)]

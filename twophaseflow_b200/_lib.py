@@ -110,6 +110,7 @@ SIGNATURES = {
     "tpf_unet_destroy": (C.c_int, [C.c_void_p]),
     "tpf_unet_set_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "tpf_unet_get_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "tpf_unet_set_forward_mode": (C.c_int, [C.c_void_p, C.c_int]),
     "tpf_unet_forward": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tpf_unet_backward": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "tpf_unet_train_step": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_float, C.c_float,

@@ -112,6 +112,35 @@ __device__ __forceinline__ bool interior_pixel(long long q, int Hp, int Wp) {
   return yy >= 1 && yy <= Hp - 2 && xx >= 1 && xx <= Wp - 2;
 }
 
+// Three input windows (rows dy = -1, 0, +1 of 130 pixels, zero outside the
+// batch) in channel-plane layout: plane c holds channels [8c, 8c+8) of the
+// 130 pixels as 16-byte rows (K-major SWIZZLE_NONE core matrices).  Lanes
+// 8k..8k+7 of a warp take 8 consecutive pixels of one channel chunk, so each
+// warp writes whole 128-byte plane rows (no shared-memory bank conflicts;
+// the plane stride of 2080 bytes would otherwise put 8 lanes on the same
+// banks) and reads whole 32-byte sectors of the pixel-major input.  For
+// 128-thread CTAs.
+template <int CIN>
+__device__ __forceinline__ void load_windows(const bf16* in, long long P, int Wp, long long q0, unsigned char* sA) {
+  constexpr int KCH = CIN / 8;
+  constexpr int WIN_BYTES = KCH * kPlane;
+  constexpr int N = ((kWin + 7) / 8) * KCH * 8;   // 17 blocks of 8 pixels x chunks x 8 lanes
+#pragma unroll 1
+  for (int w = 0; w < 3; ++w) {
+    const long long qw = q0 - 1 + (long long)(w - 1) * Wp;
+    for (int i = threadIdx.x; i < N; i += 128) {
+      const int rest = i >> 3;
+      const int c = rest % KCH, j = (rest / KCH) * 8 + (i & 7);
+      if (j < kWin) {
+        const long long q = qw + j;
+        const bool valid = (q >= 0 && q < P);
+        tpf::tc::cp_async16(sA + w * WIN_BYTES + c * kPlane + j * 16, in + (valid ? q : 0) * CIN + c * 8, valid);
+      }
+    }
+  }
+  tpf::tc::cp_async_commit();
+}
+
 // One 128-pixel tile of a 3x3 convolution as an implicit GEMM on tcgen05:
 // D[pixel][co] = sum_{tap, ci} X[pixel + shift(tap)][ci] * W[tap][co][ci].
 // 4 warps; thread 0 issues the MMAs, all warps run the TMEM epilogue.
@@ -155,17 +184,7 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(ConvArgs a) {
   }
   pdl_wait();
 
-  // three input windows (rows dy = -1, 0, +1), 130 pixels each, channel-plane layout
-  for (int i = tid; i < 3 * kWin * KCH; i += 128) {
-    const int w = i / (kWin * KCH);
-    const int rem = i - w * (kWin * KCH);
-    const int j = rem / KCH, c = rem - j * KCH;
-    const long long q = q0 - 1 + (long long)(w - 1) * a.Wp + j;
-    const bool valid = (q >= 0 && q < a.P);
-    const bf16* src = a.in + (valid ? q : 0) * CIN + c * 8;
-    cp_async16(sA + w * WIN_BYTES + c * kPlane + j * 16, src, valid);
-  }
-  cp_async_commit();
+  load_windows<CIN>(a.in, a.P, a.Wp, q0, sA);
 
   bool ok = true;
   uint32_t phase = 0;
@@ -277,52 +296,79 @@ __device__ __forceinline__ bool pix(const LevelGeom& g, long long q, int& b, int
   return yy >= 1 && yy <= g.H && xx >= 1 && xx <= g.W;
 }
 
-// out(level l+1) = 2x2 average of in(level l); C channels; one thread per 8 channels
+// Per-item bodies of the resampling layers, shared by the standalone kernels
+// and the persistent forward.  Inputs are read through L2 (ld.global.cg):
+// inside the persistent forward they were written by other SMs in an
+// earlier stage of the same launch.
+
+// out(level l+1) = 2x2 average of in(level l); item i = (pixel, 8-channel group)
 template <int C>
-__global__ void pool_kernel(LevelGeom gi, LevelGeom go, const bf16* in, bf16* out) {
-  tpf::tc::pdl_trigger();
+__device__ __forceinline__ void pool_item(const LevelGeom& gi, const LevelGeom& go, const bf16* in, bf16* out,
+                                          long long i) {
   constexpr int K = C / 8;
-  const long long n = go.P() * K;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const long long q = i / K;
-    const int c = (int)(i - q * K);
-    int b, y, x;
-    float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    if (pix(go, q, b, y, x)) {
+  const long long q = i / K;
+  const int c = (int)(i - q * K);
+  int b, y, x;
+  float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (pix(go, q, b, y, x)) {
 #pragma unroll
-      for (int dy = 0; dy < 2; ++dy)
+    for (int dy = 0; dy < 2; ++dy)
 #pragma unroll
-        for (int dx = 0; dx < 2; ++dx) {
-          float f[8];
-          unpack8(reinterpret_cast<const uint4*>(in + gi.q(b, 2 * y + dy, 2 * x + dx) * C)[c], f);
+      for (int dx = 0; dx < 2; ++dx) {
+        float f[8];
+        unpack8(__ldcg(reinterpret_cast<const uint4*>(in + gi.q(b, 2 * y + dy, 2 * x + dx) * C) + c), f);
 #pragma unroll
-          for (int k = 0; k < 8; ++k) acc[k] += 0.25f * f[k];
-        }
-    }
-    reinterpret_cast<uint4*>(out + q * C)[c] = pack8(acc);
+        for (int k = 0; k < 8; ++k) acc[k] += 0.25f * f[k];
+      }
   }
+  reinterpret_cast<uint4*>(out + q * C)[c] = pack8(acc);
 }
 
 // out(level l) = relu(up(t)(level l+1 -> l) + skip)
 template <int C>
+__device__ __forceinline__ void upadd_item(const LevelGeom& gf, const LevelGeom& gc, const bf16* t, const bf16* skip,
+                                           bf16* out, long long i) {
+  constexpr int K = C / 8;
+  const long long q = i / K;
+  const int c = (int)(i - q * K);
+  int b, y, x;
+  float o[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (pix(gf, q, b, y, x)) {
+    float f[8], s[8];
+    unpack8(__ldcg(reinterpret_cast<const uint4*>(t + gc.q(b, y >> 1, x >> 1) * C) + c), f);
+    unpack8(__ldcg(reinterpret_cast<const uint4*>(skip + q * C) + c), s);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) o[k] = fmaxf(f[k] + s[k], 0.f);
+  }
+  reinterpret_cast<uint4*>(out + q * C)[c] = pack8(o);
+}
+
+// y = d0 . w_out + b_out for the 16 channels of one pixel
+__device__ __forceinline__ float out1x1_value(const uint4& lo, const uint4& hi, const float* w, const float* bo) {
+  float f[8], acc = *bo;
+  unpack8(lo, f);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) acc += f[k] * w[k];
+  unpack8(hi, f);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) acc += f[k] * w[8 + k];
+  return acc;
+}
+
+template <int C>
+__global__ void pool_kernel(LevelGeom gi, LevelGeom go, const bf16* in, bf16* out) {
+  tpf::tc::pdl_trigger();
+  const long long n = go.P() * (C / 8);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    pool_item<C>(gi, go, in, out, i);
+}
+
+template <int C>
 __global__ void upadd_relu_kernel(LevelGeom gf, LevelGeom gc, const bf16* t, const bf16* skip, bf16* out) {
   tpf::tc::pdl_trigger();
-  constexpr int K = C / 8;
-  const long long n = gf.P() * K;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const long long q = i / K;
-    const int c = (int)(i - q * K);
-    int b, y, x;
-    float o[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    if (pix(gf, q, b, y, x)) {
-      float f[8], s[8];
-      unpack8(reinterpret_cast<const uint4*>(t + gc.q(b, y >> 1, x >> 1) * C)[c], f);
-      unpack8(reinterpret_cast<const uint4*>(skip + q * C)[c], s);
-#pragma unroll
-      for (int k = 0; k < 8; ++k) o[k] = fmaxf(f[k] + s[k], 0.f);
-    }
-    reinterpret_cast<uint4*>(out + q * C)[c] = pack8(o);
-  }
+  const long long n = gf.P() * (C / 8);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    upadd_item<C>(gf, gc, t, skip, out, i);
 }
 
 // backward of up(): out(level l+1) = 2x2 sum of in(level l)
@@ -402,14 +448,7 @@ __global__ void out1x1_kernel(LevelGeom g, const bf16* d0, const float* w, const
     const int y = (int)(t % g.H);
     const int b = (int)(t / g.H);
     const uint4* p = reinterpret_cast<const uint4*>(d0 + g.q(b, y, x) * kOutC);
-    float f[8], acc = *bo;
-    unpack8(p[0], f);
-#pragma unroll
-    for (int k = 0; k < 8; ++k) acc += f[k] * w[k];
-    unpack8(p[1], f);
-#pragma unroll
-    for (int k = 0; k < 8; ++k) acc += f[k] * w[8 + k];
-    yout[i] = acc;
+    yout[i] = out1x1_value(p[0], p[1], w, bo);
   }
 }
 
@@ -456,6 +495,311 @@ __global__ void out1x1_bwd_kernel(LevelGeom g, const bf16* d0, const float* dy, 
     if (threadIdx.x < 16) atomicAdd(gw + threadIdx.x, s);
     else atomicAdd(gb, s);
   }
+}
+
+// ---- persistent forward ---------------------------------------------------------------------
+// The whole forward pass in ONE cooperative launch (one 128-thread CTA per
+// SM): 14 convolution stages, 3 poolings and 3 upsample-adds separated by
+// grid barriers, the 1x1 output fused into the last convolution's epilogue.
+// TMEM is held for the whole launch, the next convolution's weights are
+// fetched before the barrier that precedes it, and the deep (few-tile) layers
+// split their output channels over CTAs (N = nc per MMA) so that more SMs
+// share them.  Every output element sees the same MMA sequence (taps, then
+// 16-channel K steps) as in the layered kernel, so the outputs are identical.
+// Measured at the preconditioner's 136^2 image (batch 1): ~106 us inside the
+// kernel, of which ~19 us are the 19 barriers; the largest part of a stage is
+// gathering the 16-byte channel chunks of the three input windows out of the
+// pixel-major activations (~29 GB/s per SM, against ~150 GB/s for a linear
+// copy), then the MMA issue (~37 ns per M128 x N16 x K16 instruction).
+constexpr int kPfThreads = 128;
+constexpr int kPfCols = 128;                         // TMEM columns held (max nc)
+constexpr int kPfWin = 3 * (128 / 8) * kPlane;       // windows of a 128-channel input
+constexpr int kPfW = 9 * 128 * 32 * 2;               // weights of one unit (max 9 * cin * nc * 2)
+constexpr int kPfBias = 128 * 4;                     // biases of one unit (max nc floats)
+constexpr int kPfSmem = kPfWin + kPfW + kPfBias;
+
+struct PfConv {
+  const bf16* in;     // [P][cin]
+  bf16* out;          // [P][cout]
+  const bf16* w;      // [9][cin/8][cout][8]
+  const float* bias;  // [cout]
+  long long P;
+  int Hp, Wp, cin, cout, nc, tiles, relu;
+};
+struct PfArgs {
+  PfConv c[kConvs];
+  LevelGeom g[4];
+  const bf16 *e0, *e1, *e2, *t2, *t1, *t0;
+  bf16 *p0, *p1, *p2, *d2a, *d1a, *d0a;
+  const float* w_out;
+  const float* b_out;
+  float* y;                  // [B][H][W]
+  unsigned long long* bar;   // monotonic arrival counter of the grid barriers
+  int* err;
+};
+struct PfCtx {
+  int wl, wc;          // layer / channel chunk whose weights are in (or on the way to) shared memory
+  uint32_t phase, tmem;
+  bool ok;
+};
+
+__device__ __forceinline__ unsigned long long pf_ld_acquire(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];\n" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void pf_red_release_add(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.release.gpu.global.add.u64 [%0], %1;\n" ::"l"(p), "l"(v) : "memory");
+}
+
+// Grid barrier on a monotonic 64-bit arrival counter: one release-add per CTA
+// and acquire polling, no reset.  Every launch adds exactly kPfBarriers x
+// gridDim.x arrivals (a CTA whose wait gives up still arrives at every later
+// barrier), so a launch finds its base as the counter rounded down to that
+// multiple: before barrier 0 completes the counter is at most
+// base + gridDim.x - 1.  Bounded wait; gives up (error flag) rather than hang.
+constexpr int kPfBarriers = 19;
+struct PfBarrier {
+  unsigned long long* count;
+  unsigned long long target;   // arrivals that complete the next barrier
+};
+__device__ __forceinline__ PfBarrier pf_barrier_begin(unsigned long long* count) {
+  __shared__ unsigned long long s_base;
+  if (threadIdx.x == 0) {
+    const unsigned long long c = pf_ld_acquire(count);
+    const unsigned long long per = (unsigned long long)kPfBarriers * gridDim.x;
+    s_base = c - c % per;
+  }
+  __syncthreads();
+  return PfBarrier{count, s_base + gridDim.x};
+}
+__device__ __forceinline__ void pf_grid_sync(PfBarrier& br, int* err) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    pf_red_release_add(br.count, 1ull);
+    long long spins = 0;
+    while (pf_ld_acquire(br.count) < br.target) {
+      if (++spins > kSpin) { atomicExch(err, 1); break; }
+      if ((spins & 255) == 0 && *(volatile int*)err) break;
+    }
+  }
+  br.target += gridDim.x;
+  __syncthreads();
+}
+
+// weights of output channels [chunk*nc, (chunk+1)*nc) -> smem [9][cin/8][nc][8],
+// followed (at kPfW) by their nc biases (the bias offsets of the flat
+// parameter layout are multiples of 16 floats, so the copy is 16-byte
+// aligned).  Consecutive threads copy consecutive 16-byte pieces on both sides.
+__device__ __forceinline__ void pf_load_weights(const PfConv& L, int chunk, unsigned char* sB) {
+  const int lg = L.nc == 16 ? 4 : (L.nc == 32 ? 5 : (L.nc == 64 ? 6 : 7));   // nc is a power of two
+  const int n = 9 * (L.cin / 8) << lg;      // 16-byte pieces: (tap, 8-channel) rows x nc
+  const unsigned char* src = reinterpret_cast<const unsigned char*>(L.w);
+  for (int i = threadIdx.x; i < n; i += kPfThreads) {
+    const int r = i >> lg, j = i & (L.nc - 1);
+    tpf::tc::cp_async16(sB + (size_t)i * 16, src + ((size_t)r * L.cout + (size_t)chunk * L.nc + j) * 16, true);
+  }
+  if ((int)threadIdx.x < L.nc / 4)
+    tpf::tc::cp_async16(sB + kPfW + threadIdx.x * 16, L.bias + (size_t)chunk * L.nc + threadIdx.x * 4, true);
+  tpf::tc::cp_async_commit();
+}
+
+// fetch the weights of this CTA's first unit of layer l (if it has one)
+__device__ __forceinline__ void pf_prefetch(const PfArgs& a, int l, PfCtx& cx, unsigned char* sB) {
+  if (l >= kConvs) return;
+  const PfConv& L = a.c[l];
+  if ((int)blockIdx.x >= L.tiles * (L.cout / L.nc)) return;
+  const int chunk = (int)blockIdx.x / L.tiles;
+  pf_load_weights(L, chunk, sB);
+  cx.wl = l;
+  cx.wc = chunk;
+}
+
+// One convolution stage.  Per unit (128 output pixels x nc output channels):
+// the three windows (and, unless prefetched, the weight chunk) are copied
+// into shared memory, thread 0 issues 9 x CIN/16 tcgen05.mma (M = 128,
+// N = nc, K = 16) with descriptors advanced by constant offsets, and four
+// warps read TMEM back for the bias / ReLU / border epilogue.  CIN is a
+// compile-time constant so that the addressing divides by constants and the
+// MMA issue is straight-line code.
+template <int CIN>
+__device__ void pf_conv_t(const PfArgs& a, int l, PfCtx& cx, unsigned char* smem, uint64_t* mbar) {
+  using namespace tpf::tc;
+  constexpr int WIN_BYTES = (CIN / 8) * kPlane;
+  const PfConv& L = a.c[l];
+  const int units = L.tiles * (L.cout / L.nc);
+  unsigned char* sA = smem;
+  unsigned char* sB = smem + kPfWin;
+  const float* sBias = reinterpret_cast<const float*>(sB + kPfW);
+  if ((int)blockIdx.x >= units) {
+    pf_prefetch(a, l + 1, cx, sB);
+    return;
+  }
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nc = L.nc;
+  const uint32_t idesc = idesc_bf16_f32(kTile, nc);
+  for (int u = blockIdx.x; u < units; u += gridDim.x) {
+    const int chunk = u / L.tiles;
+    const long long q0 = (long long)(u - chunk * L.tiles) * kTile;
+    if (cx.wl != l || cx.wc != chunk) {
+      pf_load_weights(L, chunk, sB);
+      cx.wl = l;
+      cx.wc = chunk;
+    }
+    load_windows<CIN>(L.in, L.P, L.Wp, q0, sA);
+    cp_async_wait_all();
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      fence_after_sync();
+      // descriptor address fields are in 16-byte units; every offset below
+      // keeps the address inside shared memory, so adding to the low field
+      // never carries into the next one
+      const uint64_t ad0 = smem_desc(smem_u32(sA), kPlane, 128);
+      const uint64_t bd0 = smem_desc(smem_u32(sB), nc * 16, 128);
+      const uint32_t tap_step = (uint32_t)(CIN * nc * 2) >> 4, kc_step = (uint32_t)(nc * 32) >> 4;
+#pragma unroll
+      for (int tap = 0; tap < 9; ++tap) {
+        const int dy = tap / 3, dx = tap % 3;
+#pragma unroll
+        for (int kc = 0; kc < CIN / 16; ++kc) {
+          const uint64_t ad = ad0 + (uint64_t)((dy * WIN_BYTES + dx * 16 + kc * 2 * kPlane) >> 4);
+          const uint64_t bd = bd0 + (uint64_t)(tap * tap_step + kc * kc_step);
+          mma_bf16(cx.tmem, ad, bd, idesc, (tap > 0 || kc > 0) ? 1u : 0u);
+        }
+      }
+      mma_commit(mbar);
+    }
+    __syncwarp();
+    if (!mbar_wait(mbar, cx.phase, kSpin)) cx.ok = false;
+    cx.phase ^= 1u;
+    fence_after_sync();
+    const long long q = q0 + warp * 32 + lane;
+    const bool inb = q < L.P;
+    const bool inner = inb && interior_pixel(q, L.Hp, L.Wp);
+    const int n0 = chunk * nc;
+    const bool last_unit = u + (int)gridDim.x >= units;
+#pragma unroll 1
+    for (int c0 = 0; c0 < nc; c0 += 16) {
+      float v[16], bv[16];
+      tmem_ld16(cx.tmem + (static_cast<uint32_t>(warp * 32) << 16) + c0, v);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) bv[i] = sBias[c0 + i];
+      if (inb) {
+        uint4 ov[2];
+        __nv_bfloat162* o2 = reinterpret_cast<__nv_bfloat162*>(ov);
+#pragma unroll
+        for (int i = 0; i < 16; i += 2) {
+          float x0 = v[i] + bv[i], x1 = v[i + 1] + bv[i + 1];
+          if (L.relu) { x0 = fmaxf(x0, 0.f); x1 = fmaxf(x1, 0.f); }
+          if (!inner) { x0 = 0.f; x1 = 0.f; }
+          o2[i / 2] = __floats2bfloat162_rn(x0, x1);
+        }
+        uint4* op = reinterpret_cast<uint4*>(L.out + q * L.cout + n0 + c0);
+        op[0] = ov[0];
+        op[1] = ov[1];
+        if (l == kConvs - 1 && inner) {   // fused 1x1 output (cout == nc == 16)
+          int b, yy, xx;
+          pix(a.g[0], q, b, yy, xx);
+          a.y[((long long)b * a.g[0].H + yy) * a.g[0].W + xx] = out1x1_value(ov[0], ov[1], a.w_out, a.b_out);
+        }
+      }
+    }
+    fence_before_sync();
+    __syncthreads();
+    // windows, weights and biases are consumed: the next layer's weights can
+    // stream in during the barrier that follows
+    if (last_unit) pf_prefetch(a, l + 1, cx, sB);
+  }
+}
+
+__device__ __forceinline__ void pf_conv(const PfArgs& a, int l, PfCtx& cx, unsigned char* smem, uint64_t* mbar) {
+  switch (a.c[l].cin) {
+    case 16: pf_conv_t<16>(a, l, cx, smem, mbar); break;
+    case 32: pf_conv_t<32>(a, l, cx, smem, mbar); break;
+    case 64: pf_conv_t<64>(a, l, cx, smem, mbar); break;
+    default: pf_conv_t<128>(a, l, cx, smem, mbar); break;
+  }
+}
+
+template <int C>
+__device__ __forceinline__ void pf_pool(const LevelGeom& gi, const LevelGeom& go, const bf16* in, bf16* out) {
+  const long long n = go.P() * (C / 8);
+  for (long long i = blockIdx.x * (long long)kPfThreads + threadIdx.x; i < n; i += (long long)gridDim.x * kPfThreads)
+    pool_item<C>(gi, go, in, out, i);
+}
+template <int C>
+__device__ __forceinline__ void pf_upadd(const LevelGeom& gf, const LevelGeom& gc, const bf16* t, const bf16* skip,
+                                         bf16* out) {
+  const long long n = gf.P() * (C / 8);
+  for (long long i = blockIdx.x * (long long)kPfThreads + threadIdx.x; i < n; i += (long long)gridDim.x * kPfThreads)
+    upadd_item<C>(gf, gc, t, skip, out, i);
+}
+
+__global__ void __launch_bounds__(kPfThreads, 1) unet_forward_persistent_kernel(const __grid_constant__ PfArgs a) {
+  using namespace tpf::tc;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ uint64_t mbar;
+  __shared__ uint32_t tmem_slot;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  if (warp == 0) tmem_alloc(&tmem_slot, kPfCols);
+  if (tid == 0) {
+    mbar_init(&mbar, 1);
+    mbar_fence_init();
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  PfCtx cx{-1, -1, 0u, tmem_slot, true};
+  pf_prefetch(a, 0, cx, smem + kPfWin);
+  PfBarrier br = pf_barrier_begin(a.bar);
+
+  pf_conv(a, 0, cx, smem, &mbar);
+  pf_grid_sync(br, a.err);
+  pf_conv(a, 1, cx, smem, &mbar);
+  pf_grid_sync(br, a.err);
+  pf_pool<16>(a.g[0], a.g[1], a.e0, a.p0);
+  pf_grid_sync(br, a.err);
+  pf_conv(a, 2, cx, smem, &mbar);
+  pf_grid_sync(br, a.err);
+  pf_conv(a, 3, cx, smem, &mbar);
+  pf_grid_sync(br, a.err);
+  pf_pool<32>(a.g[1], a.g[2], a.e1, a.p1);
+  pf_grid_sync(br, a.err);
+  pf_conv(a, 4, cx, smem, &mbar);
+  pf_grid_sync(br, a.err);
+  pf_conv(a, 5, cx, smem, &mbar);
+  pf_grid_sync(br, a.err);
+  pf_pool<64>(a.g[2], a.g[3], a.e2, a.p2);
+  pf_grid_sync(br, a.err);
+  pf_conv(a, 6, cx, smem, &mbar);
+  pf_grid_sync(br, a.err);
+  pf_conv(a, 7, cx, smem, &mbar);
+  pf_grid_sync(br, a.err);
+  pf_conv(a, 8, cx, smem, &mbar);
+  pf_grid_sync(br, a.err);
+  pf_upadd<64>(a.g[2], a.g[3], a.t2, a.e2, a.d2a);
+  pf_grid_sync(br, a.err);
+  pf_conv(a, 9, cx, smem, &mbar);
+  pf_grid_sync(br, a.err);
+  pf_conv(a, 10, cx, smem, &mbar);
+  pf_grid_sync(br, a.err);
+  pf_upadd<32>(a.g[1], a.g[2], a.t1, a.e1, a.d1a);
+  pf_grid_sync(br, a.err);
+  pf_conv(a, 11, cx, smem, &mbar);
+  pf_grid_sync(br, a.err);
+  pf_conv(a, 12, cx, smem, &mbar);
+  pf_grid_sync(br, a.err);
+  pf_upadd<16>(a.g[0], a.g[1], a.t0, a.e0, a.d0a);
+  pf_grid_sync(br, a.err);
+  pf_conv(a, 13, cx, smem, &mbar);
+
+  if (!cx.ok) atomicExch(a.err, 1);
+  // a CTA without units in the last layers may still have a weight copy in flight
+  cp_async_wait_all();
+  fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(cx.tmem, kPfCols);
 }
 
 // weight (and bias) gradient of a 3x3 convolution on the CUDA cores:
@@ -735,6 +1079,10 @@ struct tpf_unet {
   float* dy = nullptr;
   double* sums = nullptr;
   int* err = nullptr;
+  unsigned long long* bar = nullptr;   // grid-barrier counter of the persistent forward
+  int forward_mode = 0;                // 0 layered launches, 1 persistent launch
+  PfArgs* pf_args = nullptr;           // launch arguments of the persistent forward
+  int pf_batch = 0;                    // ... built for this batch size (0: none)
   bool training_buffers = false;
   int last_batch = 0;
   std::vector<void*> allocs;
@@ -864,9 +1212,128 @@ void poolbwd_t(const LevelGeom& gf, const LevelGeom& gc, const bf16* dP, const b
   pool_bwd_kernel<C><<<grid_for(gf.P() * (C / 8)), 256, 0, s>>>(gf, gc, dP, sk, act, out);
 }
 
+// CTAs of the persistent forward: one per SM (cooperative launch)
+int persistent_grid() {
+  static int grid = -1;
+  if (grid < 0) {
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaFuncSetAttribute(unet_forward_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kPfSmem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, unet_forward_persistent_kernel, kPfThreads,
+                                                      kPfSmem) != cudaSuccess ||
+        per_sm < 1) {
+      cudaGetLastError();
+      grid = 0;
+    } else {
+      grid = sms;
+    }
+  }
+  return grid;
+}
+
+// output-channel split of a convolution in the persistent forward: as many
+// 16-channel chunks as keep units (tiles x chunks) within one wave, and at
+// most 32 (128-channel input) or 64 channels per unit (shared-memory bound)
+int persistent_nc(int cin, int cout, long long tiles, int grid) {
+  const int cap = cin >= 128 ? 32 : 64;
+  int split = 1;
+  while (cout / split > cap) split *= 2;
+  while (cout / (split * 2) >= 16 && tiles * split * 2 <= grid) split *= 2;
+  return cout / split;
+}
+
+// launch arguments of the persistent forward for batch B (the channel
+// splits depend only on B, the addresses are fixed per workspace)
+int build_persistent_args(tpf_unet* n, int B, int grid, PfArgs& a) {
+  const ParamLayout& L = layout();
+  a = PfArgs{};
+  const bf16* ins[kConvs] = {n->xin, n->e0a, n->p0, n->e1a, n->p1, n->e2a, n->p2,
+                             n->e3a, n->e3,  n->d2a, n->d2, n->d1a, n->d1, n->d0a};
+  bf16* outs[kConvs] = {n->e0a, n->e0, n->e1a, n->e1, n->e2a, n->e2, n->e3a,
+                        n->e3,  n->t2, n->d2,  n->t1, n->d1,  n->t0, n->d0};
+  for (int l = 0; l < kConvs; ++l) {
+    const LevelGeom g = n->geom(kLayers[l].level, B);
+    PfConv& c = a.c[l];
+    c.in = ins[l];
+    c.out = outs[l];
+    c.w = n->wf[l];
+    c.bias = n->params + L.b[l];
+    c.P = g.P();
+    c.Hp = g.Hp;
+    c.Wp = g.Wp;
+    c.cin = cin_kernel(l);
+    c.cout = kLayers[l].cout;
+    c.relu = kLayers[l].relu;
+    const long long tiles = (c.P + kTile - 1) / kTile;
+    c.tiles = (int)tiles;
+    c.nc = persistent_nc(c.cin, c.cout, tiles, grid);
+  }
+  for (int l = 0; l < 4; ++l) a.g[l] = n->geom(l, B);
+  a.e0 = n->e0;
+  a.e1 = n->e1;
+  a.e2 = n->e2;
+  a.t2 = n->t2;
+  a.t1 = n->t1;
+  a.t0 = n->t0;
+  a.p0 = n->p0;
+  a.p1 = n->p1;
+  a.p2 = n->p2;
+  a.d2a = n->d2a;
+  a.d1a = n->d1a;
+  a.d0a = n->d0a;
+  a.w_out = n->params + L.wo;
+  a.b_out = n->params + L.bo;
+  a.y = n->out;
+  a.bar = n->bar;
+  a.err = n->err;
+  return TPF_OK;
+}
+
+int forward_persistent(tpf_unet* n, int B, cudaStream_t s) {
+  const int grid = persistent_grid();
+  if (grid <= 0) {
+    tpf::set_error("the persistent forward cannot be made co-resident on this device");
+    return TPF_ECUDA;
+  }
+  if (!n->pf_args) n->pf_args = new PfArgs();
+  if (n->pf_batch != B) {
+    n->pf_batch = 0;
+    int st = build_persistent_args(n, B, grid, *n->pf_args);
+    if (st) return st;
+    n->pf_batch = B;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(kPfThreads);
+  cfg.dynamicSmemBytes = kPfSmem;
+  cfg.stream = s;
+  cudaLaunchAttribute coop[1];
+  coop[0].id = cudaLaunchAttributeCooperative;
+  coop[0].val.cooperative = 1;
+  cfg.attrs = coop;
+  cfg.numAttrs = 1;
+  TPF_CUDA_TRY(cudaLaunchKernelEx(&cfg, unet_forward_persistent_kernel, *n->pf_args));
+  return TPF_OK;
+}
+
+// The layered launches are the default: inside the learned solver's CUDA
+// graph they overlap their prologues with the previous kernel (programmatic
+// dependent launch), which the cooperative launch cannot, and measured
+// faster there (161 vs 187 us per flexible-CG iteration at 512^2); the
+// persistent launch is faster for a stand-alone forward call.
+bool use_persistent(const tpf_unet* n, int) { return n->forward_mode == 1; }
+
 int forward(tpf_unet* n, int B, cudaStream_t s) {
   int st;
   if (!n->arranged && (st = arrange(n, s))) return st;
+  if (use_persistent(n, B)) {
+    if ((st = forward_persistent(n, B, s))) return st;
+    n->last_batch = B;
+    return TPF_OK;
+  }
+
   const LevelGeom g0 = n->geom(0, B), g1 = n->geom(1, B), g2 = n->geom(2, B), g3 = n->geom(3, B);
   if ((st = conv(n, 0, B, n->xin, n->e0a, s)) || (st = conv(n, 1, B, n->e0a, n->e0, s))) return st;
   pool_t<16>(g0, g1, n->e0, n->p0, s);
@@ -934,6 +1401,10 @@ int check_err(tpf_unet* n, cudaStream_t s) {
   TPF_CUDA_TRY(cudaMemcpyAsync(&herr, n->err, sizeof(int), cudaMemcpyDeviceToHost, s));
   TPF_CUDA_TRY(cudaStreamSynchronize(s));
   if (herr) {
+    // start the next call clean: a timed-out wait leaves the flag set
+    cudaMemsetAsync(n->bar, 0, sizeof(unsigned long long), s);
+    cudaMemsetAsync(n->err, 0, sizeof(int), s);
+    cudaStreamSynchronize(s);
     tpf::set_error("a tensor-core convolution wait timed out");
     return TPF_EABORT;
   }
@@ -996,6 +1467,8 @@ int tpf_unet_create(tpf_unet** out, int H, int W, int max_batch) {
   if ((st = ualloc(n, &n->out, (size_t)max_batch * H * W))) return fail(st);
   if ((st = ualloc(n, &n->err, 1))) return fail(st);
   TPF_CUDA_TRY(cudaMemset(n->err, 0, sizeof(int)));
+  if ((st = ualloc(n, &n->bar, 1))) return fail(st);
+  TPF_CUDA_TRY(cudaMemset(n->bar, 0, sizeof(unsigned long long)));
   *out = n;
   return TPF_OK;
 }
@@ -1004,6 +1477,7 @@ int tpf_unet_destroy(tpf_unet* n) {
   if (!n) return TPF_OK;
   cudaDeviceSynchronize();
   for (void* p : n->allocs) cudaFree(p);
+  delete n->pf_args;
   delete n;
   return TPF_OK;
 }
@@ -1026,6 +1500,13 @@ int tpf_unet_get_params(tpf_unet* n, float* params, int on_device) {
   TPF_CHECK_ARG(n && params, "null argument");
   TPF_CUDA_TRY(cudaMemcpy(params, n->params, layout().total * sizeof(float),
                           on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost));
+  return TPF_OK;
+}
+
+int tpf_unet_set_forward_mode(tpf_unet* n, int mode) {
+  TPF_CHECK_ARG(n != nullptr, "null handle");
+  TPF_CHECK_ARG(mode >= -1 && mode <= 1, "forward mode must be -1, 0 or 1 (got %d)", mode);
+  n->forward_mode = mode < 0 ? 0 : mode;
   return TPF_OK;
 }
 

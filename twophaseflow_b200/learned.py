@@ -116,6 +116,10 @@ class UNet:
         _lib.check(self.lib.tpf_unet_get_params(self.handle, a.ctypes.data_as(C.c_void_p), 0))
         return a
 
+    def set_forward_mode(self, mode: int) -> None:
+        """0 (default, also -1): one launch per layer; 1: the whole network in one persistent launch."""
+        _lib.check(self.lib.tpf_unet_set_forward_mode(self.handle, int(mode)))
+
     def forward(self, in2):
         """y[B,H,W] for in2[B,H,W,IN_CHANNELS] (FP32 CUDA tensor)."""
         torch = _torch()
