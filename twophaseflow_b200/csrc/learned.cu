@@ -889,7 +889,7 @@ void tpf_lppe_default_options(tpf_learned_options* o) {
   if (!o) return;
   o->tol = 1e-8;
   o->maxiter = 2000;
-  o->smooth = 1;
+  o->smooth = 3;
   o->omega = 0.8;
   o->check_every = 8;
   o->stall_checks = 16;

@@ -178,7 +178,7 @@ class PPESolverLearned(PPESolverFVMMatrixFree):
     (``pseudo_tol``, ``pseudo_maxiter``) plus ``ppe_learned_coarsen`` (4: the
     network solves the problem aggregated over 4 x 4 node blocks inside a
     two-grid cycle; 1: the network reads the fine residual),
-    ``ppe_learned_smooth`` (damped Jacobi sweeps after the network, default 1),
+    ``ppe_learned_smooth`` (damped Jacobi sweeps after the network, default 3),
     ``ppe_learned_omega`` (0.8), ``ppe_learned_weights`` (path of the trained
     parameters) and ``ppe_learned_fallback`` (finish with plain Jacobi PCG on a
     stall, True).
@@ -196,7 +196,7 @@ class PPESolverLearned(PPESolverFVMMatrixFree):
         if self.ndim != 2:
             raise ValueError("the learned preconditioner is two-dimensional")
         solver_cfg = getattr(config, "solver", config)
-        self.smooth = int(getattr(solver_cfg, "ppe_learned_smooth", 1))
+        self.smooth = int(getattr(solver_cfg, "ppe_learned_smooth", 3))
         self.omega = float(getattr(solver_cfg, "ppe_learned_omega", 0.8))
         self.fallback = bool(getattr(solver_cfg, "ppe_learned_fallback", True))
         self.learned_maxiter = int(getattr(solver_cfg, "ppe_learned_maxiter", max(self.maxiter, 2000)))
