@@ -376,10 +376,10 @@ def main(argv=None):
             "batched_32_cases": bat,
             "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": 2 * ndof * 8,
                     "d2h_bytes_per_step": ndof * 8, "wall_ms": round(e2e_wall, 3)},
-            "roofline": {"kernel": "pcg64_kernel (plain FP64 PCG, persistent)", "bound": "hbm",
+            "roofline": {"kernel": "cg1_band_kernel (plain FP64 PCG, one cooperative launch, per-SM node ranges resident in shared memory)", "bound": "hbm",
                          "achieved": round(ach64, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": round(ach64 / peak, 3), "traffic": None,
-                         "note": "112 B/DOF/iteration algorithmic; the 512^2 working set (~13 MB) is L2-resident"},
+                         "note": "112 B/DOF/iteration algorithmic; the vectors stay in shared memory, only range edges and the reduction cross L2"},
             "ccd": ccd,
             "ccd_roofline": {"kernel": "ccd_lane_kernel (3-D 257^3 FP64, mean over axes and wall/periodic)",
                              "bound": "hbm", "achieved": round(ccd3_gbps, 1), "peak": peak, "unit": "GB/s",

