@@ -239,6 +239,103 @@ __global__ void thomas_solve_kernel(LineArgs L, const double* __restrict__ lo, c
   }
 }
 
+// The same exact line solve with one warp per line (the one-thread-per-line
+// kernel above leaves most SMs idle and walks each line serially through
+// global memory).  Lane l owns rows [l K, l K + K).  Both sweeps are affine
+// recurrences, dp_i = (r_i - lo_i dp_{i-1}) / den_i and x_i = tmp_i - cp_i x_{i+1}:
+// each lane composes the map of its chunk, a warp scan of the maps gives
+// every lane the value entering its chunk, and the lane then runs its chunk
+// with the recurrence itself (the reference's per-row arithmetic; only the
+// carried-in values come from the composed maps).  tmp stays in registers.
+template <bool ACC, int K>
+__global__ void __launch_bounds__(128) thomas_warp_kernel(LineArgs L, const double* __restrict__ lo,
+                                                          const double* __restrict__ den,
+                                                          const double* __restrict__ cp,
+                                                          const double* __restrict__ r, double* out, int pin,
+                                                          double scale, const int* done) {
+  if (done && *done) return;
+  const int lane = threadIdx.x & 31;
+  const int l = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (l >= L.lines) return;
+  const int b = line_base(L, l);
+  const int n = L.n;
+  const int i0 = lane * K;
+  // forward: compose y -> A y + B over the chunk (row 0 of the line has no carry)
+  double rr[K], tmp[K];
+  double A = 1.0, B = 0.0;
+#pragma unroll
+  for (int q = 0; q < K; ++q) {
+    const int i = i0 + q;
+    rr[q] = 0.0;
+    if (i < n) {
+      const int e = b + i * L.stride;
+      const double ri = (e == pin) ? 0.0 : r[e];
+      rr[q] = ri;
+      const double d = den[e];
+      if (i == 0) { A = 0.0; B = ri / d; }
+      else {
+        const double m = lo[e];
+        A = -m * A / d;
+        B = (ri - m * B) / d;
+      }
+    }
+  }
+  // inclusive scan of the maps across lanes (lower lanes applied first)
+#pragma unroll
+  for (int s = 1; s < 32; s <<= 1) {
+    const double Ap = __shfl_up_sync(0xffffffffu, A, s), Bp = __shfl_up_sync(0xffffffffu, B, s);
+    if (lane >= s) { B = A * Bp + B; A = A * Ap; }
+  }
+  // value entering this lane's chunk = the previous lane's composed map applied to 0
+  double y = __shfl_up_sync(0xffffffffu, B, 1);
+  if (lane == 0) y = 0.0;
+#pragma unroll
+  for (int q = 0; q < K; ++q) {
+    const int i = i0 + q;
+    if (i < n) {
+      const int e = b + i * L.stride;
+      y = (i == 0) ? rr[q] / den[e] : (rr[q] - lo[e] * y) / den[e];
+    }
+    tmp[q] = y;
+  }
+  // backward: compose x -> C x + D over the chunk, from its last row down
+  double C = 1.0, D = 0.0;
+#pragma unroll
+  for (int q = K - 1; q >= 0; --q) {
+    const int i = i0 + q;
+    if (i < n) {
+      if (i == n - 1) { C = 0.0; D = tmp[q]; }
+      else {
+        const double c = cp[b + i * L.stride];
+        D = tmp[q] - c * D;
+        C = -c * C;
+      }
+    }
+  }
+  // suffix scan across lanes (higher lanes applied first)
+#pragma unroll
+  for (int s = 1; s < 32; s <<= 1) {
+    const double Cn = __shfl_down_sync(0xffffffffu, C, s), Dn = __shfl_down_sync(0xffffffffu, D, s);
+    if (lane + s < 32) { D = C * Dn + D; C = C * Cn; }
+  }
+  double x = __shfl_down_sync(0xffffffffu, D, 1);
+  if (lane == 31) x = 0.0;
+#pragma unroll
+  for (int q = K - 1; q >= 0; --q) {
+    const int i = i0 + q;
+    if (i < n) {
+      const int e = b + i * L.stride;
+      x = (i == n - 1) ? tmp[q] : tmp[q] - cp[e] * x;
+      if (ACC) {
+        const double v = (out[e] + x) * scale;
+        out[e] = (e == pin) ? 0.0 : v;
+      } else {
+        out[e] = x;
+      }
+    }
+  }
+}
+
 // Truncated parallel cyclic reduction along lines (the reference's GPU line
 // solver, linalg_backend.py:77-115): `stages` reduction steps of
 //   alpha = -a_i / d_{i-s}, beta = -c_i / d_{i+s} (0 beyond the line ends),
@@ -999,23 +1096,58 @@ struct GmState {
 };
 
 // partial dots: part[k*nb + block] = <V_k, w> for k < ncols, part[ncols*nb+block] = <w,w>
+// Block partials of <V_k, w> for k < ncols and of <w, w> (k = ncols):
+// part[k * nb + block].  The vectors are taken eight at a time in one sweep
+// over w, with one block reduction per group (warp j reduces vector j of the
+// group with the same shuffle tree a one-vector reduction uses).
 __global__ void mdot_kernel(int ndof, const double* __restrict__ V, int ncols, const double* __restrict__ w,
                             double* part, const int* done) {
   if (done && *done) return;
-  extern __shared__ double sh[];
-  const int nb = gridDim.x;
-  for (int k = 0; k <= ncols; ++k) {
-    const double* vk = (k < ncols) ? V + (size_t)k * ndof : w;
-    double acc = 0.0;
-    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += gridDim.x * blockDim.x)
-      acc += vk[idx] * w[idx];
-    acc = tpf::warp_sum(acc);
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  constexpr int KC = 8;   // vectors per sweep (<= warps per block)
+  extern __shared__ double sh[];   // [KC][32]
+  const int nb = gridDim.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int k0 = 0; k0 <= ncols; k0 += KC) {
+    double acc[KC];
+#pragma unroll
+    for (int j = 0; j < KC; ++j) acc[j] = 0.0;
+    // two elements per trip: 18 independent loads in flight per thread
+    const int stride = gridDim.x * blockDim.x;
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    for (; idx + stride < ndof; idx += 2 * stride) {
+      const double wa = w[idx], wb = w[idx + stride];
+      double va[KC], vb[KC];
+#pragma unroll
+      for (int j = 0; j < KC; ++j) {
+        const int k = k0 + j;
+        va[j] = (k < ncols) ? V[(size_t)k * ndof + idx] : wa;
+        vb[j] = (k < ncols) ? V[(size_t)k * ndof + idx + stride] : wb;
+      }
+#pragma unroll
+      for (int j = 0; j < KC; ++j) {
+        if (k0 + j <= ncols) {
+          acc[j] += va[j] * wa;
+          acc[j] += vb[j] * wb;
+        }
+      }
+    }
+    if (idx < ndof) {
+      const double wi = w[idx];
+#pragma unroll
+      for (int j = 0; j < KC; ++j) {
+        const int k = k0 + j;
+        if (k <= ncols) acc[j] += ((k < ncols) ? V[(size_t)k * ndof + idx] : wi) * wi;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < KC; ++j) {
+      const double v = tpf::warp_sum(acc[j]);
+      if (lane == 0) sh[j * 32 + wid] = v;
+    }
     __syncthreads();
-    if (threadIdx.x < 32) {
-      double s = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
-      s = tpf::warp_sum(s);
-      if (threadIdx.x == 0) part[(size_t)k * nb + blockIdx.x] = s;
+    if (wid < KC && k0 + wid <= ncols) {
+      double t = (lane < nw) ? sh[wid * 32 + lane] : 0.0;
+      t = tpf::warp_sum(t);
+      if (lane == 0) part[(size_t)(k0 + wid) * nb + blockIdx.x] = t;
     }
     __syncthreads();
   }
@@ -1025,32 +1157,38 @@ __global__ void mdot_kernel(int ndof, const double* __restrict__ V, int ncols, c
 // mode 0: first GS pass (h column = dots, h0 = sqrt(<w,w>)), decide re-orth
 // mode 1: second pass (h column += dots)
 // mode 2: plain norm -> out[0] = sqrt(<w,w>)
+// One block; warp j sums the partials of vectors j, j + nwarps, ... (lane l:
+// blocks l, l + 32, ..., then a shuffle tree), so all vectors are summed at
+// once; thread 0 then applies the mode's scalar logic in vector order.
 __global__ void mdot_finalize_kernel(const double* part, int nb, int ncols, double* hcol, GmState* st,
                                      int mode, double* out_norm) {
   if (mode != 2 && st->done) return;
   if (mode == 1 && !st->reorth) return;
-  __shared__ double sh[32];
-  for (int k = 0; k <= ncols; ++k) {
+  extern __shared__ double sums[];   // [ncols + 1]
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int k = wid; k <= ncols; k += nw) {
     double acc = 0.0;
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) acc += part[(size_t)k * nb + b];
+    for (int b = lane; b < nb; b += 32) acc += part[(size_t)k * nb + b];
     acc = tpf::warp_sum(acc);
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double s = 0.0;
-      for (int q = 0; q < (int)(blockDim.x >> 5); ++q) s += sh[q];
-      if (mode == 2) {
-        *out_norm = sqrt(s);
-      } else if (k < ncols) {
-        if (mode == 0) hcol[k] = s; else { hcol[k] += s; st->wn2 = 0.0; }
-      } else if (mode == 0) {
-        st->h0 = sqrt(s);
-        double proj = 0.0;
-        for (int q = 0; q < ncols; ++q) proj += hcol[q] * hcol[q];
-        st->reorth = (s - proj < 0.5 * s) ? 1 : 0;
-      }
-    }
-    __syncthreads();
+    if (lane == 0) sums[k] = acc;
+  }
+  __syncthreads();
+  if (mode == 2) {
+    if (threadIdx.x == 0) *out_norm = sqrt(sums[0]);
+    return;
+  }
+  if (mode == 1) {
+    for (int k = threadIdx.x; k < ncols; k += blockDim.x) hcol[k] += sums[k];
+    if (threadIdx.x == 0) st->wn2 = 0.0;
+    return;
+  }
+  for (int k = threadIdx.x; k < ncols; k += blockDim.x) hcol[k] = sums[k];
+  if (threadIdx.x == 0) {
+    const double sw = sums[ncols];
+    st->h0 = sqrt(sw);
+    double proj = 0.0;
+    for (int q = 0; q < ncols; ++q) proj += sums[q] * sums[q];
+    st->reorth = (sw - proj < 0.5 * sw) ? 1 : 0;
   }
 }
 
@@ -1061,6 +1199,7 @@ __global__ void maxpy_kernel(int ndof, const double* __restrict__ V, int ncols, 
   if (pass == 1 && !st->reorth) return;
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += gridDim.x * blockDim.x) {
     double acc = w[idx];
+#pragma unroll 8
     for (int k = 0; k < ncols; ++k) acc -= coef[k] * V[(size_t)k * ndof + idx];
     w[idx] = acc;
   }
@@ -1079,44 +1218,59 @@ __device__ void givens_rot(double f, double g, double& c, double& s, double& r) 
 
 // Finish Arnoldi column `col`: h1, breakdown, rotations, S, presid, done flag.
 // H is stored like SciPy's h[col, k] (row col = column of the Hessenberg matrix).
+// New Hessenberg column: fold in the second-pass coefficients, apply the
+// previous Givens rotations, generate this column's rotation and update the
+// residual vector S.  The block stages the column and the rotations in
+// shared memory; thread 0 applies them in order (the same arithmetic as a
+// serial pass over global memory, without its dependent round trips).
 __global__ void gm_column_kernel(double* H, int ldh, double* givens, double* S, GmState* st, int col,
                                  const double* w_norm, const double* hcol2) {
   if (st->done) return;
+  extern __shared__ double shc[];       // [col + 2] column, then [2 col] rotations
+  double* sg = shc + col + 2;
   double* hc = H + (size_t)col * ldh;
-  if (st->reorth) {
-    // second-pass coefficients were accumulated into hcol2; fold them in
-    for (int k = 0; k <= col; ++k) hc[k] += hcol2[k];
+  const bool reorth = st->reorth != 0;
+  for (int k = threadIdx.x; k <= col; k += blockDim.x) {
+    double v = hc[k];
+    if (reorth) v += hcol2[k];   // second-pass coefficients
+    shc[k] = v;
   }
-  const double eps = 2.220446049250313e-16;
-  double h1 = *w_norm;
-  hc[col + 1] = h1;
-  int breakdown = 0;
-  if (h1 <= eps * st->h0) {
-    hc[col + 1] = 0.0;
-    breakdown = 1;
-    st->scal = 1.0;
-  } else {
-    st->scal = 1.0 / h1;
+  for (int k = threadIdx.x; k < 2 * col; k += blockDim.x) sg[k] = givens[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const double eps = 2.220446049250313e-16;
+    double h1 = *w_norm;
+    shc[col + 1] = h1;
+    int breakdown = 0;
+    if (h1 <= eps * st->h0) {
+      shc[col + 1] = 0.0;
+      breakdown = 1;
+      st->scal = 1.0;
+    } else {
+      st->scal = 1.0 / h1;
+    }
+    for (int k = 0; k < col; ++k) {
+      const double c = sg[2 * k], s = sg[2 * k + 1];
+      const double n0 = shc[k], n1 = shc[k + 1];
+      shc[k] = c * n0 + s * n1;
+      shc[k + 1] = -s * n0 + c * n1;
+    }
+    double c, s, mag;
+    givens_rot(shc[col], shc[col + 1], c, s, mag);
+    givens[2 * col] = c;
+    givens[2 * col + 1] = s;
+    shc[col] = mag;
+    shc[col + 1] = 0.0;
+    const double t = -s * S[col];
+    S[col] = c * S[col];
+    S[col + 1] = t;
+    st->presid = fabs(t);
+    st->ncols = col + 1;
+    st->breakdown = breakdown;
+    if (st->presid <= st->ptol || breakdown) st->done = 1;
   }
-  for (int k = 0; k < col; ++k) {
-    double c = givens[2 * k], s = givens[2 * k + 1];
-    double n0 = hc[k], n1 = hc[k + 1];
-    hc[k] = c * n0 + s * n1;
-    hc[k + 1] = -s * n0 + c * n1;
-  }
-  double c, s, mag;
-  givens_rot(hc[col], hc[col + 1], c, s, mag);
-  givens[2 * col] = c;
-  givens[2 * col + 1] = s;
-  hc[col] = mag;
-  hc[col + 1] = 0.0;
-  double t = -s * S[col];
-  S[col] = c * S[col];
-  S[col + 1] = t;
-  st->presid = fabs(t);
-  st->ncols = col + 1;
-  st->breakdown = breakdown;
-  if (st->presid <= st->ptol || breakdown) st->done = 1;
+  __syncthreads();
+  for (int k = threadIdx.x; k <= col + 1; k += blockDim.x) hc[k] = shc[k];
 }
 
 __global__ void gm_scale_kernel(int ndof, const double* w, double* vout, const GmState* st) {
@@ -1316,13 +1470,29 @@ int precond_L(tpf_ppe* h, const double* r, double* z, cudaStream_t s, const int*
       // additive shifted line solves: z = (sum_a T_a^-1 r) / ndim, r[pin] = 0, z[pin] = 0
       for (int ax = 0; ax < h->ndim; ++ax) {
         LineArgs L = line_args(g, ax);
-        int blocks = (L.lines + 127) / 128;
-        if (ax == 0)
-          thomas_solve_kernel<false><<<blocks, 128, 0, s>>>(L, h->tlo[ax], h->tden[ax], h->tcp[ax], r, z, h->t2,
-                                                            g.pin, 1.0, done);
-        else
-          thomas_solve_kernel<true><<<blocks, 128, 0, s>>>(L, h->tlo[ax], h->tden[ax], h->tcp[ax], r, z, h->t2,
-                                                           g.pin, ax == h->ndim - 1 ? 1.0 / h->ndim : 1.0, done);
+        const double sc = ax == h->ndim - 1 ? 1.0 / h->ndim : 1.0;
+        const int wblocks = (L.lines + 3) / 4;   // one warp per line, 4 lines per block
+#define TPF_THOMAS_WARP(KK)                                                                                    \
+  if (ax == 0)                                                                                                 \
+    thomas_warp_kernel<false, KK><<<wblocks, 128, 0, s>>>(L, h->tlo[ax], h->tden[ax], h->tcp[ax], r, z, g.pin, \
+                                                          1.0, done);                                          \
+  else                                                                                                         \
+    thomas_warp_kernel<true, KK><<<wblocks, 128, 0, s>>>(L, h->tlo[ax], h->tden[ax], h->tcp[ax], r, z, g.pin,  \
+                                                         sc, done);
+        if (L.n <= 32 * 4) { TPF_THOMAS_WARP(4) }
+        else if (L.n <= 32 * 9) { TPF_THOMAS_WARP(9) }
+        else if (L.n <= 32 * 17) { TPF_THOMAS_WARP(17) }
+        else if (L.n <= 32 * 33) { TPF_THOMAS_WARP(33) }
+        else {
+          const int blocks = (L.lines + 127) / 128;
+          if (ax == 0)
+            thomas_solve_kernel<false><<<blocks, 128, 0, s>>>(L, h->tlo[ax], h->tden[ax], h->tcp[ax], r, z, h->t2,
+                                                              g.pin, 1.0, done);
+          else
+            thomas_solve_kernel<true><<<blocks, 128, 0, s>>>(L, h->tlo[ax], h->tden[ax], h->tcp[ax], r, z, h->t2,
+                                                             g.pin, sc, done);
+        }
+#undef TPF_THOMAS_WARP
       }
       if (h->ndim == 1) { /* unreachable: ndim >= 2 */ }
     }
@@ -1334,7 +1504,7 @@ int precond_L(tpf_ppe* h, const double* r, double* z, cudaStream_t s, const int*
 int norm2_dev(tpf_ppe* h, const double* w, double* out, cudaStream_t s) {
   int nb = std::min(h->ew_blocks, h->part_len / 2);
   mdot_kernel<<<nb, 256, 8 * 32 * sizeof(double), s>>>(h->g.ndof, nullptr, 0, w, h->part, nullptr);
-  mdot_finalize_kernel<<<1, 256, 0, s>>>(h->part, nb, 0, nullptr, h->gst, 2, out);
+  mdot_finalize_kernel<<<1, 1024, sizeof(double), s>>>(h->part, nb, 0, nullptr, h->gst, 2, out);
   TPF_CUDA_TRY(cudaGetLastError());
   return TPF_OK;
 }
@@ -1395,7 +1565,9 @@ int solve_gmres(tpf_ppe* h, const double* rhs, double* p, const double* p_init, 
   double ptol = Mb_nrm2 * std::min(ptol_max_factor, atol / bnrm2);
   double presid = 0.0, rnorm = INFINITY;
   const bool x_nonzero = p_init != nullptr;
-  const int nb_dot = std::min(h->ew_blocks, h->part_len / (m + 2));
+  // four blocks per SM for the basis dot products: enough loads in flight,
+  // few partials to sum per vector
+  const int nb_dot = std::min(std::min(h->ew_blocks, h->part_len / (m + 2)), std::max(1, 4 * tpf::sm_count()));
   const int* done = &h->gst->done;
   bool converged = false;
   for (long long iteration = 0; iteration < h->o.maxiter; ++iteration) {
@@ -1426,15 +1598,18 @@ int solve_gmres(tpf_ppe* h, const double* rhs, double* p, const double* p_init, 
       if ((st = precond_L(h, t, w, s, done))) return st;
       double* hc = H + (size_t)col * ldh;
       mdot_kernel<<<nb_dot, 256, 8 * 32 * sizeof(double), s>>>(n, h->V, col + 1, w, h->part, done);
-      mdot_finalize_kernel<<<1, 256, 0, s>>>(h->part, nb_dot, col + 1, hc, h->gst, 0, nullptr);
+      mdot_finalize_kernel<<<1, 1024, (col + 2) * sizeof(double), s>>>(h->part, nb_dot, col + 1, hc, h->gst, 0,
+                                                                       nullptr);
       maxpy_kernel<<<ew_grid(h), 256, 0, s>>>(n, h->V, col + 1, hc, w, h->gst, 0);
       // conditional re-orthogonalization pass (hcol2 accumulates its coefficients)
       TPF_CUDA_TRY(cudaMemsetAsync(hcol2, 0, sizeof(double) * (col + 1), s));
       mdot_kernel<<<nb_dot, 256, 8 * 32 * sizeof(double), s>>>(n, h->V, col + 1, w, h->part, done);
-      mdot_finalize_kernel<<<1, 256, 0, s>>>(h->part, nb_dot, col + 1, hcol2, h->gst, 1, nullptr);
+      mdot_finalize_kernel<<<1, 1024, (col + 2) * sizeof(double), s>>>(h->part, nb_dot, col + 1, hcol2, h->gst,
+                                                                       1, nullptr);
       maxpy_kernel<<<ew_grid(h), 256, 0, s>>>(n, h->V, col + 1, hcol2, w, h->gst, 1);
       if ((st = norm2_dev(h, w, wnorm, s))) return st;
-      gm_column_kernel<<<1, 1, 0, s>>>(H, ldh, givens, S, h->gst, col, wnorm, hcol2);
+      gm_column_kernel<<<1, 128, (3 * col + 2) * sizeof(double), s>>>(H, ldh, givens, S, h->gst, col, wnorm,
+                                                                     hcol2);
       gm_scale_kernel<<<ew_grid(h), 256, 0, s>>>(n, w, h->V + (size_t)(col + 1) * n, h->gst);
       TPF_CUDA_TRY(cudaGetLastError());
     }
