@@ -27,6 +27,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <mutex>
 #include <vector>
 
@@ -1363,6 +1364,9 @@ struct tpf_ppe {
   int part_len = 0;
   unsigned int* bar = nullptr;
   int* err = nullptr;
+  cudaGraphExec_t gm_exec = nullptr;   // one GMRES restart cycle, captured
+  cudaStream_t cap = nullptr;          // stream the cycle is captured on (never the caller's)
+  long long gm_key[6] = {};
   double* band_pub = nullptr;     // halo rows of the band-resident PCG
   size_t band_pub_len = 0;
   int cg_kernel = 0;              // 0 auto, 1 global-memory persistent PCG, 2 band-resident PCG
@@ -1434,6 +1438,20 @@ int ensure_gmres(tpf_ppe* h) {
 
 int ew_grid(const tpf_ppe* h) { return h->ew_blocks; }
 
+// the truncated-PCR kernels may use up to 227 KB of dynamic shared memory (set
+// once, before any stream capture)
+int pcr_attributes() {
+  static int done_attr = 0;
+  if (!done_attr) {
+    TPF_CUDA_TRY(cudaFuncSetAttribute(pcr_solve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      227 * 1024));
+    TPF_CUDA_TRY(cudaFuncSetAttribute(pcr_solve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      227 * 1024));
+    done_attr = 1;
+  }
+  return TPF_OK;
+}
+
 // z = M^-1 r on the unweighted system (reference preconditioners), done-guarded
 int precond_L(tpf_ppe* h, const double* r, double* z, cudaStream_t s, const int* done) {
   const Grid3& g = h->g;
@@ -1452,17 +1470,14 @@ int precond_L(tpf_ppe* h, const double* r, double* z, cudaStream_t s, const int*
         const size_t smem = sizeof(double) * 8 * (size_t)L.n;
         TPF_CHECK_ARG(smem <= 227 * 1024, "truncated-PCR line solve: lines of %d nodes exceed shared memory", L.n);
         const double sc = (ax == h->ndim - 1) ? 1.0 / h->ndim : 1.0;
-        if (ax == 0) {
-          TPF_CUDA_TRY(cudaFuncSetAttribute(pcr_solve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)smem));
+        const int ast = pcr_attributes();
+        if (ast) return ast;
+        if (ax == 0)
           pcr_solve_kernel<false><<<L.lines, 256, smem, s>>>(L, h->tlo[ax], h->tden[ax], h->tcp[ax], r, z, g.pin,
                                                               nstage, 1.0, done);
-        } else {
-          TPF_CUDA_TRY(cudaFuncSetAttribute(pcr_solve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)smem));
+        else
           pcr_solve_kernel<true><<<L.lines, 256, smem, s>>>(L, h->tlo[ax], h->tden[ax], h->tcp[ax], r, z, g.pin,
                                                              nstage, sc, done);
-        }
       }
       break;
     }
@@ -1570,6 +1585,40 @@ int solve_gmres(tpf_ppe* h, const double* rhs, double* p, const double* p_init, 
   const int nb_dot = std::min(std::min(h->ew_blocks, h->part_len / (m + 2)), std::max(1, 4 * tpf::sm_count()));
   const int* done = &h->gst->done;
   bool converged = false;
+  // One restart cycle (m Arnoldi columns).  Every kernel of a column skips
+  // its work once the device-side state says the cycle is done, so the whole
+  // cycle is captured once as a CUDA graph and replayed; the key holds what
+  // its launches depend on (the buffers are fixed per handle and prepare
+  // rewrites the preconditioner arrays in place).
+  const Geo geo{{h->dv[0], h->dv[1], h->dv[2]}, {h->dface[0], h->dface[1], h->dface[2]}};
+  auto enqueue_cycle = [&](cudaStream_t s) -> int {
+    int est;
+    for (int col = 0; col < m; ++col) {
+      const double* vc = h->V + (size_t)col * n;
+      apply_L_kernel<<<ew_grid(h), 256, 0, s>>>(g, geo, h->s[0], h->s[1], h->s[2], vc, t, nullptr, done);
+      if ((est = precond_L(h, t, w, s, done))) return est;
+      double* hc = H + (size_t)col * ldh;
+      mdot_kernel<<<nb_dot, 256, 8 * 32 * sizeof(double), s>>>(n, h->V, col + 1, w, h->part, done);
+      mdot_finalize_kernel<<<1, 1024, (col + 2) * sizeof(double), s>>>(h->part, nb_dot, col + 1, hc, h->gst, 0,
+                                                                       nullptr);
+      maxpy_kernel<<<ew_grid(h), 256, 0, s>>>(n, h->V, col + 1, hc, w, h->gst, 0);
+      // conditional re-orthogonalization pass (hcol2 accumulates its coefficients)
+      TPF_CUDA_TRY(cudaMemsetAsync(hcol2, 0, sizeof(double) * (col + 1), s));
+      mdot_kernel<<<nb_dot, 256, 8 * 32 * sizeof(double), s>>>(n, h->V, col + 1, w, h->part, done);
+      mdot_finalize_kernel<<<1, 1024, (col + 2) * sizeof(double), s>>>(h->part, nb_dot, col + 1, hcol2, h->gst,
+                                                                       1, nullptr);
+      maxpy_kernel<<<ew_grid(h), 256, 0, s>>>(n, h->V, col + 1, hcol2, w, h->gst, 1);
+      if ((est = norm2_dev(h, w, wnorm, s))) return est;
+      gm_column_kernel<<<1, 128, (3 * col + 2) * sizeof(double), s>>>(H, ldh, givens, S, h->gst, col, wnorm,
+                                                                     hcol2);
+      gm_scale_kernel<<<ew_grid(h), 256, 0, s>>>(n, w, h->V + (size_t)(col + 1) * n, h->gst);
+      TPF_CUDA_TRY(cudaGetLastError());
+    }
+    return TPF_OK;
+  };
+  const long long key[6] = {(long long)m, (long long)nb_dot, (long long)h->o.precond, (long long)h->o.pcr_stages,
+                            (long long)(intptr_t)h->V, (long long)n};
+  if (h->o.precond == TPF_PRECOND_LINE_PCR && (st = pcr_attributes())) return st;
   for (long long iteration = 0; iteration < h->o.maxiter; ++iteration) {
     if (iteration == 0) {
       if (x_nonzero) {
@@ -1591,28 +1640,38 @@ int solve_gmres(tpf_ppe* h, const double* rhs, double* p, const double* p_init, 
     double v0n = 0.0;
     if ((st = read_scalar(wnorm, &v0n, s))) return st;
     gm_start_kernel<<<ew_grid(h), 256, 0, s>>>(n, w, h->V, S, m + 1, h->gst, v0n, ptol);
-    const Geo geo{{h->dv[0], h->dv[1], h->dv[2]}, {h->dface[0], h->dface[1], h->dface[2]}};
-    for (int col = 0; col < m; ++col) {
-      const double* vc = h->V + (size_t)col * n;
-      apply_L_kernel<<<ew_grid(h), 256, 0, s>>>(g, geo, h->s[0], h->s[1], h->s[2], vc, t, nullptr, done);
-      if ((st = precond_L(h, t, w, s, done))) return st;
-      double* hc = H + (size_t)col * ldh;
-      mdot_kernel<<<nb_dot, 256, 8 * 32 * sizeof(double), s>>>(n, h->V, col + 1, w, h->part, done);
-      mdot_finalize_kernel<<<1, 1024, (col + 2) * sizeof(double), s>>>(h->part, nb_dot, col + 1, hc, h->gst, 0,
-                                                                       nullptr);
-      maxpy_kernel<<<ew_grid(h), 256, 0, s>>>(n, h->V, col + 1, hc, w, h->gst, 0);
-      // conditional re-orthogonalization pass (hcol2 accumulates its coefficients)
-      TPF_CUDA_TRY(cudaMemsetAsync(hcol2, 0, sizeof(double) * (col + 1), s));
-      mdot_kernel<<<nb_dot, 256, 8 * 32 * sizeof(double), s>>>(n, h->V, col + 1, w, h->part, done);
-      mdot_finalize_kernel<<<1, 1024, (col + 2) * sizeof(double), s>>>(h->part, nb_dot, col + 1, hcol2, h->gst,
-                                                                       1, nullptr);
-      maxpy_kernel<<<ew_grid(h), 256, 0, s>>>(n, h->V, col + 1, hcol2, w, h->gst, 1);
-      if ((st = norm2_dev(h, w, wnorm, s))) return st;
-      gm_column_kernel<<<1, 128, (3 * col + 2) * sizeof(double), s>>>(H, ldh, givens, S, h->gst, col, wnorm,
-                                                                     hcol2);
-      gm_scale_kernel<<<ew_grid(h), 256, 0, s>>>(n, w, h->V + (size_t)(col + 1) * n, h->gst);
-      TPF_CUDA_TRY(cudaGetLastError());
+    if (!h->gm_exec || std::memcmp(h->gm_key, key, sizeof(key)) != 0) {
+      if (h->gm_exec) { cudaGraphExecDestroy(h->gm_exec); h->gm_exec = nullptr; }
+      // captured on a private stream (the caller's may be the legacy default
+      // stream, which cannot be captured); replayed on the caller's
+      if (!h->cap && cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        h->cap = nullptr;
+        tpf::set_error("cudaStreamCreate failed");
+        return TPF_ECUDA;
+      }
+      TPF_CUDA_TRY(cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal));
+      const int cst = enqueue_cycle(h->cap);
+      cudaGraph_t graph = nullptr;
+      const cudaError_t ce = cudaStreamEndCapture(h->cap, &graph);
+      if (cst || ce != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        if (cst) return cst;
+        tpf::set_error("capturing the GMRES cycle failed: %s", cudaGetErrorString(ce));
+        return TPF_ECUDA;
+      }
+      const cudaError_t ie = cudaGraphInstantiate(&h->gm_exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ie != cudaSuccess) {
+        h->gm_exec = nullptr;
+        cudaGetLastError();
+        tpf::set_error("instantiating the GMRES cycle graph failed: %s", cudaGetErrorString(ie));
+        return TPF_ECUDA;
+      }
+      std::memcpy(h->gm_key, key, sizeof(key));
     }
+    TPF_CUDA_TRY(cudaGraphLaunch(h->gm_exec, s));
     GmState hs{};
     TPF_CUDA_TRY(cudaMemcpyAsync(&hs, h->gst, sizeof(GmState), cudaMemcpyDeviceToHost, s));
     TPF_CUDA_TRY(cudaStreamSynchronize(s));
@@ -1906,6 +1965,8 @@ int tpf_ppe_create(tpf_ppe** out, int ndim, const int64_t* N, const double* cons
 
 int tpf_ppe_destroy(tpf_ppe* h) {
   if (!h) return TPF_OK;
+  if (h->gm_exec) cudaGraphExecDestroy(h->gm_exec);
+  if (h->cap) cudaStreamDestroy(h->cap);
   for (void* p : h->allocs) cudaFree(p);
   delete h;
   return TPF_OK;
