@@ -1290,8 +1290,8 @@ __global__ void __launch_bounds__(128) ccd_lane_kernel(CcdArgs a, const T* __res
 #pragma unroll
           for (int q = 0; q < CR; ++q) {
             if (q < cnt) {
-              *o1 = yr[q].a;
-              *o2 = yr[q].b;
+              __stcs(o1, yr[q].a);   // streaming: keep L2 for the lines pass 2 re-reads
+              __stcs(o2, yr[q].b);
               o1 += inner;
               o2 += inner;
             }
