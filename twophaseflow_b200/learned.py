@@ -160,6 +160,28 @@ class UNet:
         np.savez(path, params=self.get_params(), **meta)
 
 
+def load_meta(path: str = DEFAULT_WEIGHTS) -> dict:
+    """Training metadata stored beside the parameters ({} when absent)."""
+    import json
+    with np.load(path) as d:
+        if "meta" not in d.files:
+            return {}
+        return json.loads(str(d["meta"]))
+
+
+def default_coarsen(shape, meta=None) -> int:
+    """Aggregation that puts the network's coarse grid nearest the size it was
+    trained on (grid / coarsen of the training run, 512 / 4 = 128 cells for the
+    shipped weights): 4, or 8 once the grid has more than ~5.7x that many
+    cells per axis.  Both were validated on held-out fields (4 at 512^2, 8 at
+    1024^2); with 4 at 1024^2 the coarse problem outgrows the network's
+    receptive field and flexible CG stalls."""
+    meta = meta or {}
+    c_train = float(meta.get("grid", 512)) / float(meta.get("coarsen", 4))
+    cells = max(int(n) - 1 for n in shape)
+    return 8 if cells / c_train > 4 * np.sqrt(2.0) else 4
+
+
 def load_params(path: str = DEFAULT_WEIGHTS) -> np.ndarray:
     if not os.path.exists(path):
         raise FileNotFoundError(
@@ -175,9 +197,11 @@ class PPESolverLearned(PPESolverFVMMatrixFree):
     """IPPESolver: flexible CG preconditioned by the trained U-Net (2-D, wall).
 
     Options are read from the solver config like the reference's own
-    (``pseudo_tol``, ``pseudo_maxiter``) plus ``ppe_learned_coarsen`` (4: the
-    network solves the problem aggregated over 4 x 4 node blocks inside a
-    two-grid cycle; 1: the network reads the fine residual),
+    (``pseudo_tol``, ``pseudo_maxiter``) plus ``ppe_learned_coarsen`` (b > 1:
+    the network solves the problem aggregated over b x b node blocks inside a
+    two-grid cycle; 1: the network reads the fine residual; default: 4 or 8,
+    whichever puts the coarse grid nearest the training size, see
+    ``default_coarsen``),
     ``ppe_learned_smooth`` (damped Jacobi sweeps after the network, default 3),
     ``ppe_learned_omega`` (0.8), ``ppe_learned_weights`` (path of the trained
     parameters) and ``ppe_learned_fallback`` (finish with plain Jacobi PCG on a
@@ -200,10 +224,14 @@ class PPESolverLearned(PPESolverFVMMatrixFree):
         self.omega = float(getattr(solver_cfg, "ppe_learned_omega", 0.8))
         self.fallback = bool(getattr(solver_cfg, "ppe_learned_fallback", True))
         self.learned_maxiter = int(getattr(solver_cfg, "ppe_learned_maxiter", max(self.maxiter, 2000)))
-        self.coarsen = int(getattr(solver_cfg, "ppe_learned_coarsen", 4))
         self.window = int(getattr(solver_cfg, "ppe_learned_window", 8))
+        meta = {}
         if params is None:
-            params = load_params(str(getattr(solver_cfg, "ppe_learned_weights", DEFAULT_WEIGHTS)))
+            wpath = str(getattr(solver_cfg, "ppe_learned_weights", DEFAULT_WEIGHTS))
+            params = load_params(wpath)
+            meta = load_meta(wpath)
+        coarsen = getattr(solver_cfg, "ppe_learned_coarsen", None)
+        self.coarsen = int(coarsen) if coarsen is not None else default_coarsen(self.grid.shape, meta)
         H, W = net_image(self.grid.shape, self.coarsen)
         self.net = UNet(H, W, 1, params=params)
         self._lp = None
