@@ -187,6 +187,49 @@ def time_learned(rho_d, rhs_d, steps, warmup, flush):
     return s, p, times
 
 
+def learned_heldout(sizes=((512, 512), (1024, 1024)), seeds=(11, 12, 13)):
+    """Learned preconditioner against plain FP64 PCG on density fields that were
+    used neither in training nor in choosing its settings (12 droplets, seeded
+    as the benchmark field): one warm-up and one timed solve of each, CUDA
+    events, to 1e-8 relative residual."""
+    import torch
+    from twophaseflow_b200 import PPESolverFVMMatrixFree, UniformGrid
+    from twophaseflow_b200.learned import PPESolverLearned
+    from twophaseflow_b200.workloads import divergence_rhs, droplet_density
+
+    def timed(solver, rhs, rho):
+        solver.solve(rhs, rho)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        p = solver.solve(rhs, rho)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), p
+
+    out = {}
+    for N in sizes:
+        pc = PPESolverFVMMatrixFree(None, _Cfg(pseudo_tol=TOL, pseudo_maxiter=1_000_000, ppe_iteration_method="cg",
+                                               ppe_preconditioner="jacobi"), UniformGrid(N))
+        lr = PPESolverLearned(None, _Cfg(pseudo_tol=TOL, pseudo_maxiter=1_000_000, ppe_learned_maxiter=20000),
+                              UniformGrid(N))
+        rows = []
+        for seed in seeds:
+            rho = torch.from_numpy(droplet_density(N, seed=seed)).cuda()
+            rhs = torch.from_numpy(divergence_rhs(N, seed=seed + 100)).cuda()
+            tp, pp = timed(pc, rhs, rho)
+            tl, pl = timed(lr, rhs, rho)
+            d = lr.last_diagnostics
+            diff = float(torch.max(torch.abs((pl - pl.mean()) - (pp - pp.mean()))) / torch.max(torch.abs(pp - pp.mean())))
+            rows.append({"seed": seed, "pcg_ms": round(tp, 2), "pcg_iterations": pc.last_diagnostics["ppe_low_order_cg_iterations"],
+                         "learned_ms": round(tl, 2), "learned_iterations": d["ppe_learned_iterations"],
+                         "fallback_iterations": d["ppe_learned_fallback_iterations"], "max_rel_diff": diff})
+        geo = float(np.exp(np.mean([np.log(r["pcg_ms"] / r["learned_ms"]) for r in rows])))
+        out[f"{N[0]}x{N[1]}"] = {"coarsen": lr.coarsen, "fields": rows, "speedup_geomean": round(geo, 3)}
+    return out
+
+
 def time_ppe_e2e(precision, rho_h, rhs_h, steps, warmup):
     """Public API with host NumPy inputs; H2D + solve + D2H inside the timed region."""
     import torch
@@ -309,6 +352,8 @@ def main(argv=None):
     slr, plr, tlr = time_learned(rho_d, rhs_d, max(2, args.steps // 3), 1, flush)
     _barrier(ws)
     dlr = slr.last_diagnostics
+    heldout = learned_heldout()
+    _barrier(ws)
     ms_mx = _max_over_ranks(float(np.mean(tmx)), ws)
     ms_64 = _max_over_ranks(float(np.mean(t64)), ws)
     ms_lr = _max_over_ranks(float(np.mean(tlr)), ws)
@@ -372,6 +417,7 @@ def main(argv=None):
                         "rel_residual": dlr["ppe_learned_relative_residual"], "max_rel_diff_vs_fp64": err_lr,
                         "us_per_iteration": round(ms_lr * 1e3 / max(1, dlr["ppe_learned_iterations"]), 1)},
             "learned_speedup_vs_plain_fp64": round(ms_64 / ms_lr, 3),
+            "learned_heldout": heldout,
             "mixed_speedup_vs_plain_fp64": round(ms_64 / ms_mx, 3),
             "batched_32_cases": bat,
             "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": 2 * ndof * 8,
