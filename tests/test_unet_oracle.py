@@ -50,3 +50,18 @@ def test_loss_gradient():
     y2[1, 2, 3] += h
     L2, _ = ou.loss(y2, t)
     assert abs((L2 - L) / h - dy[1, 2, 3]) < 1e-4
+
+
+def test_default_aggregation_matches_training_coarse_size():
+    """The learned solver aggregates so that the network's coarse grid is
+    nearest the size it was trained on (grid / coarsen of the training run,
+    read from the weights' metadata): 4 x 4 up to ~720 cells per axis for the
+    shipped 512 / 4 training, 8 x 8 beyond."""
+    from twophaseflow_b200.learned import default_coarsen, load_meta
+    meta = load_meta()
+    assert meta["grid"] == 512 and meta["coarsen"] == 4
+    assert [default_coarsen((n + 1, n + 1), meta) for n in (64, 256, 512, 700)] == [4, 4, 4, 4]
+    assert [default_coarsen((n + 1, n + 1), meta) for n in (1024, 2048)] == [8, 8]
+    assert default_coarsen((1025, 257), meta) == 8          # the longest axis decides
+    assert default_coarsen((1025, 1025), {"grid": 1024, "coarsen": 4}) == 4   # other training sizes
+    assert default_coarsen((513, 513), {}) == 4              # no metadata: the shipped training size

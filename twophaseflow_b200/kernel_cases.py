@@ -4,6 +4,7 @@
     python -m twophaseflow_b200.kernel_cases ppe --N 512 512 [--precision fp64] [--reps 2]
     python -m twophaseflow_b200.kernel_cases learned --N 512 512 [--maxiter 16] [--reps 2]
     python -m twophaseflow_b200.kernel_cases batched --N 32 [--reps 3]     (32 cases, grids 128..512)
+    python -m twophaseflow_b200.kernel_cases gmres --N 512 512 [--line thomas|pcr] [--maxiter 2] [--reps 1]
 
 ``ccd`` captures ``reps`` CCDSolver.differentiate calls in one CUDA graph and
 replays it, so the reported time is device time per call (no Python launch
@@ -175,16 +176,61 @@ def batched_case(n_cases=32, nmin=128, nmax=512, reps=3, seed=0, tol=1e-8):
             "iterations_total": int(sum(its))}
 
 
+def gmres_case(N, line, reps, maxiter=None, tol=1e-8):
+    """GMRES(80) with the shifted line preconditioner (the reference's default
+    PPE route) on the droplet PPE; ``maxiter`` bounds the restart cycles (the
+    solve then stops with the reference's non-convergence error, which is
+    expected) for profiling a fixed amount of work."""
+    import time
+    import torch
+    from . import PPESolverFVMMatrixFree, UniformGrid
+    from .workloads import divergence_rhs, droplet_density
+
+    class Cfg:
+        pseudo_tol = tol
+        pseudo_maxiter = maxiter if maxiter else 100000
+        ppe_iteration_method = "gmres"
+        ppe_preconditioner = "line_pcr"
+        ppe_restart = 80
+        ppe_line_solver = line
+
+    rho = torch.from_numpy(droplet_density(N, seed=0)).cuda()
+    rhs = torch.from_numpy(divergence_rhs(N, seed=1)).cuda()
+    s = PPESolverFVMMatrixFree(None, Cfg(), UniformGrid(N))
+
+    def run():
+        try:
+            s.solve(rhs, rho)
+        except RuntimeError:
+            if not maxiter:
+                raise
+
+    ts = []
+    for _ in range(max(1, reps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        run()
+        torch.cuda.synchronize()
+        ts.append((time.perf_counter() - t0) * 1e3)
+    d = s.last_diagnostics
+    it = d.get("ppe_low_order_gmres_iterations", 0)
+    ms = min(ts)
+    return {"case": "gmres", "N": list(N), "line": line, "ms": round(ms, 2), "iterations": it,
+            "us_per_iteration": round(ms * 1e3 / max(it, 1), 1)}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["ccd", "ppe", "learned", "batched"])
+    ap.add_argument("case", choices=["ccd", "ppe", "learned", "batched", "gmres"])
+    ap.add_argument("--line", default="thomas", choices=["thomas", "pcr"], help="gmres: line solver")
     ap.add_argument("--N", type=int, nargs="+", required=True)
     ap.add_argument("--axis", type=int, default=0)
     ap.add_argument("--bc", default="wall")
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--reps", type=int, default=5)
-    ap.add_argument("--maxiter", type=int, default=0, help="learned: stop after this many iterations")
+    ap.add_argument("--maxiter", type=int, default=0,
+                    help="learned: stop after this many iterations; gmres: after this many restart cycles")
     a = ap.parse_args(argv)
     if a.case == "ccd":
         r = ccd_case(tuple(a.N), a.axis, a.bc, a.dtype, a.reps)
@@ -192,6 +238,8 @@ def main(argv=None):
         r = ppe_case(tuple(a.N), a.precision, a.reps)
     elif a.case == "learned":
         r = learned_case(tuple(a.N), a.reps, a.maxiter or None)
+    elif a.case == "gmres":
+        r = gmres_case(tuple(a.N), a.line, a.reps, a.maxiter or None)
     else:
         r = batched_case(n_cases=a.N[0], reps=a.reps)
     print(json.dumps(r), flush=True)
