@@ -106,6 +106,27 @@ int tpf_ccd_apply_vd(const tpf_ccd_plan* plan, int64_t outer, int64_t inner,
                      const void* f, const void* rho, const void* drho,
                      void* out, int accumulate, int flags, void* stream);
 
+/* Velocity corrector fused into the CCD line solve
+ * (VelocityCorrector.correct with ccd_pressure_gradient,
+ * src/twophase/coupling/velocity_corrector.py:41-89):
+ *   u_out = u_star - (dt / rho) * dp/dx_axis
+ * with dp/dx_axis the CCD first derivative of pres along the plan's axis
+ * (metric applied when TPF_CCD_APPLY_METRIC), taken as 0 on wall planes
+ * (enforce_wall_neumann), i.e. u_out = u_star there.  u_out may be u_star
+ * (in place); pres must not alias the other arrays.  Dtype of the plan. */
+int tpf_ccd_apply_corrector(const tpf_ccd_plan* plan, int64_t outer, int64_t inner,
+                            const void* pres, const void* u_star, const void* rho, double dt,
+                            void* u_out, int flags, void* stream);
+
+/* CFL maxima (CFLCalculator.compute, src/twophase/time_integration/cfl.py:85-137):
+ * out[c] = max |comps[c][i]| for the ncomp (1..3) velocity components and, when
+ * mu and rho are given, out[3] = max mu[i] / rho[i] (values assumed >= 0; a
+ * NaN propagates).  n values each, dtype TPF_F64 / TPF_F32; out is a device
+ * array of 4 doubles (zeroed by the call); asynchronous on stream.  The time
+ * step itself is the host formula of the reference on these maxima. */
+int tpf_cfl_maxima(int64_t n, int ncomp, const void* const* comps, const void* mu, const void* rho,
+                   int dtype, double* out, void* stream);
+
 /* Zero grad at index 0 and n_pts-1 along the axis of a [outer, n, inner]
  * array (wall axes only; no-op for periodic plans).  Replaces
  * CCDSolver.enforce_wall_neumann (ccd_solver.py:264-281;

@@ -8,7 +8,10 @@ It imports the reference's ``twophase`` package read-only, runs its own CPU
 functions (``CCDSolver.differentiate``, ``PPESolverFVMMatrixFree``,
 ``PPESolverFVMSpsolve``, the batched tridiagonal helpers and the CCD
 variable-density Laplacian) on small seeded inputs and stores inputs and
-outputs in ``ccd_golden.npz`` / ``ppe_golden.npz`` next to this script.
+outputs in ``ccd_golden.npz`` / ``ppe_golden.npz`` next to this script;
+``step_golden.npz`` holds the steps either side of the PPE
+(``VelocityCorrector.correct``, ``ccd_pressure_gradient``,
+``CFLCalculator.compute``).
 """
 
 from __future__ import annotations
@@ -255,15 +258,56 @@ def make_ppe(out):
         out[f"{name}/Lp"] = np.asarray(compute_ccd_laplacian(p, rho, drho, ccd, be))
 
 
+def make_step(out):
+    """Velocity corrector and CFL time step of the reference on seeded fields."""
+    from twophase.backend import Backend
+    from twophase.config import GridConfig
+    from twophase.core.grid import Grid
+    from twophase.ccd.ccd_solver import CCDSolver
+    from twophase.coupling.velocity_corrector import VelocityCorrector, ccd_pressure_gradient
+    from twophase.time_integration.cfl import CFLCalculator
+
+    be = Backend(use_gpu=False)
+    rng = np.random.default_rng(4242)
+    cases = [("wall2d", (16, 12), "wall"), ("per2d", (16, 10), "periodic"), ("wall3d", (8, 10, 6), "wall")]
+    for name, N, bc in cases:
+        grid = Grid(GridConfig(ndim=len(N), N=N, L=tuple(1.0 + 0.25 * a for a in range(len(N)))), be)
+        ccd = CCDSolver(grid, be, bc_type=bc)
+        p = rng.standard_normal(grid.shape)
+        rho = 1e-3 + rng.uniform(0.0, 1.0, grid.shape)
+        mu = 1e-2 + rng.uniform(0.0, 1.0, grid.shape)
+        vel = [rng.standard_normal(grid.shape) for _ in range(len(N))]
+        dt = 0.0137
+        out[f"{name}/N"] = np.array(N)
+        out[f"{name}/L"] = np.array(grid.L, dtype=np.float64)
+        out[f"{name}/bc"] = np.array(bc)
+        out[f"{name}/p"] = p
+        out[f"{name}/rho"] = rho
+        out[f"{name}/mu"] = mu
+        out[f"{name}/dt"] = np.array(dt)
+        for ax in range(len(N)):
+            out[f"{name}/u{ax}"] = vel[ax]
+        grad = ccd_pressure_gradient(ccd, p, len(N))
+        corr = VelocityCorrector(be, grid, ccd).correct(vel, p, rho, dt)
+        for ax in range(len(N)):
+            out[f"{name}/grad{ax}"] = np.asarray(grad[ax])
+            out[f"{name}/unew{ax}"] = np.asarray(corr[ax])
+        for tag, kw in (("cn", dict(cn_viscous=True)), ("expl", dict(cn_viscous=False)),
+                        ("cap", dict(We=0.01, rho_ratio=0.1, cn_viscous=True))):
+            out[f"{name}/dt_{tag}"] = np.array(CFLCalculator(be, grid, 0.3, **kw).compute(vel, mu, rho))
+
+
 def main():
     src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
     _ref_import(src)
-    ccd_out, ppe_out = {}, {}
+    ccd_out, ppe_out, step_out = {}, {}, {}
     make_ccd(ccd_out)
     make_ppe(ppe_out)
+    make_step(step_out)
     np.savez_compressed(os.path.join(HERE, "ccd_golden.npz"), **ccd_out)
     np.savez_compressed(os.path.join(HERE, "ppe_golden.npz"), **ppe_out)
-    print("wrote", len(ccd_out), "ccd and", len(ppe_out), "ppe arrays")
+    np.savez_compressed(os.path.join(HERE, "step_golden.npz"), **step_out)
+    print("wrote", len(ccd_out), "ccd,", len(ppe_out), "ppe and", len(step_out), "step arrays")
 
 
 if __name__ == "__main__":

@@ -7,6 +7,9 @@
   variable-density operator L_H and the defect-correction PPE loop
 * ``register_with_reference`` -- installs the PPE solver in the reference's
   ``register_ppe_solver`` registry.
+* ``VelocityCorrector`` / ``CFLCalculator`` / ``ccd_pressure_gradient`` -- the
+  steps either side of the PPE (velocity correction fused into the CCD line
+  solve; CFL maxima in one reduction).
 
 All arithmetic runs in the in-tree CUDA library ``libtpf.so`` (C ABI:
 ``include/tpf.h``); build it with ``python -m twophaseflow_b200.build``.
@@ -17,6 +20,7 @@ from .ccd_ppe import CCDVariableDensityOperator, PPESolverDefectCorrection
 from .grid import BoundarySpec, UniformGrid
 from .ppe import (MatrixAssemblyUnavailable, PPESolverFVMMatrixFree, create_fvm_matrixfree, register_with_reference,
                   solve_batched)
+from .step import CFLCalculator, VelocityCorrector, ccd_pressure_gradient
 
 __all__ = [
     "CCDSolver",
@@ -29,4 +33,7 @@ __all__ = [
     "solve_batched",
     "UniformGrid",
     "BoundarySpec",
+    "VelocityCorrector",
+    "CFLCalculator",
+    "ccd_pressure_gradient",
 ]

@@ -88,6 +88,10 @@ SIGNATURES = {
                                 C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int, C.c_void_p]),
     "tpf_ccd_apply_vd": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "tpf_ccd_apply_corrector": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_double, C.c_void_p, C.c_int, C.c_void_p]),
+    "tpf_cfl_maxima": (C.c_int, [C.c_int64, C.c_int, C.POINTER(C.c_void_p), C.c_void_p, C.c_void_p, C.c_int,
+                                 C.c_void_p, C.c_void_p]),
     "tpf_ccd_enforce_wall_neumann": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]),
     "tpf_ppe_default_options": (None, [C.POINTER(tpf_ppe_options)]),
     "tpf_ppe_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_int64),

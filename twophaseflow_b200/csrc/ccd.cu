@@ -115,6 +115,13 @@ struct CcdArgs {
   const void* vd_drho;
   void* vd_out;
   int vd_accumulate;
+  // velocity-corrector epilogue: out = u* - (dt / rho) d1 instead of d1, d2;
+  // on wall planes (first / last node of a line) d1 counts as 0, so out = u*
+  const void* cr_u;
+  const void* cr_rho;
+  void* cr_out;
+  double cr_dt;
+  int cr_wall;
 };
 
 template <typename T>
@@ -123,6 +130,19 @@ struct V2 { T a, b; };
 // Write one node's result: either (d1, d2) or the variable-density term.
 template <typename T>
 __device__ __forceinline__ void store_out(const CcdArgs& a, int64_t gi, double o1, double o2) {
+  if (a.cr_out) {
+    // u_new = u* - (dt / rho) dp/dx, with the reference's operation order
+    // (quotient, product, difference; no fused multiply-add)
+    const double u = (double)static_cast<const T*>(a.cr_u)[gi];
+    double v = u;
+    const int64_t k = (gi / a.inner) % a.n;   // node along the line
+    if (!(a.cr_wall && (k == 0 || k == a.n - 1))) {
+      const double q = a.cr_dt / (double)static_cast<const T*>(a.cr_rho)[gi];
+      v = __dsub_rn(u, __dmul_rn(q, o1));
+    }
+    static_cast<T*>(a.cr_out)[gi] = (T)v;
+    return;
+  }
   if (a.vd_out) {
     const double r = (double)static_cast<const T*>(a.vd_rho)[gi];
     const double dr = (double)static_cast<const T*>(a.vd_drho)[gi];
@@ -1660,8 +1680,9 @@ int launch_lane(const tpf_ccd_plan* p, const CcdArgs& a, bool periodic, bool con
   const LaneShape def{4, std::is_same<T, double>::value ? 3 : 2, 64};
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   TPF_CUDA_TRY(cudaStreamIsCapturing(stream, &cs));
-  // an accumulating epilogue must run exactly once: no tuning runs for it
-  if (!p->autotune || cs != cudaStreamCaptureStatusNone || (a.vd_out && a.vd_accumulate))
+  // an accumulating (or in-place) epilogue must run exactly once: no tuning runs for it
+  if (!p->autotune || cs != cudaStreamCaptureStatusNone || (a.vd_out && a.vd_accumulate) ||
+      (a.cr_out && a.cr_out == a.cr_u))
     return run_lane<T>(p, a, periodic, contig, def, stream);
   const LaneShape cand[] = {{4, 3, 64}, {4, 2, 64}, {4, 3, 2}, {4, 2, 3}, {2, 3, 64}, {2, 2, 64}, {4, 2, 2}};
   cudaEvent_t e0, e1;
@@ -1699,11 +1720,13 @@ template <typename T>
 int launch_ccd(const tpf_ccd_plan* p, int64_t outer, int64_t inner, const void* f, void* d1, void* d2,
                const double* bcl, const double* bcr, int flags, cudaStream_t stream,
                const void* vd_rho = nullptr, const void* vd_drho = nullptr, void* vd_out = nullptr,
-               int vd_accumulate = 0) {
+               int vd_accumulate = 0, const CcdArgs* corrector = nullptr) {
   const bool contig = (inner == 1);
   const int64_t n_lines = outer * inner;
   if (n_lines == 0) return TPF_OK;
   TPF_CHECK_ARG(f != d1 && f != d2 && f != vd_out, "the CCD input must not alias an output array");
+  TPF_CHECK_ARG(!corrector || (f != corrector->cr_out && f != corrector->cr_u && f != corrector->cr_rho),
+                "the pressure must not alias the velocity or density arrays");
   TPF_CHECK_ARG(n_lines < ((int64_t)1 << 31), "too many lines");
   const bool warp = (p->C == 8 || p->C == 16 || p->C == 32) && p->n_rows <= 32 * p->C;
   LaunchShape s = !warp ? pick_shape<T>(p, contig, n_lines)
@@ -1732,6 +1755,13 @@ int launch_ccd(const tpf_ccd_plan* p, int64_t outer, int64_t inner, const void* 
   a.vd_drho = vd_drho;
   a.vd_out = vd_out;
   a.vd_accumulate = vd_accumulate;
+  if (corrector) {
+    a.cr_u = corrector->cr_u;
+    a.cr_rho = corrector->cr_rho;
+    a.cr_out = corrector->cr_out;
+    a.cr_dt = corrector->cr_dt;
+    a.cr_wall = corrector->cr_wall;
+  }
   const bool per = (p->bc == TPF_BC_PERIODIC) && !a.ovl && !a.ovr;
   if (use_lane_kernel(p, n_lines, per, contig)) return launch_lane<T>(p, a, per, contig, stream);
   void (*kern)(CcdArgs);
@@ -1872,6 +1902,26 @@ int tpf_ccd_apply_vd(const tpf_ccd_plan* p, int64_t outer, int64_t inner, const 
                               accumulate);
   return launch_ccd<float>(p, outer, inner, f, nullptr, nullptr, nullptr, nullptr, flags, s, rho, drho, out,
                            accumulate);
+}
+
+int tpf_ccd_apply_corrector(const tpf_ccd_plan* p, int64_t outer, int64_t inner, const void* pres,
+                            const void* u_star, const void* rho, double dt, void* u_out, int flags, void* stream) {
+  TPF_CHECK_ARG(p != nullptr, "plan is NULL");
+  TPF_CHECK_ARG(outer >= 0 && inner >= 1, "invalid line decomposition");
+  TPF_CHECK_ARG(pres && u_star && rho && u_out, "NULL argument");
+  TPF_CHECK_ARG(!(flags & TPF_CCD_APPLY_METRIC) || p->has_metric, "metric requested but not set");
+  CcdArgs cr{};
+  cr.cr_u = u_star;
+  cr.cr_rho = rho;
+  cr.cr_out = u_out;
+  cr.cr_dt = dt;
+  cr.cr_wall = (p->bc == TPF_BC_WALL) ? 1 : 0;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (p->dtype == TPF_F64)
+    return launch_ccd<double>(p, outer, inner, pres, nullptr, nullptr, nullptr, nullptr, flags, s, nullptr, nullptr,
+                              nullptr, 0, &cr);
+  return launch_ccd<float>(p, outer, inner, pres, nullptr, nullptr, nullptr, nullptr, flags, s, nullptr, nullptr,
+                           nullptr, 0, &cr);
 }
 
 int tpf_ccd_enforce_wall_neumann(const tpf_ccd_plan* p, int64_t outer, int64_t inner, void* grad,
