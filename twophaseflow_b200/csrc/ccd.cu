@@ -129,15 +129,17 @@ struct V2 { T a, b; };
 
 // Write one node's result: either (d1, d2) or the variable-density term.
 template <typename T>
-__device__ __forceinline__ void store_out(const CcdArgs& a, int64_t gi, double o1, double o2) {
+__device__ __forceinline__ void store_out(const CcdArgs& a, int64_t gi, double o1, double o2, int k) {
   if (a.cr_out) {
     // u_new = u* - (dt / rho) dp/dx, with the reference's operation order
-    // (quotient, product, difference; no fused multiply-add)
-    const double u = (double)static_cast<const T*>(a.cr_u)[gi];
+    // (quotient, product, difference; no fused multiply-add).  The loads are
+    // read-only-path loads so that they need not wait for earlier nodes'
+    // stores: every address is read once, by the lane that later writes it
+    // (u_out may be u_star), so no stale value can be read.
+    const double u = (double)__ldg(static_cast<const T*>(a.cr_u) + gi);
     double v = u;
-    const int64_t k = (gi / a.inner) % a.n;   // node along the line
-    if (!(a.cr_wall && (k == 0 || k == a.n - 1))) {
-      const double q = a.cr_dt / (double)static_cast<const T*>(a.cr_rho)[gi];
+    if (!(a.cr_wall && (k == 0 || k == a.n - 1))) {   // k: node along the line
+      const double q = a.cr_dt / (double)__ldg(static_cast<const T*>(a.cr_rho) + gi);
       v = __dsub_rn(u, __dmul_rn(q, o1));
     }
     static_cast<T*>(a.cr_out)[gi] = (T)v;
@@ -473,7 +475,7 @@ __global__ void __launch_bounds__(512, 1) ccd_line_kernel(CcdArgs a) {
             o2 = Jk * Jk * o2 + Jk * dJk * o1;
             o1 = Jk * o1;
           }
-          store_out<T>(a, base + (int64_t)k * a.inner, o1, o2);
+          store_out<T>(a, base + (int64_t)k * a.inner, o1, o2, k);
         }
       }
     }
@@ -509,18 +511,18 @@ __global__ void __launch_bounds__(512, 1) ccd_line_kernel(CcdArgs a) {
             double o1, o2;
             boundary_pair(l, true, o1, o2);
             metric(0, o1, o2);
-            store_out<T>(a, base, o1, o2);
+            store_out<T>(a, base, o1, o2, 0);
           }
           if (c == P - 1) {
             double o1, o2;
             boundary_pair(l, false, o1, o2);
             metric(n - 1, o1, o2);
-            store_out<T>(a, base + (int64_t)(n - 1) * a.inner, o1, o2);
+            store_out<T>(a, base + (int64_t)(n - 1) * a.inner, o1, o2, n - 1);
           }
         } else if (c == 0) {
           double o1 = (double)yl[0], o2 = (double)yl[1];
           metric(n - 1, o1, o2);
-          store_out<T>(a, base + (int64_t)(n - 1) * a.inner, o1, o2);
+          store_out<T>(a, base + (int64_t)(n - 1) * a.inner, o1, o2, n - 1);
         }
       }
     } else {
@@ -541,7 +543,7 @@ __global__ void __launch_bounds__(512, 1) ccd_line_kernel(CcdArgs a) {
           o2 = (double)yy[2 * kk + 1];
         }
         if (J) metric(k, o1, o2);
-        store_out<T>(a, line0 * n + e, o1, o2);
+        store_out<T>(a, line0 * n + e, o1, o2, k);
         ll += step_l;
         k += step_k;
         if (k >= n) { k -= n; ++ll; }
@@ -902,7 +904,7 @@ __global__ void __launch_bounds__(256) ccd_warp_kernel(CcdArgs a) {
           if (b >= 0) {
             double o1 = (double)f1[l * FSP + k + k / R], o2 = (double)sbuf[l * FSP + k + k / R];
             metric(k, o1, o2);
-            store_out<T>(a, b + k, o1, o2);
+            store_out<T>(a, b + k, o1, o2, k);
           }
           l += step_l;
           k += step_k;
@@ -915,7 +917,7 @@ __global__ void __launch_bounds__(256) ccd_warp_kernel(CcdArgs a) {
           if (b >= 0) {
             double o1 = (double)f1[l * FSP + k + k / R], o2 = (double)sbuf[l * FSP + k + k / R];
             metric(k, o1, o2);
-            store_out<T>(a, b + (int64_t)k * a.inner, o1, o2);
+            store_out<T>(a, b + (int64_t)k * a.inner, o1, o2, k);
           }
         }
       }
@@ -1070,7 +1072,7 @@ __global__ void __launch_bounds__(128) ccd_lane_kernel(CcdArgs a, const T* __res
         o2 = Jk * Jk * o2 + Jk * dJk * o1;
         o1 = Jk * o1;
       }
-      store_out<T>(a, base + (int64_t)k * inner, o1, o2);
+      store_out<T>(a, base + (int64_t)k * inner, o1, o2, k);
     };
     auto k0_of = [&](int c) { return PERIODIC ? c * CR - 1 : c * CR; };
     auto cnt_of = [&](int c) { return min(CR, n_rows - c * CR); };
@@ -1277,6 +1279,39 @@ __global__ void __launch_bounds__(128) ccd_lane_kernel(CcdArgs a, const T* __res
         const bool plain_c = a.d1 && a.d2 && !a.vd_out && !J;
         T* o1p = static_cast<T*>(a.d1) + g0;
         T* o2p = static_cast<T*>(a.d2) + g0;
+        if (a.cr_out) {
+          // corrector epilogue: all of this run's u* and rho first, then the
+          // stores (see the strided branch)
+          double pu[CR + 2], pr[CR + 2];
+          int l2 = ll, t2 = t;
+#pragma unroll
+          for (int i = 0; i < CR + 2; ++i) {
+            pu[i] = 0.0;
+            pr[i] = 1.0;
+            if (i < KN && l2 < nl) {
+              const int64_t gi = g0 + (int64_t)l2 * n + k0 + t2;
+              pu[i] = (double)static_cast<const T*>(a.cr_u)[gi];
+              pr[i] = (double)static_cast<const T*>(a.cr_rho)[gi];
+            }
+            l2 += dl;
+            t2 += dt_;
+            if (t2 >= KN) { t2 -= KN; ++l2; }
+          }
+#pragma unroll
+          for (int i = 0; i < CR + 2; ++i) {
+            if (i < KN && ll < nl) {
+              const int node = k0 + t;
+              double o1 = (double)ot[(t0 + t) * TS + ll];
+              if (J) o1 = J[node] * o1;
+              double v = pu[i];
+              if (!(a.cr_wall && (node == 0 || node == n - 1))) v = __dsub_rn(pu[i], __dmul_rn(a.cr_dt / pr[i], o1));
+              static_cast<T*>(a.cr_out)[g0 + (int64_t)ll * n + node] = (T)v;
+            }
+            ll += dl;
+            t += dt_;
+            if (t >= KN) { t -= KN; ++ll; }
+          }
+        } else
         for (int i = 0; i < KN; ++i) {
           if (ll < nl) {
             const int node = k0 + t;
@@ -1291,7 +1326,7 @@ __global__ void __launch_bounds__(128) ccd_lane_kernel(CcdArgs a, const T* __res
                 o2 = Jk * Jk * o2 + Jk * dJk * o1;
                 o1 = Jk * o1;
               }
-              store_out<T>(a, g0 + (int64_t)ll * n + node, o1, o2);
+              store_out<T>(a, g0 + (int64_t)ll * n + node, o1, o2, node);
             }
           }
           ll += dl;
@@ -1314,6 +1349,37 @@ __global__ void __launch_bounds__(128) ccd_lane_kernel(CcdArgs a, const T* __res
               __stcs(o2, yr[q].b);
               o1 += inner;
               o2 += inner;
+            }
+          }
+        }
+      } else if (a.cr_out) {
+        // corrector epilogue: the chunk's u* and rho are loaded before any
+        // store (the stores may alias u*, which would otherwise serialize each
+        // node's loads behind the previous node's store)
+        if (act) {
+          const int64_t o0 = base + (int64_t)(r0 + noff) * inner;
+          const T* cu = static_cast<const T*>(a.cr_u) + o0;
+          const T* crh = static_cast<const T*>(a.cr_rho) + o0;
+          T* co = static_cast<T*>(a.cr_out) + o0;
+          double pu[CR], pr[CR];
+#pragma unroll
+          for (int q = 0; q < CR; ++q) {
+            pu[q] = 0.0;
+            pr[q] = 1.0;
+            if (q < cnt) {
+              pu[q] = (double)cu[(int64_t)q * inner];
+              pr[q] = (double)crh[(int64_t)q * inner];
+            }
+          }
+#pragma unroll
+          for (int q = 0; q < CR; ++q) {
+            if (q < cnt) {
+              const int k = r0 + q + noff;
+              double o1 = (double)yr[q].a;
+              if (J) o1 = J[k] * o1;
+              double v = pu[q];
+              if (!(a.cr_wall && (k == 0 || k == n - 1))) v = __dsub_rn(pu[q], __dmul_rn(a.cr_dt / pr[q], o1));
+              co[(int64_t)q * inner] = (T)v;
             }
           }
         }

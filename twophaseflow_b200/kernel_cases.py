@@ -5,6 +5,7 @@
     python -m twophaseflow_b200.kernel_cases learned --N 512 512 [--maxiter 16] [--reps 2]
     python -m twophaseflow_b200.kernel_cases batched --N 32 [--reps 3]     (32 cases, grids 128..512)
     python -m twophaseflow_b200.kernel_cases gmres --N 512 512 [--line thomas|pcr] [--maxiter 2] [--reps 1]
+    python -m twophaseflow_b200.kernel_cases corrector --N 256 256 256 --axis 0 --bc wall [--reps 5]
 
 ``ccd`` captures ``reps`` CCDSolver.differentiate calls in one CUDA graph and
 replays it, so the reported time is device time per call (no Python launch
@@ -52,6 +53,71 @@ def ccd_case(N, axis, bc, dtype, reps, warmup=3):
     nbytes = 3 * f.numel() * f.element_size()
     return {"case": "ccd", "N": list(N), "axis": axis, "bc": bc, "dtype": dtype, "us_per_call": round(ms * 1e3, 2),
             "GBps": round(nbytes / (ms * 1e-3) / 1e9, 1), "alg_bytes": nbytes}
+
+
+def _graph_time(fn, reps, warmup=3):
+    """Device time per call of ``fn`` from a CUDA graph of ``reps`` calls."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            for _ in range(reps):
+                fn()
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    g.replay()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    g.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def corrector_case(N, axis, bc, dtype, reps):
+    """Velocity corrector along one axis: the fused CCD solve
+    (tpf_ccd_apply_corrector: read p, u*, rho, write u) against the same step
+    as separate operations (CCD differentiate, wall zeroing, elementwise
+    update), both graph-replayed."""
+    import ctypes as C
+    import torch
+    from . import CCDSolver, UniformGrid, _lib
+    from .arrays import line_split
+    from .workloads import fourier_field
+    dt_ = torch.float64 if dtype == "f64" else torch.float32
+    p = torch.from_numpy(fourier_field(N, seed=0)).to("cuda").to(dt_)
+    gen = torch.Generator(device="cuda").manual_seed(3)
+    rho = 1e-3 + torch.rand(p.shape, device="cuda", dtype=dt_, generator=gen)
+    u = torch.randn(p.shape, device="cuda", dtype=dt_, generator=gen)
+    out = torch.empty_like(u)
+    ccd = CCDSolver(UniformGrid(N), None, bc_type=bc, dtype=dt_)
+    lib = _lib.load()
+    outer, n, inner = line_split(p.shape, axis)
+    plan = ccd._plan(axis, ccd._axis_periodic(axis))
+    dt = 0.01
+
+    def fused():
+        _lib.check(lib.tpf_ccd_apply_corrector(plan, outer, inner, _lib.dptr(p), _lib.dptr(u), _lib.dptr(rho),
+                                               C.c_double(dt), _lib.dptr(out), 0, _lib.current_stream_handle()))
+
+    def separate():
+        d1, _ = ccd.differentiate(p, axis)
+        ccd.enforce_wall_neumann(d1, axis)
+        out.copy_(u - (dt / rho) * d1)
+
+    ms = _graph_time(fused, reps)
+    ms_sep = _graph_time(separate, reps)
+    nbytes = 4 * p.numel() * p.element_size()
+    return {"case": "corrector", "N": list(N), "axis": axis, "bc": bc, "dtype": dtype,
+            "us_per_call": round(ms * 1e3, 2), "GBps": round(nbytes / (ms * 1e-3) / 1e9, 1), "alg_bytes": nbytes,
+            "separate_ops_us": round(ms_sep * 1e3, 2)}
 
 
 def ppe_case(N, precision, reps, tol=1e-8):
@@ -221,7 +287,7 @@ def gmres_case(N, line, reps, maxiter=None, tol=1e-8):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["ccd", "ppe", "learned", "batched", "gmres"])
+    ap.add_argument("case", choices=["ccd", "ppe", "learned", "batched", "gmres", "corrector"])
     ap.add_argument("--line", default="thomas", choices=["thomas", "pcr"], help="gmres: line solver")
     ap.add_argument("--N", type=int, nargs="+", required=True)
     ap.add_argument("--axis", type=int, default=0)
@@ -240,6 +306,8 @@ def main(argv=None):
         r = learned_case(tuple(a.N), a.reps, a.maxiter or None)
     elif a.case == "gmres":
         r = gmres_case(tuple(a.N), a.line, a.reps, a.maxiter or None)
+    elif a.case == "corrector":
+        r = corrector_case(tuple(a.N), a.axis, a.bc, a.dtype, a.reps)
     else:
         r = batched_case(n_cases=a.N[0], reps=a.reps)
     print(json.dumps(r), flush=True)
