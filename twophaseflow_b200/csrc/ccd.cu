@@ -1311,6 +1311,44 @@ __global__ void __launch_bounds__(128) ccd_lane_kernel(CcdArgs a, const T* __res
             t += dt_;
             if (t >= KN) { t -= KN; ++ll; }
           }
+        } else if (a.vd_out) {
+          // variable-density epilogue: operands first, then the stores
+          double pr[CR + 2], pdr[CR + 2], po[CR + 2];
+          int l2 = ll, t2 = t;
+#pragma unroll
+          for (int i = 0; i < CR + 2; ++i) {
+            pr[i] = 1.0;
+            pdr[i] = 0.0;
+            po[i] = 0.0;
+            if (i < KN && l2 < nl) {
+              const int64_t gi = g0 + (int64_t)l2 * n + k0 + t2;
+              pr[i] = (double)static_cast<const T*>(a.vd_rho)[gi];
+              pdr[i] = (double)static_cast<const T*>(a.vd_drho)[gi];
+              if (a.vd_accumulate) po[i] = (double)static_cast<const T*>(a.vd_out)[gi];
+            }
+            l2 += dl;
+            t2 += dt_;
+            if (t2 >= KN) { t2 -= KN; ++l2; }
+          }
+#pragma unroll
+          for (int i = 0; i < CR + 2; ++i) {
+            if (i < KN && ll < nl) {
+              const int node = k0 + t;
+              double o1 = (double)ot[(t0 + t) * TS + ll], o2 = (double)dt[(t0 + t) * TS + ll];
+              if (J) {
+                const double Jk = J[node], dJk = J[n + node];
+                o2 = Jk * Jk * o2 + Jk * dJk * o1;
+                o1 = Jk * o1;
+              }
+              const double r = pr[i];
+              double tv = o2 / r - (pdr[i] / (r * r)) * o1;
+              if (a.vd_accumulate) tv = po[i] + tv;
+              static_cast<T*>(a.vd_out)[g0 + (int64_t)ll * n + node] = (T)tv;
+            }
+            ll += dl;
+            t += dt_;
+            if (t >= KN) { t -= KN; ++ll; }
+          }
         } else
         for (int i = 0; i < KN; ++i) {
           if (ll < nl) {
@@ -1380,6 +1418,42 @@ __global__ void __launch_bounds__(128) ccd_lane_kernel(CcdArgs a, const T* __res
               double v = pu[q];
               if (!(a.cr_wall && (k == 0 || k == n - 1))) v = __dsub_rn(pu[q], __dmul_rn(a.cr_dt / pr[q], o1));
               co[(int64_t)q * inner] = (T)v;
+            }
+          }
+        }
+      } else if (a.vd_out) {
+        // variable-density epilogue: operands first, then the stores (as above)
+        if (act) {
+          const int64_t o0 = base + (int64_t)(r0 + noff) * inner;
+          const T* vr = static_cast<const T*>(a.vd_rho) + o0;
+          const T* vdr = static_cast<const T*>(a.vd_drho) + o0;
+          T* vo = static_cast<T*>(a.vd_out) + o0;
+          double pr[CR], pdr[CR], po[CR];
+#pragma unroll
+          for (int q = 0; q < CR; ++q) {
+            pr[q] = 1.0;
+            pdr[q] = 0.0;
+            po[q] = 0.0;
+            if (q < cnt) {
+              pr[q] = (double)vr[(int64_t)q * inner];
+              pdr[q] = (double)vdr[(int64_t)q * inner];
+              if (a.vd_accumulate) po[q] = (double)vo[(int64_t)q * inner];
+            }
+          }
+#pragma unroll
+          for (int q = 0; q < CR; ++q) {
+            if (q < cnt) {
+              const int k = r0 + q + noff;
+              double o1 = (double)yr[q].a, o2 = (double)yr[q].b;
+              if (J) {
+                const double Jk = J[k], dJk = J[n + k];
+                o2 = Jk * Jk * o2 + Jk * dJk * o1;
+                o1 = Jk * o1;
+              }
+              const double r = pr[q];
+              double tv = o2 / r - (pdr[q] / (r * r)) * o1;
+              if (a.vd_accumulate) tv = po[q] + tv;
+              vo[(int64_t)q * inner] = (T)tv;
             }
           }
         }
