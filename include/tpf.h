@@ -127,6 +127,32 @@ int tpf_ccd_apply_corrector(const tpf_ccd_plan* plan, int64_t outer, int64_t inn
 int tpf_cfl_maxima(int64_t n, int ncomp, const void* const* comps, const void* mu, const void* rho,
                    int dtype, double* out, void* stream);
 
+/* DCCD dissipative filter (src/twophase/levelset/curvature.py:60-127): for
+ * each axis in turn f <- f + c (f[+1] - 2 f + f[-1]) on nodes 1..N-1 (wall)
+ * or on the N unique nodes with wrap-around, image node N <- node 0
+ * (periodic[axis] != 0); c = eps, or eps * sw[node] when sw is given; then
+ * the wall planes take the unfiltered input.  shape: nodes per axis (ndim 2
+ * or 3, C order); f, out and tmp (workspace of f's size) must be distinct. */
+int tpf_dccd_filter(int ndim, const int64_t* shape, const int* periodic, double eps, const void* sw,
+                    const void* f, void* out, void* tmp, int dtype, void* stream);
+
+/* Curvature from psi (CurvatureCalculatorPsi.compute, curvature_psi.py:72-173)
+ * given its CCD derivatives: d1[a], d2[a] per axis and the mixed derivatives
+ * (2-D: mixed[0] = psi_xy; 3-D: xy, xz, yz); kappa = 0 where
+ * psi <= psi_min or psi >= 1 - psi_min.  n values each. */
+int tpf_curvature_psi(int ndim, int64_t n, const void* psi, const void* const* d1, const void* const* d2,
+                      const void* const* mixed, double psi_min, void* kappa, int dtype, void* stream);
+
+/* 3x3 Gaussian [1 2 1; 2 4 2; 1 2 1] / 16 with edge replication, 2-D n0 x n1
+ * (curvature_psi.py:176-197); in and out distinct. */
+int tpf_gaussian3x3(int64_t n0, int64_t n1, const void* in, void* out, int dtype, void* stream);
+
+/* rho = rho_g + (rho_l - rho_g) psi and mu = mu_g + (mu_l - mu_g) psi
+ * (update_properties, src/twophase/levelset/heaviside.py:167-187); either
+ * output may be NULL. */
+int tpf_update_properties(int64_t n, const void* psi, double rho_l, double rho_g, double mu_l, double mu_g,
+                          void* rho, void* mu, int dtype, void* stream);
+
 /* Zero grad at index 0 and n_pts-1 along the axis of a [outer, n, inner]
  * array (wall axes only; no-op for periodic plans).  Replaces
  * CCDSolver.enforce_wall_neumann (ccd_solver.py:264-281;

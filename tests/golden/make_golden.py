@@ -297,17 +297,76 @@ def make_step(out):
             out[f"{name}/dt_{tag}"] = np.array(CFLCalculator(be, grid, 0.3, **kw).compute(vel, mu, rho))
 
 
+def make_levelset(out):
+    """Curvature from psi, the DCCD filter and the material properties of the
+    reference on seeded fields."""
+    from types import SimpleNamespace
+    from twophase.backend import Backend
+    from twophase.config import GridConfig
+    from twophase.core.grid import Grid
+    from twophase.ccd.ccd_solver import CCDSolver
+    from twophase.levelset.heaviside import heaviside, update_properties
+    from twophase.levelset.curvature import _dccd_filter_nd
+    from twophase.levelset.curvature_psi import CurvatureCalculatorPsi
+
+    be = Backend(use_gpu=False)
+    xp = be.xp
+    rng = np.random.default_rng(777)
+    # interface shapes on wall / periodic grids (circle, shifted ellipse, sphere)
+    cases = [("circle2d", (32, 32), (1.0, 1.0), "wall"),
+             ("ellipse2d", (24, 20), (1.2, 1.0), "periodic"),
+             ("sphere3d", (12, 10, 14), (1.0, 0.9, 1.1), "wall")]
+    for name, N, L, bc in cases:
+        grid = Grid(GridConfig(ndim=len(N), N=N, L=L), be)
+        ccd = CCDSolver(grid, be, bc_type=bc)
+        axes = [np.linspace(0.0, L[a], N[a] + 1) for a in range(len(N))]
+        X = np.meshgrid(*axes, indexing="ij")
+        c = [0.5 * L[a] + 0.03 * (a + 1) for a in range(len(N))]
+        r = [0.27 + 0.05 * a for a in range(len(N))]
+        phi = np.sqrt(sum(((X[a] - c[a]) / r[a]) ** 2 for a in range(len(N)))) - 1.0
+        phi = phi * min(r)
+        eps = 1.5 * max(L[a] / N[a] for a in range(len(N)))
+        psi = np.asarray(heaviside(xp, phi, eps))
+        out[f"{name}/N"] = np.array(N)
+        out[f"{name}/L"] = np.array(L, dtype=np.float64)
+        out[f"{name}/bc"] = np.array(bc)
+        out[f"{name}/psi"] = psi
+        for tag, kw in (("default", {}), ("nofilter", dict(dccd_eps=0.0)),
+                        ("gauss", dict(gaussian_filter=True, psi_min=0.02))):
+            if tag == "gauss" and len(N) != 2:
+                continue
+            out[f"{name}/kappa_{tag}"] = np.asarray(CurvatureCalculatorPsi(be, ccd, **kw).compute(psi.copy()))
+    fcases = [("f_wall2d", (17, 13), "wall"), ("f_pw2d", (16, 11), "periodic_wall"),
+              ("f_per3d", (9, 8, 7), "periodic"), ("f_wall3d", (7, 9, 8), "wall")]
+    for name, shape, bc in fcases:
+        f = rng.standard_normal(shape)
+        sw = rng.uniform(0.0, 1.0, shape)
+        g = SimpleNamespace(ndim=len(shape), N=tuple(n - 1 for n in shape))
+        out[f"{name}/f"] = f
+        out[f"{name}/sw"] = sw
+        out[f"{name}/bc"] = np.array(bc)
+        out[f"{name}/plain"] = np.asarray(_dccd_filter_nd(xp, f.copy(), g, 0.05, bc_type=bc))
+        out[f"{name}/switched"] = np.asarray(_dccd_filter_nd(xp, f.copy(), g, 0.05, bc_type=bc, switch=sw))
+    psi = np.concatenate([[0.0, 0.5, 1.0], rng.uniform(0.0, 1.0, 61)])
+    rho, mu = update_properties(xp, psi, 1.0, 0.001, 1.0, 0.0185)
+    out["props/psi"] = psi
+    out["props/rho"] = np.asarray(rho)
+    out["props/mu"] = np.asarray(mu)
+
+
 def main():
+    """Usage: make_golden.py [reference src dir] [only: ccd|ppe|step|levelset ...]."""
     src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
+    only = set(sys.argv[2:])
     _ref_import(src)
-    ccd_out, ppe_out, step_out = {}, {}, {}
-    make_ccd(ccd_out)
-    make_ppe(ppe_out)
-    make_step(step_out)
-    np.savez_compressed(os.path.join(HERE, "ccd_golden.npz"), **ccd_out)
-    np.savez_compressed(os.path.join(HERE, "ppe_golden.npz"), **ppe_out)
-    np.savez_compressed(os.path.join(HERE, "step_golden.npz"), **step_out)
-    print("wrote", len(ccd_out), "ccd,", len(ppe_out), "ppe and", len(step_out), "step arrays")
+    makers = {"ccd": make_ccd, "ppe": make_ppe, "step": make_step, "levelset": make_levelset}
+    for key, fn in makers.items():
+        if only and key not in only:
+            continue
+        arrays = {}
+        fn(arrays)
+        np.savez_compressed(os.path.join(HERE, f"{key}_golden.npz"), **arrays)
+        print("wrote", len(arrays), key, "arrays")
 
 
 if __name__ == "__main__":

@@ -20,6 +20,7 @@ from .ccd_ppe import CCDVariableDensityOperator, PPESolverDefectCorrection
 from .grid import BoundarySpec, UniformGrid
 from .ppe import (MatrixAssemblyUnavailable, PPESolverFVMMatrixFree, create_fvm_matrixfree, register_with_reference,
                   solve_batched)
+from .levelset import CurvatureCalculatorPsi, dccd_filter_nd, update_properties
 from .step import CFLCalculator, VelocityCorrector, ccd_pressure_gradient
 
 __all__ = [
@@ -36,4 +37,7 @@ __all__ = [
     "VelocityCorrector",
     "CFLCalculator",
     "ccd_pressure_gradient",
+    "CurvatureCalculatorPsi",
+    "dccd_filter_nd",
+    "update_properties",
 ]

@@ -92,6 +92,13 @@ SIGNATURES = {
                                           C.c_double, C.c_void_p, C.c_int, C.c_void_p]),
     "tpf_cfl_maxima": (C.c_int, [C.c_int64, C.c_int, C.POINTER(C.c_void_p), C.c_void_p, C.c_void_p, C.c_int,
                                  C.c_void_p, C.c_void_p]),
+    "tpf_dccd_filter": (C.c_int, [C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int), C.c_double, C.c_void_p,
+                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "tpf_curvature_psi": (C.c_int, [C.c_int, C.c_int64, C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                    C.POINTER(C.c_void_p), C.c_double, C.c_void_p, C.c_int, C.c_void_p]),
+    "tpf_gaussian3x3": (C.c_int, [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "tpf_update_properties": (C.c_int, [C.c_int64, C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double,
+                                        C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "tpf_ccd_enforce_wall_neumann": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]),
     "tpf_ppe_default_options": (None, [C.POINTER(tpf_ppe_options)]),
     "tpf_ppe_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_int64),
