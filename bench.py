@@ -395,6 +395,12 @@ def main(argv=None):
         r = corrector_case((256, 256, 256), axis, "wall", "f64", 5)
         corr.append({"axis": axis, "us": r["us_per_call"], "GBps": r["GBps"], "separate_ops_us": r["separate_ops_us"]})
 
+    # interface curvature from psi and the Rhie-Chow PPE right-hand side
+    # (3-D 257^3 FP64 wall; whole calls and their own kernels, graph-replayed)
+    from twophaseflow_b200.kernel_cases import curvature_case, rhiechow_case
+    curv = curvature_case((256, 256, 256), "wall", "f64", 3)
+    rcb = rhiechow_case((256, 256, 256), "wall", "f64", 3)
+
     # many independent cases in one persistent launch (32 seeded grids, 128..512 per axis)
     from twophaseflow_b200.kernel_cases import batched_case
     bat = batched_case(n_cases=32, reps=2)
@@ -438,6 +444,8 @@ def main(argv=None):
             "ccd": ccd,
             "corrector_257cubed_f64_wall": {"per_axis": corr, "peak": peak, "peak_kind": peak_kind,
                                             "frac_mean": round(float(np.mean([c["GBps"] for c in corr])) / peak, 3)},
+            "curvature_257cubed_f64_wall": {k: v for k, v in curv.items() if k not in ("case", "N", "bc", "dtype")},
+            "rhiechow_257cubed_f64_wall": {k: v for k, v in rcb.items() if k not in ("case", "N", "bc", "dtype")},
             "ccd_roofline": {"kernel": "ccd_lane_kernel (3-D 257^3 FP64, mean over axes and wall/periodic)",
                              "bound": "hbm", "achieved": round(ccd3_gbps, 1), "peak": peak, "unit": "GB/s",
                              "frac": round(ccd3_gbps / peak, 3),

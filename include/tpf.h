@@ -132,7 +132,9 @@ int tpf_cfl_maxima(int64_t n, int ncomp, const void* const* comps, const void* m
  * or on the N unique nodes with wrap-around, image node N <- node 0
  * (periodic[axis] != 0); c = eps, or eps * sw[node] when sw is given; then
  * the wall planes take the unfiltered input.  shape: nodes per axis (ndim 2
- * or 3, C order); f, out and tmp (workspace of f's size) must be distinct. */
+ * or 3, C order); f and out distinct.  tmp: workspace of f's size, distinct
+ * from f, out and sw, needed in 3-D (2-D runs both passes in one kernel and
+ * ignores it; NULL allowed there). */
 int tpf_dccd_filter(int ndim, const int64_t* shape, const int* periodic, double eps, const void* sw,
                     const void* f, void* out, void* tmp, int dtype, void* stream);
 
@@ -152,6 +154,20 @@ int tpf_gaussian3x3(int64_t n0, int64_t n1, const void* in, void* out, int dtype
  * output may be NULL. */
 int tpf_update_properties(int64_t n, const void* psi, double rho_l, double rho_g, double mu_l, double mu_g,
                           void* rho, void* mu, int dtype, void* stream);
+
+/* One axis of the Rhie-Chow face-velocity divergence
+ * (RhieChowInterpolator.face_velocity_divergence / _rc_flux_1d /
+ * _flux_divergence_1d, src/twophase/spatial/rhie_chow.py:55-284).  shape:
+ * nodes per axis (C order); h = L/N of the axis; dp = the CCD first
+ * derivative of p along the axis (its boundary values are replaced by
+ * one-sided differences on a wall axis, periodic = 0).  kappa, psi and dpsi
+ * (= CCD D1 psi along the axis) all NULL, or all given with we != 0 for the
+ * balanced-force form.  div = this axis' divergence (accumulate = 0, the first
+ * axis) or div + it (accumulate = 1). */
+int tpf_rc_divergence_axis(int ndim, const int64_t* shape, int axis, int periodic, double h, double dt,
+                           const void* u_star, const void* p, const void* rho, const void* dp,
+                           const void* kappa, const void* psi, const void* dpsi, double we,
+                           int accumulate, void* div, int dtype, void* stream);
 
 /* Zero grad at index 0 and n_pts-1 along the axis of a [outer, n, inner]
  * array (wall axes only; no-op for periodic plans).  Replaces

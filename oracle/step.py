@@ -6,8 +6,11 @@
   (``oracle.ccd.differentiate``).
 * ``cfl_dt`` -- the CFL-limited time step (reference
   ``src/twophase/time_integration/cfl.py:41-137``).
+* ``rc_divergence`` -- the Rhie-Chow face-velocity divergence (reference
+  ``src/twophase/spatial/rhie_chow.py:55-284``).
 
-Pinned against the reference's own outputs in ``tests/golden/step_golden.npz``.
+Pinned against the reference's own outputs in ``tests/golden/step_golden.npz`` and
+``tests/golden/rhiechow_golden.npz``.
 Only tests, smoke() and bench.py's CPU-baseline leg may use this module.
 """
 
@@ -58,3 +61,55 @@ def cfl_dt(vel, mu, rho, L, N, cfl: float, We=None, rho_ratio: float = 0.0, cn_v
     if dt_sigma is not None:
         cands.append(np.asarray(cfl * dt_sigma, dtype=np.float64))
     return float(np.maximum(np.min(np.stack(cands)), 1.0e-8))
+
+
+def _rc_axis(u, p, rho, dp, ax: int, h: float, dt: float, periodic: bool, kappa=None, psi=None, dpsi=None, we=None):
+    """Face velocities of one axis and their divergence (rhie_chow.py:117-284),
+    restated on lines moved to axis 0."""
+    mv = lambda a: np.moveaxis(np.asarray(a), ax, 0) if a is not None else None
+    u, p, rho, dp = mv(u), mv(p), mv(rho), np.array(mv(dp), copy=True)
+    kappa, psi, dpsi = mv(kappa), mv(psi), mv(dpsi)
+    bf = kappa is not None
+    N = p.shape[0] - 1
+    fs = None
+    if bf:
+        fs = (kappa * dpsi) / we
+    if not periodic:
+        dp[0] = (p[1] - p[0]) / h
+        dp[N] = (p[N] - p[N - 1]) / h
+        if bf:
+            fs = np.array(fs, copy=True)
+            fs[0] = (kappa[0] * (psi[1] - psi[0])) / (h * we)
+            fs[N] = (kappa[N] * (psi[N] - psi[N - 1])) / (h * we)
+
+    def face(l, r):
+        ubar = 0.5 * (u[l] + u[r])
+        br = (p[r] - p[l]) / h - 0.5 * (dp[l] + dp[r])
+        if bf:
+            kf = 0.5 * (kappa[l] + kappa[r])
+            br = br - ((kf * (psi[r] - psi[l])) / (h * we) - 0.5 * (fs[l] + fs[r]))
+        return ubar - (dt * (2.0 / (rho[l] + rho[r]))) * br
+
+    flux = np.zeros_like(p)
+    flux[1:] = face(slice(0, N), slice(1, N + 1))
+    if periodic:
+        flux[0] = face(N, 0)
+    div = np.empty_like(p)
+    div[:N] = (flux[1:] - flux[:N]) / h
+    div[N] = (flux[0] - flux[N]) / h if periodic else (-flux[N]) / h
+    return np.moveaxis(div, 0, ax)
+
+
+def rc_divergence(vel_star, p, rho, dt: float, L, N, ccd_bc: str, rc_bc: str, kappa=None, psi=None, we=None):
+    """RhieChowInterpolator.face_velocity_divergence (rhie_chow.py:55-115) on the
+    oracle CCD; rc_bc: 'wall' or 'periodic' for every axis."""
+    p = np.asarray(p, dtype=np.float64)
+    bf = kappa is not None and psi is not None and we is not None
+    div = np.zeros_like(p)
+    for ax in range(p.ndim):
+        h = float(L[ax] / N[ax])
+        dp, _ = occd.differentiate(p, ax, h, bc=ccd_bc)
+        dpsi = occd.differentiate(np.asarray(psi), ax, h, bc=ccd_bc)[0] if bf else None
+        div += _rc_axis(vel_star[ax], p, rho, dp, ax, h, dt, rc_bc == "periodic",
+                        kappa if bf else None, psi if bf else None, dpsi, we if bf else None)
+    return div

@@ -354,12 +354,52 @@ def make_levelset(out):
     out["props/mu"] = np.asarray(mu)
 
 
+def make_rhiechow(out):
+    """Rhie-Chow face-velocity divergence of the reference on seeded fields,
+    plain and balanced-force."""
+    from twophase.backend import Backend
+    from twophase.config import GridConfig
+    from twophase.core.grid import Grid
+    from twophase.ccd.ccd_solver import CCDSolver
+    from twophase.spatial.rhie_chow import RhieChowInterpolator
+
+    be = Backend(use_gpu=False)
+    rng = np.random.default_rng(9090)
+    cases = [("wall2d", (16, 12), "wall"), ("per2d", (16, 10), "periodic"), ("wall3d", (8, 10, 6), "wall"),
+             ("per3d", (6, 8, 7), "periodic")]
+    for name, N, bc in cases:
+        L = tuple(1.0 + 0.25 * a for a in range(len(N)))
+        grid = Grid(GridConfig(ndim=len(N), N=N, L=L), be)
+        ccd = CCDSolver(grid, be, bc_type=bc)
+        rc = RhieChowInterpolator(be, grid, ccd, bc_type=bc)
+        p = rng.standard_normal(grid.shape)
+        rho = 1e-3 + rng.uniform(0.0, 1.0, grid.shape)
+        vel = [rng.standard_normal(grid.shape) for _ in range(len(N))]
+        kappa = rng.standard_normal(grid.shape)
+        psi = rng.uniform(0.0, 1.0, grid.shape)
+        dt, we = 0.0137, 0.7
+        out[f"{name}/N"] = np.array(N)
+        out[f"{name}/L"] = np.array(L, dtype=np.float64)
+        out[f"{name}/bc"] = np.array(bc)
+        out[f"{name}/p"] = p
+        out[f"{name}/rho"] = rho
+        out[f"{name}/kappa"] = kappa
+        out[f"{name}/psi"] = psi
+        out[f"{name}/dt"] = np.array(dt)
+        out[f"{name}/we"] = np.array(we)
+        for ax in range(len(N)):
+            out[f"{name}/u{ax}"] = vel[ax]
+        out[f"{name}/div"] = np.asarray(rc.face_velocity_divergence(vel, p, rho, dt))
+        out[f"{name}/div_bf"] = np.asarray(rc.face_velocity_divergence(vel, p, rho, dt, kappa=kappa, psi=psi, we=we))
+
+
 def main():
-    """Usage: make_golden.py [reference src dir] [only: ccd|ppe|step|levelset ...]."""
+    """Usage: make_golden.py [reference src dir] [only: ccd|ppe|step|levelset|rhiechow ...]."""
     src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
     only = set(sys.argv[2:])
     _ref_import(src)
-    makers = {"ccd": make_ccd, "ppe": make_ppe, "step": make_step, "levelset": make_levelset}
+    makers = {"ccd": make_ccd, "ppe": make_ppe, "step": make_step, "levelset": make_levelset,
+              "rhiechow": make_rhiechow}
     for key, fn in makers.items():
         if only and key not in only:
             continue

@@ -150,3 +150,73 @@ def test_cfl_maxima_large_and_nan(cuda_device):
     u[12345] = np.nan
     sp, _ = calc.maxima([dev(u), dev(v)])
     assert np.isnan(sp[0]) and sp[1] == float(np.max(np.abs(v)))
+
+
+RCG = os.path.join(os.path.dirname(__file__), "golden", "rhiechow_golden.npz")
+RC_CASES = ["wall2d", "per2d", "wall3d", "per3d"]
+
+
+@pytest.fixture(scope="module")
+def rc_golden():
+    with np.load(RCG) as d:
+        return {k: d[k] for k in d.files}
+
+
+@pytest.mark.parametrize("name", RC_CASES)
+def test_rc_divergence_matches_reference(cuda_device, rc_golden, name):
+    """NumPy in and out; within the CCD's rounding of the reference."""
+    from twophaseflow_b200 import RhieChowInterpolator
+    g = rc_golden
+    N, grid, ccd = _grid(g, name)
+    rc = RhieChowInterpolator(None, grid, ccd, bc_type=str(g[f"{name}/bc"]))
+    vel = [g[f"{name}/u{a}"] for a in range(len(N))]
+    p, rho, dt = g[f"{name}/p"], g[f"{name}/rho"], float(g[f"{name}/dt"])
+    d = rc.face_velocity_divergence(vel, p, rho, dt)
+    ref = g[f"{name}/div"]
+    assert isinstance(d, np.ndarray)
+    assert np.abs(d - ref).max() <= TOL * np.abs(ref).max()
+    d = rc.face_velocity_divergence(vel, p, rho, dt, kappa=g[f"{name}/kappa"], psi=g[f"{name}/psi"],
+                                    we=float(g[f"{name}/we"]))
+    ref = g[f"{name}/div_bf"]
+    assert np.abs(d - ref).max() <= TOL * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("shape,periodic", [((1025, 1025), False), ((1025, 1025), True), ((129, 130, 131), False),
+                                            ((129, 130, 131), True)])
+def test_rc_axis_kernel_bit_exact(cuda_device, shape, periodic):
+    """The divergence kernel alone, every axis, plain and balanced-force, with
+    the same derivative arrays given to the oracle: bit-identical."""
+    import torch
+    from twophaseflow_b200 import _lib
+    rng = np.random.default_rng(17)
+    f = {k: rng.standard_normal(shape) for k in ("u", "p", "dp", "kappa", "psi", "dpsi")}
+    f["rho"] = 1e-3 + rng.uniform(0.0, 1.0, shape)
+    T = {k: torch.from_numpy(v).cuda() for k, v in f.items()}
+    sh = (C.c_int64 * len(shape))(*shape)
+    lib = _lib.load()
+    for bf in (False, True):
+        div = torch.empty(shape, dtype=torch.float64, device="cuda")
+        ref = np.zeros(shape)
+        for ax in range(len(shape)):
+            h = 1.0 / (shape[ax] - 1) * (1.0 + 0.1 * ax)
+            extra = [_lib.dptr(T["kappa"]), _lib.dptr(T["psi"]), _lib.dptr(T["dpsi"]), 0.7] if bf else \
+                [None, None, None, 0.0]
+            _lib.check(lib.tpf_rc_divergence_axis(len(shape), sh, ax, int(periodic), h, 0.013, _lib.dptr(T["u"]),
+                                                  _lib.dptr(T["p"]), _lib.dptr(T["rho"]), _lib.dptr(T["dp"]),
+                                                  *extra, 1 if ax else 0, _lib.dptr(div), _lib.TPF_F64,
+                                                  _lib.current_stream_handle()))
+            ref += ostep._rc_axis(f["u"], f["p"], f["rho"], f["dp"], ax, h, 0.013, periodic,
+                                  f["kappa"] if bf else None, f["psi"] if bf else None,
+                                  f["dpsi"] if bf else None, 0.7 if bf else None)
+        np.testing.assert_array_equal(div.cpu().numpy(), ref)
+
+
+def test_rc_refuses_partial_balanced_force(cuda_device):
+    import torch
+    from twophaseflow_b200 import _lib
+    x = torch.zeros((8, 8), dtype=torch.float64, device="cuda")
+    sh = (C.c_int64 * 2)(8, 8)
+    st = _lib.load().tpf_rc_divergence_axis(2, sh, 0, 0, 0.1, 0.01, _lib.dptr(x), _lib.dptr(x), _lib.dptr(x),
+                                            _lib.dptr(x), _lib.dptr(x), None, None, 0.7, 0, _lib.dptr(x),
+                                            _lib.TPF_F64, None)
+    assert st != 0 and "balanced-force" in _lib.last_error()

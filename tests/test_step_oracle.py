@@ -51,3 +51,26 @@ def test_cfl_oracle_matches_reference(golden, name):
     for tag, kw in (("cn", dict(cn_viscous=True)), ("expl", dict(cn_viscous=False)),
                     ("cap", dict(We=0.01, rho_ratio=0.1, cn_viscous=True))):
         assert ostep.cfl_dt(vel, mu, rho, L, N, 0.3, **kw) == float(golden[f"{name}/dt_{tag}"])
+
+
+RC = np.load(os.path.join(os.path.dirname(__file__), "golden", "rhiechow_golden.npz"))
+
+
+@pytest.mark.parametrize("name", ["wall2d", "per2d", "wall3d", "per3d"])
+def test_rc_divergence_matches_reference(name):
+    """The oracle's Rhie-Chow divergence, plain and balanced-force, equals the
+    reference's bit for bit (same CCD, same operation order)."""
+    N, L, bc = RC[f"{name}/N"], RC[f"{name}/L"], str(RC[f"{name}/bc"])
+    vel = [RC[f"{name}/u{a}"] for a in range(len(N))]
+    args = (vel, RC[f"{name}/p"], RC[f"{name}/rho"], float(RC[f"{name}/dt"]), L, N, bc, bc)
+    np.testing.assert_array_equal(ostep.rc_divergence(*args), RC[f"{name}/div"])
+    bf = dict(kappa=RC[f"{name}/kappa"], psi=RC[f"{name}/psi"], we=float(RC[f"{name}/we"]))
+    np.testing.assert_array_equal(ostep.rc_divergence(*args, **bf), RC[f"{name}/div_bf"])
+
+
+def test_rc_divergence_of_uniform_flow_vanishes():
+    """u* = const, p = 0 on a periodic box: zero divergence."""
+    N = (12, 10)
+    vel = [np.full((13, 11), 0.3), np.full((13, 11), -1.1)]
+    d = ostep.rc_divergence(vel, np.zeros((13, 11)), np.ones((13, 11)), 0.01, (1.0, 1.0), N, "periodic", "periodic")
+    assert np.abs(d).max() < 1e-12

@@ -21,7 +21,7 @@ from .grid import BoundarySpec, UniformGrid
 from .ppe import (MatrixAssemblyUnavailable, PPESolverFVMMatrixFree, create_fvm_matrixfree, register_with_reference,
                   solve_batched)
 from .levelset import CurvatureCalculatorPsi, dccd_filter_nd, update_properties
-from .step import CFLCalculator, VelocityCorrector, ccd_pressure_gradient
+from .step import CFLCalculator, RhieChowInterpolator, VelocityCorrector, ccd_pressure_gradient
 
 __all__ = [
     "CCDSolver",
@@ -36,6 +36,7 @@ __all__ = [
     "BoundarySpec",
     "VelocityCorrector",
     "CFLCalculator",
+    "RhieChowInterpolator",
     "ccd_pressure_gradient",
     "CurvatureCalculatorPsi",
     "dccd_filter_nd",

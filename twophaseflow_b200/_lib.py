@@ -99,6 +99,9 @@ SIGNATURES = {
     "tpf_gaussian3x3": (C.c_int, [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "tpf_update_properties": (C.c_int, [C.c_int64, C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double,
                                         C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "tpf_rc_divergence_axis": (C.c_int, [C.c_int, C.POINTER(C.c_int64), C.c_int, C.c_int, C.c_double, C.c_double,
+                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "tpf_ccd_enforce_wall_neumann": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]),
     "tpf_ppe_default_options": (None, [C.POINTER(tpf_ppe_options)]),
     "tpf_ppe_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_int64),

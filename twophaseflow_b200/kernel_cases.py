@@ -6,6 +6,8 @@
     python -m twophaseflow_b200.kernel_cases batched --N 32 [--reps 3]     (32 cases, grids 128..512)
     python -m twophaseflow_b200.kernel_cases gmres --N 512 512 [--line thomas|pcr] [--maxiter 2] [--reps 1]
     python -m twophaseflow_b200.kernel_cases corrector --N 256 256 256 --axis 0 --bc wall [--reps 5]
+    python -m twophaseflow_b200.kernel_cases curvature --N 256 256 256 --bc wall [--reps 3]
+    python -m twophaseflow_b200.kernel_cases rhiechow --N 256 256 256 --bc wall [--reps 3]
 
 ``ccd`` captures ``reps`` CCDSolver.differentiate calls in one CUDA graph and
 replays it, so the reported time is device time per call (no Python launch
@@ -118,6 +120,91 @@ def corrector_case(N, axis, bc, dtype, reps):
     return {"case": "corrector", "N": list(N), "axis": axis, "bc": bc, "dtype": dtype,
             "us_per_call": round(ms * 1e3, 2), "GBps": round(nbytes / (ms * 1e-3) / 1e9, 1), "alg_bytes": nbytes,
             "separate_ops_us": round(ms_sep * 1e3, 2)}
+
+
+def curvature_case(N, bc, dtype, reps):
+    """Curvature from psi (CurvatureCalculatorPsi.compute: CCD derivatives,
+    DCCD filter, mixed derivatives, curvature formula) on a sphere, and its
+    filter and formula kernels alone, all graph-replayed."""
+    import ctypes as C
+    import numpy as np
+    import torch
+    from . import CCDSolver, CurvatureCalculatorPsi, UniformGrid, _lib
+    from .levelset import _filter_tensor
+    dt_ = torch.float64 if dtype == "f64" else torch.float32
+    nd = len(N)
+    ax = [torch.linspace(0.0, 1.0, n + 1, dtype=torch.float64, device="cuda") for n in N]
+    X = torch.meshgrid(*ax, indexing="ij")
+    phi = torch.sqrt(sum((X[a] - 0.5 + 0.02 * a) ** 2 for a in range(nd))) - 0.3
+    eps = 1.5 / max(N)
+    psi = torch.sigmoid(phi / eps).to(dt_).contiguous()
+    del X, phi
+    ccd = CCDSolver(UniformGrid(N), None, bc_type=bc, dtype=dt_)
+    calc = CurvatureCalculatorPsi(None, ccd)
+    ms_all = _graph_time(lambda: calc.compute(psi), reps)
+    sw = ((2.0 * psi - 1.0) ** 2).contiguous()
+    g = torch.randn(psi.shape, device="cuda", dtype=dt_)
+    ms_f = _graph_time(lambda: _filter_tensor(g, ccd.grid, 0.05, bc, sw), reps)
+    d = [torch.randn(psi.shape, device="cuda", dtype=dt_) for _ in range(2 * nd + (1 if nd == 2 else 3))]
+    kap = torch.empty_like(psi)
+    P = C.c_void_p * 3
+    nm = 1 if nd == 2 else 3
+    pd1 = P(*([_lib.dptr(t) for t in d[:nd]] + [None] * (3 - nd)))
+    pd2 = P(*([_lib.dptr(t) for t in d[nd:2 * nd]] + [None] * (3 - nd)))
+    pmx = P(*([_lib.dptr(t) for t in d[2 * nd:]] + [None] * (3 - nm)))
+    tdt = _lib.TPF_F64 if dt_ == torch.float64 else _lib.TPF_F32
+    lib = _lib.load()
+
+    def formula():
+        _lib.check(lib.tpf_curvature_psi(nd, psi.numel(), _lib.dptr(psi), pd1, pd2, pmx, 0.01, _lib.dptr(kap), tdt,
+                                         _lib.current_stream_handle()))
+
+    ms_k = _graph_time(formula, reps)
+    es = psi.element_size()
+    # read f, sw; write out: once in 2-D (both passes in one kernel), per axis pass in 3-D
+    filt_bytes = (3 if nd == 2 else 3 * nd) * psi.numel() * es
+    form_bytes = (2 + 2 * nd + nm) * psi.numel() * es
+    return {"case": "curvature", "N": list(N), "bc": bc, "dtype": dtype, "us_per_compute": round(ms_all * 1e3, 1),
+            "filter_us": round(ms_f * 1e3, 1), "filter_GBps": round(filt_bytes / (ms_f * 1e-3) / 1e9, 1),
+            "formula_us": round(ms_k * 1e3, 1), "formula_GBps": round(form_bytes / (ms_k * 1e-3) / 1e9, 1),
+            "filters_per_compute": 2 * nd + (1 if nd == 2 else 0)}
+
+
+def rhiechow_case(N, bc, dtype, reps):
+    """Rhie-Chow face-velocity divergence (RhieChowInterpolator, plain and
+    balanced-force: per axis a CCD first derivative + the divergence kernel)
+    and the divergence kernel alone (axis 0), graph-replayed."""
+    import ctypes as C
+    import torch
+    from . import CCDSolver, RhieChowInterpolator, UniformGrid, _lib
+    dt_ = torch.float64 if dtype == "f64" else torch.float32
+    gen = torch.Generator(device="cuda").manual_seed(7)
+    shape = tuple(n + 1 for n in N)
+    mk = lambda: torch.randn(shape, device="cuda", dtype=dt_, generator=gen)
+    vel = [mk() for _ in N]
+    p, kappa, psi, dp = mk(), mk(), mk(), mk()
+    rho = 1e-3 + torch.rand(shape, device="cuda", dtype=dt_, generator=gen)
+    grid = UniformGrid(N)
+    rc = RhieChowInterpolator(None, grid, CCDSolver(grid, None, bc_type=bc, dtype=dt_), bc_type=bc)
+    ms = _graph_time(lambda: rc.face_velocity_divergence(vel, p, rho, 0.01), reps)
+    ms_bf = _graph_time(lambda: rc.face_velocity_divergence(vel, p, rho, 0.01, kappa=kappa, psi=psi, we=0.7), reps)
+    div = torch.empty_like(p)
+    sh = (C.c_int64 * len(shape))(*shape)
+    lib = _lib.load()
+    tdt = _lib.TPF_F64 if dt_ == torch.float64 else _lib.TPF_F32
+
+    def kern(ax):
+        _lib.check(lib.tpf_rc_divergence_axis(len(shape), sh, ax, 1 if bc == "periodic" else 0, 1.0 / N[ax], 0.01,
+                                              _lib.dptr(vel[ax]), _lib.dptr(p), _lib.dptr(rho), _lib.dptr(dp), None,
+                                              None, None, 0.0, 1, _lib.dptr(div), tdt, _lib.current_stream_handle()))
+
+    nbytes = 6 * p.numel() * p.element_size()     # read u*, p, rho, dp, div; write div
+    axes = []
+    for ax in range(len(N)):
+        ms_k = _graph_time(lambda: kern(ax), reps)
+        axes.append({"axis": ax, "us": round(ms_k * 1e3, 1), "GBps": round(nbytes / (ms_k * 1e-3) / 1e9, 1)})
+    return {"case": "rhiechow", "N": list(N), "bc": bc, "dtype": dtype, "us_per_call": round(ms * 1e3, 1),
+            "us_per_call_bf": round(ms_bf * 1e3, 1), "axis_kernel": axes}
 
 
 def ppe_case(N, precision, reps, tol=1e-8):
@@ -287,7 +374,7 @@ def gmres_case(N, line, reps, maxiter=None, tol=1e-8):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["ccd", "ppe", "learned", "batched", "gmres", "corrector"])
+    ap.add_argument("case", choices=["ccd", "ppe", "learned", "batched", "gmres", "corrector", "curvature", "rhiechow"])
     ap.add_argument("--line", default="thomas", choices=["thomas", "pcr"], help="gmres: line solver")
     ap.add_argument("--N", type=int, nargs="+", required=True)
     ap.add_argument("--axis", type=int, default=0)
@@ -308,6 +395,10 @@ def main(argv=None):
         r = gmres_case(tuple(a.N), a.line, a.reps, a.maxiter or None)
     elif a.case == "corrector":
         r = corrector_case(tuple(a.N), a.axis, a.bc, a.dtype, a.reps)
+    elif a.case == "curvature":
+        r = curvature_case(tuple(a.N), a.bc, a.dtype, a.reps)
+    elif a.case == "rhiechow":
+        r = rhiechow_case(tuple(a.N), a.bc, a.dtype, a.reps)
     else:
         r = batched_case(n_cases=a.N[0], reps=a.reps)
     print(json.dumps(r), flush=True)

@@ -49,11 +49,11 @@ def _filter_tensor(f, grid, eps_d: float, bc_type: str, switch=None):
     shape = (C.c_int64 * nd)(*[int(s) for s in f.shape])
     per = (C.c_int * nd)(*[1 if axes[a] == "periodic" else 0 for a in range(nd)])
     out = torch.empty_like(f)
-    tmp = torch.empty_like(f)
+    tmp = torch.empty_like(f) if nd == 3 else None
     sw = switch.contiguous() if switch is not None else None
     _lib.check(_lib.load().tpf_dccd_filter(nd, shape, per, float(eps_d), _lib.dptr(sw) if sw is not None else None,
-                                           _lib.dptr(f), _lib.dptr(out), _lib.dptr(tmp), _tdtype(f),
-                                           _lib.current_stream_handle()))
+                                           _lib.dptr(f), _lib.dptr(out), _lib.dptr(tmp) if tmp is not None else None,
+                                           _tdtype(f), _lib.current_stream_handle()))
     return out
 
 
@@ -95,10 +95,12 @@ class CurvatureCalculatorPsi:
             g1, g2 = ccd.differentiate(p, ax)
             d1.append(F(g1))
             d2.append(F(g2))
+        # mixed derivatives by sequential CCD, first derivative only (the same
+        # line solve; the unused second derivative is not written)
         if ndim == 2:
-            mixed = [F(ccd.differentiate(d1[0], 1)[0])]
-        else:   # the 3-D formula uses the mixed derivatives unfiltered (curvature_psi.py:153-162)
-            mixed = [ccd.differentiate(d1[i], j)[0] for i in range(3) for j in range(i + 1, 3)]
+            mixed = [F(ccd.first_derivative(d1[0], 1))]
+        else:   # the 3-D formula uses them unfiltered (curvature_psi.py:153-162)
+            mixed = [ccd.first_derivative(d1[i], j) for i in range(3) for j in range(i + 1, 3)]
         kappa = torch.empty_like(p)
         P = C.c_void_p * 3
         pd1 = P(*([_lib.dptr(t) for t in d1] + [None] * (3 - ndim)))

@@ -13,6 +13,9 @@ time step, with the reference's classes and signatures.
   time step (src/twophase/time_integration/cfl.py:41-137): the maxima come
   from one reduction kernel (tpf_cfl_maxima), the formula is the reference's,
   evaluated on the host in the same order.
+* ``RhieChowInterpolator.face_velocity_divergence(vel_star, p, rho, dt, kappa,
+  psi, we)`` -- the Rhie-Chow face-velocity divergence, the PPE right-hand side
+  (src/twophase/spatial/rhie_chow.py:55-284).
 """
 
 from __future__ import annotations
@@ -147,3 +150,54 @@ class CFLCalculator:
         if self._dt_sigma is not None:
             dt_candidates.append(cfl * self._dt_sigma)
         return max(min(dt_candidates), 1.0e-8)
+
+
+class RhieChowInterpolator:
+    """Rhie-Chow face velocities and their divergence, the PPE right-hand side
+    (src/twophase/spatial/rhie_chow.py:38-284).
+
+    Per axis: one CCD line solve for the cell pressure gradient (and for
+    D1 psi when the balanced-force terms are on), then one kernel
+    (tpf_rc_divergence_axis) that forms both faces of every node and adds the
+    axis' flux divergence into the result.  ``bc_type`` picks the face-0 and
+    node-N rules per axis, independently of the CCD's boundary type, as in the
+    reference."""
+
+    def __init__(self, backend, grid, ccd, bc_type: str = "wall"):
+        from .grid import boundary_axes
+        self.backend = backend
+        self.xp = getattr(backend, "xp", None)
+        self.grid = grid
+        self.ndim = grid.ndim
+        self.ccd = ccd
+        self.bc_type = bc_type
+        self._axes = boundary_axes(bc_type, self.ndim)
+        self.lib = _lib.load()
+
+    def face_velocity_divergence(self, vel_star: List, p, rho, dt: float, kappa=None, psi=None, we: float = None):
+        """div u_RC (rhie_chow.py:55-115); the balanced-force form when kappa,
+        psi and we are all given."""
+        torch = _torch()
+        dtype = getattr(self.ccd, "dtype", torch.float64)
+        vp = to_device(p, dtype=dtype)
+        pt = vp.tensor
+        rt = to_device(rho, dtype=dtype).tensor
+        bf = kappa is not None and psi is not None and we is not None
+        kt = to_device(kappa, dtype=dtype).tensor if bf else None
+        st = to_device(psi, dtype=dtype).tensor if bf else None
+        div = torch.empty_like(pt)
+        shape = (C.c_int64 * pt.dim())(*[int(s) for s in pt.shape])
+        tdt = _lib.TPF_F64 if dtype == torch.float64 else _lib.TPF_F32
+        for ax in range(self.ndim):
+            h = float(self.grid.L[ax] / self.grid.N[ax])
+            ut = to_device(vel_star[ax], dtype=dtype).tensor
+            if ut.shape != pt.shape or rt.shape != pt.shape:
+                raise ValueError("u*, p and rho must have the grid's shape")
+            dp = self.ccd.first_derivative(pt, ax)
+            dpsi = self.ccd.first_derivative(st, ax) if bf else None
+            _lib.check(self.lib.tpf_rc_divergence_axis(
+                pt.dim(), shape, ax, 1 if self._axes[ax] == "periodic" else 0, h, float(dt),
+                _lib.dptr(ut), _lib.dptr(pt), _lib.dptr(rt), _lib.dptr(dp),
+                _lib.dptr(kt) if bf else None, _lib.dptr(st) if bf else None, _lib.dptr(dpsi) if bf else None,
+                float(we) if bf else 0.0, 1 if ax > 0 else 0, _lib.dptr(div), tdt, _lib.current_stream_handle()))
+        return vp.out(div)
