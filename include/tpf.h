@@ -169,6 +169,40 @@ int tpf_rc_divergence_axis(int ndim, const int64_t* shape, int axis, int periodi
                            const void* kappa, const void* psi, const void* dpsi, double we,
                            int accumulate, void* div, int dtype, void* stream);
 
+/* ---- CLS transport: FCCD flux-form advection and TVD-RK3 --------------- */
+
+/* prod = u * phi, n values (the product of compute_fccd_flux_contribution,
+ * src/twophase/ccd/fccd_advection_helpers.py:8-13). */
+int tpf_fccd_product(int64_t n, const void* u, const void* phi, void* prod, int dtype, void* stream);
+
+/* acc (+)= -face_divergence(face_value(prod, q)) along one axis
+ * (fccd_advection_helpers.py:8-13; fccd.py:213-233,279-299,464-520): face
+ * value 0.5 (p_j + p_{j+1}) - (H^2/16)(q_j + q_{j+1}), divergence
+ * (F_k - F_{k-1}) / H on the N unique nodes with wrap-around and node N <-
+ * node 0 (periodic) or on nodes 1..N-1 with 0 on the wall nodes.  q = the CCD
+ * second derivative of prod along the axis; h = the uniform node spacing.
+ * accumulate = 0 writes 0 + (-div) (the first axis), 1 adds to acc.  acc must
+ * not alias prod or q. */
+int tpf_fccd_flux_divergence_axis(int ndim, const int64_t* shape, int axis, int periodic, double h,
+                                  const void* prod, const void* q, int accumulate, void* acc, int dtype,
+                                  void* stream);
+
+/* One TVD-RK3 stage (src/twophase/time_integration/tvd_rk3.py:26-48) with the
+ * post-stage clip to [lo, hi] (clip != 0) and periodic image sync of
+ * FCCDLevelSetAdvection.advance (levelset/fccd_advection.py:86-129):
+ * stage 1: out = q + dt L; stages 2 and 3: out = ca q0 + cb (q + dt L)
+ * (ca, cb = 0.75, 0.25 and 1/3, 2/3).  periodic[a] != 0 marks periodic axes
+ * (their node N takes node 0's value); with any periodic axis out must not
+ * alias an input. */
+int tpf_tvd_rk3_stage(int ndim, const int64_t* shape, const int* periodic, int stage, double ca, double cb,
+                      double dt, const void* q0, const void* q, const void* L, int clip, double lo, double hi,
+                      void* out, int dtype, void* stream);
+
+/* In place: node N of every periodic axis takes node 0's value, axes in turn
+ * (sync_periodic_image_nodes, src/twophase/core/boundary.py:116-133). */
+int tpf_sync_periodic_images(int ndim, const int64_t* shape, const int* periodic, void* arr, int dtype,
+                             void* stream);
+
 /* Zero grad at index 0 and n_pts-1 along the axis of a [outer, n, inner]
  * array (wall axes only; no-op for periodic plans).  Replaces
  * CCDSolver.enforce_wall_neumann (ccd_solver.py:264-281;

@@ -393,13 +393,63 @@ def make_rhiechow(out):
         out[f"{name}/div_bf"] = np.asarray(rc.face_velocity_divergence(vel, p, rho, dt, kappa=kappa, psi=psi, we=we))
 
 
+def make_advect(out):
+    """FCCD flux-form advection right-hand sides and one TVD-RK3 level-set
+    step of the reference on seeded fields."""
+    from twophase.backend import Backend
+    from twophase.config import GridConfig
+    from twophase.core.grid import Grid
+    from twophase.ccd.ccd_solver import CCDSolver
+    from twophase.ccd.fccd import FCCDSolver
+    from twophase.levelset.fccd_advection import FCCDLevelSetAdvection
+    from twophase.levelset.heaviside import heaviside
+
+    be = Backend(use_gpu=False)
+    xp = be.xp
+    rng = np.random.default_rng(31337)
+    cases = [("wall2d", (20, 16), (1.0, 0.8), "wall"), ("per2d", (16, 12), (1.0, 1.0), "periodic"),
+             ("wall3d", (8, 10, 6), (1.0, 1.2, 0.8), "wall"), ("per3d", (8, 6, 10), (1.0, 1.0, 1.0), "periodic")]
+    for name, N, L, bc in cases:
+        grid = Grid(GridConfig(ndim=len(N), N=N, L=L), be)
+        ccd = CCDSolver(grid, be, bc_type=bc)
+        fccd = FCCDSolver(grid, be, bc_type=bc, ccd_solver=ccd)
+        X = np.meshgrid(*[np.linspace(0.0, L[a], N[a] + 1) for a in range(len(N))], indexing="ij")
+        phi = np.sqrt(sum((X[a] - 0.5 * L[a]) ** 2 for a in range(len(N)))) - 0.25
+        psi = np.asarray(heaviside(xp, phi, 1.5 * max(L[a] / N[a] for a in range(len(N)))))
+        vel = [0.5 * rng.standard_normal(grid.shape) + 0.3 * np.cos(2 * np.pi * X[(a + 1) % len(N)])
+               for a in range(len(N))]
+        if bc == "periodic":   # periodic fields carry equal image planes
+            for v in vel + [psi]:
+                for ax in range(len(N)):
+                    src = [slice(None)] * len(N)
+                    img = [slice(None)] * len(N)
+                    src[ax] = 0
+                    img[ax] = -1
+                    v[tuple(img)] = v[tuple(src)]
+        dt = 0.004
+        out[f"{name}/N"] = np.array(N)
+        out[f"{name}/L"] = np.array(L, dtype=np.float64)
+        out[f"{name}/bc"] = np.array(bc)
+        out[f"{name}/psi"] = psi
+        out[f"{name}/dt"] = np.array(dt)
+        for a in range(len(N)):
+            out[f"{name}/u{a}"] = vel[a]
+        out[f"{name}/rhs_scalar"] = np.asarray(fccd.advection_rhs(vel, scalar=psi, mode="flux")[0])
+        mom = fccd.advection_rhs(vel, mode="flux")
+        for a in range(len(N)):
+            out[f"{name}/rhs_mom{a}"] = np.asarray(mom[a])
+        adv = FCCDLevelSetAdvection(be, grid, fccd, mode="flux")
+        out[f"{name}/psi_new"] = np.asarray(adv.advance(psi.copy(), vel, dt))
+        out[f"{name}/psi_new_noclip"] = np.asarray(adv.advance(psi.copy(), vel, dt, clip_bounds=None))
+
+
 def main():
-    """Usage: make_golden.py [reference src dir] [only: ccd|ppe|step|levelset|rhiechow ...]."""
+    """Usage: make_golden.py [reference src dir] [only: ccd|ppe|step|levelset|rhiechow|advect ...]."""
     src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
     only = set(sys.argv[2:])
     _ref_import(src)
     makers = {"ccd": make_ccd, "ppe": make_ppe, "step": make_step, "levelset": make_levelset,
-              "rhiechow": make_rhiechow}
+              "rhiechow": make_rhiechow, "advect": make_advect}
     for key, fn in makers.items():
         if only and key not in only:
             continue

@@ -15,6 +15,7 @@ All arithmetic runs in the in-tree CUDA library ``libtpf.so`` (C ABI:
 ``include/tpf.h``); build it with ``python -m twophaseflow_b200.build``.
 """
 
+from .advection import FCCDLevelSetAdvection, FCCDSolver
 from .ccd import CCDSolver
 from .ccd_ppe import CCDVariableDensityOperator, PPESolverDefectCorrection
 from .grid import BoundarySpec, UniformGrid
@@ -25,6 +26,8 @@ from .step import CFLCalculator, RhieChowInterpolator, VelocityCorrector, ccd_pr
 
 __all__ = [
     "CCDSolver",
+    "FCCDSolver",
+    "FCCDLevelSetAdvection",
     "CCDVariableDensityOperator",
     "PPESolverDefectCorrection",
     "PPESolverFVMMatrixFree",

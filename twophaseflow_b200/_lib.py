@@ -102,6 +102,14 @@ SIGNATURES = {
     "tpf_rc_divergence_axis": (C.c_int, [C.c_int, C.POINTER(C.c_int64), C.c_int, C.c_int, C.c_double, C.c_double,
                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
+    "tpf_fccd_product": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "tpf_fccd_flux_divergence_axis": (C.c_int, [C.c_int, C.POINTER(C.c_int64), C.c_int, C.c_int, C.c_double,
+                                                C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
+    "tpf_tvd_rk3_stage": (C.c_int, [C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int), C.c_int, C.c_double,
+                                    C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double,
+                                    C.c_double, C.c_void_p, C.c_int, C.c_void_p]),
+    "tpf_sync_periodic_images": (C.c_int, [C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int), C.c_void_p, C.c_int,
+                                           C.c_void_p]),
     "tpf_ccd_enforce_wall_neumann": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]),
     "tpf_ppe_default_options": (None, [C.POINTER(tpf_ppe_options)]),
     "tpf_ppe_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_int64),

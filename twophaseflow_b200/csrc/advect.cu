@@ -1,0 +1,310 @@
+// CLS transport: the FCCD flux-form advection right-hand side and the TVD-RK3
+// stages around it.
+// Reference: src/twophase/ccd/fccd.py:213-233 (face slices), :279-299 (face
+// value), :464-520 (face divergence), ccd/fccd_advection_helpers.py:8-72
+// (flux contribution and the composed right-hand side),
+// time_integration/tvd_rk3.py:26-48 (stages), levelset/fccd_advection.py:86-129
+// (clip + periodic image after every stage), core/boundary.py:116-133 (image
+// nodes).  Arithmetic uses explicit round-to-nearest operations in the order
+// NumPy evaluates the reference's expressions (no fused multiply-add), so the
+// results equal the reference's for the same CCD second derivatives.
+#include "tpf_common.cuh"
+
+#include <algorithm>
+
+namespace {
+
+__device__ __forceinline__ double rn_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double rn_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double rn_mul(double a, double b) { return __dmul_rn(a, b); }
+
+inline int blocks_for(int64_t n, int per_sm) {
+  return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)tpf::sm_count() * per_sm));
+}
+
+template <typename T>
+__global__ void product_kernel(int64_t n, const T* a, const T* b, T* out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (T)rn_mul((double)a[i], (double)b[i]);
+}
+
+struct FluxArgs {
+  const void* prod;   // u_k * phi at the nodes
+  const void* q;      // its CCD second derivative along the axis
+  void* acc;
+  int64_t outer, n, inner;
+  double inv_h, h2_16;
+  int periodic, accumulate;
+};
+
+template <typename T>
+__device__ __forceinline__ double ldv(const void* p, int64_t i) { return (double)static_cast<const T*>(p)[i]; }
+
+// face value between nodes j and j+1 (fccd.py:279-299):
+// 0.5 (u_j + u_{j+1}) - (H^2/16) (q_j + q_{j+1})
+template <typename T>
+__device__ __forceinline__ double face_val(const FluxArgs& a, int64_t il, int64_t ir) {
+  return rn_sub(rn_mul(0.5, rn_add(ldv<T>(a.prod, il), ldv<T>(a.prod, ir))),
+                rn_mul(a.h2_16, rn_add(ldv<T>(a.q, il), ldv<T>(a.q, ir))));
+}
+
+template <typename T>
+__device__ __forceinline__ void flux_store(const FluxArgs& a, int64_t idx, double div) {
+  T* acc = static_cast<T*>(a.acc);
+  const double c = -div;   // the contribution is minus the face divergence
+  acc[idx] = (T)(a.accumulate ? rn_add((double)acc[idx], c) : rn_add(0.0, c));
+}
+
+// divergence at node k of the line starting at base (fccd.py:464-520):
+// periodic: (F[k] - F[k-1]) / H over the N unique nodes (F[-1] = F[N-1], the
+// face after node N-1 wraps to node 0), node N repeats node 0; wall: nodes
+// 1..N-1, 0 on the wall nodes.
+template <typename T>
+__device__ __forceinline__ double flux_div_node(const FluxArgs& a, int64_t base, int64_t k) {
+  const int64_t N = a.n - 1, s = a.inner;
+  if (a.periodic) {
+    const int64_t kk = (k == N) ? 0 : k;
+    const int64_t kp = (kk == N - 1) ? 0 : kk + 1, km = (kk == 0) ? N - 1 : kk - 1;
+    const double fr = face_val<T>(a, base + kk * s, base + kp * s);
+    const double fl = face_val<T>(a, base + km * s, base + kk * s);
+    return rn_mul(rn_sub(fr, fl), a.inv_h);
+  }
+  if (k == 0 || k == N) return 0.0;
+  const double fr = face_val<T>(a, base + k * s, base + (k + 1) * s);
+  const double fl = face_val<T>(a, base + (k - 1) * s, base + k * s);
+  return rn_mul(rn_sub(fr, fl), a.inv_h);
+}
+
+// one thread per node (contiguous or short-stride axes: the neighbours are in
+// the same cache lines)
+template <typename T>
+__global__ void flux_div_kernel(FluxArgs a) {
+  const int64_t tot = a.outer * a.n * a.inner;
+  const bool small = tot < (int64_t(1) << 31);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t k, in;
+    if (small) {
+      const uint32_t ii = (uint32_t)i, inn = (uint32_t)a.inner;
+      in = ii % inn;
+      k = (ii / inn) % (uint32_t)a.n;
+    } else {
+      in = i % a.inner;
+      k = (i / a.inner) % a.n;
+    }
+    const int64_t base = i - k * a.inner;
+    (void)in;
+    flux_store<T>(a, i, flux_div_node<T>(a, base, k));
+  }
+}
+
+// strided axes: thread (chunk, line) marches over a chunk of one line,
+// consecutive threads on consecutive lines (coalesced), one face formed per
+// node, the next node's operands loaded before the store
+template <typename T>
+__global__ void __launch_bounds__(256) flux_march_kernel(FluxArgs a, int64_t chunk, int64_t nchunks) {
+  const int64_t lines = a.outer * a.inner, N = a.n - 1, s = a.inner;
+  const int64_t work = lines * nchunks;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < work; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t qi = t / lines, c = t - qi * lines;
+    const int64_t o = c / s, in = c - o * s;
+    const int64_t base = o * a.n * s + in;
+    const int64_t k0 = qi * chunk, k1 = min(k0 + chunk, a.n);
+    if (a.periodic) {
+      // face to the left of node k (k = N reads node 0's faces)
+      auto fleft = [&](int64_t k) {
+        const int64_t kk = (k == N) ? 0 : k;
+        const int64_t km = (kk == 0) ? N - 1 : kk - 1;
+        return face_val<T>(a, base + km * s, base + kk * s);
+      };
+      double fl = fleft(k0);
+      for (int64_t k = k0; k < k1; ++k) {
+        const int64_t kk = (k == N) ? 0 : k;
+        const int64_t kp = (kk == N - 1) ? 0 : kk + 1;
+        const double fr = (k == N) ? face_val<T>(a, base, base + kp * s) : face_val<T>(a, base + kk * s, base + kp * s);
+        const double old = a.accumulate ? (double)static_cast<const T*>(a.acc)[base + k * s] : 0.0;
+        const double flk = (k == N) ? fleft(N) : fl;
+        const double c2 = -rn_mul(rn_sub(fr, flk), a.inv_h);
+        static_cast<T*>(a.acc)[base + k * s] = (T)rn_add(old, c2);
+        fl = fr;
+      }
+    } else {
+      double fl = (k0 >= 1) ? face_val<T>(a, base + (k0 - 1) * s, base + k0 * s) : 0.0;
+      for (int64_t k = k0; k < k1; ++k) {
+        const double fr = (k < N) ? face_val<T>(a, base + k * s, base + (k + 1) * s) : 0.0;
+        const double old = a.accumulate ? (double)static_cast<const T*>(a.acc)[base + k * s] : 0.0;
+        const double div = (k == 0 || k == N) ? 0.0 : rn_mul(rn_sub(fr, fl), a.inv_h);
+        static_cast<T*>(a.acc)[base + k * s] = (T)rn_add(old, -div);
+        fl = fr;
+      }
+    }
+  }
+}
+
+struct Shape3 {
+  int64_t n[3];
+  int per[3];
+  int ndim;
+};
+
+// node whose value the periodic image node x takes (every periodic coordinate
+// N -> 0, as sync_periodic_image_nodes applies the axes in turn)
+__device__ __forceinline__ int64_t image_source(const Shape3& s, int64_t i) {
+  int64_t c[3] = {0, 0, 0}, r = i;
+  for (int a = s.ndim - 1; a >= 0; --a) {
+    c[a] = r % s.n[a];
+    r /= s.n[a];
+  }
+  int64_t j = 0;
+  for (int a = 0; a < s.ndim; ++a) {
+    const int64_t ca = (s.per[a] && c[a] == s.n[a] - 1) ? 0 : c[a];
+    j = j * s.n[a] + ca;
+  }
+  return j;
+}
+
+// TVD-RK3 stage (tvd_rk3.py:26-48) with the post-stage clip and image sync
+// (fccd_advection.py:116-120): stage 1: q + dt L; stages 2, 3:
+// a q0 + b (q + dt L); then clip to [lo, hi] (NaN kept) and the periodic
+// image nodes take their source node's value.
+template <typename T>
+__global__ void rk3_stage_kernel(Shape3 s, int stage, double ca, double cb, double dt, const T* q0, const T* q,
+                                 const T* L, int clip, double lo, double hi, int any_per, T* out) {
+  const int64_t tot = s.n[0] * s.n[1] * s.n[2];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = any_per ? image_source(s, i) : i;
+    const double up = rn_add((double)q[j], rn_mul(dt, (double)L[j]));
+    double v = (stage == 1) ? up : rn_add(rn_mul(ca, (double)q0[j]), rn_mul(cb, up));
+    v = (double)(T)v;
+    if (clip) v = v < lo ? lo : (v > hi ? hi : v);
+    out[i] = (T)v;
+  }
+}
+
+template <typename T>
+__global__ void sync_images_kernel(Shape3 s, T* arr) {
+  const int64_t tot = s.n[0] * s.n[1] * s.n[2];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = image_source(s, i);
+    if (j != i) arr[i] = arr[j];   // sources have no coordinate at N: never written
+  }
+}
+
+int make_shape(int ndim, const int64_t* shape, const int* periodic, Shape3& s) {
+  TPF_CHECK_ARG(ndim >= 1 && ndim <= 3 && shape, "ndim must be 1..3");
+  s.ndim = ndim;
+  for (int a = 0; a < 3; ++a) {
+    s.n[a] = 1;
+    s.per[a] = 0;
+  }
+  for (int a = 0; a < ndim; ++a) {
+    TPF_CHECK_ARG(shape[a] >= 1, "empty axis");
+    s.n[a] = shape[a];
+    s.per[a] = periodic ? (periodic[a] ? 1 : 0) : 0;
+    TPF_CHECK_ARG(!s.per[a] || shape[a] >= 3, "a periodic axis needs at least 3 nodes");
+  }
+  return TPF_OK;
+}
+
+}  // namespace
+
+extern "C" int tpf_fccd_product(int64_t n, const void* u, const void* phi, void* prod, int dtype, void* stream) {
+  TPF_CHECK_ARG(n >= 0 && u && phi && prod, "NULL argument");
+  TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
+  if (n == 0) return TPF_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (dtype == TPF_F64)
+    product_kernel<double><<<blocks_for(n, 16), 256, 0, st>>>(n, static_cast<const double*>(u),
+                                                             static_cast<const double*>(phi), static_cast<double*>(prod));
+  else
+    product_kernel<float><<<blocks_for(n, 16), 256, 0, st>>>(n, static_cast<const float*>(u),
+                                                            static_cast<const float*>(phi), static_cast<float*>(prod));
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
+extern "C" int tpf_fccd_flux_divergence_axis(int ndim, const int64_t* shape, int axis, int periodic, double h,
+                                             const void* prod, const void* q, int accumulate, void* acc, int dtype,
+                                             void* stream) {
+  TPF_CHECK_ARG(ndim >= 1 && ndim <= 3 && shape && axis >= 0 && axis < ndim, "invalid shape or axis");
+  TPF_CHECK_ARG(prod && q && acc && acc != prod && acc != q, "NULL or aliased argument");
+  TPF_CHECK_ARG(h > 0.0, "h must be positive");
+  TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
+  FluxArgs a{};
+  a.prod = prod; a.q = q; a.acc = acc;
+  a.outer = 1; a.inner = 1;
+  for (int d = 0; d < ndim; ++d) {
+    TPF_CHECK_ARG(shape[d] >= 1, "empty axis");
+    if (d < axis) a.outer *= shape[d];
+    if (d > axis) a.inner *= shape[d];
+  }
+  a.n = shape[axis];
+  TPF_CHECK_ARG(a.n >= (periodic ? 3 : 2), "too few nodes along the axis (%lld)", (long long)a.n);
+  // the reference's constants: inv_H = 1/H, H^2/16 = H*H/16 (fccd_helpers.py:23-34)
+  a.inv_h = 1.0 / h;
+  a.h2_16 = (h * h) / 16.0;
+  a.periodic = periodic ? 1 : 0;
+  a.accumulate = accumulate ? 1 : 0;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int64_t tot = a.outer * a.n * a.inner;
+  if (a.inner >= 32) {
+    const int64_t lines = a.outer * a.inner, sms = tpf::sm_count();
+    int64_t chunk = (lines * a.n) / (sms * 2048);
+    chunk = std::max<int64_t>(8, std::min<int64_t>(64, chunk));
+    const int64_t nchunks = (a.n + chunk - 1) / chunk;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((lines * nchunks + 255) / 256, sms * 8));
+    if (dtype == TPF_F64) flux_march_kernel<double><<<blocks, 256, 0, st>>>(a, chunk, nchunks);
+    else flux_march_kernel<float><<<blocks, 256, 0, st>>>(a, chunk, nchunks);
+  } else {
+    if (dtype == TPF_F64) flux_div_kernel<double><<<blocks_for(tot, 16), 256, 0, st>>>(a);
+    else flux_div_kernel<float><<<blocks_for(tot, 16), 256, 0, st>>>(a);
+  }
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
+extern "C" int tpf_tvd_rk3_stage(int ndim, const int64_t* shape, const int* periodic, int stage, double ca, double cb,
+                                 double dt, const void* q0, const void* q, const void* L, int clip, double lo,
+                                 double hi, void* out, int dtype, void* stream) {
+  Shape3 s;
+  const int rc = make_shape(ndim, shape, periodic, s);
+  if (rc != TPF_OK) return rc;
+  TPF_CHECK_ARG(stage >= 1 && stage <= 3, "stage must be 1, 2 or 3");
+  TPF_CHECK_ARG(q && L && out && (stage == 1 || q0), "NULL argument");
+  TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
+  int any_per = 0;
+  for (int a = 0; a < ndim; ++a) any_per |= s.per[a];
+  // out may equal q or L only without periodic axes (the image nodes read
+  // their source nodes, which another thread may already have overwritten)
+  TPF_CHECK_ARG(!any_per || (out != q && out != L && out != q0),
+                "with periodic axes the stage output must not alias its inputs");
+  const int64_t tot = s.n[0] * s.n[1] * s.n[2];
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (dtype == TPF_F64)
+    rk3_stage_kernel<double><<<blocks_for(tot, 16), 256, 0, st>>>(
+        s, stage, ca, cb, dt, static_cast<const double*>(q0), static_cast<const double*>(q),
+        static_cast<const double*>(L), clip, lo, hi, any_per, static_cast<double*>(out));
+  else
+    rk3_stage_kernel<float><<<blocks_for(tot, 16), 256, 0, st>>>(
+        s, stage, ca, cb, dt, static_cast<const float*>(q0), static_cast<const float*>(q),
+        static_cast<const float*>(L), clip, lo, hi, any_per, static_cast<float*>(out));
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
+extern "C" int tpf_sync_periodic_images(int ndim, const int64_t* shape, const int* periodic, void* arr, int dtype,
+                                        void* stream) {
+  Shape3 s;
+  const int rc = make_shape(ndim, shape, periodic, s);
+  if (rc != TPF_OK) return rc;
+  TPF_CHECK_ARG(arr, "NULL argument");
+  TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
+  int any_per = 0;
+  for (int a = 0; a < ndim; ++a) any_per |= s.per[a];
+  if (!any_per) return TPF_OK;
+  const int64_t tot = s.n[0] * s.n[1] * s.n[2];
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (dtype == TPF_F64) sync_images_kernel<double><<<blocks_for(tot, 16), 256, 0, st>>>(s, static_cast<double*>(arr));
+  else sync_images_kernel<float><<<blocks_for(tot, 16), 256, 0, st>>>(s, static_cast<float*>(arr));
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}

@@ -8,6 +8,7 @@
     python -m twophaseflow_b200.kernel_cases corrector --N 256 256 256 --axis 0 --bc wall [--reps 5]
     python -m twophaseflow_b200.kernel_cases curvature --N 256 256 256 --bc wall [--reps 3]
     python -m twophaseflow_b200.kernel_cases rhiechow --N 256 256 256 --bc wall [--reps 3]
+    python -m twophaseflow_b200.kernel_cases advect --N 256 256 256 --bc periodic [--reps 3]
 
 ``ccd`` captures ``reps`` CCDSolver.differentiate calls in one CUDA graph and
 replays it, so the reported time is device time per call (no Python launch
@@ -207,6 +208,45 @@ def rhiechow_case(N, bc, dtype, reps):
             "us_per_call_bf": round(ms_bf * 1e3, 1), "axis_kernel": axes}
 
 
+def advect_case(N, bc, dtype, reps):
+    """One TVD-RK3 level-set step with the FCCD flux-form right-hand side
+    (FCCDLevelSetAdvection.advance) on a sphere in a rotating-shear velocity,
+    and the face-value + divergence kernel alone per axis, graph-replayed."""
+    import ctypes as C
+    import math
+    import torch
+    from . import CCDSolver, FCCDLevelSetAdvection, FCCDSolver, UniformGrid, _lib
+    dt_ = torch.float64 if dtype == "f64" else torch.float32
+    nd = len(N)
+    ax = [torch.linspace(0.0, 1.0, n + 1, dtype=torch.float64, device="cuda") for n in N]
+    X = torch.meshgrid(*ax, indexing="ij")
+    r = torch.sqrt(sum((X[a] - 0.5) ** 2 for a in range(nd)))
+    psi = torch.sigmoid((0.25 - r) / (1.5 / max(N))).to(dt_).contiguous()
+    vel = [torch.sin(2 * math.pi * X[(a + 1) % nd]).to(dt_).contiguous() for a in range(nd)]
+    del X, r
+    grid = UniformGrid(N)
+    fccd = FCCDSolver(grid, None, bc_type=bc, ccd_solver=CCDSolver(grid, None, bc_type=bc, dtype=dt_))
+    adv = FCCDLevelSetAdvection(None, grid, fccd)
+    dt = 0.2 / max(N)
+    ms = _graph_time(lambda: adv.advance(psi, vel, dt), reps)
+    prod, q = torch.randn_like(psi), torch.randn_like(psi)
+    acc = torch.empty_like(psi)
+    sh = (C.c_int64 * nd)(*[n + 1 for n in N])
+    lib = _lib.load()
+    tdt = _lib.TPF_F64 if dt_ == torch.float64 else _lib.TPF_F32
+    nbytes = 4 * psi.numel() * psi.element_size()      # read prod, q, acc; write acc
+    axes = []
+    for a in range(nd):
+        def kern(a=a):
+            _lib.check(lib.tpf_fccd_flux_divergence_axis(nd, sh, a, 1 if bc == "periodic" else 0, 1.0 / N[a],
+                                                         _lib.dptr(prod), _lib.dptr(q), 1, _lib.dptr(acc), tdt,
+                                                         _lib.current_stream_handle()))
+        ms_k = _graph_time(kern, reps)
+        axes.append({"axis": a, "us": round(ms_k * 1e3, 1), "GBps": round(nbytes / (ms_k * 1e-3) / 1e9, 1)})
+    return {"case": "advect", "N": list(N), "bc": bc, "dtype": dtype, "us_per_rk3_step": round(ms * 1e3, 1),
+            "flux_kernel": axes}
+
+
 def ppe_case(N, precision, reps, tol=1e-8):
     import torch
     from . import PPESolverFVMMatrixFree, UniformGrid
@@ -374,7 +414,7 @@ def gmres_case(N, line, reps, maxiter=None, tol=1e-8):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["ccd", "ppe", "learned", "batched", "gmres", "corrector", "curvature", "rhiechow"])
+    ap.add_argument("case", choices=["ccd", "ppe", "learned", "batched", "gmres", "corrector", "curvature", "rhiechow", "advect"])
     ap.add_argument("--line", default="thomas", choices=["thomas", "pcr"], help="gmres: line solver")
     ap.add_argument("--N", type=int, nargs="+", required=True)
     ap.add_argument("--axis", type=int, default=0)
@@ -399,6 +439,8 @@ def main(argv=None):
         r = curvature_case(tuple(a.N), a.bc, a.dtype, a.reps)
     elif a.case == "rhiechow":
         r = rhiechow_case(tuple(a.N), a.bc, a.dtype, a.reps)
+    elif a.case == "advect":
+        r = advect_case(tuple(a.N), a.bc, a.dtype, a.reps)
     else:
         r = batched_case(n_cases=a.N[0], reps=a.reps)
     print(json.dumps(r), flush=True)
