@@ -400,6 +400,11 @@ def main(argv=None):
     from twophaseflow_b200.kernel_cases import curvature_case, rhiechow_case
     curv = curvature_case((256, 256, 256), "wall", "f64", 3)
     rcb = rhiechow_case((256, 256, 256), "wall", "f64", 3)
+    # CLS transport (one TVD-RK3 step, FCCD flux form) and split reinitialization
+    # (4 pseudo-steps + mass correction), 3-D 257^3 FP64
+    from twophaseflow_b200.kernel_cases import advect_case, reinit_case
+    advb = advect_case((256, 256, 256), "periodic", "f64", 2)
+    reib = reinit_case((256, 256, 256), "f64", 2)
 
     # many independent cases in one persistent launch (32 seeded grids, 128..512 per axis)
     from twophaseflow_b200.kernel_cases import batched_case
@@ -446,6 +451,8 @@ def main(argv=None):
                                             "frac_mean": round(float(np.mean([c["GBps"] for c in corr])) / peak, 3)},
             "curvature_257cubed_f64_wall": {k: v for k, v in curv.items() if k not in ("case", "N", "bc", "dtype")},
             "rhiechow_257cubed_f64_wall": {k: v for k, v in rcb.items() if k not in ("case", "N", "bc", "dtype")},
+            "cls_transport_257cubed_f64_periodic": {k: v for k, v in advb.items() if k not in ("case", "N", "bc", "dtype")},
+            "reinit_257cubed_f64": {k: v for k, v in reib.items() if k not in ("case", "N", "dtype")},
             "ccd_roofline": {"kernel": "ccd_lane_kernel (3-D 257^3 FP64, mean over axes and wall/periodic)",
                              "bound": "hbm", "achieved": round(ccd3_gbps, 1), "peak": peak, "unit": "GB/s",
                              "frac": round(ccd3_gbps / peak, 3),

@@ -203,6 +203,41 @@ int tpf_tvd_rk3_stage(int ndim, const int64_t* shape, const int* periodic, int s
 int tpf_sync_periodic_images(int ndim, const int64_t* shape, const int* periodic, void* arr, int dtype,
                              void* stream);
 
+/* ---- Split reinitialization (src/twophase/levelset/reinit_split.py:73-102) */
+
+/* flux[a] = psi (1 - psi) d1[a] / max(sqrt(max(|d1|^2, 1e-12)), 1e-6), a < ndim
+ * (compute_gradient_normal + dccd_compression_div, levelset/reinit_ops.py:57-114);
+ * d1[a] = the CCD first derivative of psi along axis a.  n values each. */
+int tpf_reinit_compression_flux(int ndim, int64_t n, const void* psi, const void* const* d1, void* const* flux,
+                                int dtype, void* stream);
+
+/* div (+)= g + eps_d ((g[+1] - 2 g) + g[-1]) along one axis with one ghost
+ * node each side: pad 0 = zero, 1 = periodic (g[n-2] / g[1]), 2 = the end
+ * node (neumann, outflow) (filtered_divergence, reinit_ops.py:83-105;
+ * pad_ghost_cells, core/boundary.py:249-292).  g = the CCD first derivative of
+ * the axis' compression flux; accumulate = 0 writes 0 + it. */
+int tpf_reinit_filtered_divergence_axis(int ndim, const int64_t* shape, int axis, int pad, double eps_d,
+                                        const void* g, int accumulate, void* div, int dtype, void* stream);
+
+/* One CN-ADI half-step along one axis (cn_diffusion_axis, reinit_ops.py:169-204):
+ * rhs = (M2 + mu B2) in with coefficients cR (off-diagonal), dR (diagonal)
+ * and doubled off-diagonals on the end rows, then the Thomas sweep with the
+ * factors f (n-1), m (n), sup (n-1) of build_cn_factors (:117-166), device
+ * FP64 arrays.  in and out distinct. */
+int tpf_reinit_cn_axis(int ndim, const int64_t* shape, int axis, double cR, double dR, const double* f,
+                       const double* m, const double* sup, const void* in, void* out, int dtype, void* stream);
+
+/* sums[0] = sum q dV, sums[1] = sum 4 q (1 - q) dV (two fixed-order passes;
+ * partials: 2048 doubles of device workspace).  dV: FP64 control volumes. */
+int tpf_mass_sums(int64_t n, const void* q, const double* dV, double* partials, double* sums, int dtype,
+                  void* stream);
+
+/* out = clip(q + gate * (target[0] - sums[0]) / W_safe * 4 q (1 - q), 0, 1),
+ * W = sums[1], W_safe = W if W > 1e-12 else 1, gate = W > 1e-12
+ * (apply_mass_correction, levelset/heaviside.py:118-149); all on the device. */
+int tpf_mass_correction_apply(int64_t n, const void* q, const double* target, const double* sums, void* out,
+                              int dtype, void* stream);
+
 /* Zero grad at index 0 and n_pts-1 along the axis of a [outer, n, inner]
  * array (wall axes only; no-op for periodic plans).  Replaces
  * CCDSolver.enforce_wall_neumann (ccd_solver.py:264-281;

@@ -7,6 +7,9 @@
 * ``advance`` -- one TVD-RK3 level-set step with clip and periodic image sync
   (``levelset/fccd_advection.py:86-129``, ``time_integration/tvd_rk3.py:26-48``,
   ``core/boundary.py:116-133``).
+* ``reinitialize`` -- the split reinitialization: compression + CN-ADI
+  diffusion + mass correction (``levelset/reinit_split.py:73-102``,
+  ``levelset/reinit_ops.py:34-204``, ``levelset/heaviside.py:118-149``).
 
 Pinned against the reference's own outputs in ``tests/golden/advect_golden.npz``.
 Only tests, smoke() and bench.py's CPU-baseline leg may use this module.
@@ -89,3 +92,128 @@ def advance(psi, vel, dt: float, L, N, bc: str, clip=(0.0, 1.0)):
     q1 = P(q0 + dt * R(q0))
     q2 = P(0.75 * q0 + 0.25 * (q1 + dt * R(q1)))
     return P((1.0 / 3.0) * q0 + (2.0 / 3.0) * (q2 + dt * R(q2)))
+
+
+# ── split reinitialization (levelset/reinit_split.py:73-102) ─────────────────
+
+BETA2 = -1.0 / 8.0
+
+
+def periodic_flags(bc, ndim):
+    """periodic_axis_flags (core/boundary.py:94-113)."""
+    if bc in ("zero", "neumann", "outflow"):
+        return [False] * ndim
+    return [k == "periodic" for k in axis_kinds(bc, ndim)]
+
+
+def cell_volumes(L, N, flags):
+    """Grid.cell_volumes for a uniform grid (core/grid.py:1123-1170)."""
+    ws = []
+    for a in range(len(N)):
+        coords = np.linspace(0.0, L[a], N[a] + 1)
+        if flags[a]:
+            cw = np.diff(coords)
+            w = np.empty_like(coords)
+            w[:-1] = 0.5 * (np.roll(cw, 1) + cw)
+            w[-1] = 0.0
+        else:
+            w = np.full(N[a] + 1, L[a] / N[a])
+        ws.append(w)
+    vol = ws[0]
+    for a in range(1, len(N)):
+        vol = np.expand_dims(vol, axis=a) * ws[a]
+    return vol
+
+
+def mass_correction(q, dV, M_target):
+    """apply_mass_correction (levelset/heaviside.py:118-149)."""
+    M_new = np.sum(q * dV)
+    w = 4.0 * q * (1.0 - q)
+    W = np.sum(w * dV)
+    W_safe = W if W > 1e-12 else 1.0
+    gate = 1.0 if W > 1e-12 else 0.0
+    return np.clip(q + (gate * ((M_target - M_new) / W_safe)) * w, 0.0, 1.0)
+
+
+def _pad(g, ax, bc):
+    label = bc.strip().lower()
+    n = g.shape[ax]
+    take = lambda i: np.take(g, [i], axis=ax)
+    if label == "periodic":
+        lo, hi = take(n - 2), take(1)
+    elif label in ("neumann", "outflow"):
+        lo, hi = take(0), take(n - 1)
+    else:
+        lo, hi = np.zeros_like(take(0)), np.zeros_like(take(0))
+    return np.concatenate([lo, g, hi], axis=ax)
+
+
+def reinitialize(psi, L, N, ccd_bc: str, eps: float, n_steps: int = 4, bc: str = "zero", eps_d: float = 0.05,
+                 mass: bool = True):
+    """SplitReinitializer.reinitialize (reinit_split.py:73-102, reinit_ops.py:34-204)."""
+    nd = len(N)
+    h = [float(L[a] / N[a]) for a in range(nd)]
+    dx = min(h)
+    dtau = min(0.5 * dx ** 2 / (2.0 * nd * float(np.min(eps))), 0.5 * dx)
+    kinds = axis_kinds(ccd_bc, nd)
+    flags = periodic_flags(bc, nd)
+    dV = cell_volumes(L, N, flags)
+
+    def sync(a):
+        for ax in range(nd):
+            if flags[ax]:
+                src = [slice(None)] * nd
+                img = [slice(None)] * nd
+                src[ax] = 0
+                img[ax] = -1
+                a[tuple(img)] = a[tuple(src)]
+        return a
+
+    def D1(f, ax):
+        return np.asarray(occd.differentiate(f, ax, h[ax], bc=kinds[ax])[0])
+
+    q = sync(np.array(psi, dtype=np.float64, copy=True))
+    M_old = np.sum(q * dV)
+    for _ in range(n_steps):
+        g = [D1(q, ax) for ax in range(nd)]
+        gs = sum(x * x for x in g)
+        sg = np.maximum(np.sqrt(np.maximum(gs, 1e-12)), 1e-6)
+        pp = q * (1.0 - q)
+        div = np.zeros_like(q)
+        for ax in range(nd):
+            gp = _pad(D1(pp * (g[ax] / sg), ax), ax, bc)
+            n = gp.shape[ax]
+            c = np.take(gp, range(1, n - 1), axis=ax)
+            pl = np.take(gp, range(2, n), axis=ax)
+            mi = np.take(gp, range(0, n - 2), axis=ax)
+            div = div + (c + eps_d * (pl - 2.0 * c + mi))
+        q_new = sync(np.clip(q - dtau * div, 0.0, 1.0))
+        for ax in range(nd):
+            mu = eps * dtau / (2.0 * h[ax] ** 2)
+            n = N[ax] + 1
+            d_L, c_L = 1.0 + 6.0 * mu, BETA2 - 3.0 * mu
+            main, sup, sub = np.full(n, d_L), np.full(n - 1, c_L), np.full(n - 1, c_L)
+            sup[0] = 2.0 * c_L
+            sub[-1] = 2.0 * c_L
+            m = main.copy()
+            f = np.empty(n - 1)
+            for i in range(1, n):
+                f[i - 1] = sub[i - 1] / m[i - 1]
+                m[i] -= f[i - 1] * sup[i - 1]
+            dR, cR = 1.0 - 6.0 * mu, BETA2 + 3.0 * mu
+            p = np.moveaxis(q_new, ax, 0)
+            d = np.empty_like(p)
+            d[1:-1] = cR * p[:-2] + dR * p[1:-1] + cR * p[2:]
+            d[0] = dR * p[0] + 2.0 * cR * p[1]
+            d[-1] = 2.0 * cR * p[-2] + dR * p[-1]
+            for i in range(1, n):
+                d[i] = d[i] - f[i - 1] * d[i - 1]
+            x = np.empty_like(d)
+            x[-1] = d[-1] / m[-1]
+            for i in range(n - 2, -1, -1):
+                x[i] = (d[i] - sup[i] * x[i + 1]) / m[i]
+            q_new = sync(np.moveaxis(x, 0, ax).copy())
+        q = sync(np.clip(q_new, 0.0, 1.0))
+    if mass:
+        q = sync(mass_correction(q, dV, M_old))
+    return q

@@ -441,15 +441,55 @@ def make_advect(out):
         adv = FCCDLevelSetAdvection(be, grid, fccd, mode="flux")
         out[f"{name}/psi_new"] = np.asarray(adv.advance(psi.copy(), vel, dt))
         out[f"{name}/psi_new_noclip"] = np.asarray(adv.advance(psi.copy(), vel, dt, clip_bounds=None))
+        adv_m = FCCDLevelSetAdvection(be, grid, fccd, mode="flux", mass_correction=True)
+        out[f"{name}/psi_new_mass"] = np.asarray(adv_m.advance(psi.copy(), vel, dt))
+
+
+def make_reinit(out):
+    """Split reinitialization (compression + CN-ADI + mass correction) of the
+    reference on seeded interface fields."""
+    from twophase.backend import Backend
+    from twophase.config import GridConfig
+    from twophase.core.grid import Grid
+    from twophase.ccd.ccd_solver import CCDSolver
+    from twophase.levelset.heaviside import heaviside
+    from twophase.levelset.reinit_split import SplitReinitializer
+
+    be = Backend(use_gpu=False)
+    xp = be.xp
+    rng = np.random.default_rng(4711)
+    cases = [("zero2d", (24, 20), (1.0, 0.9), "wall", "zero", 4, True),
+             ("per2d", (16, 16), (1.0, 1.0), "periodic", "periodic", 2, True),
+             ("neu2d", (20, 18), (1.0, 1.0), "wall", "neumann", 3, False),
+             ("zero3d", (10, 8, 12), (1.0, 0.8, 1.2), "wall", "zero", 2, True)]
+    for name, N, L, ccd_bc, bc, n_steps, mass in cases:
+        grid = Grid(GridConfig(ndim=len(N), N=N, L=L), be)
+        ccd = CCDSolver(grid, be, bc_type=ccd_bc)
+        h = max(L[a] / N[a] for a in range(len(N)))
+        X = np.meshgrid(*[np.linspace(0.0, L[a], N[a] + 1) for a in range(len(N))], indexing="ij")
+        phi = np.sqrt(sum(((X[a] - 0.5 * L[a]) / (0.3 + 0.05 * a)) ** 2 for a in range(len(N)))) - 1.0
+        psi = np.asarray(heaviside(xp, 0.3 * phi, 2.5 * h)) + 0.02 * rng.standard_normal(grid.shape)
+        psi = np.clip(psi, 0.0, 1.0)
+        eps = 1.5 * h
+        out[f"{name}/N"] = np.array(N)
+        out[f"{name}/L"] = np.array(L, dtype=np.float64)
+        out[f"{name}/ccd_bc"] = np.array(ccd_bc)
+        out[f"{name}/bc"] = np.array(bc)
+        out[f"{name}/eps"] = np.array(eps)
+        out[f"{name}/n_steps"] = np.array(n_steps)
+        out[f"{name}/mass"] = np.array(mass)
+        out[f"{name}/psi"] = psi
+        r = SplitReinitializer(be, grid, ccd, eps, n_steps=n_steps, bc=bc, mass_correction=mass)
+        out[f"{name}/psi_reinit"] = np.asarray(r.reinitialize(psi.copy()))
 
 
 def main():
-    """Usage: make_golden.py [reference src dir] [only: ccd|ppe|step|levelset|rhiechow|advect ...]."""
+    """Usage: make_golden.py [reference src dir] [only: ccd|ppe|step|levelset|rhiechow|advect|reinit ...]."""
     src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
     only = set(sys.argv[2:])
     _ref_import(src)
     makers = {"ccd": make_ccd, "ppe": make_ppe, "step": make_step, "levelset": make_levelset,
-              "rhiechow": make_rhiechow, "advect": make_advect}
+              "rhiechow": make_rhiechow, "advect": make_advect, "reinit": make_reinit}
     for key, fn in makers.items():
         if only and key not in only:
             continue

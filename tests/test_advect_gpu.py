@@ -141,3 +141,139 @@ def test_transport_full_size_properties(cuda_device):
         if check_oracle:
             ref = oa.advance(psi.cpu().numpy(), [v.cpu().numpy() for v in vel], 0.2 / n, (1.0,) * 3, N, "periodic")
             assert np.abs(out.cpu().numpy() - ref).max() <= 1e-12
+
+
+RGOLD = os.path.join(os.path.dirname(__file__), "golden", "reinit_golden.npz")
+REINIT = ["zero2d", "per2d", "neu2d", "zero3d"]
+
+
+@pytest.fixture(scope="module")
+def rgolden():
+    with np.load(RGOLD) as d:
+        return {k: d[k] for k in d.files}
+
+
+@pytest.mark.parametrize("name", REINIT)
+def test_reinit_matches_reference(cuda_device, rgolden, name):
+    """Within 1e-11 of the reference (the CCD's rounding differs; the oracle's
+    output moves by ~5e-14 for 1e-14 input noise on these fields)."""
+    from twophaseflow_b200 import CCDSolver, SplitReinitializer, UniformGrid
+    g = rgolden
+    N = tuple(int(x) for x in g[f"{name}/N"])
+    L = tuple(float(x) for x in g[f"{name}/L"])
+    grid = UniformGrid(N, L)
+    ccd = CCDSolver(grid, None, bc_type=str(g[f"{name}/ccd_bc"]))
+    r = SplitReinitializer(None, grid, ccd, float(g[f"{name}/eps"]), n_steps=int(g[f"{name}/n_steps"]),
+                           bc=str(g[f"{name}/bc"]), mass_correction=bool(g[f"{name}/mass"]))
+    out = r.reinitialize(g[f"{name}/psi"])
+    assert isinstance(out, np.ndarray)
+    assert np.abs(out - g[f"{name}/psi_reinit"]).max() <= 1e-11
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_mass_corrected_transport_matches_reference(cuda_device, golden, name):
+    from twophaseflow_b200 import FCCDLevelSetAdvection
+    N, grid, fccd = _setup(golden, name)
+    vel = [golden[f"{name}/u{a}"] for a in range(len(N))]
+    adv = FCCDLevelSetAdvection(None, grid, fccd, mode="flux", mass_correction=True)
+    out = adv.advance(golden[f"{name}/psi"].copy(), vel, float(golden[f"{name}/dt"]))
+    assert np.abs(out - golden[f"{name}/psi_new_mass"]).max() <= 1e-12
+
+
+@pytest.mark.parametrize("shape", [(1025, 1025), (129, 130, 131)])
+def test_reinit_kernels_bit_exact(cuda_device, shape):
+    """Compression flux, filtered divergence (all three paddings) and the CN
+    line solve alone, every axis, against the oracle's arithmetic."""
+    import torch
+    from twophaseflow_b200 import _lib
+    rng = np.random.default_rng(41)
+    nd = len(shape)
+    lib = _lib.load()
+    st = _lib.current_stream_handle()
+    sh = (C.c_int64 * nd)(*shape)
+    psi = rng.uniform(0.0, 1.0, shape)
+    d1 = [rng.standard_normal(shape) for _ in range(nd)]
+    d1[0][0, 0] = 1e-9   # below the |grad| floor
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    tp, td = T(psi), [T(a) for a in d1]
+    flux = [torch.empty_like(tp) for _ in range(nd)]
+    P = C.c_void_p * nd
+    _lib.check(lib.tpf_reinit_compression_flux(nd, tp.numel(), _lib.dptr(tp), P(*[_lib.dptr(t) for t in td]),
+                                               P(*[_lib.dptr(t) for t in flux]), _lib.TPF_F64, st))
+    gs = sum(x * x for x in d1)
+    sg = np.maximum(np.sqrt(np.maximum(gs, 1e-12)), 1e-6)
+    for a in range(nd):
+        np.testing.assert_array_equal(flux[a].cpu().numpy(), (psi * (1.0 - psi)) * (d1[a] / sg))
+    for pad, label in ((0, "zero"), (1, "periodic"), (2, "neumann")):
+        div = torch.empty_like(tp)
+        ref = np.zeros(shape)
+        for a in range(nd):
+            _lib.check(lib.tpf_reinit_filtered_divergence_axis(nd, sh, a, pad, 0.05, _lib.dptr(td[a]), 1 if a else 0,
+                                                               _lib.dptr(div), _lib.TPF_F64, st))
+            gp = oa._pad(d1[a], a, label)
+            n = gp.shape[a]
+            c = np.take(gp, range(1, n - 1), axis=a)
+            ref = ref + (c + 0.05 * (np.take(gp, range(2, n), axis=a) - 2.0 * c + np.take(gp, range(0, n - 2), axis=a)))
+        np.testing.assert_array_equal(div.cpu().numpy(), ref)
+    # CN line solve with factors built as the reference builds them
+    for a in range(nd):
+        n = shape[a]
+        mu = 0.7
+        c_L, d_L = oa.BETA2 - 3.0 * mu, 1.0 + 6.0 * mu
+        sup, sub, m = np.full(n - 1, c_L), np.full(n - 1, c_L), np.full(n, d_L)
+        sup[0] = 2.0 * c_L
+        sub[-1] = 2.0 * c_L
+        f = np.empty(n - 1)
+        for i in range(1, n):
+            f[i - 1] = sub[i - 1] / m[i - 1]
+            m[i] -= f[i - 1] * sup[i - 1]
+        cR, dR = oa.BETA2 + 3.0 * mu, 1.0 - 6.0 * mu
+        out = torch.empty_like(tp)
+        tf, tm, ts = T(f), T(m), T(sup)   # held until the kernel has run
+        _lib.check(lib.tpf_reinit_cn_axis(nd, sh, a, cR, dR, _lib.dptr(tf), _lib.dptr(tm), _lib.dptr(ts),
+                                          _lib.dptr(tp), _lib.dptr(out), _lib.TPF_F64, st))
+        torch.cuda.synchronize()
+        p = np.moveaxis(psi, a, 0)
+        d = np.empty_like(p)
+        d[1:-1] = cR * p[:-2] + dR * p[1:-1] + cR * p[2:]
+        d[0] = dR * p[0] + 2.0 * cR * p[1]
+        d[-1] = 2.0 * cR * p[-2] + dR * p[-1]
+        for i in range(1, n):
+            d[i] = d[i] - f[i - 1] * d[i - 1]
+        x = np.empty_like(d)
+        x[-1] = d[-1] / m[-1]
+        for i in range(n - 2, -1, -1):
+            x[i] = (d[i] - sup[i] * x[i + 1]) / m[i]
+        np.testing.assert_array_equal(out.cpu().numpy(), np.moveaxis(x, 0, a))
+
+
+def test_mass_correction_kernels(cuda_device):
+    """Device sums within rounding of NumPy's; the corrected field restores the
+    target mass and stays in [0, 1]; W <= 1e-12 leaves q unchanged."""
+    import torch
+    from twophaseflow_b200 import _lib
+    rng = np.random.default_rng(43)
+    q = rng.uniform(0.0, 1.0, (257, 257, 65))
+    dV = np.full(q.shape, 1.0 / 256 ** 2 / 64)
+    lib = _lib.load()
+    st = _lib.current_stream_handle()
+    tq, tv = torch.from_numpy(q).cuda(), torch.from_numpy(dV).cuda()
+    part = torch.empty(2048, dtype=torch.float64, device="cuda")
+    sums = torch.empty(2, dtype=torch.float64, device="cuda")
+    _lib.check(lib.tpf_mass_sums(q.size, _lib.dptr(tq), _lib.dptr(tv), _lib.dptr(part), _lib.dptr(sums),
+                                 _lib.TPF_F64, st))
+    s = sums.cpu().numpy()
+    assert abs(s[0] - np.sum(q * dV)) <= 1e-13 * abs(s[0])
+    assert abs(s[1] - np.sum(4.0 * q * (1.0 - q) * dV)) <= 1e-13 * abs(s[1])
+    target = torch.tensor([s[0] * 1.001], dtype=torch.float64, device="cuda")
+    out = torch.empty_like(tq)
+    _lib.check(lib.tpf_mass_correction_apply(q.size, _lib.dptr(tq), _lib.dptr(target), _lib.dptr(sums),
+                                             _lib.dptr(out), _lib.TPF_F64, st))
+    ref = oa.mass_correction(q, dV, s[0] * 1.001)
+    assert np.abs(out.cpu().numpy() - ref).max() <= 1e-15
+    z = torch.zeros_like(tq)
+    _lib.check(lib.tpf_mass_sums(q.size, _lib.dptr(z), _lib.dptr(tv), _lib.dptr(part), _lib.dptr(sums),
+                                 _lib.TPF_F64, st))
+    _lib.check(lib.tpf_mass_correction_apply(q.size, _lib.dptr(z), _lib.dptr(target), _lib.dptr(sums),
+                                             _lib.dptr(out), _lib.TPF_F64, st))
+    assert float(out.abs().max()) == 0.0

@@ -45,3 +45,30 @@ def test_flux_form_conserves_on_a_periodic_box():
         oa.sync_images(v, "periodic")
     r = oa.flux_rhs(vel, psi, L, N, "periodic")[0]
     assert abs(r[:-1, :-1].sum()) < 1e-10 * np.abs(r).sum()
+
+
+R = np.load(os.path.join(os.path.dirname(__file__), "golden", "reinit_golden.npz"))
+REINIT = ["zero2d", "per2d", "neu2d", "zero3d"]
+
+
+def reinit_args(g, name):
+    N = tuple(int(x) for x in g[f"{name}/N"])
+    L = tuple(float(x) for x in g[f"{name}/L"])
+    return (L, N, str(g[f"{name}/ccd_bc"]), float(g[f"{name}/eps"]), int(g[f"{name}/n_steps"]), str(g[f"{name}/bc"]),
+            0.05, bool(g[f"{name}/mass"]))
+
+
+@pytest.mark.parametrize("name", REINIT)
+def test_reinit_matches_reference(name):
+    """Split reinitialization (zero / periodic / neumann ghost padding, with and
+    without mass correction) equals the reference bit for bit."""
+    np.testing.assert_array_equal(oa.reinitialize(R[f"{name}/psi"], *reinit_args(R, name)), R[f"{name}/psi_reinit"])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_mass_corrected_transport_matches_reference(name):
+    N, L, bc, vel, psi, dt = _case(name)
+    q = oa.advance(psi, vel, dt, L, N, bc)
+    dV = oa.cell_volumes(L, N, oa.periodic_flags(bc, len(N)))
+    target = np.sum(oa.sync_images(psi.copy(), bc) * dV)
+    np.testing.assert_array_equal(oa.sync_images(oa.mass_correction(q, dV, target), bc), G[f"{name}/psi_new_mass"])

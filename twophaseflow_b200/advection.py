@@ -13,7 +13,14 @@ the TVD-RK3 level-set step, with the reference's classes and signatures.
   mass_correction=False).advance(psi, velocity_components, dt,
   clip_bounds=(0, 1))`` -- one TVD-RK3 step (levelset/fccd_advection.py:86-129,
   time_integration/tvd_rk3.py:26-48): three right-hand sides and three stage
-  kernels, each stage clipped and its periodic image nodes synchronised.
+  kernels, each stage clipped and its periodic image nodes synchronised,
+  then (mass_correction) the interface-weighted mass correction.
+* ``SplitReinitializer(backend, grid, ccd, eps, n_steps=4, bc="zero",
+  eps_d_comp=0.05, mass_correction=True).reinitialize(psi)`` -- compression
+  (forward Euler on the filtered CCD divergence of psi(1-psi) n) and CN-ADI
+  diffusion line solves per pseudo-step, then the interface-weighted mass
+  correction (levelset/reinit_split.py:22-102, reinit_ops.py:34-204,
+  heaviside.py:118-149).
 """
 
 from __future__ import annotations
@@ -120,14 +127,23 @@ class FCCDLevelSetAdvection:
             raise ValueError(f"mode must be 'node' or 'flux', got {mode!r}")
         if mode == "node":
             raise NotImplementedError("the B200 FCCD transport implements the flux form (Option B)")
-        if mass_correction:
-            raise NotImplementedError("mass_correction is not implemented on the B200 path")
         self._backend = backend
         self.xp = getattr(backend, "xp", None)
         self._grid = grid
         self._fccd = fccd
         self._mode = mode
         self._mass_correction = mass_correction
+        self._dV = None
+        if mass_correction:   # grid.cell_volumes(bc_type=fccd.bc_type), uploaded once
+            import numpy as np
+            torch = _torch()
+            per = _periodic_flags(fccd.bc_type, grid.ndim)
+            vol = _control_widths(grid, 0, per[0])
+            for ax in range(1, grid.ndim):
+                vol = np.expand_dims(vol, axis=ax) * _control_widths(grid, ax, per[ax])
+            dev = torch.device("cuda", torch.cuda.current_device())
+            self._dV = torch.from_numpy(np.ascontiguousarray(vol, dtype=np.float64)).to(dev)
+            self._partials = torch.empty(2048, dtype=torch.float64, device=dev)
 
     def advance(self, psi, velocity_components: List, dt: float, clip_bounds=(0.0, 1.0)):
         """psi after one RK3 step; psi's periodic image nodes are synchronised in
@@ -152,6 +168,10 @@ class FCCDLevelSetAdvection:
         st = _lib.current_stream_handle()
         _lib.check(lib.tpf_sync_periodic_images(q0.dim(), shape, per, _lib.dptr(q0), tdt, st))
         vel = [to_device(u, dtype=fccd.dtype).tensor for u in velocity_components]
+        if self._mass_correction:
+            m_old = torch.empty(2, dtype=torch.float64, device=q0.device)
+            _lib.check(lib.tpf_mass_sums(q0.numel(), _lib.dptr(q0), _lib.dptr(self._dV), _lib.dptr(self._partials),
+                                         _lib.dptr(m_old), tdt, st))
         clip = clip_bounds is not None
         lo, hi = (float(clip_bounds[0]), float(clip_bounds[1])) if clip else (0.0, 0.0)
         coeffs = ((1, 0.0, 0.0), (2, 0.75, 0.25), (3, 1.0 / 3.0, 2.0 / 3.0))
@@ -163,4 +183,155 @@ class FCCDLevelSetAdvection:
                                              _lib.dptr(q), _lib.dptr(L), 1 if clip else 0, lo, hi, _lib.dptr(nxt),
                                              tdt, st))
             q = nxt
+        if self._mass_correction:
+            sums = torch.empty(2, dtype=torch.float64, device=q.device)
+            _lib.check(lib.tpf_mass_sums(q.numel(), _lib.dptr(q), _lib.dptr(self._dV), _lib.dptr(self._partials),
+                                         _lib.dptr(sums), tdt, st))
+            out = torch.empty_like(q)
+            _lib.check(lib.tpf_mass_correction_apply(q.numel(), _lib.dptr(q), _lib.dptr(m_old), _lib.dptr(sums),
+                                                     _lib.dptr(out), tdt, st))
+            _lib.check(lib.tpf_sync_periodic_images(q.dim(), shape, per, _lib.dptr(out), tdt, st))
+            q = out
+        return v.out(q)
+
+
+_BETA2 = -1.0 / 8.0   # CCD Eq-II off-diagonal (reinit_ops.py:19)
+
+
+def _periodic_flags(bc, ndim: int):
+    """periodic_axis_flags (core/boundary.py:94-113): only axes labelled periodic."""
+    if isinstance(bc, (tuple, list)):
+        return tuple(str(v).strip().lower() == "periodic" for v in bc)
+    value = str(getattr(bc, "value", bc)).strip().lower()
+    if value in ("zero", "neumann", "outflow"):
+        return tuple(False for _ in range(ndim))
+    return tuple(a == "periodic" for a in boundary_axes(bc, ndim))
+
+
+def _pad_kind(bc, axis: int) -> int:
+    """Ghost padding of the filtered divergence (pad_ghost_cells): 1 periodic,
+    2 neumann / outflow (the end node), 0 otherwise (zeros)."""
+    label = str(bc[axis] if isinstance(bc, (tuple, list)) else bc).strip().lower()
+    return {"periodic": 1, "neumann": 2, "outflow": 2}.get(label, 0)
+
+
+def _control_widths(grid, axis: int, periodic: bool):
+    """Grid._axis_control_widths (core/grid.py:1158-1170) for a uniform grid."""
+    import numpy as np
+    coords = np.asarray(grid.coords[axis], dtype=float)
+    if periodic:
+        cw = np.diff(coords)
+        w = np.empty_like(coords)
+        w[:-1] = 0.5 * (np.roll(cw, 1) + cw)
+        w[-1] = 0.0
+        return w
+    return np.full(grid.N[axis] + 1, grid.L[axis] / grid.N[axis])
+
+
+class SplitReinitializer:
+    """Operator-split reinitialization, compression (forward Euler) + CN-ADI
+    diffusion (levelset/reinit_split.py:22-102) on uniform grids."""
+
+    def __init__(self, backend, grid, ccd, eps: float, n_steps: int = 4, bc: str = "zero",
+                 eps_d_comp: float = 0.05, mass_correction: bool = True):
+        import numpy as np
+        torch = _torch()
+        if not getattr(grid, "uniform", True):
+            raise NotImplementedError("the B200 reinitializer covers uniform grids")
+        self.xp = getattr(backend, "xp", None)
+        self.grid = grid
+        self.ccd = ccd
+        self.eps = eps
+        self.n_steps = n_steps
+        self._bc = bc
+        self._eps_d_comp = float(eps_d_comp)
+        self._mass_correction = mass_correction
+        nd = grid.ndim
+        self._h = [float(grid.L[ax] / grid.N[ax]) for ax in range(nd)]
+        # compute_dtau (reinit_ops.py:34-54)
+        dx_min = min(self._h)
+        eps_min = float(np.min(eps))
+        self.dtau = min(0.5 * dx_min ** 2 / (2.0 * nd * eps_min), 0.5 * dx_min)
+        dev = torch.device("cuda", torch.cuda.current_device())
+        self._cn = []
+        for ax in range(nd):   # build_cn_factors (reinit_ops.py:117-166), same host arithmetic
+            h = self._h[ax]
+            mu = eps * self.dtau / (2.0 * h ** 2)
+            n = grid.N[ax] + 1
+            d_L = 1.0 + 6.0 * mu
+            c_L = _BETA2 - 3.0 * mu
+            main = np.full(n, d_L)
+            sup = np.full(n - 1, c_L)
+            sub = np.full(n - 1, c_L)
+            sup[0] = 2.0 * c_L
+            sub[-1] = 2.0 * c_L
+            m = main.copy()
+            f = np.empty(n - 1)
+            for i in range(1, n):
+                f[i - 1] = sub[i - 1] / m[i - 1]
+                m[i] -= f[i - 1] * sup[i - 1]
+            mu_r = eps * self.dtau / (2.0 * h ** 2)
+            cR = _BETA2 + 3.0 * mu_r
+            dR = 1.0 - 6.0 * mu_r
+            self._cn.append((cR, dR, torch.from_numpy(f).to(dev), torch.from_numpy(m).to(dev),
+                             torch.from_numpy(sup).to(dev)))
+        self._per = _periodic_flags(bc, nd)
+        vol = _control_widths(grid, 0, self._per[0])
+        for ax in range(1, nd):
+            vol = np.expand_dims(vol, axis=ax) * _control_widths(grid, ax, self._per[ax])
+        self._dV = torch.from_numpy(np.ascontiguousarray(vol, dtype=np.float64)).to(dev)
+        self._partials = torch.empty(2048, dtype=torch.float64, device=dev)
+        self.lib = _lib.load()
+
+    def reinitialize(self, psi):
+        torch = _torch()
+        lib = self.lib
+        nd = self.grid.ndim
+        v = to_device(psi, dtype=self.ccd.dtype)
+        q = v.tensor.clone()
+        shape = (C.c_int64 * nd)(*[int(s) for s in q.shape])
+        per = (C.c_int * nd)(*[1 if f else 0 for f in self._per])
+        tdt = _lib.TPF_F64 if q.dtype == torch.float64 else _lib.TPF_F32
+        st = _lib.current_stream_handle()
+        n = q.numel()
+        _lib.check(lib.tpf_sync_periodic_images(nd, shape, per, _lib.dptr(q), tdt, st))
+        if self._mass_correction:
+            m_old = torch.empty(2, dtype=torch.float64, device=q.device)
+            _lib.check(lib.tpf_mass_sums(n, _lib.dptr(q), _lib.dptr(self._dV), _lib.dptr(self._partials),
+                                         _lib.dptr(m_old), tdt, st))
+        P = C.c_void_p * nd
+        for _ in range(self.n_steps):
+            d1 = [self.ccd.first_derivative(q, ax) for ax in range(nd)]
+            flux = [torch.empty_like(q) for _ in range(nd)]
+            _lib.check(lib.tpf_reinit_compression_flux(nd, n, _lib.dptr(q), P(*[_lib.dptr(t) for t in d1]),
+                                                       P(*[_lib.dptr(t) for t in flux]), tdt, st))
+            div = torch.empty_like(q)
+            for ax in range(nd):
+                g = self.ccd.first_derivative(flux[ax], ax)
+                _lib.check(lib.tpf_reinit_filtered_divergence_axis(nd, shape, ax, _pad_kind(self._bc, ax),
+                                                                   self._eps_d_comp, _lib.dptr(g), 1 if ax else 0,
+                                                                   _lib.dptr(div), tdt, st))
+            # q* = clip(q - dtau div, 0, 1) with the image nodes synchronised
+            q_new = torch.empty_like(q)
+            _lib.check(lib.tpf_tvd_rk3_stage(nd, shape, per, 1, 0.0, 0.0, -self.dtau, None, _lib.dptr(q),
+                                             _lib.dptr(div), 1, 0.0, 1.0, _lib.dptr(q_new), tdt, st))
+            for ax in range(nd):
+                cR, dR, f, m, sup = self._cn[ax]
+                out = torch.empty_like(q)
+                _lib.check(lib.tpf_reinit_cn_axis(nd, shape, ax, cR, dR, _lib.dptr(f), _lib.dptr(m), _lib.dptr(sup),
+                                                  _lib.dptr(q_new), _lib.dptr(out), tdt, st))
+                _lib.check(lib.tpf_sync_periodic_images(nd, shape, per, _lib.dptr(out), tdt, st))
+                q_new = out
+            q = torch.empty_like(q_new)
+            _lib.check(lib.tpf_tvd_rk3_stage(nd, shape, per, 0, 0.0, 0.0, 0.0, None, _lib.dptr(q_new), None, 1, 0.0,
+                                             1.0, _lib.dptr(q), tdt, st))
+        if self._mass_correction:
+            sums = torch.empty(2, dtype=torch.float64, device=q.device)
+            _lib.check(lib.tpf_mass_sums(n, _lib.dptr(q), _lib.dptr(self._dV), _lib.dptr(self._partials),
+                                         _lib.dptr(sums), tdt, st))
+            out = torch.empty_like(q)
+            _lib.check(lib.tpf_mass_correction_apply(n, _lib.dptr(q), _lib.dptr(m_old), _lib.dptr(sums),
+                                                     _lib.dptr(out), tdt, st))
+            _lib.check(lib.tpf_sync_periodic_images(nd, shape, per, _lib.dptr(out), tdt, st))
+            q = out
         return v.out(q)

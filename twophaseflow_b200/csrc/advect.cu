@@ -163,7 +163,8 @@ __device__ __forceinline__ int64_t image_source(const Shape3& s, int64_t i) {
 }
 
 // TVD-RK3 stage (tvd_rk3.py:26-48) with the post-stage clip and image sync
-// (fccd_advection.py:116-120): stage 1: q + dt L; stages 2, 3:
+// (fccd_advection.py:116-120): stage 0: q (clip and sync only); stage 1:
+// q + dt L; stages 2, 3:
 // a q0 + b (q + dt L); then clip to [lo, hi] (NaN kept) and the periodic
 // image nodes take their source node's value.
 template <typename T>
@@ -172,8 +173,13 @@ __global__ void rk3_stage_kernel(Shape3 s, int stage, double ca, double cb, doub
   const int64_t tot = s.n[0] * s.n[1] * s.n[2];
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t j = any_per ? image_source(s, i) : i;
-    const double up = rn_add((double)q[j], rn_mul(dt, (double)L[j]));
-    double v = (stage == 1) ? up : rn_add(rn_mul(ca, (double)q0[j]), rn_mul(cb, up));
+    double v;
+    if (stage == 0) {
+      v = (double)q[j];
+    } else {
+      const double up = rn_add((double)q[j], rn_mul(dt, (double)L[j]));
+      v = (stage == 1) ? up : rn_add(rn_mul(ca, (double)q0[j]), rn_mul(cb, up));
+    }
     v = (double)(T)v;
     if (clip) v = v < lo ? lo : (v > hi ? hi : v);
     out[i] = (T)v;
@@ -268,14 +274,14 @@ extern "C" int tpf_tvd_rk3_stage(int ndim, const int64_t* shape, const int* peri
   Shape3 s;
   const int rc = make_shape(ndim, shape, periodic, s);
   if (rc != TPF_OK) return rc;
-  TPF_CHECK_ARG(stage >= 1 && stage <= 3, "stage must be 1, 2 or 3");
-  TPF_CHECK_ARG(q && L && out && (stage == 1 || q0), "NULL argument");
+  TPF_CHECK_ARG(stage >= 0 && stage <= 3, "stage must be 0, 1, 2 or 3");
+  TPF_CHECK_ARG(q && out && (stage == 0 || L) && (stage <= 1 || q0), "NULL argument");
   TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
   int any_per = 0;
   for (int a = 0; a < ndim; ++a) any_per |= s.per[a];
   // out may equal q or L only without periodic axes (the image nodes read
   // their source nodes, which another thread may already have overwritten)
-  TPF_CHECK_ARG(!any_per || (out != q && out != L && out != q0),
+  TPF_CHECK_ARG(!any_per || (out != q && (stage == 0 || out != L) && (stage <= 1 || out != q0)),
                 "with periodic axes the stage output must not alias its inputs");
   const int64_t tot = s.n[0] * s.n[1] * s.n[2];
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -305,6 +311,314 @@ extern "C" int tpf_sync_periodic_images(int ndim, const int64_t* shape, const in
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (dtype == TPF_F64) sync_images_kernel<double><<<blocks_for(tot, 16), 256, 0, st>>>(s, static_cast<double*>(arr));
   else sync_images_kernel<float><<<blocks_for(tot, 16), 256, 0, st>>>(s, static_cast<float*>(arr));
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Split reinitialization (levelset/reinit_split.py:73-102, reinit_ops.py:54-204,
+// heaviside.py:118-149): compression flux psi(1-psi) n, its filtered CCD
+// divergence, the CN-ADI line solves and the interface-weighted mass
+// correction.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct CompArgs {
+  const void* d1[3];
+  void* flux[3];
+  const void* psi;
+  int64_t n;
+  int ndim;
+};
+
+// flux_a = psi (1 - psi) * d1_a / max(sqrt(max(|grad psi|^2, 1e-12)), 1e-6)
+// (compute_gradient_normal, reinit_ops.py:57-80, and dccd_compression_div :108-114)
+template <typename T>
+__global__ void compression_flux_kernel(CompArgs a) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
+    double g[3] = {0.0, 0.0, 0.0};
+    double gs = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      if (d < a.ndim) {
+        g[d] = (double)static_cast<const T*>(a.d1[d])[i];
+        gs = rn_add(gs, rn_mul(g[d], g[d]));
+      }
+    double sg = sqrt(gs > 1e-12 || gs != gs ? gs : 1e-12);
+    sg = (sg > 1e-6 || sg != sg) ? sg : 1e-6;
+    const double p = (double)static_cast<const T*>(a.psi)[i];
+    const double pp = rn_mul(p, rn_sub(1.0, p));
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      if (d < a.ndim) static_cast<T*>(a.flux[d])[i] = (T)rn_mul(pp, g[d] / sg);
+  }
+}
+
+// div (+)= g[c] + eps_d ((g[c+1] - 2 g[c]) + g[c-1]) along one axis, the ends
+// padded by one ghost node: 0 ('zero'), the opposite interior node
+// ('periodic': g[n-2] left, g[1] right) or the end node itself ('neumann',
+// 'outflow') (filtered_divergence, reinit_ops.py:83-105; pad_ghost_cells,
+// core/boundary.py:249-292).
+template <typename T>
+__global__ void filtered_div_kernel(int64_t outer, int64_t n, int64_t inner, int pad, double eps_d, const T* g,
+                                    int accumulate, T* div) {
+  const int64_t tot = outer * n * inner;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = (i / inner) % n;
+    const double c = (double)g[i];
+    double m, p;
+    if (k > 0) m = (double)g[i - inner];
+    else m = pad == 0 ? 0.0 : (pad == 1 ? (double)g[i + (n - 2) * inner] : c);
+    if (k < n - 1) p = (double)g[i + inner];
+    else p = pad == 0 ? 0.0 : (pad == 1 ? (double)g[i - (n - 2) * inner] : c);
+    const double v = rn_add(c, rn_mul(eps_d, rn_add(rn_sub(p, rn_mul(2.0, c)), m)));
+    div[i] = (T)(accumulate ? rn_add((double)div[i], v) : rn_add(0.0, v));
+  }
+}
+
+// CN half-step along one axis (cn_diffusion_axis, reinit_ops.py:169-204):
+// rhs = (M2 + mu B2) psi with the mirrored end rows, then the Thomas sweep
+// with the factors f, m, sup built once on the host (build_cn_factors).
+// One thread per line, consecutive threads on consecutive lines.  Both sweeps
+// fetch CN_CHUNK nodes ahead into registers before the dependent arithmetic,
+// so a line's loads overlap instead of each step waiting for one (a 2-D grid
+// has only N+1 lines, one thread each).
+constexpr int CN_CHUNK = 8;
+
+template <typename T>
+__global__ void __launch_bounds__(256) cn_line_kernel(int64_t outer, int64_t n, int64_t inner, double cR, double dR,
+                                                      const double* f, const double* m, const double* sup,
+                                                      const T* in, T* out) {
+  const int64_t lines = outer * inner;
+  const double c2 = rn_mul(2.0, cR);
+  for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < lines; l += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t o = l / inner, in_ = l - o * inner;
+    const int64_t base = o * n * inner + in_;
+    // forward: node k's rhs needs psi at k-1, k, k+1; d stored in out
+    double pm = 0.0, pc = (double)in[base];
+    double d = 0.0;
+    for (int64_t k0 = 0; k0 < n; k0 += CN_CHUNK) {
+      double nx[CN_CHUNK];   // psi at k+1 for k = k0 .. k0+CN_CHUNK-1
+#pragma unroll
+      for (int j = 0; j < CN_CHUNK; ++j) {
+        const int64_t k = k0 + j + 1;
+        nx[j] = k < n ? (double)in[base + k * inner] : 0.0;
+      }
+      double fk[CN_CHUNK];
+#pragma unroll
+      for (int j = 0; j < CN_CHUNK; ++j) {
+        const int64_t k = k0 + j;
+        fk[j] = (k >= 1 && k < n) ? f[k - 1] : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < CN_CHUNK; ++j) {
+        const int64_t k = k0 + j;
+        if (k >= n) break;
+        const double pn = nx[j];
+        double r;
+        if (k == 0) r = rn_add(rn_mul(dR, pc), rn_mul(c2, pn));
+        else if (k < n - 1) r = rn_add(rn_add(rn_mul(cR, pm), rn_mul(dR, pc)), rn_mul(cR, pn));
+        else r = rn_add(rn_mul(c2, pm), rn_mul(dR, pc));
+        d = (k == 0) ? r : rn_sub(r, rn_mul(fk[j], d));
+        out[base + k * inner] = (T)d;
+        pm = pc;
+        pc = pn;
+      }
+    }
+    // back substitution from node n-1 down, CN_CHUNK stored d values at a time
+    double x = d / m[n - 1];
+    out[base + (n - 1) * inner] = (T)x;
+    for (int64_t k1 = n - 2; k1 >= 0; k1 -= CN_CHUNK) {
+      double dk[CN_CHUNK], sk[CN_CHUNK], mk[CN_CHUNK];
+#pragma unroll
+      for (int j = 0; j < CN_CHUNK; ++j) {
+        const int64_t k = k1 - j;
+        dk[j] = k >= 0 ? (double)out[base + k * inner] : 0.0;
+        sk[j] = k >= 0 ? sup[k] : 0.0;
+        mk[j] = k >= 0 ? m[k] : 1.0;
+      }
+#pragma unroll
+      for (int j = 0; j < CN_CHUNK; ++j) {
+        const int64_t k = k1 - j;
+        if (k < 0) break;
+        x = rn_sub(dk[j], rn_mul(sk[j], x)) / mk[j];
+        out[base + k * inner] = (T)x;
+      }
+    }
+  }
+}
+
+constexpr int MASS_BLOCKS = 1024;
+
+// per-block partial sums of q dV and 4 q (1 - q) dV in a fixed order
+template <typename T>
+__global__ void mass_partials_kernel(int64_t n, const T* q, const double* dV, double* part) {
+  __shared__ double s0[256], s1[256];
+  double a0 = 0.0, a1 = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double qi = (double)q[i], dv = dV[i];
+    a0 = rn_add(a0, rn_mul(qi, dv));
+    a1 = rn_add(a1, rn_mul(rn_mul(rn_mul(4.0, qi), rn_sub(1.0, qi)), dv));
+  }
+  s0[threadIdx.x] = a0;
+  s1[threadIdx.x] = a1;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      s0[threadIdx.x] = rn_add(s0[threadIdx.x], s0[threadIdx.x + w]);
+      s1[threadIdx.x] = rn_add(s1[threadIdx.x], s1[threadIdx.x + w]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = s0[0];
+    part[MASS_BLOCKS + blockIdx.x] = s1[0];
+  }
+}
+
+// sums[0] = sum q dV, sums[1] = sum w dV from the partials (one block, fixed order)
+__global__ void mass_finish_kernel(int nb, const double* part, double* sums) {
+  __shared__ double s0[256], s1[256];
+  double a0 = 0.0, a1 = 0.0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+    a0 = rn_add(a0, part[i]);
+    a1 = rn_add(a1, part[MASS_BLOCKS + i]);
+  }
+  s0[threadIdx.x] = a0;
+  s1[threadIdx.x] = a1;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      s0[threadIdx.x] = rn_add(s0[threadIdx.x], s0[threadIdx.x + w]);
+      s1[threadIdx.x] = rn_add(s1[threadIdx.x], s1[threadIdx.x + w]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    sums[0] = s0[0];
+    sums[1] = s1[0];
+  }
+}
+
+// q <- clip(q + gate (M_target - M_new) / W_safe * w, 0, 1) (apply_mass_correction)
+template <typename T>
+__global__ void mass_apply_kernel(int64_t n, const T* q, const double* target, const double* sums, T* out) {
+  const double W = sums[1];
+  const double Ws = W > 1e-12 ? W : 1.0;
+  const double ratio = rn_sub(target[0], sums[0]) / Ws;
+  const double gr = rn_mul(W > 1e-12 ? 1.0 : 0.0, ratio);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double qi = (double)q[i];
+    const double w = rn_mul(rn_mul(4.0, qi), rn_sub(1.0, qi));
+    double v = rn_add(qi, rn_mul(gr, w));
+    v = (double)(T)v;
+    v = v < 0.0 ? 0.0 : (v > 1.0 ? 1.0 : v);
+    out[i] = (T)v;
+  }
+}
+
+}  // namespace
+
+extern "C" int tpf_reinit_compression_flux(int ndim, int64_t n, const void* psi, const void* const* d1,
+                                           void* const* flux, int dtype, void* stream) {
+  TPF_CHECK_ARG(ndim >= 1 && ndim <= 3 && n >= 0 && psi && d1 && flux, "invalid arguments");
+  TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
+  CompArgs a{};
+  a.psi = psi; a.n = n; a.ndim = ndim;
+  for (int d = 0; d < ndim; ++d) {
+    TPF_CHECK_ARG(d1[d] && flux[d], "NULL derivative or flux %d", d);
+    a.d1[d] = d1[d];
+    a.flux[d] = flux[d];
+  }
+  if (n == 0) return TPF_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (dtype == TPF_F64) compression_flux_kernel<double><<<blocks_for(n, 16), 256, 0, st>>>(a);
+  else compression_flux_kernel<float><<<blocks_for(n, 16), 256, 0, st>>>(a);
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
+extern "C" int tpf_reinit_filtered_divergence_axis(int ndim, const int64_t* shape, int axis, int pad, double eps_d,
+                                                   const void* g, int accumulate, void* div, int dtype,
+                                                   void* stream) {
+  TPF_CHECK_ARG(ndim >= 1 && ndim <= 3 && shape && axis >= 0 && axis < ndim, "invalid shape or axis");
+  TPF_CHECK_ARG(pad >= 0 && pad <= 2, "pad must be 0 (zero), 1 (periodic) or 2 (neumann/outflow)");
+  TPF_CHECK_ARG(g && div && g != div, "NULL or aliased argument");
+  TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
+  int64_t outer = 1, inner = 1;
+  for (int d = 0; d < ndim; ++d) {
+    TPF_CHECK_ARG(shape[d] >= 1, "empty axis");
+    if (d < axis) outer *= shape[d];
+    if (d > axis) inner *= shape[d];
+  }
+  const int64_t n = shape[axis];
+  TPF_CHECK_ARG(n >= 3, "at least 3 nodes along the axis");
+  const int64_t tot = outer * n * inner;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (dtype == TPF_F64)
+    filtered_div_kernel<double><<<blocks_for(tot, 16), 256, 0, st>>>(outer, n, inner, pad, eps_d,
+                                                                    static_cast<const double*>(g), accumulate,
+                                                                    static_cast<double*>(div));
+  else
+    filtered_div_kernel<float><<<blocks_for(tot, 16), 256, 0, st>>>(outer, n, inner, pad, eps_d,
+                                                                   static_cast<const float*>(g), accumulate,
+                                                                   static_cast<float*>(div));
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
+extern "C" int tpf_reinit_cn_axis(int ndim, const int64_t* shape, int axis, double cR, double dR, const double* f,
+                                  const double* m, const double* sup, const void* in, void* out, int dtype,
+                                  void* stream) {
+  TPF_CHECK_ARG(ndim >= 1 && ndim <= 3 && shape && axis >= 0 && axis < ndim, "invalid shape or axis");
+  TPF_CHECK_ARG(f && m && sup && in && out && in != out, "NULL or aliased argument");
+  TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
+  int64_t outer = 1, inner = 1;
+  for (int d = 0; d < ndim; ++d) {
+    TPF_CHECK_ARG(shape[d] >= 1, "empty axis");
+    if (d < axis) outer *= shape[d];
+    if (d > axis) inner *= shape[d];
+  }
+  const int64_t n = shape[axis];
+  TPF_CHECK_ARG(n >= 2, "at least 2 nodes along the axis");
+  const int64_t lines = outer * inner;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (dtype == TPF_F64)
+    cn_line_kernel<double><<<blocks_for(lines, 8), 256, 0, st>>>(outer, n, inner, cR, dR, f, m, sup,
+                                                                 static_cast<const double*>(in),
+                                                                 static_cast<double*>(out));
+  else
+    cn_line_kernel<float><<<blocks_for(lines, 8), 256, 0, st>>>(outer, n, inner, cR, dR, f, m, sup,
+                                                                static_cast<const float*>(in),
+                                                                static_cast<float*>(out));
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
+extern "C" int tpf_mass_sums(int64_t n, const void* q, const double* dV, double* partials, double* sums, int dtype,
+                             void* stream) {
+  TPF_CHECK_ARG(n >= 1 && q && dV && partials && sums, "invalid arguments");
+  TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int nb = (int)std::min<int64_t>(MASS_BLOCKS, (n + 255) / 256);
+  if (dtype == TPF_F64) mass_partials_kernel<double><<<nb, 256, 0, st>>>(n, static_cast<const double*>(q), dV, partials);
+  else mass_partials_kernel<float><<<nb, 256, 0, st>>>(n, static_cast<const float*>(q), dV, partials);
+  mass_finish_kernel<<<1, 256, 0, st>>>(nb, partials, sums);
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
+extern "C" int tpf_mass_correction_apply(int64_t n, const void* q, const double* target, const double* sums,
+                                         void* out, int dtype, void* stream) {
+  TPF_CHECK_ARG(n >= 1 && q && target && sums && out, "invalid arguments");
+  TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (dtype == TPF_F64)
+    mass_apply_kernel<double><<<blocks_for(n, 16), 256, 0, st>>>(n, static_cast<const double*>(q), target, sums,
+                                                                 static_cast<double*>(out));
+  else
+    mass_apply_kernel<float><<<blocks_for(n, 16), 256, 0, st>>>(n, static_cast<const float*>(q), target, sums,
+                                                                static_cast<float*>(out));
   TPF_CUDA_TRY(cudaGetLastError());
   return TPF_OK;
 }

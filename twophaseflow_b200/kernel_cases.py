@@ -9,6 +9,7 @@
     python -m twophaseflow_b200.kernel_cases curvature --N 256 256 256 --bc wall [--reps 3]
     python -m twophaseflow_b200.kernel_cases rhiechow --N 256 256 256 --bc wall [--reps 3]
     python -m twophaseflow_b200.kernel_cases advect --N 256 256 256 --bc periodic [--reps 3]
+    python -m twophaseflow_b200.kernel_cases reinit --N 256 256 256 [--reps 2]
 
 ``ccd`` captures ``reps`` CCDSolver.differentiate calls in one CUDA graph and
 replays it, so the reported time is device time per call (no Python launch
@@ -247,6 +248,45 @@ def advect_case(N, bc, dtype, reps):
             "flux_kernel": axes}
 
 
+def reinit_case(N, dtype, reps):
+    """SplitReinitializer.reinitialize (4 pseudo-steps, zero padding, mass
+    correction) on a noisy sphere, and its CN line-solve kernel alone per axis,
+    graph-replayed."""
+    import ctypes as C
+    import torch
+    from . import CCDSolver, SplitReinitializer, UniformGrid, _lib
+    dt_ = torch.float64 if dtype == "f64" else torch.float32
+    nd = len(N)
+    ax = [torch.linspace(0.0, 1.0, n + 1, dtype=torch.float64, device="cuda") for n in N]
+    X = torch.meshgrid(*ax, indexing="ij")
+    r = torch.sqrt(sum((X[a] - 0.5) ** 2 for a in range(nd)))
+    h = 1.0 / max(N)
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    psi = torch.sigmoid((0.25 - r) / (2.5 * h)) + 0.02 * torch.randn(r.shape, device="cuda", dtype=torch.float64,
+                                                                      generator=gen)
+    psi = psi.clamp(0.0, 1.0).to(dt_).contiguous()
+    del X, r
+    grid = UniformGrid(N)
+    rein = SplitReinitializer(None, grid, CCDSolver(grid, None, bc_type="wall", dtype=dt_), 1.5 * h)
+    ms = _graph_time(lambda: rein.reinitialize(psi), reps)
+    out = torch.empty_like(psi)
+    sh = (C.c_int64 * nd)(*[n + 1 for n in N])
+    lib = _lib.load()
+    tdt = _lib.TPF_F64 if dt_ == torch.float64 else _lib.TPF_F32
+    nbytes = 3 * psi.numel() * psi.element_size()      # read in; write d, read d, write x (d kept in out)
+    axes = []
+    for a in range(nd):
+        cR, dR, f, m, sup = rein._cn[a]
+
+        def kern(a=a, cR=cR, dR=dR, f=f, m=m, sup=sup):
+            _lib.check(lib.tpf_reinit_cn_axis(nd, sh, a, cR, dR, _lib.dptr(f), _lib.dptr(m), _lib.dptr(sup),
+                                              _lib.dptr(psi), _lib.dptr(out), tdt, _lib.current_stream_handle()))
+        ms_k = _graph_time(kern, reps)
+        axes.append({"axis": a, "us": round(ms_k * 1e3, 1), "GBps_min_traffic": round(nbytes / (ms_k * 1e-3) / 1e9, 1)})
+    return {"case": "reinit", "N": list(N), "dtype": dtype, "n_steps": rein.n_steps,
+            "us_per_reinitialize": round(ms * 1e3, 1), "cn_kernel": axes}
+
+
 def ppe_case(N, precision, reps, tol=1e-8):
     import torch
     from . import PPESolverFVMMatrixFree, UniformGrid
@@ -414,7 +454,7 @@ def gmres_case(N, line, reps, maxiter=None, tol=1e-8):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["ccd", "ppe", "learned", "batched", "gmres", "corrector", "curvature", "rhiechow", "advect"])
+    ap.add_argument("case", choices=["ccd", "ppe", "learned", "batched", "gmres", "corrector", "curvature", "rhiechow", "advect", "reinit"])
     ap.add_argument("--line", default="thomas", choices=["thomas", "pcr"], help="gmres: line solver")
     ap.add_argument("--N", type=int, nargs="+", required=True)
     ap.add_argument("--axis", type=int, default=0)
@@ -441,6 +481,8 @@ def main(argv=None):
         r = rhiechow_case(tuple(a.N), a.bc, a.dtype, a.reps)
     elif a.case == "advect":
         r = advect_case(tuple(a.N), a.bc, a.dtype, a.reps)
+    elif a.case == "reinit":
+        r = reinit_case(tuple(a.N), a.dtype, a.reps)
     else:
         r = batched_case(n_cases=a.N[0], reps=a.reps)
     print(json.dumps(r), flush=True)
