@@ -405,6 +405,8 @@ def main(argv=None):
     from twophaseflow_b200.kernel_cases import advect_case, reinit_case
     advb = advect_case((256, 256, 256), "periodic", "f64", 2)
     reib = reinit_case((256, 256, 256), "f64", 2)
+    from twophaseflow_b200.kernel_cases import viscous_case
+    visb = viscous_case((256, 256, 256), "f64", 2)
 
     # many independent cases in one persistent launch (32 seeded grids, 128..512 per axis)
     from twophaseflow_b200.kernel_cases import batched_case
@@ -453,6 +455,7 @@ def main(argv=None):
             "rhiechow_257cubed_f64_wall": {k: v for k, v in rcb.items() if k not in ("case", "N", "bc", "dtype")},
             "cls_transport_257cubed_f64_periodic": {k: v for k, v in advb.items() if k not in ("case", "N", "bc", "dtype")},
             "reinit_257cubed_f64": {k: v for k, v in reib.items() if k not in ("case", "N", "dtype")},
+            "viscous_257cubed_f64_wall": {k: v for k, v in visb.items() if k not in ("case", "N", "dtype")},
             "ccd_roofline": {"kernel": "ccd_lane_kernel (3-D 257^3 FP64, mean over axes and wall/periodic)",
                              "bound": "hbm", "achieved": round(ccd3_gbps, 1), "peak": peak, "unit": "GB/s",
                              "frac": round(ccd3_gbps / peak, 3),

@@ -238,6 +238,27 @@ int tpf_mass_sums(int64_t n, const void* q, const double* dV, double* partials, 
 int tpf_mass_correction_apply(int64_t n, const void* q, const double* target, const double* sums, void* out,
                               int dtype, void* stream);
 
+/* ---- Viscous stress divergence (src/twophase/ns_terms/viscous_spatial.py:28-153) */
+
+/* total (+)= D_lo(v) along one axis, v = mu (a + b) (mu and b given) or a
+ * (mu, b NULL), D_lo = _low_order_derivative (viscous_spatial.py:70-104):
+ * (v_1 - v_0)/dx0 and (v_{n-1} - v_{n-2})/dxl at the ends,
+ * cl[k-1] v_{k-1} + cc[k-1] v_k + cr[k-1] v_{k+1} inside (coefficients per
+ * interior node, FP64 device arrays of n-2, as the reference forms them from
+ * the node coordinates).  finalize = 1 then divides by Re rho (the last axis).
+ * accumulate = 0 writes 0 + it.  total must not alias an operand. */
+int tpf_visc_lowfd_axis(int ndim, const int64_t* shape, int axis, const double* cl, const double* cc,
+                        const double* cr, double dx0, double dxl, const void* a, const void* b, const void* mu,
+                        int accumulate, int finalize, const void* rho, double re, void* total, int dtype,
+                        void* stream);
+
+/* out = mu (a + b), n values (the stress of the legacy CCD scheme). */
+int tpf_visc_stress(int64_t n, const void* mu, const void* a, const void* b, void* out, int dtype, void* stream);
+
+/* total (+)= g, then (finalize) total / (Re rho). */
+int tpf_visc_accumulate(int64_t n, const void* g, int accumulate, int finalize, const void* rho, double re,
+                        void* total, int dtype, void* stream);
+
 /* Zero grad at index 0 and n_pts-1 along the axis of a [outer, n, inner]
  * array (wall axes only; no-op for periodic plans).  Replaces
  * CCDSolver.enforce_wall_neumann (ccd_solver.py:264-281;

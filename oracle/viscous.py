@@ -1,0 +1,57 @@
+"""CPU restatement of the viscous stress divergence (TEST INFRASTRUCTURE: the
+oracle): ViscousSpatialEvaluator.evaluate for psi = None (reference
+``src/twophase/ns_terms/viscous_spatial.py:28-153``) on the oracle's CCD.
+
+Pinned against the reference's own outputs in ``tests/golden/viscous_golden.npz``.
+Only tests, smoke() and bench.py's CPU-baseline leg may use this module.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from . import ccd as occd
+from .levelset import axis_kinds
+
+
+def low_order_derivative(arr, axis: int, coords):
+    """_low_order_derivative (viscous_spatial.py:70-104)."""
+    arr = np.asarray(arr)
+    dx = coords[1:] - coords[:-1]
+    d = np.empty_like(arr)
+    n = arr.shape[axis]
+    a = np.moveaxis(arr, axis, 0)
+    o = np.moveaxis(d, axis, 0)
+    o[0] = (a[1] - a[0]) / dx[0]
+    o[n - 1] = (a[n - 1] - a[n - 2]) / dx[-1]
+    shape = [1] * arr.ndim
+    shape[0] = n - 2
+    h_l = dx[:-1].reshape(shape)
+    h_r = dx[1:].reshape(shape)
+    o[1:n - 1] = (-(h_r / (h_l * (h_l + h_r))) * a[:n - 2] + ((h_r - h_l) / (h_l * h_r)) * a[1:n - 1]
+                  + (h_l / (h_r * (h_l + h_r))) * a[2:])
+    return d
+
+
+def viscous(vel, mu, rho, Re: float, L, N, bc: str, scheme: str = "ccd_bulk"):
+    nd = len(vel)
+    kinds = axis_kinds(bc, nd)
+    coords = [np.linspace(0.0, L[a], N[a] + 1) for a in range(nd)]
+    h = [float(L[a] / N[a]) for a in range(nd)]
+    D = lambda f, ax: np.asarray(occd.differentiate(f, ax, h[ax], bc=kinds[ax])[0])
+    lo = lambda f, ax: low_order_derivative(f, ax, coords[ax])
+    out = []
+    for al in range(nd):
+        total = np.zeros_like(vel[al])
+        for be in range(nd):
+            if scheme == "conservative_stress":
+                a, b = lo(vel[al], be), lo(vel[be], al)
+                total += lo(mu * (a + b), be)
+            elif scheme == "ccd_stress_legacy":
+                a, b = D(vel[al], be), D(vel[be], al)
+                total += D(mu * (a + b), be)
+            else:
+                a, b = D(vel[al], be), D(vel[be], al)
+                total += lo(mu * (a + b), be)
+        out.append(total / (Re * rho))
+    return out

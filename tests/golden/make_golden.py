@@ -483,13 +483,45 @@ def make_reinit(out):
         out[f"{name}/psi_reinit"] = np.asarray(r.reinitialize(psi.copy()))
 
 
+def make_viscous(out):
+    """ViscousTerm.compute_explicit of the reference in its three spatial schemes."""
+    from twophase.backend import Backend
+    from twophase.config import GridConfig
+    from twophase.core.grid import Grid
+    from twophase.ccd.ccd_solver import CCDSolver
+    from twophase.ns_terms.viscous import ViscousTerm
+
+    be = Backend(use_gpu=False)
+    rng = np.random.default_rng(2718)
+    cases = [("wall2d", (18, 14), (1.0, 0.7), "wall"), ("per2d", (16, 12), (1.0, 1.0), "periodic"),
+             ("wall3d", (8, 10, 6), (1.0, 1.2, 0.8), "wall")]
+    for name, N, L, bc in cases:
+        grid = Grid(GridConfig(ndim=len(N), N=N, L=L), be)
+        ccd = CCDSolver(grid, be, bc_type=bc)
+        vel = [rng.standard_normal(grid.shape) for _ in N]
+        mu = 0.01 + rng.uniform(0.0, 1.0, grid.shape)
+        rho = 0.001 + rng.uniform(0.0, 1.0, grid.shape)
+        out[f"{name}/N"] = np.array(N)
+        out[f"{name}/L"] = np.array(L, dtype=np.float64)
+        out[f"{name}/bc"] = np.array(bc)
+        out[f"{name}/mu"] = mu
+        out[f"{name}/rho"] = rho
+        for a in range(len(N)):
+            out[f"{name}/u{a}"] = vel[a]
+        for scheme in ("ccd_bulk", "conservative_stress", "ccd_stress_legacy"):
+            v = ViscousTerm(be, 100.0, spatial_scheme=scheme).compute_explicit(vel, mu, rho, ccd)
+            for a in range(len(N)):
+                out[f"{name}/{scheme}/v{a}"] = np.asarray(v[a])
+
+
 def main():
-    """Usage: make_golden.py [reference src dir] [only: ccd|ppe|step|levelset|rhiechow|advect|reinit ...]."""
+    """Usage: make_golden.py [reference src dir] [only: ccd|ppe|step|levelset|rhiechow|advect|reinit|viscous ...]."""
     src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
     only = set(sys.argv[2:])
     _ref_import(src)
     makers = {"ccd": make_ccd, "ppe": make_ppe, "step": make_step, "levelset": make_levelset,
-              "rhiechow": make_rhiechow, "advect": make_advect, "reinit": make_reinit}
+              "rhiechow": make_rhiechow, "advect": make_advect, "reinit": make_reinit,
+              "viscous": make_viscous}
     for key, fn in makers.items():
         if only and key not in only:
             continue

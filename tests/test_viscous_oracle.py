@@ -1,0 +1,29 @@
+"""The viscous-stress oracle against the reference's own outputs
+(tests/golden/viscous_golden.npz, written by tests/golden/make_golden.py)."""
+
+import os
+
+import numpy as np
+import pytest
+
+from oracle import viscous as ov
+
+G = np.load(os.path.join(os.path.dirname(__file__), "golden", "viscous_golden.npz"))
+SCHEMES = ["ccd_bulk", "conservative_stress", "ccd_stress_legacy"]
+
+
+@pytest.mark.parametrize("name", ["wall2d", "per2d", "wall3d"])
+@pytest.mark.parametrize("scheme", SCHEMES)
+def test_viscous_matches_reference(name, scheme):
+    N, L, bc = G[f"{name}/N"], G[f"{name}/L"], str(G[f"{name}/bc"])
+    vel = [G[f"{name}/u{a}"] for a in range(len(N))]
+    v = ov.viscous(vel, G[f"{name}/mu"], G[f"{name}/rho"], 100.0, L, N, bc, scheme)
+    for a in range(len(N)):
+        np.testing.assert_array_equal(v[a], G[f"{name}/{scheme}/v{a}"])
+
+
+def test_low_order_derivative_exact_on_quadratics():
+    """The three-point stencil differentiates x^2 exactly on a uniform grid."""
+    x = np.linspace(0.0, 1.0, 33)
+    d = ov.low_order_derivative(x ** 2, 0, x)
+    assert np.abs(d[1:-1] - 2.0 * x[1:-1]).max() < 1e-12

@@ -1,0 +1,148 @@
+// Viscous stress divergence V_a = (1/Re) sum_b d/dx_b [mu (du_a/dx_b + du_b/dx_a)] / rho
+// (ViscousSpatialEvaluator, src/twophase/ns_terms/viscous_spatial.py:28-153).
+// The CCD first derivatives come from the CCD line kernels; this file holds
+// the three-point low-order derivative of the stress (with the stress formed
+// on the fly from mu and the two derivatives), the accumulation over b and
+// the final division by Re rho.  Explicit round-to-nearest operations in the
+// reference's NumPy order.
+#include "tpf_common.cuh"
+
+#include <algorithm>
+
+namespace {
+
+__device__ __forceinline__ double rn_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double rn_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double rn_mul(double a, double b) { return __dmul_rn(a, b); }
+
+inline int blocks_for(int64_t n) {
+  return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)tpf::sm_count() * 16));
+}
+
+struct LowArgs {
+  const void *a, *b, *mu;         // value = mu (a + b), or a when mu is NULL (b NULL: a alone)
+  const double *cl, *cc, *cr;     // interior coefficients per node along the axis (index k-1)
+  double dx0, dxl;                // first and last cell widths
+  void* total;
+  const void* rho;
+  double re;
+  int64_t outer, n, inner;
+  int accumulate, finalize;
+};
+
+template <typename T>
+__device__ __forceinline__ double val(const LowArgs& a, int64_t i) {
+  const double x = (double)static_cast<const T*>(a.a)[i];
+  if (!a.mu) return x;
+  const double y = a.b ? (double)static_cast<const T*>(a.b)[i] : 0.0;
+  return rn_mul((double)static_cast<const T*>(a.mu)[i], a.b ? rn_add(x, y) : x);
+}
+
+// _low_order_derivative (viscous_spatial.py:70-104): one-sided first
+// differences / dx at the ends, the three-point non-uniform stencil inside;
+// then total (+)= it and, on the last axis, total / (Re rho).
+template <typename T>
+__global__ void lowfd_kernel(LowArgs a) {
+  const int64_t tot = a.outer * a.n * a.inner;
+  const int64_t s = a.inner, n = a.n;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = (i / s) % n;
+    double d;
+    if (k == 0) {
+      d = rn_sub(val<T>(a, i + s), val<T>(a, i)) / a.dx0;
+    } else if (k == n - 1) {
+      d = rn_sub(val<T>(a, i), val<T>(a, i - s)) / a.dxl;
+    } else {
+      const double fl = val<T>(a, i - s), fc = val<T>(a, i), fr = val<T>(a, i + s);
+      d = rn_add(rn_add(rn_mul(a.cl[k - 1], fl), rn_mul(a.cc[k - 1], fc)), rn_mul(a.cr[k - 1], fr));
+    }
+    T* tot_p = static_cast<T*>(a.total);
+    double t = a.accumulate ? rn_add((double)tot_p[i], d) : rn_add(0.0, d);
+    if (a.finalize) t = t / rn_mul(a.re, (double)static_cast<const T*>(a.rho)[i]);
+    tot_p[i] = (T)t;
+  }
+}
+
+// stress = mu (a + b)  (the CCD-differentiated stress of the legacy scheme)
+template <typename T>
+__global__ void stress_kernel(int64_t n, const T* mu, const T* a, const T* b, T* out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (T)rn_mul((double)mu[i], rn_add((double)a[i], (double)b[i]));
+}
+
+// total (+)= g, then (finalize) total / (Re rho)
+template <typename T>
+__global__ void accumulate_kernel(int64_t n, const T* g, int accumulate, int finalize, const T* rho, double re,
+                                  T* total) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double t = accumulate ? rn_add((double)total[i], (double)g[i]) : rn_add(0.0, (double)g[i]);
+    if (finalize) t = t / rn_mul(re, (double)rho[i]);
+    total[i] = (T)t;
+  }
+}
+
+}  // namespace
+
+extern "C" int tpf_visc_lowfd_axis(int ndim, const int64_t* shape, int axis, const double* cl, const double* cc,
+                                   const double* cr, double dx0, double dxl, const void* a, const void* b,
+                                   const void* mu, int accumulate, int finalize, const void* rho, double re,
+                                   void* total, int dtype, void* stream) {
+  TPF_CHECK_ARG(ndim >= 1 && ndim <= 3 && shape && axis >= 0 && axis < ndim, "invalid shape or axis");
+  TPF_CHECK_ARG(a && total && cl && cc && cr, "NULL argument");
+  TPF_CHECK_ARG(total != a && total != b && total != mu, "total must not alias an operand");
+  TPF_CHECK_ARG(!b || mu, "b is only used inside mu (a + b)");
+  TPF_CHECK_ARG(!finalize || (rho && re != 0.0), "finalize needs rho and a nonzero Re");
+  TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
+  LowArgs A{};
+  A.a = a; A.b = b; A.mu = mu; A.cl = cl; A.cc = cc; A.cr = cr; A.dx0 = dx0; A.dxl = dxl;
+  A.total = total; A.rho = rho; A.re = re; A.accumulate = accumulate ? 1 : 0; A.finalize = finalize ? 1 : 0;
+  A.outer = 1; A.inner = 1;
+  for (int d = 0; d < ndim; ++d) {
+    TPF_CHECK_ARG(shape[d] >= 1, "empty axis");
+    if (d < axis) A.outer *= shape[d];
+    if (d > axis) A.inner *= shape[d];
+  }
+  A.n = shape[axis];
+  TPF_CHECK_ARG(A.n >= 3, "at least 3 nodes along the axis");
+  const int64_t tot = A.outer * A.n * A.inner;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (dtype == TPF_F64) lowfd_kernel<double><<<blocks_for(tot), 256, 0, st>>>(A);
+  else lowfd_kernel<float><<<blocks_for(tot), 256, 0, st>>>(A);
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
+extern "C" int tpf_visc_stress(int64_t n, const void* mu, const void* a, const void* b, void* out, int dtype,
+                               void* stream) {
+  TPF_CHECK_ARG(n >= 0 && mu && a && b && out, "NULL argument");
+  TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
+  if (n == 0) return TPF_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (dtype == TPF_F64)
+    stress_kernel<double><<<blocks_for(n), 256, 0, st>>>(n, static_cast<const double*>(mu), static_cast<const double*>(a),
+                                                         static_cast<const double*>(b), static_cast<double*>(out));
+  else
+    stress_kernel<float><<<blocks_for(n), 256, 0, st>>>(n, static_cast<const float*>(mu), static_cast<const float*>(a),
+                                                        static_cast<const float*>(b), static_cast<float*>(out));
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
+extern "C" int tpf_visc_accumulate(int64_t n, const void* g, int accumulate, int finalize, const void* rho, double re,
+                                   void* total, int dtype, void* stream) {
+  TPF_CHECK_ARG(n >= 0 && g && total && g != total, "NULL or aliased argument");
+  TPF_CHECK_ARG(!finalize || (rho && re != 0.0), "finalize needs rho and a nonzero Re");
+  TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
+  if (n == 0) return TPF_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (dtype == TPF_F64)
+    accumulate_kernel<double><<<blocks_for(n), 256, 0, st>>>(n, static_cast<const double*>(g), accumulate, finalize,
+                                                             static_cast<const double*>(rho), re,
+                                                             static_cast<double*>(total));
+  else
+    accumulate_kernel<float><<<blocks_for(n), 256, 0, st>>>(n, static_cast<const float*>(g), accumulate, finalize,
+                                                            static_cast<const float*>(rho), re,
+                                                            static_cast<float*>(total));
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}

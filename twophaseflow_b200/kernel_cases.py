@@ -10,6 +10,7 @@
     python -m twophaseflow_b200.kernel_cases rhiechow --N 256 256 256 --bc wall [--reps 3]
     python -m twophaseflow_b200.kernel_cases advect --N 256 256 256 --bc periodic [--reps 3]
     python -m twophaseflow_b200.kernel_cases reinit --N 256 256 256 [--reps 2]
+    python -m twophaseflow_b200.kernel_cases viscous --N 256 256 256 [--reps 2]
 
 ``ccd`` captures ``reps`` CCDSolver.differentiate calls in one CUDA graph and
 replays it, so the reported time is device time per call (no Python launch
@@ -287,6 +288,45 @@ def reinit_case(N, dtype, reps):
             "us_per_reinitialize": round(ms * 1e3, 1), "cn_kernel": axes}
 
 
+def viscous_case(N, dtype, reps):
+    """ViscousTerm.compute_explicit (ccd_bulk: CCD velocity derivatives, the
+    low-order stress derivative kernel) on random fields, graph-replayed, and
+    the low-order kernel alone per axis."""
+    import ctypes as C
+    import torch
+    from . import CCDSolver, UniformGrid, ViscousTerm, _lib
+    dt_ = torch.float64 if dtype == "f64" else torch.float32
+    nd = len(N)
+    shape = tuple(n + 1 for n in N)
+    gen = torch.Generator(device="cuda").manual_seed(9)
+    mk = lambda: torch.randn(shape, device="cuda", dtype=dt_, generator=gen)
+    vel = [mk() for _ in N]
+    mu = 0.01 + torch.rand(shape, device="cuda", dtype=dt_, generator=gen)
+    rho = 0.001 + torch.rand(shape, device="cuda", dtype=dt_, generator=gen)
+    grid = UniformGrid(N)
+    ccd = CCDSolver(grid, None, bc_type="wall", dtype=dt_)
+    vt = ViscousTerm(None, 100.0)
+    ms = _graph_time(lambda: vt.compute_explicit(vel, mu, rho, ccd), reps)
+    a, b = mk(), mk()
+    total = torch.empty_like(a)
+    sh = (C.c_int64 * nd)(*shape)
+    lib = _lib.load()
+    tdt = _lib.TPF_F64 if dt_ == torch.float64 else _lib.TPF_F32
+    nbytes = 5 * a.numel() * a.element_size()     # read a, b, mu, total; write total
+    axes = []
+    for ax in range(nd):
+        (cl, cc, cr), dx0, dxl = vt._coefficients(grid, ax)
+
+        def kern(ax=ax, cl=cl, cc=cc, cr=cr, dx0=dx0, dxl=dxl):
+            _lib.check(lib.tpf_visc_lowfd_axis(nd, sh, ax, _lib.dptr(cl), _lib.dptr(cc), _lib.dptr(cr), dx0, dxl,
+                                               _lib.dptr(a), _lib.dptr(b), _lib.dptr(mu), 1, 0, _lib.dptr(rho),
+                                               100.0, _lib.dptr(total), tdt, _lib.current_stream_handle()))
+        ms_k = _graph_time(kern, reps)
+        axes.append({"axis": ax, "us": round(ms_k * 1e3, 1), "GBps": round(nbytes / (ms_k * 1e-3) / 1e9, 1)})
+    return {"case": "viscous", "N": list(N), "dtype": dtype, "scheme": vt.spatial_scheme,
+            "us_per_compute": round(ms * 1e3, 1), "lowfd_kernel": axes}
+
+
 def ppe_case(N, precision, reps, tol=1e-8):
     import torch
     from . import PPESolverFVMMatrixFree, UniformGrid
@@ -454,7 +494,7 @@ def gmres_case(N, line, reps, maxiter=None, tol=1e-8):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["ccd", "ppe", "learned", "batched", "gmres", "corrector", "curvature", "rhiechow", "advect", "reinit"])
+    ap.add_argument("case", choices=["ccd", "ppe", "learned", "batched", "gmres", "corrector", "curvature", "rhiechow", "advect", "reinit", "viscous"])
     ap.add_argument("--line", default="thomas", choices=["thomas", "pcr"], help="gmres: line solver")
     ap.add_argument("--N", type=int, nargs="+", required=True)
     ap.add_argument("--axis", type=int, default=0)
@@ -483,6 +523,8 @@ def main(argv=None):
         r = advect_case(tuple(a.N), a.bc, a.dtype, a.reps)
     elif a.case == "reinit":
         r = reinit_case(tuple(a.N), a.dtype, a.reps)
+    elif a.case == "viscous":
+        r = viscous_case(tuple(a.N), a.dtype, a.reps)
     else:
         r = batched_case(n_cases=a.N[0], reps=a.reps)
     print(json.dumps(r), flush=True)

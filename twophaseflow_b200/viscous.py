@@ -1,0 +1,141 @@
+"""Viscous stress divergence on the GPU with the reference's class and
+signature: ``ViscousTerm(backend, Re, cn_viscous=True,
+spatial_scheme="ccd_bulk").compute_explicit(velocity_components, mu, rho, ccd)``
+returns V_a = (1/Re) sum_b d/dx_b [mu (du_a/dx_b + du_b/dx_a)] / rho
+(src/twophase/ns_terms/viscous.py:50-133, viscous_spatial.py:28-153) for the
+three spatial schemes:
+
+* ``ccd_bulk`` (default): CCD velocity derivatives, low-order stress derivative;
+* ``conservative_stress``: low-order everywhere;
+* ``ccd_stress_legacy``: CCD everywhere.
+
+The CCD derivatives run on the CCD line kernels, each of the ndim^2
+velocity gradients once (the reference forms each twice); the stress
+mu (a + b) is formed inside the low-order derivative kernel, which also
+accumulates over b and divides by Re rho on the last axis.  The interface-band variant
+(``psi`` given with ``ccd_bulk``) and the CN predictor are not built.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from typing import List
+
+from . import _lib
+from .arrays import to_device
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("twophaseflow_b200 needs a CUDA device; there is no CPU fallback")
+    return torch
+
+
+_ALIASES = {"stress_divergence": "conservative_stress", "low_order_conservative": "conservative_stress",
+            "ccd": "ccd_bulk", "ccd_legacy": "ccd_stress_legacy"}
+
+
+def canonical_viscous_spatial_scheme(name: str) -> str:
+    """viscous_spatial.py:9-25."""
+    c = _ALIASES.get(str(name).strip().lower(), str(name).strip().lower())
+    if c not in ("conservative_stress", "ccd_bulk", "ccd_stress_legacy"):
+        raise ValueError("viscous spatial scheme must be one of 'conservative_stress', 'ccd_bulk', or "
+                         f"'ccd_stress_legacy', got {name!r}")
+    return c
+
+
+class ViscousTerm:
+    """(1/Re) div[mu (grad u + grad u^T)] / rho (viscous.py:50-133)."""
+
+    def __init__(self, backend, Re: float, cn_viscous: bool = True, spatial_scheme: str = "ccd_bulk",
+                 cn_advance=None):
+        self.backend = backend
+        self.xp = getattr(backend, "xp", None)
+        self.Re = Re
+        self.cn_viscous = cn_viscous
+        self.spatial_scheme = canonical_viscous_spatial_scheme(spatial_scheme)
+        self.cn_advance = cn_advance
+        self._coef = {}
+        self.lib = _lib.load()
+
+    def _coefficients(self, grid, axis: int):
+        """Interior three-point coefficients of _low_order_derivative from the
+        node coordinates, as the reference evaluates them (viscous_spatial.py:70-104)."""
+        import numpy as np
+        torch = _torch()
+        key = (tuple(grid.N), tuple(float(x) for x in grid.L), axis)
+        if key not in self._coef:
+            coords = np.asarray(grid.coords[axis], dtype=float)
+            dx = coords[1:] - coords[:-1]
+            h_l, h_r = dx[:-1], dx[1:]
+            cl = -(h_r / (h_l * (h_l + h_r)))
+            cc = (h_r - h_l) / (h_l * h_r)
+            cr = h_l / (h_r * (h_l + h_r))
+            dev = torch.device("cuda", torch.cuda.current_device())
+            self._coef[key] = ([torch.from_numpy(np.ascontiguousarray(c)).to(dev) for c in (cl, cc, cr)],
+                               float(dx[0]), float(dx[-1]))
+        return self._coef[key]
+
+    def compute(self, ctx) -> List:
+        return self.compute_explicit(ctx.velocity, ctx.mu, ctx.rho, ctx.ccd)
+
+    def compute_explicit(self, velocity_components: List, mu, rho, ccd, psi=None) -> List:
+        torch = _torch()
+        if psi is not None and self.spatial_scheme == "ccd_bulk":
+            raise NotImplementedError("the interface-band viscous scheme (psi given) is not built on the B200 path")
+        dtype = getattr(ccd, "dtype", torch.float64)
+        vs = [to_device(v, dtype=dtype) for v in velocity_components]
+        vel = [v.tensor for v in vs]
+        mt = to_device(mu, dtype=dtype).tensor
+        rt = to_device(rho, dtype=dtype).tensor
+        nd = len(vel)
+        shape = (C.c_int64 * nd)(*[int(s) for s in vel[0].shape])
+        tdt = _lib.TPF_F64 if dtype == torch.float64 else _lib.TPF_F32
+        st = _lib.current_stream_handle()
+        lib = self.lib
+        grid = ccd.grid
+
+        def lowfd(total, ax, a, b=None, m=None, accumulate=False, finalize=False):
+            (cl, cc, cr), dx0, dxl = self._coefficients(grid, ax)
+            _lib.check(lib.tpf_visc_lowfd_axis(nd, shape, ax, _lib.dptr(cl), _lib.dptr(cc), _lib.dptr(cr), dx0, dxl,
+                                               _lib.dptr(a), _lib.dptr(b) if b is not None else None,
+                                               _lib.dptr(m) if m is not None else None, 1 if accumulate else 0,
+                                               1 if finalize else 0, _lib.dptr(rt), float(self.Re), _lib.dptr(total),
+                                               tdt, st))
+
+        # each velocity gradient du_i/dx_j is needed twice (as du_a/dx_b for
+        # component a and as du_b/dx_a for component b): computed once
+        grads = {}
+
+        def grad(i, j):
+            if (i, j) not in grads:
+                if self.spatial_scheme == "conservative_stress":
+                    g = torch.empty_like(vel[i])
+                    lowfd(g, j, vel[i])
+                else:
+                    g = ccd.first_derivative(vel[i], j)
+                grads[(i, j)] = g
+            return grads[(i, j)]
+
+        out = []
+        for al in range(nd):
+            total = torch.empty_like(vel[al])
+            for be in range(nd):
+                last = be == nd - 1
+                a = grad(al, be)
+                b = grad(be, al)
+                if self.spatial_scheme == "ccd_stress_legacy":
+                    stress = torch.empty_like(a)
+                    _lib.check(lib.tpf_visc_stress(a.numel(), _lib.dptr(mt), _lib.dptr(a), _lib.dptr(b),
+                                                   _lib.dptr(stress), tdt, st))
+                    g = ccd.first_derivative(stress, be)
+                    _lib.check(lib.tpf_visc_accumulate(g.numel(), _lib.dptr(g), 1 if be else 0, 1 if last else 0,
+                                                       _lib.dptr(rt), float(self.Re), _lib.dptr(total), tdt, st))
+                else:
+                    lowfd(total, be, a, b, mt, accumulate=be > 0, finalize=last)
+            out.append(vs[al].out(total))
+        return out
+
+    def apply_cn_predictor(self, *args, **kwargs):
+        raise NotImplementedError("the Crank-Nicolson viscous predictor is not built on the B200 path")
