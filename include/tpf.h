@@ -259,6 +259,15 @@ int tpf_visc_stress(int64_t n, const void* mu, const void* a, const void* b, voi
 int tpf_visc_accumulate(int64_t n, const void* g, int accumulate, int finalize, const void* rho, double re,
                         void* total, int dtype, void* stream);
 
+/* Predictor combinations (PicardCNAdvance.advance,
+ * src/twophase/time_integration/cn_advance/picard_cn.py:43-96; the explicit
+ * branch of ViscousTerm.apply_cn_predictor, ns_terms/viscous.py:161-167):
+ * mode 0: out = u + dt (e / rho + vn); mode 1: out = u + dt ((e / rho + 0.5 vn)
+ * + 0.5 vs).  e = explicit right-hand side, vn / vs = viscous force at u and at
+ * the predicted state.  n values each; out may alias u. */
+int tpf_cn_predictor_combine(int64_t n, int mode, double dt, const void* u, const void* e, const void* rho,
+                             const void* vn, const void* vs, void* out, int dtype, void* stream);
+
 /* Zero grad at index 0 and n_pts-1 along the axis of a [outer, n, inner]
  * array (wall axes only; no-op for periodic plans).  Replaces
  * CCDSolver.enforce_wall_neumann (ccd_solver.py:264-281;

@@ -55,3 +55,15 @@ def viscous(vel, mu, rho, Re: float, L, N, bc: str, scheme: str = "ccd_bulk"):
                 total += lo(mu * (a + b), be)
         out.append(total / (Re * rho))
     return out
+
+
+def cn_predictor(u_old, e, mu, rho, Re, L, N, bc, dt, cn_viscous=True, scheme="ccd_bulk"):
+    """ViscousTerm.apply_cn_predictor (ns_terms/viscous.py:135-181) with the
+    default PicardCNAdvance (time_integration/cn_advance/picard_cn.py:43-96)."""
+    nd = len(u_old)
+    vn = viscous(u_old, mu, rho, Re, L, N, bc, scheme)
+    pred = [u_old[c] + dt * (e[c] / rho + vn[c]) for c in range(nd)]
+    if not cn_viscous:
+        return pred
+    vs = viscous(pred, mu, rho, Re, L, N, bc, scheme)
+    return [u_old[c] + dt * (e[c] / rho + 0.5 * vn[c] + 0.5 * vs[c]) for c in range(nd)]

@@ -512,6 +512,13 @@ def make_viscous(out):
             v = ViscousTerm(be, 100.0, spatial_scheme=scheme).compute_explicit(vel, mu, rho, ccd)
             for a in range(len(N)):
                 out[f"{name}/{scheme}/v{a}"] = np.asarray(v[a])
+        e = [rng.standard_normal(grid.shape) for _ in N]
+        for a in range(len(N)):
+            out[f"{name}/e{a}"] = e[a]
+        for tag, cn in (("cn", True), ("fe", False)):
+            u = ViscousTerm(be, 100.0, cn_viscous=cn).apply_cn_predictor(vel, e, mu, rho, ccd, 0.003)
+            for a in range(len(N)):
+                out[f"{name}/pred_{tag}{a}"] = np.asarray(u[a])
 
 
 def main():

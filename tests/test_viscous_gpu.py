@@ -81,3 +81,38 @@ def test_viscous_of_rigid_rotation_vanishes(cuda_device):
         v = ViscousTerm(None, 10.0, spatial_scheme=scheme).compute_explicit([-Y, X], np.full(X.shape, 0.3),
                                                                             np.ones(X.shape), ccd)
         assert max(np.abs(c).max() for c in v) < 1e-9
+
+
+@pytest.mark.parametrize("name", ["wall2d", "per2d", "wall3d"])
+@pytest.mark.parametrize("tag,cn", [("cn", True), ("fe", False)])
+def test_cn_predictor_matches_reference(cuda_device, golden, name, tag, cn):
+    from twophaseflow_b200 import CCDSolver, UniformGrid, ViscousTerm
+    N = tuple(int(n) for n in golden[f"{name}/N"])
+    L = tuple(float(x) for x in golden[f"{name}/L"])
+    ccd = CCDSolver(UniformGrid(N, L), None, bc_type=str(golden[f"{name}/bc"]))
+    vel = [golden[f"{name}/u{a}"] for a in range(len(N))]
+    e = [golden[f"{name}/e{a}"] for a in range(len(N))]
+    u = ViscousTerm(None, 100.0, cn_viscous=cn).apply_cn_predictor(vel, e, golden[f"{name}/mu"],
+                                                                   golden[f"{name}/rho"], ccd, 0.003)
+    for a in range(len(N)):
+        ref = golden[f"{name}/pred_{tag}{a}"]
+        assert isinstance(u[a], np.ndarray)
+        assert np.abs(u[a] - ref).max() <= TOL * np.abs(ref).max()
+
+
+def test_cn_combine_kernel_bit_exact(cuda_device):
+    """Both combinations against NumPy on the same operands."""
+    import torch
+    from twophaseflow_b200 import _lib
+    rng = np.random.default_rng(67)
+    shape = (129, 130, 131)
+    u, e, vn, vs = (rng.standard_normal(shape) for _ in range(4))
+    rho = 0.001 + rng.uniform(0.0, 1.0, shape)
+    T = [torch.from_numpy(a).cuda() for a in (u, e, rho, vn, vs)]
+    out = torch.empty_like(T[0])
+    lib = _lib.load()
+    for mode in (0, 1):
+        _lib.check(lib.tpf_cn_predictor_combine(u.size, mode, 0.0037, *[_lib.dptr(t) for t in T], _lib.dptr(out),
+                                                _lib.TPF_F64, _lib.current_stream_handle()))
+        ref = u + 0.0037 * (e / rho + vn) if mode == 0 else u + 0.0037 * (e / rho + 0.5 * vn + 0.5 * vs)
+        np.testing.assert_array_equal(out.cpu().numpy(), ref)

@@ -27,3 +27,15 @@ def test_low_order_derivative_exact_on_quadratics():
     x = np.linspace(0.0, 1.0, 33)
     d = ov.low_order_derivative(x ** 2, 0, x)
     assert np.abs(d[1:-1] - 2.0 * x[1:-1]).max() < 1e-12
+
+
+@pytest.mark.parametrize("name", ["wall2d", "per2d", "wall3d"])
+@pytest.mark.parametrize("tag,cn", [("cn", True), ("fe", False)])
+def test_cn_predictor_matches_reference(name, tag, cn):
+    """ViscousTerm.apply_cn_predictor: Picard CN (Heun) and forward Euler."""
+    N, L, bc = G[f"{name}/N"], G[f"{name}/L"], str(G[f"{name}/bc"])
+    vel = [G[f"{name}/u{a}"] for a in range(len(N))]
+    e = [G[f"{name}/e{a}"] for a in range(len(N))]
+    u = ov.cn_predictor(vel, e, G[f"{name}/mu"], G[f"{name}/rho"], 100.0, L, N, bc, 0.003, cn)
+    for a in range(len(N)):
+        np.testing.assert_array_equal(u[a], G[f"{name}/pred_{tag}{a}"])

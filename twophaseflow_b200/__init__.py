@@ -22,7 +22,7 @@ from .grid import BoundarySpec, UniformGrid
 from .ppe import (MatrixAssemblyUnavailable, PPESolverFVMMatrixFree, create_fvm_matrixfree, register_with_reference,
                   solve_batched)
 from .levelset import CurvatureCalculatorPsi, dccd_filter_nd, update_properties
-from .viscous import ViscousTerm
+from .viscous import PicardCNAdvance, ViscousTerm
 from .step import CFLCalculator, RhieChowInterpolator, VelocityCorrector, ccd_pressure_gradient
 
 __all__ = [
@@ -42,6 +42,7 @@ __all__ = [
     "VelocityCorrector",
     "CFLCalculator",
     "ViscousTerm",
+    "PicardCNAdvance",
     "RhieChowInterpolator",
     "ccd_pressure_gradient",
     "CurvatureCalculatorPsi",

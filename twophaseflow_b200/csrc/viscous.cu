@@ -146,3 +146,45 @@ extern "C" int tpf_visc_accumulate(int64_t n, const void* g, int accumulate, int
   TPF_CUDA_TRY(cudaGetLastError());
   return TPF_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Predictor combinations of PicardCNAdvance.advance
+// (src/twophase/time_integration/cn_advance/picard_cn.py:43-96) and of the
+// explicit branch of ViscousTerm.apply_cn_predictor (ns_terms/viscous.py:161-167):
+//   mode 0 (forward Euler): u + dt (e / rho + vn)
+//   mode 1 (trapezoid):     u + dt ((e / rho + 0.5 vn) + 0.5 vs)
+// ---------------------------------------------------------------------------
+namespace {
+
+template <typename T>
+__global__ void cn_combine_kernel(int64_t n, int mode, double dt, const T* u, const T* e, const T* rho, const T* vn,
+                                  const T* vs, T* out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double er = (double)e[i] / (double)rho[i];
+    double b;
+    if (mode == 0) b = rn_add(er, (double)vn[i]);
+    else b = rn_add(rn_add(er, rn_mul(0.5, (double)vn[i])), rn_mul(0.5, (double)vs[i]));
+    out[i] = (T)rn_add((double)u[i], rn_mul(dt, b));
+  }
+}
+
+}  // namespace
+
+extern "C" int tpf_cn_predictor_combine(int64_t n, int mode, double dt, const void* u, const void* e, const void* rho,
+                                        const void* vn, const void* vs, void* out, int dtype, void* stream) {
+  TPF_CHECK_ARG(mode == 0 || mode == 1, "mode must be 0 (forward Euler) or 1 (trapezoid)");
+  TPF_CHECK_ARG(n >= 0 && u && e && rho && vn && out && (mode == 0 || vs), "NULL argument");
+  TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
+  if (n == 0) return TPF_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (dtype == TPF_F64)
+    cn_combine_kernel<double><<<blocks_for(n), 256, 0, st>>>(
+        n, mode, dt, static_cast<const double*>(u), static_cast<const double*>(e), static_cast<const double*>(rho),
+        static_cast<const double*>(vn), static_cast<const double*>(vs), static_cast<double*>(out));
+  else
+    cn_combine_kernel<float><<<blocks_for(n), 256, 0, st>>>(
+        n, mode, dt, static_cast<const float*>(u), static_cast<const float*>(e), static_cast<const float*>(rho),
+        static_cast<const float*>(vn), static_cast<const float*>(vs), static_cast<float*>(out));
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}

@@ -12,8 +12,10 @@ three spatial schemes:
 The CCD derivatives run on the CCD line kernels, each of the ndim^2
 velocity gradients once (the reference forms each twice); the stress
 mu (a + b) is formed inside the low-order derivative kernel, which also
-accumulates over b and divides by Re rho on the last axis.  The interface-band variant
-(``psi`` given with ``ccd_bulk``) and the CN predictor are not built.
+accumulates over b and divides by Re rho on the last axis.  ``apply_cn_predictor`` runs the
+explicit Euler branch or ``PicardCNAdvance`` (Heun: two viscous evaluations,
+two combination kernels).  The interface-band variant (``psi`` given with
+``ccd_bulk``) is not built.
 """
 
 from __future__ import annotations
@@ -137,5 +139,66 @@ class ViscousTerm:
             out.append(vs[al].out(total))
         return out
 
-    def apply_cn_predictor(self, *args, **kwargs):
-        raise NotImplementedError("the Crank-Nicolson viscous predictor is not built on the B200 path")
+    def _evaluate(self, vel: List, mu, rho, ccd, psi=None) -> List:
+        return self.compute_explicit(vel, mu, rho, ccd, psi=psi)
+
+    def _combine(self, mode, dt, u, e, rho, vn, vs=None):
+        torch = _torch()
+        out = torch.empty_like(u)
+        _lib.check(self.lib.tpf_cn_predictor_combine(
+            u.numel(), mode, float(dt), _lib.dptr(u), _lib.dptr(e), _lib.dptr(rho), _lib.dptr(vn),
+            _lib.dptr(vs) if vs is not None else None, _lib.dptr(out),
+            _lib.TPF_F64 if u.dtype == torch.float64 else _lib.TPF_F32, _lib.current_stream_handle()))
+        return out
+
+    def apply_cn_predictor(self, u_old: List, explicit_rhs: List, mu, rho, ccd, dt: float, psi=None,
+                           intermediate_velocity_operator_transform=None, predictor_state_assembly=None,
+                           convective_rhs=None, buoyancy_rhs=None) -> List:
+        """The viscous predictor step (viscous.py:135-181): forward Euler when
+        cn_viscous is False, else the CN strategy (PicardCNAdvance by default)."""
+        torch = _torch()
+        dtype = getattr(ccd, "dtype", torch.float64)
+        vs = [to_device(u, dtype=dtype) for u in u_old]
+        u = [v.tensor for v in vs]
+        e = [to_device(x, dtype=dtype).tensor for x in explicit_rhs]
+        rt = to_device(rho, dtype=dtype).tensor
+        if not self.cn_viscous:
+            visc_n = self.compute_explicit(u, mu, rt, ccd)
+            return [vs[c].out(self._combine(0, dt, u[c], e[c], rt, visc_n[c])) for c in range(len(u))]
+        adv = self.cn_advance if self.cn_advance is not None else PicardCNAdvance(self.backend)
+        out = adv.advance(u, e, mu, rt, self, ccd, dt, psi=psi,
+                          intermediate_velocity_operator_transform=intermediate_velocity_operator_transform,
+                          predictor_state_assembly=predictor_state_assembly, convective_rhs=convective_rhs,
+                          buoyancy_rhs=buoyancy_rhs)
+        return [vs[c].out(out[c]) for c in range(len(out))]
+
+
+class PicardCNAdvance:
+    """One Picard step on the CN equation, i.e. Heun's predictor-corrector
+    (src/twophase/time_integration/cn_advance/picard_cn.py:31-96):
+    u_pred = u + dt (e/rho + V(u)); u* = u + dt (e/rho + V(u)/2 + V(u_pred)/2).
+    Two viscous evaluations and two combination kernels; the optional
+    predictor-assembly and operator-transform hooks are called like the
+    reference calls them (with device tensors)."""
+
+    def __init__(self, backend=None):
+        self.backend = backend
+        self.xp = getattr(backend, "xp", None)
+
+    def advance(self, u_old: List, explicit_rhs: List, mu, rho, viscous_op: ViscousTerm, ccd, dt: float, psi=None,
+                intermediate_velocity_operator_transform=None, predictor_state_assembly=None, convective_rhs=None,
+                buoyancy_rhs=None) -> List:
+        nd = len(u_old)
+        visc_n = viscous_op._evaluate(u_old, mu, rho, ccd, psi=psi)
+        if predictor_state_assembly is not None:
+            u_pred = predictor_state_assembly(u_old=u_old, explicit_rhs=explicit_rhs, convective_rhs=convective_rhs,
+                                              buoyancy_rhs=buoyancy_rhs, visc_n=visc_n, rho=rho, dt=dt, xp=self.xp)
+        else:
+            u_pred = [viscous_op._combine(0, dt, u_old[c], explicit_rhs[c], rho, visc_n[c]) for c in range(nd)]
+        u_eval = u_pred
+        if intermediate_velocity_operator_transform is not None:
+            u_eval = [c.clone() for c in u_pred]
+            intermediate_velocity_operator_transform(u_eval)
+        visc_star = viscous_op._evaluate(u_eval, mu, rho, ccd, psi=psi)
+        return [viscous_op._combine(1, dt, u_old[c], explicit_rhs[c], rho, visc_n[c], visc_star[c])
+                for c in range(nd)]
