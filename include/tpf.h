@@ -203,6 +203,14 @@ int tpf_tvd_rk3_stage(int ndim, const int64_t* shape, const int* periodic, int s
 int tpf_sync_periodic_images(int ndim, const int64_t* shape, const int* periodic, void* arr, int dtype,
                              void* stream);
 
+/* UCCD6 convection, one (component j, axis k) term
+ * (UCCD6ConvectionTerm.compute, src/twophase/ns_terms/uccd6_convection.py:83-128):
+ * acc = (first ? 0 : acc) - 0.5 (uk d1 + cons), then acc - coeff (uref[0] d8);
+ * d1 = CCD D1_k u_j, cons = CCD D1_k (u_k u_j), d8 = (CCD D2_k)^4 u_j,
+ * uref = max |u_k| on the device (tpf_cfl_maxima), coeff = sigma h_k^7. */
+int tpf_uccd6_accumulate(int64_t n, int first, const void* uk, const void* d1, const void* cons, const void* d8,
+                         double coeff, const double* uref, void* acc, int dtype, void* stream);
+
 /* ---- Split reinitialization (src/twophase/levelset/reinit_split.py:73-102) */
 
 /* flux[a] = psi (1 - psi) d1[a] / max(sqrt(max(|d1|^2, 1e-12)), 1e-6), a < ndim

@@ -217,3 +217,23 @@ def reinitialize(psi, L, N, ccd_bc: str, eps: float, n_steps: int = 4, bc: str =
     if mass:
         q = sync(mass_correction(q, dV, M_old))
     return q
+
+
+def uccd6(vel, L, N, bc: str, sigma: float = 1.0e-3):
+    """UCCD6ConvectionTerm.compute (ns_terms/uccd6_convection.py:83-128)."""
+    nd = len(vel)
+    kinds = axis_kinds(bc, nd)
+    h = [float(L[a] / N[a]) for a in range(nd)]
+    h7 = [(float(L[a]) / int(N[a])) ** 7 for a in range(nd)]
+    D = lambda f, ax: occd.differentiate(f, ax, h[ax], bc=kinds[ax])
+    out = []
+    for j in range(nd):
+        acc = np.zeros_like(vel[j])
+        for k in range(nd):
+            d1, d2 = D(vel[j], k)
+            cons = D(vel[k] * vel[j], k)[0]
+            acc = acc - 0.5 * (vel[k] * d1 + cons)
+            d8 = D(D(D(d2, k)[1], k)[1], k)[1]
+            acc = acc - (sigma * h7[k]) * (np.abs(vel[k]).max() * d8)
+        out.append(acc)
+    return out

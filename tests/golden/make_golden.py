@@ -443,6 +443,10 @@ def make_advect(out):
         out[f"{name}/psi_new_noclip"] = np.asarray(adv.advance(psi.copy(), vel, dt, clip_bounds=None))
         adv_m = FCCDLevelSetAdvection(be, grid, fccd, mode="flux", mass_correction=True)
         out[f"{name}/psi_new_mass"] = np.asarray(adv_m.advance(psi.copy(), vel, dt))
+        from twophase.ns_terms.uccd6_convection import UCCD6ConvectionTerm
+        uc = UCCD6ConvectionTerm(be, grid, ccd, sigma=1.0e-3).compute(vel)
+        for a in range(len(N)):
+            out[f"{name}/uccd6_{a}"] = np.asarray(uc[a])
 
 
 def make_reinit(out):

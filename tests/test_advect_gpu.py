@@ -277,3 +277,38 @@ def test_mass_correction_kernels(cuda_device):
     _lib.check(lib.tpf_mass_correction_apply(q.size, _lib.dptr(z), _lib.dptr(target), _lib.dptr(sums),
                                              _lib.dptr(out), _lib.TPF_F64, st))
     assert float(out.abs().max()) == 0.0
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_uccd6_matches_reference(cuda_device, golden, name):
+    """Within the CCD chain's rounding (the oracle moves by ~2e-15 relative for
+    1e-15 input noise)."""
+    from twophaseflow_b200 import CCDSolver, UCCD6ConvectionTerm, UniformGrid
+    N = tuple(int(n) for n in golden[f"{name}/N"])
+    L = tuple(float(x) for x in golden[f"{name}/L"])
+    grid = UniformGrid(N, L)
+    ccd = CCDSolver(grid, None, bc_type=str(golden[f"{name}/bc"]))
+    vel = [golden[f"{name}/u{a}"] for a in range(len(N))]
+    u = UCCD6ConvectionTerm(None, grid, ccd, sigma=1.0e-3).compute(vel)
+    for a in range(len(N)):
+        ref = golden[f"{name}/uccd6_{a}"]
+        assert isinstance(u[a], np.ndarray)
+        assert np.abs(u[a] - ref).max() <= TOL * np.abs(ref).max()
+
+
+def test_uccd6_accumulate_kernel_bit_exact(cuda_device):
+    import torch
+    from twophaseflow_b200 import _lib
+    rng = np.random.default_rng(71)
+    shape = (257, 129, 65)
+    uk, d1, cons, d8, acc0 = (rng.standard_normal(shape) for _ in range(5))
+    T = [torch.from_numpy(a).cuda() for a in (uk, d1, cons, d8)]
+    ur = torch.tensor([float(np.abs(uk).max())], dtype=torch.float64, device="cuda")
+    lib = _lib.load()
+    for first in (1, 0):
+        acc = torch.from_numpy(acc0.copy()).cuda()
+        _lib.check(lib.tpf_uccd6_accumulate(uk.size, first, *[_lib.dptr(t) for t in T], 3.7e-9, _lib.dptr(ur),
+                                            _lib.dptr(acc), _lib.TPF_F64, _lib.current_stream_handle()))
+        a = (np.zeros(shape) if first else acc0) - 0.5 * (uk * d1 + cons)
+        a = a - 3.7e-9 * (np.abs(uk).max() * d8)
+        np.testing.assert_array_equal(acc.cpu().numpy(), a)

@@ -72,3 +72,12 @@ def test_mass_corrected_transport_matches_reference(name):
     dV = oa.cell_volumes(L, N, oa.periodic_flags(bc, len(N)))
     target = np.sum(oa.sync_images(psi.copy(), bc) * dV)
     np.testing.assert_array_equal(oa.sync_images(oa.mass_correction(q, dV, target), bc), G[f"{name}/psi_new_mass"])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_uccd6_matches_reference(name):
+    """UCCD6 skew convection + hyperviscosity (five CCD solves per pair)."""
+    N, L, bc, vel, psi, dt = _case(name)
+    u = oa.uccd6(vel, L, N, bc)
+    for a in range(len(N)):
+        np.testing.assert_array_equal(u[a], G[f"{name}/uccd6_{a}"])

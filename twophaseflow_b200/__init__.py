@@ -15,7 +15,7 @@ All arithmetic runs in the in-tree CUDA library ``libtpf.so`` (C ABI:
 ``include/tpf.h``); build it with ``python -m twophaseflow_b200.build``.
 """
 
-from .advection import FCCDLevelSetAdvection, FCCDSolver, SplitReinitializer
+from .advection import FCCDLevelSetAdvection, FCCDSolver, SplitReinitializer, UCCD6ConvectionTerm
 from .ccd import CCDSolver
 from .ccd_ppe import CCDVariableDensityOperator, PPESolverDefectCorrection
 from .grid import BoundarySpec, UniformGrid
@@ -30,6 +30,7 @@ __all__ = [
     "FCCDSolver",
     "FCCDLevelSetAdvection",
     "SplitReinitializer",
+    "UCCD6ConvectionTerm",
     "CCDVariableDensityOperator",
     "PPESolverDefectCorrection",
     "PPESolverFVMMatrixFree",

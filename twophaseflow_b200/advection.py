@@ -335,3 +335,56 @@ class SplitReinitializer:
             _lib.check(lib.tpf_sync_periodic_images(nd, shape, per, _lib.dptr(out), tdt, st))
             q = out
         return v.out(q)
+
+
+class UCCD6ConvectionTerm:
+    """Skew-symmetric CCD convection with sixth-order-scaled hyperviscosity
+    (src/twophase/ns_terms/uccd6_convection.py:31-128):
+    -0.5 [(u.grad) u_j + div(u_j u)] - sigma max|u_k| h_k^7 (D2_k)^4 u_j.
+    Per (j, k): CCD solves for D1/D2 of u_j, D1 of u_k u_j and the three further
+    second derivatives, max|u_k| by the CFL reduction kernel (kept on the
+    device), one accumulation kernel."""
+
+    scheme_names = ("uccd6",)
+
+    def __init__(self, backend, grid, ccd, sigma: float = 1.0e-3):
+        if sigma <= 0.0:
+            raise ValueError(f"sigma must be > 0, got {sigma}")
+        self._backend = backend
+        self.xp = getattr(backend, "xp", None)
+        self._ccd = ccd
+        self._grid = grid
+        self._sigma = float(sigma)
+        self._h7 = [(float(grid.L[ax]) / int(grid.N[ax])) ** 7 for ax in range(grid.ndim)]
+        self.lib = _lib.load()
+
+    def compute(self, ctx_or_velocity, ccd=None) -> List:
+        torch = _torch()
+        comps = ctx_or_velocity if isinstance(ctx_or_velocity, list) else ctx_or_velocity.velocity
+        cc = self._ccd
+        vs = [to_device(v, dtype=cc.dtype) for v in comps]
+        vel = [v.tensor for v in vs]
+        nd = len(vel)
+        n = vel[0].numel()
+        tdt = _lib.TPF_F64 if vel[0].dtype == torch.float64 else _lib.TPF_F32
+        st = _lib.current_stream_handle()
+        lib = self.lib
+        # max |u_k| of every component in one reduction, kept on the device
+        uref = torch.empty(4, dtype=torch.float64, device=vel[0].device)
+        ptrs = (C.c_void_p * nd)(*[_lib.dptr(v) for v in vel])
+        _lib.check(lib.tpf_cfl_maxima(n, nd, ptrs, None, None, tdt, _lib.dptr(uref), st))
+        prod = torch.empty_like(vel[0])
+        out = []
+        for j in range(nd):
+            acc = torch.empty_like(vel[j])
+            for k in range(nd):
+                d1, d2 = cc.differentiate(vel[j], k)
+                _lib.check(lib.tpf_fccd_product(n, _lib.dptr(vel[k]), _lib.dptr(vel[j]), _lib.dptr(prod), tdt, st))
+                cons = cc.first_derivative(prod, k)
+                d8 = cc.second_derivative(cc.second_derivative(cc.second_derivative(d2, k), k), k)
+                ur = uref[k:k + 1]
+                _lib.check(lib.tpf_uccd6_accumulate(n, 1 if k == 0 else 0, _lib.dptr(vel[k]), _lib.dptr(d1),
+                                                    _lib.dptr(cons), _lib.dptr(d8), self._sigma * self._h7[k],
+                                                    _lib.dptr(ur), _lib.dptr(acc), tdt, st))
+            out.append(vs[j].out(acc))
+        return out

@@ -622,3 +622,47 @@ extern "C" int tpf_mass_correction_apply(int64_t n, const void* q, const double*
   TPF_CUDA_TRY(cudaGetLastError());
   return TPF_OK;
 }
+
+// ---------------------------------------------------------------------------
+// UCCD6 convection accumulation (UCCD6ConvectionTerm.compute,
+// src/twophase/ns_terms/uccd6_convection.py:83-128), per (component j, axis k):
+//   acc = acc - 0.5 (u_k d1 + dcons);  acc = acc - coeff (u_ref d8)
+// with d1 = D1_k u_j, dcons = D1_k (u_k u_j), d8 = (D2_k)^4 u_j from the CCD
+// kernels, u_ref = max |u_k| (device scalar), coeff = sigma h_k^7.
+// ---------------------------------------------------------------------------
+namespace {
+
+template <typename T>
+__global__ void uccd6_acc_kernel(int64_t n, int first, const T* uk, const T* d1, const T* cons, const T* d8,
+                                 double coeff, const double* uref, T* acc) {
+  const double ur = *uref;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double a0 = first ? 0.0 : (double)acc[i];
+    const double adv = rn_mul((double)uk[i], (double)d1[i]);
+    double a = rn_sub(a0, rn_mul(0.5, rn_add(adv, (double)cons[i])));
+    a = (double)(T)a;
+    a = rn_sub(a, rn_mul(coeff, rn_mul(ur, (double)d8[i])));
+    acc[i] = (T)a;
+  }
+}
+
+}  // namespace
+
+extern "C" int tpf_uccd6_accumulate(int64_t n, int first, const void* uk, const void* d1, const void* cons,
+                                    const void* d8, double coeff, const double* uref, void* acc, int dtype,
+                                    void* stream) {
+  TPF_CHECK_ARG(n >= 0 && uk && d1 && cons && d8 && uref && acc, "NULL argument");
+  TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
+  if (n == 0) return TPF_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (dtype == TPF_F64)
+    uccd6_acc_kernel<double><<<blocks_for(n, 16), 256, 0, st>>>(
+        n, first, static_cast<const double*>(uk), static_cast<const double*>(d1), static_cast<const double*>(cons),
+        static_cast<const double*>(d8), coeff, uref, static_cast<double*>(acc));
+  else
+    uccd6_acc_kernel<float><<<blocks_for(n, 16), 256, 0, st>>>(
+        n, first, static_cast<const float*>(uk), static_cast<const float*>(d1), static_cast<const float*>(cons),
+        static_cast<const float*>(d8), coeff, uref, static_cast<float*>(acc));
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
