@@ -271,10 +271,27 @@ int tpf_visc_accumulate(int64_t n, const void* g, int accumulate, int finalize, 
  * src/twophase/time_integration/cn_advance/picard_cn.py:43-96; the explicit
  * branch of ViscousTerm.apply_cn_predictor, ns_terms/viscous.py:161-167):
  * mode 0: out = u + dt (e / rho + vn); mode 1: out = u + dt ((e / rho + 0.5 vn)
- * + 0.5 vs).  e = explicit right-hand side, vn / vs = viscous force at u and at
+ * + 0.5 vs); mode 2 (the explicit branch of Predictor.compute,
+ * time_integration/ab2_predictor.py:196-201): out = u + dt (e + rho vn) / rho.  e = explicit right-hand side, vn / vs = viscous force at u and at
  * the predicted state.  n values each; out may alias u. */
 int tpf_cn_predictor_combine(int64_t n, int mode, double dt, const void* u, const void* e, const void* rho,
                              const void* vn, const void* vs, void* out, int dtype, void* stream);
+
+/* ---- AB2 + IPC momentum predictor (time_integration/ab2_predictor.py:110-209) */
+
+/* acc = (first ? 0 : acc) - u du (ConvectionTerm.compute, ns_terms/convection.py:43-82). */
+int tpf_ns_conv_accumulate(int64_t n, int first, const void* u, const void* du, void* acc, int dtype, void* stream);
+
+/* mode 0: out = -a / s (GravityTerm, s = Fr^2, ns_terms/gravity.py:53-86);
+ * mode 1: out = (a b) / s (SurfaceTensionTerm CSF kappa dpsi / We,
+ * ns_terms/surface_tension.py:48-96). */
+int tpf_ns_scaled(int64_t n, int mode, const void* a, const void* b, double s, void* out, int dtype, void* stream);
+
+/* out = ((rho c + grav) + st) + (-gradp), c = 1.5 conv_n - 0.5 conv_prev (ab2)
+ * or conv_n; grav / st NULL add +0 (the reference's zero arrays). */
+int tpf_ns_explicit_rhs(int64_t n, int ab2, const void* conv_n, const void* conv_prev, const void* rho,
+                        const void* grav, const void* st_force, const void* gradp, void* out, int dtype,
+                        void* stream);
 
 /* Zero grad at index 0 and n_pts-1 along the axis of a [outer, n, inner]
  * array (wall axes only; no-op for periodic plans).  Replaces

@@ -67,3 +67,46 @@ def cn_predictor(u_old, e, mu, rho, Re, L, N, bc, dt, cn_viscous=True, scheme="c
         return pred
     vs = viscous(pred, mu, rho, Re, L, N, bc, scheme)
     return [u_old[c] + dt * (e[c] / rho + 0.5 * vn[c] + 0.5 * vs[c]) for c in range(nd)]
+
+
+def predictor_steps(states, dts, Re, Fr, We, L, N, bc, cn_viscous=True, use_gfm=False):
+    """Predictor.compute called once per state in turn (ab2_predictor.py:110-209):
+    AB2 convection (forward Euler first), gravity, CSF, IPC, viscous predictor."""
+    nd = len(N)
+    kinds = axis_kinds(bc, nd)
+    h = [float(L[a] / N[a]) for a in range(nd)]
+    D = lambda f, ax: np.asarray(occd.differentiate(f, ax, h[ax], bc=kinds[ax])[0])
+    prev = None
+    outs = []
+    for st, dt in zip(states, dts):
+        vel, rho, mu, kappa, psi, p = st
+        conv = []
+        for c in range(nd):
+            acc = np.zeros_like(vel[c])
+            for ax in range(nd):
+                acc -= vel[ax] * D(vel[c], ax)
+            conv.append(acc)
+        ab2 = [1.5 * conv[c] - 0.5 * prev[c] for c in range(nd)] if prev is not None else conv
+        grav = [np.zeros(rho.shape) for _ in range(nd)]
+        grav[nd - 1] = -rho / (Fr ** 2)
+        stf = [np.zeros_like(vel[c]) for c in range(nd)] if use_gfm else [kappa * D(psi, ax) / We for ax in range(nd)]
+        gp = []
+        for ax in range(nd):
+            g = D(p, ax).copy()
+            if kinds[ax] == "wall":
+                lo = [slice(None)] * nd
+                hi = [slice(None)] * nd
+                lo[ax] = 0
+                hi[ax] = -1
+                g[tuple(lo)] = 0.0
+                g[tuple(hi)] = 0.0
+            gp.append(g)
+        e = [rho * ab2[c] + grav[c] + stf[c] + (-gp[c]) for c in range(nd)]
+        if cn_viscous:
+            u = cn_predictor(vel, e, mu, rho, Re, L, N, bc, dt, True)
+        else:
+            v = viscous(vel, mu, rho, Re, L, N, bc)
+            u = [vel[c] + dt * (e[c] + rho * v[c]) / rho for c in range(nd)]
+        outs.append(u)
+        prev = [c.copy() for c in conv]
+    return outs

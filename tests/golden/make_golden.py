@@ -525,14 +525,57 @@ def make_viscous(out):
                 out[f"{name}/pred_{tag}{a}"] = np.asarray(u[a])
 
 
+def make_predictor(out):
+    """Two consecutive AB2 + IPC predictor steps of the reference (forward Euler
+    convection, then AB2), CN and explicit viscous, CSF and GFM."""
+    from twophase.backend import Backend
+    from twophase.config import FluidConfig, GridConfig, NumericsConfig, SimulationConfig
+    from twophase.core.grid import Grid
+    from twophase.core.flow_state import FlowState
+    from twophase.ccd.ccd_solver import CCDSolver
+    from twophase.time_integration.ab2_predictor import Predictor
+
+    be = Backend(use_gpu=False)
+    rng = np.random.default_rng(1618)
+    cases = [("wall2d", (16, 12), (1.0, 0.8), "wall", True, False), ("per2d", (12, 14), (1.0, 1.0), "periodic", False, False),
+             ("wall3d", (8, 6, 10), (1.0, 0.8, 1.2), "wall", True, True)]
+    for name, N, L, bc, cn, gfm in cases:
+        cfg = SimulationConfig(grid=GridConfig(ndim=len(N), N=N, L=L), fluid=FluidConfig(Re=50.0, Fr=0.8, We=4.0),
+                               numerics=NumericsConfig(cn_viscous=cn, bc_type=bc))
+        grid = Grid(cfg.grid, be)
+        ccd = CCDSolver(grid, be, bc_type=bc)
+        pred = Predictor(be, cfg, ccd, use_gfm=gfm)
+        out[f"{name}/N"] = np.array(N)
+        out[f"{name}/L"] = np.array(L, dtype=np.float64)
+        out[f"{name}/bc"] = np.array(bc)
+        out[f"{name}/cn"] = np.array(cn)
+        out[f"{name}/gfm"] = np.array(gfm)
+        for step, dt in enumerate((0.002, 0.0025)):
+            vel = [0.3 * rng.standard_normal(grid.shape) for _ in N]
+            psi = rng.uniform(0.0, 1.0, grid.shape)
+            rho = 0.1 + 0.9 * psi
+            mu = 0.01 + 0.99 * psi
+            kappa = rng.standard_normal(grid.shape)
+            p = rng.standard_normal(grid.shape)
+            for a in range(len(N)):
+                out[f"{name}/s{step}/u{a}"] = vel[a]
+            out[f"{name}/s{step}/psi"] = psi
+            out[f"{name}/s{step}/kappa"] = kappa
+            out[f"{name}/s{step}/p"] = p
+            out[f"{name}/s{step}/dt"] = np.array(dt)
+            u = pred.compute(FlowState(velocity=vel, psi=psi, rho=rho, mu=mu, kappa=kappa, pressure=p), dt)
+            for a in range(len(N)):
+                out[f"{name}/s{step}/ustar{a}"] = np.asarray(u[a])
+
+
 def main():
-    """Usage: make_golden.py [reference src dir] [only: ccd|ppe|step|levelset|rhiechow|advect|reinit|viscous ...]."""
+    """Usage: make_golden.py [reference src dir] [only: ccd|ppe|step|levelset|rhiechow|advect|reinit|viscous|predictor ...]."""
     src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
     only = set(sys.argv[2:])
     _ref_import(src)
     makers = {"ccd": make_ccd, "ppe": make_ppe, "step": make_step, "levelset": make_levelset,
               "rhiechow": make_rhiechow, "advect": make_advect, "reinit": make_reinit,
-              "viscous": make_viscous}
+              "viscous": make_viscous, "predictor": make_predictor}
     for key, fn in makers.items():
         if only and key not in only:
             continue

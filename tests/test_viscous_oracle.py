@@ -39,3 +39,31 @@ def test_cn_predictor_matches_reference(name, tag, cn):
     u = ov.cn_predictor(vel, e, G[f"{name}/mu"], G[f"{name}/rho"], 100.0, L, N, bc, 0.003, cn)
     for a in range(len(N)):
         np.testing.assert_array_equal(u[a], G[f"{name}/pred_{tag}{a}"])
+
+
+P = np.load(os.path.join(os.path.dirname(__file__), "golden", "predictor_golden.npz"))
+
+
+def predictor_states(g, name):
+    nd = len(g[f"{name}/N"])
+    states, dts = [], []
+    for s in range(2):
+        vel = [g[f"{name}/s{s}/u{a}"] for a in range(nd)]
+        psi = g[f"{name}/s{s}/psi"]
+        states.append((vel, 0.1 + 0.9 * psi, 0.01 + 0.99 * psi, g[f"{name}/s{s}/kappa"], psi, g[f"{name}/s{s}/p"]))
+        dts.append(float(g[f"{name}/s{s}/dt"]))
+    return states, dts
+
+
+@pytest.mark.parametrize("name", ["wall2d", "per2d", "wall3d"])
+def test_predictor_matches_reference(name):
+    """Two Predictor.compute calls (forward Euler then AB2 convection; CN or
+    explicit viscous; CSF or GFM) equal the reference bit for bit."""
+    N = tuple(int(x) for x in P[f"{name}/N"])
+    L = tuple(float(x) for x in P[f"{name}/L"])
+    states, dts = predictor_states(P, name)
+    outs = ov.predictor_steps(states, dts, 50.0, 0.8, 4.0, L, N, str(P[f"{name}/bc"]), bool(P[f"{name}/cn"]),
+                              bool(P[f"{name}/gfm"]))
+    for s in range(2):
+        for a in range(len(N)):
+            np.testing.assert_array_equal(outs[s][a], P[f"{name}/s{s}/ustar{a}"])

@@ -23,6 +23,7 @@ from .ppe import (MatrixAssemblyUnavailable, PPESolverFVMMatrixFree, create_fvm_
                   solve_batched)
 from .levelset import CurvatureCalculatorPsi, dccd_filter_nd, update_properties
 from .viscous import PicardCNAdvance, ViscousTerm
+from .predictor import ConvectionTerm, FlowState, GravityTerm, NSComputeContext, Predictor, SurfaceTensionTerm
 from .step import CFLCalculator, RhieChowInterpolator, VelocityCorrector, ccd_pressure_gradient
 
 __all__ = [
@@ -44,6 +45,12 @@ __all__ = [
     "CFLCalculator",
     "ViscousTerm",
     "PicardCNAdvance",
+    "ConvectionTerm",
+    "GravityTerm",
+    "SurfaceTensionTerm",
+    "NSComputeContext",
+    "FlowState",
+    "Predictor",
     "RhieChowInterpolator",
     "ccd_pressure_gradient",
     "CurvatureCalculatorPsi",

@@ -129,6 +129,12 @@ SIGNATURES = {
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "tpf_uccd6_accumulate": (C.c_int, [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                        C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "tpf_ns_conv_accumulate": (C.c_int, [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                         C.c_void_p]),
+    "tpf_ns_scaled": (C.c_int, [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_int,
+                                C.c_void_p]),
+    "tpf_ns_explicit_rhs": (C.c_int, [C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "tpf_ccd_enforce_wall_neumann": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]),
     "tpf_ppe_default_options": (None, [C.POINTER(tpf_ppe_options)]),
     "tpf_ppe_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_int64),

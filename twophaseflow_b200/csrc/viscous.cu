@@ -153,6 +153,7 @@ extern "C" int tpf_visc_accumulate(int64_t n, const void* g, int accumulate, int
 // explicit branch of ViscousTerm.apply_cn_predictor (ns_terms/viscous.py:161-167):
 //   mode 0 (forward Euler): u + dt (e / rho + vn)
 //   mode 1 (trapezoid):     u + dt ((e / rho + 0.5 vn) + 0.5 vs)
+//   mode 2 (Predictor.compute, explicit viscous): u + dt (e + rho vn) / rho
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -160,6 +161,11 @@ template <typename T>
 __global__ void cn_combine_kernel(int64_t n, int mode, double dt, const T* u, const T* e, const T* rho, const T* vn,
                                   const T* vs, T* out) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (mode == 2) {   // explicit viscous predictor of Predictor.compute: u + dt (e + rho vn) / rho
+      const double r = (double)rho[i];
+      out[i] = (T)rn_add((double)u[i], rn_mul(dt, rn_add((double)e[i], rn_mul(r, (double)vn[i]))) / r);
+      continue;
+    }
     const double er = (double)e[i] / (double)rho[i];
     double b;
     if (mode == 0) b = rn_add(er, (double)vn[i]);
@@ -172,8 +178,8 @@ __global__ void cn_combine_kernel(int64_t n, int mode, double dt, const T* u, co
 
 extern "C" int tpf_cn_predictor_combine(int64_t n, int mode, double dt, const void* u, const void* e, const void* rho,
                                         const void* vn, const void* vs, void* out, int dtype, void* stream) {
-  TPF_CHECK_ARG(mode == 0 || mode == 1, "mode must be 0 (forward Euler) or 1 (trapezoid)");
-  TPF_CHECK_ARG(n >= 0 && u && e && rho && vn && out && (mode == 0 || vs), "NULL argument");
+  TPF_CHECK_ARG(mode >= 0 && mode <= 2, "mode must be 0 (forward Euler), 1 (trapezoid) or 2 (explicit predictor)");
+  TPF_CHECK_ARG(n >= 0 && u && e && rho && vn && out && (mode != 1 || vs), "NULL argument");
   TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
   if (n == 0) return TPF_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -185,6 +191,100 @@ extern "C" int tpf_cn_predictor_combine(int64_t n, int mode, double dt, const vo
     cn_combine_kernel<float><<<blocks_for(n), 256, 0, st>>>(
         n, mode, dt, static_cast<const float*>(u), static_cast<const float*>(e), static_cast<const float*>(rho),
         static_cast<const float*>(vn), static_cast<const float*>(vs), static_cast<float*>(out));
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Momentum predictor terms (src/twophase/time_integration/ab2_predictor.py:110-209;
+// ns_terms/convection.py:43-82, gravity.py:53-86, surface_tension.py:48-96)
+// ---------------------------------------------------------------------------
+namespace {
+
+// acc = (first ? 0 : acc) - u du   (ConvectionTerm: acc -= u_ax * du/dx_ax)
+template <typename T>
+__global__ void conv_acc_kernel(int64_t n, int first, const T* u, const T* du, T* acc) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double a0 = first ? 0.0 : (double)acc[i];
+    acc[i] = (T)rn_sub(a0, rn_mul((double)u[i], (double)du[i]));
+  }
+}
+
+// mode 0: out = -a / s (gravity, s = Fr^2); mode 1: out = (a b) / s (CSF, s = We)
+template <typename T>
+__global__ void scaled_kernel(int64_t n, int mode, const T* a, const T* b, double s, T* out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (T)((mode == 0 ? -(double)a[i] : rn_mul((double)a[i], (double)b[i])) / s);
+}
+
+// explicit_rhs = ((rho ab2 + grav) + st) + (-gradp), ab2 = 1.5 cn - 0.5 cp (AB2)
+// or cn (first step); a NULL grav / st adds +0 as the reference's zero arrays do
+template <typename T>
+__global__ void explicit_rhs_kernel(int64_t n, int ab2, const T* cn, const T* cp, const T* rho, const T* grav,
+                                    const T* st, const T* gradp, T* out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double c = (double)cn[i];
+    if (ab2) c = (double)(T)rn_sub(rn_mul(1.5, c), rn_mul(0.5, (double)cp[i]));
+    double e = rn_mul((double)rho[i], c);
+    e = rn_add(e, grav ? (double)grav[i] : 0.0);
+    e = rn_add(e, st ? (double)st[i] : 0.0);
+    e = rn_add(e, -(double)gradp[i]);
+    out[i] = (T)e;
+  }
+}
+
+}  // namespace
+
+extern "C" int tpf_ns_conv_accumulate(int64_t n, int first, const void* u, const void* du, void* acc, int dtype,
+                                      void* stream) {
+  TPF_CHECK_ARG(n >= 0 && u && du && acc, "NULL argument");
+  TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
+  if (n == 0) return TPF_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (dtype == TPF_F64)
+    conv_acc_kernel<double><<<blocks_for(n), 256, 0, st>>>(n, first, static_cast<const double*>(u),
+                                                           static_cast<const double*>(du), static_cast<double*>(acc));
+  else
+    conv_acc_kernel<float><<<blocks_for(n), 256, 0, st>>>(n, first, static_cast<const float*>(u),
+                                                          static_cast<const float*>(du), static_cast<float*>(acc));
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
+extern "C" int tpf_ns_scaled(int64_t n, int mode, const void* a, const void* b, double s, void* out, int dtype,
+                             void* stream) {
+  TPF_CHECK_ARG(mode == 0 || mode == 1, "mode must be 0 (gravity) or 1 (CSF)");
+  TPF_CHECK_ARG(n >= 0 && a && out && (mode == 0 || b) && s != 0.0, "invalid arguments");
+  TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
+  if (n == 0) return TPF_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (dtype == TPF_F64)
+    scaled_kernel<double><<<blocks_for(n), 256, 0, st>>>(n, mode, static_cast<const double*>(a),
+                                                         static_cast<const double*>(b), s, static_cast<double*>(out));
+  else
+    scaled_kernel<float><<<blocks_for(n), 256, 0, st>>>(n, mode, static_cast<const float*>(a),
+                                                        static_cast<const float*>(b), s, static_cast<float*>(out));
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
+extern "C" int tpf_ns_explicit_rhs(int64_t n, int ab2, const void* conv_n, const void* conv_prev, const void* rho,
+                                   const void* grav, const void* st_force, const void* gradp, void* out, int dtype,
+                                   void* stream) {
+  TPF_CHECK_ARG(n >= 0 && conv_n && rho && gradp && out && (!ab2 || conv_prev), "NULL argument");
+  TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
+  if (n == 0) return TPF_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (dtype == TPF_F64)
+    explicit_rhs_kernel<double><<<blocks_for(n), 256, 0, st>>>(
+        n, ab2, static_cast<const double*>(conv_n), static_cast<const double*>(conv_prev),
+        static_cast<const double*>(rho), static_cast<const double*>(grav), static_cast<const double*>(st_force),
+        static_cast<const double*>(gradp), static_cast<double*>(out));
+  else
+    explicit_rhs_kernel<float><<<blocks_for(n), 256, 0, st>>>(
+        n, ab2, static_cast<const float*>(conv_n), static_cast<const float*>(conv_prev),
+        static_cast<const float*>(rho), static_cast<const float*>(grav), static_cast<const float*>(st_force),
+        static_cast<const float*>(gradp), static_cast<float*>(out));
   TPF_CUDA_TRY(cudaGetLastError());
   return TPF_OK;
 }
