@@ -284,7 +284,7 @@ int tpf_ns_conv_accumulate(int64_t n, int first, const void* u, const void* du, 
 
 /* mode 0: out = -a / s (GravityTerm, s = Fr^2, ns_terms/gravity.py:53-86);
  * mode 1: out = (a b) / s (SurfaceTensionTerm CSF kappa dpsi / We,
- * ns_terms/surface_tension.py:48-96). */
+ * ns_terms/surface_tension.py:48-96); mode 2: out = a / s (b unused). */
 int tpf_ns_scaled(int64_t n, int mode, const void* a, const void* b, double s, void* out, int dtype, void* stream);
 
 /* out = ((rho c + grav) + st) + (-gradp), c = 1.5 conv_n - 0.5 conv_prev (ab2)

@@ -24,6 +24,7 @@ from .ppe import (MatrixAssemblyUnavailable, PPESolverFVMMatrixFree, create_fvm_
 from .levelset import CurvatureCalculatorPsi, dccd_filter_nd, update_properties
 from .viscous import PicardCNAdvance, ViscousTerm
 from .predictor import ConvectionTerm, FlowState, GravityTerm, NSComputeContext, Predictor, SurfaceTensionTerm
+from .ns_step import TwoPhaseStep
 from .step import CFLCalculator, RhieChowInterpolator, VelocityCorrector, ccd_pressure_gradient
 
 __all__ = [
@@ -51,6 +52,7 @@ __all__ = [
     "NSComputeContext",
     "FlowState",
     "Predictor",
+    "TwoPhaseStep",
     "RhieChowInterpolator",
     "ccd_pressure_gradient",
     "CurvatureCalculatorPsi",

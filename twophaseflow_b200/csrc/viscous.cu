@@ -210,11 +210,12 @@ __global__ void conv_acc_kernel(int64_t n, int first, const T* u, const T* du, T
   }
 }
 
-// mode 0: out = -a / s (gravity, s = Fr^2); mode 1: out = (a b) / s (CSF, s = We)
+// mode 0: out = -a / s (gravity, s = Fr^2); mode 1: out = (a b) / s (CSF, s = We);
+// mode 2: out = a / s (the projection right-hand side div u* / dt)
 template <typename T>
 __global__ void scaled_kernel(int64_t n, int mode, const T* a, const T* b, double s, T* out) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    out[i] = (T)((mode == 0 ? -(double)a[i] : rn_mul((double)a[i], (double)b[i])) / s);
+    out[i] = (T)((mode == 0 ? -(double)a[i] : (mode == 1 ? rn_mul((double)a[i], (double)b[i]) : (double)a[i])) / s);
 }
 
 // explicit_rhs = ((rho ab2 + grav) + st) + (-gradp), ab2 = 1.5 cn - 0.5 cp (AB2)
@@ -253,8 +254,8 @@ extern "C" int tpf_ns_conv_accumulate(int64_t n, int first, const void* u, const
 
 extern "C" int tpf_ns_scaled(int64_t n, int mode, const void* a, const void* b, double s, void* out, int dtype,
                              void* stream) {
-  TPF_CHECK_ARG(mode == 0 || mode == 1, "mode must be 0 (gravity) or 1 (CSF)");
-  TPF_CHECK_ARG(n >= 0 && a && out && (mode == 0 || b) && s != 0.0, "invalid arguments");
+  TPF_CHECK_ARG(mode >= 0 && mode <= 2, "mode must be 0 (gravity), 1 (CSF) or 2 (quotient)");
+  TPF_CHECK_ARG(n >= 0 && a && out && (mode != 1 || b) && s != 0.0, "invalid arguments");
   TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
   if (n == 0) return TPF_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);

@@ -11,6 +11,7 @@
     python -m twophaseflow_b200.kernel_cases advect --N 256 256 256 --bc periodic [--reps 3]
     python -m twophaseflow_b200.kernel_cases reinit --N 256 256 256 [--reps 2]
     python -m twophaseflow_b200.kernel_cases viscous --N 256 256 256 [--reps 2]
+    python -m twophaseflow_b200.kernel_cases step --N 192 192 192 [--reps 3]    (rising bubble, whole step)
 
 ``ccd`` captures ``reps`` CCDSolver.differentiate calls in one CUDA graph and
 replays it, so the reported time is device time per call (no Python launch
@@ -327,6 +328,55 @@ def viscous_case(N, dtype, reps):
             "us_per_compute": round(ms * 1e3, 1), "lowfd_kernel": axes}
 
 
+def step_case(N, reps, use_graphs=True):
+    """Whole two-phase time steps (TwoPhaseStep): a gas bubble of radius 0.2 at
+    (0.5, 0.5, 0.3) in liquid ((0.5, 0.3) in 2-D), density ratio 1000,
+    viscosity ratio 100, Re 100, We 10, Fr 1, dt = 0.25 h.  Two warm-up steps
+    (eager + capture, then one replay), then ``reps`` timed steps split into
+    the pre-PPE graph, the PPE solve and the post-PPE graph (CUDA events)."""
+    import torch
+    from . import TwoPhaseStep, UniformGrid
+    nd = len(N)
+    ax = [torch.linspace(0.0, 1.0, n + 1, dtype=torch.float64, device="cuda") for n in N]
+    X = torch.meshgrid(*ax, indexing="ij")
+    c = [0.5] * (nd - 1) + [0.3]
+    r = torch.sqrt(sum((X[a] - c[a]) ** 2 for a in range(nd)))
+    h = 1.0 / max(N)
+    psi = torch.sigmoid((r - 0.2) / (1.5 * h)).contiguous()   # liquid (psi = 1) outside the bubble
+    del X, r
+    stp = TwoPhaseStep(UniformGrid(N), psi, Re=100.0, Fr=1.0, We=10.0, rho_ratio=1e-3, mu_ratio=1e-2,
+                       use_graphs=use_graphs)
+    dt = 0.25 * h
+    for _ in range(2):
+        stp.step(dt)
+    torch.cuda.synchronize()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(reps)]
+    its = []
+    for k in range(reps):
+        e = ev[k]
+        e[0].record()
+        if use_graphs:
+            stp._g1.replay()
+        else:
+            stp._phase1(dt)
+        e[1].record()
+        stp._solve()
+        e[2].record()
+        if use_graphs:
+            stp._g2.replay()
+        else:
+            stp._phase2(dt)
+        e[3].record()
+        its.append(stp.last_ppe_iterations)
+    torch.cuda.synchronize()
+    t = [[e[i].elapsed_time(e[i + 1]) for i in range(3)] for e in ev]
+    return {"case": "step", "N": list(N), "graphs": use_graphs, "ms_per_step": round(sum(sum(x) for x in t) / reps, 2),
+            "pre_ppe_ms": round(sum(x[0] for x in t) / reps, 2), "ppe_ms": round(sum(x[1] for x in t) / reps, 2),
+            "post_ppe_ms": round(sum(x[2] for x in t) / reps, 2), "ppe_iterations": its,
+            "psi_range": [round(float(stp.psi.min()), 6), round(float(stp.psi.max()), 6)],
+            "u_max": round(float(max(v.abs().max() for v in stp.vel)), 6)}
+
+
 def ppe_case(N, precision, reps, tol=1e-8):
     import torch
     from . import PPESolverFVMMatrixFree, UniformGrid
@@ -494,7 +544,7 @@ def gmres_case(N, line, reps, maxiter=None, tol=1e-8):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["ccd", "ppe", "learned", "batched", "gmres", "corrector", "curvature", "rhiechow", "advect", "reinit", "viscous"])
+    ap.add_argument("case", choices=["ccd", "ppe", "learned", "batched", "gmres", "corrector", "curvature", "rhiechow", "advect", "reinit", "viscous", "step"])
     ap.add_argument("--line", default="thomas", choices=["thomas", "pcr"], help="gmres: line solver")
     ap.add_argument("--N", type=int, nargs="+", required=True)
     ap.add_argument("--axis", type=int, default=0)
@@ -525,6 +575,8 @@ def main(argv=None):
         r = reinit_case(tuple(a.N), a.dtype, a.reps)
     elif a.case == "viscous":
         r = viscous_case(tuple(a.N), a.dtype, a.reps)
+    elif a.case == "step":
+        r = step_case(tuple(a.N), a.reps)
     else:
         r = batched_case(n_cases=a.N[0], reps=a.reps)
     print(json.dumps(r), flush=True)

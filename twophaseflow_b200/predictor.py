@@ -204,6 +204,12 @@ class Predictor:
                                                              _lib.dptr(explicit_rhs[c]), _lib.dptr(rho),
                                                              _lib.dptr(visc[c]), None, _lib.dptr(u), _tdt(u), st))
                 vel_star.append(u)
-        self._conv_prev = [c.clone() for c in conv_n]
+        # the stored convection is updated in place once it exists, so a CUDA
+        # graph that captured this call keeps reading and writing the same buffers
+        if self._conv_prev is None:
+            self._conv_prev = [c.clone() for c in conv_n]
+        else:
+            for c in range(ndim):
+                self._conv_prev[c].copy_(conv_n[c])
         self._ab2_ready = True
         return [vs[c].out(vel_star[c]) for c in range(ndim)]
