@@ -83,7 +83,7 @@ def _layer_rel(g, ref):
 
 
 def test_unet_backward_matches_oracle(cuda_device):
-    """GPU gradients vs the BF16 oracle, judged against the oracle's own
+    """GPU gradients vs the BF16 oracle, measured against the oracle's own
     sensitivity: BF16 storage makes the gradients chaotic (a 1e-6 relative
     change of the parameters already moves them by several percent), so the
     bar per layer is a multiple of that measured sensitivity, plus a cosine

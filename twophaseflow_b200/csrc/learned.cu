@@ -15,7 +15,7 @@
 // products an iteration needs come from one fused stencil+reduction pass
 // (S symmetric: (p', S z) = (S p', z)), vectors and scalars stay in FP64 on
 // the device, and one iteration is replayed as a CUDA graph.  Convergence is
-// judged on the true residual b - S x at the end; when the residual stops
+// checked on the true residual b - S x at the end; when the residual stops
 // falling the solve continues with the plain Jacobi PCG kernel from the
 // current iterate.
 //
@@ -1095,7 +1095,7 @@ int tpf_lppe_solve(tpf_lppe* lp, const double* rhs, const double* rho, double* p
       graph_ready = true;
     }
     if (lp->st_host->done) {
-      // judge convergence on the true residual; restart the recurrence from it otherwise
+      // test convergence on the true residual; restart the recurrence from it otherwise
       if ((st = true_residual(lp, s, o.tol, 0, o.window))) return st;
       if ((st = read_state(lp, s))) return st;
       converged = lp->st_host->done != 0;

@@ -15,7 +15,7 @@ the B200 addition built on top of the plain method:
 * ``train`` -- Adam on the relative squared error of the scaled correction.
 * ``PPESolverLearned`` -- an ``IPPESolver`` with the reference's
   ``solve(rhs, rho, dt, p_init)`` contract whose solve is flexible CG
-  preconditioned by the network (tpf_lppe_solve), judged on the true residual,
+  preconditioned by the network (tpf_lppe_solve), checked on the true residual,
   falling back to plain Jacobi PCG when the residual stalls.
 
 All arithmetic runs on the GPU in the CUDA library; PyTorch only holds device
