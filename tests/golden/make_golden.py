@@ -568,14 +568,61 @@ def make_predictor(out):
                 out[f"{name}/s{step}/ustar{a}"] = np.asarray(u[a])
 
 
+def make_fccd_ppe(out):
+    """The FCCD matrix-free PPE of the reference on its default path
+    (phase_density coefficients, full faces): operator applies, the Jacobi
+    inverse and GMRES solutions."""
+    from types import SimpleNamespace
+    from twophase.backend import Backend
+    from twophase.config import GridConfig
+    from twophase.core.grid import Grid
+    from twophase.ccd.ccd_solver import CCDSolver
+    from twophase.ccd.fccd import FCCDSolver
+    from twophase.ppe.fccd_matrixfree import PPESolverFCCDMatrixFree
+
+    be = Backend(use_gpu=False)
+    rng = np.random.default_rng(5151)
+    cases = [("wall2d", (16, 12), (1.0, 0.8), "wall", "jacobi"), ("per2d", (12, 12), (1.0, 1.0), "periodic", "none"),
+             ("wall3d", (8, 6, 10), (1.0, 0.8, 1.2), "wall", "jacobi")]
+    for name, N, L, bc, pre in cases:
+        grid = Grid(GridConfig(ndim=len(N), N=N, L=L), be)
+        ccd = CCDSolver(grid, be, bc_type=bc)
+        fccd = FCCDSolver(grid, be, bc_type=bc, ccd_solver=ccd)
+        cfg = SimpleNamespace(pseudo_tol=1e-9, pseudo_maxiter=500, ppe_restart=None, ppe_preconditioner=pre)
+        solver = PPESolverFCCDMatrixFree(be, cfg, grid, fccd)
+        rho = 0.5 + rng.uniform(0.0, 1.0, grid.shape)
+        if bc == "periodic":
+            for ax in range(len(N)):
+                src = [slice(None)] * len(N)
+                img = [slice(None)] * len(N)
+                src[ax] = 0
+                img[ax] = -1
+                rho[tuple(img)] = rho[tuple(src)]
+        p = rng.standard_normal(grid.shape)
+        rhs = rng.standard_normal(grid.shape)
+        solver.prepare_operator(rho)
+        out[f"{name}/N"] = np.array(N)
+        out[f"{name}/L"] = np.array(L, dtype=np.float64)
+        out[f"{name}/bc"] = np.array(bc)
+        out[f"{name}/pre"] = np.array(pre)
+        out[f"{name}/rho"] = rho
+        out[f"{name}/p"] = p
+        out[f"{name}/rhs"] = rhs
+        out[f"{name}/apply"] = np.asarray(solver.apply(p))
+        if pre == "jacobi":
+            out[f"{name}/diag_inv"] = np.asarray(solver._diag_inv)
+        out[f"{name}/sol"] = np.asarray(solver.solve(rhs, rho))
+
+
 def main():
-    """Usage: make_golden.py [reference src dir] [only: ccd|ppe|step|levelset|rhiechow|advect|reinit|viscous|predictor ...]."""
+    """Usage: make_golden.py [reference src dir] [only: ccd|ppe|step|levelset|rhiechow|advect|reinit|viscous|predictor|fccd_ppe ...]."""
     src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
     only = set(sys.argv[2:])
     _ref_import(src)
     makers = {"ccd": make_ccd, "ppe": make_ppe, "step": make_step, "levelset": make_levelset,
               "rhiechow": make_rhiechow, "advect": make_advect, "reinit": make_reinit,
-              "viscous": make_viscous, "predictor": make_predictor}
+              "viscous": make_viscous, "predictor": make_predictor,
+              "fccd_ppe": make_fccd_ppe}
     for key, fn in makers.items():
         if only and key not in only:
             continue
