@@ -614,15 +614,40 @@ def make_fccd_ppe(out):
         out[f"{name}/sol"] = np.asarray(solver.solve(rhs, rho))
 
 
+def make_c1(out):
+    """The reference's stable quick-start (64^2 bubble, R = 0.25 at the centre,
+    Re 100, Fr 1, We 10, density and viscosity ratios 0.1, extension_method
+    'none'): three steps of SimulationBuilder(cfg).build().step_forward(dt) with
+    the reference's CFL time step, fields after each step."""
+    from twophase.config import FluidConfig, GridConfig, NumericsConfig, SimulationConfig
+    from twophase.simulation.builder import SimulationBuilder
+
+    cfg = SimulationConfig(grid=GridConfig(ndim=2, N=(64, 64), L=(1.0, 1.0)),
+                           fluid=FluidConfig(Re=100.0, Fr=1.0, We=10.0, rho_ratio=0.1, mu_ratio=0.1),
+                           numerics=NumericsConfig(extension_method="none"))
+    sim = SimulationBuilder(cfg).build()
+    X, Y = sim.grid.meshgrid()
+    sim.psi.data[:] = 1.0 / (1.0 + np.exp(-(np.sqrt((X - 0.5) ** 2 + (Y - 0.5) ** 2) - 0.25) / (1.5 / 64)))
+    out["psi0"] = np.array(sim.psi.data)
+    for k in range(3):
+        dt = float(sim.cfl_calc.compute([sim.velocity[0], sim.velocity[1]], sim.mu.data, sim.rho.data))
+        sim.step_forward(dt)
+        out[f"s{k}/dt"] = np.array(dt)
+        out[f"s{k}/psi"] = np.array(sim.psi.data)
+        out[f"s{k}/u"] = np.array(sim.velocity[0])
+        out[f"s{k}/v"] = np.array(sim.velocity[1])
+        out[f"s{k}/p"] = np.array(sim.pressure.data)
+
+
 def main():
-    """Usage: make_golden.py [reference src dir] [only: ccd|ppe|step|levelset|rhiechow|advect|reinit|viscous|predictor|fccd_ppe ...]."""
+    """Usage: make_golden.py [reference src dir] [only: ccd|ppe|step|levelset|rhiechow|advect|reinit|viscous|predictor|fccd_ppe|c1 ...]."""
     src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
     only = set(sys.argv[2:])
     _ref_import(src)
     makers = {"ccd": make_ccd, "ppe": make_ppe, "step": make_step, "levelset": make_levelset,
               "rhiechow": make_rhiechow, "advect": make_advect, "reinit": make_reinit,
               "viscous": make_viscous, "predictor": make_predictor,
-              "fccd_ppe": make_fccd_ppe}
+              "fccd_ppe": make_fccd_ppe, "c1": make_c1}
     for key, fn in makers.items():
         if only and key not in only:
             continue
