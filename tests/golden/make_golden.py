@@ -617,7 +617,7 @@ def make_fccd_ppe(out):
 def make_c1(out):
     """The reference's stable quick-start (64^2 bubble, R = 0.25 at the centre,
     Re 100, Fr 1, We 10, density and viscosity ratios 0.1, extension_method
-    'none'): three steps of SimulationBuilder(cfg).build().step_forward(dt) with
+    'none'): six steps of SimulationBuilder(cfg).build().step_forward(dt) with
     the reference's CFL time step, fields after each step."""
     from twophase.config import FluidConfig, GridConfig, NumericsConfig, SimulationConfig
     from twophase.simulation.builder import SimulationBuilder
@@ -629,7 +629,7 @@ def make_c1(out):
     X, Y = sim.grid.meshgrid()
     sim.psi.data[:] = 1.0 / (1.0 + np.exp(-(np.sqrt((X - 0.5) ** 2 + (Y - 0.5) ** 2) - 0.25) / (1.5 / 64)))
     out["psi0"] = np.array(sim.psi.data)
-    for k in range(3):
+    for k in range(6):
         dt = float(sim.cfl_calc.compute([sim.velocity[0], sim.velocity[1]], sim.mu.data, sim.rho.data))
         sim.step_forward(dt)
         out[f"s{k}/dt"] = np.array(dt)

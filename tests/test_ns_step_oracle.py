@@ -1,5 +1,5 @@
 """The full-step oracle (the reference's stable quick-start pipeline composed
-from this repository's operator oracles) against three steps of the
+from this repository's operator oracles) against six steps of the
 reference itself (tests/golden/c1_golden.npz, written by
 tests/golden/make_golden.py): psi, u, v and p bit for bit."""
 
@@ -15,7 +15,7 @@ G = np.load(os.path.join(os.path.dirname(__file__), "golden", "c1_golden.npz"))
 
 def test_quickstart_steps_match_reference():
     s = QuickStartStep((64, 64), (1.0, 1.0), G["psi0"])
-    for k in range(3):
+    for k in range(6):
         dt = float(G[f"s{k}/dt"])
         if k > 0:   # the reference's CFL time step from the previous state (convective + capillary bounds)
             assert ostep.cfl_dt(s.vel, s.mu, s.rho, (1.0, 1.0), (64, 64), 0.3, We=10.0, rho_ratio=0.1) == dt
