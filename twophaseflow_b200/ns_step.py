@@ -25,7 +25,7 @@ import ctypes as C
 from types import SimpleNamespace
 
 from . import _lib
-from .advection import FCCDLevelSetAdvection, FCCDSolver, SplitReinitializer
+from .advection import FCCDLevelSetAdvection, FCCDSolver, SplitReinitializer, UCCD6ConvectionTerm
 from .ccd import CCDSolver
 from .levelset import CurvatureCalculatorPsi, update_properties
 from .ppe import PPESolverFVMMatrixFree
@@ -47,7 +47,17 @@ class TwoPhaseStep:
     rho_l = mu_l = 1, rho_g = rho_ratio, mu_g = mu_ratio."""
 
     def __init__(self, grid, psi, Re=100.0, Fr=1.0, We=10.0, rho_ratio=1e-3, mu_ratio=1e-2, cfl=0.3,
-                 eps=None, reinit_steps=4, ppe_tol=1e-8, ppe_maxiter=20000, use_graphs=True):
+                 eps=None, reinit_steps=4, ppe_tol=1e-8, ppe_maxiter=20000, use_graphs=True,
+                 convection="ccd", transport_mass_correction=False, reinit_bc="zero", ppe_method="cg",
+                 no_slip=False):
+        """The keyword options after ``use_graphs`` select the reference
+        quick-start pipeline's components (simulation/_core.py:126-172):
+        ``convection="uccd6"``, ``transport_mass_correction=True``,
+        ``reinit_bc="neumann"``, ``ppe_method="gmres"`` (GMRES(80) with the
+        exact line preconditioner) and ``no_slip=True`` (every velocity
+        component zeroed on every wall plane of u* and of the corrected u,
+        simulation/boundary_condition.py:22-70).  The defaults keep the
+        CCD convection, Jacobi-PCG composition."""
         torch = _torch()
         self.grid = grid
         nd = grid.ndim
@@ -56,15 +66,22 @@ class TwoPhaseStep:
         self.fccd = FCCDSolver(grid, None, bc_type="wall", ccd_solver=self.ccd)
         h = min(float(grid.L[a] / grid.N[a]) for a in range(nd))
         self.eps = 1.5 * h if eps is None else eps
-        self.transport = FCCDLevelSetAdvection(None, grid, self.fccd)
-        self.reinit = SplitReinitializer(None, grid, self.ccd, self.eps, n_steps=reinit_steps)
+        if convection not in ("ccd", "uccd6"):
+            raise ValueError("convection must be 'ccd' or 'uccd6'")
+        if ppe_method not in ("cg", "gmres"):
+            raise ValueError("ppe_method must be 'cg' (Jacobi) or 'gmres' (line preconditioner)")
+        self.transport = FCCDLevelSetAdvection(None, grid, self.fccd, mass_correction=transport_mass_correction)
+        self.reinit = SplitReinitializer(None, grid, self.ccd, self.eps, n_steps=reinit_steps, bc=reinit_bc)
         self.curv = CurvatureCalculatorPsi(None, self.ccd)
         cfg = SimpleNamespace(grid=SimpleNamespace(ndim=nd), fluid=SimpleNamespace(Re=Re, Fr=Fr, We=We),
                               numerics=SimpleNamespace(cn_viscous=True, cn_mode="picard"))
-        self.predictor = Predictor(None, cfg, self.ccd)
+        conv = UCCD6ConvectionTerm(None, grid, self.ccd) if convection == "uccd6" else None
+        self.predictor = Predictor(None, cfg, self.ccd, convection=conv)
         self.rc = RhieChowInterpolator(None, grid, self.ccd, bc_type="wall")
-        ppe_cfg = SimpleNamespace(pseudo_tol=ppe_tol, pseudo_maxiter=ppe_maxiter, ppe_iteration_method="cg",
-                                  ppe_preconditioner="jacobi")
+        self.no_slip = bool(no_slip)
+        ppe_cfg = SimpleNamespace(pseudo_tol=ppe_tol, pseudo_maxiter=ppe_maxiter, ppe_iteration_method=ppe_method,
+                                  ppe_preconditioner="jacobi" if ppe_method == "cg" else "line_pcr",
+                                  ppe_line_solver="thomas")
         self.ppe = PPESolverFVMMatrixFree(None, ppe_cfg, grid)
         self.corrector = VelocityCorrector(None, grid, self.ccd)
         self.rho_l, self.rho_g, self.mu_l, self.mu_g = 1.0, rho_ratio, 1.0, mu_ratio
@@ -97,6 +114,8 @@ class TwoPhaseStep:
         kappa = self.curv.compute(self.psi)
         st = FlowState(velocity=self.vel, psi=self.psi, rho=self.rho, mu=self.mu, kappa=kappa, pressure=self.p)
         self._vel_star = self.predictor.compute(st, dt)
+        if self.no_slip:
+            self._wall_zero(self._vel_star)
         div = self.rc.face_velocity_divergence(self._vel_star, self.p, self.rho, dt)
         _lib.check(self.lib.tpf_ns_scaled(div.numel(), 2, _lib.dptr(div), None, float(dt), _lib.dptr(self.rhs),
                                           _lib.TPF_F64, _lib.current_stream_handle()))
@@ -106,6 +125,8 @@ class TwoPhaseStep:
         vel = self.corrector.correct(self._vel_star, self.dp, self.rho, dt)
         for c in range(self.nd):
             self.vel[c].copy_(vel[c])
+        if self.no_slip:
+            self._wall_zero(self.vel)
         st = _lib.current_stream_handle()
         _lib.check(self.lib.tpf_visc_accumulate(self.p.numel(), _lib.dptr(self.dp), 1, 0, None, 0.0,
                                                 _lib.dptr(self.p), _lib.TPF_F64, st))
@@ -113,11 +134,17 @@ class TwoPhaseStep:
         _lib.check(self.lib.tpf_cfl_maxima(self.p.numel(), self.nd, ptrs, None, None, _lib.TPF_F64,
                                            _lib.dptr(self.maxima), st))
 
+    def _wall_zero(self, comps):
+        """No-slip: every component zero on both planes of every (wall) axis."""
+        for ax in range(self.nd):
+            for c in comps:
+                self.ccd.enforce_wall_neumann(c, ax)
+
     def _solve(self):
         dp = self.ppe.solve(self.rhs, self.rho)
         self.dp.copy_(dp)
         d = getattr(self.ppe, "last_diagnostics", {}) or {}
-        self.last_ppe_iterations = int(d.get("ppe_low_order_cg_iterations", 0))
+        self.last_ppe_iterations = int(d.get(f"ppe_low_order_{self.ppe.iteration_method}_iterations", 0))
 
     def _capture(self, dt):
         torch = _torch()
