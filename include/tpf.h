@@ -360,14 +360,19 @@ int tpf_ppe_create(tpf_ppe** h, int ndim, const int64_t* N,
 int tpf_ppe_destroy(tpf_ppe* h);
 int tpf_ppe_set_options(tpf_ppe* h, const tpf_ppe_options* opts);
 /* Kernel of the FP64 CG solve (same iteration, same stopping rule):
- * 0 (default) = the band-resident kernel when it applies, else 1;
+ * 0 (default) = the band-resident kernel when it applies, else 3 for 3-D
+ *     FP64 systems, else 1;
  * 1 = one persistent cooperative launch with every vector in global memory
  *     (any grid, FP64 or mixed);
  * 2 = the band-resident kernel: 2-D systems whose nodes, split into one
  *     contiguous range per SM (at least one row each, at most 768 nodes per
  *     row), fit in shared memory with 12 vectors (513^2 on a B200); only the
  *     ranges' first and last rows cross L2 each iteration.
- *     TPF_EINVAL from tpf_ppe_solve when it does not apply. */
+ *     TPF_EINVAL from tpf_ppe_solve when it does not apply;
+ * 3 = streaming (FP64): each iteration as two ordinary full-occupancy
+ *     kernels (vector update; stencil + inner products, the last block
+ *     advancing the scalars on the device), chunks of 32 iterations
+ *     replayed from a CUDA graph.  The mixed-precision route keeps 1. */
 int tpf_ppe_set_cg_kernel(tpf_ppe* h, int kind);
 
 /* Build face coefficients, Jacobi diagonal and line-preconditioner state
@@ -406,6 +411,51 @@ int tpf_ppe_solve(tpf_ppe* h, const double* rhs, const double* rho, double* p,
 int tpf_ppe_solve_batched(tpf_ppe* const* handles, int n, const double* const* rhs, const double* const* rho,
                           double* const* p, void* stream, tpf_ppe_result* results);
 
+/* ---- FCCD matrix-free PPE ----------------------------------------------
+ *
+ * Replaces PPESolverFCCDMatrixFree on its default path
+ * (src/twophase/ppe/fccd_matrixfree.py:105-611: constructor :117-215, apply
+ * :378-398, operator core :400-428, solve :506-611, wall divergence
+ * :762-829; face gradient src/twophase/ccd/fccd.py:243-277; Jacobi inverse
+ * ppe/fccd_matrixfree_helpers.py:251-265): phase-density face coefficients
+ * 2/(rho_L + rho_R), no interface coupling, full boundary faces, the legacy
+ * operator pairing, SciPy GMRES (ppe/gmres_helpers.py:16-80) with the Jacobi
+ * or no preconditioner.  Uniform grids; every axis wall or periodic. */
+typedef struct tpf_fccd_ppe tpf_fccd_ppe;
+
+typedef struct tpf_fccd_ppe_options {
+  double tol;        /* GMRES relative tolerance (pseudo_tol, default 1e-8)        */
+  int64_t maxiter;   /* GMRES restart cycles (pseudo_maxiter, default 500)          */
+  int restart;       /* ppe_restart; 20 (SciPy's default) when the config has none  */
+  int precond;       /* TPF_PRECOND_NONE (default) or TPF_PRECOND_JACOBI           */
+} tpf_fccd_ppe_options;
+
+void tpf_fccd_ppe_default_options(tpf_fccd_ppe_options* o);
+
+/* ndim (2 or 3) axes of N[a] cells; coords[a]: HOST arrays of N[a]+1 node
+ * coordinates (face weights H = x1 - x0, control-volume widths); h_ccd[a]:
+ * the CCD spacing (L/N); periodic[a]: nonzero for a periodic axis; pin: the
+ * pinned node (the reference's BoundarySpec.pin_dof, the centre node).
+ * Allocates the handle's device state and one CCD plan per axis. */
+int tpf_fccd_ppe_create(tpf_fccd_ppe** h, int ndim, const int64_t* N, const double* const* coords,
+                        const double* h_ccd, const int* periodic, int64_t pin, const tpf_fccd_ppe_options* o);
+int tpf_fccd_ppe_destroy(tpf_fccd_ppe* h);
+int tpf_fccd_ppe_set_options(tpf_fccd_ppe* h, const tpf_fccd_ppe_options* o);
+/* prepare_operator (fccd_matrixfree_lifecycle.py:44-95): keeps a device copy
+ * of rho and forms the Jacobi inverse diagonal.  The first call also runs
+ * one operator application (synchronizes `stream`). */
+int tpf_fccd_ppe_prepare(tpf_fccd_ppe* h, const double* rho, void* stream);
+/* out = L p with the pinned and periodic-image rows (apply, :378-398);
+ * p and out distinct device arrays of the grid's nodes. */
+int tpf_fccd_ppe_apply(tpf_fccd_ppe* h, const double* p, double* out, void* stream);
+/* the Jacobi inverse diagonal of the last prepare, into out */
+int tpf_fccd_ppe_diag_inv(tpf_fccd_ppe* h, double* out, void* stream);
+/* solve (:506-611): prepare(rho), GMRES on the rhs with the pinned and image
+ * rows zeroed, p[pin] = 0, images synchronised.  Synchronizes `stream`;
+ * TPF_ENOCONV when GMRES does not converge (info = maxiter). */
+int tpf_fccd_ppe_solve(tpf_fccd_ppe* h, const double* rhs, const double* rho, double* p, const double* p_init,
+                       void* stream, tpf_ppe_result* result);
+
 /* ---- allocation-free CG solve (no counterpart in the reference) ----------
  *
  * For callers that cannot allocate device memory while they run: a host whose
@@ -418,16 +468,26 @@ int tpf_ppe_solve_batched(tpf_ppe* const* handles, int n, const double* const* r
  * call issues no cudaMalloc / cudaFree and calls no allocating library.
  *
  * Limits: at most TPF_PPE_STATIC_MAX_DOF nodes in total (e.g. 256 x 256 cells
- * in 2-D, 40 x 40 x 40 in 3-D) and TPF_PPE_STATIC_MAX_AXIS nodes per axis;
- * larger grids are rejected with TPF_EINVAL (use tpf_ppe_create /
+ * in 2-D, 39 x 39 x 39 cells in 3-D) and TPF_PPE_STATIC_MAX_AXIS nodes per
+ * axis; larger grids are rejected with TPF_EINVAL (use tpf_ppe_create /
  * tpf_ppe_solve).  coords[a] are HOST arrays of N[a]+1 node coordinates (as
  * for tpf_ppe_create); rhs, rho, p, p_init are device arrays of the grid's
- * nodes.  The first call on a device looks up the workspace address for that
- * device; a caller that will capture work into a stream should make one call
- * on each device beforehand.  All calls on one device share the workspace:
- * calls that overlap in time on the same device (two host threads, or two
- * streams without ordering between them) race and must be serialised by the
- * caller.  Synchronizes `stream`; returns TPF_ENOCONV like tpf_ppe_solve. */
+ * nodes.
+ *
+ * Set-up: the first call on a device (with that device current) looks up the
+ * workspace's device address and keeps it for later calls on that device.
+ * Under CUDA's lazy module loading that lookup is also what loads the module
+ * holding the array, so the array's device memory is reserved by that first
+ * call: make it at start-up, before any stream capture and before a fixed
+ * memory budget is measured.  The kept address is not valid after
+ * cudaDeviceReset on that device; the entry point must not be used after one.
+ *
+ * All calls on one device share the workspace, which keeps the last call's
+ * contents (each call initialises what it reads): calls that overlap in time
+ * on the same device (two host threads, or two streams without ordering
+ * between them) race and must be serialised by the caller.  The call waits
+ * for `stream` to drain before it returns (it reads the solve status back);
+ * returns TPF_ENOCONV like tpf_ppe_solve. */
 #define TPF_PPE_STATIC_MAX_DOF 66049
 #define TPF_PPE_STATIC_MAX_AXIS 4097
 int tpf_ppe_solve_cg_static(int ndim, const int64_t* N, const double* const* coords,

@@ -2,7 +2,9 @@
 
 Run in a container that has the reference source tree (not needed at test time):
 
-    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py /root/reference/src
+    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py <reference>/src [only ...]
+
+or with the source directory in ``TWOPHASE_REFERENCE_SRC``.
 
 It imports the reference's ``twophase`` package read-only, runs its own CPU
 functions (``CCDSolver.differentiate``, ``PPESolverFVMMatrixFree``,
@@ -640,9 +642,18 @@ def make_c1(out):
 
 
 def main():
-    """Usage: make_golden.py [reference src dir] [only: ccd|ppe|step|levelset|rhiechow|advect|reinit|viscous|predictor|fccd_ppe|c1 ...]."""
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
-    only = set(sys.argv[2:])
+    """Usage: make_golden.py <reference src dir> [only: ccd|ppe|step|levelset|rhiechow|advect|reinit|viscous|predictor|fccd_ppe|c1 ...].
+
+    The source directory comes from the first argument or, when the
+    argument list is empty, from the TWOPHASE_REFERENCE_SRC environment variable."""
+    args = sys.argv[1:]
+    if args and os.path.isdir(os.path.join(args[0], "twophase")):
+        src, only = args[0], set(args[1:])
+    else:
+        src, only = os.environ.get("TWOPHASE_REFERENCE_SRC", ""), set(args)
+    if not src or not os.path.isdir(os.path.join(src, "twophase")):
+        raise SystemExit("make_golden.py: give the reference's src directory as the first argument "
+                         "or in TWOPHASE_REFERENCE_SRC")
     _ref_import(src)
     makers = {"ccd": make_ccd, "ppe": make_ppe, "step": make_step, "levelset": make_levelset,
               "rhiechow": make_rhiechow, "advect": make_advect, "reinit": make_reinit,

@@ -1,0 +1,135 @@
+"""The FCCD matrix-free PPE on the GPU (PPESolverFCCDMatrixFree, tpf_fccd_ppe_*)
+against the reference's own outputs (tests/golden/fccd_ppe_golden.npz, written
+by tests/golden/make_golden.py from the reference's PPESolverFCCDMatrixFree)
+and against the oracle (oracle/fccd_ppe.py, bit-identical to those outputs).
+
+Bars: the operator within 1e-12 of max|ref| (the CCD second derivative
+inside the face gradient rounds differently from LAPACK; everything else is
+the reference's arithmetic in the same order); the Jacobi inverse diagonal
+bit for bit; solutions whose true residual, measured with the oracle's
+operator, meets the solve tolerance, within 1e-6 of the reference's solution
+and with a GMRES inner iteration count within 2 of the reference's.
+"""
+
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from oracle.fccd_ppe import FCCDPPE
+
+pytestmark = pytest.mark.gpu
+
+G = np.load(os.path.join(os.path.dirname(__file__), "golden", "fccd_ppe_golden.npz"))
+CASES = ["wall2d", "per2d", "wall3d"]
+
+
+class _Cfg:
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+
+
+def _gpu_solver(N, L, bc, pre, tol=1e-9, restart=None):
+    from twophaseflow_b200 import FCCDSolver, PPESolverFCCDMatrixFree, UniformGrid
+    grid = UniformGrid(tuple(int(n) for n in N), tuple(float(x) for x in L))
+    fccd = FCCDSolver(grid, None, bc_type=bc)
+    cfg = _Cfg(pseudo_tol=tol, pseudo_maxiter=500, ppe_restart=restart, ppe_preconditioner=pre)
+    return PPESolverFCCDMatrixFree(None, cfg, grid, fccd)
+
+
+def _case(name):
+    return G[f"{name}/N"], G[f"{name}/L"], str(G[f"{name}/bc"]), str(G[f"{name}/pre"])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fccd_apply_and_jacobi_match_reference(cuda_device, name):
+    import torch
+    N, L, bc, pre = _case(name)
+    s = _gpu_solver(N, L, bc, pre)
+    s.prepare_operator(torch.from_numpy(G[f"{name}/rho"]).to(cuda_device))
+    out = s.apply(torch.from_numpy(G[f"{name}/p"]).to(cuda_device)).cpu().numpy()
+    ref = G[f"{name}/apply"]
+    err = np.abs(out - ref).max() / np.abs(ref).max()
+    assert err <= 1e-12, err
+    if pre == "jacobi":
+        np.testing.assert_array_equal(s.jacobi_inverse_diagonal().cpu().numpy(), G[f"{name}/diag_inv"])
+    # host NumPy in, host NumPy out (the reference's CPU call shape)
+    out_h = s.apply(G[f"{name}/p"])
+    assert isinstance(out_h, np.ndarray)
+    np.testing.assert_array_equal(out_h, out)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fccd_solve_matches_reference(cuda_device, name):
+    import torch
+    N, L, bc, pre = _case(name)
+    rho, rhs = G[f"{name}/rho"], G[f"{name}/rhs"]
+    s = _gpu_solver(N, L, bc, pre)
+    p = s.solve(torch.from_numpy(rhs).to(cuda_device), torch.from_numpy(rho).to(cuda_device)).cpu().numpy()
+    o = FCCDPPE(L, N, bc, tol=1e-9, maxiter=500, preconditioner=pre)
+    sol, info, its = o.solve(rhs, rho)
+    np.testing.assert_array_equal(sol, G[f"{name}/sol"])   # the oracle is the reference here
+    d = s.last_diagnostics
+    assert d["ppe_linear_info"] == 0
+    assert abs(d["ppe_gmres_iterations"] - its) <= 2, (d, its)
+    # the GPU solution's true residual on the oracle's operator
+    b = np.array(rhs, copy=True)
+    b.ravel()[o.pin] = 0.0
+    if o.images is not None:
+        b.ravel()[o.images] = 0.0
+    r = o.apply(p) - b
+    assert np.linalg.norm(r) <= 2e-9 * np.linalg.norm(b), np.linalg.norm(r) / np.linalg.norm(b)
+    assert float(p.ravel()[o.pin]) == 0.0
+    err = np.abs(p - sol).max() / np.abs(sol).max()
+    assert err <= 1e-6, err
+
+
+@pytest.mark.parametrize("N,bc", [((256, 256), "wall"), ((128, 96), "periodic"), ((48, 40, 56), "wall"),
+                                  ((32, 32, 32), "periodic")])
+def test_fccd_apply_matches_oracle_large(cuda_device, N, bc):
+    """Larger grids than the golden cases, every axis, against the oracle."""
+    import torch
+    L = tuple(1.0 + 0.1 * a for a in range(len(N)))
+    rng = np.random.default_rng(7)
+    shape = tuple(n + 1 for n in N)
+    rho = 0.2 + rng.uniform(0.0, 1.0, shape)
+    p = rng.standard_normal(shape)
+    o = FCCDPPE(L, N, bc)
+    o.prepare(rho)
+    ref = o.apply(p)
+    s = _gpu_solver(N, L, bc, "none")
+    s.prepare_operator(torch.from_numpy(rho).to(cuda_device))
+    out = s.apply(torch.from_numpy(p).to(cuda_device)).cpu().numpy()
+    err = np.abs(out - ref).max() / np.abs(ref).max()
+    assert err <= 1e-12, err
+
+
+def test_fccd_zero_rhs_and_warm_start(cuda_device):
+    """A zero right-hand side gives p = 0 without iterating; a warm start at
+    the solution converges at once to the same field."""
+    import torch
+    N, L, bc, pre = _case("wall2d")
+    rho = torch.from_numpy(G["wall2d/rho"]).to(cuda_device)
+    s = _gpu_solver(N, L, bc, pre)
+    z = s.solve(torch.zeros_like(rho), rho)
+    assert float(z.abs().max()) == 0.0
+    rhs = torch.from_numpy(G["wall2d/rhs"]).to(cuda_device)
+    p = s.solve(rhs, rho)
+    p2 = s.solve(rhs, rho, p_init=p)
+    assert s.last_diagnostics["ppe_gmres_iterations"] <= 2
+    assert float((p2 - p).abs().max()) <= 1e-8 * float(p.abs().max())
+
+
+def test_fccd_rejects_unsupported_options(cuda_device):
+    from twophaseflow_b200 import FCCDSolver, PPESolverFCCDMatrixFree, UniformGrid
+    grid = UniformGrid((16, 16))
+    fccd = FCCDSolver(grid, None, bc_type="wall")
+    with pytest.raises(ValueError, match="preconditioner"):
+        PPESolverFCCDMatrixFree(None, _Cfg(ppe_preconditioner="line_pcr"), grid, fccd)
+    with pytest.raises(NotImplementedError):
+        PPESolverFCCDMatrixFree(None, _Cfg(ppe_coefficient_scheme="phase_separated"), grid, fccd)
+    s = PPESolverFCCDMatrixFree(None, _Cfg(), grid, fccd)
+    with pytest.raises(RuntimeError, match="prepare_operator"):
+        s.apply(np.zeros(grid.shape))

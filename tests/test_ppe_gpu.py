@@ -270,3 +270,52 @@ def test_band_resident_pcg_is_refused_where_it_does_not_apply(cuda_device):
         _lib.check(lib.tpf_ppe_set_cg_kernel(s._handle, C.c_int(2)))
         with pytest.raises(ValueError):
             s.solve(divergence_rhs(N, seed=1), droplet_density(N, seed=2))
+
+
+@pytest.mark.parametrize("N,precond", [((40, 36, 44), "jacobi"), ((96, 80), "jacobi"), ((24, 20, 28), "none")])
+def test_streaming_pcg_matches_persistent_kernel(cuda_device, N, precond):
+    """The streaming PCG (two full-occupancy kernels per iteration, chunks of
+    iterations replayed from a CUDA graph; the default for 3-D) against the
+    persistent cooperative kernel on the same system: the same recurrences,
+    so iteration counts within 1 and solutions within 1e-10 of max|p|; both
+    against the oracle's PCG iteration count."""
+    import ctypes
+    from twophaseflow_b200 import PPESolverFVMMatrixFree, UniformGrid, _lib
+    rho = droplet_density(N, seed=3, rho_g=1e-2)
+    rhs = divergence_rhs(N, seed=4)
+    cfg = _Cfg(pseudo_tol=1e-10, pseudo_maxiter=100000, ppe_iteration_method="cg", ppe_preconditioner=precond)
+    out = {}
+    for kind in (1, 3):
+        s = PPESolverFVMMatrixFree(None, cfg, UniformGrid(N))
+        _lib.check(s.lib.tpf_ppe_set_cg_kernel(s._handle, kind))
+        for _ in range(2):   # the second solve replays the captured chunk graph
+            p = s.solve(rhs, rho)
+        out[kind] = (p, s.last_diagnostics["ppe_low_order_cg_iterations"])
+    coords = oppe.uniform_coords(N, (1.0,) * len(N))
+    o = oppe.FVMMatrixFree(coords, method="cg", preconditioner=precond, tol=1e-10, maxiter=100000)
+    po = o.solve(rhs, rho)
+    (p1, i1), (p3, i3) = out[1], out[3]
+    assert abs(i1 - i3) <= 1, (i1, i3)
+    assert abs(i3 - o.last_iterations) <= max(2, o.last_iterations // 100), (i3, o.last_iterations)
+    scale = np.abs(p1).max()
+    assert np.abs(p3 - p1).max() <= 1e-10 * scale
+    assert np.abs(p3 - po).max() <= 1e-8 * np.abs(po).max()
+    assert float(p3.ravel()[int(np.ravel_multi_index(tuple(n // 2 for n in N), tuple(n + 1 for n in N)))]) == 0.0
+
+
+def test_streaming_pcg_budget_and_zero_rhs(cuda_device):
+    """maxiter reached -> RuntimeError with info = maxiter; a zero right-hand
+    side returns p = 0 without iterating (3-D, streaming kernel)."""
+    from twophaseflow_b200 import PPESolverFVMMatrixFree, UniformGrid
+    N = (16, 18, 20)
+    rho = droplet_density(N, seed=5)
+    rhs = divergence_rhs(N, seed=6)
+    s = PPESolverFVMMatrixFree(None, _Cfg(pseudo_tol=1e-12, pseudo_maxiter=7, ppe_iteration_method="cg",
+                                          ppe_preconditioner="jacobi"), UniformGrid(N))
+    with pytest.raises(RuntimeError, match="info=7"):
+        s.solve(rhs, rho)
+    assert s.last_diagnostics["ppe_low_order_cg_iterations"] == 7
+    s2 = PPESolverFVMMatrixFree(None, _Cfg(pseudo_tol=1e-10, pseudo_maxiter=100, ppe_iteration_method="cg",
+                                           ppe_preconditioner="jacobi"), UniformGrid(N))
+    p = s2.solve(np.zeros_like(rhs), rho)
+    assert np.abs(p).max() == 0.0 and s2.last_diagnostics["ppe_low_order_cg_iterations"] == 0

@@ -1,10 +1,13 @@
 """The allocation-free CG entry point (tpf_ppe_solve_cg_static) against the
 handle-based solve (tpf_ppe_solve, CG, FP64), both called through the C ABI.
 
-The static entry point runs the same kernels on the same grid shape, so its
+The entry point is for callers that cannot allocate device memory while they
+run (a caching allocator that already holds the device, a memory budget fixed
+at start-up).  It runs the same kernels on the same grid shape, so its
 iterates match the handle path: the test asks for the same iteration count and
 solutions within 1e-12 of the solution's magnitude, on two calls in a row (the
-second call reuses the workspace left by the first).
+second call reuses the workspace left by the first), and checks that a call
+after the first leaves the device's free memory unchanged.
 """
 
 from __future__ import annotations
@@ -59,6 +62,7 @@ CASES = [
     ((96, 40), "none"),
     ((24, 20, 28), "jacobi"),
     ((256, 256), "jacobi"),
+    ((39, 39, 39), "jacobi"),   # 40^3 = 64 000 nodes: the 3-D size at the limit
 ]
 
 
@@ -93,6 +97,31 @@ def test_static_cg_matches_handle_solve(cuda_device, N, precond):
         err = float((p - p_ref).abs().max())
         assert err <= 1e-12 * scale, (call, err, scale)
         assert float(p.flatten()[pin]) == 0.0
+
+
+def test_static_cg_allocates_no_device_memory(cuda_device):
+    """After the first call on the device (which looks the workspace up and,
+    under lazy module loading, loads it), further calls change the device's
+    free memory by nothing: no cudaMalloc, no allocating library call."""
+    import torch
+    lib = _lib.load()
+    N = (128, 128)
+    coords = node_coords(N)
+    rho_d = torch.from_numpy(droplet_density(N, n_drops=6, rho_g=1e-2)).to(cuda_device)
+    rhs_d = torch.from_numpy(divergence_rhs(N)).to(cuda_device)
+    p = torch.zeros_like(rho_d)
+    stream = _lib.current_stream_handle()
+    _static_solve(lib, N, coords, 0, rhs_d, rho_d, p, _lib.TPF_PRECOND_JACOBI, 1e-10, 20000, stream)
+    torch.cuda.synchronize()
+    reserved = torch.cuda.memory_reserved()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(2):
+        r = _static_solve(lib, N, coords, 0, rhs_d, rho_d, p, _lib.TPF_PRECOND_JACOBI, 1e-10, 20000, stream)
+        assert r.info == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    assert torch.cuda.memory_reserved() == reserved
 
 
 def test_static_cg_rejects_oversize_and_bad_arguments(cuda_device):

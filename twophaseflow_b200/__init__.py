@@ -5,6 +5,8 @@
   ``twophase.ppe.fvm_matrixfree.PPESolverFVMMatrixFree`` (an ``IPPESolver``)
 * ``CCDVariableDensityOperator`` / ``PPESolverDefectCorrection`` -- the CCD
   variable-density operator L_H and the defect-correction PPE loop
+* ``PPESolverFCCDMatrixFree`` -- drop-in for
+  ``twophase.ppe.fccd_matrixfree.PPESolverFCCDMatrixFree`` (default path)
 * ``register_with_reference`` -- installs the PPE solver in the reference's
   ``register_ppe_solver`` registry.
 * ``VelocityCorrector`` / ``CFLCalculator`` / ``ccd_pressure_gradient`` -- the
@@ -18,6 +20,7 @@ All arithmetic runs in the in-tree CUDA library ``libtpf.so`` (C ABI:
 from .advection import FCCDLevelSetAdvection, FCCDSolver, SplitReinitializer, UCCD6ConvectionTerm
 from .ccd import CCDSolver
 from .ccd_ppe import CCDVariableDensityOperator, PPESolverDefectCorrection
+from .fccd_ppe import PPESolverFCCDMatrixFree
 from .grid import BoundarySpec, UniformGrid
 from .ppe import (MatrixAssemblyUnavailable, PPESolverFVMMatrixFree, create_fvm_matrixfree, register_with_reference,
                   solve_batched)
@@ -36,6 +39,7 @@ __all__ = [
     "CCDVariableDensityOperator",
     "PPESolverDefectCorrection",
     "PPESolverFVMMatrixFree",
+    "PPESolverFCCDMatrixFree",
     "MatrixAssemblyUnavailable",
     "create_fvm_matrixfree",
     "register_with_reference",

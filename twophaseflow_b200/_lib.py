@@ -50,6 +50,15 @@ class tpf_ppe_result(C.Structure):
     ]
 
 
+class tpf_fccd_ppe_options(C.Structure):
+    _fields_ = [
+        ("tol", C.c_double),
+        ("maxiter", C.c_int64),
+        ("restart", C.c_int),
+        ("precond", C.c_int),
+    ]
+
+
 class tpf_learned_options(C.Structure):
     _fields_ = [
         ("tol", C.c_double),
@@ -102,6 +111,17 @@ SIGNATURES = {
     "tpf_rc_divergence_axis": (C.c_int, [C.c_int, C.POINTER(C.c_int64), C.c_int, C.c_int, C.c_double, C.c_double,
                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
+    "tpf_fccd_ppe_default_options": (None, [C.c_void_p]),
+    "tpf_fccd_ppe_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_int64),
+                                      C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.c_double), C.POINTER(C.c_int),
+                                      C.c_int64, C.c_void_p]),
+    "tpf_fccd_ppe_destroy": (C.c_int, [C.c_void_p]),
+    "tpf_fccd_ppe_set_options": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "tpf_fccd_ppe_prepare": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tpf_fccd_ppe_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tpf_fccd_ppe_diag_inv": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "tpf_fccd_ppe_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p]),
     "tpf_fccd_product": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "tpf_fccd_flux_divergence_axis": (C.c_int, [C.c_int, C.POINTER(C.c_int64), C.c_int, C.c_int, C.c_double,
                                                 C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),

@@ -145,9 +145,17 @@ class FCCDLevelSetAdvection:
             self._dV = torch.from_numpy(np.ascontiguousarray(vol, dtype=np.float64)).to(dev)
             self._partials = torch.empty(2048, dtype=torch.float64, device=dev)
 
-    def advance(self, psi, velocity_components: List, dt: float, clip_bounds=(0.0, 1.0)):
+    def advance(self, psi, velocity_components: List, dt: float, clip_bounds=(0.0, 1.0), velocity_is_zero=False):
         """psi after one RK3 step; psi's periodic image nodes are synchronised in
-        place first, as the reference does."""
+        place first, as the reference does.
+
+        ``velocity_is_zero=True`` is the caller's statement that every velocity
+        component is exactly zero.  The reference's CPU backend tests this
+        itself and then skips the RK3 stages, returning the clipped (and
+        mass-corrected) psi (fccd_advection.py:99-110); its GPU backend has
+        no such shortcut.  The stages would leave psi within an ulp, but not
+        bit-equal (0.75 q + 0.25 q), so callers that compare with the CPU
+        reference pass the flag when they know the velocity is zero."""
         import numpy as np
         torch = _torch()
         fccd = self._fccd
@@ -175,7 +183,14 @@ class FCCDLevelSetAdvection:
         clip = clip_bounds is not None
         lo, hi = (float(clip_bounds[0]), float(clip_bounds[1])) if clip else (0.0, 0.0)
         coeffs = ((1, 0.0, 0.0), (2, 0.75, 0.25), (3, 1.0 / 3.0, 2.0 / 3.0))
-        q = q0
+        if velocity_is_zero:
+            coeffs = ()   # stage 0 below: q0 copied through the clip and the image sync
+            nxt = torch.empty_like(q0)
+            _lib.check(lib.tpf_tvd_rk3_stage(q0.dim(), shape, per, 0, 0.0, 0.0, 0.0, None, _lib.dptr(q0), None,
+                                             1 if clip else 0, lo, hi, _lib.dptr(nxt), tdt, st))
+            q = nxt
+        else:
+            q = q0
         for stage, ca, cb in coeffs:
             L = fccd._rhs_tensors(vel, q)[0]
             nxt = torch.empty_like(q0)

@@ -1,0 +1,471 @@
+// Restarted GMRES on the device: SciPy 1.18.1's left-preconditioned gmres
+// (scipy/sparse/linalg/_isolve/iterative.py) with its gh-8400 inner
+// tolerance control, restated for CUDA.  The Hessenberg matrix, the Givens
+// rotations and the residual vector live on the device; the host reads one
+// small state block per restart cycle.  Classical Gram-Schmidt with a
+// conditional re-orthogonalization pass stands in for SciPy's modified
+// Gram-Schmidt (the same basis up to rounding).  Every kernel of an Arnoldi
+// column skips its work once the device-side state marks the cycle done, so
+// a whole cycle (m columns) is captured once as a CUDA graph and replayed.
+//
+// The operator, the residual and the preconditioner are the caller's
+// (functors enqueueing kernels on a stream): the FVM PPE (ppe.cu) and the
+// FCCD PPE (fccd_ppe.cu) share this driver.
+#pragma once
+
+#include "tpf_common.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace {
+
+// ---- GMRES building blocks ---------------------------------------------------------
+
+struct GmState {
+  int done;          // inner loop finished (presid <= ptol or breakdown)
+  int breakdown;
+  int ncols;         // columns completed in this cycle
+  int reorth;        // second Gram-Schmidt pass requested
+  double presid;
+  double ptol;
+  double h0;         // ||w|| before orthogonalization
+  double wn2;        // ||w||^2 scratch
+  double rnorm;      // true residual norm (end of cycle)
+  double scal;       // scale factor for the new basis vector
+};
+
+// partial dots: part[k*nb + block] = <V_k, w> for k < ncols, part[ncols*nb+block] = <w,w>
+// Block partials of <V_k, w> for k < ncols and of <w, w> (k = ncols):
+// part[k * nb + block].  The vectors are taken eight at a time in one sweep
+// over w, with one block reduction per group (warp j reduces vector j of the
+// group with the same shuffle tree a one-vector reduction uses).
+__global__ void mdot_kernel(int ndof, const double* __restrict__ V, int ncols, const double* __restrict__ w,
+                            double* part, const int* done) {
+  if (done && *done) return;
+  constexpr int KC = 8;   // vectors per sweep (<= warps per block)
+  extern __shared__ double sh[];   // [KC][32]
+  const int nb = gridDim.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int k0 = 0; k0 <= ncols; k0 += KC) {
+    double acc[KC];
+#pragma unroll
+    for (int j = 0; j < KC; ++j) acc[j] = 0.0;
+    // two elements per trip: 18 independent loads in flight per thread
+    const int stride = gridDim.x * blockDim.x;
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    for (; idx + stride < ndof; idx += 2 * stride) {
+      const double wa = w[idx], wb = w[idx + stride];
+      double va[KC], vb[KC];
+#pragma unroll
+      for (int j = 0; j < KC; ++j) {
+        const int k = k0 + j;
+        va[j] = (k < ncols) ? V[(size_t)k * ndof + idx] : wa;
+        vb[j] = (k < ncols) ? V[(size_t)k * ndof + idx + stride] : wb;
+      }
+#pragma unroll
+      for (int j = 0; j < KC; ++j) {
+        if (k0 + j <= ncols) {
+          acc[j] += va[j] * wa;
+          acc[j] += vb[j] * wb;
+        }
+      }
+    }
+    if (idx < ndof) {
+      const double wi = w[idx];
+#pragma unroll
+      for (int j = 0; j < KC; ++j) {
+        const int k = k0 + j;
+        if (k <= ncols) acc[j] += ((k < ncols) ? V[(size_t)k * ndof + idx] : wi) * wi;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < KC; ++j) {
+      const double v = tpf::warp_sum(acc[j]);
+      if (lane == 0) sh[j * 32 + wid] = v;
+    }
+    __syncthreads();
+    if (wid < KC && k0 + wid <= ncols) {
+      double t = (lane < nw) ? sh[wid * 32 + lane] : 0.0;
+      t = tpf::warp_sum(t);
+      if (lane == 0) part[(size_t)(k0 + wid) * nb + blockIdx.x] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// sum partials -> out[k] (k <= ncols); mode selects how the state uses them.
+// mode 0: first GS pass (h column = dots, h0 = sqrt(<w,w>)), decide re-orth
+// mode 1: second pass (h column += dots)
+// mode 2: plain norm -> out[0] = sqrt(<w,w>)
+// One block; warp j sums the partials of vectors j, j + nwarps, ... (lane l:
+// blocks l, l + 32, ..., then a shuffle tree), so all vectors are summed at
+// once; thread 0 then applies the mode's scalar logic in vector order.
+__global__ void mdot_finalize_kernel(const double* part, int nb, int ncols, double* hcol, GmState* st,
+                                     int mode, double* out_norm) {
+  if (mode != 2 && st->done) return;
+  if (mode == 1 && !st->reorth) return;
+  extern __shared__ double sums[];   // [ncols + 1]
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int k = wid; k <= ncols; k += nw) {
+    double acc = 0.0;
+    for (int b = lane; b < nb; b += 32) acc += part[(size_t)k * nb + b];
+    acc = tpf::warp_sum(acc);
+    if (lane == 0) sums[k] = acc;
+  }
+  __syncthreads();
+  if (mode == 2) {
+    if (threadIdx.x == 0) *out_norm = sqrt(sums[0]);
+    return;
+  }
+  if (mode == 1) {
+    for (int k = threadIdx.x; k < ncols; k += blockDim.x) hcol[k] += sums[k];
+    if (threadIdx.x == 0) st->wn2 = 0.0;
+    return;
+  }
+  for (int k = threadIdx.x; k < ncols; k += blockDim.x) hcol[k] = sums[k];
+  if (threadIdx.x == 0) {
+    const double sw = sums[ncols];
+    st->h0 = sqrt(sw);
+    double proj = 0.0;
+    for (int q = 0; q < ncols; ++q) proj += sums[q] * sums[q];
+    st->reorth = (sw - proj < 0.5 * sw) ? 1 : 0;
+  }
+}
+
+// w -= sum_k c_k V_k  (c = hcol, or the second-pass dots in part-summed form)
+__global__ void maxpy_kernel(int ndof, const double* __restrict__ V, int ncols, const double* coef, double* w,
+                             const GmState* st, int pass) {
+  if (st->done) return;
+  if (pass == 1 && !st->reorth) return;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += gridDim.x * blockDim.x) {
+    double acc = w[idx];
+#pragma unroll 8
+    for (int k = 0; k < ncols; ++k) acc -= coef[k] * V[(size_t)k * ndof + idx];
+    w[idx] = acc;
+  }
+}
+
+// Givens rotation generator for real (f, g): c f + s g = r, -s f + c g = 0,
+// r carries the sign of f (the convention of LAPACK's lartg).
+__device__ void givens_rot(double f, double g, double& c, double& s, double& r) {
+  if (g == 0.0) { c = 1.0; s = 0.0; r = f; return; }
+  if (f == 0.0) { c = 0.0; s = (g > 0.0) ? 1.0 : -1.0; r = fabs(g); return; }
+  double d = hypot(f, g);
+  c = fabs(f) / d;
+  r = copysign(d, f);
+  s = g / r;
+}
+
+// Finish Arnoldi column `col`: h1, breakdown, rotations, S, presid, done flag.
+// H is stored like SciPy's h[col, k] (row col = column of the Hessenberg matrix).
+// New Hessenberg column: fold in the second-pass coefficients, apply the
+// previous Givens rotations, generate this column's rotation and update the
+// residual vector S.  The block stages the column and the rotations in
+// shared memory; thread 0 applies them in order (the same arithmetic as a
+// serial pass over global memory, without its dependent round trips).
+__global__ void gm_column_kernel(double* H, int ldh, double* givens, double* S, GmState* st, int col,
+                                 const double* w_norm, const double* hcol2) {
+  if (st->done) return;
+  extern __shared__ double shc[];       // [col + 2] column, then [2 col] rotations
+  double* sg = shc + col + 2;
+  double* hc = H + (size_t)col * ldh;
+  const bool reorth = st->reorth != 0;
+  for (int k = threadIdx.x; k <= col; k += blockDim.x) {
+    double v = hc[k];
+    if (reorth) v += hcol2[k];   // second-pass coefficients
+    shc[k] = v;
+  }
+  for (int k = threadIdx.x; k < 2 * col; k += blockDim.x) sg[k] = givens[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const double eps = 2.220446049250313e-16;
+    double h1 = *w_norm;
+    shc[col + 1] = h1;
+    int breakdown = 0;
+    if (h1 <= eps * st->h0) {
+      shc[col + 1] = 0.0;
+      breakdown = 1;
+      st->scal = 1.0;
+    } else {
+      st->scal = 1.0 / h1;
+    }
+    for (int k = 0; k < col; ++k) {
+      const double c = sg[2 * k], s = sg[2 * k + 1];
+      const double n0 = shc[k], n1 = shc[k + 1];
+      shc[k] = c * n0 + s * n1;
+      shc[k + 1] = -s * n0 + c * n1;
+    }
+    double c, s, mag;
+    givens_rot(shc[col], shc[col + 1], c, s, mag);
+    givens[2 * col] = c;
+    givens[2 * col + 1] = s;
+    shc[col] = mag;
+    shc[col + 1] = 0.0;
+    const double t = -s * S[col];
+    S[col] = c * S[col];
+    S[col + 1] = t;
+    st->presid = fabs(t);
+    st->ncols = col + 1;
+    st->breakdown = breakdown;
+    if (st->presid <= st->ptol || breakdown) st->done = 1;
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k <= col + 1; k += blockDim.x) hc[k] = shc[k];
+}
+
+__global__ void gm_scale_kernel(int ndof, const double* w, double* vout, const GmState* st) {
+  if (st->done && st->scal == 0.0) return;
+  // executed even when this column set done (the vector is then unused)
+  const double sc = st->scal;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += gridDim.x * blockDim.x)
+    vout[idx] = w[idx] * sc;
+}
+
+// y = H(:ncols,:ncols)^-1 S (SciPy's trsv loop), then coef = y
+__global__ void gm_backsolve_kernel(const double* H, int ldh, double* S, double* y, const GmState* st) {
+  int col = st->ncols - 1;
+  if (col < 0) return;
+  if (H[(size_t)col * ldh + col] == 0.0) S[col] = 0.0;
+  for (int k = 0; k <= col; ++k) y[k] = S[k];
+  for (int k = col; k > 0; --k) {
+    if (y[k] != 0.0) {
+      y[k] /= H[(size_t)k * ldh + k];
+      double t = y[k];
+      for (int q = 0; q < k; ++q) y[q] -= t * H[(size_t)k * ldh + q];
+    }
+  }
+  if (y[0] != 0.0) y[0] /= H[0];
+}
+
+__global__ void gm_update_x_kernel(int ndof, const double* __restrict__ V, const double* y, double* x,
+                                   const GmState* st) {
+  int ncols = st->ncols;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int k = 0; k < ncols; ++k) acc += y[k] * V[(size_t)k * ndof + idx];
+    x[idx] += acc;
+  }
+}
+
+__global__ void gm_start_kernel(int ndof, const double* w, double* v0, double* S, int m1, GmState* st,
+                                double vnorm, double ptol) {
+  const double inv = 1.0 / vnorm;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += gridDim.x * blockDim.x)
+    v0[idx] = w[idx] * inv;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    for (int k = 0; k < m1; ++k) S[k] = 0.0;
+    S[0] = vnorm;
+    st->done = 0;
+    st->breakdown = 0;
+    st->ncols = 0;
+    st->reorth = 0;
+    st->ptol = ptol;
+    st->presid = 0.0;
+  }
+}
+
+
+// Device GMRES workspace of one solver handle.  V holds restart_cap + 1
+// basis vectors; gm holds H (restart_cap x (restart_cap + 2)), the Givens
+// pairs, S, y, two Hessenberg columns and two norms; part holds the block
+// partial sums (at least 2 x blocks doubles).  exec / cap / key persist per
+// handle: the captured cycle graph, the private capture stream and the key
+// of what the graph's launches depend on.
+struct GmresWork {
+  int n = 0;
+  int ew_blocks = 0;
+  int part_len = 0;
+  int restart_cap = 0;
+  double* V = nullptr;
+  double* gm = nullptr;
+  double* part = nullptr;
+  GmState* gst = nullptr;
+  double* b = nullptr;     // right-hand side (prepared by the caller)
+  double* x = nullptr;     // iterate (x0 set by the caller)
+  double* r = nullptr;     // residual scratch
+  double* w = nullptr;     // preconditioned-vector scratch
+  double* t = nullptr;     // operator-output scratch
+  cudaGraphExec_t* exec = nullptr;
+  cudaStream_t* cap = nullptr;
+  long long* key = nullptr;   // 6 entries
+};
+
+inline int gm_norm2(const GmresWork& W, const double* v, double* out, cudaStream_t s) {
+  const int nb = std::min(W.ew_blocks, W.part_len / 2);
+  mdot_kernel<<<nb, 256, 8 * 32 * sizeof(double), s>>>(W.n, nullptr, 0, v, W.part, nullptr);
+  mdot_finalize_kernel<<<1, 1024, sizeof(double), s>>>(W.part, nb, 0, nullptr, W.gst, 2, out);
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
+inline int gm_read_scalar(const double* dev, double* host, cudaStream_t s) {
+  TPF_CUDA_TRY(cudaMemcpyAsync(host, dev, sizeof(double), cudaMemcpyDeviceToHost, s));
+  TPF_CUDA_TRY(cudaStreamSynchronize(s));
+  return TPF_OK;
+}
+
+struct GmresOutcome {
+  long long inner = 0;     // Arnoldi columns (SciPy's inner iterations)
+  long long applies = 0;   // operator applications
+  double bnrm2 = 0.0;
+  double rnorm = 0.0;      // true residual norm at exit
+  bool converged = false;
+};
+
+// SciPy gmres(A, b, x0, rtol=tol, atol=0, restart, maxiter, M) on the
+// device.  apply(in, out, stream, done): out = A in; resid(x, r, stream):
+// r = b - A x; precond(in, out, stream, done): out = M in.  Kernels given a
+// non-null `done` may skip their work once *done is set.  W.b and W.x
+// (x0; x_nonzero says whether it is nonzero) are set by the caller; on
+// return W.x holds the iterate.  key_a / key_b: the caller's part of the
+// cycle graph's key (what its operator launches depend on besides the
+// buffers).
+template <class Apply, class Resid, class Precond>
+int gmres_solve(GmresWork& W, int restart, double tol, long long maxiter, bool x_nonzero, long long key_a,
+                long long key_b, Apply apply, Resid resid, Precond precond, cudaStream_t s, GmresOutcome& out) {
+  const int n = W.n;
+  int st;
+  const int m = std::min(restart, n);
+  const int ldh = W.restart_cap + 2;
+  double* H = W.gm;
+  double* givens = H + (size_t)W.restart_cap * ldh;
+  double* S = givens + 2 * W.restart_cap;
+  double* y = S + (W.restart_cap + 1);
+  double* hcol = y + (W.restart_cap + 1);
+  double* hcol2 = hcol + (W.restart_cap + 1);
+  double* wnorm = hcol2 + (W.restart_cap + 1);
+  double* bnorm_d = wnorm + 1;
+  (void)hcol;
+  TPF_CUDA_TRY(cudaMemsetAsync(H, 0, sizeof(double) * (size_t)W.restart_cap * ldh, s));
+  TPF_CUDA_TRY(cudaMemsetAsync(W.gst, 0, sizeof(GmState), s));
+  if ((st = gm_norm2(W, W.b, bnorm_d, s))) return st;
+  double bnrm2 = 0.0;
+  if ((st = gm_read_scalar(bnorm_d, &bnrm2, s))) return st;
+  out = GmresOutcome{};
+  out.bnrm2 = bnrm2;
+  if (bnrm2 == 0.0) {
+    TPF_CUDA_TRY(cudaMemsetAsync(W.x, 0, sizeof(double) * n, s));
+    out.converged = true;
+    return TPF_OK;
+  }
+  const double atol = tol * bnrm2;
+  const double eps = 2.220446049250313e-16;
+  // Mb_nrm2 = ||M b||
+  if ((st = precond(W.b, W.w, s, nullptr))) return st;
+  if ((st = gm_norm2(W, W.w, wnorm, s))) return st;
+  double Mb_nrm2 = 0.0;
+  if ((st = gm_read_scalar(wnorm, &Mb_nrm2, s))) return st;
+  double ptol_max_factor = 1.0;
+  double ptol = Mb_nrm2 * std::min(ptol_max_factor, atol / bnrm2);
+  double presid = 0.0, rnorm = INFINITY;
+  // four blocks per SM for the basis dot products: enough loads in flight,
+  // few partials to sum per vector
+  const int nb_dot = std::min(std::min(W.ew_blocks, W.part_len / (m + 2)), std::max(1, 4 * tpf::sm_count()));
+  const int* done = &W.gst->done;
+  bool converged = false;
+  long long applies = 0, inner = 0;
+  auto enqueue_cycle = [&](cudaStream_t cs) -> int {
+    int est;
+    for (int col = 0; col < m; ++col) {
+      const double* vc = W.V + (size_t)col * n;
+      if ((est = apply(vc, W.t, cs, done))) return est;
+      if ((est = precond(W.t, W.w, cs, done))) return est;
+      double* hc = H + (size_t)col * ldh;
+      mdot_kernel<<<nb_dot, 256, 8 * 32 * sizeof(double), cs>>>(n, W.V, col + 1, W.w, W.part, done);
+      mdot_finalize_kernel<<<1, 1024, (col + 2) * sizeof(double), cs>>>(W.part, nb_dot, col + 1, hc, W.gst, 0,
+                                                                        nullptr);
+      maxpy_kernel<<<W.ew_blocks, 256, 0, cs>>>(n, W.V, col + 1, hc, W.w, W.gst, 0);
+      // conditional re-orthogonalization pass (hcol2 accumulates its coefficients)
+      TPF_CUDA_TRY(cudaMemsetAsync(hcol2, 0, sizeof(double) * (col + 1), cs));
+      mdot_kernel<<<nb_dot, 256, 8 * 32 * sizeof(double), cs>>>(n, W.V, col + 1, W.w, W.part, done);
+      mdot_finalize_kernel<<<1, 1024, (col + 2) * sizeof(double), cs>>>(W.part, nb_dot, col + 1, hcol2, W.gst,
+                                                                        1, nullptr);
+      maxpy_kernel<<<W.ew_blocks, 256, 0, cs>>>(n, W.V, col + 1, hcol2, W.w, W.gst, 1);
+      if ((est = gm_norm2(W, W.w, wnorm, cs))) return est;
+      gm_column_kernel<<<1, 128, (3 * col + 2) * sizeof(double), cs>>>(H, ldh, givens, S, W.gst, col, wnorm,
+                                                                      hcol2);
+      gm_scale_kernel<<<W.ew_blocks, 256, 0, cs>>>(n, W.w, W.V + (size_t)(col + 1) * n, W.gst);
+      TPF_CUDA_TRY(cudaGetLastError());
+    }
+    return TPF_OK;
+  };
+  const long long key[6] = {(long long)m, (long long)nb_dot, key_a, key_b, (long long)(intptr_t)W.V, (long long)n};
+  for (long long iteration = 0; iteration < maxiter; ++iteration) {
+    if (iteration == 0) {
+      if (x_nonzero) {
+        if ((st = resid(W.x, W.r, s))) return st;
+        ++applies;
+      } else {
+        TPF_CUDA_TRY(cudaMemcpyAsync(W.r, W.b, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+      }
+      if ((st = gm_norm2(W, W.r, wnorm, s))) return st;
+      double r0 = 0.0;
+      if ((st = gm_read_scalar(wnorm, &r0, s))) return st;
+      if (r0 < atol) { rnorm = r0; converged = true; break; }
+    }
+    // v0 = M r / ||M r||
+    TPF_CUDA_TRY(cudaMemsetAsync(W.gst, 0, sizeof(int), s));  // done = 0 for the precond call
+    if ((st = precond(W.r, W.w, s, nullptr))) return st;
+    if ((st = gm_norm2(W, W.w, wnorm, s))) return st;
+    double v0n = 0.0;
+    if ((st = gm_read_scalar(wnorm, &v0n, s))) return st;
+    gm_start_kernel<<<W.ew_blocks, 256, 0, s>>>(n, W.w, W.V, S, m + 1, W.gst, v0n, ptol);
+    if (!*W.exec || std::memcmp(W.key, key, sizeof(key)) != 0) {
+      if (*W.exec) { cudaGraphExecDestroy(*W.exec); *W.exec = nullptr; }
+      // captured on a private stream (the caller's may be the legacy default
+      // stream, which cannot be captured); replayed on the caller's
+      if (!*W.cap && cudaStreamCreateWithFlags(W.cap, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        *W.cap = nullptr;
+        tpf::set_error("cudaStreamCreate failed");
+        return TPF_ECUDA;
+      }
+      TPF_CUDA_TRY(cudaStreamBeginCapture(*W.cap, cudaStreamCaptureModeThreadLocal));
+      const int cst = enqueue_cycle(*W.cap);
+      cudaGraph_t graph = nullptr;
+      const cudaError_t ce = cudaStreamEndCapture(*W.cap, &graph);
+      if (cst || ce != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        if (cst) return cst;
+        tpf::set_error("capturing the GMRES cycle failed: %s", cudaGetErrorString(ce));
+        return TPF_ECUDA;
+      }
+      const cudaError_t ie = cudaGraphInstantiate(W.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ie != cudaSuccess) {
+        *W.exec = nullptr;
+        cudaGetLastError();
+        tpf::set_error("instantiating the GMRES cycle graph failed: %s", cudaGetErrorString(ie));
+        return TPF_ECUDA;
+      }
+      std::memcpy(W.key, key, sizeof(key));
+    }
+    TPF_CUDA_TRY(cudaGraphLaunch(*W.exec, s));
+    GmState hs{};
+    TPF_CUDA_TRY(cudaMemcpyAsync(&hs, W.gst, sizeof(GmState), cudaMemcpyDeviceToHost, s));
+    TPF_CUDA_TRY(cudaStreamSynchronize(s));
+    inner += hs.ncols;
+    applies += hs.ncols;
+    presid = hs.presid;
+    gm_backsolve_kernel<<<1, 1, 0, s>>>(H, ldh, S, y, W.gst);
+    gm_update_x_kernel<<<W.ew_blocks, 256, 0, s>>>(n, W.V, y, W.x, W.gst);
+    if ((st = resid(W.x, W.r, s))) return st;
+    ++applies;
+    if ((st = gm_norm2(W, W.r, wnorm, s))) return st;
+    if ((st = gm_read_scalar(wnorm, &rnorm, s))) return st;
+    if (rnorm <= atol) { converged = true; break; }
+    if (hs.breakdown) break;
+    if (presid <= ptol) ptol_max_factor = std::max(eps, 0.25 * ptol_max_factor);
+    else ptol_max_factor = std::min(1.0, 1.5 * ptol_max_factor);
+    ptol = presid * std::min(ptol_max_factor, atol / rnorm);
+  }
+  out.inner = inner;
+  out.applies = applies;
+  out.rnorm = rnorm;
+  out.converged = converged;
+  return TPF_OK;
+}
+
+}  // namespace

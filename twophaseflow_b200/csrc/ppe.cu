@@ -24,6 +24,7 @@
 //    re-orthogonalization replaces modified Gram-Schmidt.
 #include "tpf_common.cuh"
 #include "ppe_view.cuh"
+#include "gmres.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -1081,247 +1082,194 @@ __global__ void __launch_bounds__(kThreads, 1) cg1_band_kernel(BandArgs a) {
   }
 }
 
-// ---- GMRES building blocks ---------------------------------------------------------
+}  // namespace
 
-struct GmState {
-  int done;          // inner loop finished (presid <= ptol or breakdown)
-  int breakdown;
-  int ncols;         // columns completed in this cycle
-  int reorth;        // second Gram-Schmidt pass requested
-  double presid;
-  double ptol;
-  double h0;         // ||w|| before orthogonalization
-  double wn2;        // ||w||^2 scratch
-  double rnorm;      // true residual norm (end of cycle)
-  double scal;       // scale factor for the new basis vector
+namespace {
+
+// ---- streaming PCG (large systems) --------------------------------------------------
+//
+// The same Jacobi-PCG recurrences as cg1_kernel (Chronopoulos-Gear, one
+// reduction per iteration, SciPy's stopping rule), for systems whose vectors
+// stream from HBM (3-D grids): an iteration is two ordinary kernels at full
+// occupancy instead of one persistent kernel with one CTA per SM, since the
+// persistent kernel's register budget (126 per thread) leaves 16 warps per SM,
+// too few loads in flight to stream at HBM bandwidth.
+//   update : s = w + beta s, p = M r + beta p, x += alpha p, r -= alpha s
+//   stencil: w = S M r (M r recomputed at the neighbours), the six inner
+//            products; the last block to finish sums the block partials in
+//            block order and advances the scalars (alpha, beta, ...) and the
+//            convergence state on the device.
+// Chunks of iterations are captured as one CUDA graph and replayed; every
+// kernel returns at once after the device-side state says done, so the host
+// reads the state once per chunk.
+
+struct CgScal {
+  double gamma, denom, beta, rr, bb, atol2, tol, pad;
+  long long it, applies, maxiter, pad2;
+  int done, conv, x_nonzero;
+  unsigned int arrive;
 };
 
-// partial dots: part[k*nb + block] = <V_k, w> for k < ncols, part[ncols*nb+block] = <w,w>
-// Block partials of <V_k, w> for k < ncols and of <w, w> (k = ncols):
-// part[k * nb + block].  The vectors are taken eight at a time in one sweep
-// over w, with one block reduction per group (warp j reduces vector j of the
-// group with the same shuffle tree a one-vector reduction uses).
-__global__ void mdot_kernel(int ndof, const double* __restrict__ V, int ncols, const double* __restrict__ w,
-                            double* part, const int* done) {
-  if (done && *done) return;
-  constexpr int KC = 8;   // vectors per sweep (<= warps per block)
-  extern __shared__ double sh[];   // [KC][32]
-  const int nb = gridDim.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int k0 = 0; k0 <= ncols; k0 += KC) {
-    double acc[KC];
-#pragma unroll
-    for (int j = 0; j < KC; ++j) acc[j] = 0.0;
-    // two elements per trip: 18 independent loads in flight per thread
-    const int stride = gridDim.x * blockDim.x;
-    int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    for (; idx + stride < ndof; idx += 2 * stride) {
-      const double wa = w[idx], wb = w[idx + stride];
-      double va[KC], vb[KC];
-#pragma unroll
-      for (int j = 0; j < KC; ++j) {
-        const int k = k0 + j;
-        va[j] = (k < ncols) ? V[(size_t)k * ndof + idx] : wa;
-        vb[j] = (k < ncols) ? V[(size_t)k * ndof + idx + stride] : wb;
-      }
-#pragma unroll
-      for (int j = 0; j < KC; ++j) {
-        if (k0 + j <= ncols) {
-          acc[j] += va[j] * wa;
-          acc[j] += vb[j] * wb;
-        }
-      }
-    }
-    if (idx < ndof) {
-      const double wi = w[idx];
-#pragma unroll
-      for (int j = 0; j < KC; ++j) {
-        const int k = k0 + j;
-        if (k <= ncols) acc[j] += ((k < ncols) ? V[(size_t)k * ndof + idx] : wi) * wi;
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < KC; ++j) {
-      const double v = tpf::warp_sum(acc[j]);
-      if (lane == 0) sh[j * 32 + wid] = v;
-    }
-    __syncthreads();
-    if (wid < KC && k0 + wid <= ncols) {
-      double t = (lane < nw) ? sh[wid * 32 + lane] : 0.0;
-      t = tpf::warp_sum(t);
-      if (lane == 0) part[(size_t)(k0 + wid) * nb + blockIdx.x] = t;
-    }
-    __syncthreads();
-  }
-}
-
-// sum partials -> out[k] (k <= ncols); mode selects how the state uses them.
-// mode 0: first GS pass (h column = dots, h0 = sqrt(<w,w>)), decide re-orth
-// mode 1: second pass (h column += dots)
-// mode 2: plain norm -> out[0] = sqrt(<w,w>)
-// One block; warp j sums the partials of vectors j, j + nwarps, ... (lane l:
-// blocks l, l + 32, ..., then a shuffle tree), so all vectors are summed at
-// once; thread 0 then applies the mode's scalar logic in vector order.
-__global__ void mdot_finalize_kernel(const double* part, int nb, int ncols, double* hcol, GmState* st,
-                                     int mode, double* out_norm) {
-  if (mode != 2 && st->done) return;
-  if (mode == 1 && !st->reorth) return;
-  extern __shared__ double sums[];   // [ncols + 1]
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int k = wid; k <= ncols; k += nw) {
-    double acc = 0.0;
-    for (int b = lane; b < nb; b += 32) acc += part[(size_t)k * nb + b];
-    acc = tpf::warp_sum(acc);
-    if (lane == 0) sums[k] = acc;
-  }
-  __syncthreads();
-  if (mode == 2) {
-    if (threadIdx.x == 0) *out_norm = sqrt(sums[0]);
-    return;
-  }
-  if (mode == 1) {
-    for (int k = threadIdx.x; k < ncols; k += blockDim.x) hcol[k] += sums[k];
-    if (threadIdx.x == 0) st->wn2 = 0.0;
-    return;
-  }
-  for (int k = threadIdx.x; k < ncols; k += blockDim.x) hcol[k] = sums[k];
-  if (threadIdx.x == 0) {
-    const double sw = sums[ncols];
-    st->h0 = sqrt(sw);
-    double proj = 0.0;
-    for (int q = 0; q < ncols; ++q) proj += sums[q] * sums[q];
-    st->reorth = (sw - proj < 0.5 * sw) ? 1 : 0;
-  }
-}
-
-// w -= sum_k c_k V_k  (c = hcol, or the second-pass dots in part-summed form)
-__global__ void maxpy_kernel(int ndof, const double* __restrict__ V, int ncols, const double* coef, double* w,
-                             const GmState* st, int pass) {
-  if (st->done) return;
-  if (pass == 1 && !st->reorth) return;
-  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += gridDim.x * blockDim.x) {
-    double acc = w[idx];
-#pragma unroll 8
-    for (int k = 0; k < ncols; ++k) acc -= coef[k] * V[(size_t)k * ndof + idx];
-    w[idx] = acc;
-  }
-}
-
-// Givens rotation generator for real (f, g): c f + s g = r, -s f + c g = 0,
-// r carries the sign of f (the convention of LAPACK's lartg).
-__device__ void givens_rot(double f, double g, double& c, double& s, double& r) {
-  if (g == 0.0) { c = 1.0; s = 0.0; r = f; return; }
-  if (f == 0.0) { c = 0.0; s = (g > 0.0) ? 1.0 : -1.0; r = fabs(g); return; }
-  double d = hypot(f, g);
-  c = fabs(f) / d;
-  r = copysign(d, f);
-  s = g / r;
-}
-
-// Finish Arnoldi column `col`: h1, breakdown, rotations, S, presid, done flag.
-// H is stored like SciPy's h[col, k] (row col = column of the Hessenberg matrix).
-// New Hessenberg column: fold in the second-pass coefficients, apply the
-// previous Givens rotations, generate this column's rotation and update the
-// residual vector S.  The block stages the column and the rotations in
-// shared memory; thread 0 applies them in order (the same arithmetic as a
-// serial pass over global memory, without its dependent round trips).
-__global__ void gm_column_kernel(double* H, int ldh, double* givens, double* S, GmState* st, int col,
-                                 const double* w_norm, const double* hcol2) {
-  if (st->done) return;
-  extern __shared__ double shc[];       // [col + 2] column, then [2 col] rotations
-  double* sg = shc + col + 2;
-  double* hc = H + (size_t)col * ldh;
-  const bool reorth = st->reorth != 0;
-  for (int k = threadIdx.x; k <= col; k += blockDim.x) {
-    double v = hc[k];
-    if (reorth) v += hcol2[k];   // second-pass coefficients
-    shc[k] = v;
-  }
-  for (int k = threadIdx.x; k < 2 * col; k += blockDim.x) sg[k] = givens[k];
+__device__ __forceinline__ bool cgs_last_block(CgScal* sc) {
+  __shared__ int s_last;
+  __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
-    const double eps = 2.220446049250313e-16;
-    double h1 = *w_norm;
-    shc[col + 1] = h1;
-    int breakdown = 0;
-    if (h1 <= eps * st->h0) {
-      shc[col + 1] = 0.0;
-      breakdown = 1;
-      st->scal = 1.0;
+    const unsigned int prev = atomicAdd(&sc->arrive, 1u);
+    s_last = (prev == gridDim.x - 1) ? 1 : 0;
+  }
+  __syncthreads();
+  if (s_last) __threadfence();
+  return s_last != 0;
+}
+
+// sum of NV block partials part[k * nb + b] in block order (same tree every call)
+template <int NV>
+__device__ __forceinline__ void cgs_sum_partials(const double* part, int nb, double (&v)[NV], double* scratch) {
+#pragma unroll
+  for (int k = 0; k < NV; ++k) v[k] = 0.0;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] += __ldcg(part + (size_t)k * nb + b);
+  }
+  tpf::block_sum<NV>(v, scratch);
+}
+
+// r = b - S x (x_nonzero) or b; then (b, b), (r, r)
+__global__ void __launch_bounds__(256) cgs_resid_kernel(Grid3 g, const double* s0, const double* s1,
+                                                        const double* s2, const double* b, const double* x,
+                                                        double* r, double* part, CgScal* sc) {
+  __shared__ double scratch[2 * 32];
+  double v[2] = {0.0, 0.0};
+  const bool xnz = sc->x_nonzero != 0;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < g.ndof; idx += gridDim.x * blockDim.x) {
+    const double bi = b[idx];
+    double ri = bi;
+    if (xnz) {
+      double sx;
+      if (idx == g.pin) sx = x[idx];
+      else {
+        int i0, i1, i2;
+        coords3(g, idx, i0, i1, i2);
+        double d, off;
+        s_row<double>(g, idx, i0, i1, i2, s0, s1, s2, [&](int j) { return (j == g.pin) ? 0.0 : x[j]; }, d, off);
+        sx = d * x[idx] - off;
+      }
+      ri = bi - sx;
+    }
+    r[idx] = ri;
+    v[0] += bi * bi;
+    v[1] += ri * ri;
+  }
+  tpf::block_sum<2>(v, scratch);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = v[0];
+    part[gridDim.x + blockIdx.x] = v[1];
+  }
+  if (!cgs_last_block(sc)) return;
+  double t[2];
+  cgs_sum_partials<2>(part, gridDim.x, t, scratch);
+  if (threadIdx.x == 0) {
+    sc->arrive = 0u;
+    sc->bb = t[0];
+    sc->rr = t[1];
+    const double atol = sc->tol * sqrt(t[0]);
+    sc->atol2 = atol * atol;
+    sc->it = 0;
+    sc->applies = 0;
+    sc->conv = 0;
+    sc->done = 0;
+    if (t[0] == 0.0) { sc->done = 1; sc->conv = 1; }
+  }
+}
+
+// w = S M r and the six inner products {(r,u), (w,u), (u,s), (p,w), (p,s), (r,r)}
+// (INIT: s = p = 0 are written first, as the first w_pass of cg1_kernel)
+template <bool INIT>
+__global__ void __launch_bounds__(256) cgs_stencil_kernel(Grid3 g, const double* __restrict__ s0,
+                                                          const double* __restrict__ s1,
+                                                          const double* __restrict__ s2,
+                                                          const double* __restrict__ dinv,
+                                                          const double* __restrict__ r, double* __restrict__ w,
+                                                          double* __restrict__ sv, double* __restrict__ pv,
+                                                          double* part, CgScal* sc) {
+  if (sc->done) return;
+  __shared__ double scratch[6 * 32];
+  double red[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < g.ndof; idx += gridDim.x * blockDim.x) {
+    const double ri = r[idx];
+    const double ui = dinv[idx] * ri;
+    double wi;
+    if (idx == g.pin) {
+      wi = ui;
     } else {
-      st->scal = 1.0 / h1;
+      int i0, i1, i2;
+      coords3(g, idx, i0, i1, i2);
+      double d, off;
+      s_row<double>(g, idx, i0, i1, i2, s0, s1, s2, [&](int j) { return (j == g.pin) ? 0.0 : dinv[j] * r[j]; },
+                    d, off);
+      wi = d * ui - off;
     }
-    for (int k = 0; k < col; ++k) {
-      const double c = sg[2 * k], s = sg[2 * k + 1];
-      const double n0 = shc[k], n1 = shc[k + 1];
-      shc[k] = c * n0 + s * n1;
-      shc[k + 1] = -s * n0 + c * n1;
+    w[idx] = wi;
+    double si = 0.0, pi = 0.0;
+    if (INIT) {
+      sv[idx] = 0.0;
+      pv[idx] = 0.0;
+    } else {
+      si = sv[idx];
+      pi = pv[idx];
     }
-    double c, s, mag;
-    givens_rot(shc[col], shc[col + 1], c, s, mag);
-    givens[2 * col] = c;
-    givens[2 * col + 1] = s;
-    shc[col] = mag;
-    shc[col + 1] = 0.0;
-    const double t = -s * S[col];
-    S[col] = c * S[col];
-    S[col + 1] = t;
-    st->presid = fabs(t);
-    st->ncols = col + 1;
-    st->breakdown = breakdown;
-    if (st->presid <= st->ptol || breakdown) st->done = 1;
+    red[0] += ri * ui;
+    red[1] += wi * ui;
+    red[2] += ui * si;
+    red[3] += pi * wi;
+    red[4] += pi * si;
+    red[5] += ri * ri;
   }
-  __syncthreads();
-  for (int k = threadIdx.x; k <= col + 1; k += blockDim.x) hc[k] = shc[k];
-}
-
-__global__ void gm_scale_kernel(int ndof, const double* w, double* vout, const GmState* st) {
-  if (st->done && st->scal == 0.0) return;
-  // executed even when this column set done (the vector is then unused)
-  const double sc = st->scal;
-  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += gridDim.x * blockDim.x)
-    vout[idx] = w[idx] * sc;
-}
-
-// y = H(:ncols,:ncols)^-1 S (SciPy's trsv loop), then coef = y
-__global__ void gm_backsolve_kernel(const double* H, int ldh, double* S, double* y, const GmState* st) {
-  int col = st->ncols - 1;
-  if (col < 0) return;
-  if (H[(size_t)col * ldh + col] == 0.0) S[col] = 0.0;
-  for (int k = 0; k <= col; ++k) y[k] = S[k];
-  for (int k = col; k > 0; --k) {
-    if (y[k] != 0.0) {
-      y[k] /= H[(size_t)k * ldh + k];
-      double t = y[k];
-      for (int q = 0; q < k; ++q) y[q] -= t * H[(size_t)k * ldh + q];
-    }
+  tpf::block_sum<6>(red, scratch);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) part[(size_t)k * gridDim.x + blockIdx.x] = red[k];
   }
-  if (y[0] != 0.0) y[0] /= H[0];
+  if (!cgs_last_block(sc)) return;
+  double t[6];
+  cgs_sum_partials<6>(part, gridDim.x, t, scratch);
+  if (threadIdx.x == 0) {
+    sc->arrive = 0u;
+    if (INIT) {
+      sc->gamma = t[0];
+      sc->denom = t[1];
+      sc->beta = 0.0;
+      sc->applies = sc->x_nonzero ? 2 : 1;
+    } else {
+      const double gnew = t[0];
+      const double beta = gnew / sc->gamma;
+      sc->beta = beta;
+      sc->denom = t[1] + beta * (t[2] + t[3]) + beta * beta * t[4];
+      sc->gamma = gnew;
+      sc->it += 1;
+      sc->applies += 1;
+    }
+    sc->rr = t[5];
+    if (t[5] < sc->atol2) { sc->conv = 1; sc->done = 1; }
+    else if (sc->it >= sc->maxiter) sc->done = 1;
+  }
 }
 
-__global__ void gm_update_x_kernel(int ndof, const double* __restrict__ V, const double* y, double* x,
-                                   const GmState* st) {
-  int ncols = st->ncols;
+__global__ void __launch_bounds__(256) cgs_update_kernel(int ndof, const double* __restrict__ dinv,
+                                                         const double* __restrict__ w, double* __restrict__ sv,
+                                                         double* __restrict__ pv, double* __restrict__ x,
+                                                         double* __restrict__ r, const CgScal* sc) {
+  if (sc->done) return;
+  const double alpha = sc->gamma / sc->denom, beta = sc->beta;
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += gridDim.x * blockDim.x) {
-    double acc = 0.0;
-    for (int k = 0; k < ncols; ++k) acc += y[k] * V[(size_t)k * ndof + idx];
-    x[idx] += acc;
-  }
-}
-
-__global__ void gm_start_kernel(int ndof, const double* w, double* v0, double* S, int m1, GmState* st,
-                                double vnorm, double ptol) {
-  const double inv = 1.0 / vnorm;
-  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += gridDim.x * blockDim.x)
-    v0[idx] = w[idx] * inv;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    for (int k = 0; k < m1; ++k) S[k] = 0.0;
-    S[0] = vnorm;
-    st->done = 0;
-    st->breakdown = 0;
-    st->ncols = 0;
-    st->reorth = 0;
-    st->ptol = ptol;
-    st->presid = 0.0;
+    const double ri = r[idx];
+    const double si = w[idx] + beta * sv[idx];
+    const double pi = dinv[idx] * ri + beta * pv[idx];
+    sv[idx] = si;
+    pv[idx] = pi;
+    x[idx] += alpha * pi;
+    r[idx] = ri - alpha * si;
   }
 }
 
@@ -1365,6 +1313,9 @@ struct tpf_ppe {
   unsigned int* bar = nullptr;
   int* err = nullptr;
   cudaGraphExec_t gm_exec = nullptr;   // one GMRES restart cycle, captured
+  cudaGraphExec_t cg_exec = nullptr;   // a chunk of streaming-PCG iterations, captured
+  long long cg_key[6] = {};
+  void* cgs = nullptr;                 // streaming-PCG device scalars (CgScal)
   cudaStream_t cap = nullptr;          // stream the cycle is captured on (never the caller's)
   long long gm_key[6] = {};
   double* band_pub = nullptr;     // halo rows of the band-resident PCG
@@ -1516,188 +1467,70 @@ int precond_L(tpf_ppe* h, const double* r, double* z, cudaStream_t s, const int*
   return TPF_OK;
 }
 
-int norm2_dev(tpf_ppe* h, const double* w, double* out, cudaStream_t s) {
-  int nb = std::min(h->ew_blocks, h->part_len / 2);
-  mdot_kernel<<<nb, 256, 8 * 32 * sizeof(double), s>>>(h->g.ndof, nullptr, 0, w, h->part, nullptr);
-  mdot_finalize_kernel<<<1, 1024, sizeof(double), s>>>(h->part, nb, 0, nullptr, h->gst, 2, out);
-  TPF_CUDA_TRY(cudaGetLastError());
-  return TPF_OK;
-}
-
-int read_scalar(double* dev, double* host, cudaStream_t s) {
-  TPF_CUDA_TRY(cudaMemcpyAsync(host, dev, sizeof(double), cudaMemcpyDeviceToHost, s));
-  TPF_CUDA_TRY(cudaStreamSynchronize(s));
-  return TPF_OK;
-}
-
-// SciPy 1.18.1 gmres restated on the device (see the file header).
+// SciPy 1.18.1 gmres restated on the device (gmres.cuh) over the FVM
+// operator and the handle's preconditioner.
 int solve_gmres(tpf_ppe* h, const double* rhs, double* p, const double* p_init, cudaStream_t s,
                 tpf_ppe_result* res) {
   const Grid3& g = h->g;
   const int n = g.ndof;
   int st;
   if ((st = ensure_gmres(h))) return st;
-  const int m = std::min(h->o.restart, n);
-  const int ldh = h->o.restart + 2;
-  double* H = h->gm;
-  double* givens = H + (size_t)h->o.restart * ldh;
-  double* S = givens + 2 * h->o.restart;
-  double* y = S + (h->o.restart + 1);
-  double* hcol = y + (h->o.restart + 1);
-  double* hcol2 = hcol + (h->o.restart + 1);
-  double* wnorm = hcol2 + (h->o.restart + 1);
-  double* bnorm_d = wnorm + 1;
-  double* b = h->b;
-  double* x = h->x;
-  double* r = h->r;
-  double* w = h->z;
-  double* t = h->q;
+  GmresWork W;
+  W.n = n;
+  W.ew_blocks = h->ew_blocks;
+  W.part_len = h->part_len;
+  W.restart_cap = h->o.restart;
+  W.V = h->V;
+  W.gm = h->gm;
+  W.part = h->part;
+  W.gst = h->gst;
+  W.b = h->b;
+  W.x = h->x;
+  W.r = h->r;
+  W.w = h->z;
+  W.t = h->q;
+  W.exec = &h->gm_exec;
+  W.cap = &h->cap;
+  W.key = h->gm_key;
   // b = rhs with b[pin] = 0 ; x0 = p_init with pin = 0
-  copy_pin0_kernel<<<ew_grid(h), 256, 0, s>>>(n, g.pin, rhs, b);
-  if (p_init) copy_pin0_kernel<<<ew_grid(h), 256, 0, s>>>(n, g.pin, p_init, x);
-  else TPF_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(double) * n, s));
-  TPF_CUDA_TRY(cudaMemsetAsync(H, 0, sizeof(double) * (size_t)h->o.restart * ldh, s));
-  TPF_CUDA_TRY(cudaMemsetAsync(h->gst, 0, sizeof(GmState), s));
-  if ((st = norm2_dev(h, b, bnorm_d, s))) return st;
-  double bnrm2 = 0.0;
-  if ((st = read_scalar(bnorm_d, &bnrm2, s))) return st;
-  long long applies = 0, inner = 0;
-  res->refinements = 0;
-  if (bnrm2 == 0.0) {
+  copy_pin0_kernel<<<ew_grid(h), 256, 0, s>>>(n, g.pin, rhs, W.b);
+  if (p_init) copy_pin0_kernel<<<ew_grid(h), 256, 0, s>>>(n, g.pin, p_init, W.x);
+  else TPF_CUDA_TRY(cudaMemsetAsync(W.x, 0, sizeof(double) * n, s));
+  if (h->o.precond == TPF_PRECOND_LINE_PCR && (st = pcr_attributes())) return st;
+  const Geo geo{{h->dv[0], h->dv[1], h->dv[2]}, {h->dface[0], h->dface[1], h->dface[2]}};
+  auto apply = [&](const double* in, double* out, cudaStream_t cs, const int* done) -> int {
+    apply_L_kernel<<<ew_grid(h), 256, 0, cs>>>(g, geo, h->s[0], h->s[1], h->s[2], in, out, nullptr, done);
+    TPF_CUDA_TRY(cudaGetLastError());
+    return TPF_OK;
+  };
+  auto resid = [&](const double* x, double* r, cudaStream_t cs) -> int {
+    apply_L_kernel<<<ew_grid(h), 256, 0, cs>>>(g, geo, h->s[0], h->s[1], h->s[2], x, r, W.b, nullptr);
+    TPF_CUDA_TRY(cudaGetLastError());
+    return TPF_OK;
+  };
+  auto precond = [&](const double* in, double* out, cudaStream_t cs, const int* done) -> int {
+    return precond_L(h, in, out, cs, done);
+  };
+  GmresOutcome o;
+  st = gmres_solve(W, h->o.restart, h->o.tol, h->o.maxiter, p_init != nullptr, (long long)h->o.precond,
+                   (long long)h->o.pcr_stages, apply, resid, precond, s, o);
+  if (st) return st;
+  if (o.bnrm2 == 0.0) {
     TPF_CUDA_TRY(cudaMemsetAsync(p, 0, sizeof(double) * n, s));
     TPF_CUDA_TRY(cudaStreamSynchronize(s));
+    res->refinements = 0;
     res->iterations = 0; res->applies = 0; res->rel_residual = 0.0; res->info = 0;
     return TPF_OK;
   }
-  const double atol = h->o.tol * bnrm2;
-  const double eps = 2.220446049250313e-16;
-  // Mb_nrm2 = ||M b||
-  if ((st = precond_L(h, b, w, s, nullptr))) return st;
-  if ((st = norm2_dev(h, w, wnorm, s))) return st;
-  double Mb_nrm2 = 0.0;
-  if ((st = read_scalar(wnorm, &Mb_nrm2, s))) return st;
-  double ptol_max_factor = 1.0;
-  double ptol = Mb_nrm2 * std::min(ptol_max_factor, atol / bnrm2);
-  double presid = 0.0, rnorm = INFINITY;
-  const bool x_nonzero = p_init != nullptr;
-  // four blocks per SM for the basis dot products: enough loads in flight,
-  // few partials to sum per vector
-  const int nb_dot = std::min(std::min(h->ew_blocks, h->part_len / (m + 2)), std::max(1, 4 * tpf::sm_count()));
-  const int* done = &h->gst->done;
-  bool converged = false;
-  // One restart cycle (m Arnoldi columns).  Every kernel of a column skips
-  // its work once the device-side state says the cycle is done, so the whole
-  // cycle is captured once as a CUDA graph and replayed; the key holds what
-  // its launches depend on (the buffers are fixed per handle and prepare
-  // rewrites the preconditioner arrays in place).
-  const Geo geo{{h->dv[0], h->dv[1], h->dv[2]}, {h->dface[0], h->dface[1], h->dface[2]}};
-  auto enqueue_cycle = [&](cudaStream_t s) -> int {
-    int est;
-    for (int col = 0; col < m; ++col) {
-      const double* vc = h->V + (size_t)col * n;
-      apply_L_kernel<<<ew_grid(h), 256, 0, s>>>(g, geo, h->s[0], h->s[1], h->s[2], vc, t, nullptr, done);
-      if ((est = precond_L(h, t, w, s, done))) return est;
-      double* hc = H + (size_t)col * ldh;
-      mdot_kernel<<<nb_dot, 256, 8 * 32 * sizeof(double), s>>>(n, h->V, col + 1, w, h->part, done);
-      mdot_finalize_kernel<<<1, 1024, (col + 2) * sizeof(double), s>>>(h->part, nb_dot, col + 1, hc, h->gst, 0,
-                                                                       nullptr);
-      maxpy_kernel<<<ew_grid(h), 256, 0, s>>>(n, h->V, col + 1, hc, w, h->gst, 0);
-      // conditional re-orthogonalization pass (hcol2 accumulates its coefficients)
-      TPF_CUDA_TRY(cudaMemsetAsync(hcol2, 0, sizeof(double) * (col + 1), s));
-      mdot_kernel<<<nb_dot, 256, 8 * 32 * sizeof(double), s>>>(n, h->V, col + 1, w, h->part, done);
-      mdot_finalize_kernel<<<1, 1024, (col + 2) * sizeof(double), s>>>(h->part, nb_dot, col + 1, hcol2, h->gst,
-                                                                       1, nullptr);
-      maxpy_kernel<<<ew_grid(h), 256, 0, s>>>(n, h->V, col + 1, hcol2, w, h->gst, 1);
-      if ((est = norm2_dev(h, w, wnorm, s))) return est;
-      gm_column_kernel<<<1, 128, (3 * col + 2) * sizeof(double), s>>>(H, ldh, givens, S, h->gst, col, wnorm,
-                                                                     hcol2);
-      gm_scale_kernel<<<ew_grid(h), 256, 0, s>>>(n, w, h->V + (size_t)(col + 1) * n, h->gst);
-      TPF_CUDA_TRY(cudaGetLastError());
-    }
-    return TPF_OK;
-  };
-  const long long key[6] = {(long long)m, (long long)nb_dot, (long long)h->o.precond, (long long)h->o.pcr_stages,
-                            (long long)(intptr_t)h->V, (long long)n};
-  if (h->o.precond == TPF_PRECOND_LINE_PCR && (st = pcr_attributes())) return st;
-  for (long long iteration = 0; iteration < h->o.maxiter; ++iteration) {
-    if (iteration == 0) {
-      if (x_nonzero) {
-        apply_L_kernel<<<ew_grid(h), 256, 0, s>>>(g, Geo{{h->dv[0], h->dv[1], h->dv[2]}, {h->dface[0], h->dface[1], h->dface[2]}},
-                                                  h->s[0], h->s[1], h->s[2], x, r, b, nullptr);
-        ++applies;
-      } else {
-        TPF_CUDA_TRY(cudaMemcpyAsync(r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-      }
-      if ((st = norm2_dev(h, r, wnorm, s))) return st;
-      double r0 = 0.0;
-      if ((st = read_scalar(wnorm, &r0, s))) return st;
-      if (r0 < atol) { rnorm = r0; converged = true; break; }
-    }
-    // v0 = M r / ||M r||
-    TPF_CUDA_TRY(cudaMemsetAsync(h->gst, 0, sizeof(int), s));  // done = 0 for the precond call
-    if ((st = precond_L(h, r, w, s, nullptr))) return st;
-    if ((st = norm2_dev(h, w, wnorm, s))) return st;
-    double v0n = 0.0;
-    if ((st = read_scalar(wnorm, &v0n, s))) return st;
-    gm_start_kernel<<<ew_grid(h), 256, 0, s>>>(n, w, h->V, S, m + 1, h->gst, v0n, ptol);
-    if (!h->gm_exec || std::memcmp(h->gm_key, key, sizeof(key)) != 0) {
-      if (h->gm_exec) { cudaGraphExecDestroy(h->gm_exec); h->gm_exec = nullptr; }
-      // captured on a private stream (the caller's may be the legacy default
-      // stream, which cannot be captured); replayed on the caller's
-      if (!h->cap && cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking) != cudaSuccess) {
-        cudaGetLastError();
-        h->cap = nullptr;
-        tpf::set_error("cudaStreamCreate failed");
-        return TPF_ECUDA;
-      }
-      TPF_CUDA_TRY(cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal));
-      const int cst = enqueue_cycle(h->cap);
-      cudaGraph_t graph = nullptr;
-      const cudaError_t ce = cudaStreamEndCapture(h->cap, &graph);
-      if (cst || ce != cudaSuccess) {
-        if (graph) cudaGraphDestroy(graph);
-        cudaGetLastError();
-        if (cst) return cst;
-        tpf::set_error("capturing the GMRES cycle failed: %s", cudaGetErrorString(ce));
-        return TPF_ECUDA;
-      }
-      const cudaError_t ie = cudaGraphInstantiate(&h->gm_exec, graph, 0);
-      cudaGraphDestroy(graph);
-      if (ie != cudaSuccess) {
-        h->gm_exec = nullptr;
-        cudaGetLastError();
-        tpf::set_error("instantiating the GMRES cycle graph failed: %s", cudaGetErrorString(ie));
-        return TPF_ECUDA;
-      }
-      std::memcpy(h->gm_key, key, sizeof(key));
-    }
-    TPF_CUDA_TRY(cudaGraphLaunch(h->gm_exec, s));
-    GmState hs{};
-    TPF_CUDA_TRY(cudaMemcpyAsync(&hs, h->gst, sizeof(GmState), cudaMemcpyDeviceToHost, s));
-    TPF_CUDA_TRY(cudaStreamSynchronize(s));
-    inner += hs.ncols;
-    applies += hs.ncols;
-    presid = hs.presid;
-    gm_backsolve_kernel<<<1, 1, 0, s>>>(H, ldh, S, y, h->gst);
-    gm_update_x_kernel<<<ew_grid(h), 256, 0, s>>>(n, h->V, y, x, h->gst);
-    apply_L_kernel<<<ew_grid(h), 256, 0, s>>>(g, geo, h->s[0], h->s[1], h->s[2], x, r, b, nullptr);
-    ++applies;
-    if ((st = norm2_dev(h, r, wnorm, s))) return st;
-    if ((st = read_scalar(wnorm, &rnorm, s))) return st;
-    if (rnorm <= atol) { converged = true; break; }
-    if (hs.breakdown) break;
-    if (presid <= ptol) ptol_max_factor = std::max(eps, 0.25 * ptol_max_factor);
-    else ptol_max_factor = std::min(1.0, 1.5 * ptol_max_factor);
-    ptol = presid * std::min(ptol_max_factor, atol / rnorm);
-  }
-  copy_pin0_kernel<<<ew_grid(h), 256, 0, s>>>(n, g.pin, x, p);
+  copy_pin0_kernel<<<ew_grid(h), 256, 0, s>>>(n, g.pin, W.x, p);
   TPF_CUDA_TRY(cudaGetLastError());
   TPF_CUDA_TRY(cudaStreamSynchronize(s));
-  res->iterations = inner;
-  res->applies = applies;
-  res->rel_residual = rnorm / bnrm2;
-  res->info = converged ? 0 : (int)std::min<long long>(h->o.maxiter, 0x7fffffff);
-  if (!converged) {
+  res->refinements = 0;
+  res->iterations = o.inner;
+  res->applies = o.applies;
+  res->rel_residual = o.rnorm / o.bnrm2;
+  res->info = o.converged ? 0 : (int)std::min<long long>(h->o.maxiter, 0x7fffffff);
+  if (!o.converged) {
     tpf::set_error("PPESolverFVMMatrixFree did not converge cleanly (info=%d); no alternate PPE solver was applied.",
                    res->info);
     return TPF_ENOCONV;
@@ -1768,6 +1601,97 @@ int launch_band(tpf_ppe* h, const BandPlan& bp, const Cg1Args& c, cudaStream_t s
   return TPF_OK;
 }
 
+// Streaming PCG: the iteration as two kernels at full occupancy, chunks of
+// kCgsChunk iterations replayed from a CUDA graph (see the kernels above).
+constexpr int kCgsChunk = 32;
+
+int solve_cg_stream(tpf_ppe* h, const double* rhs, double* p, const double* p_init, cudaStream_t s,
+                    tpf_ppe_result* res) {
+  const Grid3& g = h->g;
+  const int n = g.ndof;
+  int st;
+  if (!h->cgs) {
+    CgScal* c = nullptr;
+    if ((st = dalloc(h, &c, 1))) return st;
+    h->cgs = c;
+  }
+  CgScal* sc = static_cast<CgScal*>(h->cgs);
+  const Geo geo{{h->dv[0], h->dv[1], h->dv[2]}, {h->dface[0], h->dface[1], h->dface[2]}};
+  cg_rhs_kernel<<<ew_grid(h), 256, 0, s>>>(g, geo, rhs, h->b, p_init, h->x);
+  CgScal init{};
+  init.tol = h->o.tol;
+  init.maxiter = h->o.maxiter;
+  init.x_nonzero = p_init ? 1 : 0;
+  TPF_CUDA_TRY(cudaMemcpyAsync(sc, &init, sizeof(CgScal), cudaMemcpyHostToDevice, s));
+  const bool none = (h->o.precond == TPF_PRECOND_NONE);
+  const double* dinv = none ? h->ones64 : h->dinvS;
+  double* r = h->c64[0];
+  double* w = h->c64[2];
+  double* sv = h->c64[4];
+  double* pv = h->c64[6];
+  const double* s2 = (g.N2 > 0) ? h->s[2] : h->s[1];
+  const int nb = std::max(1, std::min(h->ew_blocks, h->part_len / 8));
+  cgs_resid_kernel<<<nb, 256, 0, s>>>(g, h->s[0], h->s[1], s2, h->b, h->x, r, h->part, sc);
+  cgs_stencil_kernel<true><<<nb, 256, 0, s>>>(g, h->s[0], h->s[1], s2, dinv, r, w, sv, pv, h->part, sc);
+  TPF_CUDA_TRY(cudaGetLastError());
+  const long long key[6] = {(long long)nb, (long long)(intptr_t)dinv, (long long)(intptr_t)h->x,
+                            (long long)(intptr_t)r, (long long)n, (long long)(intptr_t)sc};
+  if (!h->cg_exec || std::memcmp(h->cg_key, key, sizeof(key)) != 0) {
+    if (h->cg_exec) { cudaGraphExecDestroy(h->cg_exec); h->cg_exec = nullptr; }
+    if (!h->cap && cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      h->cap = nullptr;
+      tpf::set_error("cudaStreamCreate failed");
+      return TPF_ECUDA;
+    }
+    TPF_CUDA_TRY(cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < kCgsChunk; ++k) {
+      cgs_update_kernel<<<h->ew_blocks, 256, 0, h->cap>>>(n, dinv, w, sv, pv, h->x, r, sc);
+      cgs_stencil_kernel<false><<<nb, 256, 0, h->cap>>>(g, h->s[0], h->s[1], s2, dinv, r, w, sv, pv, h->part, sc);
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(h->cap, &graph);
+    if (ce != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      cudaGetLastError();
+      tpf::set_error("capturing the PCG iteration chunk failed: %s", cudaGetErrorString(ce));
+      return TPF_ECUDA;
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&h->cg_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) {
+      h->cg_exec = nullptr;
+      cudaGetLastError();
+      tpf::set_error("instantiating the PCG iteration graph failed: %s", cudaGetErrorString(ie));
+      return TPF_ECUDA;
+    }
+    std::memcpy(h->cg_key, key, sizeof(key));
+  }
+  CgScal hs{};
+  TPF_CUDA_TRY(cudaMemcpyAsync(&hs, sc, sizeof(CgScal), cudaMemcpyDeviceToHost, s));
+  TPF_CUDA_TRY(cudaStreamSynchronize(s));
+  while (!hs.done) {
+    TPF_CUDA_TRY(cudaGraphLaunch(h->cg_exec, s));
+    TPF_CUDA_TRY(cudaMemcpyAsync(&hs, sc, sizeof(CgScal), cudaMemcpyDeviceToHost, s));
+    TPF_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  if (hs.bb == 0.0) TPF_CUDA_TRY(cudaMemsetAsync(h->x, 0, sizeof(double) * n, s));
+  copy_pin0_kernel<<<ew_grid(h), 256, 0, s>>>(n, g.pin, h->x, p);
+  TPF_CUDA_TRY(cudaGetLastError());
+  TPF_CUDA_TRY(cudaStreamSynchronize(s));
+  res->iterations = hs.it;
+  res->applies = hs.applies;
+  res->refinements = 0;
+  res->rel_residual = hs.bb > 0.0 ? std::sqrt(hs.rr / hs.bb) : 0.0;
+  res->info = hs.conv ? 0 : (int)std::min<long long>(h->o.maxiter, 0x7fffffff);
+  if (!hs.conv) {
+    tpf::set_error("PPESolverFVMMatrixFree did not converge cleanly (info=%d); no alternate PPE solver was applied.",
+                   res->info);
+    return TPF_ENOCONV;
+  }
+  return TPF_OK;
+}
+
 int solve_cg(tpf_ppe* h, const double* rhs, double* p, const double* p_init, cudaStream_t s,
              tpf_ppe_result* res) {
   const Grid3& g = h->g;
@@ -1800,6 +1724,8 @@ int solve_cg(tpf_ppe* h, const double* rhs, double* p, const double* p_init, cud
   a.err = h->err;
   a.st = h->st;
   const bool mixed = (h->o.precision == TPF_PREC_MIXED);
+  if (!mixed && (h->cg_kernel == 3 || (h->cg_kernel == 0 && g.N2 > 0)))
+    return solve_cg_stream(h, rhs, p, p_init, s, res);
   a.maxiter = h->o.maxiter;
   a.replace_drop = h->o.inner_tol > 0.0 ? h->o.inner_tol : 1e-3;
   BandPlan bp;
@@ -1966,6 +1892,7 @@ int tpf_ppe_create(tpf_ppe** out, int ndim, const int64_t* N, const double* cons
 int tpf_ppe_destroy(tpf_ppe* h) {
   if (!h) return TPF_OK;
   if (h->gm_exec) cudaGraphExecDestroy(h->gm_exec);
+  if (h->cg_exec) cudaGraphExecDestroy(h->cg_exec);
   if (h->cap) cudaStreamDestroy(h->cap);
   for (void* p : h->allocs) cudaFree(p);
   delete h;
@@ -1974,8 +1901,8 @@ int tpf_ppe_destroy(tpf_ppe* h) {
 
 int tpf_ppe_set_cg_kernel(tpf_ppe* h, int kind) {
   TPF_CHECK_ARG(h != nullptr, "null handle");
-  TPF_CHECK_ARG(kind >= 0 && kind <= 2, "CG kernel must be 0 (auto), 1 (global memory) or 2 (band-resident), got %d",
-                kind);
+  TPF_CHECK_ARG(kind >= 0 && kind <= 3,
+                "CG kernel must be 0 (auto), 1 (global memory), 2 (band-resident) or 3 (streaming), got %d", kind);
   h->cg_kernel = kind;
   return TPF_OK;
 }
@@ -2240,6 +2167,8 @@ double* g_static_ptr[kStaticMaxDevices] = {};
 
 // Device address of g_static_ws for the current device, looked up once per
 // device (the first call on a device does the lookup; later calls reuse it).
+// Under lazy module loading the lookup also loads the module, which reserves
+// the array's device memory.  A cudaDeviceReset invalidates the kept address.
 int static_workspace(double** out) {
   int dev = -1;
   TPF_CUDA_TRY(cudaGetDevice(&dev));

@@ -22,6 +22,7 @@ restatement of one reference pipeline variant.
 from __future__ import annotations
 
 import ctypes as C
+import math
 from types import SimpleNamespace
 
 from . import _lib
@@ -49,15 +50,22 @@ class TwoPhaseStep:
     def __init__(self, grid, psi, Re=100.0, Fr=1.0, We=10.0, rho_ratio=1e-3, mu_ratio=1e-2, cfl=0.3,
                  eps=None, reinit_steps=4, ppe_tol=1e-8, ppe_maxiter=20000, use_graphs=True,
                  convection="ccd", transport_mass_correction=False, reinit_bc="zero", ppe_method="cg",
-                 no_slip=False):
+                 no_slip=False, zero_velocity_shortcut=False):
         """The keyword options after ``use_graphs`` select the reference
         quick-start pipeline's components (simulation/_core.py:126-172):
         ``convection="uccd6"``, ``transport_mass_correction=True``,
         ``reinit_bc="neumann"``, ``ppe_method="gmres"`` (GMRES(80) with the
         exact line preconditioner) and ``no_slip=True`` (every velocity
         component zeroed on every wall plane of u* and of the corrected u,
-        simulation/boundary_condition.py:22-70).  The defaults keep the
-        CCD convection, Jacobi-PCG composition."""
+        simulation/boundary_condition.py:22-70).  ``zero_velocity_shortcut``
+        skips the transport stages while the velocity is exactly zero (before
+        the first step), as the reference's CPU backend does
+        (levelset/fccd_advection.py:99-110).  The defaults keep the CCD
+        convection, Jacobi-PCG composition.
+
+        ``cfl_dt`` is the reference's CFLCalculator (time_integration/cfl.py:
+        58-137) with Crank-Nicolson viscosity: the convective bound and the
+        capillary bound cfl * sqrt((1 + rho_ratio) We h^3 / (2 pi))."""
         torch = _torch()
         self.grid = grid
         nd = grid.ndim
@@ -87,6 +95,9 @@ class TwoPhaseStep:
         self.rho_l, self.rho_g, self.mu_l, self.mu_g = 1.0, rho_ratio, 1.0, mu_ratio
         self.cfl = cfl
         self.h = h
+        self._dt_sigma = math.sqrt((1.0 + rho_ratio) * We * h ** 3 / (2.0 * math.pi)) if We and We > 0.0 else None
+        self.zero_velocity_shortcut = bool(zero_velocity_shortcut)
+        self._vel_zero = True   # the velocity starts exactly zero
         dev = torch.device("cuda", torch.cuda.current_device())
         self.psi = torch.as_tensor(psi, dtype=torch.float64, device=dev).contiguous().clone()
         self.vel = [torch.zeros_like(self.psi) for _ in range(nd)]
@@ -105,7 +116,8 @@ class TwoPhaseStep:
     # -- phases ---------------------------------------------------------------
     def _phase1(self, dt):
         """psi, rho, mu, kappa, u* and the PPE right-hand side (no host sync)."""
-        psi = self.transport.advance(self.psi, self.vel, dt)
+        skip = self.zero_velocity_shortcut and self._vel_zero
+        psi = self.transport.advance(self.psi, self.vel, dt, velocity_is_zero=skip)
         psi = self.reinit.reinitialize(psi)
         self.psi.copy_(psi)
         rho, mu = update_properties(None, self.psi, self.rho_l, self.rho_g, self.mu_l, self.mu_g)
@@ -164,8 +176,12 @@ class TwoPhaseStep:
     # -- public ----------------------------------------------------------------
     def step(self, dt: float):
         """Advance one step with time step dt (the graphs belong to one dt)."""
-        if not self.use_graphs:
+        first = self._vel_zero
+        self._vel_zero = False
+        if not self.use_graphs or (first and self.zero_velocity_shortcut):
+            self._vel_zero = first   # read by _phase1 of this step only
             self._phase1(dt)
+            self._vel_zero = False
             self._solve()
             self._phase2(dt)
             return
@@ -180,6 +196,13 @@ class TwoPhaseStep:
         self._g2.replay()
 
     def cfl_dt(self) -> float:
-        """Convective CFL time step from the last step's velocity maxima (cfl.py:85-137)."""
+        """CFL time step from the last step's velocity maxima (cfl.py:85-137):
+        the smaller of the convective and the capillary bound, at least 1e-8."""
         m = self.maxima.cpu().tolist()
-        return self.cfl * self.h / max(sum(m[:self.nd]), 1.0e-14)
+        u_sum = 0.0
+        for v in m[:self.nd]:
+            u_sum = u_sum + v
+        cands = [self.cfl * self.h / max(u_sum, 1.0e-14)]
+        if self._dt_sigma is not None:
+            cands.append(self.cfl * self._dt_sigma)
+        return max(min(cands), 1.0e-8)

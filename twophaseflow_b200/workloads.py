@@ -126,6 +126,17 @@ def bubble_density(N, centre=(0.5, 0.5), radius: float = 0.25, rho_l: float = 1.
     return rho_g + (rho_l - rho_g) * psi
 
 
+def quickstart_psi(N=(64, 64), centre=(0.5, 0.5), radius: float = 0.25, eps_factor: float = 1.5):
+    """CLS field of the quick-start rising bubble: a gas bubble (psi ~ 0
+    inside) of radius 0.25 at the box centre, psi = 1/(1+exp(-(r-R)/eps)) with
+    eps = 1.5 h on the unit box (the reference's quick-start initial state)."""
+    coords = node_coords(N)
+    grids = np.meshgrid(*coords, indexing="ij")
+    eps = eps_factor / float(max(N))
+    r = np.sqrt(sum((g - c) ** 2 for g, c in zip(grids, centre)))
+    return 1.0 / (1.0 + np.exp(-(r - radius) / eps))
+
+
 def divergence_rhs(N, n_modes: int = 8, seed: int = 1):
     """rhs = div u for u_d = sum_m a_{m,d} prod_e sin/cos(pi k_{m,e} x_e + phi)."""
     ndim = len(N)
