@@ -375,16 +375,6 @@ int tpf_ppe_set_options(tpf_ppe* h, const tpf_ppe_options* opts);
  *     replayed from a CUDA graph.  The mixed-precision route keeps 1. */
 int tpf_ppe_set_cg_kernel(tpf_ppe* h, int kind);
 
-/* GMRES cycle implementation (no counterpart in the reference; numerics
- * unchanged): 0 (default) = the persistent kernel when it applies and the
- * system has at most 2^17 nodes, else 1; 1 = the restart cycle as a captured
- * graph of per-column kernels replayed on the stream (any system);
- * 2 = one cooperative launch per restart cycle with grid barriers between the
- *     column's phases (the Jacobi, no or the exact line preconditioner with
- *     lines of at most 1056 nodes, restart <= 128); TPF_EINVAL from
- *     tpf_ppe_solve when it does not apply. */
-int tpf_ppe_set_gmres_kernel(tpf_ppe* h, int kind);
-
 /* Build face coefficients, Jacobi diagonal and line-preconditioner state
  * from rho (device, grid shape, FP64).  Replaces prepare_operator /
  * _prepare_preconditioner_state (fvm_matrixfree.py:262-279,352-363;

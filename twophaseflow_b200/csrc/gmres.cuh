@@ -321,22 +321,9 @@ struct GmresOutcome {
 // return W.x holds the iterate.  key_a / key_b: the caller's part of the
 // cycle graph's key (what its operator launches depend on besides the
 // buffers).
-//
-// cycle(stream, m, used): optional replacement of the captured cycle graph
-// (a persistent kernel running the m Arnoldi columns with the same state
-// updates); it sets used = true when it ran the cycle, false to fall back to
-// the graph.
-struct NoCycle {
-  int operator()(cudaStream_t, int, bool& used) const {
-    used = false;
-    return TPF_OK;
-  }
-};
-
-template <class Apply, class Resid, class Precond, class Cycle = NoCycle>
+template <class Apply, class Resid, class Precond>
 int gmres_solve(GmresWork& W, int restart, double tol, long long maxiter, bool x_nonzero, long long key_a,
-                long long key_b, Apply apply, Resid resid, Precond precond, cudaStream_t s, GmresOutcome& out,
-                Cycle cycle = Cycle()) {
+                long long key_b, Apply apply, Resid resid, Precond precond, cudaStream_t s, GmresOutcome& out) {
   const int n = W.n;
   int st;
   const int m = std::min(restart, n);
@@ -424,9 +411,7 @@ int gmres_solve(GmresWork& W, int restart, double tol, long long maxiter, bool x
     double v0n = 0.0;
     if ((st = gm_read_scalar(wnorm, &v0n, s))) return st;
     gm_start_kernel<<<W.ew_blocks, 256, 0, s>>>(n, W.w, W.V, S, m + 1, W.gst, v0n, ptol);
-    bool used = false;
-    if ((st = cycle(s, m, used))) return st;
-    if (!used && (!*W.exec || std::memcmp(W.key, key, sizeof(key)) != 0)) {
+    if (!*W.exec || std::memcmp(W.key, key, sizeof(key)) != 0) {
       if (*W.exec) { cudaGraphExecDestroy(*W.exec); *W.exec = nullptr; }
       // captured on a private stream (the caller's may be the legacy default
       // stream, which cannot be captured); replayed on the caller's
@@ -457,7 +442,7 @@ int gmres_solve(GmresWork& W, int restart, double tol, long long maxiter, bool x
       }
       std::memcpy(W.key, key, sizeof(key));
     }
-    if (!used) TPF_CUDA_TRY(cudaGraphLaunch(*W.exec, s));
+    TPF_CUDA_TRY(cudaGraphLaunch(*W.exec, s));
     GmState hs{};
     TPF_CUDA_TRY(cudaMemcpyAsync(&hs, W.gst, sizeof(GmState), cudaMemcpyDeviceToHost, s));
     TPF_CUDA_TRY(cudaStreamSynchronize(s));

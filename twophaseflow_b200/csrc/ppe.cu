@@ -1094,345 +1094,6 @@ __global__ void __launch_bounds__(kThreads, 1) cg1_band_kernel(BandArgs a) {
 
 namespace {
 
-// ---- persistent GMRES cycle (small systems) ------------------------------------------
-//
-// One restart cycle of the device GMRES (gmres.cuh: SciPy's left-preconditioned
-// GMRES, classical Gram-Schmidt with conditional re-orthogonalization) in ONE
-// cooperative launch for the FVM operator: per Arnoldi column the operator,
-// the preconditioner (Jacobi, none, or the exact line solves with one warp per
-// line), the Gram-Schmidt inner products and updates, the norm and the Givens
-// step, separated by grid barriers on a monotonic counter (bounded waits ->
-// error flag).  On small grids (the 65^2 quick-start) the graph of ~15
-// kernels per column is bound by launch gaps; here a column costs 4-6
-// barriers.  Every CTA repeats the scalar Hessenberg / Givens arithmetic on
-// the same summed inner products in its own shared memory (identical
-// results, no extra barrier); CTA 0 writes the state the host reads.  Vectors
-// other CTAs wrote during the launch are read through L2 (ld.global.cg).
-constexpr int kGmpThreads = 256;
-constexpr int kGmpMaxCols = 128;
-
-struct GmpArgs {
-  Grid3 g;
-  Geo geo;
-  const double* s0;
-  const double* s1;
-  const double* s2;
-  int precond;
-  const double* dinvL;
-  const double* tlo[3];
-  const double* tden[3];
-  const double* tcp[3];
-  LineArgs L[3];
-  int ndim;
-  double* V;
-  int m;
-  int ldh;
-  double* H;
-  double* givens;
-  double* S;
-  GmState* st;
-  double* t;
-  double* w;
-  double* part;   // [(m + 2) slots][gridDim.x]
-  unsigned int* count;
-  int* err;
-};
-
-struct GmpBarrier {
-  unsigned int* count;
-  int* err;
-  GmState* st;
-  unsigned int nb;
-  unsigned int epoch;
-  __device__ __forceinline__ bool sync() {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      __threadfence();
-      red_release_add(count, 1u);
-      const unsigned int target = (epoch + 1) * nb;
-      int ok = 1;
-      long long spins = 0;
-      while (ld_acquire(count) < target) {
-        if (++spins > kSpinLimit * 8) { atomicExch(err, 1); ok = 0; break; }
-        if ((spins & 1023) == 0 && *(volatile int*)err) { ok = 0; break; }
-      }
-      if (!ok) {   // end the cycle: the host sees breakdown and then the error flag
-        st->breakdown = 1;
-        st->done = 1;
-      }
-      s_ok = ok;
-    }
-    __syncthreads();
-    ++epoch;
-    return s_ok != 0;
-  }
-};
-
-// the line solve of thomas_warp_line with L2 loads of r and out (written by
-// other CTAs in this launch)
-template <bool ACC, int K>
-__device__ __forceinline__ void gmp_thomas_line(const LineArgs& L, const double* __restrict__ lo,
-                                                const double* __restrict__ den, const double* __restrict__ cp,
-                                                const double* r, double* out, int pin, double scale, int l,
-                                                int lane) {
-  const int b = line_base(L, l);
-  const int n = L.n;
-  const int i0 = lane * K;
-  double rr[K], tmp[K];
-  double A = 1.0, B = 0.0;
-#pragma unroll
-  for (int q = 0; q < K; ++q) {
-    const int i = i0 + q;
-    rr[q] = 0.0;
-    if (i < n) {
-      const int e = b + i * L.stride;
-      const double ri = (e == pin) ? 0.0 : __ldcg(r + e);
-      rr[q] = ri;
-      const double d = den[e];
-      if (i == 0) { A = 0.0; B = ri / d; }
-      else {
-        const double mm = lo[e];
-        A = -mm * A / d;
-        B = (ri - mm * B) / d;
-      }
-    }
-  }
-#pragma unroll
-  for (int sft = 1; sft < 32; sft <<= 1) {
-    const double Ap = __shfl_up_sync(0xffffffffu, A, sft), Bp = __shfl_up_sync(0xffffffffu, B, sft);
-    if (lane >= sft) { B = A * Bp + B; A = A * Ap; }
-  }
-  double y = __shfl_up_sync(0xffffffffu, B, 1);
-  if (lane == 0) y = 0.0;
-#pragma unroll
-  for (int q = 0; q < K; ++q) {
-    const int i = i0 + q;
-    if (i < n) {
-      const int e = b + i * L.stride;
-      y = (i == 0) ? rr[q] / den[e] : (rr[q] - lo[e] * y) / den[e];
-    }
-    tmp[q] = y;
-  }
-  double C = 1.0, D = 0.0;
-#pragma unroll
-  for (int q = K - 1; q >= 0; --q) {
-    const int i = i0 + q;
-    if (i < n) {
-      if (i == n - 1) { C = 0.0; D = tmp[q]; }
-      else {
-        const double c = cp[b + i * L.stride];
-        D = tmp[q] - c * D;
-        C = -c * C;
-      }
-    }
-  }
-#pragma unroll
-  for (int sft = 1; sft < 32; sft <<= 1) {
-    const double Cn = __shfl_down_sync(0xffffffffu, C, sft), Dn = __shfl_down_sync(0xffffffffu, D, sft);
-    if (lane + sft < 32) { D = C * Dn + D; C = C * Cn; }
-  }
-  double x = __shfl_down_sync(0xffffffffu, D, 1);
-  if (lane == 31) x = 0.0;
-#pragma unroll
-  for (int q = K - 1; q >= 0; --q) {
-    const int i = i0 + q;
-    if (i < n) {
-      const int e = b + i * L.stride;
-      x = (i == n - 1) ? tmp[q] : tmp[q] - cp[e] * x;
-      if (ACC) {
-        const double v = (__ldcg(out + e) + x) * scale;
-        out[e] = (e == pin) ? 0.0 : v;
-      } else {
-        out[e] = x;
-      }
-    }
-  }
-}
-
-template <int K>
-__global__ void __launch_bounds__(kGmpThreads, 1) gmres_cycle_kernel(const __grid_constant__ GmpArgs a) {
-  __shared__ double sh_h[kGmpMaxCols + 2];      // this column's Gram-Schmidt coefficients
-  __shared__ double sh_h2[kGmpMaxCols + 2];     // second-pass coefficients
-  __shared__ double sh_col[kGmpMaxCols + 2];    // Hessenberg column being rotated
-  __shared__ double sh_g[2 * kGmpMaxCols];      // Givens pairs of this cycle
-  __shared__ double sh_S[kGmpMaxCols + 2];      // residual vector
-  __shared__ double sh_red[8 * 32];
-  __shared__ double sh_scal[4];                 // scal, h0, reorth, done
-  const Grid3& g = a.g;
-  const int n = g.ndof;
-  const int nb = gridDim.x;
-  const int chunk = (n + nb - 1) / nb;
-  const int beg = blockIdx.x * chunk, end = min(n, beg + chunk);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = kGmpThreads / 32;
-  const int gwarp = blockIdx.x * nw + wid, nwarps = nb * nw;
-  GmpBarrier bar{a.count, a.err, a.st, (unsigned int)nb, 0u};
-  for (int k = threadIdx.x; k < kGmpMaxCols + 2; k += blockDim.x) sh_S[k] = (k <= a.m) ? a.S[k] : 0.0;
-  __syncthreads();
-  const double ptol = a.st->ptol;
-  const double eps = 2.220446049250313e-16;
-  for (int col = 0; col < a.m; ++col) {
-    // v_col complete (written by every CTA in the previous column or by gm_start)
-    if (!bar.sync()) return;
-    const double* vc = a.V + (size_t)col * n;
-    // ---- operator (and pointwise preconditioner) ----
-    double* dst = (a.precond == TPF_PRECOND_LINE) ? a.t : a.w;
-    for (int idx = beg + threadIdx.x; idx < end; idx += blockDim.x) {
-      double v;
-      if (idx == g.pin) {
-        v = __ldcg(vc + idx);
-      } else {
-        int i0, i1, i2;
-        coords3(g, idx, i0, i1, i2);
-        double d, off;
-        s_row<double>(g, idx, i0, i1, i2, a.s0, a.s1, a.s2, [&](int j) { return __ldcg(vc + j); }, d, off);
-        const double W = a.geo.dv[0][i0] * a.geo.dv[1][i1] * (g.N2 > 0 ? a.geo.dv[2][i2] : 1.0);
-        v = (off - d * __ldcg(vc + idx)) / W;
-      }
-      if (a.precond == TPF_PRECOND_JACOBI) v = (idx == g.pin) ? 0.0 : v * a.dinvL[idx];
-      dst[idx] = v;
-    }
-    if (a.precond == TPF_PRECOND_LINE) {
-      // additive shifted line solves: w = (sum_a T_a^-1 t) / ndim
-      for (int ax = 0; ax < a.ndim; ++ax) {
-        if (!bar.sync()) return;
-        const LineArgs& L = a.L[ax];
-        const double sc = (ax == a.ndim - 1) ? 1.0 / a.ndim : 1.0;
-        for (int l = gwarp; l < L.lines; l += nwarps) {
-          if (ax == 0) gmp_thomas_line<false, K>(L, a.tlo[ax], a.tden[ax], a.tcp[ax], a.t, a.w, g.pin, 1.0, l, lane);
-          else gmp_thomas_line<true, K>(L, a.tlo[ax], a.tden[ax], a.tcp[ax], a.t, a.w, g.pin, sc, l, lane);
-        }
-      }
-      if (!bar.sync()) return;   // line solves finished before the inner products
-    }
-    // ---- Gram-Schmidt: <V_k, w> (k <= col) and, in the first pass, <w, w> ----
-    for (int pass = 0; pass < 2; ++pass) {
-      const int nv = col + 1 + (pass == 0 ? 1 : 0);   // slot col + 1 = <w, w> in the first pass
-      for (int k0 = 0; k0 < nv; k0 += 8) {
-        double acc[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) acc[j] = 0.0;
-        for (int idx = beg + threadIdx.x; idx < end; idx += blockDim.x) {
-          const double wi = __ldcg(a.w + idx);
-#pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const int k = k0 + j;
-            if (k < nv) acc[j] += ((k <= col) ? a.V[(size_t)k * n + idx] : wi) * wi;
-          }
-        }
-        tpf::block_sum<8>(acc, sh_red);
-        if (threadIdx.x < 8 && k0 + (int)threadIdx.x < nv)
-          a.part[(size_t)(k0 + threadIdx.x) * nb + blockIdx.x] = acc[threadIdx.x];
-      }
-      if (!bar.sync()) return;
-      // sums of the partials in block order (same tree in every CTA)
-      double* hsum = (pass == 0) ? sh_h : sh_h2;
-      for (int k = wid; k < nv; k += nw) {
-        double acc = 0.0;
-        for (int b = lane; b < nb; b += 32) acc += __ldcg(a.part + (size_t)k * nb + b);
-        acc = tpf::warp_sum(acc);
-        if (lane == 0) hsum[k] = acc;
-      }
-      __syncthreads();
-      if (pass == 0) {
-        if (threadIdx.x == 0) {
-          const double sw = sh_h[col + 1];
-          double proj = 0.0;
-          for (int q = 0; q <= col; ++q) proj += sh_h[q] * sh_h[q];
-          sh_scal[1] = sqrt(sw);
-          sh_scal[2] = (sw - proj < 0.5 * sw) ? 1.0 : 0.0;
-        }
-        __syncthreads();
-      }
-      // w -= sum_k h_k V_k on own nodes
-      for (int idx = beg + threadIdx.x; idx < end; idx += blockDim.x) {
-        double acc = __ldcg(a.w + idx);
-        for (int k = 0; k <= col; ++k) acc -= hsum[k] * a.V[(size_t)k * n + idx];
-        a.w[idx] = acc;
-      }
-      if (sh_scal[2] == 0.0) break;   // no re-orthogonalization pass
-      if (!bar.sync()) return;         // partial slots are reused
-    }
-    // ---- ||w|| ----
-    {
-      double acc[1] = {0.0};
-      for (int idx = beg + threadIdx.x; idx < end; idx += blockDim.x) {
-        const double wi = a.w[idx];
-        acc[0] += wi * wi;
-      }
-      tpf::block_sum<1>(acc, sh_red);
-      // slot m + 1: never used by the Gram-Schmidt passes (slots <= col + 1 <= m)
-      if (threadIdx.x == 0) a.part[(size_t)(a.m + 1) * nb + blockIdx.x] = acc[0];
-    }
-    if (!bar.sync()) return;
-    if (wid == 0) {
-      double acc = 0.0;
-      for (int b = lane; b < nb; b += 32) acc += __ldcg(a.part + (size_t)(a.m + 1) * nb + b);
-      acc = tpf::warp_sum(acc);
-      // ---- Hessenberg column, Givens rotations, residual estimate (gm_column_kernel) ----
-      if (lane == 0) {
-        const bool reorth = sh_scal[2] != 0.0;
-        for (int k = 0; k <= col; ++k) sh_col[k] = sh_h[k] + (reorth ? sh_h2[k] : 0.0);
-        const double h1 = sqrt(acc);
-        sh_col[col + 1] = h1;
-        int breakdown = 0;
-        double scal;
-        if (h1 <= eps * sh_scal[1]) {
-          sh_col[col + 1] = 0.0;
-          breakdown = 1;
-          scal = 1.0;
-        } else {
-          scal = 1.0 / h1;
-        }
-        for (int k = 0; k < col; ++k) {
-          const double c = sh_g[2 * k], sn = sh_g[2 * k + 1];
-          const double n0 = sh_col[k], n1 = sh_col[k + 1];
-          sh_col[k] = c * n0 + sn * n1;
-          sh_col[k + 1] = -sn * n0 + c * n1;
-        }
-        double c, sn, mag;
-        givens_rot(sh_col[col], sh_col[col + 1], c, sn, mag);
-        sh_g[2 * col] = c;
-        sh_g[2 * col + 1] = sn;
-        sh_col[col] = mag;
-        sh_col[col + 1] = 0.0;
-        const double tt = -sn * sh_S[col];
-        sh_S[col] = c * sh_S[col];
-        sh_S[col + 1] = tt;
-        const double presid = fabs(tt);
-        const int done = (presid <= ptol || breakdown) ? 1 : 0;
-        sh_scal[0] = scal;
-        sh_scal[3] = done;
-        if (blockIdx.x == 0) {
-          double* hc = a.H + (size_t)col * a.ldh;
-          for (int k = 0; k <= col + 1; ++k) hc[k] = sh_col[k];
-          a.givens[2 * col] = c;
-          a.givens[2 * col + 1] = sn;
-          a.S[col] = sh_S[col];
-          a.S[col + 1] = sh_S[col + 1];
-          a.st->presid = presid;
-          a.st->ncols = col + 1;
-          a.st->breakdown = breakdown;
-          a.st->reorth = reorth ? 1 : 0;
-          a.st->h0 = sh_scal[1];
-          a.st->scal = scal;
-          a.st->done = done;
-        }
-      }
-    }
-    __syncthreads();
-    // v_{col+1} = w * scal (also when this column ended the cycle)
-    const double scal = sh_scal[0];
-    double* vn = a.V + (size_t)(col + 1) * n;
-    for (int idx = beg + threadIdx.x; idx < end; idx += blockDim.x) vn[idx] = a.w[idx] * scal;
-    if (sh_scal[3] != 0.0) break;
-  }
-}
-
-}  // namespace
-
-namespace {
-
 // ---- streaming PCG (large systems) --------------------------------------------------
 //
 // The same Jacobi-PCG recurrences as cg1_kernel (Chronopoulos-Gear, one
@@ -1718,7 +1379,6 @@ struct tpf_ppe {
   double* band_pub = nullptr;     // halo rows of the band-resident PCG
   size_t band_pub_len = 0;
   int cg_kernel = 0;              // 0 auto, 1 global-memory persistent PCG, 2 band-resident PCG
-  int gm_kernel = 0;              // 0 auto, 1 captured cycle graph, 2 persistent cycle kernel
   SolveStatus* st = nullptr;
   int coop_blocks = 0;
   int ew_blocks = 0;
@@ -1909,82 +1569,10 @@ int solve_gmres(tpf_ppe* h, const double* rhs, double* p, const double* p_init, 
   auto precond = [&](const double* in, double* out, cudaStream_t cs, const int* done) -> int {
     return precond_L(h, in, out, cs, done);
   };
-  // persistent cycle kernel: FVM operator with Jacobi / none / exact line
-  // solves (lines up to 32 x 33 nodes), restart <= kGmpMaxCols; the default
-  // for systems up to 2^17 nodes
-  int max_line = 0, max_lines = 0;
-  for (int ax = 0; ax < h->ndim; ++ax) {
-    const LineArgs L = line_args(g, ax);
-    max_line = std::max(max_line, L.n);
-    max_lines = std::max(max_lines, L.lines);
-  }
-  const bool gmp_ok = (h->o.precond == TPF_PRECOND_NONE || h->o.precond == TPF_PRECOND_JACOBI ||
-                       h->o.precond == TPF_PRECOND_LINE) &&
-                      std::min(h->o.restart, n) <= kGmpMaxCols && max_line <= 32 * 33;
-  if (h->gm_kernel == 2 && !gmp_ok) {
-    tpf::set_error("the persistent GMRES cycle needs Jacobi, no or the exact line preconditioner, restart <= %d "
-                   "and lines of at most 1056 nodes", kGmpMaxCols);
-    return TPF_EINVAL;
-  }
-  const bool use_gmp = gmp_ok && (h->gm_kernel == 2 || (h->gm_kernel == 0 && n <= (1 << 17)));
-  int gmp_blocks = 0;
-  void* gmp_fn = nullptr;
-  if (use_gmp) {
-    const int K = (max_line <= 32 * 4) ? 4 : (max_line <= 32 * 9) ? 9 : (max_line <= 32 * 17) ? 17 : 33;
-    gmp_fn = (K == 4) ? (void*)gmres_cycle_kernel<4> : (K == 9) ? (void*)gmres_cycle_kernel<9>
-           : (K == 17) ? (void*)gmres_cycle_kernel<17> : (void*)gmres_cycle_kernel<33>;
-    int per_sm = 0;
-    TPF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gmp_fn, kGmpThreads, 0));
-    const int cap = std::max(1, per_sm) * tpf::sm_count();
-    const int want = std::max((n + 1023) / 1024, h->o.precond == TPF_PRECOND_LINE ? (max_lines + 7) / 8 : 1);
-    gmp_blocks = std::max(1, std::min(std::min(cap, want), h->part_len / (std::min(h->o.restart, n) + 2)));
-  }
-  auto cycle = [&](cudaStream_t cs, int m, bool& used) -> int {
-    used = false;
-    if (!use_gmp) return TPF_OK;
-    GmpArgs ga{};
-    ga.g = g;
-    ga.geo = geo;
-    ga.s0 = h->s[0]; ga.s1 = h->s[1]; ga.s2 = h->s[2];
-    ga.precond = (h->o.precond == TPF_PRECOND_LINE) ? TPF_PRECOND_LINE : h->o.precond;
-    ga.dinvL = h->dinvL;
-    for (int ax = 0; ax < 3; ++ax) {
-      ga.tlo[ax] = h->tlo[ax]; ga.tden[ax] = h->tden[ax]; ga.tcp[ax] = h->tcp[ax];
-      if (ax < h->ndim) ga.L[ax] = line_args(g, ax);
-    }
-    ga.ndim = h->ndim;
-    ga.V = h->V;
-    ga.m = m;
-    ga.ldh = h->o.restart + 2;
-    ga.H = h->gm;
-    ga.givens = ga.H + (size_t)h->o.restart * ga.ldh;
-    ga.S = ga.givens + 2 * h->o.restart;
-    ga.st = h->gst;
-    ga.t = h->q;
-    ga.w = h->z;
-    ga.part = h->part;
-    ga.count = h->bar;
-    ga.err = h->err;
-    TPF_CUDA_TRY(cudaMemsetAsync(h->bar, 0, 2 * sizeof(unsigned int), cs));
-    void* args[] = {&ga};
-    TPF_CUDA_TRY(cudaLaunchCooperativeKernel(gmp_fn, dim3(gmp_blocks), dim3(kGmpThreads), args, 0, cs));
-    used = true;
-    return TPF_OK;
-  };
-  if (use_gmp) TPF_CUDA_TRY(cudaMemsetAsync(h->err, 0, sizeof(int), s));
   GmresOutcome o;
   st = gmres_solve(W, h->o.restart, h->o.tol, h->o.maxiter, p_init != nullptr, (long long)h->o.precond,
-                   (long long)h->o.pcr_stages, apply, resid, precond, s, o, cycle);
+                   (long long)h->o.pcr_stages, apply, resid, precond, s, o);
   if (st) return st;
-  if (use_gmp) {
-    int herr = 0;
-    TPF_CUDA_TRY(cudaMemcpyAsync(&herr, h->err, sizeof(int), cudaMemcpyDeviceToHost, s));
-    TPF_CUDA_TRY(cudaStreamSynchronize(s));
-    if (herr) {
-      tpf::set_error("GMRES cycle grid barrier timed out; the solve was aborted");
-      return TPF_EABORT;
-    }
-  }
   if (o.bnrm2 == 0.0) {
     TPF_CUDA_TRY(cudaMemsetAsync(p, 0, sizeof(double) * n, s));
     TPF_CUDA_TRY(cudaStreamSynchronize(s));
@@ -2388,14 +1976,6 @@ int tpf_ppe_set_cg_kernel(tpf_ppe* h, int kind) {
   TPF_CHECK_ARG(kind >= 0 && kind <= 3,
                 "CG kernel must be 0 (auto), 1 (global memory), 2 (band-resident) or 3 (streaming), got %d", kind);
   h->cg_kernel = kind;
-  return TPF_OK;
-}
-
-int tpf_ppe_set_gmres_kernel(tpf_ppe* h, int kind) {
-  TPF_CHECK_ARG(h != nullptr, "null handle");
-  TPF_CHECK_ARG(kind >= 0 && kind <= 2,
-                "GMRES kernel must be 0 (auto), 1 (captured cycle graph) or 2 (persistent cycle), got %d", kind);
-  h->gm_kernel = kind;
   return TPF_OK;
 }
 
