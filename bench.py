@@ -486,12 +486,12 @@ def main(argv=None):
     from twophaseflow_b200.kernel_cases import viscous_case
     visb = viscous_case((256, 256, 256), "f64", 2)
 
-    # one whole two-phase time step, 3-D 192^3 rising bubble (density ratio 1000):
-    # pre-PPE work and corrector as replayed CUDA graphs, the PPE solve between
-    # them; fixed dt = h/4 (a measurement of the step's work, not a validated run)
+    # whole two-phase time steps, 3-D 192^3 rising bubble (density ratio 1000):
+    # CFL time step with the capillary bound, the step (pressure solve
+    # included) replayed as one CUDA graph
     try:
         from twophaseflow_b200.kernel_cases import step_case
-        stepb = step_case((192, 192, 192), 2)
+        stepb = step_case((192, 192, 192), 4)
     except Exception as exc:   # the headline line must still print
         stepb = {"error": f"{type(exc).__name__}: {exc}"[:200]}
 

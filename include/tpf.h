@@ -360,8 +360,8 @@ int tpf_ppe_create(tpf_ppe** h, int ndim, const int64_t* N,
 int tpf_ppe_destroy(tpf_ppe* h);
 int tpf_ppe_set_options(tpf_ppe* h, const tpf_ppe_options* opts);
 /* Kernel of the FP64 CG solve (same iteration, same stopping rule):
- * 0 (default) = the band-resident kernel when it applies, else 3 for 3-D
- *     FP64 systems, else 1;
+ * 0 (default) = the band-resident kernel when it applies, else 3 for FP64
+ *     systems, else (mixed precision) 1;
  * 1 = one persistent cooperative launch with every vector in global memory
  *     (any grid, FP64 or mixed);
  * 2 = the band-resident kernel: 2-D systems whose nodes, split into one
@@ -374,6 +374,18 @@ int tpf_ppe_set_options(tpf_ppe* h, const tpf_ppe_options* opts);
  *     advancing the scalars on the device), chunks of 32 iterations
  *     replayed from a CUDA graph.  The mixed-precision route keeps 1. */
 int tpf_ppe_set_cg_kernel(tpf_ppe* h, int kind);
+
+/* Stream capture (no counterpart in the reference, which has no CUDA graphs):
+ * tpf_ppe_solve with method TPF_PPE_CG may be called while `stream` is being
+ * captured into a CUDA graph.  The whole solve is then recorded in the graph
+ * (the persistent kernels as one cooperative launch; the streaming PCG as a
+ * conditional WHILE node whose body runs 32 iterations and re-tests the
+ * device-side convergence state), nothing is read back, and the result
+ * fields are -1.  After a replay, tpf_ppe_read_result synchronizes `stream`
+ * and returns that replay's result and status (TPF_ENOCONV as tpf_ppe_solve).
+ * The GMRES route reads its residual on the host and returns TPF_EINVAL under
+ * capture. */
+int tpf_ppe_read_result(tpf_ppe* h, void* stream, tpf_ppe_result* result);
 
 /* Build face coefficients, Jacobi diagonal and line-preconditioner state
  * from rho (device, grid shape, FP64).  Replaces prepare_operator /

@@ -161,6 +161,7 @@ SIGNATURES = {
                                  C.POINTER(C.POINTER(C.c_double)), C.c_int64, C.POINTER(tpf_ppe_options)]),
     "tpf_ppe_destroy": (C.c_int, [C.c_void_p]),
     "tpf_ppe_set_options": (C.c_int, [C.c_void_p, C.POINTER(tpf_ppe_options)]),
+    "tpf_ppe_read_result": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "tpf_ppe_set_cg_kernel": (C.c_int, [C.c_void_p, C.c_int]),
     "tpf_ppe_prepare": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "tpf_ppe_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

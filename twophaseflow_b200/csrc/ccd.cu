@@ -174,6 +174,19 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
+// Stage a read-only table into shared memory with asynchronous copies: every
+// thread issues its share and waits once, so the copy costs one global round
+// trip rather than one per element a thread copies (a block of one warp and a
+// 700-entry table otherwise spends ~10 us here, longer than a small field's
+// whole solve).  Called before any other asynchronous copy of the block.
+template <typename T>
+__device__ __forceinline__ void stage_table(T* dst, const T* src, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) cp_async<sizeof(T)>(dst + i, src + i, true);
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+}
+
 // Issue the asynchronous copy of tile `t` (TL lines x n points) into fb.
 // Strided axis: fb[k*TL + l]; contiguous axis: fb[l*FS + k].  lb receives the
 // global base offset of each line (strided) for the output pass.
@@ -232,8 +245,7 @@ __global__ void __launch_bounds__(512, 1) ccd_line_kernel(CcdArgs a) {
 
   const T* __restrict__ f = static_cast<const T*>(a.f);
   const T* tabT = static_cast<const T*>(a.tabT);
-  for (int i = threadIdx.x; i < a.tab_total; i += blockDim.x) tab[i] = tabT[i];
-  __syncthreads();   // the table is read below (c1, c2) and in every phase
+  stage_table<T>(tab, tabT, a.tab_total);   // the table is read below (c1, c2) and in every phase
 
   const int tid = threadIdx.x;
   const int l = tid & (TL - 1), c = tid >> a.tl_shift;
@@ -643,7 +655,10 @@ __device__ __forceinline__ void issue_tile_padded(const CcdArgs& a, const T* __r
   cp_async_commit();
 }
 
-template <typename T, bool PERIODIC, bool CONTIG, int R>
+// W warps per line: the line's rows are cut into 32 W chunks of R rows (lane
+// l of warp w of the line owns chunk 32 w + l); the carry scans run within
+// each warp by shuffles, then across the line's warps through shared memory.
+template <typename T, bool PERIODIC, bool CONTIG, int R, int W>
 __global__ void __launch_bounds__(256) ccd_warp_kernel(CcdArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int TL = a.TL, n = a.n, n_rows = a.n_rows, H0 = a.H0, FSP = a.FS;
@@ -657,13 +672,15 @@ __global__ void __launch_bounds__(256) ccd_warp_kernel(CcdArgs a) {
 
   const T* __restrict__ f = static_cast<const T*>(a.f);
   const T* tabT = static_cast<const T*>(a.tabT);
-  for (int i = threadIdx.x; i < a.tab_total; i += blockDim.x) tab[i] = tabT[i];
-  __syncthreads();
+  stage_table<T>(tab, tabT, a.tab_total);
 
   const int lane = threadIdx.x & 31;
-  const int wl = threadIdx.x >> 5;              // line of the tile owned by this warp
-  const int j0 = lane * R;
+  const int wl = (threadIdx.x >> 5) / W;        // line of the tile owned by this warp
+  const int wq = (threadIdx.x >> 5) - wl * W;   // this warp's segment of the line
+  const int q = wq * 32 + lane;                 // chunk of the line owned by this lane
+  const int j0 = q * R;
   const int cnt = max(0, min(R, n_rows - j0));  // rows of this lane
+  __shared__ Aff<T> s_tot[8 * W];               // per line of the tile (TL <= 8): warp totals
   const T c1 = tab[lay.bc() + 30], c2 = tab[lay.bc() + 31];
   const T* Lfi = tab + lay.cst();
   const T Lf0 = Lfi[0], Lf1 = Lfi[1], Lf2 = Lfi[2], Lf3 = Lfi[3];
@@ -698,10 +715,10 @@ __global__ void __launch_bounds__(256) ccd_warp_kernel(CcdArgs a) {
 
     if (wl < TL) {
       // ---- closures (FP64, lanes 0 and last) --------------------------------
-      const int last = (n_rows - 1) / R;
+      const int last = (n_rows - 1) / R;   // chunk holding the last row
       double bl0 = 0.0, bl1 = 0.0, br0 = 0.0, br1 = 0.0;
       if (!PERIODIC) {
-        if (lane == 0) {
+        if (q == 0) {
           if (a.ovl) { bl0 = a.bcl0; bl1 = a.bcl1; }
           else {
             double fv[6];
@@ -711,7 +728,7 @@ __global__ void __launch_bounds__(256) ccd_warp_kernel(CcdArgs a) {
             bl1 = tb[24] * fv[0] + tb[25] * fv[1] + tb[26] * fv[2] + tb[27] * fv[3] + tb[28] * fv[4] + tb[29] * fv[5];
           }
         }
-        if (lane == last) {
+        if (q == last) {
           if (a.ovr) { br0 = a.bcr0; br1 = a.bcr1; }
           else {
             double fv[6];
@@ -779,14 +796,27 @@ __global__ void __launch_bounds__(256) ccd_warp_kernel(CcdArgs a) {
         }
         Aff<T> ex = aff_shfl_up(m, 1);
         if (lane == 0) ex = aff_identity<T>();
+        T l0 = __shfl_sync(0xffffffffu, m.v0, 31), l1 = __shfl_sync(0xffffffffu, m.v1, 31);
+        if (W > 1) {
+          // the warps before this one: P = total_{wq-1} o ... o total_0
+          if (lane == 31) s_tot[wl * W + wq] = m;
+          __syncthreads();
+          Aff<T> P = aff_identity<T>();
+          for (int v = 0; v < wq; ++v) P = aff_compose(s_tot[wl * W + v], P);
+          ex = aff_compose(ex, P);
+          Aff<T> all = P;
+          for (int v = wq; v < W; ++v) all = aff_compose(s_tot[wl * W + v], all);
+          l0 = all.v0;
+          l1 = all.v1;
+          __syncthreads();   // s_tot is reused by the backward scan
+        }
         V2<T> Yin{ex.v0, ex.v1};
         if (PERIODIC) {
-          // ring closure: Y_{-1} = Gf * (scan result of the last lane)
-          const T l0 = __shfl_sync(0xffffffffu, m.v0, 31), l1 = __shfl_sync(0xffffffffu, m.v1, 31);
+          // ring closure: Y_{-1} = Gf * (scan result of the last chunk)
           const V2<T> ring = mv(Lfi + 16, V2<T>{l0, l1});
           Yin = {ex.v0 + ex.m0 * ring.a + ex.m1 * ring.b, ex.v1 + ex.m2 * ring.a + ex.m3 * ring.b};
         }
-        if ((PERIODIC || lane > 0) && cnt > 0) {
+        if ((PERIODIC || q > 0) && cnt > 0) {
 #pragma unroll R
           for (int r = 0; r < R; ++r) {
             const int j = j0 + r;
@@ -833,13 +863,25 @@ __global__ void __launch_bounds__(256) ccd_warp_kernel(CcdArgs a) {
         }
         Aff<T> ex = aff_shfl_down(m, 1);
         if (lane == 31) ex = aff_identity<T>();
+        T l0 = __shfl_sync(0xffffffffu, m.v0, 0), l1 = __shfl_sync(0xffffffffu, m.v1, 0);
+        if (W > 1) {
+          // the warps after this one: Q = total_{wq+1} o ... o total_{W-1}
+          if (lane == 0) s_tot[wl * W + wq] = m;
+          __syncthreads();
+          Aff<T> Q = aff_identity<T>();
+          for (int v = W - 1; v > wq; --v) Q = aff_compose(s_tot[wl * W + v], Q);
+          ex = aff_compose(ex, Q);
+          Aff<T> all = Q;
+          for (int v = wq; v >= 0; --v) all = aff_compose(s_tot[wl * W + v], all);
+          l0 = all.v0;
+          l1 = all.v1;
+        }
         V2<T> Xin{ex.v0, ex.v1};
         if (PERIODIC) {
-          const T l0 = __shfl_sync(0xffffffffu, m.v0, 0), l1 = __shfl_sync(0xffffffffu, m.v1, 0);
           const V2<T> ring = mv(Lfi + 20, V2<T>{l0, l1});
           Xin = {ex.v0 + ex.m0 * ring.a + ex.m1 * ring.b, ex.v1 + ex.m2 * ring.a + ex.m3 * ring.b};
         }
-        if ((PERIODIC || lane < last) && cnt > 0) {
+        if ((PERIODIC || q < last) && cnt > 0) {
 #pragma unroll R
           for (int r = 0; r < R; ++r) {
             const int j = j0 + r;
@@ -862,12 +904,12 @@ __global__ void __launch_bounds__(256) ccd_warp_kernel(CcdArgs a) {
         }
       }
       if (!PERIODIC) {
-        if (lane == 0 && cnt > 0) {
+        if (q == 0 && cnt > 0) {
           const double x0 = (double)y[0].a, x1 = (double)y[0].b;
           fl[0] = (T)((tb[8] * x0 + tb[9] * x1) + bl0);
           sl[0] = (T)((tb[10] * x0 + tb[11] * x1) + bl1);
         }
-        if (lane == last) {
+        if (q == last) {
 #pragma unroll R
           for (int r = 0; r < R; ++r)
             if (r == cnt - 1) {
@@ -877,7 +919,7 @@ __global__ void __launch_bounds__(256) ccd_warp_kernel(CcdArgs a) {
               sl[k + k / R] = (T)((tb[14] * x0 + tb[15] * x1) + br1);
             }
         }
-      } else if (lane == 0) {
+      } else if (q == 0) {
         const int k = n - 1;
         fl[k + k / R] = y[0].a;
         sl[k + k / R] = y[0].b;
@@ -1001,8 +1043,7 @@ __global__ void __launch_bounds__(128) ccd_lane_kernel(CcdArgs a, const T* __res
   T* fb0 = lt + lt_pad + (size_t)wid * (NT * TR * TS + 64 * P);   // ring of f tiles [TR][TS]
   T* dt = fb0 + NBUF * TR * TS;                                       // contiguous axis: d2 tile
   T* cy = fb0 + NT * TR * TS;                                         // chunk-end carries [P][2][32]
-  for (int i = threadIdx.x; i < ltab_total; i += blockDim.x) lt[i] = ltab_g[i];
-  __syncthreads();
+  stage_table<T>(lt, ltab_g, ltab_total);
 
   const T* __restrict__ f = static_cast<const T*>(a.f);
   const TabLayout lay{a.C, a.H0};
@@ -1723,7 +1764,7 @@ LaunchShape pick_shape(const tpf_ccd_plan* p, bool contig, int64_t n_lines) {
 }
 
 template <typename T, int R>
-LaunchShape pick_warp_shape(const tpf_ccd_plan* p, int64_t n_lines) {
+LaunchShape pick_warp_shape(const tpf_ccd_plan* p, int64_t n_lines, int W) {
   const int n = (int)p->n_pts;
   int FSP = n + (n - 1) / R + 1;
   if (FSP % 2 == 0) ++FSP;
@@ -1736,7 +1777,8 @@ LaunchShape pick_warp_shape(const tpf_ccd_plan* p, int64_t n_lines) {
   const int tl_opts[4] = {8, 4, 2, 1};
   for (int t = 0; t < 4; ++t) {
     const int TL = tl_opts[t];
-    const int threads = 32 * TL;
+    const int threads = 32 * W * TL;
+    if (threads > 256) continue;
     const int64_t tiles = (n_lines + TL - 1) / TL;
     const size_t fsz = (size_t)TL * FSP;
     for (int nbuf = 2; nbuf >= 1; --nbuf) {
@@ -1868,11 +1910,10 @@ int launch_ccd(const tpf_ccd_plan* p, int64_t outer, int64_t inner, const void* 
   TPF_CHECK_ARG(!corrector || (f != corrector->cr_out && f != corrector->cr_u && f != corrector->cr_rho),
                 "the pressure must not alias the velocity or density arrays");
   TPF_CHECK_ARG(n_lines < ((int64_t)1 << 31), "too many lines");
-  const bool warp = (p->C == 8 || p->C == 16 || p->C == 32) && p->n_rows <= 32 * p->C;
-  LaunchShape s = !warp ? pick_shape<T>(p, contig, n_lines)
-                        : (p->C == 8 ? pick_warp_shape<T, 8>(p, n_lines)
-                                     : (p->C == 16 ? pick_warp_shape<T, 16>(p, n_lines)
-                                                   : pick_warp_shape<T, 32>(p, n_lines)));
+  // warp kernel: chunks of 8 rows, 1, 2 or 4 warps per line (lines up to 1024 rows)
+  const bool warp = p->C == 8 && p->n_rows <= 32 * 8 * 4;
+  const int W = p->n_rows <= 256 ? 1 : (p->n_rows <= 512 ? 2 : 4);
+  LaunchShape s = !warp ? pick_shape<T>(p, contig, n_lines) : pick_warp_shape<T, 8>(p, n_lines, W);
   TPF_CHECK_ARG(s.TL > 0, "CCD axis of %lld points does not fit the line kernel's shared memory",
                 (long long)p->n_pts);
   CcdArgs a{};
@@ -1908,18 +1949,17 @@ int launch_ccd(const tpf_ccd_plan* p, int64_t outer, int64_t inner, const void* 
   if (!warp) {
     if (per) kern = contig ? ccd_line_kernel<T, true, true> : ccd_line_kernel<T, true, false>;
     else kern = contig ? ccd_line_kernel<T, false, true> : ccd_line_kernel<T, false, false>;
-  } else if (p->C == 8) {
-    if (per) kern = contig ? ccd_warp_kernel<T, true, true, 8> : ccd_warp_kernel<T, true, false, 8>;
-    else kern = contig ? ccd_warp_kernel<T, false, true, 8> : ccd_warp_kernel<T, false, false, 8>;
-  } else if (p->C == 16) {
-    if (per) kern = contig ? ccd_warp_kernel<T, true, true, 16> : ccd_warp_kernel<T, true, false, 16>;
-    else kern = contig ? ccd_warp_kernel<T, false, true, 16> : ccd_warp_kernel<T, false, false, 16>;
   } else {
-    if (per) kern = contig ? ccd_warp_kernel<T, true, true, 32> : ccd_warp_kernel<T, true, false, 32>;
-    else kern = contig ? ccd_warp_kernel<T, false, true, 32> : ccd_warp_kernel<T, false, false, 32>;
+#define TPF_WARP_KERN(WW)                                                                               \
+  if (per) kern = contig ? ccd_warp_kernel<T, true, true, 8, WW> : ccd_warp_kernel<T, true, false, 8, WW>; \
+  else kern = contig ? ccd_warp_kernel<T, false, true, 8, WW> : ccd_warp_kernel<T, false, false, 8, WW>;
+    if (W == 1) { TPF_WARP_KERN(1) }
+    else if (W == 2) { TPF_WARP_KERN(2) }
+    else { TPF_WARP_KERN(4) }
+#undef TPF_WARP_KERN
   }
   TPF_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem));
-  kern<<<s.grid, warp ? 32 * s.TL : s.TL * p->P, s.smem, stream>>>(a);
+  kern<<<s.grid, warp ? 32 * W * s.TL : s.TL * p->P, s.smem, stream>>>(a);
   TPF_CUDA_TRY(cudaGetLastError());
   return TPF_OK;
 }
@@ -1947,9 +1987,10 @@ int tpf_ccd_plan_create(tpf_ccd_plan** out, int64_t n_pts, double h, int bc, int
   p->bc = bc;
   p->dtype = dtype;
   p->n_rows = (bc == TPF_BC_WALL) ? (int)(n_pts - 2) : (int)(n_pts - 1);
-  // chunk length = rows per lane of the warp-per-line kernel (8, 16, 32); longer
-  // lines use the shared-memory chunk kernel with C = ceil(n_rows / 32)
-  p->C = p->n_rows <= 256 ? 8 : (p->n_rows <= 512 ? 16 : (p->n_rows <= 1024 ? 32 : (p->n_rows + 31) / 32));
+  // chunk length = rows per lane of the warp kernel (8; 1, 2 or 4 warps per
+  // line up to 1024 rows); longer lines use the shared-memory chunk kernel
+  // with C = ceil(n_rows / 32)
+  p->C = p->n_rows <= 1024 ? 8 : (p->n_rows + 31) / 32;
   std::vector<double> tab;
   int st = build_tables(p, tab);
   if (st != TPF_OK) { delete p; return st; }

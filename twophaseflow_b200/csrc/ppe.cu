@@ -1199,6 +1199,24 @@ __global__ void __launch_bounds__(256) cgs_resid_kernel(Grid3 g, const double* s
 // INIT: u = M r, s = p = 0.  Else: s = w + beta s, p = M r + beta p,
 // x += alpha p, r -= alpha s, u = M r (new r).
 template <bool INIT>
+__device__ __forceinline__ void cgs_update_node(int idx, int pin, double ri, double di, double wi, double svi,
+                                                double pvi, double& xi, double alpha, double beta, double& rn,
+                                                double& si, double& pi, double& un) {
+  rn = ri;
+  si = 0.0;
+  pi = 0.0;
+  if (!INIT) {
+    si = wi + beta * svi;
+    pi = di * ri + beta * pvi;
+    xi += alpha * pi;
+    rn = ri - alpha * si;
+  }
+  un = (idx == pin) ? 0.0 : di * rn;   // r[pin] stays 0: u[pin] = 0 either way
+}
+
+// Two consecutive nodes per thread and trip (16-byte loads and stores; the
+// vectors come from cudaMalloc, so even node indices are 16-byte aligned).
+template <bool INIT>
 __global__ void __launch_bounds__(256) cgs_update_kernel(int ndof, int pin, const double* __restrict__ dinv,
                                                          const double* __restrict__ w, double* __restrict__ sv,
                                                          double* __restrict__ pv, double* __restrict__ x,
@@ -1212,21 +1230,50 @@ __global__ void __launch_bounds__(256) cgs_update_kernel(int ndof, int pin, cons
     beta = sc->beta;
   }
   double red[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += gridDim.x * blockDim.x) {
-    const double ri = r[idx];
-    const double di = dinv[idx];
-    double rn = ri, si = 0.0, pi = 0.0;
+  const int npair = ndof >> 1;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < npair; k += gridDim.x * blockDim.x) {
+    const int i0 = 2 * k;
+    const double2 r2 = reinterpret_cast<const double2*>(r)[k];
+    const double2 d2 = reinterpret_cast<const double2*>(dinv)[k];
+    double2 w2 = make_double2(0.0, 0.0), s2 = w2, p2 = w2, x2 = w2;
     if (!INIT) {
-      si = w[idx] + beta * sv[idx];
-      pi = di * ri + beta * pv[idx];
-      x[idx] += alpha * pi;
-      rn = ri - alpha * si;
-      r[idx] = rn;
+      w2 = reinterpret_cast<const double2*>(w)[k];
+      s2 = reinterpret_cast<const double2*>(sv)[k];
+      p2 = reinterpret_cast<const double2*>(pv)[k];
+      x2 = reinterpret_cast<const double2*>(x)[k];
     }
-    sv[idx] = si;
-    pv[idx] = pi;
-    const double un = (idx == pin) ? 0.0 : di * rn;   // r[pin] stays 0: u[pin] = 0 either way
-    u[idx] = un;
+    double rn0, si0, pi0, un0, rn1, si1, pi1, un1;
+    cgs_update_node<INIT>(i0, pin, r2.x, d2.x, w2.x, s2.x, p2.x, x2.x, alpha, beta, rn0, si0, pi0, un0);
+    cgs_update_node<INIT>(i0 + 1, pin, r2.y, d2.y, w2.y, s2.y, p2.y, x2.y, alpha, beta, rn1, si1, pi1, un1);
+    if (!INIT) {
+      reinterpret_cast<double2*>(x)[k] = x2;
+      reinterpret_cast<double2*>(r)[k] = make_double2(rn0, rn1);
+    }
+    reinterpret_cast<double2*>(sv)[k] = make_double2(si0, si1);
+    reinterpret_cast<double2*>(pv)[k] = make_double2(pi0, pi1);
+    reinterpret_cast<double2*>(u)[k] = make_double2(un0, un1);
+    red[0] += rn0 * un0;
+    red[1] += un0 * si0;
+    red[2] += pi0 * si0;
+    red[3] += rn0 * rn0;
+    red[0] += rn1 * un1;
+    red[1] += un1 * si1;
+    red[2] += pi1 * si1;
+    red[3] += rn1 * rn1;
+  }
+  if ((ndof & 1) && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {   // odd node count: the last node
+    const int i = ndof - 1;
+    double xi = INIT ? 0.0 : x[i];
+    double rn, si, pi, un;
+    cgs_update_node<INIT>(i, pin, r[i], dinv[i], INIT ? 0.0 : w[i], INIT ? 0.0 : sv[i], INIT ? 0.0 : pv[i], xi,
+                          alpha, beta, rn, si, pi, un);
+    if (!INIT) {
+      x[i] = xi;
+      r[i] = rn;
+    }
+    sv[i] = si;
+    pv[i] = pi;
+    u[i] = un;
     red[0] += rn * un;
     red[1] += un * si;
     red[2] += pi * si;
@@ -1273,6 +1320,7 @@ __global__ void __launch_bounds__(256) cgs_stencil_kernel(Grid3 g, int chunk, co
     double um = (c0 > 0) ? u[idx - nplane] : 0.0;
     double s0m = (c0 > 0) ? s0[idx - nplane] : 0.0;
     double uc = u[idx];
+#pragma unroll 4
     for (int i0 = c0; i0 < c1; ++i0, idx += nplane) {
       const double up = (i0 < g.N0) ? u[idx + nplane] : 0.0;
       const double s0p = s0[idx];   // zero on the last plane
@@ -1331,6 +1379,27 @@ __global__ void __launch_bounds__(256) cgs_stencil_kernel(Grid3 g, int chunk, co
   }
 }
 
+__global__ void cgs_init_kernel(CgScal* sc, double tol, long long maxiter, int x_nonzero) {
+  CgScal z{};
+  z.tol = tol;
+  z.maxiter = maxiter;
+  z.x_nonzero = x_nonzero;
+  *sc = z;
+}
+
+// body of the captured while node: run again while the solve is not done
+__global__ void cgs_cond_kernel(const CgScal* sc, cudaGraphConditionalHandle handle) {
+  cudaGraphSetConditional(handle, sc->done ? 0u : 1u);
+}
+
+// p = x with p[pin] = 0 (x = 0 when the right-hand side is zero)
+__global__ void cgs_finish_kernel(int ndof, int pin, const CgScal* sc, const double* __restrict__ x,
+                                  double* __restrict__ p) {
+  const bool zero = sc->bb == 0.0;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += gridDim.x * blockDim.x)
+    p[idx] = (zero || idx == pin) ? 0.0 : x[idx];
+}
+
 }  // namespace
 
 // ---- handle -------------------------------------------------------------------------
@@ -1374,6 +1443,7 @@ struct tpf_ppe {
   cudaGraphExec_t cg_exec = nullptr;   // a chunk of streaming-PCG iterations, captured
   long long cg_key[6] = {};
   void* cgs = nullptr;                 // streaming-PCG device scalars (CgScal)
+  int pending = 0;                     // captured CG solve: 1 status in st, 2 in cgs
   cudaStream_t cap = nullptr;          // stream the cycle is captured on (never the caller's)
   long long gm_key[6] = {};
   double* band_pub = nullptr;     // halo rows of the band-resident PCG
@@ -1532,6 +1602,11 @@ int solve_gmres(tpf_ppe* h, const double* rhs, double* p, const double* p_init, 
   const Grid3& g = h->g;
   const int n = g.ndof;
   int st;
+  cudaStreamCaptureStatus cap_state = cudaStreamCaptureStatusNone;
+  TPF_CUDA_TRY(cudaStreamIsCapturing(s, &cap_state));
+  TPF_CHECK_ARG(cap_state == cudaStreamCaptureStatusNone,
+                "the GMRES route reads its residual on the host between restart cycles and cannot be captured "
+                "into a CUDA graph (the CG route can)");
   if ((st = ensure_gmres(h))) return st;
   GmresWork W;
   W.n = n;
@@ -1674,13 +1749,12 @@ int solve_cg_stream(tpf_ppe* h, const double* rhs, double* p, const double* p_in
     h->cgs = c;
   }
   CgScal* sc = static_cast<CgScal*>(h->cgs);
+  cudaStreamCaptureStatus cap_state = cudaStreamCaptureStatusNone;
+  TPF_CUDA_TRY(cudaStreamIsCapturing(s, &cap_state));
+  const bool capturing = cap_state == cudaStreamCaptureStatusActive;
   const Geo geo{{h->dv[0], h->dv[1], h->dv[2]}, {h->dface[0], h->dface[1], h->dface[2]}};
   cg_rhs_kernel<<<ew_grid(h), 256, 0, s>>>(g, geo, rhs, h->b, p_init, h->x);
-  CgScal init{};
-  init.tol = h->o.tol;
-  init.maxiter = h->o.maxiter;
-  init.x_nonzero = p_init ? 1 : 0;
-  TPF_CUDA_TRY(cudaMemcpyAsync(sc, &init, sizeof(CgScal), cudaMemcpyHostToDevice, s));
+  cgs_init_kernel<<<1, 1, 0, s>>>(sc, h->o.tol, h->o.maxiter, p_init ? 1 : 0);
   const bool none = (h->o.precond == TPF_PRECOND_NONE);
   const double* dinv = none ? h->ones64 : h->dinvS;
   double* r = h->c64[0];
@@ -1706,6 +1780,52 @@ int solve_cg_stream(tpf_ppe* h, const double* rhs, double* p, const double* p_in
   cgs_update_kernel<true><<<nb, 256, 0, s>>>(n, g.pin, dinv, w, sv, pv, h->x, r, u, h->part, sc);
   cgs_stencil_kernel<true><<<sgrid, 256, 0, s>>>(g, chunk, h->s[0], h->s[1], s2, u, pv, w, h->part, sc);
   TPF_CUDA_TRY(cudaGetLastError());
+  if (capturing) {
+    // inside the caller's stream capture: the iterations become a conditional
+    // WHILE node of the captured graph whose body runs kCgsChunk iterations
+    // and then sets the condition from the device-side state; the result is
+    // read after a replay with tpf_ppe_read_result
+    cudaStreamCaptureStatus cs2 = cudaStreamCaptureStatusNone;
+    unsigned long long cid = 0;
+    cudaGraph_t cgraph = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    TPF_CUDA_TRY(cudaStreamGetCaptureInfo(s, &cs2, &cid, &cgraph, &deps, &ndeps));
+    cudaGraphConditionalHandle handle;
+    TPF_CUDA_TRY(cudaGraphConditionalHandleCreate(&handle, cgraph, 1u, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = handle;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    TPF_CUDA_TRY(cudaGraphAddNode(&wnode, cgraph, deps, ndeps, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    TPF_CUDA_TRY(cudaStreamBeginCaptureToGraph(h->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    for (int k = 0; k < kCgsChunk; ++k) {
+      cgs_update_kernel<false><<<nb, 256, 0, h->cap>>>(n, g.pin, dinv, w, sv, pv, h->x, r, u, h->part, sc);
+      cgs_stencil_kernel<false><<<sgrid, 256, 0, h->cap>>>(g, chunk, h->s[0], h->s[1], s2, u, pv, w, h->part, sc);
+    }
+    cgs_cond_kernel<<<1, 1, 0, h->cap>>>(sc, handle);
+    cudaGraph_t body_out = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(h->cap, &body_out);
+    if (ce != cudaSuccess) {
+      cudaGetLastError();
+      tpf::set_error("capturing the PCG loop body failed: %s", cudaGetErrorString(ce));
+      return TPF_ECUDA;
+    }
+    TPF_CUDA_TRY(cudaStreamUpdateCaptureDependencies(s, &wnode, 1, cudaStreamSetCaptureDependencies));
+    cgs_finish_kernel<<<ew_grid(h), 256, 0, s>>>(n, g.pin, sc, h->x, p);
+    TPF_CUDA_TRY(cudaGetLastError());
+    h->pending = 2;
+    res->iterations = -1;
+    res->applies = -1;
+    res->refinements = 0;
+    res->rel_residual = -1.0;
+    res->info = 0;
+    return TPF_OK;
+  }
+  h->pending = 0;
   const long long key[6] = {(long long)nb * 4096 + chunk, (long long)(intptr_t)dinv, (long long)(intptr_t)h->x,
                             (long long)(intptr_t)r, (long long)n, (long long)(intptr_t)sc};
   if (!h->cg_exec || std::memcmp(h->cg_key, key, sizeof(key)) != 0) {
@@ -1747,8 +1867,7 @@ int solve_cg_stream(tpf_ppe* h, const double* rhs, double* p, const double* p_in
     TPF_CUDA_TRY(cudaMemcpyAsync(&hs, sc, sizeof(CgScal), cudaMemcpyDeviceToHost, s));
     TPF_CUDA_TRY(cudaStreamSynchronize(s));
   }
-  if (hs.bb == 0.0) TPF_CUDA_TRY(cudaMemsetAsync(h->x, 0, sizeof(double) * n, s));
-  copy_pin0_kernel<<<ew_grid(h), 256, 0, s>>>(n, g.pin, h->x, p);
+  cgs_finish_kernel<<<ew_grid(h), 256, 0, s>>>(n, g.pin, sc, h->x, p);
   TPF_CUDA_TRY(cudaGetLastError());
   TPF_CUDA_TRY(cudaStreamSynchronize(s));
   res->iterations = hs.it;
@@ -1796,12 +1915,13 @@ int solve_cg(tpf_ppe* h, const double* rhs, double* p, const double* p_init, cud
   a.err = h->err;
   a.st = h->st;
   const bool mixed = (h->o.precision == TPF_PREC_MIXED);
-  if (!mixed && (h->cg_kernel == 3 || (h->cg_kernel == 0 && g.N2 > 0)))
+  BandPlan bp;
+  const bool band = !mixed && band_plan(h, bp);
+  if (!mixed && (h->cg_kernel == 3 || (h->cg_kernel == 0 && !band)))
     return solve_cg_stream(h, rhs, p, p_init, s, res);
   a.maxiter = h->o.maxiter;
   a.replace_drop = h->o.inner_tol > 0.0 ? h->o.inner_tol : 1e-3;
-  BandPlan bp;
-  if (!mixed && band_plan(h, bp)) {
+  if (band) {
     int st = launch_band(h, bp, a, s);
     if (st) return st;
   } else {
@@ -1814,6 +1934,20 @@ int solve_cg(tpf_ppe* h, const double* rhs, double* p, const double* p_init, cud
     TPF_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(h->coop_blocks), dim3(kThreads), args, 0, s));
   }
   copy_pin0_kernel<<<ew_grid(h), 256, 0, s>>>(n, g.pin, h->x, p);
+  cudaStreamCaptureStatus cap_state = cudaStreamCaptureStatusNone;
+  TPF_CUDA_TRY(cudaStreamIsCapturing(s, &cap_state));
+  if (cap_state == cudaStreamCaptureStatusActive) {
+    // captured into the caller's graph: the status is read after a replay
+    TPF_CUDA_TRY(cudaGetLastError());
+    h->pending = 1;
+    res->iterations = -1;
+    res->applies = -1;
+    res->refinements = 0;
+    res->rel_residual = -1.0;
+    res->info = 0;
+    return TPF_OK;
+  }
+  h->pending = 0;
   SolveStatus hs{};
   int herr = 0;
   TPF_CUDA_TRY(cudaMemcpyAsync(&hs, h->st, sizeof(SolveStatus), cudaMemcpyDeviceToHost, s));
@@ -1957,6 +2091,19 @@ int tpf_ppe_create(tpf_ppe** out, int ndim, const int64_t* N, const double* cons
   if ((st = dalloc(h, &h->err, 1))) return fail(st);
   if ((st = dalloc(h, &h->st, 1))) return fail(st);
   if ((st = dalloc(h, &h->gst, 1))) return fail(st);
+  {
+    // the streaming-PCG scalars and the private capture stream exist before
+    // any solve, so a first solve inside a stream capture allocates nothing
+    CgScal* c = nullptr;
+    if ((st = dalloc(h, &c, 1))) return fail(st);
+    h->cgs = c;
+    if (cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      h->cap = nullptr;
+      tpf::set_error("cudaStreamCreate failed");
+      return fail(TPF_ECUDA);
+    }
+  }
   *out = h;
   return TPF_OK;
 }
@@ -2065,6 +2212,45 @@ int tpf_ppe_solve(tpf_ppe* h, const double* rhs, const double* rho, double* p, c
   *res = tpf_ppe_result{};
   if (h->o.method == TPF_PPE_CG) return solve_cg(h, rhs, p, p_init, s, res);
   return solve_gmres(h, rhs, p, p_init, s, res);
+}
+
+int tpf_ppe_read_result(tpf_ppe* h, void* stream, tpf_ppe_result* result) {
+  TPF_CHECK_ARG(h && result, "NULL argument");
+  TPF_CHECK_ARG(h->pending == 1 || h->pending == 2, "no captured CG solve on this handle");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  *result = tpf_ppe_result{};
+  bool conv = false;
+  if (h->pending == 1) {
+    SolveStatus hs{};
+    int herr = 0;
+    TPF_CUDA_TRY(cudaMemcpyAsync(&hs, h->st, sizeof(SolveStatus), cudaMemcpyDeviceToHost, s));
+    TPF_CUDA_TRY(cudaMemcpyAsync(&herr, h->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    TPF_CUDA_TRY(cudaStreamSynchronize(s));
+    if (herr) {
+      tpf::set_error("PCG grid barrier timed out; the solve was aborted");
+      return TPF_EABORT;
+    }
+    result->iterations = hs.iters;
+    result->applies = hs.applies;
+    result->refinements = hs.refinements;
+    result->rel_residual = hs.bb > 0.0 ? std::sqrt(hs.rr / hs.bb) : 0.0;
+    conv = hs.converged != 0;
+  } else {
+    CgScal hs{};
+    TPF_CUDA_TRY(cudaMemcpyAsync(&hs, h->cgs, sizeof(CgScal), cudaMemcpyDeviceToHost, s));
+    TPF_CUDA_TRY(cudaStreamSynchronize(s));
+    result->iterations = hs.it;
+    result->applies = hs.applies;
+    result->rel_residual = hs.bb > 0.0 ? std::sqrt(hs.rr / hs.bb) : 0.0;
+    conv = hs.conv != 0;
+  }
+  result->info = conv ? 0 : (int)std::min<long long>(h->o.maxiter, 0x7fffffff);
+  if (!conv) {
+    tpf::set_error("PPESolverFVMMatrixFree did not converge cleanly (info=%d); no alternate PPE solver was applied.",
+                   result->info);
+    return TPF_ENOCONV;
+  }
+  return TPF_OK;
 }
 
 int tpf_ppe_solve_batched(tpf_ppe* const* hs, int n, const double* const* rhs, const double* const* rho,

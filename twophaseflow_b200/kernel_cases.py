@@ -331,9 +331,12 @@ def viscous_case(N, dtype, reps):
 def step_case(N, reps, use_graphs=True):
     """Whole two-phase time steps (TwoPhaseStep): a gas bubble of radius 0.2 at
     (0.5, 0.5, 0.3) in liquid ((0.5, 0.3) in 2-D), density ratio 1000,
-    viscosity ratio 100, Re 100, We 10, Fr 1, dt = 0.25 h.  Two warm-up steps
-    (eager + capture, then one replay), then ``reps`` timed steps split into
-    the pre-PPE graph, the PPE solve and the post-PPE graph (CUDA events)."""
+    viscosity ratio 100, Re 100, We 10, Fr 1, each step at the CFL time step
+    with the capillary bound (time_integration/cfl.py:85-137).  The CG
+    pressure solve is recorded in the same CUDA graph as the rest of the step,
+    so a replayed step is one graph launch plus the read-back of the solve's
+    status.  Two warm-up steps (eager + capture), then ``reps`` timed steps
+    (CUDA events around each step)."""
     import torch
     from . import TwoPhaseStep, UniformGrid
     nd = len(N)
@@ -346,33 +349,23 @@ def step_case(N, reps, use_graphs=True):
     del X, r
     stp = TwoPhaseStep(UniformGrid(N), psi, Re=100.0, Fr=1.0, We=10.0, rho_ratio=1e-3, mu_ratio=1e-2,
                        use_graphs=use_graphs)
-    dt = 0.25 * h
     for _ in range(2):
-        stp.step(dt)
+        stp.step(stp.cfl_dt())
     torch.cuda.synchronize()
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(reps)]
-    its = []
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(reps)]
+    its, dts = [], []
     for k in range(reps):
-        e = ev[k]
-        e[0].record()
-        if use_graphs:
-            stp._g1.replay()
-        else:
-            stp._phase1(dt)
-        e[1].record()
-        stp._solve()
-        e[2].record()
-        if use_graphs:
-            stp._g2.replay()
-        else:
-            stp._phase2(dt)
-        e[3].record()
+        dt = stp.cfl_dt()
+        dts.append(dt)
+        ev[k][0].record()
+        stp.step(dt)
+        ev[k][1].record()
         its.append(stp.last_ppe_iterations)
     torch.cuda.synchronize()
-    t = [[e[i].elapsed_time(e[i + 1]) for i in range(3)] for e in ev]
-    return {"case": "step", "N": list(N), "graphs": use_graphs, "ms_per_step": round(sum(sum(x) for x in t) / reps, 2),
-            "pre_ppe_ms": round(sum(x[0] for x in t) / reps, 2), "ppe_ms": round(sum(x[1] for x in t) / reps, 2),
-            "post_ppe_ms": round(sum(x[2] for x in t) / reps, 2), "ppe_iterations": its,
+    t = [e[0].elapsed_time(e[1]) for e in ev]
+    return {"case": "step", "N": list(N), "graphs": use_graphs, "one_graph_per_step": stp._g2 is None,
+            "ms_per_step": round(sum(t) / reps, 2), "ppe_iterations": its, "dt": dts[-1],
+            "steps_total": reps + 2,
             "psi_range": [round(float(stp.psi.min()), 6), round(float(stp.psi.max()), 6)],
             "u_max": round(float(max(v.abs().max() for v in stp.vel)), 6)}
 

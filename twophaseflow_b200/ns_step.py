@@ -50,7 +50,7 @@ class TwoPhaseStep:
     def __init__(self, grid, psi, Re=100.0, Fr=1.0, We=10.0, rho_ratio=1e-3, mu_ratio=1e-2, cfl=0.3,
                  eps=None, reinit_steps=4, ppe_tol=1e-8, ppe_maxiter=20000, use_graphs=True,
                  convection="ccd", transport_mass_correction=False, reinit_bc="zero", ppe_method="cg",
-                 no_slip=False, zero_velocity_shortcut=False):
+                 no_slip=False, zero_velocity_shortcut=False, ppe_in_graph=None):
         """The keyword options after ``use_graphs`` select the reference
         quick-start pipeline's components (simulation/_core.py:126-172):
         ``convection="uccd6"``, ``transport_mass_correction=True``,
@@ -62,6 +62,12 @@ class TwoPhaseStep:
         the first step), as the reference's CPU backend does
         (levelset/fccd_advection.py:99-110).  The defaults keep the CCD
         convection, Jacobi-PCG composition.
+
+        ``ppe_in_graph`` (default: True for the CG route) records the pressure
+        solve inside the same CUDA graph as the rest of the step, so a step is
+        ONE graph replay; the solve's iteration count and convergence are read
+        back after the replay.  The GMRES route is host-driven and stays
+        between two graphs.
 
         ``cfl_dt`` is the reference's CFLCalculator (time_integration/cfl.py:
         58-137) with Crank-Nicolson viscosity: the convective bound and the
@@ -107,6 +113,9 @@ class TwoPhaseStep:
         self.dp = torch.zeros_like(self.psi)
         self.maxima = torch.zeros(4, dtype=torch.float64, device=dev)
         self.use_graphs = use_graphs
+        self.ppe_in_graph = (ppe_method == "cg") if ppe_in_graph is None else bool(ppe_in_graph)
+        if self.ppe_in_graph and ppe_method != "cg":
+            raise ValueError("ppe_in_graph needs the CG route (the GMRES route reads its residual on the host)")
         self._g1 = self._g2 = None
         self._dt_graph = None
         self._vel_star = None
@@ -163,12 +172,21 @@ class TwoPhaseStep:
         s = torch.cuda.Stream()
         s.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(s):
-            g1 = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(g1, stream=s):
-                self._phase1(dt)
-            g2 = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(g2, stream=s):
-                self._phase2(dt)
+            if self.ppe_in_graph:
+                g1 = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g1, stream=s):
+                    self._phase1(dt)
+                    dp = self.ppe.solve(self.rhs, self.rho)
+                    self.dp.copy_(dp)
+                    self._phase2(dt)
+                g2 = None
+            else:
+                g1 = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g1, stream=s):
+                    self._phase1(dt)
+                g2 = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g2, stream=s):
+                    self._phase2(dt)
         torch.cuda.current_stream().wait_stream(s)
         torch.cuda.synchronize()
         self._g1, self._g2, self._dt_graph = g1, g2, dt
@@ -190,6 +208,12 @@ class TwoPhaseStep:
             self._solve()
             self._phase2(dt)
             self._capture(dt)   # records only: the state has advanced by the eager step
+            return
+        if self._g2 is None:
+            # the whole step, pressure solve included, as one graph
+            self._g1.replay()
+            d = self.ppe.read_result()
+            self.last_ppe_iterations = int(d.get(f"ppe_low_order_{self.ppe.iteration_method}_iterations", 0))
             return
         self._g1.replay()
         self._solve()

@@ -219,6 +219,36 @@ class PPESolverFVMMatrixFree:
                                     _lib.current_stream_handle(), C.byref(res))
         self._prepared = True
         self._rho_keep = vrho.tensor
+        self._fill_diagnostics(res)
+        if st == _lib.TPF_ENOCONV:
+            raise RuntimeError(
+                f"{type(self).__name__} did not converge cleanly (info={res.info}); "
+                "no alternate PPE solver was applied. Increase the matrix-free "
+                "iteration budget/tolerance or select ppe_solver_type='fvm_direct' "
+                "explicitly if sparse FVM is intended.")
+        _lib.check(st)
+        return vr.out(p)
+
+    def read_result(self):
+        """Result of the last replay of a solve captured into a CUDA graph
+        (the CG route records its whole solve when called under stream
+        capture; nothing is read back then).  Synchronizes the current stream,
+        fills ``last_diagnostics`` and raises RuntimeError like ``solve`` when
+        that replay did not converge."""
+        res = _lib.tpf_ppe_result()
+        st = self.lib.tpf_ppe_read_result(self._handle, _lib.current_stream_handle(), C.byref(res))
+        if st not in (_lib.TPF_OK, _lib.TPF_ENOCONV):
+            _lib.check(st)
+        self._fill_diagnostics(res)
+        if st == _lib.TPF_ENOCONV:
+            raise RuntimeError(
+                f"{type(self).__name__} did not converge cleanly (info={res.info}); "
+                "no alternate PPE solver was applied. Increase the matrix-free "
+                "iteration budget/tolerance or select ppe_solver_type='fvm_direct' "
+                "explicitly if sparse FVM is intended.")
+        return dict(self.last_diagnostics)
+
+    def _fill_diagnostics(self, res):
         key = f"ppe_low_order_{self.iteration_method}"
         self.last_diagnostics = {
             f"{key}_info": int(res.info),
@@ -229,14 +259,6 @@ class PPESolverFVMMatrixFree:
             f"{key}_refinements": int(res.refinements),
             f"{key}_relative_residual": float(res.rel_residual),
         }
-        if st == _lib.TPF_ENOCONV:
-            raise RuntimeError(
-                f"{type(self).__name__} did not converge cleanly (info={res.info}); "
-                "no alternate PPE solver was applied. Increase the matrix-free "
-                "iteration budget/tolerance or select ppe_solver_type='fvm_direct' "
-                "explicitly if sparse FVM is intended.")
-        _lib.check(st)
-        return vr.out(p)
 
     def _check_shape(self, t):
         if tuple(t.shape) != tuple(self.grid.shape):
