@@ -4,9 +4,14 @@
 // rotations and the residual vector live on the device; the host reads one
 // small state block per restart cycle.  Classical Gram-Schmidt with a
 // conditional re-orthogonalization pass stands in for SciPy's modified
-// Gram-Schmidt (the same basis up to rounding).  Every kernel of an Arnoldi
-// column skips its work once the device-side state marks the cycle done, so
-// a whole cycle (m columns) is captured once as a CUDA graph and replayed.
+// Gram-Schmidt (the same basis up to rounding).  An Arnoldi column is the
+// caller's operator and preconditioner plus four kernels (gs1: first-pass
+// inner products; gs2: the update and, without re-orthogonalization, the
+// norm and the Givens step; gs3: the second pass when needed; the scaling of
+// the new basis vector), each finishing its reductions in its last block.
+// Every kernel of a column skips its work once the device-side state marks
+// the cycle done, so a whole cycle (m columns) is captured once as a CUDA
+// graph and replayed.
 //
 // The operator, the residual and the preconditioner are the caller's
 // (functors enqueueing kernels on a stream): the FVM PPE (ppe.cu) and the
@@ -21,6 +26,10 @@
 
 namespace {
 
+// restart length limit of the fused kernels' shared staging (columns; the
+// options accept restarts up to 1024)
+constexpr int kGmMaxCols = 1024;
+
 // ---- GMRES building blocks ---------------------------------------------------------
 
 struct GmState {
@@ -34,6 +43,8 @@ struct GmState {
   double wn2;        // ||w||^2 scratch
   double rnorm;      // true residual norm (end of cycle)
   double scal;       // scale factor for the new basis vector
+  unsigned int arrive;   // blocks finished in the current fused kernel (last-block reductions)
+  int pad;
 };
 
 // partial dots: part[k*nb + block] = <V_k, w> for k < ncols, part[ncols*nb+block] = <w,w>
@@ -133,19 +144,6 @@ __global__ void mdot_finalize_kernel(const double* part, int nb, int ncols, doub
   }
 }
 
-// w -= sum_k c_k V_k  (c = hcol, or the second-pass dots in part-summed form)
-__global__ void maxpy_kernel(int ndof, const double* __restrict__ V, int ncols, const double* coef, double* w,
-                             const GmState* st, int pass) {
-  if (st->done) return;
-  if (pass == 1 && !st->reorth) return;
-  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += gridDim.x * blockDim.x) {
-    double acc = w[idx];
-#pragma unroll 8
-    for (int k = 0; k < ncols; ++k) acc -= coef[k] * V[(size_t)k * ndof + idx];
-    w[idx] = acc;
-  }
-}
-
 // Givens rotation generator for real (f, g): c f + s g = r, -s f + c g = 0,
 // r carries the sign of f (the convention of LAPACK's lartg).
 __device__ void givens_rot(double f, double g, double& c, double& s, double& r) {
@@ -155,63 +153,6 @@ __device__ void givens_rot(double f, double g, double& c, double& s, double& r) 
   c = fabs(f) / d;
   r = copysign(d, f);
   s = g / r;
-}
-
-// Finish Arnoldi column `col`: h1, breakdown, rotations, S, presid, done flag.
-// H is stored like SciPy's h[col, k] (row col = column of the Hessenberg matrix).
-// New Hessenberg column: fold in the second-pass coefficients, apply the
-// previous Givens rotations, generate this column's rotation and update the
-// residual vector S.  The block stages the column and the rotations in
-// shared memory; thread 0 applies them in order (the same arithmetic as a
-// serial pass over global memory, without its dependent round trips).
-__global__ void gm_column_kernel(double* H, int ldh, double* givens, double* S, GmState* st, int col,
-                                 const double* w_norm, const double* hcol2) {
-  if (st->done) return;
-  extern __shared__ double shc[];       // [col + 2] column, then [2 col] rotations
-  double* sg = shc + col + 2;
-  double* hc = H + (size_t)col * ldh;
-  const bool reorth = st->reorth != 0;
-  for (int k = threadIdx.x; k <= col; k += blockDim.x) {
-    double v = hc[k];
-    if (reorth) v += hcol2[k];   // second-pass coefficients
-    shc[k] = v;
-  }
-  for (int k = threadIdx.x; k < 2 * col; k += blockDim.x) sg[k] = givens[k];
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const double eps = 2.220446049250313e-16;
-    double h1 = *w_norm;
-    shc[col + 1] = h1;
-    int breakdown = 0;
-    if (h1 <= eps * st->h0) {
-      shc[col + 1] = 0.0;
-      breakdown = 1;
-      st->scal = 1.0;
-    } else {
-      st->scal = 1.0 / h1;
-    }
-    for (int k = 0; k < col; ++k) {
-      const double c = sg[2 * k], s = sg[2 * k + 1];
-      const double n0 = shc[k], n1 = shc[k + 1];
-      shc[k] = c * n0 + s * n1;
-      shc[k + 1] = -s * n0 + c * n1;
-    }
-    double c, s, mag;
-    givens_rot(shc[col], shc[col + 1], c, s, mag);
-    givens[2 * col] = c;
-    givens[2 * col + 1] = s;
-    shc[col] = mag;
-    shc[col + 1] = 0.0;
-    const double t = -s * S[col];
-    S[col] = c * S[col];
-    S[col + 1] = t;
-    st->presid = fabs(t);
-    st->ncols = col + 1;
-    st->breakdown = breakdown;
-    if (st->presid <= st->ptol || breakdown) st->done = 1;
-  }
-  __syncthreads();
-  for (int k = threadIdx.x; k <= col + 1; k += blockDim.x) hc[k] = shc[k];
 }
 
 __global__ void gm_scale_kernel(int ndof, const double* w, double* vout, const GmState* st) {
@@ -265,6 +206,194 @@ __global__ void gm_start_kernel(int ndof, const double* w, double* v0, double* S
   }
 }
 
+
+// ---- fused Gram-Schmidt kernels (one column = operator, preconditioner, gs1,
+// gs2, gs3, scale) ------------------------------------------------------------------
+//
+// Block partials of <V_k, w> (k < nv, slot nv - 1 may be <w, w>) accumulated
+// eight vectors per sweep as in mdot_kernel; the last block to finish sums
+// the partials in block order (fixed tree) and applies the column's scalar
+// logic, so no separate finalize launch is needed.
+
+__device__ __forceinline__ bool gm_last_block(GmState* st) {
+  __shared__ int s_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = (atomicAdd(&st->arrive, 1u) == gridDim.x - 1) ? 1 : 0;
+  __syncthreads();
+  if (s_last) __threadfence();
+  return s_last != 0;
+}
+
+// partials of <V_k, w> for k < nv; with_ww: slot nv is <w, w>
+__device__ __forceinline__ void gm_partials(int ndof, const double* __restrict__ V, int nv, bool with_ww,
+                                            const double* w, double* part, double* sh) {
+  constexpr int KC = 8;
+  const int nb = gridDim.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int ntot = nv + (with_ww ? 1 : 0);
+  for (int k0 = 0; k0 < ntot; k0 += KC) {
+    double acc[KC];
+#pragma unroll
+    for (int j = 0; j < KC; ++j) acc[j] = 0.0;
+    const int stride = gridDim.x * blockDim.x;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += stride) {
+      const double wi = w[idx];
+#pragma unroll
+      for (int j = 0; j < KC; ++j) {
+        const int k = k0 + j;
+        if (k < ntot) acc[j] += ((k < nv) ? V[(size_t)k * ndof + idx] : wi) * wi;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < KC; ++j) {
+      const double v = tpf::warp_sum(acc[j]);
+      if (lane == 0) sh[j * 32 + wid] = v;
+    }
+    __syncthreads();
+    if (wid < KC && k0 + wid < ntot) {
+      double t = (lane < nw) ? sh[wid * 32 + lane] : 0.0;
+      t = tpf::warp_sum(t);
+      if (lane == 0) part[(size_t)(k0 + wid) * nb + blockIdx.x] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// sums of partial slots [0, ntot) in block order into out[] (last block only)
+__device__ __forceinline__ void gm_sum_partials(const double* part, int nb, int ntot, double* out) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int k = wid; k < ntot; k += nw) {
+    double acc = 0.0;
+    for (int b = lane; b < nb; b += 32) acc += __ldcg(part + (size_t)k * nb + b);
+    acc = tpf::warp_sum(acc);
+    if (lane == 0) out[k] = acc;
+  }
+  __syncthreads();
+}
+
+// The column's scalar step (gm_column_kernel's arithmetic), run by the last
+// block of gs2 / gs3 with the column staged in shared memory.
+__device__ void gm_column_step(double* H, int ldh, double* givens, double* S, GmState* st, int col, double h1,
+                               const double* hcol2, double* shc) {
+  double* hc = H + (size_t)col * ldh;
+  double* sg = shc + col + 2;
+  const bool reorth = st->reorth != 0;
+  for (int k = threadIdx.x; k <= col; k += blockDim.x) {
+    double v = __ldcg(hc + k);
+    if (reorth) v += __ldcg(hcol2 + k);
+    shc[k] = v;
+  }
+  for (int k = threadIdx.x; k < 2 * col; k += blockDim.x) sg[k] = __ldcg(givens + k);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const double eps = 2.220446049250313e-16;
+    shc[col + 1] = h1;
+    int breakdown = 0;
+    if (h1 <= eps * st->h0) {
+      shc[col + 1] = 0.0;
+      breakdown = 1;
+      st->scal = 1.0;
+    } else {
+      st->scal = 1.0 / h1;
+    }
+    for (int k = 0; k < col; ++k) {
+      const double c = sg[2 * k], sn = sg[2 * k + 1];
+      const double n0 = shc[k], n1 = shc[k + 1];
+      shc[k] = c * n0 + sn * n1;
+      shc[k + 1] = -sn * n0 + c * n1;
+    }
+    double c, sn, mag;
+    givens_rot(shc[col], shc[col + 1], c, sn, mag);
+    givens[2 * col] = c;
+    givens[2 * col + 1] = sn;
+    shc[col] = mag;
+    shc[col + 1] = 0.0;
+    const double t = -sn * S[col];
+    S[col] = c * S[col];
+    S[col + 1] = t;
+    st->presid = fabs(t);
+    st->ncols = col + 1;
+    st->breakdown = breakdown;
+    if (st->presid <= st->ptol || breakdown) st->done = 1;
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k <= col + 1; k += blockDim.x) hc[k] = shc[k];
+}
+
+// gs1: <V_k, w> (k <= col) and <w, w>; last block: H column = the dots,
+// h0 = ||w||, the re-orthogonalization decision, hcol2 = 0
+__global__ void gs1_kernel(int ndof, const double* __restrict__ V, int col, const double* __restrict__ w,
+                           double* part, double* hcol, double* hcol2, GmState* st) {
+  if (st->done) return;
+  __shared__ double sh[8 * 32];
+  __shared__ double sums[kGmMaxCols + 2];
+  gm_partials(ndof, V, col + 1, true, w, part, sh);
+  if (!gm_last_block(st)) return;
+  gm_sum_partials(part, gridDim.x, col + 2, sums);
+  for (int k = threadIdx.x; k <= col; k += blockDim.x) {
+    hcol[k] = sums[k];
+    hcol2[k] = 0.0;
+  }
+  if (threadIdx.x == 0) {
+    const double sw = sums[col + 1];
+    st->h0 = sqrt(sw);
+    double proj = 0.0;
+    for (int q = 0; q <= col; ++q) proj += sums[q] * sums[q];
+    st->reorth = (sw - proj < 0.5 * sw) ? 1 : 0;
+    st->arrive = 0u;
+  }
+}
+
+// gs2: w -= sum_k hcol_k V_k; then either the second pass's dots
+// (re-orthogonalization: last block -> hcol2) or ||w|| and the column step
+__global__ void gs2_kernel(int ndof, const double* __restrict__ V, int col, double* w, const double* hcol,
+                           double* part, double* H, int ldh, double* givens, double* S, double* hcol2, GmState* st) {
+  if (st->done) return;
+  __shared__ double sh[8 * 32];
+  __shared__ double sums[3 * kGmMaxCols + 4];
+  const bool reorth = st->reorth != 0;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += gridDim.x * blockDim.x) {
+    double acc = w[idx];
+#pragma unroll 8
+    for (int k = 0; k <= col; ++k) acc -= hcol[k] * V[(size_t)k * ndof + idx];
+    w[idx] = acc;
+  }
+  if (reorth) gm_partials(ndof, V, col + 1, false, w, part, sh);
+  else gm_partials(ndof, V, 0, true, w, part, sh);
+  if (!gm_last_block(st)) return;
+  if (reorth) {
+    gm_sum_partials(part, gridDim.x, col + 1, sums);
+    for (int k = threadIdx.x; k <= col; k += blockDim.x) hcol2[k] = sums[k];
+    if (threadIdx.x == 0) st->arrive = 0u;
+    return;
+  }
+  gm_sum_partials(part, gridDim.x, 1, sums);
+  const double h1 = sqrt(sums[0]);
+  __syncthreads();
+  gm_column_step(H, ldh, givens, S, st, col, h1, hcol2, sums);
+  if (threadIdx.x == 0) st->arrive = 0u;
+}
+
+// gs3 (re-orthogonalization only): w -= sum_k hcol2_k V_k; ||w||; column step
+__global__ void gs3_kernel(int ndof, const double* __restrict__ V, int col, double* w, double* part, double* H,
+                           int ldh, double* givens, double* S, const double* hcol2, GmState* st) {
+  if (st->done || !st->reorth) return;
+  __shared__ double sh[8 * 32];
+  __shared__ double sums[3 * kGmMaxCols + 4];
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += gridDim.x * blockDim.x) {
+    double acc = w[idx];
+#pragma unroll 8
+    for (int k = 0; k <= col; ++k) acc -= hcol2[k] * V[(size_t)k * ndof + idx];
+    w[idx] = acc;
+  }
+  gm_partials(ndof, V, 0, true, w, part, sh);
+  if (!gm_last_block(st)) return;
+  gm_sum_partials(part, gridDim.x, 1, sums);
+  const double h1 = sqrt(sums[0]);
+  __syncthreads();
+  gm_column_step(H, ldh, givens, S, st, col, h1, hcol2, sums);
+  if (threadIdx.x == 0) st->arrive = 0u;
+}
 
 // Device GMRES workspace of one solver handle.  V holds restart_cap + 1
 // basis vectors; gm holds H (restart_cap x (restart_cap + 2)), the Givens
@@ -372,19 +501,9 @@ int gmres_solve(GmresWork& W, int restart, double tol, long long maxiter, bool x
       if ((est = apply(vc, W.t, cs, done))) return est;
       if ((est = precond(W.t, W.w, cs, done))) return est;
       double* hc = H + (size_t)col * ldh;
-      mdot_kernel<<<nb_dot, 256, 8 * 32 * sizeof(double), cs>>>(n, W.V, col + 1, W.w, W.part, done);
-      mdot_finalize_kernel<<<1, 1024, (col + 2) * sizeof(double), cs>>>(W.part, nb_dot, col + 1, hc, W.gst, 0,
-                                                                        nullptr);
-      maxpy_kernel<<<W.ew_blocks, 256, 0, cs>>>(n, W.V, col + 1, hc, W.w, W.gst, 0);
-      // conditional re-orthogonalization pass (hcol2 accumulates its coefficients)
-      TPF_CUDA_TRY(cudaMemsetAsync(hcol2, 0, sizeof(double) * (col + 1), cs));
-      mdot_kernel<<<nb_dot, 256, 8 * 32 * sizeof(double), cs>>>(n, W.V, col + 1, W.w, W.part, done);
-      mdot_finalize_kernel<<<1, 1024, (col + 2) * sizeof(double), cs>>>(W.part, nb_dot, col + 1, hcol2, W.gst,
-                                                                        1, nullptr);
-      maxpy_kernel<<<W.ew_blocks, 256, 0, cs>>>(n, W.V, col + 1, hcol2, W.w, W.gst, 1);
-      if ((est = gm_norm2(W, W.w, wnorm, cs))) return est;
-      gm_column_kernel<<<1, 128, (3 * col + 2) * sizeof(double), cs>>>(H, ldh, givens, S, W.gst, col, wnorm,
-                                                                      hcol2);
+      gs1_kernel<<<nb_dot, 256, 0, cs>>>(n, W.V, col, W.w, W.part, hc, hcol2, W.gst);
+      gs2_kernel<<<nb_dot, 256, 0, cs>>>(n, W.V, col, W.w, hc, W.part, H, ldh, givens, S, hcol2, W.gst);
+      gs3_kernel<<<nb_dot, 256, 0, cs>>>(n, W.V, col, W.w, W.part, H, ldh, givens, S, hcol2, W.gst);
       gm_scale_kernel<<<W.ew_blocks, 256, 0, cs>>>(n, W.w, W.V + (size_t)(col + 1) * n, W.gst);
       TPF_CUDA_TRY(cudaGetLastError());
     }
