@@ -460,6 +460,10 @@ def main(argv=None):
             for bc in ("wall", "periodic"):
                 for axis in range(len(N)):
                     ccd.append(time_ccd(N, bc, axis, dtype=dt))
+    # FP32 line solves under FP64 iterative refinement against the direct FP64
+    # solve (257^3 wall, strided and contiguous axis; error vs FP64 stated)
+    from twophaseflow_b200.kernel_cases import ccd_refined_case
+    ccd_ref = [ccd_refined_case((256, 256, 256), ax, 2, 3) for ax in (0, 2)]
     ccd3 = [c for c in ccd if len(c["N"]) == 3 and c["dtype"] == "f64"]
     ccd3_gbps = float(np.mean([c["GBps"] for c in ccd3]))
     ccd3_best = max(ccd3, key=lambda c: c["GBps"])
@@ -514,6 +518,7 @@ def main(argv=None):
             "learned_heldout": heldout,
             "batched_32_cases": bat,
             "ccd": ccd,
+            "ccd_fp32_refined_257cubed": ccd_ref,
             "corrector_257cubed_f64_wall": {"per_axis": corr, "peak": peak, "peak_kind": peak_kind,
                                             "frac_mean": round(float(np.mean([c["GBps"] for c in corr])) / peak, 3)},
             "curvature_257cubed_f64_wall": {k: v for k, v in curv.items() if k not in ("case", "N", "bc", "dtype")},

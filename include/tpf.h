@@ -96,6 +96,19 @@ int tpf_ccd_apply(const tpf_ccd_plan* plan, int64_t outer, int64_t inner,
                   const void* f, void* d1, void* d2, const double* bc_left,
                   const double* bc_right, int flags, void* stream);
 
+/* FP32 line solves under FP64 iterative refinement (no counterpart in the
+ * reference, whose CCD is FP64): d1, d2 (FP64) of the FP64 field f along the
+ * plans' axis, viewed as [outer, n_pts, inner].  The FP32 plan solves the
+ * FP32-rounded field; then `refinements` times (0..8) the residual of the
+ * full CCD system (interior Eq-I/Eq-II rows and the one-sided wall closures,
+ * ccd_solver.py:11-22,408-465) is formed in FP64 and an FP32 correction solve
+ * of the folded system is added in FP64.  Both plans: the same n_pts and h,
+ * TPF_BC_WALL, dtypes TPF_F64 and TPF_F32.  work: device scratch of
+ * 5 * outer * n_pts * inner floats.  The first call builds the plan's FP32
+ * per-row factors (a host factorization and one allocation). */
+int tpf_ccd_apply_refined(const tpf_ccd_plan* p64, const tpf_ccd_plan* p32, int64_t outer, int64_t inner,
+                          const double* f, double* d1, double* d2, int refinements, float* work, void* stream);
+
 /* Variable-density CCD term along the plan's axis, fused into the line
  * solve's output stage: out (+)= D2 f / rho - (drho / rho^2) D1 f, where drho
  * is d(rho)/dx along this axis (accumulate != 0 adds to out).  Summed over

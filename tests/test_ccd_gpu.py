@@ -352,3 +352,36 @@ def test_ccd_autotune_is_bitwise_neutral(cuda_device, bc):
     c1, c2 = plain.differentiate(f, 0)      # default shape
     assert torch.equal(a1, c1) and torch.equal(a2, c2)
     assert torch.equal(b1, c1) and torch.equal(b2, c2)
+
+
+@pytest.mark.parametrize("N,axis", [((128, 96), 0), ((128, 96), 1), ((40, 36, 48), 2), ((40, 36, 48), 0)])
+def test_ccd_refined_fp32_reaches_fp64(cuda_device, N, axis):
+    """FP32 line solves under FP64 iterative refinement: without refinement the
+    error is FP32-level; two refinements bring d1 and d2 to the FP64 solve
+    within 1e-12 of max|d| (and the FP64 oracle within the wall bar)."""
+    import torch
+    from oracle import ccd as occd
+    from twophaseflow_b200 import CCDSolver, UniformGrid
+    from twophaseflow_b200.workloads import fourier_field
+    f = fourier_field(N, n_modes=16, kmax=12, seed=3)
+    ft = torch.from_numpy(f).to(cuda_device)
+    ccd = CCDSolver(UniformGrid(N), None, bc_type="wall")
+    d1, d2 = ccd.differentiate(ft, axis)
+    errs = []
+    for r in (0, 1, 2):
+        a1, a2 = ccd.differentiate_refined(ft, axis, r)
+        errs.append((float((a1 - d1).abs().max() / d1.abs().max()), float((a2 - d2).abs().max() / d2.abs().max())))
+    assert max(errs[0]) > 1e-9          # FP32 alone
+    assert errs[1][0] < errs[0][0] and errs[1][1] < errs[0][1]
+    assert max(errs[2]) <= 1e-12, errs
+    o1, o2 = occd.differentiate(f, axis, 1.0 / N[axis])
+    a1, a2 = ccd.differentiate_refined(f, axis, 2)
+    assert np.abs(a1 - o1).max() <= 1e-11 * np.abs(o1).max()
+    assert np.abs(a2 - o2).max() <= 1e-11 * np.abs(o2).max()
+
+
+def test_ccd_refined_rejects_periodic(cuda_device):
+    from twophaseflow_b200 import CCDSolver, UniformGrid
+    ccd = CCDSolver(UniformGrid((32, 32)), None, bc_type="periodic")
+    with pytest.raises(NotImplementedError):
+        ccd.differentiate_refined(np.zeros((33, 33)), 0)

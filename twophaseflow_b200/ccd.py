@@ -121,6 +121,42 @@ class CCDSolver:
         v, _, d2 = self._run(data, axis, bc_left, bc_right, apply_metric, False, True)
         return v.out(d2)
 
+    def differentiate_refined(self, data, axis: int, refinements: int = 2):
+        """(d1, d2) of FP64 data from FP32 line solves under FP64 iterative
+        refinement (no counterpart in the reference, whose CCD is FP64): the
+        FP32 solve of the FP32-rounded field, then ``refinements`` times the
+        residual of the full CCD system (interior rows and the one-sided wall
+        closures) in FP64 and an FP32 correction solve added in FP64.  Wall
+        axes of a uniform grid; FP64 solver only."""
+        import torch
+        if self.dtype != torch.float64:
+            raise ValueError("differentiate_refined needs an FP64 CCDSolver")
+        if self._axis_periodic(axis):
+            raise NotImplementedError("iterative refinement of the CCD line solves covers wall axes")
+        if not getattr(self.grid, "uniform", True):
+            raise NotImplementedError("iterative refinement of the CCD line solves covers uniform grids")
+        v = to_device(data, dtype=torch.float64)
+        f = v.tensor
+        outer, n, inner = line_split(f.shape, axis)
+        if n != int(self.grid.N[axis]) + 1:
+            raise ValueError(f"data has {n} points along axis {axis}, grid has {int(self.grid.N[axis]) + 1}")
+        p64 = self._plan(axis, False)
+        key = (axis, "f32")
+        p32 = self._plans.get(key)
+        if p32 is None:
+            h = C.c_void_p()
+            _lib.check(self.lib.tpf_ccd_plan_create(C.byref(h), n, self._axis_solver_spacing(axis), _lib.TPF_BC_WALL,
+                                                    _lib.TPF_F32))
+            self._plans[key] = h
+            p32 = h
+        d1 = torch.empty_like(f)
+        d2 = torch.empty_like(f)
+        work = torch.empty(5 * f.numel(), dtype=torch.float32, device=f.device)
+        _lib.check(self.lib.tpf_ccd_apply_refined(p64, p32, outer, inner, _lib.dptr(f), _lib.dptr(d1), _lib.dptr(d2),
+                                                  int(refinements), _lib.dptr(work), _lib.current_stream_handle()))
+        self._work_keep = work
+        return v.out(d1), v.out(d2)
+
     def differentiate_raw(self, data, axis: int):
         """xi-space derivatives of a 1-D array of N[axis]+1 values (wall closure),
         ccd_solver.py:174-203."""

@@ -91,6 +91,9 @@ struct tpf_ccd_plan {
   // lane-kernel launch shapes picked by the autotuner, per call signature
   mutable std::map<uint64_t, LaneShape_> lane_tuned;
   bool autotune = true;
+  // FP32 per-row block-LU factors of the folded wall system (Lf, P, H per
+  // row) for the iterative-refinement correction solves, built on first use
+  mutable float* d_rfac = nullptr;
 };
 
 namespace {
@@ -1964,6 +1967,174 @@ int launch_ccd(const tpf_ccd_plan* p, int64_t outer, int64_t inner, const void* 
   return TPF_OK;
 }
 
+// ---- FP32 line solves under FP64 iterative refinement (wall axes) ----------------
+//
+// d = K32(f) in FP32, then per refinement the residual of the full
+// (N+1)-node CCD system, R = B f - A d, in FP64 (interior Eq-I / Eq-II rows,
+// the one-sided closure rows at both walls, ccd_solver.py:11-22,408-465),
+// and d += A^-1 R with the correction solved in FP32: the boundary rows are
+// folded into the first / last interior rows (delta_0 = M_l delta_1 + R_0,
+// ccd_solver_helpers.py:242-245), one thread runs the block-Thomas sweeps of
+// a line with per-row factors, and the boundary corrections are recovered.
+
+__device__ __forceinline__ float2 mv2f(const float* m, float a, float b) {
+  return make_float2(m[0] * a + m[1] * b, m[2] * a + m[3] * b);
+}
+
+__global__ void ccd_cast_kernel(int64_t n, const double* __restrict__ in, float* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (float)in[i];
+}
+
+__global__ void ccd_widen_kernel(int64_t n, const float* __restrict__ in, double* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (double)in[i];
+}
+
+// R = B f - A d at every node, FP64 arithmetic, FP32 storage
+__global__ void ccd_resid_kernel(int64_t total, int64_t inner, int n, double h, const double* __restrict__ f,
+                                 const double* __restrict__ d1, const double* __restrict__ d2,
+                                 float* __restrict__ R1, float* __restrict__ R2) {
+  const double a1h = kA1 / h, a2h2 = kA2 / (h * h), b1h = kB1 * h, b2h = kB2 / h;
+  const double inv12h2 = 1.0 / (12.0 * h * h);
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t ln = e / inner;
+    const int k = (int)(ln % n);
+    const int64_t s = inner;
+    double r1, r2;
+    if (k == 0) {
+      const double cI = (-23.0 / 6.0 * f[e] + 21.0 / 4.0 * f[e + s] - 1.5 * f[e + 2 * s] + 1.0 / 12.0 * f[e + 3 * s]) / h;
+      const double cII = (45.0 * f[e] - 154.0 * f[e + s] + 214.0 * f[e + 2 * s] - 156.0 * f[e + 3 * s] +
+                          61.0 * f[e + 4 * s] - 10.0 * f[e + 5 * s]) * inv12h2;
+      r1 = cI - (d1[e] - (-1.5 * d1[e + s] + 1.5 * h * d2[e + s]));
+      r2 = cII - d2[e];
+    } else if (k == n - 1) {
+      const double cI = (23.0 / 6.0 * f[e] - 21.0 / 4.0 * f[e - s] + 1.5 * f[e - 2 * s] - 1.0 / 12.0 * f[e - 3 * s]) / h;
+      const double cII = (45.0 * f[e] - 154.0 * f[e - s] + 214.0 * f[e - 2 * s] - 156.0 * f[e - 3 * s] +
+                          61.0 * f[e - 4 * s] - 10.0 * f[e - 5 * s]) * inv12h2;
+      r1 = cI - (d1[e] - (-1.5 * d1[e - s] - 1.5 * h * d2[e - s]));
+      r2 = cII - d2[e];
+    } else {
+      const double fm = f[e - s], f0 = f[e], fp = f[e + s];
+      const double pm = d1[e - s], p0 = d1[e], pp = d1[e + s];
+      const double qm = d2[e - s], q0 = d2[e], qp = d2[e + s];
+      r1 = a1h * (fp - fm) - (kAlpha1 * (pm + pp) + p0 - b1h * (qp - qm));
+      r2 = a2h2 * ((fm - 2.0 * f0) + fp) - (kBeta2 * (qm + qp) + q0 - b2h * (pp - pm));
+    }
+    R1[e] = (float)r1;
+    R2[e] = (float)r2;
+  }
+}
+
+// d += A^-1 R on every line (FP32 sweeps; R is overwritten by the forward sweep)
+__global__ void ccd_corr_kernel(int64_t n_lines, int64_t inner, int n, float h, const float* __restrict__ fac,
+                                float* R1, float* R2, double* d1, double* d2) {
+  const int64_t L = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (L >= n_lines) return;
+  const int64_t o = L / inner, i = L - o * inner;
+  const int64_t base = o * (int64_t)n * inner + i;
+  const int64_t s = inner;
+  const int nr = n - 2;
+  const float La[4] = {(float)kAlpha1, (float)kB1 * h, (float)kB2 / h, (float)kBeta2};
+  const float Ua[4] = {(float)kAlpha1, -(float)kB1 * h, -(float)kB2 / h, (float)kBeta2};
+  const float Ml[4] = {-1.5f, 1.5f * h, 0.0f, 0.0f};
+  const float Mr[4] = {-1.5f, -1.5f * h, 0.0f, 0.0f};
+  const float r0a = R1[base], r0b = R2[base];
+  const float rNa = R1[base + (int64_t)(n - 1) * s], rNb = R2[base + (int64_t)(n - 1) * s];
+  float ya = 0.0f, yb = 0.0f;
+  for (int j = 0; j < nr; ++j) {
+    const int64_t e = base + (int64_t)(j + 1) * s;
+    float ra = R1[e], rb = R2[e];
+    if (j == 0) {
+      const float2 q = mv2f(La, r0a, r0b);
+      ra -= q.x;
+      rb -= q.y;
+    }
+    if (j == nr - 1) {
+      const float2 q = mv2f(Ua, rNa, rNb);
+      ra -= q.x;
+      rb -= q.y;
+    }
+    const float* lf = fac + 12 * j;
+    const float2 q = mv2f(lf, ya, yb);
+    ya = ra - q.x;
+    yb = rb - q.y;
+    R1[e] = ya;
+    R2[e] = yb;
+  }
+  float xa = 0.0f, xb = 0.0f, x1a = 0.0f, x1b = 0.0f, xla = 0.0f, xlb = 0.0f;
+  for (int j = nr - 1; j >= 0; --j) {
+    const int64_t e = base + (int64_t)(j + 1) * s;
+    const float* pm = fac + 12 * j + 4;
+    const float* hm = pm + 4;
+    const float2 py = mv2f(pm, R1[e], R2[e]);
+    const float2 hx = mv2f(hm, xa, xb);
+    xa = py.x - hx.x;
+    xb = py.y - hx.y;
+    d1[e] += (double)xa;
+    d2[e] += (double)xb;
+    if (j == nr - 1) { xla = xa; xlb = xb; }
+    if (j == 0) { x1a = xa; x1b = xb; }
+  }
+  const float2 b0 = mv2f(Ml, x1a, x1b);
+  const float2 bN = mv2f(Mr, xla, xlb);
+  d1[base] += (double)(b0.x + r0a);
+  d2[base] += (double)(b0.y + r0b);
+  d1[base + (int64_t)(n - 1) * s] += (double)(bN.x + rNa);
+  d2[base + (int64_t)(n - 1) * s] += (double)(bN.y + rNb);
+}
+
+// per-row factors of the folded wall system (the recurrence of build_tables)
+int refine_factors(const tpf_ccd_plan* p) {
+  if (p->d_rfac) return TPF_OK;
+  const double h = p->h;
+  const int nr = p->n_rows;
+  const M2 L = {kAlpha1, kB1 * h, kB2 / h, kBeta2};
+  const M2 U = {kAlpha1, -kB1 * h, -kB2 / h, kBeta2};
+  const M2 Ml = {-1.5, 1.5 * h, 0.0, 0.0};
+  const M2 Mr = {-1.5, -1.5 * h, 0.0, 0.0};
+  std::vector<float> fac((size_t)12 * nr);
+  M2 LUp = eye();
+  for (int j = 0; j < nr; ++j) {
+    M2 D = eye();
+    if (j == 0) D = add(D, mul(L, Ml));
+    if (j == nr - 1) D = add(D, mul(U, Mr));
+    M2 Lf = {0, 0, 0, 0}, LU;
+    if (j == 0) LU = D;
+    else {
+      Lf = mul(L, inv(LUp));
+      LU = sub(D, mul(Lf, U));
+    }
+    const double dt = det(LU);
+    if (!std::isfinite(dt) || std::fabs(dt) < 1e-300) {
+      tpf::set_error("CCD block-tridiagonal factorization encountered a singular pivot at block %d", j);
+      return TPF_ESINGULAR;
+    }
+    const M2 Pm = inv(LU);
+    const M2 Hm = (j < nr - 1) ? mul(Pm, U) : M2{0, 0, 0, 0};
+    for (int q = 0; q < 4; ++q) {
+      fac[12 * j + q] = (float)Lf[q];
+      fac[12 * j + 4 + q] = (float)Pm[q];
+      fac[12 * j + 8 + q] = (float)Hm[q];
+    }
+    LUp = LU;
+  }
+  float* d = nullptr;
+  if (cudaMalloc(&d, fac.size() * sizeof(float)) != cudaSuccess) {
+    cudaGetLastError();
+    tpf::set_error("cudaMalloc of the refinement factors failed");
+    return TPF_ECUDA;
+  }
+  if (cudaMemcpy(d, fac.data(), fac.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(d);
+    tpf::set_error("cudaMemcpy of the refinement factors failed");
+    return TPF_ECUDA;
+  }
+  p->d_rfac = d;
+  return TPF_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -2045,6 +2216,7 @@ int tpf_ccd_plan_destroy(tpf_ccd_plan* p) {
   cudaFree(p->d_ltab);
   cudaFree(p->d_ltabf);
   cudaFree(p->d_J);
+  cudaFree(p->d_rfac);
   delete p;
   return TPF_OK;
 }
@@ -2069,6 +2241,43 @@ int tpf_ccd_apply(const tpf_ccd_plan* p, int64_t outer, int64_t inner, const voi
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (p->dtype == TPF_F64) return launch_ccd<double>(p, outer, inner, f, d1, d2, bc_left, bc_right, flags, s);
   return launch_ccd<float>(p, outer, inner, f, d1, d2, bc_left, bc_right, flags, s);
+}
+
+int tpf_ccd_apply_refined(const tpf_ccd_plan* p64, const tpf_ccd_plan* p32, int64_t outer, int64_t inner,
+                          const double* f, double* d1, double* d2, int refinements, float* work, void* stream) {
+  TPF_CHECK_ARG(p64 && p32 && f && d1 && d2 && work, "NULL argument");
+  TPF_CHECK_ARG(p64->dtype == TPF_F64 && p32->dtype == TPF_F32, "plans must be FP64 and FP32");
+  TPF_CHECK_ARG(p64->bc == TPF_BC_WALL && p32->bc == TPF_BC_WALL,
+                "iterative refinement of the CCD line solves covers wall axes");
+  TPF_CHECK_ARG(p64->n_pts == p32->n_pts && p64->h == p32->h, "the FP64 and FP32 plans differ");
+  TPF_CHECK_ARG(outer >= 0 && inner >= 1, "invalid line decomposition");
+  TPF_CHECK_ARG(refinements >= 0 && refinements <= 8, "refinements must be in [0, 8]");
+  TPF_CHECK_ARG(f != d1 && f != d2 && d1 != d2, "f, d1 and d2 must be distinct");
+  const int64_t n_lines = outer * inner;
+  if (n_lines == 0) return TPF_OK;
+  int st = refine_factors(p64);
+  if (st) return st;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int n = (int)p64->n_pts;
+  const int64_t total = n_lines * n;
+  float* f32 = work;
+  float* a32 = work + total;
+  float* b32 = work + 2 * total;
+  float* R1 = work + 3 * total;
+  float* R2 = work + 4 * total;
+  const int eb = (int)std::min<int64_t>((total + 255) / 256, 8 * 148 * 4);
+  ccd_cast_kernel<<<eb, 256, 0, s>>>(total, f, f32);
+  TPF_CUDA_TRY(cudaGetLastError());
+  if ((st = launch_ccd<float>(p32, outer, inner, f32, a32, b32, nullptr, nullptr, 0, s))) return st;
+  ccd_widen_kernel<<<eb, 256, 0, s>>>(total, a32, d1);
+  ccd_widen_kernel<<<eb, 256, 0, s>>>(total, b32, d2);
+  for (int r = 0; r < refinements; ++r) {
+    ccd_resid_kernel<<<eb, 256, 0, s>>>(total, inner, n, p64->h, f, d1, d2, R1, R2);
+    ccd_corr_kernel<<<(int)((n_lines + 127) / 128), 128, 0, s>>>(n_lines, inner, n, (float)p64->h, p64->d_rfac, R1,
+                                                                 R2, d1, d2);
+  }
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
 }
 
 int tpf_ccd_apply_vd(const tpf_ccd_plan* p, int64_t outer, int64_t inner, const void* f, const void* rho,

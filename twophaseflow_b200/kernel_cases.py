@@ -61,6 +61,27 @@ def ccd_case(N, axis, bc, dtype, reps, warmup=3):
             "GBps": round(nbytes / (ms * 1e-3) / 1e9, 1), "alg_bytes": nbytes}
 
 
+def ccd_refined_case(N, axis, refinements=2, reps=5):
+    """FP32 CCD line solves under FP64 iterative refinement against the direct
+    FP64 solve (wall, FP64 field f = 32 seeded Fourier modes): device time per
+    call (graph-replayed, the workspace allocated outside the graph) and the
+    error of each against the FP64 result relative to max |d|."""
+    import torch
+    from . import CCDSolver, UniformGrid
+    from .workloads import fourier_field
+    f = torch.from_numpy(fourier_field(N, seed=0)).to("cuda")
+    ccd = CCDSolver(UniformGrid(N), None, bc_type="wall")
+    d1, d2 = ccd.differentiate(f, axis)
+    r1, r2 = ccd.differentiate_refined(f, axis, refinements)
+    e1 = float((r1 - d1).abs().max() / d1.abs().max())
+    e2 = float((r2 - d2).abs().max() / d2.abs().max())
+    t64 = _graph_time(lambda: ccd.differentiate(f, axis), reps)
+    tref = _graph_time(lambda: ccd.differentiate_refined(f, axis, refinements), reps)
+    return {"case": "ccd_refined", "N": list(N), "axis": axis, "refinements": refinements,
+            "us_fp64": round(t64 * 1e3, 2), "us_refined": round(tref * 1e3, 2),
+            "err_d1_vs_fp64": e1, "err_d2_vs_fp64": e2}
+
+
 def _graph_time(fn, reps, warmup=3):
     """Device time per call of ``fn`` from a CUDA graph of ``reps`` calls."""
     import torch
