@@ -464,6 +464,9 @@ def main(argv=None):
     # solve (257^3 wall, strided and contiguous axis; error vs FP64 stated)
     from twophaseflow_b200.kernel_cases import ccd_refined_case
     ccd_ref = [ccd_refined_case((256, 256, 256), ax, 2, 3) for ax in (0, 2)]
+    # the FCCD matrix-free PPE operator (2-D 1025^2 wall, 3-D 257^3 wall)
+    from twophaseflow_b200.kernel_cases import fccd_ppe_case
+    fccd_b = [fccd_ppe_case((1024, 1024), "wall", 5), fccd_ppe_case((256, 256, 256), "wall", 3)]
     ccd3 = [c for c in ccd if len(c["N"]) == 3 and c["dtype"] == "f64"]
     ccd3_gbps = float(np.mean([c["GBps"] for c in ccd3]))
     ccd3_best = max(ccd3, key=lambda c: c["GBps"])
@@ -519,6 +522,7 @@ def main(argv=None):
             "batched_32_cases": bat,
             "ccd": ccd,
             "ccd_fp32_refined_257cubed": ccd_ref,
+            "fccd_ppe_apply": fccd_b,
             "corrector_257cubed_f64_wall": {"per_axis": corr, "peak": peak, "peak_kind": peak_kind,
                                             "frac_mean": round(float(np.mean([c["GBps"] for c in corr])) / peak, 3)},
             "curvature_257cubed_f64_wall": {k: v for k, v in curv.items() if k not in ("case", "N", "bc", "dtype")},

@@ -67,11 +67,12 @@ int tpf_ccd_plan_create(tpf_ccd_plan** plan, int64_t n_pts, double h, int bc,
                         int dtype);
 int tpf_ccd_plan_destroy(tpf_ccd_plan* plan);
 
-/* Launch-shape autotuning of the many-line kernel (default on; no counterpart
+/* Launch-shape autotuning of the line kernels (default on; no counterpart
  * in the reference): the first tpf_ccd_apply of each (line count, axis kind,
  * boundary, outputs, dtype) combination times a few launch shapes on the
- * caller's stream and keeps the fastest (results are identical for every
- * shape).  That first call synchronizes the stream; it is skipped while the
+ * caller's stream and keeps the fastest -- warps per block and tile ring depth
+ * of the lane-per-line kernel (3-D grids), lines per block and tile buffers of
+ * the warp kernel (2-D grids) -- results are identical for every shape.  That first call synchronizes the stream; it is skipped while the
  * stream is being captured.  enable = 0 switches tuning off and forgets the
  * choices. */
 int tpf_ccd_plan_set_autotune(tpf_ccd_plan* plan, int enable);

@@ -354,6 +354,30 @@ def test_ccd_autotune_is_bitwise_neutral(cuda_device, bc):
     assert torch.equal(b1, c1) and torch.equal(b2, c2)
 
 
+@pytest.mark.parametrize("N,bc,axis", [((1024, 600), "wall", 0), ((1024, 600), "periodic", 1),
+                                       ((300, 200), "wall", 1), ((200, 64), "periodic", 0)])
+def test_ccd_warp_kernel_autotune_is_bitwise_neutral(cuda_device, N, bc, axis):
+    """2-D grids (the warp kernel, 1-4 warps per line): the tuned launch shape
+    (lines per block, tile buffers), the cached one and the heuristic one give
+    bitwise identical derivatives, which match the oracle."""
+    import torch
+    from twophaseflow_b200 import CCDSolver, UniformGrid, _lib
+    f = fourier_field(N, n_modes=6, kmax=6, seed=8)
+    ft = torch.from_numpy(f).to(cuda_device)
+    tuned = CCDSolver(UniformGrid(N), None, bc_type=bc)
+    plain = CCDSolver(UniformGrid(N), None, bc_type=bc)
+    plan = plain._plan(axis, bc == "periodic")
+    _lib.check(plain.lib.tpf_ccd_plan_set_autotune(plan, 0))
+    a1, a2 = tuned.differentiate(ft, axis)
+    b1, b2 = tuned.differentiate(ft, axis)
+    c1, c2 = plain.differentiate(ft, axis)
+    assert torch.equal(a1, c1) and torch.equal(a2, c2)
+    assert torch.equal(b1, c1) and torch.equal(b2, c2)
+    o1, o2 = occd.differentiate(f, axis, 1.0 / N[axis], bc=bc)
+    assert np.abs(c1.cpu().numpy() - o1).max() <= 1e-11 * np.abs(o1).max()
+    assert np.abs(c2.cpu().numpy() - o2).max() <= 1e-11 * np.abs(o2).max()
+
+
 @pytest.mark.parametrize("N,axis", [((128, 96), 0), ((128, 96), 1), ((40, 36, 48), 2), ((40, 36, 48), 0)])
 def test_ccd_refined_fp32_reaches_fp64(cuda_device, N, axis):
     """FP32 line solves under FP64 iterative refinement: without refinement the

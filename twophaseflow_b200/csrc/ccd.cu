@@ -1804,6 +1804,32 @@ LaunchShape pick_warp_shape(const tpf_ccd_plan* p, int64_t n_lines, int W) {
   return best;
 }
 
+// launch shape of the warp kernel for one (lines per block, tile buffers) choice
+template <typename T, int R>
+LaunchShape warp_shape(const tpf_ccd_plan* p, int64_t n_lines, int W, int TL, int nbuf) {
+  const int n = (int)p->n_pts;
+  int FSP = n + (n - 1) / R + 1;
+  if (FSP % 2 == 0) ++FSP;
+  const int nsm = tpf::sm_count();
+  const int regs = R == 8 ? 128 : (R == 16 ? 168 : 255);
+  TabLayout lay{R, p->H0};
+  LaunchShape out{};
+  out.TL = 0;
+  const int threads = 32 * W * TL;
+  if (threads > 256) return out;
+  const size_t fsz = (size_t)TL * FSP;
+  const size_t sm = sizeof(long long) * 2 * TL + sizeof(T) * (((size_t)lay.total() + 1) & ~(size_t)1) +
+                    sizeof(T) * (nbuf + 1) * fsz + 64;
+  if (sm > 225 * 1024) return out;
+  const int by_smem = (int)((228 * 1024) / (sm + 1024));
+  const int by_regs = 65536 / (regs * threads);
+  const int per_sm = std::max(1, std::min(std::min(by_smem, by_regs), 16));
+  const int64_t tiles = (n_lines + TL - 1) / TL;
+  const int64_t grid = std::min<int64_t>(tiles, (int64_t)nsm * per_sm);
+  out = {TL, 0, FSP, nbuf, (int)grid, sm};
+  return out;
+}
+
 // many lines (3-D grids) and long enough lines: the lane-per-line kernel
 bool use_lane_kernel(const tpf_ccd_plan* p, int64_t n_lines, bool periodic, bool contig) {
   if (p->n_rows < 128 || p->n_rows > 2048) return false;
@@ -1961,9 +1987,67 @@ int launch_ccd(const tpf_ccd_plan* p, int64_t outer, int64_t inner, const void* 
     else { TPF_WARP_KERN(4) }
 #undef TPF_WARP_KERN
   }
-  TPF_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem));
-  kern<<<s.grid, warp ? 32 * W * s.TL : s.TL * p->P, s.smem, stream>>>(a);
-  TPF_CUDA_TRY(cudaGetLastError());
+  auto launch = [&](const LaunchShape& sh) -> int {
+    CcdArgs b = a;
+    b.TL = sh.TL;
+    b.tl_shift = 0;
+    while ((1 << b.tl_shift) < sh.TL) ++b.tl_shift;
+    b.FS = (contig || warp) ? sh.FS : 0;
+    b.LS = sh.LS;
+    b.nbuf = sh.nbuf;
+    b.n_tiles = (int)((n_lines + sh.TL - 1) / sh.TL);
+    TPF_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem));
+    kern<<<sh.grid, warp ? 32 * W * sh.TL : sh.TL * p->P, sh.smem, stream>>>(b);
+    TPF_CUDA_TRY(cudaGetLastError());
+    return TPF_OK;
+  };
+  if (!warp) return launch(s);
+  // Warp kernel: the launch shape (lines per block, tile buffers) is picked by
+  // timing on the first call of each (line count, axis kind, boundary,
+  // outputs, dtype) combination, like the lane kernel's; every shape gives
+  // identical results (the lines are solved independently).
+  const bool plain = a.d1 && a.d2 && !a.vd_out && !a.J && !a.cr_out;
+  const uint64_t key = ((uint64_t)n_lines << 8) | (1ull << 7) | ((uint64_t)contig << 0) | ((uint64_t)per << 1) |
+                       ((uint64_t)plain << 2) | ((uint64_t)(sizeof(T) == 8) << 3) | ((uint64_t)W << 4);
+  auto it = p->lane_tuned.find(key);
+  if (it != p->lane_tuned.end()) {
+    const LaunchShape ts = warp_shape<T, 8>(p, n_lines, W, it->second.warps, it->second.nbuf);
+    if (ts.TL > 0) return launch(ts);
+  }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  TPF_CUDA_TRY(cudaStreamIsCapturing(stream, &cs));
+  if (!p->autotune || cs != cudaStreamCaptureStatusNone || (a.vd_out && a.vd_accumulate) ||
+      (a.cr_out && a.cr_out == a.cr_u))
+    return launch(s);
+  cudaEvent_t e0, e1;
+  TPF_CUDA_TRY(cudaEventCreate(&e0));
+  TPF_CUDA_TRY(cudaEventCreate(&e1));
+  float best = 1e30f;
+  LaunchShape bs = s;
+  int st = TPF_OK;
+  const int tls[4] = {8, 4, 2, 1};
+  for (int ti = 0; ti < 4 && !st; ++ti) {
+    for (int nbuf = 1; nbuf <= 2 && !st; ++nbuf) {
+      const LaunchShape c = warp_shape<T, 8>(p, n_lines, W, tls[ti], nbuf);
+      if (c.TL == 0) continue;
+      if ((st = launch(c))) break;
+      cudaEventRecord(e0, stream);
+      for (int r = 0; r < 2 && !st; ++r) st = launch(c);
+      cudaEventRecord(e1, stream);
+      if (cudaEventSynchronize(e1) != cudaSuccess || st) break;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best) {
+        best = ms;
+        bs = c;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st) return st;
+  p->lane_tuned[key] = LaneShape_{bs.TL, bs.nbuf, 0};
+  // the last candidate's results are in place and identical for every shape
   return TPF_OK;
 }
 

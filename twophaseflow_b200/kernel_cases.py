@@ -82,6 +82,33 @@ def ccd_refined_case(N, axis, refinements=2, reps=5):
             "err_d1_vs_fp64": e1, "err_d2_vs_fp64": e2}
 
 
+def fccd_ppe_case(N, bc="wall", reps=5):
+    """FCCD matrix-free PPE operator application (the image gather on periodic
+    axes, one CCD second-derivative solve per axis, the fused face-gradient /
+    coefficient / divergence kernel), graph-replayed, with its algorithmic
+    bytes: per axis 16 B/node for the CCD call (read p, write q) plus
+    (3 + ndim) x 8 B/node for the fused kernel (p, rho, the q's, out)."""
+    import torch
+    from . import FCCDSolver, PPESolverFCCDMatrixFree, UniformGrid
+    from .workloads import divergence_rhs, droplet_density
+
+    class Cfg:
+        pseudo_tol = 1e-8
+        pseudo_maxiter = 500
+        ppe_preconditioner = "jacobi"
+
+    grid = UniformGrid(N)
+    s = PPESolverFCCDMatrixFree(None, Cfg(), grid, FCCDSolver(grid, None, bc_type=bc))
+    rho = torch.from_numpy(droplet_density(N, seed=0, rho_g=0.1)).cuda()
+    p = torch.from_numpy(divergence_rhs(N, seed=1)).cuda()
+    s.prepare_operator(rho)
+    t = _graph_time(lambda: s.apply(p), reps)
+    nd = len(N)
+    nbytes = p.numel() * 8 * (2 * nd + 3 + nd) + (p.numel() * 16 if bc == "periodic" else 0)
+    return {"case": "fccd_apply", "N": list(N), "bc": bc, "us_per_apply": round(t * 1e3, 2),
+            "GBps": round(nbytes / (t * 1e-3) / 1e9, 1), "alg_bytes": nbytes}
+
+
 def _graph_time(fn, reps, warmup=3):
     """Device time per call of ``fn`` from a CUDA graph of ``reps`` calls."""
     import torch
