@@ -641,8 +641,63 @@ def make_c1(out):
         out[f"s{k}/p"] = np.array(sim.pressure.data)
 
 
+C1_CHECKPOINT_YAML = """\
+run:
+  T_final: 0.05
+  cfl: 0.3
+grid:
+  ndim: 2
+  N: [64, 64]
+  L: [1.0, 1.0]
+fluid:
+  Re: 100.0
+  Fr: 1.0
+  We: 10.0
+  rho_ratio: 0.1
+  mu_ratio: 0.1
+numerics:
+  extension_method: none
+output:
+  dir: results/c1
+"""
+
+
+def make_checkpoint(out):
+    """A restart checkpoint written by the reference's own writer
+    (simulation/checkpoint.py save_checkpoint) after three quick-start steps
+    (the make_c1 run): state/psi, u, v, p, the grid, p^n as
+    solver/p_prev_dev and the predictor's AB2 convection history as
+    solver/conv_prev.  Writes c1_checkpoint_ref.npz and c1_checkpoint.yaml
+    (the config the fingerprint covers) next to this script; ``out`` stays
+    empty."""
+    from types import SimpleNamespace
+    from twophase.config import FluidConfig, GridConfig, NumericsConfig, SimulationConfig
+    from twophase.simulation.builder import SimulationBuilder
+    from twophase.simulation.checkpoint import save_checkpoint
+
+    cfg = SimulationConfig(grid=GridConfig(ndim=2, N=(64, 64), L=(1.0, 1.0)),
+                           fluid=FluidConfig(Re=100.0, Fr=1.0, We=10.0, rho_ratio=0.1, mu_ratio=0.1),
+                           numerics=NumericsConfig(extension_method="none"))
+    sim = SimulationBuilder(cfg).build()
+    X, Y = sim.grid.meshgrid()
+    sim.psi.data[:] = 1.0 / (1.0 + np.exp(-(np.sqrt((X - 0.5) ** 2 + (Y - 0.5) ** 2) - 0.25) / (1.5 / 64)))
+    t = 0.0
+    for _ in range(3):
+        dt = float(sim.cfl_calc.compute([sim.velocity[0], sim.velocity[1]], sim.mu.data, sim.rho.data))
+        sim.step_forward(dt)
+        t += dt
+    yaml_path = os.path.join(HERE, "c1_checkpoint.yaml")
+    with open(yaml_path, "w") as fh:
+        fh.write(C1_CHECKPOINT_YAML)
+    solver = SimpleNamespace(_backend=sim.backend, _grid=sim.grid, _p_prev_dev=np.array(sim.pressure.data),
+                             _conv_prev=sim.predictor._conv_prev, _conv_ab2_ready=sim.predictor._ab2_ready)
+    save_checkpoint(os.path.join(HERE, "c1_checkpoint_ref.npz"), solver=solver, psi=sim.psi.data,
+                    u=sim.velocity[0], v=sim.velocity[1], p=sim.pressure.data, t=t, step=3,
+                    config_path=yaml_path, state_phase="post_step", dt_candidate=dt, dt_effective=dt)
+
+
 def main():
-    """Usage: make_golden.py <reference src dir> [only: ccd|ppe|step|levelset|rhiechow|advect|reinit|viscous|predictor|fccd_ppe|c1 ...].
+    """Usage: make_golden.py <reference src dir> [only: ccd|ppe|step|levelset|rhiechow|advect|reinit|viscous|predictor|fccd_ppe|c1|checkpoint ...].
 
     The source directory comes from the first argument or, when the
     argument list is empty, from the TWOPHASE_REFERENCE_SRC environment variable."""
@@ -658,12 +713,15 @@ def main():
     makers = {"ccd": make_ccd, "ppe": make_ppe, "step": make_step, "levelset": make_levelset,
               "rhiechow": make_rhiechow, "advect": make_advect, "reinit": make_reinit,
               "viscous": make_viscous, "predictor": make_predictor,
-              "fccd_ppe": make_fccd_ppe, "c1": make_c1}
+              "fccd_ppe": make_fccd_ppe, "c1": make_c1, "checkpoint": make_checkpoint}
     for key, fn in makers.items():
         if only and key not in only:
             continue
         arrays = {}
         fn(arrays)
+        if not arrays:      # the maker wrote its own files
+            print("wrote", key, "files")
+            continue
         np.savez_compressed(os.path.join(HERE, f"{key}_golden.npz"), **arrays)
         print("wrote", len(arrays), key, "arrays")
 

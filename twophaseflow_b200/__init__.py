@@ -12,11 +12,14 @@
 * ``VelocityCorrector`` / ``CFLCalculator`` / ``ccd_pressure_gradient`` -- the
   steps either side of the PPE (velocity correction fused into the CCD line
   solve; CFL maxima in one reduction).
+* ``TwoPhaseStep`` -- the whole two-phase step; ``save_checkpoint`` /
+  ``load_checkpoint`` -- restart files in the reference's ``.npz`` format.
 
 All arithmetic runs in the in-tree CUDA library ``libtpf.so`` (C ABI:
 ``include/tpf.h``); build it with ``python -m twophaseflow_b200.build``.
 """
 
+from . import checkpoint
 from .advection import FCCDLevelSetAdvection, FCCDSolver, SplitReinitializer, UCCD6ConvectionTerm
 from .ccd import CCDSolver
 from .ccd_ppe import CCDVariableDensityOperator, PPESolverDefectCorrection
@@ -29,6 +32,7 @@ from .viscous import PicardCNAdvance, ViscousTerm
 from .predictor import ConvectionTerm, FlowState, GravityTerm, NSComputeContext, Predictor, SurfaceTensionTerm
 from .ns_step import TwoPhaseStep
 from .step import CFLCalculator, RhieChowInterpolator, VelocityCorrector, ccd_pressure_gradient
+from .checkpoint import CheckpointError, load_checkpoint, save_checkpoint
 
 __all__ = [
     "CCDSolver",
@@ -62,4 +66,8 @@ __all__ = [
     "CurvatureCalculatorPsi",
     "dccd_filter_nd",
     "update_properties",
+    "checkpoint",
+    "CheckpointError",
+    "save_checkpoint",
+    "load_checkpoint",
 ]

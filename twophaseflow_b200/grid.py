@@ -3,7 +3,7 @@
 The reference's own ``twophase.core.grid.Grid`` (src/twophase/core/grid.py:36-120)
 and ``BoundarySpec`` (src/twophase/core/boundary.py:143-204) can be passed
 wherever these are accepted: only ``ndim``, ``N``, ``L``, ``shape``,
-``uniform``, ``coords`` and, for non-uniform grids, ``J`` / ``dJ_dxi`` are read.
+``uniform``, ``coords``, ``h`` (checkpoints) and, for non-uniform grids, ``J`` / ``dJ_dxi`` are read.
 """
 
 from __future__ import annotations
@@ -24,6 +24,8 @@ class UniformGrid:
         self.coords = [np.linspace(0.0, l, n + 1) for n, l in zip(self.N, self.L)]
         self.uniform = True
         self.J = [np.full(n + 1, n / l) for n, l in zip(self.N, self.L)]
+        # per-node spacing, the reference grid's ``h`` (core/grid.py:60-68)
+        self.h = [np.full(n + 1, l / n) for n, l in zip(self.N, self.L)]
         self.dJ_dxi = [np.zeros(n + 1) for n in self.N]
 
 

@@ -9,14 +9,16 @@ gravity, CSF, -grad p^n, Picard-CN viscous) -> Rhie-Chow face-velocity
 divergence / dt -> PPE for the pressure increment (FVM matrix-free CG, the
 persistent kernel) -> velocity corrector, p += dp -> CFL maxima.
 
-``TwoPhaseStep.step(dt)`` replays graph 1 (everything up to the PPE
-right-hand side), runs the PPE solve (one persistent kernel; it reports its
-iteration count to the host, so it stays outside the graphs), then replays
-graph 2 (corrector, pressure update, CFL maxima).  The first call for a given
-dt runs the step eagerly (CCD plans, autotuning, allocator pools) and then
-captures the two graphs.  Each operator is pinned to the reference by its
-own tests; this composition integrates them and is not a bitwise
-restatement of one reference pipeline variant.
+``TwoPhaseStep.step(dt)`` with the CG pressure route replays ONE graph that
+holds the whole step, the solve included (its iteration count is read after
+the replay).  With the GMRES route it replays graph 1 (everything up to the
+PPE right-hand side), runs the host-driven solve, then replays graph 2
+(corrector, pressure update, CFL maxima).  The first call for a given dt runs
+the step eagerly (CCD plans, autotuning, allocator pools) and then captures.
+With the quick-start selection the composition is pinned to six steps of the
+reference's own pipeline; ``save_checkpoint`` / ``restore_checkpoint_state``
+carry its state through the reference's restart format
+(twophaseflow_b200.checkpoint).
 """
 
 from __future__ import annotations
@@ -24,6 +26,8 @@ from __future__ import annotations
 import ctypes as C
 import math
 from types import SimpleNamespace
+
+import numpy as np
 
 from . import _lib
 from .advection import FCCDLevelSetAdvection, FCCDSolver, SplitReinitializer, UCCD6ConvectionTerm
@@ -73,6 +77,11 @@ class TwoPhaseStep:
         58-137) with Crank-Nicolson viscosity: the convective bound and the
         capillary bound cfl * sqrt((1 + rho_ratio) We h^3 / (2 pi))."""
         torch = _torch()
+        self.options = dict(Re=Re, Fr=Fr, We=We, rho_ratio=rho_ratio, mu_ratio=mu_ratio, cfl=cfl, eps=eps,
+                            reinit_steps=reinit_steps, ppe_tol=ppe_tol, ppe_maxiter=ppe_maxiter,
+                            convection=convection, transport_mass_correction=bool(transport_mass_correction),
+                            reinit_bc=reinit_bc, ppe_method=ppe_method, no_slip=bool(no_slip),
+                            zero_velocity_shortcut=bool(zero_velocity_shortcut))
         self.grid = grid
         nd = grid.ndim
         self.nd = nd
@@ -151,9 +160,12 @@ class TwoPhaseStep:
         st = _lib.current_stream_handle()
         _lib.check(self.lib.tpf_visc_accumulate(self.p.numel(), _lib.dptr(self.dp), 1, 0, None, 0.0,
                                                 _lib.dptr(self.p), _lib.TPF_F64, st))
+        self._update_maxima()
+
+    def _update_maxima(self):
         ptrs = (C.c_void_p * self.nd)(*[_lib.dptr(v) for v in self.vel])
         _lib.check(self.lib.tpf_cfl_maxima(self.p.numel(), self.nd, ptrs, None, None, _lib.TPF_F64,
-                                           _lib.dptr(self.maxima), st))
+                                           _lib.dptr(self.maxima), _lib.current_stream_handle()))
 
     def _wall_zero(self, comps):
         """No-slip: every component zero on both planes of every (wall) axis."""
@@ -230,3 +242,70 @@ class TwoPhaseStep:
         if self._dt_sigma is not None:
             cands.append(self.cfl * self._dt_sigma)
         return max(min(cands), 1.0e-8)
+
+    # -- restart checkpoints (twophaseflow_b200.checkpoint) --------------------------
+    backend_device = "gpu"
+
+    def checkpoint_config(self) -> dict:
+        """The options that define this run (the config fingerprint of a
+        checkpoint written without a YAML config)."""
+        return {"N": list(self.grid.N), "L": list(self.grid.L), **self.options}
+
+    def checkpoint_state(self) -> dict:
+        """History the next step reads besides psi, u, p: p^n for the
+        incremental pressure correction (after a step), the AB2 convection
+        history and its ready flag."""
+        pr = self.predictor
+        return {"p_prev_dev": None if self._vel_zero else self.p,
+                "conv_prev": pr._conv_prev if pr._ab2_ready else None,
+                "conv_ab2_ready": bool(pr._ab2_ready and pr._conv_prev is not None)}
+
+    def save_checkpoint(self, path, *, t: float, step: int, config_path=None, **kw) -> None:
+        """``checkpoint.save_checkpoint`` with this step's own fields."""
+        from .checkpoint import save_checkpoint
+        save_checkpoint(path, solver=self, psi=self.psi, u=self.vel[0], v=self.vel[1], p=self.p,
+                        w=self.vel[2] if self.nd == 3 else None, t=t, step=step, config_path=config_path, **kw)
+
+    def restore_checkpoint_state(self, st: dict) -> dict:
+        """Copy a checkpoint's state into this step's device tensors: psi, the
+        velocity, p, the AB2 history; rho, mu and the CFL maxima are
+        recomputed from them and the captured graphs are dropped (the next
+        step runs eagerly and captures again)."""
+        from .checkpoint import CheckpointError
+        torch = _torch()
+        for a, c in enumerate(st.get("grid_coords") or ()):
+            if not np.array_equal(np.asarray(c, dtype=np.float64), np.asarray(self.grid.coords[a], dtype=np.float64)):
+                raise CheckpointError("checkpoint grid coordinates differ from this step's uniform grid")
+        if len(st["velocity"]) != self.nd:
+            raise CheckpointError(f"checkpoint holds {len(st['velocity'])} velocity components, the grid has {self.nd}")
+        dev = self.psi.device
+
+        def put(dst, arr):
+            dst.copy_(torch.as_tensor(np.asarray(arr, dtype=np.float64), device=dev))
+        put(self.psi, st["psi"])
+        for c in range(self.nd):
+            put(self.vel[c], st["velocity"][c])
+        put(self.p, st["p"])
+        pr = self.predictor
+        conv = st.get("conv_prev")
+        if st.get("conv_ab2_ready") and conv is not None:
+            if len(conv) != self.nd:
+                raise CheckpointError("checkpoint AB2 history has the wrong number of components")
+            if pr._conv_prev is None:
+                pr._conv_prev = [torch.empty_like(self.psi) for _ in range(self.nd)]
+            for c in range(self.nd):
+                put(pr._conv_prev[c], conv[c])
+            pr._ab2_ready = True
+        else:
+            pr._ab2_ready = False
+        rho, mu = update_properties(None, self.psi, self.rho_l, self.rho_g, self.mu_l, self.mu_g)
+        self.rho.copy_(rho)
+        self.mu.copy_(mu)
+        self._vel_zero = (not pr._ab2_ready) and all(float(v.abs().max()) == 0.0 for v in self.vel)
+        self._g1 = self._g2 = None
+        self._dt_graph = None
+        self._update_maxima()
+        fields = {"psi": self.psi, "u": self.vel[0], "v": self.vel[1], "p": self.p}
+        if self.nd == 3:
+            fields["w"] = self.vel[2]
+        return fields
