@@ -152,10 +152,15 @@ def _solver(precision):
     return PPESolverFVMMatrixFree(None, cfg, UniformGrid(N_PPE))
 
 
-def time_ppe(precision, rho_d, rhs_d, steps, warmup, flush):
-    """Device-resident solves; L2 flushed before every step (untimed)."""
+def time_ppe(precision, rho_d, rhs_d, steps, warmup, flush, cg_kernel=0):
+    """Device-resident solves; L2 flushed before every step (untimed).
+    ``cg_kernel``: 0 the default choice, 1 the all-global persistent kernel."""
+    import ctypes
     import torch
+    from twophaseflow_b200 import _lib
     s = _solver(precision)
+    if cg_kernel:
+        _lib.check(s.lib.tpf_ppe_set_cg_kernel(s._handle, ctypes.c_int(cg_kernel)))
     for _ in range(warmup):
         s.solve(rhs_d, rho_d)
     torch.cuda.synchronize()
@@ -427,6 +432,10 @@ def main(argv=None):
     smx, pmx, tmx = time_ppe("mixed", rho_d, rhs_d, max(2, args.steps // 2), 1, flush)
     _barrier(ws)
     dmx = smx.last_diagnostics
+    # the same mixed solve on the all-global FP32 kernel (kernel-for-kernel context)
+    smg, _, tmg = time_ppe("mixed", rho_d, rhs_d, 2, 1, flush, cg_kernel=1)
+    _barrier(ws)
+    dmg = smg.last_diagnostics
     slr, plr, tlr = time_learned(rho_d, rhs_d, max(2, args.steps // 3), 1, flush)
     _barrier(ws)
     dlr = slr.last_diagnostics
@@ -505,6 +514,7 @@ def main(argv=None):
     # many independent cases in one persistent launch (32 seeded grids, 128..512 per axis)
     from twophaseflow_b200.kernel_cases import batched_case
     bat = batched_case(n_cases=32, reps=2)
+    bat_small = batched_case(n_cases=64, nmin=64, nmax=64, reps=3)
     bat.pop("grids", None)
 
     cpu = None
@@ -520,6 +530,7 @@ def main(argv=None):
             "bench_detail": True,
             "learned_heldout": heldout,
             "batched_32_cases": bat,
+            "batched_64_cases_64x64": bat_small,
             "ccd": ccd,
             "ccd_fp32_refined_257cubed": ccd_ref,
             "fccd_ppe_apply": fccd_b,
@@ -531,9 +542,15 @@ def main(argv=None):
             "reinit_257cubed_f64": {k: v for k, v in reib.items() if k not in ("case", "N", "dtype")},
             "viscous_257cubed_f64_wall": {k: v for k, v in visb.items() if k not in ("case", "N", "dtype")},
             "two_phase_step_192cubed": {k: v for k, v in stepb.items() if k not in ("case", "N")},
-            "mixed_detail": {"inner_iterations": dmx["ppe_low_order_cg_iterations"],
+            "mixed_detail": {"kernel": "band-resident FP32 (shared-memory vectors), FP64 residual replacement",
+                             "inner_iterations": dmx["ppe_low_order_cg_iterations"],
                              "replacements": dmx["ppe_low_order_cg_refinements"],
-                             "rel_residual": dmx["ppe_low_order_cg_relative_residual"]},
+                             "rel_residual": dmx["ppe_low_order_cg_relative_residual"],
+                             "us_per_iteration": round(float(np.mean(tmx)) * 1e3
+                                                       / max(1, dmx["ppe_low_order_cg_iterations"]), 2),
+                             "fp64_us_per_iteration": round(float(np.mean(t64)) * 1e3 / max(1, it64), 2),
+                             "global_fp32_kernel_ms": round(float(np.mean(tmg)), 3),
+                             "global_fp32_kernel_iterations": dmg["ppe_low_order_cg_iterations"]},
             "learned_detail": {"fallback_iterations": dlr["ppe_learned_fallback_iterations"],
                                "rel_residual": dlr["ppe_learned_relative_residual"],
                                "us_per_iteration": round(ms_lr * 1e3 / max(1, dlr["ppe_learned_iterations"]), 1)},
@@ -546,7 +563,7 @@ def main(argv=None):
             "data": "synthetic (seeded droplets, seeded velocity divergence)",
             "config": {"workload": WORKLOAD, "grid": list(N_PPE), "tol": TOL,
                        "method": {"fp64": "FP64 Jacobi-PCG, persistent single-reduction kernel",
-                                  "mixed": "mixed: FP32 Jacobi-PCG with FP64 residual replacement",
+                                  "mixed": "mixed: band-resident FP32 Jacobi-PCG with FP64 residual replacement",
                                   "learned": "two-level U-Net-preconditioned flexible CG"}[best],
                        "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{ws}"},
             "plain_fp64_pcg_ms": round(ms_64, 3), "plain_fp64_iterations": it64,

@@ -373,15 +373,16 @@ int tpf_ppe_create(tpf_ppe** h, int ndim, const int64_t* N,
                    const tpf_ppe_options* opts);
 int tpf_ppe_destroy(tpf_ppe* h);
 int tpf_ppe_set_options(tpf_ppe* h, const tpf_ppe_options* opts);
-/* Kernel of the FP64 CG solve (same iteration, same stopping rule):
+/* Kernel of the CG solve (same iteration, same stopping rule):
  * 0 (default) = the band-resident kernel when it applies, else 3 for FP64
  *     systems, else (mixed precision) 1;
  * 1 = one persistent cooperative launch with every vector in global memory
  *     (any grid, FP64 or mixed);
  * 2 = the band-resident kernel: 2-D systems whose nodes, split into one
  *     contiguous range per SM (at least one row each, at most 768 nodes per
- *     row), fit in shared memory with 12 vectors (513^2 on a B200); only the
- *     ranges' first and last rows cross L2 each iteration.
+ *     row), fit in shared memory with 12 FP64 vectors (~550^2 on a B200) or,
+ *     mixed, 11 FP32 vectors and x in FP64 (~770^2); only the ranges' first
+ *     and last rows cross L2 each iteration.
  *     TPF_EINVAL from tpf_ppe_solve when it does not apply;
  * 3 = streaming (FP64): each iteration as two ordinary full-occupancy
  *     kernels (vector update; stencil + inner products, the last block
@@ -429,11 +430,17 @@ int tpf_ppe_solve(tpf_ppe* h, const double* rhs, const double* rho, double* p,
 /* Batched solve (no counterpart in the reference, which solves one system
  * per call): n independent systems (n <= 64, each its own handle and grid,
  * all with method TPF_PPE_CG and one precision) in ONE cooperative launch;
- * every system runs the persistent PCG of tpf_ppe_solve on a share of the
- * SMs proportional to its node count, with its own grid barrier.  rho may be
- * NULL (or hold NULL entries) for handles prepared beforehand.  results[c]
- * as tpf_ppe_solve; returns the first failure (TPF_ENOCONV / TPF_EABORT)
- * after all systems finished.  Synchronizes `stream`. */
+ * every system runs the persistent PCG of tpf_ppe_solve on its own share of
+ * the SMs (proportional to ndof^1.5, its expected work), with its own grid
+ * barrier.  When every system is 2-D and all their bands fit in shared
+ * memory at once (the systems' nodes summing to at most ~340 000 in FP64,
+ * ~640 000 mixed, on 148 SMs), each runs band-resident; otherwise each runs
+ * the all-global body.  tpf_ppe_set_cg_kernel on any handle selects: 1 the
+ * all-global body, 2 the band-resident batch (TPF_EINVAL if it does not
+ * fit).  rho may be NULL (or hold NULL entries) for handles prepared
+ * beforehand.  results[c] as tpf_ppe_solve; returns the first failure
+ * (TPF_ENOCONV / TPF_EABORT) after all systems finished.  Synchronizes
+ * `stream`. */
 int tpf_ppe_solve_batched(tpf_ppe* const* handles, int n, const double* const* rhs, const double* const* rho,
                           double* const* p, void* stream, tpf_ppe_result* results);
 

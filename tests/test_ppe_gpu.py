@@ -202,16 +202,21 @@ def test_gmres_with_truncated_pcr_converges(cuda_device):
     np.testing.assert_allclose(p, pd, rtol=1e-5, atol=1e-6 * np.abs(pd).max())
 
 
-def test_batched_solve_matches_individual_solves(cuda_device):
+@pytest.mark.parametrize("kind", [0, 1, 2])
+def test_batched_solve_matches_individual_solves(cuda_device, kind):
     """Uneven grids in one persistent launch: same solutions (and iteration
-    counts within one) as solving each system on its own."""
+    counts within one) as solving each system on its own -- band-resident
+    (kind 0, the default here, and 2, forced) and all-global (kind 1)."""
+    import ctypes as C
     import torch
-    from twophaseflow_b200 import PPESolverFVMMatrixFree, UniformGrid, solve_batched
+    from twophaseflow_b200 import PPESolverFVMMatrixFree, UniformGrid, _lib, solve_batched
     shapes = [(32, 32), (48, 40), (64, 64), (17, 25), (80, 64), (128, 128)]
     solvers, rhs, rho = [], [], []
     for k, N in enumerate(shapes):
         cfg = _Cfg(pseudo_tol=1e-10, pseudo_maxiter=50000, ppe_iteration_method="cg", ppe_preconditioner="jacobi")
         solvers.append(PPESolverFVMMatrixFree(None, cfg, UniformGrid(N)))
+        if kind:
+            _lib.check(solvers[-1].lib.tpf_ppe_set_cg_kernel(solvers[-1]._handle, C.c_int(kind)))
         rho.append(torch.from_numpy(droplet_density(N, n_drops=3, seed=40 + k)).to(cuda_device))
         rhs.append(torch.from_numpy(divergence_rhs(N, seed=60 + k)).to(cuda_device))
     pb = solve_batched(solvers, rhs, rho)
@@ -222,6 +227,53 @@ def test_batched_solve_matches_individual_solves(cuda_device):
         assert abs(it1 - its_b[k]) <= 1, (k, it1, its_b[k])
         scale = float(torch.max(torch.abs(p1)))
         assert float(torch.max(torch.abs(pb[k] - p1))) <= 1e-8 * scale
+
+
+def test_band_batch_many_small_systems_and_mixed(cuda_device):
+    """64 systems of the quick-start grid (64^2, density ratio 1000) in one
+    band-resident launch, FP64 and mixed: every system reaches its tolerance
+    and the direct solution (FP64 within 1e-8, mixed within 1e-6)."""
+    import torch
+    from twophaseflow_b200 import PPESolverFVMMatrixFree, UniformGrid, solve_batched
+    N = (64, 64)
+    coords = oppe.uniform_coords(N, (1.0, 1.0))
+    rho = [droplet_density(N, n_drops=4, seed=300 + k) for k in range(64)]
+    rhs = [divergence_rhs(N, seed=400 + k) for k in range(64)]
+    direct = [oppe.spsolve_fvm(rhs[k], rho[k], coords) for k in (0, 17, 63)]
+    for extra, bar in (({}, 1e-8), ({"ppe_precision": "mixed"}, 1e-6)):
+        cfg = _Cfg(pseudo_tol=1e-10, pseudo_maxiter=50000, ppe_iteration_method="cg", ppe_preconditioner="jacobi",
+                   **extra)
+        solvers = [PPESolverFVMMatrixFree(None, cfg, UniformGrid(N)) for _ in range(64)]
+        pb = solve_batched(solvers, [torch.from_numpy(r).to(cuda_device) for r in rhs],
+                           [torch.from_numpy(r).to(cuda_device) for r in rho])
+        for s in solvers:
+            assert s.last_diagnostics["ppe_low_order_cg_relative_residual"] < 1e-10
+        for j, k in enumerate((0, 17, 63)):
+            pd = direct[j]
+            assert np.abs(pb[k].cpu().numpy() - pd).max() <= bar * np.abs(pd).max(), (extra, k)
+
+
+def test_band_batch_refused_when_bands_do_not_fit(cuda_device):
+    """Forcing the band-resident batch (kind 2) on systems whose bands cannot
+    all be resident at once is an error; the default falls back to the
+    all-global body and still solves."""
+    import ctypes as C
+    import torch
+    from twophaseflow_b200 import PPESolverFVMMatrixFree, UniformGrid, _lib, solve_batched
+    N = (400, 400)   # 160 801 nodes: three systems need more blocks than there are SMs
+    cfg = _Cfg(pseudo_tol=1e-8, pseudo_maxiter=100000, ppe_iteration_method="cg", ppe_preconditioner="jacobi")
+    rho = [torch.from_numpy(droplet_density(N, n_drops=4, seed=500 + k)).to(cuda_device) for k in range(3)]
+    rhs = [torch.from_numpy(divergence_rhs(N, seed=600 + k)).to(cuda_device) for k in range(3)]
+    solvers = [PPESolverFVMMatrixFree(None, cfg, UniformGrid(N)) for _ in range(3)]
+    _lib.check(solvers[1].lib.tpf_ppe_set_cg_kernel(solvers[1]._handle, C.c_int(2)))
+    with pytest.raises(ValueError):
+        solve_batched(solvers, rhs, rho)
+    _lib.check(solvers[1].lib.tpf_ppe_set_cg_kernel(solvers[1]._handle, C.c_int(0)))
+    pb = solve_batched(solvers, rhs, rho)
+    for k, s in enumerate(solvers):
+        assert s.last_diagnostics["ppe_low_order_cg_relative_residual"] < 1e-8
+        p1 = s.solve(rhs[k], rho[k])
+        assert float(torch.max(torch.abs(pb[k] - p1))) <= 1e-6 * float(torch.max(torch.abs(p1)))
 
 
 @pytest.mark.parametrize("N,warm", [((512, 512), False), ((48, 80), True), ((200, 64), False), ((16, 24), True)])
@@ -256,6 +308,38 @@ def test_band_resident_pcg_matches_global_kernel(cuda_device, N, warm):
     # the partial sums of the reduction, which ill-conditioned small systems
     # (ratio 1000, hundreds of iterations for a few thousand unknowns) amplify
     assert abs(its[1] - its[2]) <= max(1, its[1] // 10), its
+
+
+@pytest.mark.parametrize("N,warm", [((512, 512), False), ((200, 64), True), ((700, 700), False)])
+def test_mixed_band_pcg_matches_mixed_global_kernel(cuda_device, N, warm):
+    """ppe_precision='mixed' on the band-resident kernel (FP32 vectors and
+    couplings in shared memory, FP64 x and inner products, FP64 residual
+    replacement through global memory) against the all-global FP32 kernel
+    with the same replacement rule: both reach the 1e-10 FP64 true residual
+    and the FP64 solution within 1e-6; their iteration counts agree within
+    the spread FP32 summation order gives.  700^2 fits the band in FP32 but
+    not in FP64."""
+    import ctypes as C
+    import torch
+    from twophaseflow_b200 import PPESolverFVMMatrixFree, UniformGrid, _lib
+    lib = _lib.load()
+    rho = torch.from_numpy(droplet_density(N, seed=31)).to(cuda_device)
+    rhs = torch.from_numpy(divergence_rhs(N, seed=32)).to(cuda_device)
+    p0 = torch.from_numpy(divergence_rhs(N, seed=33)).to(cuda_device) if warm else None
+    base = dict(pseudo_tol=1e-10, pseudo_maxiter=400000, ppe_iteration_method="cg", ppe_preconditioner="jacobi")
+    ref = PPESolverFVMMatrixFree(None, _Cfg(**base), UniformGrid(N)).solve(rhs, rho)
+    scale = float(torch.max(torch.abs(ref)))
+    its, reps = {}, {}
+    for kind in (1, 2):
+        s = PPESolverFVMMatrixFree(None, _Cfg(ppe_precision="mixed", **base), UniformGrid(N))
+        _lib.check(lib.tpf_ppe_set_cg_kernel(s._handle, C.c_int(kind)))
+        p = s.solve(rhs, rho, 0.0, p0)
+        d = s.last_diagnostics
+        its[kind], reps[kind] = d["ppe_low_order_cg_iterations"], d["ppe_low_order_cg_refinements"]
+        assert d["ppe_low_order_cg_relative_residual"] < 1e-10, (kind, d)
+        assert reps[kind] >= 1
+        assert float(torch.max(torch.abs(p - ref))) <= 1e-6 * scale, (kind, its)
+    assert 0.75 <= its[2] / its[1] <= 1.34, (its, reps)
 
 
 def test_band_resident_pcg_is_refused_where_it_does_not_apply(cuda_device):

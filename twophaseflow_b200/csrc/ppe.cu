@@ -803,22 +803,22 @@ __global__ void __launch_bounds__(kThreads, 1) cg1_batch_kernel(const __grid_con
   cg1_body<T, MIXED>(b.c[c], blockIdx.x - b.first[c], b.first[c + 1] - b.first[c]);
 }
 
-// ---- band-resident PCG (2-D, FP64) ---------------------------------------------------------
+// ---- band-resident PCG (2-D; FP64, or FP32 under FP64 residual replacement) ----------------
 //
-// The same Chronopoulos-Gear iteration as cg1_body (FP64, Jacobi or none),
-// for 2-D systems whose per-SM share fits in shared memory (513^2 on 148
-// SMs: ~1 780 nodes per SM).  CTA b owns the contiguous node range
-// [b ndof / G, (b+1) ndof / G) (balanced to one node; every range is at least
-// one row of W = n1 nodes long); its r, w, s (double-buffered), p, x, M^-1
-// and both face couplings stay in shared memory for the whole solve.  The
-// stencil reaches W nodes back and forward, which lie in the two adjacent
-// ranges: each CTA publishes its first and last W nodes' (r, w, s) before
-// the barrier (double-buffered by iteration parity; a slot is rewritten only
-// after its readers have arrived at the next barrier) and reads its
-// neighbours' after it.  Per iteration: u = M r once per node (sub-pass 1),
-// w = S u from shared memory (sub-pass 2), one grid-wide reduction; x is
-// written back once at the end, so the only global traffic of an iteration
-// is the halo and the reduction.
+// The same Chronopoulos-Gear iteration as cg1_body (Jacobi or none), for 2-D
+// systems whose per-SM share fits in shared memory (513^2 on 148 SMs:
+// ~1 780 nodes per SM in FP64, twice that in FP32).  CTA b owns the
+// contiguous node range [b ndof / G, (b+1) ndof / G) (balanced to one node;
+// every range is at least one row of W = n1 nodes long); its r, w, s
+// (double-buffered), p, x, M^-1 and both face couplings stay in shared memory
+// for the whole solve.  The stencil reaches W nodes back and forward, which
+// lie in the two adjacent ranges: each CTA publishes its first and last W
+// nodes' (r, w, s) before the barrier (double-buffered by iteration parity; a
+// slot is rewritten only after its readers have arrived at the next barrier)
+// and reads its neighbours' after it.  Per iteration: u = M r once per node
+// (sub-pass 1), w = S u from shared memory (sub-pass 2), one grid-wide
+// reduction; x is written back once at the end, so the only global traffic
+// of an iteration is the halo and the reduction.
 //
 // Layout: u is stored as [W nodes before the range | the range | W nodes
 // after it] and the couplings as [W nodes before | the range], so every
@@ -829,54 +829,83 @@ __global__ void __launch_bounds__(kThreads, 1) cg1_batch_kernel(const __grid_con
 // (zero outside the domain), so they add exact zeros, as the clamped form of
 // s_row does.  The pin node's u is stored as 0 (its column is zero); its own
 // u is recomputed where its row needs it.
+//
+// MIXED (T = float): the vectors, couplings and M^-1 are FP32, x and the
+// inner products FP64, and the residual is replaced by the FP64 b - S x
+// (couplings from the FP64 arrays in global memory, the neighbours' x edges
+// published through global memory) whenever ||r|| has fallen by
+// replace_drop since the last replacement and before accepting convergence,
+// followed by a CG restart -- the rule of cg1_body<float, true>.
 struct BandArgs {
   Grid3 g;
   const double* s0;      // couplings to the next row (axis 0), 0 on the last row
   const double* s1;      // couplings to the next column (axis 1), 0 on the last column
   const double* dinv;    // Jacobi 1/diag(S) (pin -> 1), or ones
+  const float* s0f;      // FP32 copies (MIXED)
+  const float* s1f;
+  const float* dinvf;
   const double* b;       // SPD-system rhs
   double* x;             // solution
   long long maxiter;
   double tol;
+  double replace_drop;   // MIXED: replace the residual when ||r|| fell by this factor
   int x_nonzero;
   int n_max;             // nodes of the largest range
-  double* pub;           // [2 parity][G][2 side: first / last W nodes][3 vec: r, w, s][W]
+  void* pub;             // [2 parity][G][2 side: first / last W nodes][3 vec: r, w, s][W] of T
   double* part;          // [2 slots][8][G]
   unsigned int* count;   // monotonic arrival counter
   int* err;
   SolveStatus* st;
 };
 
-// shared-memory doubles: 12 range arrays + 6 rows of halo (u 2, couplings 2, M^-1 2)
-inline size_t band_smem_bytes(int n_max, int n1) { return ((size_t)12 * n_max + 6 * (size_t)n1) * sizeof(double); }
+// shared-memory bytes: x (FP64) + 11 range arrays of T + 6 rows of halo of T
+// (u 2, couplings 2, M^-1 2)
+template <typename T>
+inline size_t band_smem_bytes(int n_max, int n1) {
+  return (size_t)n_max * sizeof(double) + ((size_t)11 * n_max + 6 * (size_t)n1) * sizeof(T);
+}
 
-__global__ void __launch_bounds__(kThreads, 1) cg1_band_kernel(BandArgs a) {
-  extern __shared__ __align__(16) double sm[];
+// The whole band-resident solve of one system by blocks [0, G) of a grid
+// (bid = this block's index): the full grid for a single solve, or one
+// case's share of a batched launch.
+template <typename T, bool MIXED>
+__device__ __forceinline__ void cg1_band_body(const BandArgs& a, const int bid, const int G) {
+  extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ double scratch[256];
   const Grid3& g = a.g;
-  const int G = gridDim.x, bid = blockIdx.x, t = threadIdx.x, T = blockDim.x;
+  const int t = threadIdx.x, NT = blockDim.x;
   const int W = g.n1, NM = a.n_max;
   const int base = (int)((long long)bid * g.ndof / G), end = (int)((long long)(bid + 1) * g.ndof / G);
   const int nown = end - base;
-  double* rb[2] = {sm, sm + NM};
-  double* wb[2] = {sm + 2 * NM, sm + 3 * NM};
-  double* sb[2] = {sm + 4 * NM, sm + 5 * NM};
-  double* P = sm + 6 * NM;
-  double* D = sm + 7 * NM;
-  double* X = sm + 8 * NM;
-  double* Ue = sm + 9 * NM;            // [W before | range | W after]  (NM + 2 W)
-  double* A0e = Ue + NM + 2 * W;       // [W before | range]            (NM + W)
-  double* A1e = A0e + NM + W;          // [W before | range]            (NM + W)
-  double* HD = A1e + NM + W;           // [2][W]: M^-1 of the nodes before / after the range
-  double* Ua = Ue + W + nown;          // u of the W nodes after the range
+  double* X = reinterpret_cast<double*>(smraw);
+  T* sm = reinterpret_cast<T*>(smraw + (size_t)NM * sizeof(double));
+  T* rb[2] = {sm, sm + NM};
+  T* wb[2] = {sm + 2 * NM, sm + 3 * NM};
+  T* sb[2] = {sm + 4 * NM, sm + 5 * NM};
+  T* P = sm + 6 * NM;
+  T* D = sm + 7 * NM;
+  T* Ue = sm + 8 * NM;            // [W before | range | W after]  (NM + 2 W)
+  T* A0e = Ue + NM + 2 * W;       // [W before | range]            (NM + W)
+  T* A1e = A0e + NM + W;          // [W before | range]            (NM + W)
+  T* HD = A1e + NM + W;           // [2][W]: M^-1 of the nodes before / after the range
+  T* Ua = Ue + W + nown;          // u of the W nodes after the range
+  const T* s0t;
+  const T* s1t;
+  const T* dit;
+  if constexpr (MIXED) {
+    s0t = a.s0f; s1t = a.s1f; dit = a.dinvf;
+  } else {
+    s0t = a.s0; s1t = a.s1; dit = a.dinv;
+  }
+  T* const pubv = static_cast<T*>(a.pub);
   const bool has_up = bid > 0, has_dn = bid < G - 1;
   GridSum gs{a.part, a.count, a.err, (unsigned int)G, 0u, (unsigned int)bid};
-  auto pub = [&](int par, int blk, int side, int vec) -> double* {
-    return a.pub + ((((size_t)par * G + blk) * 2 + side) * 3 + vec) * W;
+  auto pub = [&](int par, int blk, int side, int vec) -> T* {
+    return pubv + ((((size_t)par * G + blk) * 2 + side) * 3 + vec) * W;
   };
   // S-row of own node o on a field V stored in the extended layout
-  auto stencil = [&](const double* V, int o, double& d, double& off) {
-    const double sm0 = A0e[o], sp0 = A0e[o + W], sm1 = A1e[o + W - 1], sp1 = A1e[o + W];
+  auto stencil = [&](const T* V, int o, T& d, T& off) {
+    const T sm0 = A0e[o], sp0 = A0e[o + W], sm1 = A1e[o + W - 1], sp1 = A1e[o + W];
     d = (sm0 + sp0) + (sm1 + sp1);
     off = sm0 * V[o] + sp0 * V[o + 2 * W] + sm1 * V[o + W - 1] + sp1 * V[o + W + 1];
   };
@@ -886,122 +915,192 @@ __global__ void __launch_bounds__(kThreads, 1) cg1_band_kernel(BandArgs a) {
     const int q = hq(side, k);
     return (side == 0 ? has_up : has_dn) && q >= 0 && q < g.ndof;
   };
-  auto hslot = [&](int side, int k) -> double& { return side == 0 ? Ue[k] : Ua[k]; };
+  auto hslot = [&](int side, int k) -> T& { return side == 0 ? Ue[k] : Ua[k]; };
+  // FP64 (S x)_idx of own node o (MIXED): x of own nodes from shared memory,
+  // of the neighbour ranges' edges from global memory, couplings FP64 from
+  // global memory (0 on boundary faces; out-of-domain neighbours skipped)
+  auto sx64 = [&](int o) -> double {
+    const int idx = base + o;
+    if (idx == g.pin) return X[o];
+    auto xv = [&](int q) -> double {
+      if (q == g.pin) return 0.0;
+      const int oo = q - base;
+      return (oo >= 0 && oo < nown) ? X[oo] : __ldcg(a.x + q);
+    };
+    const double sm0 = idx >= W ? a.s0[idx - W] : 0.0, sp0 = a.s0[idx];
+    const double sm1 = idx >= 1 ? a.s1[idx - 1] : 0.0, sp1 = a.s1[idx];
+    const double d = (sm0 + sp0) + (sm1 + sp1);
+    const double off = (idx >= W ? sm0 * xv(idx - W) : 0.0) + (idx + W < g.ndof ? sp0 * xv(idx + W) : 0.0) +
+                       (idx >= 1 ? sm1 * xv(idx - 1) : 0.0) + (idx + 1 < g.ndof ? sp1 * xv(idx + 1) : 0.0);
+    return d * X[o] - off;
+  };
+  // u = M r, w = S u and the six inner products with p = s = 0, r in rb[c]
+  // and its halo published at parity c ^ 1; (r, w, s = 0) edges published at
+  // parity c
+  auto init_pass = [&](int c, double (&red)[6]) {
+    for (int k = t; k < 2 * W; k += NT) {
+      const int side = k / W, kk = k - side * W;
+      T u = T(0);
+      if (hlive(side, kk) && hq(side, kk) != g.pin)
+        u = HD[k] * __ldcg(pub(c ^ 1, side == 0 ? bid - 1 : bid + 1, side ^ 1, 0) + kk);
+      hslot(side, kk) = u;
+    }
+    for (int o = t; o < nown; o += NT) Ue[W + o] = (base + o == g.pin) ? T(0) : D[o] * rb[c][o];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 6; ++k) red[k] = 0.0;
+    for (int o = t; o < nown; o += NT) {
+      const int idx = base + o;
+      const T ri = rb[c][o];
+      T ui, wi;
+      if (idx == g.pin) {
+        ui = D[o] * ri;
+        wi = ui;
+      } else {
+        ui = Ue[W + o];
+        T d, off;
+        stencil(Ue, o, d, off);
+        wi = d * ui - off;
+      }
+      wb[c][o] = wi;
+      sb[c][o] = T(0);
+      P[o] = T(0);
+      red[0] += (double)ri * (double)ui;
+      red[1] += (double)wi * (double)ui;
+      red[5] += (double)ri * (double)ri;
+      if (o < W) { pub(c, bid, 0, 0)[o] = ri; pub(c, bid, 0, 1)[o] = wi; pub(c, bid, 0, 2)[o] = T(0); }
+      if (o >= nown - W) {
+        const int k = o - (nown - W);
+        pub(c, bid, 1, 0)[k] = ri; pub(c, bid, 1, 1)[k] = wi; pub(c, bid, 1, 2)[k] = T(0);
+      }
+    }
+  };
 
   // static data
-  for (int o = t; o < nown; o += T) {
-    D[o] = a.dinv[base + o];
-    A0e[W + o] = a.s0[base + o];
-    A1e[W + o] = a.s1[base + o];
+  for (int o = t; o < nown; o += NT) {
+    D[o] = dit[base + o];
+    A0e[W + o] = s0t[base + o];
+    A1e[W + o] = s1t[base + o];
     X[o] = a.x[base + o];
   }
-  for (int k = t; k < 2 * W; k += T) {
+  for (int k = t; k < 2 * W; k += NT) {
     const int side = k / W, kk = k - side * W;
     const bool live = hlive(side, kk);
-    HD[k] = live ? a.dinv[hq(side, kk)] : 0.0;
+    HD[k] = live ? dit[hq(side, kk)] : T(0);
     if (side == 0) {
-      A0e[kk] = live ? a.s0[hq(0, kk)] : 0.0;
-      A1e[kk] = live ? a.s1[hq(0, kk)] : 0.0;
+      A0e[kk] = live ? s0t[hq(0, kk)] : T(0);
+      A1e[kk] = live ? s1t[hq(0, kk)] : T(0);
     }
   }
   __syncthreads();
 
-  // r0 = b - S x (pin column zero / pin row identity): x, pin zeroed, staged in Ue
+  // r0 = b - S x (pin column zero / pin row identity); FP64: x, pin zeroed,
+  // staged in Ue; MIXED: sx64 over the initial x in global memory
   double red0[2] = {0.0, 0.0};
-  if (a.x_nonzero) {
-    for (int o = t; o < nown; o += T) Ue[W + o] = (base + o == g.pin) ? 0.0 : X[o];
-    for (int k = t; k < 2 * W; k += T) {
+  if (!MIXED && a.x_nonzero) {
+    for (int o = t; o < nown; o += NT) Ue[W + o] = (base + o == g.pin) ? T(0) : (T)X[o];
+    for (int k = t; k < 2 * W; k += NT) {
       const int side = k / W, kk = k - side * W;
       const int q = hq(side, kk);
-      hslot(side, kk) = (hlive(side, kk) && q != g.pin) ? a.x[q] : 0.0;
+      hslot(side, kk) = (hlive(side, kk) && q != g.pin) ? (T)a.x[q] : T(0);
     }
     __syncthreads();
   }
-  for (int o = t; o < nown; o += T) {
+  for (int o = t; o < nown; o += NT) {
     const int idx = base + o;
     const double bi = a.b[idx];
     double ri = bi;
     if (a.x_nonzero) {
       double sx;
-      if (idx == g.pin) {
-        sx = X[o];
+      if constexpr (MIXED) {
+        sx = sx64(o);
       } else {
-        double d, off;
-        stencil(Ue, o, d, off);
-        sx = d * X[o] - off;
+        if (idx == g.pin) {
+          sx = X[o];
+        } else {
+          T d, off;
+          stencil(Ue, o, d, off);
+          sx = d * X[o] - off;
+        }
       }
       ri = bi - sx;
     }
-    rb[0][o] = ri;
+    rb[0][o] = (T)ri;
     red0[0] += bi * bi;
     red0[1] += ri * ri;
-    if (o < W) pub(1, bid, 0, 0)[o] = ri;
-    if (o >= nown - W) pub(1, bid, 1, 0)[o - (nown - W)] = ri;
+    if (o < W) pub(1, bid, 0, 0)[o] = (T)ri;
+    if (o >= nown - W) pub(1, bid, 1, 0)[o - (nown - W)] = (T)ri;
   }
   if (!gs.sum<2>(red0, scratch)) return;
   const double bb = red0[0];
   if (bb == 0.0) {
-    for (int o = t; o < nown; o += T) a.x[base + o] = 0.0;
-    if (bid == 0 && t == 0) { a.st->iters = 0; a.st->applies = 0; a.st->rr = 0.0; a.st->bb = 0.0; a.st->converged = 1; }
+    for (int o = t; o < nown; o += NT) a.x[base + o] = 0.0;
+    if (bid == 0 && t == 0) {
+      a.st->iters = 0; a.st->applies = 0; a.st->refinements = 0; a.st->rr = 0.0; a.st->bb = 0.0;
+      a.st->converged = 1;
+    }
     return;
   }
   const double atol = a.tol * sqrt(bb);
   const double atol2 = atol * atol;
 
-  // u = M r, w = S u and the six inner products with p = s = 0
-  for (int k = t; k < 2 * W; k += T) {
-    const int side = k / W, kk = k - side * W;
-    double u = 0.0;
-    if (hlive(side, kk) && hq(side, kk) != g.pin)
-      u = HD[k] * __ldcg(pub(1, side == 0 ? bid - 1 : bid + 1, side ^ 1, 0) + kk);
-    hslot(side, kk) = u;
-  }
-  for (int o = t; o < nown; o += T) Ue[W + o] = (base + o == g.pin) ? 0.0 : D[o] * rb[0][o];
-  __syncthreads();
-  double red[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  for (int o = t; o < nown; o += T) {
-    const int idx = base + o;
-    const double ri = rb[0][o];
-    double ui, wi;
-    if (idx == g.pin) {
-      ui = D[o] * ri;
-      wi = ui;
-    } else {
-      ui = Ue[W + o];
-      double d, off;
-      stencil(Ue, o, d, off);
-      wi = d * ui - off;
-    }
-    wb[0][o] = wi;
-    sb[0][o] = 0.0;
-    P[o] = 0.0;
-    red[0] += ri * ui;
-    red[1] += wi * ui;
-    red[5] += ri * ri;
-    if (o < W) { pub(0, bid, 0, 0)[o] = ri; pub(0, bid, 0, 1)[o] = wi; pub(0, bid, 0, 2)[o] = 0.0; }
-    if (o >= nown - W) {
-      const int k = o - (nown - W);
-      pub(0, bid, 1, 0)[k] = ri; pub(0, bid, 1, 1)[k] = wi; pub(0, bid, 1, 2)[k] = 0.0;
-    }
-  }
+  double red[6];
+  init_pass(0, red);
   bool ok = gs.sum<6>(red, scratch);
   double gamma = red[0], rr = red[5];
   double beta = 0.0, denom = red[1];
-  long long it = 0, applies = a.x_nonzero ? 2 : 1;
+  double rr_ref = rr;    // ||r||^2 at the last FP64 residual replacement (MIXED)
+  long long it = 0, replacements = 0, applies = a.x_nonzero ? 2 : 1;
   bool conv = false;
   int cur = 0;
   constexpr int KH = 3;   // halo entries per thread: 2 * W <= KH * kThreads
   while (ok) {
-    if (rr < atol2) { conv = true; break; }
-    if (it >= a.maxiter) break;
-    const double alpha = gamma / denom, bt = beta;
+    if constexpr (MIXED) {
+      const bool small = rr < atol2;
+      if (!small && it >= a.maxiter) break;
+      if (small || rr < a.replace_drop * a.replace_drop * rr_ref) {
+        // publish the x edges, barrier, r = b - S x in FP64 (halo r at
+        // parity cur ^ 1), barrier with ||r||^2, then a CG restart
+        for (int o = t; o < nown; o += NT)
+          if (o < W || o >= nown - W) a.x[base + o] = X[o];
+        double bar1[1] = {0.0};
+        if (!(ok = gs.sum<1>(bar1, scratch))) break;
+        double rt[1] = {0.0};
+        for (int o = t; o < nown; o += NT) {
+          const double ri = a.b[base + o] - sx64(o);
+          rb[cur][o] = (T)ri;
+          rt[0] += ri * ri;
+          if (o < W) pub(cur ^ 1, bid, 0, 0)[o] = (T)ri;
+          if (o >= nown - W) pub(cur ^ 1, bid, 1, 0)[o - (nown - W)] = (T)ri;
+        }
+        ++replacements;
+        ++applies;
+        if (!(ok = gs.sum<1>(rt, scratch))) break;
+        if (rt[0] < atol2) { rr = rt[0]; conv = true; break; }
+        if (it >= a.maxiter) { rr = rt[0]; break; }
+        init_pass(cur, red);
+        ++applies;
+        if (!(ok = gs.sum<6>(red, scratch))) break;
+        beta = 0.0;
+        denom = red[1];
+        gamma = red[0];
+        rr = red[5];
+        rr_ref = rr;
+        continue;
+      }
+    } else {
+      if (rr < atol2) { conv = true; break; }
+      if (it >= a.maxiter) break;
+    }
+    const double alpha_d = gamma / denom;
+    const T alpha = (T)alpha_d, bt = (T)beta;
     const int nxt = cur ^ 1;
     // halo (r, w, s) of the neighbour ranges: loads in flight during sub-pass 1
-    double hr[KH], hw[KH], hs[KH];
+    T hr[KH], hw[KH], hs[KH];
 #pragma unroll
     for (int e = 0; e < KH; ++e) {
-      const int k = t + e * T;
-      hr[e] = hw[e] = hs[e] = 0.0;
+      const int k = t + e * NT;
+      hr[e] = hw[e] = hs[e] = T(0);
       if (k < 2 * W) {
         const int side = k / W, kk = k - side * W;
         if (hlive(side, kk)) {
@@ -1013,56 +1112,56 @@ __global__ void __launch_bounds__(kThreads, 1) cg1_band_kernel(BandArgs a) {
       }
     }
     // sub-pass 1: p, x, r, s and u = M r_new for own nodes
-    const double* __restrict__ rc = rb[cur];
-    const double* __restrict__ wc = wb[cur];
-    const double* __restrict__ sc = sb[cur];
-    double* __restrict__ rn_o = rb[nxt];
-    double* __restrict__ sn_o = sb[nxt];
-    for (int o = t; o < nown; o += T) {
-      const double ri = rc[o];
-      const double ui = D[o] * ri;
-      const double si = wc[o] + bt * sc[o];
-      const double pi = ui + bt * P[o];
+    const T* __restrict__ rc = rb[cur];
+    const T* __restrict__ wc = wb[cur];
+    const T* __restrict__ sc = sb[cur];
+    T* __restrict__ rn_o = rb[nxt];
+    T* __restrict__ sn_o = sb[nxt];
+    for (int o = t; o < nown; o += NT) {
+      const T ri = rc[o];
+      const T ui = D[o] * ri;
+      const T si = wc[o] + bt * sc[o];
+      const T pi = ui + bt * P[o];
       P[o] = pi;
-      X[o] += alpha * pi;
-      const double rn = ri - alpha * si;
+      X[o] += alpha_d * (double)pi;
+      const T rn = ri - alpha * si;
       rn_o[o] = rn;
       sn_o[o] = si;
-      Ue[W + o] = (base + o == g.pin) ? 0.0 : D[o] * rn;
+      Ue[W + o] = (base + o == g.pin) ? T(0) : D[o] * rn;
     }
 #pragma unroll
     for (int e = 0; e < KH; ++e) {
-      const int k = t + e * T;
+      const int k = t + e * NT;
       if (k < 2 * W) {
         const int side = k / W, kk = k - side * W;
         hslot(side, kk) =
-            (!hlive(side, kk) || hq(side, kk) == g.pin) ? 0.0 : HD[k] * (hr[e] - alpha * (hw[e] + bt * hs[e]));
+            (!hlive(side, kk) || hq(side, kk) == g.pin) ? T(0) : HD[k] * (hr[e] - alpha * (hw[e] + bt * hs[e]));
       }
     }
     __syncthreads();
     // sub-pass 2: w = S u, the six inner products, publication of the edges
 #pragma unroll
     for (int k = 0; k < 6; ++k) red[k] = 0.0;
-    double* __restrict__ wn_o = wb[nxt];
-    for (int o = t; o < nown; o += T) {
-      const double rn = rn_o[o], si = sn_o[o], pi = P[o];
-      double un, wn;
+    T* __restrict__ wn_o = wb[nxt];
+    for (int o = t; o < nown; o += NT) {
+      const T rn = rn_o[o], si = sn_o[o], pi = P[o];
+      T un, wn;
       if (base + o == g.pin) {
         un = D[o] * rn;
         wn = un;
       } else {
         un = Ue[W + o];
-        double d, off;
+        T d, off;
         stencil(Ue, o, d, off);
         wn = d * un - off;
       }
       wn_o[o] = wn;
-      red[0] += rn * un;
-      red[1] += wn * un;
-      red[2] += un * si;
-      red[3] += pi * wn;
-      red[4] += pi * si;
-      red[5] += rn * rn;
+      red[0] += (double)rn * (double)un;
+      red[1] += (double)wn * (double)un;
+      red[2] += (double)un * (double)si;
+      red[3] += (double)pi * (double)wn;
+      red[4] += (double)pi * (double)si;
+      red[5] += (double)rn * (double)rn;
       if (o < W) { pub(nxt, bid, 0, 0)[o] = rn; pub(nxt, bid, 0, 1)[o] = wn; pub(nxt, bid, 0, 2)[o] = si; }
       if (o >= nown - W) {
         const int k = o - (nown - W);
@@ -1079,15 +1178,36 @@ __global__ void __launch_bounds__(kThreads, 1) cg1_band_kernel(BandArgs a) {
     ++it;
     ++applies;
   }
-  for (int o = t; o < nown; o += T) a.x[base + o] = X[o];
+  for (int o = t; o < nown; o += NT) a.x[base + o] = X[o];
   if (bid == 0 && t == 0) {
     a.st->iters = it;
     a.st->applies = applies;
-    a.st->refinements = 0;
+    a.st->refinements = replacements;
     a.st->rr = rr;
     a.st->bb = bb;
     a.st->converged = conv ? 1 : 0;
   }
+}
+
+template <typename T, bool MIXED>
+__global__ void __launch_bounds__(kThreads, 1) cg1_band_kernel(BandArgs a) {
+  cg1_band_body<T, MIXED>(a, blockIdx.x, gridDim.x);
+}
+
+// Many independent 2-D systems in one cooperative launch, each band-resident
+// in the shared memory of its own blocks: case c owns blocks [first[c],
+// first[c + 1]) with its own barrier counter, halo buffer and status.
+struct BandBatch {
+  BandArgs c[kBatchMax];
+  int first[kBatchMax + 1];
+  int n;
+};
+
+template <typename T, bool MIXED>
+__global__ void __launch_bounds__(kThreads, 1) cg1_band_batch_kernel(const __grid_constant__ BandBatch b) {
+  int c = 0;
+  while (c + 1 < b.n && (int)blockIdx.x >= b.first[c + 1]) ++c;
+  cg1_band_body<T, MIXED>(b.c[c], blockIdx.x - b.first[c], b.first[c + 1] - b.first[c]);
 }
 
 }  // namespace
@@ -1673,12 +1793,14 @@ int solve_gmres(tpf_ppe* h, const double* rhs, double* p, const double* p_init, 
 
 // band-resident PCG: applicable to 2-D systems whose largest node range
 // (one per CTA, at least one row long) fits in the opt-in shared memory of
-// one SM with 12 vectors and 6 halo rows
+// one SM with 12 vectors and 6 halo rows (11 vectors and the halo in FP32
+// for the mixed mode)
 struct BandPlan {
   int grid, n_max;
   size_t smem;
+  bool mixed;
 };
-bool band_plan(const tpf_ppe* h, BandPlan& bp) {
+bool band_plan(const tpf_ppe* h, BandPlan& bp, bool mixed) {
   if (h->cg_kernel == 1) return false;
   const Grid3& g = h->g;
   if (h->ndim != 2 || g.N2 != 0) return false;
@@ -1686,7 +1808,7 @@ bool band_plan(const tpf_ppe* h, BandPlan& bp) {
   const int grid = std::min(h->coop_blocks, g.ndof / g.n1);
   if (grid < 1) return false;
   const int n_max = (g.ndof + grid - 1) / grid;
-  const size_t smem = band_smem_bytes(n_max, g.n1);
+  const size_t smem = mixed ? band_smem_bytes<float>(n_max, g.n1) : band_smem_bytes<double>(n_max, g.n1);
   int dev = 0, optin = 0;
   cudaGetDevice(&dev);
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {
@@ -1698,30 +1820,42 @@ bool band_plan(const tpf_ppe* h, BandPlan& bp) {
   bp.grid = grid;
   bp.n_max = n_max;
   bp.smem = smem;
+  bp.mixed = mixed;
   return true;
 }
 
-int launch_band(tpf_ppe* h, const BandPlan& bp, const Cg1Args& c, cudaStream_t s) {
-  const size_t need = (size_t)2 * bp.grid * 2 * 3 * h->g.n1;
+// halo buffer of a band-resident solve over `grid` blocks: [2][grid][2][3][n1]
+int ensure_band_pub(tpf_ppe* h, int grid) {
+  const size_t need = (size_t)2 * grid * 2 * 3 * h->g.n1;
   if (h->band_pub_len < need) {
     int st = dalloc(h, &h->band_pub, need);
     if (st) return st;
     h->band_pub_len = need;
   }
-  static size_t smem_set = 0;
-  if (bp.smem > smem_set) {
-    TPF_CUDA_TRY(cudaFuncSetAttribute(cg1_band_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bp.smem));
-    smem_set = bp.smem;
+  return TPF_OK;
+}
+
+int launch_band(tpf_ppe* h, const BandPlan& bp, const Cg1Args& c, cudaStream_t s) {
+  if (int st = ensure_band_pub(h, bp.grid)) return st;
+  static size_t smem_set[2] = {0, 0};
+  void* fn = bp.mixed ? (void*)cg1_band_kernel<float, true> : (void*)cg1_band_kernel<double, false>;
+  if (bp.smem > smem_set[bp.mixed]) {
+    TPF_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bp.smem));
+    smem_set[bp.mixed] = bp.smem;
   }
   BandArgs a{};
   a.g = c.g;
-  a.s0 = c.v64.s0;
-  a.s1 = c.v64.s1;
+  a.s0 = c.s64[0];
+  a.s1 = c.s64[1];
   a.dinv = c.v64.dinv;
+  a.s0f = c.v32.s0;
+  a.s1f = c.v32.s1;
+  a.dinvf = c.v32.dinv;
   a.b = c.b;
   a.x = c.x;
   a.maxiter = c.maxiter;
   a.tol = c.tol;
+  a.replace_drop = c.replace_drop;
   a.x_nonzero = c.x_nonzero;
   a.n_max = bp.n_max;
   a.pub = h->band_pub;
@@ -1730,7 +1864,7 @@ int launch_band(tpf_ppe* h, const BandPlan& bp, const Cg1Args& c, cudaStream_t s
   a.err = c.err;
   a.st = c.st;
   void* args[] = {&a};
-  TPF_CUDA_TRY(cudaLaunchCooperativeKernel((void*)cg1_band_kernel, dim3(bp.grid), dim3(kThreads), args, bp.smem, s));
+  TPF_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(bp.grid), dim3(kThreads), args, bp.smem, s));
   return TPF_OK;
 }
 
@@ -1916,7 +2050,7 @@ int solve_cg(tpf_ppe* h, const double* rhs, double* p, const double* p_init, cud
   a.st = h->st;
   const bool mixed = (h->o.precision == TPF_PREC_MIXED);
   BandPlan bp;
-  const bool band = !mixed && band_plan(h, bp);
+  const bool band = band_plan(h, bp, mixed);
   if (!mixed && (h->cg_kernel == 3 || (h->cg_kernel == 0 && !band)))
     return solve_cg_stream(h, rhs, p, p_init, s, res);
   a.maxiter = h->o.maxiter;
@@ -1926,7 +2060,7 @@ int solve_cg(tpf_ppe* h, const double* rhs, double* p, const double* p_init, cud
     if (st) return st;
   } else {
     if (h->cg_kernel == 2) {
-      tpf::set_error("the band-resident PCG needs a 2-D FP64 system whose per-SM band fits in shared memory");
+      tpf::set_error("the band-resident PCG needs a 2-D system whose per-SM band fits in shared memory");
       return TPF_EINVAL;
     }
     void* args[] = {&a};
@@ -2253,6 +2387,119 @@ int tpf_ppe_read_result(tpf_ppe* h, void* stream, tpf_ppe_result* result) {
   return TPF_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Band-resident batch: every system 2-D and the bands of all of them resident
+// at once, one block per SM.  Each system gets at least the fewest blocks
+// whose largest range fits in a block's shared memory and at most one block
+// per grid row (or its single-solve grid); the blocks are shared in
+// proportion to the expected work, nodes x iterations ~ ndof^1.5, and trimmed
+// to the SM count.
+bool band_batch_plan(tpf_ppe* const* hs, int n, bool mixed, std::vector<int>& nb, std::vector<int>& nmax,
+                     size_t& smem) {
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  const size_t lim = (size_t)optin - 4096;
+  auto bytes = [&](int nm, int n1) {
+    return mixed ? band_smem_bytes<float>(nm, n1) : band_smem_bytes<double>(nm, n1);
+  };
+  const int cap = tpf::sm_count();
+  std::vector<int> lo(n), hi(n);
+  double wsum = 0.0;
+  int sum_lo = 0;
+  for (int c = 0; c < n; ++c) {
+    const tpf_ppe* h = hs[c];
+    const Grid3& g = h->g;
+    if (h->cg_kernel == 1 || h->cg_kernel == 3 || h->ndim != 2 || g.N2 != 0 || 2 * g.n1 > 3 * kThreads)
+      return false;
+    hi[c] = std::min(h->coop_blocks, g.ndof / g.n1);
+    int k = 1;
+    while (k <= hi[c] && bytes((g.ndof + k - 1) / k, g.n1) > lim) ++k;
+    if (k > hi[c]) return false;
+    lo[c] = k;
+    sum_lo += k;
+    wsum += std::pow((double)g.ndof, 1.5);
+  }
+  if (sum_lo > cap) return false;
+  int used = 0;
+  for (int c = 0; c < n; ++c) {
+    const int share = (int)((double)cap * std::pow((double)hs[c]->g.ndof, 1.5) / wsum);
+    nb[c] = std::max(lo[c], std::min(hi[c], share));
+    used += nb[c];
+  }
+  while (used > cap) {   // trim the largest shares above their minimum
+    int m = -1;
+    for (int c = 0; c < n; ++c)
+      if (nb[c] > lo[c] && (m < 0 || nb[c] > nb[m])) m = c;
+    --nb[m];
+    --used;
+  }
+  smem = 0;
+  for (int c = 0; c < n; ++c) {
+    nmax[c] = (hs[c]->g.ndof + nb[c] - 1) / nb[c];
+    smem = std::max(smem, bytes(nmax[c], hs[c]->g.n1));
+  }
+  return true;
+}
+
+int launch_band_batch(tpf_ppe* const* hs, int n, const double* const* rhs, bool mixed, const std::vector<int>& nb,
+                      const std::vector<int>& nmax, size_t smem, cudaStream_t s) {
+  auto* b = new BandBatch();
+  b->n = n;
+  b->first[0] = 0;
+  for (int c = 0; c < n; ++c) {
+    tpf_ppe* h = hs[c];
+    if (int st = ensure_band_pub(h, nb[c])) { delete b; return st; }
+    const Geo geo{{h->dv[0], h->dv[1], h->dv[2]}, {h->dface[0], h->dface[1], h->dface[2]}};
+    cg_rhs_kernel<<<ew_grid(h), 256, 0, s>>>(h->g, geo, rhs[c], h->b, nullptr, h->x);
+    cudaMemsetAsync(h->bar, 0, 2 * sizeof(unsigned int), s);
+    cudaMemsetAsync(h->err, 0, sizeof(int), s);
+    cudaMemsetAsync(h->st, 0, sizeof(SolveStatus), s);
+    const bool none = (h->o.precond == TPF_PRECOND_NONE);
+    BandArgs& a = b->c[c];
+    a = BandArgs{};
+    a.g = h->g;
+    a.s0 = h->s[0];
+    a.s1 = h->s[1];
+    a.dinv = none ? h->ones64 : h->dinvS;
+    a.s0f = h->s32[0];
+    a.s1f = h->s32[1];
+    a.dinvf = none ? h->ones32 : h->dinvS32;
+    a.b = h->b;
+    a.x = h->x;
+    a.maxiter = h->o.maxiter;
+    a.tol = h->o.tol;
+    a.replace_drop = h->o.inner_tol > 0.0 ? h->o.inner_tol : 1e-3;
+    a.x_nonzero = 0;
+    a.n_max = nmax[c];
+    a.pub = h->band_pub;
+    a.part = h->part;
+    a.count = h->bar;
+    a.err = h->err;
+    a.st = h->st;
+    b->first[c + 1] = b->first[c] + nb[c];
+  }
+  void* fn = mixed ? (void*)cg1_band_batch_kernel<float, true> : (void*)cg1_band_batch_kernel<double, false>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) {
+    void* args[] = {b};
+    e = cudaLaunchCooperativeKernel(fn, dim3(b->first[n]), dim3(kThreads), args, smem, s);
+  }
+  delete b;
+  TPF_CUDA_TRY(e);
+  return TPF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int tpf_ppe_solve_batched(tpf_ppe* const* hs, int n, const double* const* rhs, const double* const* rho,
                           double* const* p, void* stream, tpf_ppe_result* results) {
   TPF_CHECK_ARG(hs && rhs && p && n >= 1, "NULL argument or empty batch");
@@ -2268,71 +2515,84 @@ int tpf_ppe_solve_batched(tpf_ppe* const* hs, int n, const double* const* rhs, c
     if (rho && rho[c] && (st = tpf_ppe_prepare(h, rho[c], stream))) return st;
     TPF_CHECK_ARG(h->prepared, "operator coefficients of system %d are not initialised", c);
   }
-  double wsum = 0.0;
-  for (int c = 0; c < n; ++c) wsum += std::pow((double)hs[c]->g.ndof, 1.5);
-  // blocks: one per SM (the kernel's occupancy), shared in proportion to the
-  // expected work, nodes x iterations ~ ndof^1.5 (Jacobi-PCG iteration counts
-  // grow like the grid's linear size)
-  void* fn = mixed ? (void*)cg1_batch_kernel<float, true> : (void*)cg1_batch_kernel<double, false>;
-  int per_sm = 0;
-  TPF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, 0));
-  const int cap = tpf::sm_count() * std::max(1, per_sm);
-  TPF_CHECK_ARG(n <= cap, "batch of %d systems exceeds the %d co-resident blocks", n, cap);
-  std::vector<int> nb(n);
-  int used = 0;
-  for (int c = 0; c < n; ++c) {
-    const double share = (double)cap * std::pow((double)hs[c]->g.ndof, 1.5) / wsum;
-    nb[c] = std::max(1, std::min(hs[c]->coop_blocks, (int)share));
-    used += nb[c];
-  }
-  while (used > cap) {   // trim the largest shares
-    int m = 0;
-    for (int c = 1; c < n; ++c)
-      if (nb[c] > nb[m]) m = c;
-    --nb[m];
-    --used;
-  }
-  auto* b = new Cg1Batch();
-  b->n = n;
-  b->first[0] = 0;
-  for (int c = 0; c < n; ++c) {
-    tpf_ppe* h = hs[c];
-    const Geo geo{{h->dv[0], h->dv[1], h->dv[2]}, {h->dface[0], h->dface[1], h->dface[2]}};
-    cg_rhs_kernel<<<ew_grid(h), 256, 0, s>>>(h->g, geo, rhs[c], h->b, nullptr, h->x);
-    TPF_CUDA_TRY(cudaMemsetAsync(h->bar, 0, 2 * sizeof(unsigned int), s));
-    TPF_CUDA_TRY(cudaMemsetAsync(h->err, 0, sizeof(int), s));
-    TPF_CUDA_TRY(cudaMemsetAsync(h->st, 0, sizeof(SolveStatus), s));
-    Cg1Args& a = b->c[c];
-    a = Cg1Args{};
-    a.g = h->g;
-    const bool none = (h->o.precond == TPF_PRECOND_NONE);
-    a.v64.s0 = h->s[0]; a.v64.s1 = h->s[1]; a.v64.s2 = h->s[2];
-    a.v64.dinv = none ? h->ones64 : h->dinvS;
-    a.v32.s0 = h->s32[0]; a.v32.s1 = h->s32[1]; a.v32.s2 = h->s32[2];
-    a.v32.dinv = none ? h->ones32 : h->dinvS32;
-    for (int k = 0; k < 2; ++k) {
-      a.v64.r[k] = h->c64[k]; a.v64.w[k] = h->c64[2 + k]; a.v64.s[k] = h->c64[4 + k];
-      a.v32.r[k] = h->c32[k]; a.v32.w[k] = h->c32[2 + k]; a.v32.s[k] = h->c32[4 + k];
+  // the band-resident batch where every band fits at once, else the
+  // all-global persistent body
+  std::vector<int> bnb(n), bnmax(n);
+  size_t bsmem = 0;
+  bool force_band = false;
+  for (int c = 0; c < n; ++c) force_band = force_band || hs[c]->cg_kernel == 2;
+  if (band_batch_plan(hs, n, mixed, bnb, bnmax, bsmem)) {
+    if ((st = launch_band_batch(hs, n, rhs, mixed, bnb, bnmax, bsmem, s))) return st;
+  } else if (force_band) {
+    tpf::set_error("the band-resident batch needs 2-D systems whose bands all fit in shared memory at once");
+    return TPF_EINVAL;
+  } else {
+    double wsum = 0.0;
+    for (int c = 0; c < n; ++c) wsum += std::pow((double)hs[c]->g.ndof, 1.5);
+    // blocks: one per SM (the kernel's occupancy), shared in proportion to the
+    // expected work, nodes x iterations ~ ndof^1.5 (Jacobi-PCG iteration counts
+    // grow like the grid's linear size)
+    void* fn = mixed ? (void*)cg1_batch_kernel<float, true> : (void*)cg1_batch_kernel<double, false>;
+    int per_sm = 0;
+    TPF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, 0));
+    const int cap = tpf::sm_count() * std::max(1, per_sm);
+    TPF_CHECK_ARG(n <= cap, "batch of %d systems exceeds the %d co-resident blocks", n, cap);
+    std::vector<int> nb(n);
+    int used = 0;
+    for (int c = 0; c < n; ++c) {
+      const double share = (double)cap * std::pow((double)hs[c]->g.ndof, 1.5) / wsum;
+      nb[c] = std::max(1, std::min(hs[c]->coop_blocks, (int)share));
+      used += nb[c];
     }
-    a.v64.p = h->c64[6];
-    a.v32.p = h->c32[6];
-    a.s64[0] = h->s[0]; a.s64[1] = h->s[1]; a.s64[2] = h->s[2];
-    a.b = h->b;
-    a.x = h->x;
-    a.tol = h->o.tol;
-    a.x_nonzero = 0;
-    a.part = h->part;
-    a.count = h->bar;
-    a.err = h->err;
-    a.st = h->st;
-    a.maxiter = h->o.maxiter;
-    a.replace_drop = h->o.inner_tol > 0.0 ? h->o.inner_tol : 1e-3;
-    b->first[c + 1] = b->first[c] + nb[c];
+    while (used > cap) {   // trim the largest shares
+      int m = 0;
+      for (int c = 1; c < n; ++c)
+        if (nb[c] > nb[m]) m = c;
+      --nb[m];
+      --used;
+    }
+    auto* b = new Cg1Batch();
+    b->n = n;
+    b->first[0] = 0;
+    for (int c = 0; c < n; ++c) {
+      tpf_ppe* h = hs[c];
+      const Geo geo{{h->dv[0], h->dv[1], h->dv[2]}, {h->dface[0], h->dface[1], h->dface[2]}};
+      cg_rhs_kernel<<<ew_grid(h), 256, 0, s>>>(h->g, geo, rhs[c], h->b, nullptr, h->x);
+      TPF_CUDA_TRY(cudaMemsetAsync(h->bar, 0, 2 * sizeof(unsigned int), s));
+      TPF_CUDA_TRY(cudaMemsetAsync(h->err, 0, sizeof(int), s));
+      TPF_CUDA_TRY(cudaMemsetAsync(h->st, 0, sizeof(SolveStatus), s));
+      Cg1Args& a = b->c[c];
+      a = Cg1Args{};
+      a.g = h->g;
+      const bool none = (h->o.precond == TPF_PRECOND_NONE);
+      a.v64.s0 = h->s[0]; a.v64.s1 = h->s[1]; a.v64.s2 = h->s[2];
+      a.v64.dinv = none ? h->ones64 : h->dinvS;
+      a.v32.s0 = h->s32[0]; a.v32.s1 = h->s32[1]; a.v32.s2 = h->s32[2];
+      a.v32.dinv = none ? h->ones32 : h->dinvS32;
+      for (int k = 0; k < 2; ++k) {
+        a.v64.r[k] = h->c64[k]; a.v64.w[k] = h->c64[2 + k]; a.v64.s[k] = h->c64[4 + k];
+        a.v32.r[k] = h->c32[k]; a.v32.w[k] = h->c32[2 + k]; a.v32.s[k] = h->c32[4 + k];
+      }
+      a.v64.p = h->c64[6];
+      a.v32.p = h->c32[6];
+      a.s64[0] = h->s[0]; a.s64[1] = h->s[1]; a.s64[2] = h->s[2];
+      a.b = h->b;
+      a.x = h->x;
+      a.tol = h->o.tol;
+      a.x_nonzero = 0;
+      a.part = h->part;
+      a.count = h->bar;
+      a.err = h->err;
+      a.st = h->st;
+      a.maxiter = h->o.maxiter;
+      a.replace_drop = h->o.inner_tol > 0.0 ? h->o.inner_tol : 1e-3;
+      b->first[c + 1] = b->first[c] + nb[c];
+    }
+    void* args[] = {b};
+    cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(b->first[n]), dim3(kThreads), args, 0, s);
+    delete b;
+    TPF_CUDA_TRY(e);
   }
-  void* args[] = {b};
-  cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(b->first[n]), dim3(kThreads), args, 0, s);
-  delete b;
-  TPF_CUDA_TRY(e);
   std::vector<SolveStatus> hst(n);
   std::vector<int> herr(n);
   for (int c = 0; c < n; ++c) {

@@ -497,7 +497,9 @@ def learned_case(N, reps, maxiter=None, tol=1e-8):
 def batched_case(n_cases=32, nmin=128, nmax=512, reps=3, seed=0, tol=1e-8):
     """``n_cases`` independent 2-D droplet PPEs with seeded uneven grids
     (N_x, N_y uniform in [nmin, nmax]) solved in ONE persistent launch
-    (solve_batched) against one solve after the other with the same kernels."""
+    (solve_batched) against one solve after the other (each on the whole
+    GPU, band-resident where it fits).  The batch is band-resident when the
+    bands of all cases fit in shared memory at once, else all-global."""
     import numpy as np
     import torch
     from . import PPESolverFVMMatrixFree, UniformGrid, solve_batched
