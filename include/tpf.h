@@ -50,6 +50,22 @@ int tpf_version(void);
 /* Message of the last failing call on this host thread ("" if none). */
 const char* tpf_last_error(void);
 
+/* Launch-shape autotuning of the stencil kernels whose results do not
+ * depend on the launch shape (no counterpart in the reference): the CLS flux
+ * divergence and Rhie-Chow march kernels (nodes per thread along the axis)
+ * and the reinitialization's Crank-Nicolson line solves on the strided axes
+ * (threads per block).  The first call of a signature (kernel, shape, dtype)
+ * outside stream capture times every candidate on scratch memory and keeps
+ * the fastest for the process; results are bit-for-bit those of any other
+ * shape.  mode 1 (default) tunes; 0 switches tuning off and forgets the
+ * choices (the heuristic shapes are then used); 2 + k makes every tuned
+ * kernel take its candidate k (clamped to its last one) without timing, to
+ * check that every shape gives the same bits.  The CCD plans carry their own
+ * autotuner (tpf_ccd_plan_set_autotune). */
+int tpf_set_launch_autotune(int mode);
+/* Number of signatures tuned so far in this process. */
+int tpf_launch_autotune_entries(void);
+
 /* ------------------------------------------------------------------------ */
 /* CCD operator                                                              */
 /* ------------------------------------------------------------------------ */

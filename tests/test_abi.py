@@ -44,6 +44,10 @@ def test_python_binding_covers_header():
 def test_host_only_calls_without_gpu():
     lib = _lib.load()
     assert lib.tpf_version() >= 10000
+    # the launch autotuner's switch and counter need no device
+    assert lib.tpf_launch_autotune_entries() >= 0
+    assert lib.tpf_set_launch_autotune(1) == _lib.TPF_OK
+    assert lib.tpf_set_launch_autotune(-1) == _lib.TPF_EINVAL
     o = _lib.tpf_ppe_options()
     lib.tpf_ppe_default_options(ctypes.byref(o))
     # reference defaults (fvm_matrixfree.py:90-127)

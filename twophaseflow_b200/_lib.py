@@ -89,6 +89,8 @@ class tpf_lppe_result(C.Structure):
 SIGNATURES = {
     "tpf_version": (C.c_int, []),
     "tpf_last_error": (C.c_char_p, []),
+    "tpf_set_launch_autotune": (C.c_int, [C.c_int]),
+    "tpf_launch_autotune_entries": (C.c_int, []),
     "tpf_ccd_plan_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int64, C.c_double, C.c_int, C.c_int]),
     "tpf_ccd_plan_destroy": (C.c_int, [C.c_void_p]),
     "tpf_ccd_plan_set_autotune": (C.c_int, [C.c_void_p, C.c_int]),

@@ -254,12 +254,25 @@ extern "C" int tpf_fccd_flux_divergence_axis(int ndim, const int64_t* shape, int
   const int64_t tot = a.outer * a.n * a.inner;
   if (a.inner >= 32) {
     const int64_t lines = a.outer * a.inner, sms = tpf::sm_count();
+    // nodes per thread along the axis: autotuned among kChunks (the march
+    // gives the same values for every chunk length), else enough threads to
+    // fill the GPU (about 2048 per SM), 8..64 nodes
     int64_t chunk = (lines * a.n) / (sms * 2048);
     chunk = std::max<int64_t>(8, std::min<int64_t>(64, chunk));
-    const int64_t nchunks = (a.n + chunk - 1) / chunk;
-    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((lines * nchunks + 255) / 256, sms * 8));
-    if (dtype == TPF_F64) flux_march_kernel<double><<<blocks, 256, 0, st>>>(a, chunk, nchunks);
-    else flux_march_kernel<float><<<blocks, 256, 0, st>>>(a, chunk, nchunks);
+    static constexpr int64_t kChunks[5] = {8, 16, 32, 64, 128};
+    auto launch = [&](int64_t ck, void* out, cudaStream_t s2) -> int {
+      FluxArgs b = a;
+      b.acc = out;
+      const int64_t nchunks = (a.n + ck - 1) / ck;
+      const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((lines * nchunks + 255) / 256, sms * 8));
+      if (dtype == TPF_F64) flux_march_kernel<double><<<blocks, 256, 0, s2>>>(b, ck, nchunks);
+      else flux_march_kernel<float><<<blocks, 256, 0, s2>>>(b, ck, nchunks);
+      return cudaPeekAtLastError() == cudaSuccess ? TPF_OK : TPF_ECUDA;
+    };
+    auto cand = [&](int c, void* scratch, cudaStream_t s2) { return launch(kChunks[c], scratch, s2); };
+    const tpf::TuneKey key{tpf::kTuneFluxMarch, dtype, {a.outer, a.n, a.inner, 2 * a.periodic + a.accumulate}};
+    const int pick = tpf::tuned_choice(key, 5, -1, (size_t)tot * (dtype == TPF_F64 ? 8 : 4), st, cand);
+    launch(pick >= 0 ? kChunks[pick] : chunk, a.acc, st);
   } else {
     if (dtype == TPF_F64) flux_div_kernel<double><<<blocks_for(tot, 16), 256, 0, st>>>(a);
     else flux_div_kernel<float><<<blocks_for(tot, 16), 256, 0, st>>>(a);
@@ -448,6 +461,96 @@ __global__ void __launch_bounds__(256) cn_line_kernel(int64_t outer, int64_t n, 
   }
 }
 
+// The same CN half-step on the contiguous axis (inner == 1).  There the 32
+// lines of a warp's group are consecutive in memory, so a chunk of CNC_KC
+// nodes of all 32 lines is staged through shared memory with one coalesced
+// 256-byte access per line (lane = node), and lane l runs line l's recurrences
+// from the tile: the forward sweep over the staged psi (d written back through
+// the tile, coalesced), then the back substitution over the staged d -- the
+// arithmetic of cn_line_kernel in the same order, so the results are the
+// same bits.  (One thread per line reading its own contiguous line touches a
+// different 32-byte sector per lane on every load.)
+constexpr int CNC_KC = 32;
+constexpr int CNC_WARPS = 4;
+
+template <typename T>
+__global__ void __launch_bounds__(CNC_WARPS * 32) cn_contig_kernel(int64_t lines, int64_t n, double cR, double dR,
+                                                                   const double* f, const double* m,
+                                                                   const double* sup, const T* in, T* out) {
+  __shared__ double tile_all[CNC_WARPS][32][CNC_KC + 1];
+  __shared__ double coef_all[CNC_WARPS][2][CNC_KC];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double(*tile)[CNC_KC + 1] = tile_all[wid];
+  double* ca = coef_all[wid][0];
+  double* cb = coef_all[wid][1];
+  const double c2 = rn_mul(2.0, cR);
+  const int64_t ngroups = (lines + 31) / 32;
+  for (int64_t g = blockIdx.x * (int64_t)CNC_WARPS + wid; g < ngroups; g += (int64_t)gridDim.x * CNC_WARPS) {
+    const int64_t l0 = g * 32;
+    const int nl = (int)(lines - l0 < 32 ? lines - l0 : 32);
+    const T* gin = in + l0 * n;   // line j of the group starts at gin + j n
+    T* gout = out + l0 * n;
+    const bool act = lane < nl;
+    double pm = 0.0, pc = act ? (double)gin[(int64_t)lane * n] : 0.0;
+    double d = 0.0;
+    // forward sweep, chunks of nodes k0 .. k0 + cnt - 1
+    for (int64_t k0 = 0; k0 < n; k0 += CNC_KC) {
+      const int cnt = (int)(n - k0 < CNC_KC ? n - k0 : CNC_KC);
+      {
+        const int64_t k = k0 + 1 + lane;   // psi at k + 1 for the chunk's nodes
+        double v[32];
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] = (j < nl && k < n) ? (double)gin[(int64_t)j * n + k] : 0.0;
+#pragma unroll
+        for (int j = 0; j < 32; ++j) tile[j][lane] = v[j];
+        const int64_t kc = k0 + lane;
+        ca[lane] = (kc >= 1 && kc < n) ? f[kc - 1] : 0.0;
+      }
+      __syncwarp();
+      for (int t = 0; t < cnt; ++t) {
+        const int64_t k = k0 + t;
+        const double pn = tile[lane][t];
+        double r;
+        if (k == 0) r = rn_add(rn_mul(dR, pc), rn_mul(c2, pn));
+        else if (k < n - 1) r = rn_add(rn_add(rn_mul(cR, pm), rn_mul(dR, pc)), rn_mul(cR, pn));
+        else r = rn_add(rn_mul(c2, pm), rn_mul(dR, pc));
+        d = (k == 0) ? r : rn_sub(r, rn_mul(ca[t], d));
+        tile[lane][t] = d;
+        pm = pc;
+        pc = pn;
+      }
+      __syncwarp();
+      if (lane < cnt) {
+        for (int j = 0; j < nl; ++j) gout[(int64_t)j * n + k0 + lane] = (T)tile[j][lane];
+      }
+      __syncwarp();
+    }
+    // back substitution: node n - 1 from the unrounded d, then down from n - 2
+    // over the stored (T-rounded) d, chunks of nodes kb .. kb + cnt - 1 from the top
+    double x = d / m[n - 1];
+    for (int64_t top = n - 1; top >= 0; top -= CNC_KC) {
+      const int64_t kb = top - CNC_KC + 1 > 0 ? top - CNC_KC + 1 : 0;
+      const int cnt = (int)(top - kb + 1);
+      if (lane < cnt) {
+        for (int j = 0; j < nl; ++j) tile[j][lane] = (double)gout[(int64_t)j * n + kb + lane];
+        ca[lane] = sup[kb + lane < n - 1 ? kb + lane : 0];
+        cb[lane] = m[kb + lane];
+      }
+      __syncwarp();
+      for (int t = cnt - 1; t >= 0; --t) {
+        const int64_t k = kb + t;
+        if (k < n - 1) x = rn_sub(tile[lane][t], rn_mul(ca[t], x)) / cb[t];
+        tile[lane][t] = x;
+      }
+      __syncwarp();
+      if (lane < cnt) {
+        for (int j = 0; j < nl; ++j) gout[(int64_t)j * n + kb + lane] = (T)tile[j][lane];
+      }
+      __syncwarp();
+    }
+  }
+}
+
 constexpr int MASS_BLOCKS = 1024;
 
 // per-block partial sums of q dV and 4 q (1 - q) dV in a fixed order
@@ -583,14 +686,51 @@ extern "C" int tpf_reinit_cn_axis(int ndim, const int64_t* shape, int axis, doub
   TPF_CHECK_ARG(n >= 2, "at least 2 nodes along the axis");
   const int64_t lines = outer * inner;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (dtype == TPF_F64)
+  if (inner == 1) {
+    // contiguous axis: groups of 32 consecutive lines staged through shared memory
+    const int64_t ngroups = (lines + 31) / 32;
+    const int blocks = (int)std::max<int64_t>(
+        1, std::min<int64_t>((ngroups + CNC_WARPS - 1) / CNC_WARPS, (int64_t)tpf::sm_count() * 8));
+    if (dtype == TPF_F64)
+      cn_contig_kernel<double><<<blocks, CNC_WARPS * 32, 0, st>>>(lines, n, cR, dR, f, m, sup,
+                                                                  static_cast<const double*>(in),
+                                                                  static_cast<double*>(out));
+    else
+      cn_contig_kernel<float><<<blocks, CNC_WARPS * 32, 0, st>>>(lines, n, cR, dR, f, m, sup,
+                                                                 static_cast<const float*>(in),
+                                                                 static_cast<float*>(out));
+    TPF_CUDA_TRY(cudaGetLastError());
+    return TPF_OK;
+  }
+  // one thread per line; threads per block autotuned among kThreadsCand (a
+  // line's solve does not depend on the launch shape), else 256 with up to
+  // 8 blocks per SM
+  static constexpr int kThreadsCand[3] = {64, 128, 256};
+  const int64_t sms = tpf::sm_count();
+  auto launch = [&](int bs, void* dst, cudaStream_t s2) -> int {
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((lines + bs - 1) / bs, sms * (2048 / bs)));
+    if (dtype == TPF_F64)
+      cn_line_kernel<double><<<blocks, bs, 0, s2>>>(outer, n, inner, cR, dR, f, m, sup, static_cast<const double*>(in),
+                                                    static_cast<double*>(dst));
+    else
+      cn_line_kernel<float><<<blocks, bs, 0, s2>>>(outer, n, inner, cR, dR, f, m, sup, static_cast<const float*>(in),
+                                                   static_cast<float*>(dst));
+    return cudaPeekAtLastError() == cudaSuccess ? TPF_OK : TPF_ECUDA;
+  };
+  auto cand = [&](int c, void* scratch, cudaStream_t s2) { return launch(kThreadsCand[c], scratch, s2); };
+  const tpf::TuneKey key{tpf::kTuneCnLine, dtype, {outer, n, inner, 0}};
+  const int pick = tpf::tuned_choice(key, 3, -1, (size_t)(outer * n * inner) * (dtype == TPF_F64 ? 8 : 4), st, cand);
+  if (pick >= 0) {
+    launch(kThreadsCand[pick], out, st);
+  } else if (dtype == TPF_F64) {
     cn_line_kernel<double><<<blocks_for(lines, 8), 256, 0, st>>>(outer, n, inner, cR, dR, f, m, sup,
                                                                  static_cast<const double*>(in),
                                                                  static_cast<double*>(out));
-  else
+  } else {
     cn_line_kernel<float><<<blocks_for(lines, 8), 256, 0, st>>>(outer, n, inner, cR, dR, f, m, sup,
                                                                 static_cast<const float*>(in),
                                                                 static_cast<float*>(out));
+  }
   TPF_CUDA_TRY(cudaGetLastError());
   return TPF_OK;
 }

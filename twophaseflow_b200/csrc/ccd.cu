@@ -173,6 +173,26 @@ __device__ __forceinline__ void cp_async(void* smem, const void* gmem, bool vali
   asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(sa), "l"(gmem), "n"(BYTES), "r"(src)
                : "memory");
 }
+// cp.async with an L2 eviction-priority policy (createpolicy), for staging
+// copies whose lines are re-read later (evict_last) or read for the last
+// time (evict_first)
+template <int BYTES>
+__device__ __forceinline__ void cp_async_pol(void* smem, const void* gmem, uint64_t pol) {
+  unsigned int sa = (unsigned int)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], %2, %2, %3;\n" ::"r"(sa), "l"(gmem), "n"(BYTES),
+               "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ uint64_t pol_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t pol_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
@@ -1070,7 +1090,11 @@ __global__ void __launch_bounds__(128) ccd_lane_kernel(CcdArgs a, const T* __res
     }
     const T* __restrict__ fl = f + base;
     // asynchronous copy of nodes k0 + t, t in [0, KN), into tile[t][lane]
-    auto stage = [&](T* tile, int k0, int KN) {
+    // FP64 strided axes: pass-1 chunks are staged with L2 evict_last (pass 2
+    // re-reads them), pass-2 chunks and the reused last chunk with
+    // evict_first (measured 2-3.5 % faster at 257^3; FP32 unchanged, so plain)
+    const uint64_t pol_keep = pol_evict_last(), pol_last = pol_evict_first();
+    auto stage = [&](T* tile, int k0, int KN, bool keep) {
       if (CONTIG) {
         // element e = (line ll, node t) of the chunk, e = lane + 32 i: runs of KN
         // contiguous nodes per line, so each warp copy reads ~2 contiguous runs
@@ -1101,9 +1125,17 @@ __global__ void __launch_bounds__(128) ccd_lane_kernel(CcdArgs a, const T* __res
           }
         } else {
           const T* src = fl + (int64_t)k0 * inner;
-          for (int t = 0; t < KN; ++t) {
-            cp_async<sizeof(T)>(tile + t * TS + lane, src, true);
-            src += inner;
+          if (sizeof(T) == 8) {
+            const uint64_t pol = keep ? pol_keep : pol_last;
+            for (int t = 0; t < KN; ++t) {
+              cp_async_pol<sizeof(T)>(tile + t * TS + lane, src, pol);
+              src += inner;
+            }
+          } else {
+            for (int t = 0; t < KN; ++t) {
+              cp_async<sizeof(T)>(tile + t * TS + lane, src, true);
+              src += inner;
+            }
           }
         }
       }
@@ -1131,7 +1163,7 @@ __global__ void __launch_bounds__(128) ccd_lane_kernel(CcdArgs a, const T* __res
       const int want = min(n_loads, need + NBUF);
       while (issued < want) {
         const int c = chunk_of_load(issued);
-        stage(fb0 + (issued % NBUF) * TR * TS, k0_of(c), cnt_of(c) + 2);
+        stage(fb0 + (issued % NBUF) * TR * TS, k0_of(c), cnt_of(c) + 2, issued < P - 1);
         ++issued;
       }
       cp_async_wait_dyn<NBUF>(issued - need - 1);

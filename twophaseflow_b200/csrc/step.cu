@@ -690,14 +690,27 @@ void launch_rc_t(const RcArgs& a, cudaStream_t st) {
     const int64_t ntiles = (tot + RC_TILE - 1) / RC_TILE;
     rc_tile_kernel<T, BF><<<(int)std::max<int64_t>(1, std::min<int64_t>(ntiles, sms * 8)), 256, 0, st>>>(a);
   } else if (a.inner >= 32) {
-    // chunk length: enough threads to fill the GPU (about 2048 per SM), 8..64 nodes
+    // chunk length: autotuned among kChunks (the march gives the same values
+    // for every chunk length), else enough threads to fill the GPU (about
+    // 2048 per SM), 8..64 nodes
     const int64_t lines = a.outer * a.inner;
     int64_t chunk = (lines * a.n) / (sms * 2048);
     chunk = std::max<int64_t>(8, std::min<int64_t>(64, chunk));
-    const int64_t nchunks = (a.n + chunk - 1) / chunk;
-    const int64_t work = lines * nchunks;
-    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, sms * 8));
-    rc_march_kernel<T, BF><<<blocks, 256, 0, st>>>(a, chunk, nchunks);
+    static constexpr int64_t kChunks[5] = {8, 16, 32, 64, 128};
+    auto launch = [&](int64_t ck, void* out, cudaStream_t s2) -> int {
+      RcArgs b = a;
+      b.out = out;
+      const int64_t nchunks = (a.n + ck - 1) / ck;
+      const int64_t work = lines * nchunks;
+      const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, sms * 8));
+      rc_march_kernel<T, BF><<<blocks, 256, 0, s2>>>(b, ck, nchunks);
+      return cudaPeekAtLastError() == cudaSuccess ? TPF_OK : TPF_ECUDA;
+    };
+    auto cand = [&](int c, void* scratch, cudaStream_t s2) { return launch(kChunks[c], scratch, s2); };
+    const tpf::TuneKey key{tpf::kTuneRcMarch, (int)sizeof(T) + (BF ? 16 : 0),
+                           {a.outer, a.n, a.inner, 2 * a.periodic + a.accumulate}};
+    const int pick = tpf::tuned_choice(key, 5, -1, (size_t)tot * sizeof(T), st, cand);
+    launch(pick >= 0 ? kChunks[pick] : chunk, a.out, st);
   } else {
     rc_divergence_kernel<T><<<ew_blocks64(tot), 256, 0, st>>>(a);
   }

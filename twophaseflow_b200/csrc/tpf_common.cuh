@@ -34,6 +34,32 @@ const char* last_error();
     }                                 \
   } while (0)
 
+// Launch-shape autotuning for kernels whose results do not depend on the
+// launch shape (march chunk lengths, threads per block): tuned_choice returns
+// the index of the fastest of `ncand` candidates for the signature `key`.
+// The first eager call of a signature allocates `scratch_bytes` of zeroed
+// scratch, runs each candidate through run(c, scratch, stream) once to warm
+// up and three times under CUDA events on `stream`, keeps the fastest for the
+// process and frees the scratch; `run` must write only to the scratch.
+// Under stream capture, with tuning switched off (tpf_set_launch_autotune),
+// or when the scratch cannot be allocated, an untuned signature gets
+// `fallback` and nothing is cached.
+struct TuneKey {
+  int kernel, dtype;
+  int64_t d[4];
+};
+enum TuneKernel { kTuneFluxMarch = 1, kTuneRcMarch = 2, kTuneCnLine = 3 };
+typedef int (*TuneRun)(int cand, void* scratch, cudaStream_t s, void* ctx);
+int tuned_choice_impl(const TuneKey& key, int ncand, int fallback, size_t scratch_bytes, cudaStream_t s, TuneRun run,
+                      void* ctx);
+template <typename F>
+int tuned_choice(const TuneKey& key, int ncand, int fallback, size_t scratch_bytes, cudaStream_t s, F& f) {
+  TuneRun thunk = [](int c, void* scratch, cudaStream_t st, void* ctx) -> int {
+    return (*static_cast<F*>(ctx))(c, scratch, st);
+  };
+  return tuned_choice_impl(key, ncand, fallback, scratch_bytes, s, thunk, &f);
+}
+
 inline int sm_count() {
   int dev = 0, n = 0;
   cudaGetDevice(&dev);
