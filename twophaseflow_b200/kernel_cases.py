@@ -595,6 +595,8 @@ def main(argv=None):
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--nmin", type=int, default=128, help="batched: smallest nodes per axis")
+    ap.add_argument("--nmax", type=int, default=512, help="batched: largest nodes per axis")
     ap.add_argument("--maxiter", type=int, default=0,
                     help="learned: stop after this many iterations; gmres: after this many restart cycles")
     a = ap.parse_args(argv)
@@ -621,7 +623,7 @@ def main(argv=None):
     elif a.case == "step":
         r = step_case(tuple(a.N), a.reps)
     else:
-        r = batched_case(n_cases=a.N[0], reps=a.reps)
+        r = batched_case(n_cases=a.N[0], nmin=a.nmin, nmax=a.nmax, reps=a.reps)
     print(json.dumps(r), flush=True)
     return 0
 
