@@ -302,8 +302,11 @@ int tpf_visc_accumulate(int64_t n, const void* g, int accumulate, int finalize, 
  * branch of ViscousTerm.apply_cn_predictor, ns_terms/viscous.py:161-167):
  * mode 0: out = u + dt (e / rho + vn); mode 1: out = u + dt ((e / rho + 0.5 vn)
  * + 0.5 vs); mode 2 (the explicit branch of Predictor.compute,
- * time_integration/ab2_predictor.py:196-201): out = u + dt (e + rho vn) / rho.  e = explicit right-hand side, vn / vs = viscous force at u and at
- * the predicted state.  n values each; out may alias u. */
+ * time_integration/ab2_predictor.py:196-201): out = u + dt (e + rho vn) / rho;
+ * mode 3 (RichardsonCNAdvance.advance, cn_advance/richardson_cn.py:76-109):
+ * out = (4 u - vn) / 3 with u the two half steps and vn the full step (e, rho,
+ * vs unused, may be NULL).  e = explicit right-hand side, vn / vs = viscous
+ * force at u and at the predicted state.  n values each; out may alias u. */
 int tpf_cn_predictor_combine(int64_t n, int mode, double dt, const void* u, const void* e, const void* rho,
                              const void* vn, const void* vs, void* out, int dtype, void* stream);
 

@@ -69,6 +69,17 @@ def cn_predictor(u_old, e, mu, rho, Re, L, N, bc, dt, cn_viscous=True, scheme="c
     return [u_old[c] + dt * (e[c] / rho + 0.5 * vn[c] + 0.5 * vs[c]) for c in range(nd)]
 
 
+def cn_predictor_richardson(u_old, e, mu, rho, Re, L, N, bc, dt, scheme="ccd_bulk"):
+    """ViscousTerm.apply_cn_predictor with RichardsonCNAdvance(PicardCNAdvance)
+    (time_integration/cn_advance/richardson_cn.py:76-109): one Picard step of
+    dt, two of dt/2 with the explicit right-hand side frozen, then
+    (4 u_{dt/2,2} - u_dt) / 3."""
+    u1 = cn_predictor(u_old, e, mu, rho, Re, L, N, bc, dt, True, scheme)
+    uh = cn_predictor(u_old, e, mu, rho, Re, L, N, bc, 0.5 * dt, True, scheme)
+    u2 = cn_predictor(uh, e, mu, rho, Re, L, N, bc, 0.5 * dt, True, scheme)
+    return [(4.0 * u2[c] - u1[c]) / 3.0 for c in range(len(u_old))]
+
+
 def predictor_steps(states, dts, Re, Fr, We, L, N, bc, cn_viscous=True, use_gfm=False):
     """Predictor.compute called once per state in turn (ab2_predictor.py:110-209):
     AB2 convection (forward Euler first), gravity, CSF, IPC, viscous predictor."""

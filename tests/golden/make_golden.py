@@ -525,6 +525,12 @@ def make_viscous(out):
             u = ViscousTerm(be, 100.0, cn_viscous=cn).apply_cn_predictor(vel, e, mu, rho, ccd, 0.003)
             for a in range(len(N)):
                 out[f"{name}/pred_{tag}{a}"] = np.asarray(u[a])
+        # Richardson extrapolation around Picard (cn_mode='richardson_picard')
+        from twophase.time_integration.cn_advance import make_cn_advance
+        u = ViscousTerm(be, 100.0, cn_viscous=True, cn_advance=make_cn_advance(be, "richardson_picard")
+                        ).apply_cn_predictor(vel, e, mu, rho, ccd, 0.003)
+        for a in range(len(N)):
+            out[f"{name}/pred_rich{a}"] = np.asarray(u[a])
 
 
 def make_predictor(out):

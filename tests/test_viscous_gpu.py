@@ -100,8 +100,35 @@ def test_cn_predictor_matches_reference(cuda_device, golden, name, tag, cn):
         assert np.abs(u[a] - ref).max() <= TOL * np.abs(ref).max()
 
 
+@pytest.mark.parametrize("name", ["wall2d", "per2d", "wall3d"])
+def test_richardson_cn_predictor_matches_reference(cuda_device, golden, name):
+    """cn_mode='richardson_picard' (RichardsonCNAdvance around Picard, three
+    Picard steps and one combination kernel) against the reference's own
+    output, at the CN predictor's bar; the factory rejects unknown modes."""
+    from types import SimpleNamespace
+    from twophaseflow_b200 import CCDSolver, RichardsonCNAdvance, UniformGrid, ViscousTerm, make_cn_advance
+    from twophaseflow_b200.predictor import Predictor
+    N = tuple(int(n) for n in golden[f"{name}/N"])
+    L = tuple(float(x) for x in golden[f"{name}/L"])
+    ccd = CCDSolver(UniformGrid(N, L), None, bc_type=str(golden[f"{name}/bc"]))
+    vel = [golden[f"{name}/u{a}"] for a in range(len(N))]
+    e = [golden[f"{name}/e{a}"] for a in range(len(N))]
+    adv = make_cn_advance(None, "richardson_picard")
+    assert isinstance(adv, RichardsonCNAdvance)
+    u = ViscousTerm(None, 100.0, cn_viscous=True, cn_advance=adv).apply_cn_predictor(
+        vel, e, golden[f"{name}/mu"], golden[f"{name}/rho"], ccd, 0.003)
+    for a in range(len(N)):
+        ref = golden[f"{name}/pred_rich{a}"]
+        assert np.abs(u[a] - ref).max() <= TOL * np.abs(ref).max()
+    with pytest.raises(ValueError, match="cn_mode"):
+        make_cn_advance(None, "pade22")
+    cfg = SimpleNamespace(grid=SimpleNamespace(ndim=len(N)), fluid=SimpleNamespace(Re=100.0, Fr=1.0, We=10.0),
+                          numerics=SimpleNamespace(cn_viscous=True, cn_mode="richardson_picard"))
+    assert isinstance(Predictor(None, cfg, ccd).viscous.cn_advance, RichardsonCNAdvance)
+
+
 def test_cn_combine_kernel_bit_exact(cuda_device):
-    """Both combinations against NumPy on the same operands."""
+    """The combinations against NumPy on the same operands."""
     import torch
     from twophaseflow_b200 import _lib
     rng = np.random.default_rng(67)
@@ -116,6 +143,10 @@ def test_cn_combine_kernel_bit_exact(cuda_device):
                                                 _lib.TPF_F64, _lib.current_stream_handle()))
         ref = u + 0.0037 * (e / rho + vn) if mode == 0 else u + 0.0037 * (e / rho + 0.5 * vn + 0.5 * vs)
         np.testing.assert_array_equal(out.cpu().numpy(), ref)
+    # mode 3: the Richardson extrapolation (4 u - vn) / 3, e and rho unused
+    _lib.check(lib.tpf_cn_predictor_combine(u.size, 3, 0.0, _lib.dptr(T[0]), None, None, _lib.dptr(T[3]), None,
+                                            _lib.dptr(out), _lib.TPF_F64, _lib.current_stream_handle()))
+    np.testing.assert_array_equal(out.cpu().numpy(), (4.0 * u - vn) / 3.0)
 
 
 PGOLD = os.path.join(os.path.dirname(__file__), "golden", "predictor_golden.npz")

@@ -41,6 +41,18 @@ def test_cn_predictor_matches_reference(name, tag, cn):
         np.testing.assert_array_equal(u[a], G[f"{name}/pred_{tag}{a}"])
 
 
+@pytest.mark.parametrize("name", ["wall2d", "per2d", "wall3d"])
+def test_cn_predictor_richardson_matches_reference(name):
+    """cn_mode='richardson_picard': the reference's RichardsonCNAdvance around
+    Picard, bit for bit."""
+    N, L, bc = G[f"{name}/N"], G[f"{name}/L"], str(G[f"{name}/bc"])
+    vel = [G[f"{name}/u{a}"] for a in range(len(N))]
+    e = [G[f"{name}/e{a}"] for a in range(len(N))]
+    u = ov.cn_predictor_richardson(vel, e, G[f"{name}/mu"], G[f"{name}/rho"], 100.0, L, N, bc, 0.003)
+    for a in range(len(N)):
+        np.testing.assert_array_equal(u[a], G[f"{name}/pred_rich{a}"])
+
+
 P = np.load(os.path.join(os.path.dirname(__file__), "golden", "predictor_golden.npz"))
 
 

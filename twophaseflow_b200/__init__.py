@@ -28,7 +28,7 @@ from .grid import BoundarySpec, UniformGrid
 from .ppe import (MatrixAssemblyUnavailable, PPESolverFVMMatrixFree, create_fvm_matrixfree, register_with_reference,
                   solve_batched)
 from .levelset import CurvatureCalculatorPsi, dccd_filter_nd, update_properties
-from .viscous import PicardCNAdvance, ViscousTerm
+from .viscous import PicardCNAdvance, RichardsonCNAdvance, ViscousTerm, make_cn_advance
 from .predictor import ConvectionTerm, FlowState, GravityTerm, NSComputeContext, Predictor, SurfaceTensionTerm
 from .ns_step import TwoPhaseStep
 from .step import CFLCalculator, RhieChowInterpolator, VelocityCorrector, ccd_pressure_gradient
@@ -54,6 +54,8 @@ __all__ = [
     "CFLCalculator",
     "ViscousTerm",
     "PicardCNAdvance",
+    "RichardsonCNAdvance",
+    "make_cn_advance",
     "ConvectionTerm",
     "GravityTerm",
     "SurfaceTensionTerm",

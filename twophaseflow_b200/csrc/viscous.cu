@@ -166,6 +166,10 @@ __global__ void cn_combine_kernel(int64_t n, int mode, double dt, const T* u, co
       out[i] = (T)rn_add((double)u[i], rn_mul(dt, rn_add((double)e[i], rn_mul(r, (double)vn[i]))) / r);
       continue;
     }
+    if (mode == 3) {   // Richardson extrapolation: (4 u_{dt/2,2} - u_dt) / 3, u = the half steps, vn = the big step
+      out[i] = (T)(rn_sub(rn_mul(4.0, (double)u[i]), (double)vn[i]) / 3.0);
+      continue;
+    }
     const double er = (double)e[i] / (double)rho[i];
     double b;
     if (mode == 0) b = rn_add(er, (double)vn[i]);
@@ -178,8 +182,9 @@ __global__ void cn_combine_kernel(int64_t n, int mode, double dt, const T* u, co
 
 extern "C" int tpf_cn_predictor_combine(int64_t n, int mode, double dt, const void* u, const void* e, const void* rho,
                                         const void* vn, const void* vs, void* out, int dtype, void* stream) {
-  TPF_CHECK_ARG(mode >= 0 && mode <= 2, "mode must be 0 (forward Euler), 1 (trapezoid) or 2 (explicit predictor)");
-  TPF_CHECK_ARG(n >= 0 && u && e && rho && vn && out && (mode != 1 || vs), "NULL argument");
+  TPF_CHECK_ARG(mode >= 0 && mode <= 3,
+                "mode must be 0 (forward Euler), 1 (trapezoid), 2 (explicit predictor) or 3 (Richardson)");
+  TPF_CHECK_ARG(n >= 0 && u && vn && out && (mode == 3 || (e && rho)) && (mode != 1 || vs), "NULL argument");
   TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
   if (n == 0) return TPF_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);

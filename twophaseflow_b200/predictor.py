@@ -24,7 +24,7 @@ from typing import List, Optional
 from . import _lib
 from .arrays import to_device
 from .step import ccd_pressure_gradient
-from .viscous import ViscousTerm
+from .viscous import ViscousTerm, make_cn_advance
 
 
 def _torch():
@@ -156,10 +156,10 @@ class Predictor:
         self.use_gfm = use_gfm
         fluid, numerics = config.fluid, config.numerics
         ndim = config.grid.ndim
-        if viscous is None and str(getattr(numerics, "cn_mode", "picard")).lower() != "picard":
-            raise NotImplementedError("only the Picard CN strategy is built on the B200 path")
+        cn_mode = str(getattr(numerics, "cn_mode", "picard")).strip().lower()
         self.convection = convection or ConvectionTerm(backend)
-        self.viscous = viscous or ViscousTerm(backend, fluid.Re, getattr(numerics, "cn_viscous", True))
+        self.viscous = viscous or ViscousTerm(backend, fluid.Re, getattr(numerics, "cn_viscous", True),
+                                              cn_advance=make_cn_advance(backend, cn_mode))
         self.gravity = gravity or GravityTerm(backend, fluid.Fr, ndim)
         self.surface_tens = surface_tension or SurfaceTensionTerm(backend, fluid.We)
         self._conv_prev: Optional[List] = None

@@ -173,6 +173,47 @@ class ViscousTerm:
         return [vs[c].out(out[c]) for c in range(len(out))]
 
 
+class RichardsonCNAdvance:
+    """Richardson extrapolation around a base CN strategy
+    (src/twophase/time_integration/cn_advance/richardson_cn.py:62-109): one
+    base step of dt, two of dt/2 from the same frozen explicit right-hand
+    side, combined as (4 u_{dt/2,2} - u_dt) / 3 by one kernel."""
+
+    def __init__(self, base):
+        self.base = base
+
+    def advance(self, u_old: List, explicit_rhs: List, mu, rho, viscous_op: ViscousTerm, ccd, dt: float, psi=None,
+                intermediate_velocity_operator_transform=None, predictor_state_assembly=None, convective_rhs=None,
+                buoyancy_rhs=None) -> List:
+        torch = _torch()
+        kw = dict(psi=psi, intermediate_velocity_operator_transform=intermediate_velocity_operator_transform,
+                  predictor_state_assembly=predictor_state_assembly, convective_rhs=convective_rhs,
+                  buoyancy_rhs=buoyancy_rhs)
+        u1 = self.base.advance(u_old, explicit_rhs, mu, rho, viscous_op, ccd, dt, **kw)
+        half = 0.5 * dt
+        uh = self.base.advance(u_old, explicit_rhs, mu, rho, viscous_op, ccd, half, **kw)
+        u2 = self.base.advance(uh, explicit_rhs, mu, rho, viscous_op, ccd, half, **kw)
+        out = []
+        lib = viscous_op.lib
+        for c in range(len(u_old)):
+            o = torch.empty_like(u2[c])
+            _lib.check(lib.tpf_cn_predictor_combine(
+                o.numel(), 3, 0.0, _lib.dptr(u2[c]), None, None, _lib.dptr(u1[c]), None, _lib.dptr(o),
+                _lib.TPF_F64 if o.dtype == torch.float64 else _lib.TPF_F32, _lib.current_stream_handle()))
+            out.append(o)
+        return out
+
+
+def make_cn_advance(backend, mode: str = "picard"):
+    """``numerics.cn_mode`` -> CN strategy (cn_advance/__init__.py:25-55):
+    'picard' or 'richardson_picard'; anything else is a ValueError."""
+    if mode == "picard":
+        return PicardCNAdvance(backend)
+    if mode == "richardson_picard":
+        return RichardsonCNAdvance(PicardCNAdvance(backend))
+    raise ValueError(f"Unknown cn_mode={mode!r}; supported in this build: 'picard', 'richardson_picard'.")
+
+
 class PicardCNAdvance:
     """One Picard step on the CN equation, i.e. Heun's predictor-corrector
     (src/twophase/time_integration/cn_advance/picard_cn.py:31-96):
