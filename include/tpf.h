@@ -293,6 +293,24 @@ int tpf_visc_lowfd_axis(int ndim, const int64_t* shape, int axis, const double* 
 /* out = mu (a + b), n values (the stress of the legacy CCD scheme). */
 int tpf_visc_stress(int64_t n, const void* mu, const void* a, const void* b, void* out, int dtype, void* stream);
 
+/* Interface-band form of the ccd_bulk viscous scheme, used when psi is given
+ * (ViscousSpatialEvaluator.evaluate, ns_terms/viscous_spatial.py:50-64,
+ * 158-221).  tpf_visc_band_masks: band[i] = 1 where any node of the 3^ndim box
+ * around i (inside the domain) has 1e-6 < psi < 1 - 1e-6
+ * (_interface_band_mask); normal[a][i] = 1 where |grads[a]| is the largest
+ * of the axes' |grads| and that maximum exceeds 1e-14, or where the maximum
+ * is <= 1e-14 (_normal_axis_masks); grads = the low-order derivatives of psi
+ * (tpf_visc_lowfd_axis).  Masks are one byte per node.
+ * tpf_visc_select: s = mask ? lo : hi (lo when mask is NULL, hi may then be
+ * NULL); mode 0 out = s, 1 out += s, 2 out = 0 + s.
+ * tpf_visc_band_finalize: out = (band ? nt : mu lap) / (Re rho). */
+int tpf_visc_band_masks(int ndim, const int64_t* shape, const void* psi, const void* const* grads,
+                        unsigned char* band, unsigned char* const* normal, int dtype, void* stream);
+int tpf_visc_select(int64_t n, const unsigned char* mask, const void* lo, const void* hi, int mode, void* out,
+                    int dtype, void* stream);
+int tpf_visc_band_finalize(int64_t n, const unsigned char* band, const void* nt, const void* lap, const void* mu,
+                           const void* rho, double re, void* out, int dtype, void* stream);
+
 /* total (+)= g, then (finalize) total / (Re rho). */
 int tpf_visc_accumulate(int64_t n, const void* g, int accumulate, int finalize, const void* rho, double re,
                         void* total, int dtype, void* stream);

@@ -1,6 +1,7 @@
 """CPU restatement of the viscous stress divergence (TEST INFRASTRUCTURE: the
-oracle): ViscousSpatialEvaluator.evaluate for psi = None (reference
-``src/twophase/ns_terms/viscous_spatial.py:28-153``) on the oracle's CCD.
+oracle): ViscousSpatialEvaluator.evaluate (reference
+``src/twophase/ns_terms/viscous_spatial.py:28-221``, the three schemes and
+the interface-band form of ccd_bulk when psi is given) on the oracle's CCD.
 
 Pinned against the reference's own outputs in ``tests/golden/viscous_golden.npz``.
 Only tests, smoke() and bench.py's CPU-baseline leg may use this module.
@@ -33,13 +34,48 @@ def low_order_derivative(arr, axis: int, coords):
     return d
 
 
-def viscous(vel, mu, rho, Re: float, L, N, bc: str, scheme: str = "ccd_bulk"):
+def band_masks(psi, coords):
+    """_interface_band_mask and _normal_axis_masks (viscous_spatial.py:175-200):
+    the band 1e-6 < psi < 1 - 1e-6 dilated by one node along each axis in
+    turn; per axis, whether |d psi / dx_a| (low-order) is the largest."""
+    p = np.asarray(psi)
+    band = (p > 1.0e-6) & (p < 1.0 - 1.0e-6)
+    for ax in range(p.ndim):
+        base = band.copy()
+        lo = [slice(None)] * p.ndim
+        hi = [slice(None)] * p.ndim
+        lo[ax] = slice(1, None)
+        hi[ax] = slice(None, -1)
+        band[tuple(lo)] = band[tuple(lo)] | base[tuple(hi)]
+        band[tuple(hi)] = band[tuple(hi)] | base[tuple(lo)]
+    ag = [np.abs(low_order_derivative(p, ax, coords[ax])) for ax in range(p.ndim)]
+    mx = ag[0]
+    for g in ag[1:]:
+        mx = np.maximum(mx, g)
+    flat = mx <= 1.0e-14
+    return band, [((g >= mx) & (mx > 1.0e-14)) | flat for g in ag]
+
+
+def viscous(vel, mu, rho, Re: float, L, N, bc: str, scheme: str = "ccd_bulk", psi=None):
     nd = len(vel)
     kinds = axis_kinds(bc, nd)
     coords = [np.linspace(0.0, L[a], N[a] + 1) for a in range(nd)]
     h = [float(L[a] / N[a]) for a in range(nd)]
     D = lambda f, ax: np.asarray(occd.differentiate(f, ax, h[ax], bc=kinds[ax])[0])
     lo = lambda f, ax: low_order_derivative(f, ax, coords[ax])
+    if psi is not None and scheme == "ccd_bulk":
+        band, normal = band_masks(psi, coords)
+        sw = lambda f, ax: np.where(normal[ax], lo(f, ax), D(f, ax))
+        out = []
+        for al in range(nd):
+            total = np.zeros_like(vel[al])
+            for be in range(nd):
+                total += sw(mu * (sw(vel[al], be) + sw(vel[be], al)), be)
+            lap = np.zeros_like(vel[al])
+            for ax in range(nd):
+                lap += np.asarray(occd.differentiate(vel[al], ax, h[ax], bc=kinds[ax])[1])
+            out.append(np.where(band, total, mu * lap) / (Re * rho))
+        return out
     out = []
     for al in range(nd):
         total = np.zeros_like(vel[al])

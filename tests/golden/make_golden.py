@@ -525,6 +525,18 @@ def make_viscous(out):
             u = ViscousTerm(be, 100.0, cn_viscous=cn).apply_cn_predictor(vel, e, mu, rho, ccd, 0.003)
             for a in range(len(N)):
                 out[f"{name}/pred_{tag}{a}"] = np.asarray(u[a])
+        # interface-band form of ccd_bulk (psi given): a thin sigmoid
+        # interface (psi < 1e-6 deep inside, exactly 1 far outside)
+        X = np.meshgrid(*[np.asarray(c) for c in grid.coords], indexing="ij")
+        r = np.sqrt(sum((x - 0.45 * l) ** 2 for x, l in zip(X, L)))
+        psi = 1.0 / (1.0 + np.exp(-(r - 0.3 * min(L)) / 0.02))
+        out[f"{name}/psi"] = psi
+        v = ViscousTerm(be, 100.0, spatial_scheme="ccd_bulk").compute_explicit(vel, mu, rho, ccd, psi=psi)
+        for a in range(len(N)):
+            out[f"{name}/ccd_bulk_band/v{a}"] = np.asarray(v[a])
+        u = ViscousTerm(be, 100.0, cn_viscous=True).apply_cn_predictor(vel, e, mu, rho, ccd, 0.003, psi=psi)
+        for a in range(len(N)):
+            out[f"{name}/pred_band{a}"] = np.asarray(u[a])
         # Richardson extrapolation around Picard (cn_mode='richardson_picard')
         from twophase.time_integration.cn_advance import make_cn_advance
         u = ViscousTerm(be, 100.0, cn_viscous=True, cn_advance=make_cn_advance(be, "richardson_picard")

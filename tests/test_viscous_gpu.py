@@ -101,6 +101,56 @@ def test_cn_predictor_matches_reference(cuda_device, golden, name, tag, cn):
 
 
 @pytest.mark.parametrize("name", ["wall2d", "per2d", "wall3d"])
+def test_interface_band_viscous_matches_reference(cuda_device, golden, name):
+    """ccd_bulk with psi (compute_explicit and the Picard CN predictor) against
+    the reference's own outputs at the viscous bar."""
+    from twophaseflow_b200 import CCDSolver, UniformGrid, ViscousTerm
+    N = tuple(int(n) for n in golden[f"{name}/N"])
+    L = tuple(float(x) for x in golden[f"{name}/L"])
+    ccd = CCDSolver(UniformGrid(N, L), None, bc_type=str(golden[f"{name}/bc"]))
+    vel = [golden[f"{name}/u{a}"] for a in range(len(N))]
+    e = [golden[f"{name}/e{a}"] for a in range(len(N))]
+    mu, rho, psi = golden[f"{name}/mu"], golden[f"{name}/rho"], golden[f"{name}/psi"]
+    v = ViscousTerm(None, 100.0, spatial_scheme="ccd_bulk").compute_explicit(vel, mu, rho, ccd, psi=psi)
+    u = ViscousTerm(None, 100.0, cn_viscous=True).apply_cn_predictor(vel, e, mu, rho, ccd, 0.003, psi=psi)
+    for a in range(len(N)):
+        ref = golden[f"{name}/ccd_bulk_band/v{a}"]
+        assert np.abs(v[a] - ref).max() <= TOL * np.abs(ref).max(), (a, np.abs(v[a] - ref).max())
+        ref = golden[f"{name}/pred_band{a}"]
+        assert np.abs(u[a] - ref).max() <= TOL * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("shape", [(129, 130), (41, 38, 45)])
+def test_band_mask_kernel_bit_exact(cuda_device, shape):
+    """The band and normal-axis masks against the oracle on seeded psi with
+    exact 0 / 1 plateaus, ties between axes and a flat region."""
+    import ctypes as C
+    import torch
+    from oracle import viscous as ov
+    from twophaseflow_b200 import _lib
+    rng = np.random.default_rng(71)
+    nd = len(shape)
+    psi = rng.uniform(0.0, 1.0, shape)
+    psi[psi < 0.3] = 0.0
+    psi[psi > 0.7] = 1.0
+    psi[tuple(slice(0, 5) for _ in shape)] = 0.5        # flat: every axis normal
+    coords = [np.linspace(0.0, 1.0 + 0.2 * a, n) for a, n in enumerate(shape)]
+    band, normal = ov.band_masks(psi, coords)
+    grads = [torch.from_numpy(ov.low_order_derivative(psi, a, coords[a])).cuda() for a in range(nd)]
+    tp = torch.from_numpy(psi).cuda()
+    b = torch.empty(shape, dtype=torch.uint8, device="cuda")
+    m = [torch.empty_like(b) for _ in range(nd)]
+    lib = _lib.load()
+    _lib.check(lib.tpf_visc_band_masks(nd, (C.c_int64 * nd)(*shape), _lib.dptr(tp),
+                                       (C.c_void_p * nd)(*[_lib.dptr(g) for g in grads]), _lib.dptr(b),
+                                       (C.c_void_p * nd)(*[_lib.dptr(x) for x in m]), _lib.TPF_F64,
+                                       _lib.current_stream_handle()))
+    np.testing.assert_array_equal(b.cpu().numpy().astype(bool), band)
+    for a in range(nd):
+        np.testing.assert_array_equal(m[a].cpu().numpy().astype(bool), normal[a])
+
+
+@pytest.mark.parametrize("name", ["wall2d", "per2d", "wall3d"])
 def test_richardson_cn_predictor_matches_reference(cuda_device, golden, name):
     """cn_mode='richardson_picard' (RichardsonCNAdvance around Picard, three
     Picard steps and one combination kernel) against the reference's own

@@ -42,6 +42,22 @@ def test_cn_predictor_matches_reference(name, tag, cn):
 
 
 @pytest.mark.parametrize("name", ["wall2d", "per2d", "wall3d"])
+def test_interface_band_ccd_bulk_matches_reference(name):
+    """ccd_bulk with psi given (interface band: normal-axis low-order /
+    tangential CCD stress divergence; bulk: mu times the CCD Laplacian),
+    bit for bit; both branches occur in every case."""
+    N, L, bc = G[f"{name}/N"], G[f"{name}/L"], str(G[f"{name}/bc"])
+    vel = [G[f"{name}/u{a}"] for a in range(len(N))]
+    psi = G[f"{name}/psi"]
+    coords = [np.linspace(0.0, L[a], N[a] + 1) for a in range(len(N))]
+    band, _ = ov.band_masks(psi, coords)
+    assert band.any() and (~band).any()
+    v = ov.viscous(vel, G[f"{name}/mu"], G[f"{name}/rho"], 100.0, L, N, bc, "ccd_bulk", psi=psi)
+    for a in range(len(N)):
+        np.testing.assert_array_equal(v[a], G[f"{name}/ccd_bulk_band/v{a}"])
+
+
+@pytest.mark.parametrize("name", ["wall2d", "per2d", "wall3d"])
 def test_cn_predictor_richardson_matches_reference(name):
     """cn_mode='richardson_picard': the reference's RichardsonCNAdvance around
     Picard, bit for bit."""

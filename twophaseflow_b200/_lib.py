@@ -147,6 +147,12 @@ SIGNATURES = {
                                       C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                                       C.c_void_p, C.c_double, C.c_void_p, C.c_int, C.c_void_p]),
     "tpf_visc_stress": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "tpf_visc_band_masks": (C.c_int, [C.c_int, C.POINTER(C.c_int64), C.c_void_p, C.POINTER(C.c_void_p), C.c_void_p,
+                                      C.POINTER(C.c_void_p), C.c_int, C.c_void_p]),
+    "tpf_visc_select": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                                  C.c_void_p]),
+    "tpf_visc_band_finalize": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_double, C.c_void_p, C.c_int, C.c_void_p]),
     "tpf_visc_accumulate": (C.c_int, [C.c_int64, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_double, C.c_void_p,
                                       C.c_int, C.c_void_p]),
     "tpf_cn_predictor_combine": (C.c_int, [C.c_int64, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,

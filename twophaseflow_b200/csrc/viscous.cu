@@ -148,6 +148,148 @@ extern "C" int tpf_visc_accumulate(int64_t n, const void* g, int accumulate, int
 }
 
 // ---------------------------------------------------------------------------
+// Interface-band form of the ccd_bulk scheme, used when psi is given
+// (ViscousSpatialEvaluator.evaluate, viscous_spatial.py:50-64,158-221): inside
+// the band around the interface the stress divergence with, per axis, the
+// low-order derivative where that axis is the normal axis and the CCD
+// derivative elsewhere; outside it mu times the CCD Laplacian; both / (Re rho).
+// ---------------------------------------------------------------------------
+namespace {
+
+// NumPy's maximum: NaN if either is NaN, else the larger
+__device__ __forceinline__ double np_maximum(double a, double b) {
+  if (a != a || b != b) return a + b;
+  return a > b ? a : b;
+}
+
+// band = core dilated by one node along every axis in turn (= the 3^ndim box
+// around each node, inside the domain), core = 1e-6 < psi < 1 - 1e-6
+// (_interface_band_mask, :175-187); normal[a] = (|g_a| >= max_b |g_b| and
+// max > 1e-14) or max <= 1e-14, g = the low-order derivatives of psi
+// (_normal_axis_masks, :189-200)
+template <typename T>
+__global__ void band_masks_kernel(int nd, int64_t n0, int64_t n1, int64_t n2, const T* psi, const T* g0, const T* g1,
+                                  const T* g2, unsigned char* band, unsigned char* m0, unsigned char* m1,
+                                  unsigned char* m2) {
+  const int64_t tot = n0 * n1 * n2;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k2 = i % n2, k1 = (i / n2) % n1, k0 = i / (n1 * n2);
+    bool b = false;
+    for (int d0 = -1; d0 <= 1 && !b; ++d0) {
+      const int64_t j0 = k0 + d0;
+      if (j0 < 0 || j0 >= n0) continue;
+      for (int d1 = -1; d1 <= 1 && !b; ++d1) {
+        const int64_t j1 = k1 + d1;
+        if (j1 < 0 || j1 >= n1 || (nd < 2 && d1 != 0)) continue;
+        for (int d2 = -1; d2 <= 1 && !b; ++d2) {
+          const int64_t j2 = k2 + d2;
+          if (j2 < 0 || j2 >= n2 || (nd < 3 && d2 != 0)) continue;
+          const double p = (double)psi[(j0 * n1 + j1) * n2 + j2];
+          b = (p > 1.0e-6) && (p < 1.0 - 1.0e-6);
+        }
+      }
+    }
+    band[i] = b ? 1 : 0;
+    const double a0 = fabs((double)g0[i]);
+    const double a1 = nd > 1 ? fabs((double)g1[i]) : 0.0;
+    const double a2 = nd > 2 ? fabs((double)g2[i]) : 0.0;
+    double mx = a0;
+    if (nd > 1) mx = np_maximum(mx, a1);
+    if (nd > 2) mx = np_maximum(mx, a2);
+    const bool flat = mx <= 1.0e-14, big = mx > 1.0e-14;
+    m0[i] = ((a0 >= mx && big) || flat) ? 1 : 0;
+    if (nd > 1) m1[i] = ((a1 >= mx && big) || flat) ? 1 : 0;
+    if (nd > 2) m2[i] = ((a2 >= mx && big) || flat) ? 1 : 0;
+  }
+}
+
+// s = mask ? lo : hi (lo when mask is NULL); mode 0: out = s, 1: out += s,
+// 2: out = 0 + s (the first term of a sum started from zeros)
+template <typename T>
+__global__ void select_kernel(int64_t n, const unsigned char* mask, const T* lo, const T* hi, int mode, T* out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double s = (!mask || mask[i]) ? (double)lo[i] : (double)hi[i];
+    if (mode == 0) out[i] = (T)s;
+    else if (mode == 1) out[i] = (T)rn_add((double)out[i], s);
+    else out[i] = (T)rn_add(0.0, s);
+  }
+}
+
+// out = where(band, nt, mu lap) / (Re rho)
+template <typename T>
+__global__ void band_finalize_kernel(int64_t n, const unsigned char* band, const T* nt, const T* lap, const T* mu,
+                                     const T* rho, double re, T* out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double v = band[i] ? (double)nt[i] : rn_mul((double)mu[i], (double)lap[i]);
+    out[i] = (T)(v / rn_mul(re, (double)rho[i]));
+  }
+}
+
+}  // namespace
+
+extern "C" int tpf_visc_band_masks(int ndim, const int64_t* shape, const void* psi, const void* const* grads,
+                                   unsigned char* band, unsigned char* const* normal, int dtype, void* stream) {
+  TPF_CHECK_ARG(ndim >= 1 && ndim <= 3 && shape && psi && grads && band && normal, "NULL argument or bad ndim");
+  TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
+  int64_t n[3] = {1, 1, 1};
+  for (int a = 0; a < ndim; ++a) {
+    TPF_CHECK_ARG(shape[a] >= 1 && grads[a] && normal[a], "empty axis or NULL gradient / mask");
+    n[a] = shape[a];
+  }
+  const int64_t tot = n[0] * n[1] * n[2];
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  unsigned char* m1 = ndim > 1 ? normal[1] : nullptr;
+  unsigned char* m2 = ndim > 2 ? normal[2] : nullptr;
+  if (dtype == TPF_F64)
+    band_masks_kernel<double><<<blocks_for(tot), 256, 0, st>>>(
+        ndim, n[0], n[1], n[2], static_cast<const double*>(psi), static_cast<const double*>(grads[0]),
+        ndim > 1 ? static_cast<const double*>(grads[1]) : nullptr,
+        ndim > 2 ? static_cast<const double*>(grads[2]) : nullptr, band, normal[0], m1, m2);
+  else
+    band_masks_kernel<float><<<blocks_for(tot), 256, 0, st>>>(
+        ndim, n[0], n[1], n[2], static_cast<const float*>(psi), static_cast<const float*>(grads[0]),
+        ndim > 1 ? static_cast<const float*>(grads[1]) : nullptr,
+        ndim > 2 ? static_cast<const float*>(grads[2]) : nullptr, band, normal[0], m1, m2);
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
+extern "C" int tpf_visc_select(int64_t n, const unsigned char* mask, const void* lo, const void* hi, int mode,
+                               void* out, int dtype, void* stream) {
+  TPF_CHECK_ARG(n >= 0 && lo && out && (!mask || hi), "NULL argument");
+  TPF_CHECK_ARG(mode >= 0 && mode <= 2, "mode must be 0 (set), 1 (accumulate) or 2 (zero plus)");
+  TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
+  if (n == 0) return TPF_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (dtype == TPF_F64)
+    select_kernel<double><<<blocks_for(n), 256, 0, st>>>(n, mask, static_cast<const double*>(lo),
+                                                         static_cast<const double*>(hi), mode, static_cast<double*>(out));
+  else
+    select_kernel<float><<<blocks_for(n), 256, 0, st>>>(n, mask, static_cast<const float*>(lo),
+                                                        static_cast<const float*>(hi), mode, static_cast<float*>(out));
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
+extern "C" int tpf_visc_band_finalize(int64_t n, const unsigned char* band, const void* nt, const void* lap,
+                                      const void* mu, const void* rho, double re, void* out, int dtype, void* stream) {
+  TPF_CHECK_ARG(n >= 0 && band && nt && lap && mu && rho && out && re != 0.0, "NULL argument or zero Re");
+  TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
+  if (n == 0) return TPF_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (dtype == TPF_F64)
+    band_finalize_kernel<double><<<blocks_for(n), 256, 0, st>>>(
+        n, band, static_cast<const double*>(nt), static_cast<const double*>(lap), static_cast<const double*>(mu),
+        static_cast<const double*>(rho), re, static_cast<double*>(out));
+  else
+    band_finalize_kernel<float><<<blocks_for(n), 256, 0, st>>>(
+        n, band, static_cast<const float*>(nt), static_cast<const float*>(lap), static_cast<const float*>(mu),
+        static_cast<const float*>(rho), re, static_cast<float*>(out));
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
+// ---------------------------------------------------------------------------
 // Predictor combinations of PicardCNAdvance.advance
 // (src/twophase/time_integration/cn_advance/picard_cn.py:43-96) and of the
 // explicit branch of ViscousTerm.apply_cn_predictor (ns_terms/viscous.py:161-167):

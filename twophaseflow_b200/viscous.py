@@ -84,8 +84,6 @@ class ViscousTerm:
 
     def compute_explicit(self, velocity_components: List, mu, rho, ccd, psi=None) -> List:
         torch = _torch()
-        if psi is not None and self.spatial_scheme == "ccd_bulk":
-            raise NotImplementedError("the interface-band viscous scheme (psi given) is not built on the B200 path")
         dtype = getattr(ccd, "dtype", torch.float64)
         vs = [to_device(v, dtype=dtype) for v in velocity_components]
         vel = [v.tensor for v in vs]
@@ -105,6 +103,9 @@ class ViscousTerm:
                                                _lib.dptr(m) if m is not None else None, 1 if accumulate else 0,
                                                1 if finalize else 0, _lib.dptr(rt), float(self.Re), _lib.dptr(total),
                                                tdt, st))
+
+        if psi is not None and self.spatial_scheme == "ccd_bulk":
+            return [vs[c].out(v) for c, v in enumerate(self._band_evaluate(vel, mt, rt, psi, ccd, lowfd, dtype))]
 
         # each velocity gradient du_i/dx_j is needed twice (as du_a/dx_b for
         # component a and as du_b/dx_a for component b): computed once
@@ -138,6 +139,58 @@ class ViscousTerm:
                     lowfd(total, be, a, b, mt, accumulate=be > 0, finalize=last)
             out.append(vs[al].out(total))
         return out
+
+    def _band_evaluate(self, vel, mt, rt, psi, ccd, lowfd, dtype) -> List:
+        """ccd_bulk with psi (viscous_spatial.py:50-64,158-221): inside the
+        interface band the stress divergence whose derivatives are low-order
+        along each node's normal axis and CCD along the others; outside it
+        mu times the CCD Laplacian; both / (Re rho)."""
+        torch = _torch()
+        lib = self.lib
+        st = _lib.current_stream_handle()
+        tdt = _lib.TPF_F64 if dtype == torch.float64 else _lib.TPF_F32
+        nd = len(vel)
+        n = vel[0].numel()
+        p = to_device(psi, dtype=dtype).tensor
+
+        def low(arr, ax):
+            out = torch.empty_like(arr)
+            lowfd(out, ax, arr)
+            return out
+
+        def select(mask, lo, hi, mode, out):
+            _lib.check(lib.tpf_visc_select(n, _lib.dptr(mask) if mask is not None else None, _lib.dptr(lo),
+                                           _lib.dptr(hi) if hi is not None else None, mode, _lib.dptr(out), tdt, st))
+
+        gpsi = [low(p, a) for a in range(nd)]
+        band = torch.empty(p.shape, dtype=torch.uint8, device=p.device)
+        normal = [torch.empty_like(band) for _ in range(nd)]
+        shape = (C.c_int64 * nd)(*[int(x) for x in p.shape])
+        _lib.check(lib.tpf_visc_band_masks(nd, shape, _lib.dptr(p), (C.c_void_p * nd)(*[_lib.dptr(g) for g in gpsi]),
+                                           _lib.dptr(band), (C.c_void_p * nd)(*[_lib.dptr(m) for m in normal]),
+                                           tdt, st))
+
+        def switch(data, ax):
+            out = torch.empty_like(data)
+            select(normal[ax], low(data, ax), ccd.first_derivative(data, ax), 0, out)
+            return out
+
+        outs = []
+        for al in range(nd):
+            nt = torch.empty_like(vel[al])
+            for be in range(nd):
+                stress = torch.empty_like(vel[al])
+                _lib.check(lib.tpf_visc_stress(n, _lib.dptr(mt), _lib.dptr(switch(vel[al], be)),
+                                               _lib.dptr(switch(vel[be], al)), _lib.dptr(stress), tdt, st))
+                select(normal[be], low(stress, be), ccd.first_derivative(stress, be), 2 if be == 0 else 1, nt)
+            lap = torch.empty_like(vel[al])
+            for ax in range(nd):
+                select(None, ccd.second_derivative(vel[al], ax), None, 2 if ax == 0 else 1, lap)
+            out = torch.empty_like(vel[al])
+            _lib.check(lib.tpf_visc_band_finalize(n, _lib.dptr(band), _lib.dptr(nt), _lib.dptr(lap), _lib.dptr(mt),
+                                                  _lib.dptr(rt), float(self.Re), _lib.dptr(out), tdt, st))
+            outs.append(out)
+        return outs
 
     def _evaluate(self, vel: List, mu, rho, ccd, psi=None) -> List:
         return self.compute_explicit(vel, mu, rho, ccd, psi=psi)
