@@ -213,6 +213,17 @@ int tpf_fccd_product(int64_t n, const void* u, const void* phi, void* prod, int 
  * second derivative of prod along the axis; h = the uniform node spacing.
  * accumulate = 0 writes 0 + (-div) (the first axis), 1 adds to acc.  acc must
  * not alias prod or q. */
+/* Option C node gradient along one axis (FCCDSolver.node_gradient,
+ * fccd.py:392-462, with the face gradient of :243-277): face gradients
+ * (u_{j+1} - u_j)/H - (H/24)(q_{j+1} - q_j), then at the nodes
+ * 0.5 (d_L + d_R) - (H/16)(q_{i+1} - q_{i-1}); wall nodes 0 and N take their
+ * one face gradient; periodic axes wrap over the N unique nodes and node N
+ * repeats node 0.  q = the CCD second derivative of u along the axis.
+ * mode 0: out = gradient; 1: out = 0 - uk * gradient; 2: out -= uk *
+ * gradient (the nodal advection sum, fccd_advection_helpers.py:46-72).
+ * out must not alias u, q or uk. */
+int tpf_fccd_node_gradient_axis(int ndim, const int64_t* shape, int axis, int periodic, double h, const void* u,
+                                const void* q, const void* uk, int mode, void* out, int dtype, void* stream);
 int tpf_fccd_flux_divergence_axis(int ndim, const int64_t* shape, int axis, int periodic, double h,
                                   const void* prod, const void* q, int accumulate, void* acc, int dtype,
                                   void* stream);

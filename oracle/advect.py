@@ -4,6 +4,9 @@
   -sum_k div(P_f(u_k phi)) (reference ``src/twophase/ccd/fccd_advection_helpers.py:8-72``,
   face value ``ccd/fccd.py:279-299``, face slices ``:213-233``, face divergence
   ``:464-520``) on the oracle's CCD second derivative.
+* ``node_gradient`` / ``node_rhs`` -- Option C: the R_4 Hermite node gradient
+  and the nodal right-hand side -sum_k u_k grad_k phi (``ccd/fccd.py:392-462``,
+  ``fccd_advection_helpers.py:46-72``).
 * ``advance`` -- one TVD-RK3 level-set step with clip and periodic image sync
   (``levelset/fccd_advection.py:86-129``, ``time_integration/tvd_rk3.py:26-48``,
   ``core/boundary.py:116-133``).
@@ -69,6 +72,54 @@ def flux_rhs(vel, scalar, L, N, bc: str):
     return out
 
 
+def node_gradient(u, q, ax: int, H: float, periodic: bool):
+    """Option C R_4 node gradient (fccd.py:90-94,131-134,243-277,392-462):
+    face gradients (u_hi - u_lo)/H - (H/24)(q_hi - q_lo), then
+    0.5 (d_L + d_R) - (H/16)(q_{i+1} - q_{i-1}); wall nodes take their one
+    face gradient, periodic node N repeats node 0."""
+    a = np.moveaxis(np.asarray(u), ax, 0)
+    qa = np.moveaxis(np.asarray(q), ax, 0)
+    N = a.shape[0] - 1
+    inv_H, h24, h16 = 1.0 / H, H / 24.0, H / 16.0
+    if periodic:
+        lo, hi = a[:N], np.roll(a[:N], -1, axis=0)
+        qlo, qhi = qa[:N], np.roll(qa[:N], -1, axis=0)
+    else:
+        lo, hi, qlo, qhi = a[:-1], a[1:], qa[:-1], qa[1:]
+    d = (hi - lo) * inv_H - h24 * (qhi - qlo)
+    out = np.empty_like(a)
+    if periodic:
+        qu = qa[:N]
+        g = 0.5 * (np.roll(d, 1, axis=0) + d) - h16 * (np.roll(qu, -1, axis=0) - np.roll(qu, 1, axis=0))
+        out[:N] = g
+        out[N] = g[0]
+    else:
+        out[1:N] = 0.5 * (d[:-1] + d[1:]) - h16 * (qa[2:] - qa[:-2])
+        out[0] = d[0]
+        out[N] = d[N - 1]
+    return np.moveaxis(out, 0, ax)
+
+
+def node_rhs(vel, scalar, L, N, bc: str):
+    """advection_rhs(..., mode='node'): -sum_k u_k (R_4 grad_k phi)
+    (fccd_advection_helpers.py:46-72)."""
+    nd = len(vel)
+    kinds = axis_kinds(bc, nd)
+    H = [float(np.linspace(0.0, L[a], N[a] + 1)[1]) for a in range(nd)]
+    h = [float(L[a] / N[a]) for a in range(nd)]
+    targets = [scalar] if scalar is not None else list(vel)
+    out = []
+    for phi in targets:
+        phi = np.asarray(phi, dtype=np.float64)
+        acc = np.zeros_like(phi)
+        for k in range(nd):
+            per = kinds[k] == "periodic"
+            q = occd.differentiate(phi, k, h[k], bc="periodic" if per else "wall")[1]
+            acc -= np.asarray(vel[k]) * node_gradient(phi, q, k, H[k], per)
+        out.append(acc)
+    return out
+
+
 def sync_images(a, bc: str):
     for ax, kind in enumerate(axis_kinds(bc, a.ndim)):
         if kind == "periodic":
@@ -80,7 +131,7 @@ def sync_images(a, bc: str):
     return a
 
 
-def advance(psi, vel, dt: float, L, N, bc: str, clip=(0.0, 1.0)):
+def advance(psi, vel, dt: float, L, N, bc: str, clip=(0.0, 1.0), mode: str = "flux"):
     q0 = sync_images(np.array(psi, dtype=np.float64, copy=True), bc)
     if all(not np.any(np.asarray(v)) for v in vel):
         # the reference's CPU backend skips the stages for an exactly zero
@@ -93,7 +144,8 @@ def advance(psi, vel, dt: float, L, N, bc: str, clip=(0.0, 1.0)):
             q = np.clip(q, clip[0], clip[1])
         return sync_images(q, bc)
 
-    R = lambda q: flux_rhs(vel, q, L, N, bc)[0]
+    rhs = node_rhs if mode == "node" else flux_rhs
+    R = lambda q: rhs(vel, q, L, N, bc)[0]
     q1 = P(q0 + dt * R(q0))
     q2 = P(0.75 * q0 + 0.25 * (q1 + dt * R(q1)))
     return P((1.0 / 3.0) * q0 + (2.0 / 3.0) * (q2 + dt * R(q2)))

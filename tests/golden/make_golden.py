@@ -449,6 +449,16 @@ def make_advect(out):
         uc = UCCD6ConvectionTerm(be, grid, ccd, sigma=1.0e-3).compute(vel)
         for a in range(len(N)):
             out[f"{name}/uccd6_{a}"] = np.asarray(uc[a])
+        # Option C (mode="node"): R_4 Hermite node gradients and the nodal
+        # advection right-hand sides, and one TVD-RK3 step in that mode
+        for a in range(len(N)):
+            out[f"{name}/node_grad_psi{a}"] = np.asarray(fccd.node_gradient(psi, a))
+        out[f"{name}/rhs_scalar_node"] = np.asarray(fccd.advection_rhs(vel, scalar=psi, mode="node")[0])
+        mom = fccd.advection_rhs(vel, mode="node")
+        for a in range(len(N)):
+            out[f"{name}/rhs_mom_node{a}"] = np.asarray(mom[a])
+        adv_n = FCCDLevelSetAdvection(be, grid, fccd, mode="node")
+        out[f"{name}/psi_new_node"] = np.asarray(adv_n.advance(psi.copy(), vel, dt))
 
 
 def make_reinit(out):

@@ -51,6 +51,55 @@ def test_rhs_matches_reference(cuda_device, golden, name):
 
 
 @pytest.mark.parametrize("name", CASES)
+def test_node_mode_matches_reference(cuda_device, golden, name):
+    """Option C (mode="node"): node gradients, nodal right-hand sides and one
+    RK3 step against the reference's own outputs."""
+    from twophaseflow_b200 import FCCDLevelSetAdvection
+    N, grid, fccd = _setup(golden, name)
+    vel = [golden[f"{name}/u{a}"] for a in range(len(N))]
+    psi = golden[f"{name}/psi"]
+    for a in range(len(N)):
+        g = fccd.node_gradient(psi, a)
+        ref = golden[f"{name}/node_grad_psi{a}"]
+        assert np.abs(g - ref).max() <= TOL * np.abs(ref).max(), (a, np.abs(g - ref).max())
+    r = fccd.advection_rhs(vel, scalar=psi, mode="node")[0]
+    ref = golden[f"{name}/rhs_scalar_node"]
+    assert np.abs(r - ref).max() <= TOL * np.abs(ref).max()
+    mom = fccd.advection_rhs(vel, mode="node")
+    for a in range(len(N)):
+        ref = golden[f"{name}/rhs_mom_node{a}"]
+        assert np.abs(mom[a] - ref).max() <= TOL * np.abs(ref).max()
+    out = FCCDLevelSetAdvection(None, grid, fccd, mode="node").advance(psi.copy(), vel, float(golden[f"{name}/dt"]))
+    assert np.abs(out - golden[f"{name}/psi_new_node"]).max() <= 1e-12
+
+
+@pytest.mark.parametrize("shape,periodic", [((1025, 1025), False), ((129, 130, 131), True)])
+def test_node_gradient_kernel_bit_exact(cuda_device, shape, periodic):
+    """The Option C kernel alone on every axis, given the oracle's operands:
+    bit-identical gradient and accumulation."""
+    import torch
+    from twophaseflow_b200 import _lib
+    rng = np.random.default_rng(29)
+    u, q, uk = (rng.standard_normal(shape) for _ in range(3))
+    U, Q, K = (torch.from_numpy(a).cuda() for a in (u, q, uk))
+    out = torch.empty_like(U)
+    acc = torch.empty_like(U)
+    sh = (C.c_int64 * len(shape))(*shape)
+    lib = _lib.load()
+    ref_acc = np.zeros(shape)
+    for ax in range(len(shape)):
+        H = 1.0 / (shape[ax] - 1) * (1.0 + 0.25 * ax)
+        for mode, dst in ((0, out), (1 if ax == 0 else 2, acc)):
+            _lib.check(lib.tpf_fccd_node_gradient_axis(len(shape), sh, ax, int(periodic), H, _lib.dptr(U),
+                                                       _lib.dptr(Q), _lib.dptr(K), mode, _lib.dptr(dst),
+                                                       _lib.TPF_F64, _lib.current_stream_handle()))
+        g = oa.node_gradient(u, q, ax, H, periodic)
+        np.testing.assert_array_equal(out.cpu().numpy(), g)
+        ref_acc = ref_acc - uk * g
+    np.testing.assert_array_equal(acc.cpu().numpy(), ref_acc)
+
+
+@pytest.mark.parametrize("name", CASES)
 def test_rk3_step_matches_reference(cuda_device, golden, name):
     from twophaseflow_b200 import FCCDLevelSetAdvection
     N, grid, fccd = _setup(golden, name)

@@ -35,6 +35,26 @@ def test_rk3_step_matches_reference(name):
     np.testing.assert_array_equal(oa.advance(psi, vel, dt, L, N, bc, clip=None), G[f"{name}/psi_new_noclip"])
 
 
+@pytest.mark.parametrize("name", CASES)
+def test_node_mode_matches_reference(name):
+    """Option C: node gradients, the nodal right-hand sides and one RK3 step in
+    node mode, bit for bit."""
+    N, L, bc, vel, psi, dt = _case(name)
+    from oracle import ccd as occd
+    from oracle.levelset import axis_kinds
+    kinds = axis_kinds(bc, len(N))
+    for a in range(len(N)):
+        H = float(np.linspace(0.0, L[a], N[a] + 1)[1])
+        q = occd.differentiate(psi, a, float(L[a] / N[a]), bc=kinds[a])[1]
+        np.testing.assert_array_equal(oa.node_gradient(psi, q, a, H, kinds[a] == "periodic"),
+                                      G[f"{name}/node_grad_psi{a}"])
+    np.testing.assert_array_equal(oa.node_rhs(vel, psi, L, N, bc)[0], G[f"{name}/rhs_scalar_node"])
+    mom = oa.node_rhs(vel, None, L, N, bc)
+    for a in range(len(N)):
+        np.testing.assert_array_equal(mom[a], G[f"{name}/rhs_mom_node{a}"])
+    np.testing.assert_array_equal(oa.advance(psi, vel, dt, L, N, bc, mode="node"), G[f"{name}/psi_new_node"])
+
+
 def test_flux_form_conserves_on_a_periodic_box():
     """sum over the unique nodes of -div(F) vanishes (telescoping faces)."""
     rng = np.random.default_rng(3)

@@ -9,6 +9,10 @@ the TVD-RK3 level-set step, with the reference's classes and signatures.
   ccd/fccd_advection_helpers.py:16-72 composes it.  Per axis: one product
   kernel, one CCD line solve for the second derivative of the product (the
   B200 CCD kernels), one face-value + divergence kernel that accumulates.
+  ``mode="node"`` (Option C) is -sum_k u_k (R_4 grad_k phi) instead: per axis
+  one CCD second derivative of phi and one kernel that forms the face
+  gradients, the Hermite node gradient and the accumulation;
+  ``node_gradient(u, axis, q=None)`` is that gradient alone (fccd.py:392-462).
 * ``FCCDLevelSetAdvection(backend, grid, fccd, mode="flux",
   mass_correction=False).advance(psi, velocity_components, dt,
   clip_bounds=(0, 1))`` -- one TVD-RK3 step (levelset/fccd_advection.py:86-129,
@@ -86,36 +90,54 @@ class FCCDSolver:
             phi.dim(), self._shape(phi), axis, 1 if self._axes[axis] == "periodic" else 0, self._H[axis],
             _lib.dptr(prod), _lib.dptr(q), 1 if accumulate else 0, _lib.dptr(acc), self._tdt(phi), st))
 
-    def _rhs_tensors(self, vel: List, scalar=None):
+    def _node_into(self, out, phi, axis: int, mode: int, u_k=None, q=None):
+        """Option C: out = the R_4 node gradient of phi (mode 0), or
+        out (=, -=) u_k * gradient (modes 1, 2) (fccd.py:392-462)."""
+        if q is None:
+            q = self._ccd.second_derivative(phi, axis)
+        _lib.check(self.lib.tpf_fccd_node_gradient_axis(
+            phi.dim(), self._shape(phi), axis, 1 if self._axes[axis] == "periodic" else 0, self._H[axis],
+            _lib.dptr(phi), _lib.dptr(q), _lib.dptr(u_k) if u_k is not None else None, mode, _lib.dptr(out),
+            self._tdt(phi), _lib.current_stream_handle()))
+
+    def _rhs_tensors(self, vel: List, scalar=None, mode: str = "flux"):
         torch = _torch()
         ndim = len(vel)
         prod = torch.empty_like(vel[0])
-        if scalar is not None:
-            acc = torch.empty_like(scalar)
-            for k in range(ndim):
-                self._flux_into(acc, vel[k], scalar, k, k > 0, prod)
-            return [acc]
+        fields = [scalar] if scalar is not None else vel
         out = []
-        for j in range(ndim):
-            acc = torch.empty_like(vel[j])
+        for phi in fields:
+            acc = torch.empty_like(phi)
             for k in range(ndim):
-                self._flux_into(acc, vel[k], vel[j], k, k > 0, prod)
+                if mode == "node":   # acc -= u_k * R_4 grad_k phi (fccd_advection_helpers.py:53-69)
+                    self._node_into(acc, phi, k, 1 if k == 0 else 2, u_k=vel[k])
+                else:
+                    self._flux_into(acc, vel[k], phi, k, k > 0, prod)
             out.append(acc)
         return out
+
+    def node_gradient(self, u, axis: int, q=None):
+        """4th-order node gradient by R_4 Hermite reconstruction of the FCCD
+        face gradients (fccd.py:392-462): O(H^4) inside, the one-sided face
+        gradient on wall nodes; ``q`` the CCD second derivative if known."""
+        torch = _torch()
+        v = to_device(u, dtype=self.dtype)
+        qt = to_device(q, dtype=self.dtype).tensor if q is not None else None
+        out = torch.empty_like(v.tensor)
+        self._node_into(out, v.tensor, axis, 0, q=qt)
+        return v.out(out)
 
     def advection_rhs(self, velocity_components: List, scalar=None, mode: str = "flux", *,
                       skip_zero_check: bool = False) -> List:
         """-(u.grad) u per component (scalar None) or [-u.grad psi] (fccd.py:523-563)."""
         if mode not in ("node", "flux"):
             raise ValueError(f"mode must be 'node' or 'flux', got {mode!r}")
-        if mode == "node":
-            raise NotImplementedError("the B200 FCCD operator implements the flux form (Option B)")
         vs = [to_device(v, dtype=self.dtype) for v in velocity_components]
         vel = [v.tensor for v in vs]
         if scalar is not None:
             sv = to_device(scalar, dtype=self.dtype)
-            return [sv.out(t) for t in self._rhs_tensors(vel, sv.tensor)]
-        return [vs[j].out(t) for j, t in enumerate(self._rhs_tensors(vel))]
+            return [sv.out(t) for t in self._rhs_tensors(vel, sv.tensor, mode)]
+        return [vs[j].out(t) for j, t in enumerate(self._rhs_tensors(vel, None, mode))]
 
 
 class FCCDLevelSetAdvection:
@@ -125,8 +147,6 @@ class FCCDLevelSetAdvection:
     def __init__(self, backend, grid, fccd: FCCDSolver, mode: str = "flux", mass_correction: bool = False):
         if mode not in ("node", "flux"):
             raise ValueError(f"mode must be 'node' or 'flux', got {mode!r}")
-        if mode == "node":
-            raise NotImplementedError("the B200 FCCD transport implements the flux form (Option B)")
         self._backend = backend
         self.xp = getattr(backend, "xp", None)
         self._grid = grid
@@ -192,7 +212,7 @@ class FCCDLevelSetAdvection:
         else:
             q = q0
         for stage, ca, cb in coeffs:
-            L = fccd._rhs_tensors(vel, q)[0]
+            L = fccd._rhs_tensors(vel, q, self._mode)[0]
             nxt = torch.empty_like(q0)
             _lib.check(lib.tpf_tvd_rk3_stage(q0.dim(), shape, per, stage, ca, cb, float(dt), _lib.dptr(q0),
                                              _lib.dptr(q), _lib.dptr(L), 1 if clip else 0, lo, hi, _lib.dptr(nxt),

@@ -281,6 +281,79 @@ extern "C" int tpf_fccd_flux_divergence_axis(int ndim, const int64_t* shape, int
   return TPF_OK;
 }
 
+// Option C node gradient (FCCDSolver.node_gradient, fccd.py:90-94,131-134,
+// 243-277,392-462): face gradients d_f = (u_hi - u_lo)/H - (H/24)(q_hi - q_lo)
+// and the R_4 Hermite reconstruction 0.5 (d_L + d_R) - (H/16)(q_{i+1} -
+// q_{i-1}) at the nodes; wall nodes 0 and N take their one face gradient,
+// periodic axes wrap over the N unique nodes and node N repeats node 0.
+// mode 0: out = g; 1: out = 0 - uk g (the first term of the nodal advection
+// sum, fccd_advection_helpers.py:46-72); 2: out -= uk g.
+template <typename T>
+__global__ void fccd_node_grad_kernel(int64_t outer, int64_t n, int64_t inner, int periodic, double inv_h, double h24,
+                                      double h16, const T* u, const T* q, const T* uk, int mode, T* out) {
+  const int64_t tot = outer * n * inner, N = n - 1;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t in = i % inner, k = (i / inner) % n, o = i / (inner * n);
+    const int64_t base = o * n * inner + in;
+    auto at = [&](const T* f, int64_t j) { return (double)f[base + j * inner]; };
+    // face gradient between nodes j and j+1 (periodic: j+1 wraps over N unique nodes)
+    auto dface = [&](int64_t j) {
+      const int64_t jp = periodic ? (j + 1 == N ? 0 : j + 1) : j + 1;
+      return rn_sub(rn_mul(rn_sub(at(u, jp), at(u, j)), inv_h), rn_mul(h24, rn_sub(at(q, jp), at(q, j))));
+    };
+    double g;
+    if (periodic) {
+      const int64_t kk = (k == N) ? 0 : k;
+      const int64_t km = (kk == 0) ? N - 1 : kk - 1, kp = (kk + 1 == N) ? 0 : kk + 1;
+      g = rn_sub(rn_mul(0.5, rn_add(dface(km), dface(kk))), rn_mul(h16, rn_sub(at(q, kp), at(q, km))));
+    } else if (k == 0) {
+      g = dface(0);
+    } else if (k == N) {
+      g = dface(N - 1);
+    } else {
+      g = rn_sub(rn_mul(0.5, rn_add(dface(k - 1), dface(k))), rn_mul(h16, rn_sub(at(q, k + 1), at(q, k - 1))));
+    }
+    if (mode == 0) {
+      out[i] = (T)g;
+    } else {
+      const double prev = (mode == 1) ? 0.0 : (double)out[i];
+      out[i] = (T)rn_sub(prev, rn_mul((double)uk[i], g));
+    }
+  }
+}
+
+extern "C" int tpf_fccd_node_gradient_axis(int ndim, const int64_t* shape, int axis, int periodic, double h,
+                                           const void* u, const void* q, const void* uk, int mode, void* out,
+                                           int dtype, void* stream) {
+  TPF_CHECK_ARG(ndim >= 1 && ndim <= 3 && shape && axis >= 0 && axis < ndim, "invalid shape or axis");
+  TPF_CHECK_ARG(u && q && out && out != u && out != q && (mode == 0 || (uk && out != uk)), "NULL or aliased argument");
+  TPF_CHECK_ARG(mode >= 0 && mode <= 2, "mode must be 0 (gradient), 1 (0 - uk g) or 2 (out -= uk g)");
+  TPF_CHECK_ARG(h > 0.0, "h must be positive");
+  TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
+  int64_t outer = 1, inner = 1;
+  for (int d = 0; d < ndim; ++d) {
+    TPF_CHECK_ARG(shape[d] >= 1, "empty axis");
+    if (d < axis) outer *= shape[d];
+    if (d > axis) inner *= shape[d];
+  }
+  const int64_t n = shape[axis];
+  TPF_CHECK_ARG(n >= (periodic ? 3 : 2), "too few nodes along the axis (%lld)", (long long)n);
+  // the reference's constants: 1/H, H/24, H/16 (fccd_helpers.py:23-35)
+  const double inv_h = 1.0 / h, h24 = h / 24.0, h16 = h / 16.0;
+  const int64_t tot = outer * n * inner;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (dtype == TPF_F64)
+    fccd_node_grad_kernel<double><<<blocks_for(tot, 16), 256, 0, st>>>(
+        outer, n, inner, periodic ? 1 : 0, inv_h, h24, h16, static_cast<const double*>(u),
+        static_cast<const double*>(q), static_cast<const double*>(uk), mode, static_cast<double*>(out));
+  else
+    fccd_node_grad_kernel<float><<<blocks_for(tot, 16), 256, 0, st>>>(
+        outer, n, inner, periodic ? 1 : 0, inv_h, h24, h16, static_cast<const float*>(u),
+        static_cast<const float*>(q), static_cast<const float*>(uk), mode, static_cast<float*>(out));
+  TPF_CUDA_TRY(cudaGetLastError());
+  return TPF_OK;
+}
+
 extern "C" int tpf_tvd_rk3_stage(int ndim, const int64_t* shape, const int* periodic, int stage, double ca, double cb,
                                  double dt, const void* q0, const void* q, const void* L, int clip, double lo,
                                  double hi, void* out, int dtype, void* stream) {
