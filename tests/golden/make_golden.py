@@ -555,6 +555,42 @@ def make_viscous(out):
             out[f"{name}/pred_rich{a}"] = np.asarray(u[a])
 
 
+def make_viscous_nonuniform(out):
+    """ViscousTerm.compute_explicit on an interface-fitted (non-uniform) 2-D
+    wall grid, the three spatial schemes (separate file so the uniform
+    cases' arrays stay as they are)."""
+    from twophase.backend import Backend
+    from twophase.config import GridConfig
+    from twophase.core.grid import Grid
+    from twophase.ccd.ccd_solver import CCDSolver
+    from twophase.levelset.heaviside import heaviside
+    from twophase.ns_terms.viscous import ViscousTerm
+
+    be = Backend(use_gpu=False)
+    N = 32
+    grid = Grid(GridConfig(ndim=2, N=(N, N), L=(1.0, 1.0), alpha_grid=2.0, eps_g_factor=2.0), be)
+    ccd = CCDSolver(grid, be, bc_type="wall")
+    X, Y = grid.meshgrid()
+    grid.update_from_levelset(heaviside(np, X - 0.5, 0.5 / N), 0.5 / N, ccd=ccd)
+    ccd = CCDSolver(grid, be, bc_type="wall")
+    rng = np.random.default_rng(4242)
+    vel = [rng.standard_normal(grid.shape) for _ in range(2)]
+    mu = 0.01 + rng.uniform(0.0, 1.0, grid.shape)
+    rho = 0.001 + rng.uniform(0.0, 1.0, grid.shape)
+    out["N"] = np.array((N, N))
+    for ax in range(2):
+        out[f"J{ax}"] = np.asarray(grid.J[ax], dtype=np.float64)
+        out[f"dJ{ax}"] = np.asarray(grid.dJ_dxi[ax], dtype=np.float64)
+        out[f"coords{ax}"] = np.asarray(grid.coords[ax])
+        out[f"u{ax}"] = vel[ax]
+    out["mu"] = mu
+    out["rho"] = rho
+    for scheme in ("ccd_bulk", "conservative_stress", "ccd_stress_legacy"):
+        v = ViscousTerm(be, 100.0, spatial_scheme=scheme).compute_explicit(vel, mu, rho, ccd)
+        for a in range(2):
+            out[f"{scheme}/v{a}"] = np.asarray(v[a])
+
+
 def make_predictor(out):
     """Two consecutive AB2 + IPC predictor steps of the reference (forward Euler
     convection, then AB2), CN and explicit viscous, CSF and GFM."""
@@ -725,7 +761,7 @@ def make_checkpoint(out):
 
 
 def main():
-    """Usage: make_golden.py <reference src dir> [only: ccd|ppe|step|levelset|rhiechow|advect|reinit|viscous|predictor|fccd_ppe|c1|checkpoint ...].
+    """Usage: make_golden.py <reference src dir> [only: ccd|ppe|step|levelset|rhiechow|advect|reinit|viscous|viscous_nonuniform|predictor|fccd_ppe|c1|checkpoint ...].
 
     The source directory comes from the first argument or, when the
     argument list is empty, from the TWOPHASE_REFERENCE_SRC environment variable."""
@@ -741,7 +777,8 @@ def main():
     makers = {"ccd": make_ccd, "ppe": make_ppe, "step": make_step, "levelset": make_levelset,
               "rhiechow": make_rhiechow, "advect": make_advect, "reinit": make_reinit,
               "viscous": make_viscous, "predictor": make_predictor,
-              "fccd_ppe": make_fccd_ppe, "c1": make_c1, "checkpoint": make_checkpoint}
+              "fccd_ppe": make_fccd_ppe, "c1": make_c1, "checkpoint": make_checkpoint,
+              "viscous_nonuniform": make_viscous_nonuniform}
     for key, fn in makers.items():
         if only and key not in only:
             continue

@@ -66,9 +66,9 @@ class ViscousTerm:
         node coordinates, as the reference evaluates them (viscous_spatial.py:70-104)."""
         import numpy as np
         torch = _torch()
-        key = (tuple(grid.N), tuple(float(x) for x in grid.L), axis)
+        coords = np.asarray(grid.coords[axis], dtype=float)
+        key = (axis, coords.tobytes())   # the coordinates themselves: non-uniform grids of equal N, L differ
         if key not in self._coef:
-            coords = np.asarray(grid.coords[axis], dtype=float)
             dx = coords[1:] - coords[:-1]
             h_l, h_r = dx[:-1], dx[1:]
             cl = -(h_r / (h_l * (h_l + h_r)))
@@ -180,8 +180,11 @@ class ViscousTerm:
             nt = torch.empty_like(vel[al])
             for be in range(nd):
                 stress = torch.empty_like(vel[al])
-                _lib.check(lib.tpf_visc_stress(n, _lib.dptr(mt), _lib.dptr(switch(vel[al], be)),
-                                               _lib.dptr(switch(vel[be], al)), _lib.dptr(stress), tdt, st))
+                # both gradients held by name until the stress kernel is queued (a temporary
+                # freed after dptr() would hand its memory to the second one)
+                ga, gb = switch(vel[al], be), switch(vel[be], al)
+                _lib.check(lib.tpf_visc_stress(n, _lib.dptr(mt), _lib.dptr(ga), _lib.dptr(gb), _lib.dptr(stress),
+                                               tdt, st))
                 select(normal[be], low(stress, be), ccd.first_derivative(stress, be), 2 if be == 0 else 1, nt)
             lap = torch.empty_like(vel[al])
             for ax in range(nd):
