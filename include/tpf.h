@@ -224,9 +224,27 @@ int tpf_fccd_product(int64_t n, const void* u, const void* phi, void* prod, int 
  * out must not alias u, q or uk. */
 int tpf_fccd_node_gradient_axis(int ndim, const int64_t* shape, int axis, int periodic, double h, const void* u,
                                 const void* q, const void* uk, int mode, void* out, int dtype, void* stream);
+/* The same on a non-uniform axis (the reference's array weights,
+ * fccd_helpers.py:8-52): face_inv_h[f] = 1/H_f and face_h_24[f] = H_f/24 for
+ * the N faces (H_f = x_{f+1} - x_f), node_h_16[i] = H_node_i/16 for the N+1
+ * nodes (H_node = (H_{i-1} + H_i)/2 inside, H_0 and H_{N-1} at the ends);
+ * device arrays in FP64. */
+int tpf_fccd_node_gradient_axis_nonuniform(int ndim, const int64_t* shape, int axis, int periodic,
+                                           const double* face_inv_h, const double* face_h_24,
+                                           const double* node_h_16, const void* u, const void* q, const void* uk,
+                                           int mode, void* out, int dtype, void* stream);
 int tpf_fccd_flux_divergence_axis(int ndim, const int64_t* shape, int axis, int periodic, double h,
                                   const void* prod, const void* q, int accumulate, void* acc, int dtype,
                                   void* stream);
+/* The same on a non-uniform axis (fccd.py:279-299,464-520 with array
+ * weights): face_h2_16[f] = H_f H_f / 16 for the N faces; node_inv_width =
+ * 1 / ((H_{i-1} + H_i)/2) for the interior nodes i = 1..N-1 of a wall axis
+ * (N-1 values) or for the N unique nodes of a periodic axis (H_{-1} = H_{N-1});
+ * device arrays in FP64. */
+int tpf_fccd_flux_divergence_axis_nonuniform(int ndim, const int64_t* shape, int axis, int periodic,
+                                             const double* face_h2_16, const double* node_inv_width,
+                                             const void* prod, const void* q, int accumulate, void* acc, int dtype,
+                                             void* stream);
 
 /* One TVD-RK3 stage (src/twophase/time_integration/tvd_rk3.py:26-48) with the
  * post-stage clip to [lo, hi] (clip != 0) and periodic image sync of

@@ -591,6 +591,48 @@ def make_viscous_nonuniform(out):
             out[f"{scheme}/v{a}"] = np.asarray(v[a])
 
 
+def make_fccd_nonuniform(out):
+    """FCCD advection right-hand sides (flux and node forms), node gradients
+    and one TVD-RK3 step (both forms) on an interface-fitted (non-uniform)
+    2-D wall grid."""
+    from twophase.backend import Backend
+    from twophase.config import GridConfig
+    from twophase.core.grid import Grid
+    from twophase.ccd.ccd_solver import CCDSolver
+    from twophase.ccd.fccd import FCCDSolver
+    from twophase.levelset.fccd_advection import FCCDLevelSetAdvection
+    from twophase.levelset.heaviside import heaviside
+
+    be = Backend(use_gpu=False)
+    N = 32
+    grid = Grid(GridConfig(ndim=2, N=(N, N), L=(1.0, 1.0), alpha_grid=2.0, eps_g_factor=2.0), be)
+    ccd = CCDSolver(grid, be, bc_type="wall")
+    X, Y = grid.meshgrid()
+    grid.update_from_levelset(heaviside(np, np.sqrt((X - 0.5) ** 2 + (Y - 0.5) ** 2) - 0.25, 0.5 / N), 0.5 / N,
+                              ccd=ccd)
+    ccd = CCDSolver(grid, be, bc_type="wall")
+    fccd = FCCDSolver(grid, be, bc_type="wall", ccd_solver=ccd)
+    X, Y = np.meshgrid(grid.coords[0], grid.coords[1], indexing="ij")
+    psi = np.asarray(heaviside(np, np.sqrt((X - 0.5) ** 2 + (Y - 0.5) ** 2) - 0.25, 1.5 / N))
+    rng = np.random.default_rng(777)
+    vel = [0.5 * rng.standard_normal(grid.shape) + 0.3 * np.cos(2 * np.pi * (Y if a == 0 else X)) for a in range(2)]
+    out["N"] = np.array((N, N))
+    for ax in range(2):
+        out[f"J{ax}"] = np.asarray(grid.J[ax], dtype=np.float64)
+        out[f"dJ{ax}"] = np.asarray(grid.dJ_dxi[ax], dtype=np.float64)
+        out[f"coords{ax}"] = np.asarray(grid.coords[ax])
+        out[f"u{ax}"] = vel[ax]
+        out[f"node_grad_psi{ax}"] = np.asarray(fccd.node_gradient(psi, ax))
+    out["psi"] = psi
+    for mode in ("flux", "node"):
+        out[f"rhs_scalar_{mode}"] = np.asarray(fccd.advection_rhs(vel, scalar=psi, mode=mode)[0])
+        mom = fccd.advection_rhs(vel, mode=mode)
+        for a in range(2):
+            out[f"rhs_mom_{mode}{a}"] = np.asarray(mom[a])
+        out[f"psi_new_{mode}"] = np.asarray(FCCDLevelSetAdvection(be, grid, fccd, mode=mode).advance(psi.copy(), vel,
+                                                                                                    0.004))
+
+
 def make_predictor(out):
     """Two consecutive AB2 + IPC predictor steps of the reference (forward Euler
     convection, then AB2), CN and explicit viscous, CSF and GFM."""
@@ -761,7 +803,7 @@ def make_checkpoint(out):
 
 
 def main():
-    """Usage: make_golden.py <reference src dir> [only: ccd|ppe|step|levelset|rhiechow|advect|reinit|viscous|viscous_nonuniform|predictor|fccd_ppe|c1|checkpoint ...].
+    """Usage: make_golden.py <reference src dir> [only: ccd|ppe|step|levelset|rhiechow|advect|reinit|viscous|viscous_nonuniform|fccd_nonuniform|predictor|fccd_ppe|c1|checkpoint ...].
 
     The source directory comes from the first argument or, when the
     argument list is empty, from the TWOPHASE_REFERENCE_SRC environment variable."""
@@ -778,7 +820,7 @@ def main():
               "rhiechow": make_rhiechow, "advect": make_advect, "reinit": make_reinit,
               "viscous": make_viscous, "predictor": make_predictor,
               "fccd_ppe": make_fccd_ppe, "c1": make_c1, "checkpoint": make_checkpoint,
-              "viscous_nonuniform": make_viscous_nonuniform}
+              "viscous_nonuniform": make_viscous_nonuniform, "fccd_nonuniform": make_fccd_nonuniform}
     for key, fn in makers.items():
         if only and key not in only:
             continue

@@ -361,3 +361,33 @@ def test_uccd6_accumulate_kernel_bit_exact(cuda_device):
         a = (np.zeros(shape) if first else acc0) - 0.5 * (uk * d1 + cons)
         a = a - 3.7e-9 * (np.abs(uk).max() * d8)
         np.testing.assert_array_equal(acc.cpu().numpy(), a)
+
+
+def test_fccd_nonuniform_grid_matches_reference(cuda_device):
+    """Flux and node forms, node gradients and one RK3 step of each on the
+    reference's interface-fitted 32^2 wall grid (cell widths 0.024..0.049;
+    tests/golden/fccd_nonuniform_golden.npz): the reference's per-face and
+    per-node weights, the CCD second derivatives with the grid metric."""
+    from types import SimpleNamespace
+    from twophaseflow_b200 import CCDSolver, FCCDLevelSetAdvection, FCCDSolver
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "fccd_nonuniform_golden.npz"))
+    N = tuple(int(n) for n in g["N"])
+    grid = SimpleNamespace(N=N, ndim=2, L=(1.0, 1.0), shape=tuple(n + 1 for n in N), uniform=False,
+                           J=[g["J0"], g["J1"]], dJ_dxi=[g["dJ0"], g["dJ1"]], coords=[g["coords0"], g["coords1"]])
+    fccd = FCCDSolver(grid, None, bc_type="wall", ccd_solver=CCDSolver(grid, None, bc_type="wall"))
+    vel, psi = [g["u0"], g["u1"]], g["psi"]
+
+    def close(a, ref, tol=TOL):
+        assert np.abs(a - ref).max() <= tol * np.abs(ref).max(), np.abs(a - ref).max() / np.abs(ref).max()
+
+    for a in range(2):
+        close(fccd.node_gradient(psi, a), g[f"node_grad_psi{a}"])
+    for mode in ("flux", "node"):
+        close(fccd.advection_rhs(vel, scalar=psi, mode=mode)[0], g[f"rhs_scalar_{mode}"])
+        mom = fccd.advection_rhs(vel, mode=mode)
+        for a in range(2):
+            close(mom[a], g[f"rhs_mom_{mode}{a}"])
+        out = FCCDLevelSetAdvection(None, grid, fccd, mode=mode).advance(psi.copy(), vel, 0.004)
+        assert np.abs(out - g[f"psi_new_{mode}"]).max() <= 1e-11
+    with pytest.raises(NotImplementedError, match="wall axes"):
+        FCCDSolver(grid, None, bc_type="periodic")

@@ -127,6 +127,12 @@ SIGNATURES = {
     "tpf_fccd_ppe_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_void_p]),
     "tpf_fccd_product": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "tpf_fccd_node_gradient_axis_nonuniform": (C.c_int, [C.c_int, C.POINTER(C.c_int64), C.c_int, C.c_int, C.c_void_p,
+                                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                           C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
+    "tpf_fccd_flux_divergence_axis_nonuniform": (C.c_int, [C.c_int, C.POINTER(C.c_int64), C.c_int, C.c_int,
+                                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                                             C.c_void_p, C.c_int, C.c_void_p]),
     "tpf_fccd_node_gradient_axis": (C.c_int, [C.c_int, C.POINTER(C.c_int64), C.c_int, C.c_int, C.c_double, C.c_void_p,
                                                 C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "tpf_fccd_flux_divergence_axis": (C.c_int, [C.c_int, C.POINTER(C.c_int64), C.c_int, C.c_int, C.c_double,

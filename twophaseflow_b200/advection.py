@@ -45,7 +45,9 @@ def _torch():
 
 
 class FCCDSolver:
-    """Face-centred compact operator on a B200 ``CCDSolver`` (uniform grids)."""
+    """Face-centred compact operator on a B200 ``CCDSolver`` (uniform grids,
+    and non-uniform grids with wall axes: the reference's per-face and
+    per-node weights, the CCD derivatives with the grid metric)."""
 
     def __init__(self, grid, backend=None, bc_type: str = "wall", ccd_solver=None):
         from .ccd import CCDSolver
@@ -57,12 +59,31 @@ class FCCDSolver:
         self._axes = boundary_axes(bc_type, self.ndim)
         if ccd_solver is not None and boundary_axes(getattr(ccd_solver, "bc_type", bc_type), self.ndim) != self._axes:
             raise ValueError("FCCD and CCD solvers must share the same boundary topology")
-        if not getattr(grid, "uniform", True):
-            raise NotImplementedError("the B200 FCCD operator covers uniform grids")
+        self._uniform = bool(getattr(grid, "uniform", True))
+        if not self._uniform and any(a == "periodic" for a in self._axes):
+            raise NotImplementedError("the B200 FCCD operator covers non-uniform grids on wall axes")
         self._ccd = ccd_solver if ccd_solver is not None else CCDSolver(grid, backend, bc_type=bc_type)
         # H = x_1 - x_0 of the node coordinates, as the reference's weights take it
         self._H = [float(grid.coords[ax][1] - grid.coords[ax][0]) for ax in range(self.ndim)]
+        self._w = [self._nonuniform_weights(ax) for ax in range(self.ndim)] if not self._uniform else None
         self.lib = _lib.load()
+
+    def _nonuniform_weights(self, ax: int):
+        """The reference's array weights of a non-uniform wall axis
+        (fccd_helpers.py:8-52), computed on the host in the same order:
+        H_f^2/16, 1/H_node (interior nodes), 1/H_f, H_f/24, H_node/16."""
+        import numpy as np
+        torch = _torch()
+        H = np.asarray(self.grid.coords[ax], dtype=np.float64)
+        H = H[1:] - H[:-1]
+        node = np.zeros(len(H) + 1)
+        node[1:-1] = 0.5 * (H[:-1] + H[1:])
+        node[0] = H[0]
+        node[-1] = H[-1]
+        arrays = {"face_h2_16": H * H / 16.0, "node_inv_width": 1.0 / (0.5 * (H[:-1] + H[1:])),
+                  "face_inv_h": 1.0 / H, "face_h_24": H / 24.0, "node_h_16": node / 16.0}
+        dev = torch.device("cuda", torch.cuda.current_device())
+        return {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in arrays.items()}
 
     @property
     def dtype(self):
@@ -86,8 +107,15 @@ class FCCDSolver:
         _lib.check(self.lib.tpf_fccd_product(phi.numel(), _lib.dptr(u_k), _lib.dptr(phi), _lib.dptr(prod),
                                              self._tdt(phi), st))
         q = self._ccd.second_derivative(prod, axis)
+        per = 1 if self._axes[axis] == "periodic" else 0
+        if self._w is not None:
+            w = self._w[axis]
+            _lib.check(self.lib.tpf_fccd_flux_divergence_axis_nonuniform(
+                phi.dim(), self._shape(phi), axis, per, _lib.dptr(w["face_h2_16"]), _lib.dptr(w["node_inv_width"]),
+                _lib.dptr(prod), _lib.dptr(q), 1 if accumulate else 0, _lib.dptr(acc), self._tdt(phi), st))
+            return
         _lib.check(self.lib.tpf_fccd_flux_divergence_axis(
-            phi.dim(), self._shape(phi), axis, 1 if self._axes[axis] == "periodic" else 0, self._H[axis],
+            phi.dim(), self._shape(phi), axis, per, self._H[axis],
             _lib.dptr(prod), _lib.dptr(q), 1 if accumulate else 0, _lib.dptr(acc), self._tdt(phi), st))
 
     def _node_into(self, out, phi, axis: int, mode: int, u_k=None, q=None):
@@ -95,10 +123,18 @@ class FCCDSolver:
         out (=, -=) u_k * gradient (modes 1, 2) (fccd.py:392-462)."""
         if q is None:
             q = self._ccd.second_derivative(phi, axis)
+        per = 1 if self._axes[axis] == "periodic" else 0
+        uk = _lib.dptr(u_k) if u_k is not None else None
+        st = _lib.current_stream_handle()
+        if self._w is not None:
+            w = self._w[axis]
+            _lib.check(self.lib.tpf_fccd_node_gradient_axis_nonuniform(
+                phi.dim(), self._shape(phi), axis, per, _lib.dptr(w["face_inv_h"]), _lib.dptr(w["face_h_24"]),
+                _lib.dptr(w["node_h_16"]), _lib.dptr(phi), _lib.dptr(q), uk, mode, _lib.dptr(out), self._tdt(phi), st))
+            return
         _lib.check(self.lib.tpf_fccd_node_gradient_axis(
-            phi.dim(), self._shape(phi), axis, 1 if self._axes[axis] == "periodic" else 0, self._H[axis],
-            _lib.dptr(phi), _lib.dptr(q), _lib.dptr(u_k) if u_k is not None else None, mode, _lib.dptr(out),
-            self._tdt(phi), _lib.current_stream_handle()))
+            phi.dim(), self._shape(phi), axis, per, self._H[axis], _lib.dptr(phi), _lib.dptr(q), uk, mode,
+            _lib.dptr(out), self._tdt(phi), st))
 
     def _rhs_tensors(self, vel: List, scalar=None, mode: str = "flux"):
         torch = _torch()

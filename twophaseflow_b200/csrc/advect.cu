@@ -35,6 +35,8 @@ struct FluxArgs {
   int64_t outer, n, inner;
   double inv_h, h2_16;
   int periodic, accumulate;
+  const double* wf;   // non-uniform: H_f^2 / 16 per face f (else h2_16)
+  const double* wn;   // non-uniform: 1 / node width per node (wall: nodes 1..N-1 at k-1; periodic: N) (else inv_h)
 };
 
 template <typename T>
@@ -43,9 +45,16 @@ __device__ __forceinline__ double ldv(const void* p, int64_t i) { return (double
 // face value between nodes j and j+1 (fccd.py:279-299):
 // 0.5 (u_j + u_{j+1}) - (H^2/16) (q_j + q_{j+1})
 template <typename T>
-__device__ __forceinline__ double face_val(const FluxArgs& a, int64_t il, int64_t ir) {
+__device__ __forceinline__ double face_val(const FluxArgs& a, int64_t il, int64_t ir, int64_t f) {
+  const double c = a.wf ? a.wf[f] : a.h2_16;
   return rn_sub(rn_mul(0.5, rn_add(ldv<T>(a.prod, il), ldv<T>(a.prod, ir))),
-                rn_mul(a.h2_16, rn_add(ldv<T>(a.q, il), ldv<T>(a.q, ir))));
+                rn_mul(c, rn_add(ldv<T>(a.q, il), ldv<T>(a.q, ir))));
+}
+
+// 1 / width of node k (periodic: the unique node k; wall: interior node k)
+__device__ __forceinline__ double node_inv_w(const FluxArgs& a, int64_t k) {
+  if (!a.wn) return a.inv_h;
+  return a.periodic ? a.wn[k] : a.wn[k - 1];
 }
 
 template <typename T>
@@ -65,14 +74,14 @@ __device__ __forceinline__ double flux_div_node(const FluxArgs& a, int64_t base,
   if (a.periodic) {
     const int64_t kk = (k == N) ? 0 : k;
     const int64_t kp = (kk == N - 1) ? 0 : kk + 1, km = (kk == 0) ? N - 1 : kk - 1;
-    const double fr = face_val<T>(a, base + kk * s, base + kp * s);
-    const double fl = face_val<T>(a, base + km * s, base + kk * s);
-    return rn_mul(rn_sub(fr, fl), a.inv_h);
+    const double fr = face_val<T>(a, base + kk * s, base + kp * s, kk);
+    const double fl = face_val<T>(a, base + km * s, base + kk * s, km);
+    return rn_mul(rn_sub(fr, fl), node_inv_w(a, kk));
   }
   if (k == 0 || k == N) return 0.0;
-  const double fr = face_val<T>(a, base + k * s, base + (k + 1) * s);
-  const double fl = face_val<T>(a, base + (k - 1) * s, base + k * s);
-  return rn_mul(rn_sub(fr, fl), a.inv_h);
+  const double fr = face_val<T>(a, base + k * s, base + (k + 1) * s, k);
+  const double fl = face_val<T>(a, base + (k - 1) * s, base + k * s, k - 1);
+  return rn_mul(rn_sub(fr, fl), node_inv_w(a, k));
 }
 
 // one thread per node (contiguous or short-stride axes: the neighbours are in
@@ -114,25 +123,25 @@ __global__ void __launch_bounds__(256) flux_march_kernel(FluxArgs a, int64_t chu
       auto fleft = [&](int64_t k) {
         const int64_t kk = (k == N) ? 0 : k;
         const int64_t km = (kk == 0) ? N - 1 : kk - 1;
-        return face_val<T>(a, base + km * s, base + kk * s);
+        return face_val<T>(a, base + km * s, base + kk * s, km);
       };
       double fl = fleft(k0);
       for (int64_t k = k0; k < k1; ++k) {
         const int64_t kk = (k == N) ? 0 : k;
         const int64_t kp = (kk == N - 1) ? 0 : kk + 1;
-        const double fr = (k == N) ? face_val<T>(a, base, base + kp * s) : face_val<T>(a, base + kk * s, base + kp * s);
+        const double fr = (k == N) ? face_val<T>(a, base, base + kp * s, 0) : face_val<T>(a, base + kk * s, base + kp * s, kk);
         const double old = a.accumulate ? (double)static_cast<const T*>(a.acc)[base + k * s] : 0.0;
         const double flk = (k == N) ? fleft(N) : fl;
-        const double c2 = -rn_mul(rn_sub(fr, flk), a.inv_h);
+        const double c2 = -rn_mul(rn_sub(fr, flk), node_inv_w(a, kk));
         static_cast<T*>(a.acc)[base + k * s] = (T)rn_add(old, c2);
         fl = fr;
       }
     } else {
-      double fl = (k0 >= 1) ? face_val<T>(a, base + (k0 - 1) * s, base + k0 * s) : 0.0;
+      double fl = (k0 >= 1) ? face_val<T>(a, base + (k0 - 1) * s, base + k0 * s, k0 - 1) : 0.0;
       for (int64_t k = k0; k < k1; ++k) {
-        const double fr = (k < N) ? face_val<T>(a, base + k * s, base + (k + 1) * s) : 0.0;
+        const double fr = (k < N) ? face_val<T>(a, base + k * s, base + (k + 1) * s, k) : 0.0;
         const double old = a.accumulate ? (double)static_cast<const T*>(a.acc)[base + k * s] : 0.0;
-        const double div = (k == 0 || k == N) ? 0.0 : rn_mul(rn_sub(fr, fl), a.inv_h);
+        const double div = (k == 0 || k == N) ? 0.0 : rn_mul(rn_sub(fr, fl), node_inv_w(a, k));
         static_cast<T*>(a.acc)[base + k * s] = (T)rn_add(old, -div);
         fl = fr;
       }
@@ -228,15 +237,18 @@ extern "C" int tpf_fccd_product(int64_t n, const void* u, const void* phi, void*
   return TPF_OK;
 }
 
-extern "C" int tpf_fccd_flux_divergence_axis(int ndim, const int64_t* shape, int axis, int periodic, double h,
-                                             const void* prod, const void* q, int accumulate, void* acc, int dtype,
-                                             void* stream) {
+// the face-value + divergence launch of both entry points below; wf / wn
+// NULL on uniform grids (h then gives the constants)
+static int flux_divergence_axis(int ndim, const int64_t* shape, int axis, int periodic, double h, const double* wf,
+                                const double* wn, const void* prod, const void* q, int accumulate, void* acc,
+                                int dtype, void* stream) {
   TPF_CHECK_ARG(ndim >= 1 && ndim <= 3 && shape && axis >= 0 && axis < ndim, "invalid shape or axis");
   TPF_CHECK_ARG(prod && q && acc && acc != prod && acc != q, "NULL or aliased argument");
   TPF_CHECK_ARG(h > 0.0, "h must be positive");
   TPF_CHECK_ARG(dtype == TPF_F64 || dtype == TPF_F32, "dtype must be TPF_F64 or TPF_F32");
   FluxArgs a{};
   a.prod = prod; a.q = q; a.acc = acc;
+  a.wf = wf; a.wn = wn;
   a.outer = 1; a.inner = 1;
   for (int d = 0; d < ndim; ++d) {
     TPF_CHECK_ARG(shape[d] >= 1, "empty axis");
@@ -270,7 +282,8 @@ extern "C" int tpf_fccd_flux_divergence_axis(int ndim, const int64_t* shape, int
       return cudaPeekAtLastError() == cudaSuccess ? TPF_OK : TPF_ECUDA;
     };
     auto cand = [&](int c, void* scratch, cudaStream_t s2) { return launch(kChunks[c], scratch, s2); };
-    const tpf::TuneKey key{tpf::kTuneFluxMarch, dtype, {a.outer, a.n, a.inner, 2 * a.periodic + a.accumulate}};
+    const tpf::TuneKey key{tpf::kTuneFluxMarch, dtype,
+                           {a.outer, a.n, a.inner, 2 * a.periodic + a.accumulate + (wf ? 4 : 0)}};
     const int pick = tpf::tuned_choice(key, 5, -1, (size_t)tot * (dtype == TPF_F64 ? 8 : 4), st, cand);
     launch(pick >= 0 ? kChunks[pick] : chunk, a.acc, st);
   } else {
@@ -279,6 +292,22 @@ extern "C" int tpf_fccd_flux_divergence_axis(int ndim, const int64_t* shape, int
   }
   TPF_CUDA_TRY(cudaGetLastError());
   return TPF_OK;
+}
+
+extern "C" int tpf_fccd_flux_divergence_axis(int ndim, const int64_t* shape, int axis, int periodic, double h,
+                                             const void* prod, const void* q, int accumulate, void* acc, int dtype,
+                                             void* stream) {
+  return flux_divergence_axis(ndim, shape, axis, periodic, h, nullptr, nullptr, prod, q, accumulate, acc, dtype,
+                              stream);
+}
+
+extern "C" int tpf_fccd_flux_divergence_axis_nonuniform(int ndim, const int64_t* shape, int axis, int periodic,
+                                                        const double* face_h2_16, const double* node_inv_width,
+                                                        const void* prod, const void* q, int accumulate, void* acc,
+                                                        int dtype, void* stream) {
+  TPF_CHECK_ARG(face_h2_16 && node_inv_width, "NULL weight array");
+  return flux_divergence_axis(ndim, shape, axis, periodic, 1.0, face_h2_16, node_inv_width, prod, q, accumulate, acc,
+                              dtype, stream);
 }
 
 // Option C node gradient (FCCDSolver.node_gradient, fccd.py:90-94,131-134,
@@ -290,7 +319,8 @@ extern "C" int tpf_fccd_flux_divergence_axis(int ndim, const int64_t* shape, int
 // sum, fccd_advection_helpers.py:46-72); 2: out -= uk g.
 template <typename T>
 __global__ void fccd_node_grad_kernel(int64_t outer, int64_t n, int64_t inner, int periodic, double inv_h, double h24,
-                                      double h16, const T* u, const T* q, const T* uk, int mode, T* out) {
+                                      double h16, const double* winv, const double* w24, const double* w16,
+                                      const T* u, const T* q, const T* uk, int mode, T* out) {
   const int64_t tot = outer * n * inner, N = n - 1;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t in = i % inner, k = (i / inner) % n, o = i / (inner * n);
@@ -299,19 +329,21 @@ __global__ void fccd_node_grad_kernel(int64_t outer, int64_t n, int64_t inner, i
     // face gradient between nodes j and j+1 (periodic: j+1 wraps over N unique nodes)
     auto dface = [&](int64_t j) {
       const int64_t jp = periodic ? (j + 1 == N ? 0 : j + 1) : j + 1;
-      return rn_sub(rn_mul(rn_sub(at(u, jp), at(u, j)), inv_h), rn_mul(h24, rn_sub(at(q, jp), at(q, j))));
+      const double ih = winv ? winv[j] : inv_h, c24 = w24 ? w24[j] : h24;
+      return rn_sub(rn_mul(rn_sub(at(u, jp), at(u, j)), ih), rn_mul(c24, rn_sub(at(q, jp), at(q, j))));
     };
     double g;
     if (periodic) {
       const int64_t kk = (k == N) ? 0 : k;
       const int64_t km = (kk == 0) ? N - 1 : kk - 1, kp = (kk + 1 == N) ? 0 : kk + 1;
-      g = rn_sub(rn_mul(0.5, rn_add(dface(km), dface(kk))), rn_mul(h16, rn_sub(at(q, kp), at(q, km))));
+      g = rn_sub(rn_mul(0.5, rn_add(dface(km), dface(kk))), rn_mul(w16 ? w16[kk] : h16, rn_sub(at(q, kp), at(q, km))));
     } else if (k == 0) {
       g = dface(0);
     } else if (k == N) {
       g = dface(N - 1);
     } else {
-      g = rn_sub(rn_mul(0.5, rn_add(dface(k - 1), dface(k))), rn_mul(h16, rn_sub(at(q, k + 1), at(q, k - 1))));
+      g = rn_sub(rn_mul(0.5, rn_add(dface(k - 1), dface(k))),
+                 rn_mul(w16 ? w16[k] : h16, rn_sub(at(q, k + 1), at(q, k - 1))));
     }
     if (mode == 0) {
       out[i] = (T)g;
@@ -322,9 +354,9 @@ __global__ void fccd_node_grad_kernel(int64_t outer, int64_t n, int64_t inner, i
   }
 }
 
-extern "C" int tpf_fccd_node_gradient_axis(int ndim, const int64_t* shape, int axis, int periodic, double h,
-                                           const void* u, const void* q, const void* uk, int mode, void* out,
-                                           int dtype, void* stream) {
+static int node_gradient_axis(int ndim, const int64_t* shape, int axis, int periodic, double h, const double* winv,
+                              const double* w24, const double* w16, const void* u, const void* q, const void* uk,
+                              int mode, void* out, int dtype, void* stream) {
   TPF_CHECK_ARG(ndim >= 1 && ndim <= 3 && shape && axis >= 0 && axis < ndim, "invalid shape or axis");
   TPF_CHECK_ARG(u && q && out && out != u && out != q && (mode == 0 || (uk && out != uk)), "NULL or aliased argument");
   TPF_CHECK_ARG(mode >= 0 && mode <= 2, "mode must be 0 (gradient), 1 (0 - uk g) or 2 (out -= uk g)");
@@ -344,14 +376,30 @@ extern "C" int tpf_fccd_node_gradient_axis(int ndim, const int64_t* shape, int a
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (dtype == TPF_F64)
     fccd_node_grad_kernel<double><<<blocks_for(tot, 16), 256, 0, st>>>(
-        outer, n, inner, periodic ? 1 : 0, inv_h, h24, h16, static_cast<const double*>(u),
+        outer, n, inner, periodic ? 1 : 0, inv_h, h24, h16, winv, w24, w16, static_cast<const double*>(u),
         static_cast<const double*>(q), static_cast<const double*>(uk), mode, static_cast<double*>(out));
   else
     fccd_node_grad_kernel<float><<<blocks_for(tot, 16), 256, 0, st>>>(
-        outer, n, inner, periodic ? 1 : 0, inv_h, h24, h16, static_cast<const float*>(u),
+        outer, n, inner, periodic ? 1 : 0, inv_h, h24, h16, winv, w24, w16, static_cast<const float*>(u),
         static_cast<const float*>(q), static_cast<const float*>(uk), mode, static_cast<float*>(out));
   TPF_CUDA_TRY(cudaGetLastError());
   return TPF_OK;
+}
+
+extern "C" int tpf_fccd_node_gradient_axis(int ndim, const int64_t* shape, int axis, int periodic, double h,
+                                           const void* u, const void* q, const void* uk, int mode, void* out,
+                                           int dtype, void* stream) {
+  return node_gradient_axis(ndim, shape, axis, periodic, h, nullptr, nullptr, nullptr, u, q, uk, mode, out, dtype,
+                            stream);
+}
+
+extern "C" int tpf_fccd_node_gradient_axis_nonuniform(int ndim, const int64_t* shape, int axis, int periodic,
+                                                      const double* face_inv_h, const double* face_h_24,
+                                                      const double* node_h_16, const void* u, const void* q,
+                                                      const void* uk, int mode, void* out, int dtype, void* stream) {
+  TPF_CHECK_ARG(face_inv_h && face_h_24 && node_h_16, "NULL weight array");
+  return node_gradient_axis(ndim, shape, axis, periodic, 1.0, face_inv_h, face_h_24, node_h_16, u, q, uk, mode, out,
+                            dtype, stream);
 }
 
 extern "C" int tpf_tvd_rk3_stage(int ndim, const int64_t* shape, const int* periodic, int stage, double ca, double cb,
