@@ -285,6 +285,13 @@ int tpf_reinit_compression_flux(int ndim, int64_t n, const void* psi, const void
  * the axis' compression flux; accumulate = 0 writes 0 + it. */
 int tpf_reinit_filtered_divergence_axis(int ndim, const int64_t* shape, int axis, int pad, double eps_d,
                                         const void* g, int accumulate, void* div, int dtype, void* stream);
+/* The same on a non-uniform grid (filtered_divergence, reinit_ops.py:95-105):
+ * g is the CCD derivative in xi-space (no metric) and each filtered value is
+ * multiplied by J[k] (the metric of node k along the axis, FP64 device array)
+ * before it is written or added. */
+int tpf_reinit_filtered_divergence_axis_metric(int ndim, const int64_t* shape, int axis, int pad, double eps_d,
+                                               const double* J, const void* g, int accumulate, void* div, int dtype,
+                                               void* stream);
 
 /* One CN-ADI half-step along one axis (cn_diffusion_axis, reinit_ops.py:169-204):
  * rhs = (M2 + mu B2) in with coefficients cR (off-diagonal), dR (diagonal)

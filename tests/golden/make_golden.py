@@ -633,6 +633,43 @@ def make_fccd_nonuniform(out):
                                                                                                     0.004))
 
 
+def make_reinit_nonuniform(out):
+    """Split reinitialization on an interface-fitted (non-uniform) 2-D wall
+    grid: zero and Neumann ghost padding, with and without mass correction."""
+    from twophase.backend import Backend
+    from twophase.config import GridConfig
+    from twophase.core.grid import Grid
+    from twophase.ccd.ccd_solver import CCDSolver
+    from twophase.levelset.heaviside import heaviside
+    from twophase.levelset.reinit_split import SplitReinitializer
+
+    be = Backend(use_gpu=False)
+    N = 32
+    grid = Grid(GridConfig(ndim=2, N=(N, N), L=(1.0, 1.0), alpha_grid=2.0, eps_g_factor=2.0), be)
+    ccd = CCDSolver(grid, be, bc_type="wall")
+    X, Y = grid.meshgrid()
+    grid.update_from_levelset(heaviside(np, np.sqrt((X - 0.5) ** 2 + (Y - 0.45) ** 2) - 0.3, 0.5 / N), 0.5 / N,
+                              ccd=ccd)
+    ccd = CCDSolver(grid, be, bc_type="wall")
+    X, Y = np.meshgrid(grid.coords[0], grid.coords[1], indexing="ij")
+    rng = np.random.default_rng(9191)
+    psi = np.asarray(heaviside(np, np.sqrt((X - 0.5) ** 2 + (Y - 0.45) ** 2) - 0.3, 2.5 / N))
+    psi = np.clip(psi + 0.02 * rng.standard_normal(grid.shape), 0.0, 1.0)
+    eps = 1.5 / N
+    out["N"] = np.array((N, N))
+    for ax in range(2):
+        out[f"J{ax}"] = np.asarray(grid.J[ax], dtype=np.float64)
+        out[f"dJ{ax}"] = np.asarray(grid.dJ_dxi[ax], dtype=np.float64)
+        out[f"coords{ax}"] = np.asarray(grid.coords[ax])
+        out[f"h{ax}"] = np.asarray(grid.h[ax], dtype=np.float64)
+    out["psi"] = psi
+    out["eps"] = np.array(eps)
+    for tag, bc, mass in (("zero_mass", "zero", True), ("neumann", "neumann", False)):
+        r = SplitReinitializer(be, grid, ccd, eps, n_steps=3, bc=bc, mass_correction=mass)
+        out[f"{tag}/dtau"] = np.array(r.dtau)
+        out[f"{tag}/psi_reinit"] = np.asarray(r.reinitialize(psi.copy()))
+
+
 def make_predictor(out):
     """Two consecutive AB2 + IPC predictor steps of the reference (forward Euler
     convection, then AB2), CN and explicit viscous, CSF and GFM."""
@@ -803,7 +840,7 @@ def make_checkpoint(out):
 
 
 def main():
-    """Usage: make_golden.py <reference src dir> [only: ccd|ppe|step|levelset|rhiechow|advect|reinit|viscous|viscous_nonuniform|fccd_nonuniform|predictor|fccd_ppe|c1|checkpoint ...].
+    """Usage: make_golden.py <reference src dir> [only: ccd|ppe|step|levelset|rhiechow|advect|reinit|reinit_nonuniform|viscous|viscous_nonuniform|fccd_nonuniform|predictor|fccd_ppe|c1|checkpoint ...].
 
     The source directory comes from the first argument or, when the
     argument list is empty, from the TWOPHASE_REFERENCE_SRC environment variable."""
@@ -820,7 +857,8 @@ def main():
               "rhiechow": make_rhiechow, "advect": make_advect, "reinit": make_reinit,
               "viscous": make_viscous, "predictor": make_predictor,
               "fccd_ppe": make_fccd_ppe, "c1": make_c1, "checkpoint": make_checkpoint,
-              "viscous_nonuniform": make_viscous_nonuniform, "fccd_nonuniform": make_fccd_nonuniform}
+              "viscous_nonuniform": make_viscous_nonuniform, "fccd_nonuniform": make_fccd_nonuniform,
+              "reinit_nonuniform": make_reinit_nonuniform}
     for key, fn in makers.items():
         if only and key not in only:
             continue

@@ -391,3 +391,22 @@ def test_fccd_nonuniform_grid_matches_reference(cuda_device):
         assert np.abs(out - g[f"psi_new_{mode}"]).max() <= 1e-11
     with pytest.raises(NotImplementedError, match="wall axes"):
         FCCDSolver(grid, None, bc_type="periodic")
+
+
+@pytest.mark.parametrize("tag,bc,mass", [("zero_mass", "zero", True), ("neumann", "neumann", False)])
+def test_reinit_nonuniform_grid_matches_reference(cuda_device, tag, bc, mass):
+    """Split reinitialization on the reference's interface-fitted 32^2 wall
+    grid (tests/golden/reinit_nonuniform_golden.npz): dtau from the smallest
+    node spacing equal bit for bit, the result within the uniform reinit bar."""
+    from types import SimpleNamespace
+    from twophaseflow_b200 import CCDSolver, SplitReinitializer
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "reinit_nonuniform_golden.npz"))
+    N = tuple(int(n) for n in g["N"])
+    grid = SimpleNamespace(N=N, ndim=2, L=(1.0, 1.0), shape=tuple(n + 1 for n in N), uniform=False,
+                           J=[g["J0"], g["J1"]], dJ_dxi=[g["dJ0"], g["dJ1"]], coords=[g["coords0"], g["coords1"]],
+                           h=[g["h0"], g["h1"]])
+    ccd = CCDSolver(grid, None, bc_type="wall")
+    r = SplitReinitializer(None, grid, ccd, float(g["eps"]), n_steps=3, bc=bc, mass_correction=mass)
+    assert r.dtau == float(g[f"{tag}/dtau"])
+    out = r.reinitialize(g["psi"].copy())
+    assert np.abs(out - g[f"{tag}/psi_reinit"]).max() <= 1e-11, np.abs(out - g[f"{tag}/psi_reinit"]).max()

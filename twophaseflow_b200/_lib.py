@@ -144,6 +144,9 @@ SIGNATURES = {
                                            C.c_void_p]),
     "tpf_reinit_compression_flux": (C.c_int, [C.c_int, C.c_int64, C.c_void_p, C.POINTER(C.c_void_p),
                                               C.POINTER(C.c_void_p), C.c_int, C.c_void_p]),
+    "tpf_reinit_filtered_divergence_axis_metric": (C.c_int, [C.c_int, C.POINTER(C.c_int64), C.c_int, C.c_int,
+                                                               C.c_double, C.c_void_p, C.c_void_p, C.c_int,
+                                                               C.c_void_p, C.c_int, C.c_void_p]),
     "tpf_reinit_filtered_divergence_axis": (C.c_int, [C.c_int, C.POINTER(C.c_int64), C.c_int, C.c_int, C.c_double,
                                                       C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "tpf_reinit_cn_axis": (C.c_int, [C.c_int, C.POINTER(C.c_int64), C.c_int, C.c_double, C.c_double, C.c_void_p,

@@ -287,7 +287,9 @@ def _pad_kind(bc, axis: int) -> int:
 
 
 def _control_widths(grid, axis: int, periodic: bool):
-    """Grid._axis_control_widths (core/grid.py:1158-1170) for a uniform grid."""
+    """Grid._axis_control_widths (core/grid.py:1158-1170): half-cell sums on
+    periodic axes, the node metric spacing ``grid.h`` on wall axes (L/N on a
+    uniform grid without ``h``)."""
     import numpy as np
     coords = np.asarray(grid.coords[axis], dtype=float)
     if periodic:
@@ -296,19 +298,22 @@ def _control_widths(grid, axis: int, periodic: bool):
         w[:-1] = 0.5 * (np.roll(cw, 1) + cw)
         w[-1] = 0.0
         return w
+    if getattr(grid, "h", None) is not None:
+        return np.asarray(grid.h[axis], dtype=float)
     return np.full(grid.N[axis] + 1, grid.L[axis] / grid.N[axis])
 
 
 class SplitReinitializer:
     """Operator-split reinitialization, compression (forward Euler) + CN-ADI
-    diffusion (levelset/reinit_split.py:22-102) on uniform grids."""
+    diffusion (levelset/reinit_split.py:22-102).  On non-uniform grids (as
+    the reference): dtau and the CN factors from the smallest node spacing
+    ``grid.h``, the filtered divergence in xi-space times the metric J, the
+    mass correction over the grid's control volumes."""
 
     def __init__(self, backend, grid, ccd, eps: float, n_steps: int = 4, bc: str = "zero",
                  eps_d_comp: float = 0.05, mass_correction: bool = True):
         import numpy as np
         torch = _torch()
-        if not getattr(grid, "uniform", True):
-            raise NotImplementedError("the B200 reinitializer covers uniform grids")
         self.xp = getattr(backend, "xp", None)
         self.grid = grid
         self.ccd = ccd
@@ -318,7 +323,14 @@ class SplitReinitializer:
         self._eps_d_comp = float(eps_d_comp)
         self._mass_correction = mass_correction
         nd = grid.ndim
-        self._h = [float(grid.L[ax] / grid.N[ax]) for ax in range(nd)]
+        # smallest node spacing per axis (reinit_split.py:64-66); L/N on a uniform grid
+        hs = getattr(grid, "h", None)
+        self._h = [float(np.min(hs[ax])) if hs is not None else float(grid.L[ax] / grid.N[ax]) for ax in range(nd)]
+        self._J = None
+        if not getattr(grid, "uniform", True):
+            dev0 = torch.device("cuda", torch.cuda.current_device())
+            self._J = [torch.from_numpy(np.ascontiguousarray(np.asarray(grid.J[ax], dtype=np.float64))).to(dev0)
+                       for ax in range(nd)]
         # compute_dtau (reinit_ops.py:34-54)
         dx_min = min(self._h)
         eps_min = float(np.min(eps))
@@ -378,10 +390,16 @@ class SplitReinitializer:
                                                        P(*[_lib.dptr(t) for t in flux]), tdt, st))
             div = torch.empty_like(q)
             for ax in range(nd):
-                g = self.ccd.first_derivative(flux[ax], ax)
-                _lib.check(lib.tpf_reinit_filtered_divergence_axis(nd, shape, ax, _pad_kind(self._bc, ax),
-                                                                   self._eps_d_comp, _lib.dptr(g), 1 if ax else 0,
-                                                                   _lib.dptr(div), tdt, st))
+                if self._J is None:
+                    g = self.ccd.first_derivative(flux[ax], ax)
+                    _lib.check(lib.tpf_reinit_filtered_divergence_axis(nd, shape, ax, _pad_kind(self._bc, ax),
+                                                                       self._eps_d_comp, _lib.dptr(g), 1 if ax else 0,
+                                                                       _lib.dptr(div), tdt, st))
+                else:   # xi-space derivative and filter, then J (reinit_ops.py:95-105)
+                    g = self.ccd.first_derivative(flux[ax], ax, apply_metric=False)
+                    _lib.check(lib.tpf_reinit_filtered_divergence_axis_metric(
+                        nd, shape, ax, _pad_kind(self._bc, ax), self._eps_d_comp, _lib.dptr(self._J[ax]),
+                        _lib.dptr(g), 1 if ax else 0, _lib.dptr(div), tdt, st))
             # q* = clip(q - dtau div, 0, 1) with the image nodes synchronised
             q_new = torch.empty_like(q)
             _lib.check(lib.tpf_tvd_rk3_stage(nd, shape, per, 1, 0.0, 0.0, -self.dtau, None, _lib.dptr(q),

@@ -495,7 +495,7 @@ __global__ void compression_flux_kernel(CompArgs a) {
 // core/boundary.py:249-292).
 template <typename T>
 __global__ void filtered_div_kernel(int64_t outer, int64_t n, int64_t inner, int pad, double eps_d, const T* g,
-                                    int accumulate, T* div) {
+                                    const double* J, int accumulate, T* div) {
   const int64_t tot = outer * n * inner;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t k = (i / inner) % n;
@@ -505,7 +505,8 @@ __global__ void filtered_div_kernel(int64_t outer, int64_t n, int64_t inner, int
     else m = pad == 0 ? 0.0 : (pad == 1 ? (double)g[i + (n - 2) * inner] : c);
     if (k < n - 1) p = (double)g[i + inner];
     else p = pad == 0 ? 0.0 : (pad == 1 ? (double)g[i - (n - 2) * inner] : c);
-    const double v = rn_add(c, rn_mul(eps_d, rn_add(rn_sub(p, rn_mul(2.0, c)), m)));
+    double v = rn_add(c, rn_mul(eps_d, rn_add(rn_sub(p, rn_mul(2.0, c)), m)));
+    if (J) v = rn_mul(J[k], v);   // non-uniform: the filter in xi-space, then J (reinit_ops.py:95-105)
     div[i] = (T)(accumulate ? rn_add((double)div[i], v) : rn_add(0.0, v));
   }
 }
@@ -762,9 +763,8 @@ extern "C" int tpf_reinit_compression_flux(int ndim, int64_t n, const void* psi,
   return TPF_OK;
 }
 
-extern "C" int tpf_reinit_filtered_divergence_axis(int ndim, const int64_t* shape, int axis, int pad, double eps_d,
-                                                   const void* g, int accumulate, void* div, int dtype,
-                                                   void* stream) {
+static int filtered_divergence_axis(int ndim, const int64_t* shape, int axis, int pad, double eps_d, const double* J,
+                                    const void* g, int accumulate, void* div, int dtype, void* stream) {
   TPF_CHECK_ARG(ndim >= 1 && ndim <= 3 && shape && axis >= 0 && axis < ndim, "invalid shape or axis");
   TPF_CHECK_ARG(pad >= 0 && pad <= 2, "pad must be 0 (zero), 1 (periodic) or 2 (neumann/outflow)");
   TPF_CHECK_ARG(g && div && g != div, "NULL or aliased argument");
@@ -781,14 +781,27 @@ extern "C" int tpf_reinit_filtered_divergence_axis(int ndim, const int64_t* shap
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (dtype == TPF_F64)
     filtered_div_kernel<double><<<blocks_for(tot, 16), 256, 0, st>>>(outer, n, inner, pad, eps_d,
-                                                                    static_cast<const double*>(g), accumulate,
+                                                                    static_cast<const double*>(g), J, accumulate,
                                                                     static_cast<double*>(div));
   else
     filtered_div_kernel<float><<<blocks_for(tot, 16), 256, 0, st>>>(outer, n, inner, pad, eps_d,
-                                                                   static_cast<const float*>(g), accumulate,
+                                                                   static_cast<const float*>(g), J, accumulate,
                                                                    static_cast<float*>(div));
   TPF_CUDA_TRY(cudaGetLastError());
   return TPF_OK;
+}
+
+extern "C" int tpf_reinit_filtered_divergence_axis(int ndim, const int64_t* shape, int axis, int pad, double eps_d,
+                                                   const void* g, int accumulate, void* div, int dtype,
+                                                   void* stream) {
+  return filtered_divergence_axis(ndim, shape, axis, pad, eps_d, nullptr, g, accumulate, div, dtype, stream);
+}
+
+extern "C" int tpf_reinit_filtered_divergence_axis_metric(int ndim, const int64_t* shape, int axis, int pad,
+                                                          double eps_d, const double* J, const void* g,
+                                                          int accumulate, void* div, int dtype, void* stream) {
+  TPF_CHECK_ARG(J, "NULL metric");
+  return filtered_divergence_axis(ndim, shape, axis, pad, eps_d, J, g, accumulate, div, dtype, stream);
 }
 
 extern "C" int tpf_reinit_cn_axis(int ndim, const int64_t* shape, int axis, double cR, double dR, const double* f,
