@@ -177,12 +177,13 @@ def time_ppe(precision, rho_d, rhs_d, steps, warmup, flush, cg_kernel=0):
     return s, p, times
 
 
-def time_learned(rho_d, rhs_d, steps, warmup, flush):
-    """Network-preconditioned flexible CG (shipped weights, two-level mode), device-resident inputs."""
+def time_learned(rho_d, rhs_d, steps, warmup, flush, outer="fcg"):
+    """Network-preconditioned flexible CG (or flexible GMRES(30) with
+    ``outer='fgmres'``; shipped weights, two-level mode), device-resident inputs."""
     import torch
     from twophaseflow_b200 import UniformGrid
     from twophaseflow_b200.learned import PPESolverLearned
-    cfg = _Cfg(pseudo_tol=TOL, pseudo_maxiter=1_000_000, ppe_learned_maxiter=20000)
+    cfg = _Cfg(pseudo_tol=TOL, pseudo_maxiter=1_000_000, ppe_learned_maxiter=20000, ppe_learned_outer=outer)
     s = PPESolverLearned(None, cfg, UniformGrid(N_PPE))
     for _ in range(warmup):
         s.solve(rhs_d, rho_d)
@@ -439,6 +440,9 @@ def main(argv=None):
     slr, plr, tlr = time_learned(rho_d, rhs_d, max(2, args.steps // 3), 1, flush)
     _barrier(ws)
     dlr = slr.last_diagnostics
+    sgm, pgm, tgm = time_learned(rho_d, rhs_d, 2, 1, flush, outer="fgmres")
+    _barrier(ws)
+    dgm = dict(sgm.last_diagnostics)
     heldout = learned_heldout()
     _barrier(ws)
     ms_mx = _max_over_ranks(float(np.mean(tmx)), ws)
@@ -551,6 +555,9 @@ def main(argv=None):
                              "fp64_us_per_iteration": round(float(np.mean(t64)) * 1e3 / max(1, it64), 2),
                              "global_fp32_kernel_ms": round(float(np.mean(tmg)), 3),
                              "global_fp32_kernel_iterations": dmg["ppe_low_order_cg_iterations"]},
+            "learned_fgmres30": {"ms": round(float(np.mean(tgm)), 3), "iterations": dgm["ppe_learned_iterations"],
+                                 "fell_back": bool(dgm["ppe_learned_fell_back"]),
+                                 "max_rel_diff_vs_fp64": float(f"{float(torch.max(torch.abs(pgm - p64))) / float(torch.max(torch.abs(p64))):.3g}")},
             "learned_detail": {"fallback_iterations": dlr["ppe_learned_fallback_iterations"],
                                "rel_residual": dlr["ppe_learned_relative_residual"],
                                "us_per_iteration": round(ms_lr * 1e3 / max(1, dlr["ppe_learned_iterations"]), 1)},

@@ -661,10 +661,12 @@ typedef struct tpf_learned_options {
   int fallback;         /* 1: finish with plain Jacobi PCG after a stall          */
   int use_graph;        /* 1: replay one iteration as a CUDA graph                */
   int window;           /* stored directions of the truncated flexible CG (1..8) */
+  int outer;            /* outer method: 0 flexible CG, 1 flexible GMRES          */
+  int restart;          /* flexible GMRES restart length (1..128)                 */
 } tpf_learned_options;
 
 typedef struct tpf_lppe_result {
-  int64_t iterations;           /* flexible-CG iterations (network applications)  */
+  int64_t iterations;           /* flexible-CG / -GMRES iterations (network applications) */
   int64_t fallback_iterations;  /* plain PCG iterations after a stall             */
   int64_t restarts;             /* restarts from the true residual                */
   double rel_residual;          /* ||b - S p|| / ||b|| at exit                     */

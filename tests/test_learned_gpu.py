@@ -282,3 +282,54 @@ def test_learned_solve_is_deterministic(cuda_device):
     it2 = s.last_diagnostics["ppe_learned_iterations"]
     assert it1 == it2
     assert torch.equal(p1, p2)
+
+
+@pytest.mark.parametrize("smooth,coarsen,restart", [(1, 1, 30), (1, 4, 30), (2, 1, 7)])
+def test_flexible_gmres_matches_direct_solution(cuda_device, smooth, coarsen, restart):
+    """ppe_learned_outer='fgmres': with all-zero network parameters the
+    preconditioner is a fixed map (damped Jacobi, or the two-grid cycle), so
+    flexible GMRES(restart) must reach the tolerance on the true residual and
+    the direct solution, restarts included (restart 7)."""
+    import torch
+    from twophaseflow_b200 import UniformGrid
+    from twophaseflow_b200.learned import PPESolverLearned, num_params
+    N = (64, 64)
+    rho, rhs = _case(N, seed=3)
+    cfg = _Cfg(pseudo_tol=1e-10, pseudo_maxiter=4000, ppe_learned_smooth=smooth, ppe_learned_fallback=False,
+               ppe_learned_coarsen=coarsen, ppe_learned_outer="fgmres", ppe_learned_restart=restart,
+               ppe_learned_maxiter=4000)
+    s = PPESolverLearned(None, cfg, UniformGrid(N), params=np.zeros(num_params(), np.float32))
+    p = s.solve(torch.from_numpy(rhs).to(cuda_device), torch.from_numpy(rho).to(cuda_device)).cpu().numpy()
+    d = s.last_diagnostics
+    assert d["ppe_learned_info"] == 0 and not d["ppe_learned_fell_back"], d
+    assert d["ppe_learned_relative_residual"] <= 1e-10
+    pd = oppe.spsolve_fvm(rhs, rho, oppe.uniform_coords(N, (1.0, 1.0)))
+    assert np.abs(p - pd).max() <= 1e-7 * np.abs(pd).max()
+    assert p.ravel()[s._pin_dof] == 0.0
+
+
+def test_flexible_gmres_with_trained_network(cuda_device):
+    """The shipped network under flexible GMRES(30) on the held-out 256^2
+    density: converges without the fallback to the flexible CG's solution,
+    deterministically."""
+    import torch
+    from twophaseflow_b200 import UniformGrid
+    from twophaseflow_b200.learned import PPESolverLearned
+    from twophaseflow_b200.workloads import divergence_rhs, droplet_density
+    N = (256, 256)
+    rho = torch.from_numpy(droplet_density(N, seed=101)).to(cuda_device)
+    rhs = torch.from_numpy(divergence_rhs(N, seed=102)).to(cuda_device)
+    base = dict(pseudo_tol=1e-8, pseudo_maxiter=5000, ppe_learned_maxiter=5000, ppe_learned_fallback=False)
+    sg = PPESolverLearned(None, _Cfg(ppe_learned_outer="fgmres", **base), UniformGrid(N))
+    pg = sg.solve(rhs, rho)
+    dg = dict(sg.last_diagnostics)
+    assert dg["ppe_learned_info"] == 0 and not dg["ppe_learned_fell_back"], dg
+    pg2 = sg.solve(rhs, rho)
+    assert torch.equal(pg, pg2) and sg.last_diagnostics["ppe_learned_iterations"] == dg["ppe_learned_iterations"]
+    sc = PPESolverLearned(None, _Cfg(**base), UniformGrid(N))
+    pc = sc.solve(rhs, rho)
+    print("fgmres", dg["ppe_learned_iterations"], "fcg", sc.last_diagnostics["ppe_learned_iterations"])
+    scale = float(torch.max(torch.abs(pc)))
+    assert float(torch.max(torch.abs(pg - pc))) <= 1e-6 * scale
+    with pytest.raises(ValueError, match="ppe_learned_outer"):
+        PPESolverLearned(None, _Cfg(ppe_learned_outer="bicgstab", **base), UniformGrid(N))

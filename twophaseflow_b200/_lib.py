@@ -71,6 +71,8 @@ class tpf_learned_options(C.Structure):
         ("fallback", C.c_int),
         ("use_graph", C.c_int),
         ("window", C.c_int),
+        ("outer", C.c_int),
+        ("restart", C.c_int),
     ]
 
 

@@ -588,3 +588,130 @@ int gmres_solve(GmresWork& W, int restart, double tol, long long maxiter, bool x
 }
 
 }  // namespace
+
+namespace {
+
+// Flexible restarted GMRES (Saad, "A flexible inner-outer preconditioned
+// GMRES algorithm", SIAM J. Sci. Comput. 14, 1993): right preconditioning by
+// a preconditioner that may change from column to column (a network), so
+// z_j = M_j(v_j) is kept in Z (restart columns of n), w = A z_j is
+// orthogonalized against V with the same column kernels as gmres_solve, and
+// a cycle ends with x += Z y.  The Givens estimate is then the
+// unpreconditioned residual norm, so a cycle stops once it meets tol ||b||;
+// each restart starts from the true residual r = b - A x.
+// apply / resid / precond as for gmres_solve; Z: restart * n doubles.
+template <class Apply, class Resid, class Precond>
+int fgmres_solve(GmresWork& W, double* Z, int restart, double tol, long long maxiter, bool x_nonzero,
+                 long long key_a, long long key_b, Apply apply, Resid resid, Precond precond, cudaStream_t s,
+                 GmresOutcome& out) {
+  const int n = W.n;
+  int st;
+  const int m = std::min(restart, n);
+  const int ldh = W.restart_cap + 2;
+  double* H = W.gm;
+  double* givens = H + (size_t)W.restart_cap * ldh;
+  double* S = givens + 2 * W.restart_cap;
+  double* y = S + (W.restart_cap + 1);
+  double* hcol = y + (W.restart_cap + 1);
+  double* hcol2 = hcol + (W.restart_cap + 1);
+  double* wnorm = hcol2 + (W.restart_cap + 1);
+  double* bnorm_d = wnorm + 1;
+  TPF_CUDA_TRY(cudaMemsetAsync(H, 0, sizeof(double) * (size_t)W.restart_cap * ldh, s));
+  TPF_CUDA_TRY(cudaMemsetAsync(W.gst, 0, sizeof(GmState), s));
+  if ((st = gm_norm2(W, W.b, bnorm_d, s))) return st;
+  double bnrm2 = 0.0;
+  if ((st = gm_read_scalar(bnorm_d, &bnrm2, s))) return st;
+  out = GmresOutcome{};
+  out.bnrm2 = bnrm2;
+  if (bnrm2 == 0.0) {
+    TPF_CUDA_TRY(cudaMemsetAsync(W.x, 0, sizeof(double) * n, s));
+    out.converged = true;
+    return TPF_OK;
+  }
+  const double atol = tol * bnrm2;
+  const int nb_dot = std::min(std::min(W.ew_blocks, W.part_len / (m + 2)), std::max(1, 4 * tpf::sm_count()));
+  const int* done = &W.gst->done;
+  auto enqueue_cycle = [&](cudaStream_t cs) -> int {
+    int est;
+    for (int col = 0; col < m; ++col) {
+      const double* vc = W.V + (size_t)col * n;
+      double* zc = Z + (size_t)col * n;
+      if ((est = precond(vc, zc, cs, done))) return est;
+      if ((est = apply(zc, W.w, cs, done))) return est;
+      double* hc = H + (size_t)col * ldh;
+      gs1_kernel<<<nb_dot, 256, 0, cs>>>(n, W.V, col, W.w, W.part, hc, hcol2, W.gst);
+      gs2_kernel<<<nb_dot, 256, 0, cs>>>(n, W.V, col, W.w, hc, W.part, H, ldh, givens, S, hcol2, W.gst);
+      gs3_kernel<<<nb_dot, 256, 0, cs>>>(n, W.V, col, W.w, W.part, H, ldh, givens, S, hcol2, W.gst);
+      gm_scale_kernel<<<W.ew_blocks, 256, 0, cs>>>(n, W.w, W.V + (size_t)(col + 1) * n, W.gst);
+      TPF_CUDA_TRY(cudaGetLastError());
+    }
+    return TPF_OK;
+  };
+  // -m marks the flexible cycle (a different graph from gmres_solve's)
+  const long long key[6] = {-(long long)m, (long long)nb_dot, key_a, key_b, (long long)(intptr_t)Z, (long long)n};
+  long long applies = 0, inner = 0;
+  double rnorm = INFINITY;
+  bool converged = false;
+  if (x_nonzero) {
+    if ((st = resid(W.x, W.r, s))) return st;
+    ++applies;
+  } else {
+    TPF_CUDA_TRY(cudaMemcpyAsync(W.r, W.b, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  }
+  if ((st = gm_norm2(W, W.r, wnorm, s))) return st;
+  if ((st = gm_read_scalar(wnorm, &rnorm, s))) return st;
+  for (long long iteration = 0; iteration < maxiter && !converged; ++iteration) {
+    if (rnorm <= atol) { converged = true; break; }
+    gm_start_kernel<<<W.ew_blocks, 256, 0, s>>>(n, W.r, W.V, S, m + 1, W.gst, rnorm, atol);
+    if (!*W.exec || std::memcmp(W.key, key, sizeof(key)) != 0) {
+      if (*W.exec) { cudaGraphExecDestroy(*W.exec); *W.exec = nullptr; }
+      if (!*W.cap && cudaStreamCreateWithFlags(W.cap, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        *W.cap = nullptr;
+        tpf::set_error("cudaStreamCreate failed");
+        return TPF_ECUDA;
+      }
+      TPF_CUDA_TRY(cudaStreamBeginCapture(*W.cap, cudaStreamCaptureModeThreadLocal));
+      const int cst = enqueue_cycle(*W.cap);
+      cudaGraph_t graph = nullptr;
+      const cudaError_t ce = cudaStreamEndCapture(*W.cap, &graph);
+      if (cst || ce != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        if (cst) return cst;
+        tpf::set_error("capturing the flexible GMRES cycle failed: %s", cudaGetErrorString(ce));
+        return TPF_ECUDA;
+      }
+      const cudaError_t ie = cudaGraphInstantiate(W.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ie != cudaSuccess) {
+        *W.exec = nullptr;
+        cudaGetLastError();
+        tpf::set_error("instantiating the flexible GMRES cycle graph failed: %s", cudaGetErrorString(ie));
+        return TPF_ECUDA;
+      }
+      std::memcpy(W.key, key, sizeof(key));
+    }
+    TPF_CUDA_TRY(cudaGraphLaunch(*W.exec, s));
+    GmState hs{};
+    TPF_CUDA_TRY(cudaMemcpyAsync(&hs, W.gst, sizeof(GmState), cudaMemcpyDeviceToHost, s));
+    TPF_CUDA_TRY(cudaStreamSynchronize(s));
+    inner += hs.ncols;
+    applies += hs.ncols;
+    gm_backsolve_kernel<<<1, 1, 0, s>>>(H, ldh, S, y, W.gst);
+    gm_update_x_kernel<<<W.ew_blocks, 256, 0, s>>>(n, Z, y, W.x, W.gst);
+    if ((st = resid(W.x, W.r, s))) return st;
+    ++applies;
+    if ((st = gm_norm2(W, W.r, wnorm, s))) return st;
+    if ((st = gm_read_scalar(wnorm, &rnorm, s))) return st;
+    if (rnorm <= atol) converged = true;
+    if (hs.breakdown) break;
+  }
+  out.inner = inner;
+  out.applies = applies;
+  out.rnorm = rnorm;
+  out.converged = converged;
+  return TPF_OK;
+}
+
+}  // namespace

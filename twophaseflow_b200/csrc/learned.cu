@@ -24,6 +24,7 @@
 #include "tpf_common.cuh"
 #include "ppe_view.cuh"
 #include "tc_sm100.cuh"
+#include "gmres.cuh"
 
 #include <cuda_bf16.h>
 
@@ -721,6 +722,15 @@ struct tpf_lppe {
   int win = 1;            // window of the current solve
   int graph_win = -1;
   bool have_feat = false;
+  // flexible GMRES outer method: bases V (restart + 1) and Z (restart), the
+  // Hessenberg block, partials, state, residual / operator scratch, graph
+  int gm_cap = 0;
+  double *gV = nullptr, *gZ = nullptr, *ggm = nullptr, *gpart = nullptr, *gr = nullptr, *gw = nullptr,
+         *gt = nullptr;
+  int gpart_len = 0;
+  GmState* ggst = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  long long gkey[6] = {0, 0, 0, 0, 0, 0};
   std::vector<void*> allocs;
 };
 
@@ -808,6 +818,47 @@ int enqueue_precond(tpf_lppe* lp, int smooth, double omega, cudaStream_t s, doub
   return TPF_OK;
 }
 
+// ---- flexible GMRES outer method (fgmres_solve, gmres.cuh) ------------------------------
+
+// the preconditioner's input v (a basis vector) into r, with the partials of
+// its D^-1-weighted norm (the network input scale); nothing once the cycle is done
+__global__ void __launch_bounds__(kRedThreads) fgm_in_kernel(LGrid g, const double* v, const int* gdone, double* r,
+                                                             double* part) {
+  double acc[1] = {0.0};
+  if (!*gdone) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.ndof; i += gridDim.x * blockDim.x) {
+      const double vi = v[i];
+      r[i] = vi;
+      acc[0] += vi * vi * g.dinvS[i];
+    }
+  }
+  block_partials<1>(acc, part);
+}
+
+// the scale s of the network input and the preconditioner kernels' skip flag
+__global__ void fgm_scale_kernel(const double* part, int nb, int ndof, const int* gdone, FcgState* st) {
+  double v[1];
+  reduce_partials<1>(part, nb, v);
+  if (threadIdx.x == 0) {
+    st->done = *gdone;
+    set_scale(st, v[0], ndof);
+  }
+}
+
+__global__ void fgm_out_kernel(int n, const double* z, const int* gdone, double* out) {
+  if (*gdone) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = z[i];
+}
+
+// w = S z with the pinned row w[pin] = z[pin] (z[pin] = 0 on this Krylov space)
+__global__ void fgm_apply_kernel(LGrid g, const double* z, const int* gdone, double* w) {
+  if (gdone && *gdone) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.ndof; i += gridDim.x * blockDim.x) {
+    const int i0 = i / g.n1, i1 = i - i0 * g.n1;
+    w[i] = (i == g.pin) ? z[i] : s_apply(g, z, i, i0, i1);
+  }
+}
+
 // one flexible-CG step with M stored directions (the window length picks the instance)
 template <int M>
 void enqueue_fcg_step(tpf_lppe* lp, const double* z, cudaStream_t s) {
@@ -868,6 +919,78 @@ int build_graph(tpf_lppe* lp, int smooth, double omega) {
   return TPF_OK;
 }
 
+// flexible GMRES workspace for restart length R (kept for the handle's life)
+int ensure_fgmres_work(tpf_lppe* lp, int R) {
+  if (lp->gm_cap >= R) return TPF_OK;
+  const int n = lp->g.ndof;
+  int st;
+  const size_t gm_len = (size_t)R * (R + 2) + 2 * (size_t)R + (size_t)(R + 1) * 4 + 8;
+  const int part_len = (R + 2) * std::max(1, 4 * tpf::sm_count());
+  if ((st = lalloc(lp, &lp->gV, (size_t)(R + 1) * n)) || (st = lalloc(lp, &lp->gZ, (size_t)R * n)) ||
+      (st = lalloc(lp, &lp->ggm, gm_len)) || (st = lalloc(lp, &lp->gpart, (size_t)part_len)) ||
+      (st = lalloc(lp, &lp->gr, (size_t)n)) || (st = lalloc(lp, &lp->gw, (size_t)n)) ||
+      (st = lalloc(lp, &lp->gt, (size_t)n)) || (st = lalloc(lp, &lp->ggst, 1)))
+    return st;
+  if (lp->gexec) {
+    cudaGraphExecDestroy(lp->gexec);
+    lp->gexec = nullptr;
+  }
+  lp->gpart_len = part_len;
+  lp->gm_cap = R;
+  return TPF_OK;
+}
+
+// the learned solve with flexible GMRES(R) as the outer method: the same
+// weighted system and network application as the flexible CG, each basis
+// vector preconditioned by the network (its own input scale), x += Z y per
+// cycle; returns whether the true residual met the tolerance
+int solve_fgmres(tpf_lppe* lp, const tpf_learned_options& o, cudaStream_t s, bool x_nonzero, GmresOutcome& out) {
+  const LGrid& g = lp->g;
+  int st;
+  if ((st = ensure_fgmres_work(lp, o.restart))) return st;
+  GmresWork W;
+  W.n = g.ndof;
+  W.ew_blocks = ew_blocks(g.ndof);
+  W.part_len = lp->gpart_len;
+  W.restart_cap = lp->gm_cap;
+  W.V = lp->gV;
+  W.gm = lp->ggm;
+  W.part = lp->gpart;
+  W.gst = lp->ggst;
+  W.b = lp->b;
+  W.x = lp->x;
+  W.r = lp->gr;
+  W.w = lp->gw;
+  W.t = lp->gt;
+  W.exec = &lp->gexec;
+  W.cap = &lp->cap;
+  W.key = lp->gkey;
+  auto apply = [&](const double* in, double* outv, cudaStream_t cs, const int* done) -> int {
+    fgm_apply_kernel<<<ew_blocks(g.ndof), 256, 0, cs>>>(g, in, done, outv);
+    TPF_CUDA_TRY(cudaGetLastError());
+    return TPF_OK;
+  };
+  auto resid = [&](const double* x, double* r, cudaStream_t cs) -> int {
+    fcg_residual_kernel<<<kRedBlocks, kRedThreads, 0, cs>>>(g, lp->b, x, r, lp->part);
+    TPF_CUDA_TRY(cudaGetLastError());
+    return TPF_OK;
+  };
+  auto precond = [&](const double* in, double* outv, cudaStream_t cs, const int* done) -> int {
+    fgm_in_kernel<<<kRedBlocks, kRedThreads, 0, cs>>>(g, in, done, lp->r, lp->part);
+    fgm_scale_kernel<<<1, 256, 0, cs>>>(lp->part, kRedBlocks, g.ndof, done, lp->st);
+    double* z = nullptr;
+    int est = enqueue_precond(lp, o.smooth, o.omega, cs, &z);
+    if (est) return est;
+    fgm_out_kernel<<<ew_blocks(g.ndof), 256, 0, cs>>>(g.ndof, z, done, outv);
+    TPF_CUDA_TRY(cudaGetLastError());
+    return TPF_OK;
+  };
+  const long long cycles = std::max<long long>(1, (o.maxiter + o.restart - 1) / o.restart);
+  const long long key_a = (long long)o.smooth * 1000003LL + (long long)(o.omega * 1e9);
+  return fgmres_solve(W, lp->gZ, o.restart, o.tol, cycles, x_nonzero, key_a, (long long)(intptr_t)lp->st, apply,
+                      resid, precond, s, out);
+}
+
 int read_state(tpf_lppe* lp, cudaStream_t s) {
   TPF_CUDA_TRY(cudaMemcpyAsync(lp->st_host, lp->st, sizeof(FcgState), cudaMemcpyDeviceToHost, s));
   TPF_CUDA_TRY(cudaStreamSynchronize(s));
@@ -897,6 +1020,8 @@ void tpf_lppe_default_options(tpf_learned_options* o) {
   o->fallback = 1;
   o->use_graph = 1;
   o->window = 8;
+  o->outer = 0;
+  o->restart = 30;
 }
 
 int tpf_lppe_create(tpf_lppe** out, tpf_ppe* ppe, tpf_unet* net, int coarsen) {
@@ -972,6 +1097,7 @@ int tpf_lppe_destroy(tpf_lppe* lp) {
   if (!lp) return TPF_OK;
   cudaDeviceSynchronize();
   if (lp->exec) cudaGraphExecDestroy(lp->exec);
+  if (lp->gexec) cudaGraphExecDestroy(lp->gexec);
   for (void* p : lp->allocs) cudaFree(p);
   if (lp->st_host) cudaFreeHost(lp->st_host);
   if (lp->cap) cudaStreamDestroy(lp->cap);
@@ -1056,6 +1182,8 @@ int tpf_lppe_solve(tpf_lppe* lp, const double* rhs, const double* rho, double* p
   TPF_CHECK_ARG(o.smooth >= 0 && o.smooth <= 8, "smooth must be in [0, 8]");
   TPF_CHECK_ARG(o.check_every >= 1 && o.check_every <= 1024, "check_every must be in [1, 1024]");
   TPF_CHECK_ARG(o.window >= 1 && o.window <= kMaxWin, "window must be in [1, %d]", kMaxWin);
+  TPF_CHECK_ARG(o.outer == 0 || o.outer == 1, "outer must be 0 (flexible CG) or 1 (flexible GMRES)");
+  TPF_CHECK_ARG(o.outer == 0 || (o.restart >= 1 && o.restart <= 128), "restart must be in [1, 128]");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int st;
   if (rho && (st = tpf_lppe_prepare(lp, rho, stream))) return st;
@@ -1068,6 +1196,44 @@ int tpf_lppe_solve(tpf_lppe* lp, const double* rhs, const double* rho, double* p
   lp->win = o.window;
   const LGrid& g = lp->g;
   fcg_init_kernel<<<ew_blocks(g.ndof), 256, 0, s>>>(g, rhs, p_init, lp->b, lp->x);
+
+  if (o.outer == 1) {
+    GmresOutcome out;
+    if ((st = solve_fgmres(lp, o, s, p_init != nullptr, out))) return st;
+    res->iterations = out.inner;
+    res->restarts = out.inner > 0 ? (out.inner + o.restart - 1) / o.restart : 0;
+    res->rel_residual = out.bnrm2 > 0.0 ? out.rnorm / out.bnrm2 : 0.0;
+    copy_x_kernel<<<ew_blocks(g.ndof), 256, 0, s>>>(g.ndof, g.pin, lp->x, p);
+    TPF_CUDA_TRY(cudaGetLastError());
+    TPF_CUDA_TRY(cudaStreamSynchronize(s));
+    if ((st = tpf::unet_check(lp->net, s))) return st;
+    if (out.converged) {
+      res->info = 0;
+      return TPF_OK;
+    }
+    if (o.fallback) {
+      tpf_ppe_options saved{}, po{};
+      tpf::ppe_options(lp->ppe, &saved);
+      po = saved;
+      po.method = TPF_PPE_CG;
+      po.precond = TPF_PRECOND_JACOBI;
+      po.precision = TPF_PREC_F64;
+      po.tol = o.tol;
+      po.maxiter = std::max<int64_t>(o.maxiter, 20000);
+      if ((st = tpf_ppe_set_options(lp->ppe, &po))) return st;
+      tpf_ppe_result pr{};
+      st = tpf_ppe_solve(lp->ppe, rhs, nullptr, p, p, stream, &pr);
+      tpf_ppe_set_options(lp->ppe, &saved);
+      res->fell_back = 1;
+      res->fallback_iterations = pr.iterations;
+      res->rel_residual = pr.rel_residual;
+      res->info = pr.info;
+      return st;
+    }
+    res->info = (int)std::min<long long>(o.maxiter, 0x7fffffff);
+    tpf::set_error("learned flexible GMRES did not converge (info=%d)", res->info);
+    return TPF_ENOCONV;
+  }
 
   if ((st = true_residual(lp, s, o.tol, 1, o.window))) return st;
   if ((st = read_state(lp, s))) return st;

@@ -204,8 +204,12 @@ class PPESolverLearned(PPESolverFVMMatrixFree):
     ``default_coarsen``),
     ``ppe_learned_smooth`` (damped Jacobi sweeps after the network, default 3),
     ``ppe_learned_omega`` (0.8), ``ppe_learned_weights`` (path of the trained
-    parameters) and ``ppe_learned_fallback`` (finish with plain Jacobi PCG on a
-    stall, True).
+    parameters), ``ppe_learned_fallback`` (finish with plain Jacobi PCG on a
+    stall, True) and ``ppe_learned_outer``: 'fcg' (truncated flexible CG with
+    ``ppe_learned_window`` stored directions, default) or 'fgmres' (flexible
+    GMRES with restart ``ppe_learned_restart``, 30: each basis vector
+    preconditioned by the network, the solution built from the preconditioned
+    basis).
     """
 
     scheme_names = ("fvm_learned",)
@@ -225,6 +229,11 @@ class PPESolverLearned(PPESolverFVMMatrixFree):
         self.fallback = bool(getattr(solver_cfg, "ppe_learned_fallback", True))
         self.learned_maxiter = int(getattr(solver_cfg, "ppe_learned_maxiter", max(self.maxiter, 2000)))
         self.window = int(getattr(solver_cfg, "ppe_learned_window", 8))
+        outer = str(getattr(solver_cfg, "ppe_learned_outer", "fcg")).strip().lower()
+        if outer not in ("fcg", "fgmres"):
+            raise ValueError("ppe_learned_outer must be 'fcg' (flexible CG) or 'fgmres' (flexible GMRES)")
+        self.outer = outer
+        self.restart = int(getattr(solver_cfg, "ppe_learned_restart", 30))
         meta = {}
         if params is None:
             wpath = str(getattr(solver_cfg, "ppe_learned_weights", DEFAULT_WEIGHTS))
@@ -267,6 +276,8 @@ class PPESolverLearned(PPESolverFVMMatrixFree):
         o.omega = self.omega
         o.fallback = 1 if self.fallback else 0
         o.window = self.window
+        o.outer = 1 if self.outer == "fgmres" else 0
+        o.restart = self.restart
         return o
 
     def prepare_operator(self, rho) -> None:
