@@ -146,7 +146,12 @@ def make_inputs():
 
 
 def _solver(precision):
+    """'fp64' / 'mixed': Jacobi PCG; 'learned': the learned solver's defaults."""
     from twophaseflow_b200 import PPESolverFVMMatrixFree, UniformGrid
+    if precision == "learned":
+        from twophaseflow_b200.learned import PPESolverLearned
+        return PPESolverLearned(None, _Cfg(pseudo_tol=TOL, pseudo_maxiter=1_000_000, ppe_learned_maxiter=20000),
+                                UniformGrid(N_PPE))
     cfg = _Cfg(pseudo_tol=TOL, pseudo_maxiter=1_000_000, ppe_iteration_method="cg", ppe_preconditioner="jacobi",
                ppe_precision=precision, ppe_inner_tol=1e-3)
     return PPESolverFVMMatrixFree(None, cfg, UniformGrid(N_PPE))
@@ -177,13 +182,14 @@ def time_ppe(precision, rho_d, rhs_d, steps, warmup, flush, cg_kernel=0):
     return s, p, times
 
 
-def time_learned(rho_d, rhs_d, steps, warmup, flush, outer="fcg"):
-    """Network-preconditioned flexible CG (or flexible GMRES(30) with
-    ``outer='fgmres'``; shipped weights, two-level mode), device-resident inputs."""
+def time_learned(rho_d, rhs_d, steps, warmup, flush, **opts):
+    """Network-preconditioned solve (shipped weights, two-level mode; the
+    solver's defaults -- flexible GMRES(80), 16 sweeps -- unless ``opts`` give
+    ``ppe_learned_*`` settings), device-resident inputs."""
     import torch
     from twophaseflow_b200 import UniformGrid
     from twophaseflow_b200.learned import PPESolverLearned
-    cfg = _Cfg(pseudo_tol=TOL, pseudo_maxiter=1_000_000, ppe_learned_maxiter=20000, ppe_learned_outer=outer)
+    cfg = _Cfg(pseudo_tol=TOL, pseudo_maxiter=1_000_000, ppe_learned_maxiter=20000, **opts)
     s = PPESolverLearned(None, cfg, UniformGrid(N_PPE))
     for _ in range(warmup):
         s.solve(rhs_d, rho_d)
@@ -201,11 +207,12 @@ def time_learned(rho_d, rhs_d, steps, warmup, flush, outer="fcg"):
     return s, p, times
 
 
-def learned_heldout(sizes=((512, 512), (1024, 1024)), seeds=(11, 12, 13)):
+def learned_heldout(sizes=((512, 512), (1024, 1024)), seeds=(11, 12, 13), **opts):
     """Learned preconditioner against plain FP64 PCG on density fields that were
     used neither in training nor in choosing its settings (12 droplets, seeded
     as the benchmark field): one warm-up and one timed solve of each, CUDA
-    events, to 1e-8 relative residual."""
+    events, to 1e-8 relative residual; ``opts``: ``ppe_learned_*`` settings
+    (default: the solver's)."""
     import torch
     from twophaseflow_b200 import PPESolverFVMMatrixFree, UniformGrid
     from twophaseflow_b200.learned import PPESolverLearned
@@ -226,8 +233,8 @@ def learned_heldout(sizes=((512, 512), (1024, 1024)), seeds=(11, 12, 13)):
     for N in sizes:
         pc = PPESolverFVMMatrixFree(None, _Cfg(pseudo_tol=TOL, pseudo_maxiter=1_000_000, ppe_iteration_method="cg",
                                                ppe_preconditioner="jacobi"), UniformGrid(N))
-        lr = PPESolverLearned(None, _Cfg(pseudo_tol=TOL, pseudo_maxiter=1_000_000, ppe_learned_maxiter=20000),
-                              UniformGrid(N))
+        lr = PPESolverLearned(None, _Cfg(pseudo_tol=TOL, pseudo_maxiter=1_000_000, ppe_learned_maxiter=20000,
+                                         **opts), UniformGrid(N))
         rows = []
         for seed in seeds:
             rho = torch.from_numpy(droplet_density(N, seed=seed)).cuda()
@@ -428,6 +435,11 @@ def main(argv=None):
     with ClockSampler(local) as clk:
         s64, p64, t64 = time_ppe("fp64", rho_d, rhs_d, args.steps, args.warmup, flush)
         torch.cuda.synchronize()
+        _barrier(ws)
+        # the learned solve (flexible GMRES(80), U-Net two-level preconditioner),
+        # the same steps / warm-up and L2 flush
+        slr, plr, tlr = time_learned(rho_d, rhs_d, args.steps, args.warmup, flush)
+        torch.cuda.synchronize()
     _barrier(ws)
     it64 = s64.last_diagnostics["ppe_low_order_cg_iterations"]
     smx, pmx, tmx = time_ppe("mixed", rho_d, rhs_d, max(2, args.steps // 2), 1, flush)
@@ -437,13 +449,17 @@ def main(argv=None):
     smg, _, tmg = time_ppe("mixed", rho_d, rhs_d, 2, 1, flush, cg_kernel=1)
     _barrier(ws)
     dmg = smg.last_diagnostics
-    slr, plr, tlr = time_learned(rho_d, rhs_d, max(2, args.steps // 3), 1, flush)
-    _barrier(ws)
     dlr = slr.last_diagnostics
-    sgm, pgm, tgm = time_learned(rho_d, rhs_d, 2, 1, flush, outer="fgmres")
+    # the configuration's flexible GMRES(30), and flexible CG(8) with 3 sweeps
+    sgm, pgm, tgm = time_learned(rho_d, rhs_d, 2, 1, flush, ppe_learned_outer="fgmres", ppe_learned_restart=30)
     _barrier(ws)
     dgm = dict(sgm.last_diagnostics)
+    sfc, pfc, tfc = time_learned(rho_d, rhs_d, 2, 1, flush, ppe_learned_outer="fcg", ppe_learned_smooth=3)
+    _barrier(ws)
+    dfc = dict(sfc.last_diagnostics)
     heldout = learned_heldout()
+    _barrier(ws)
+    heldout30 = learned_heldout(ppe_learned_outer="fgmres", ppe_learned_restart=30)
     _barrier(ws)
     ms_mx = _max_over_ranks(float(np.mean(tmx)), ws)
     ms_64 = _max_over_ranks(float(np.mean(t64)), ws)
@@ -454,7 +470,7 @@ def main(argv=None):
     ms_best = min(ms_64, ms_mx, ms_lr)
 
     # e2e through the public API with host buffers (same method as the headline)
-    e2e_ms, e2e_wall, _ = time_ppe_e2e(best if best != "learned" else "fp64", rho, rhs, max(2, args.steps // 2), 1)
+    e2e_ms, e2e_wall, _ = time_ppe_e2e(best, rho, rhs, max(2, args.steps // 2), 1)
     e2e_ms = _max_over_ranks(e2e_ms, ws)
 
     # roofline of the dominant kernel (persistent PCG, one launch per solve):
@@ -465,6 +481,26 @@ def main(argv=None):
     peak, peak_kind = _peaks()
     alg64 = it64 * 112 * ndof
     ach64 = alg64 / (np.mean(t64) * 1e-3) / 1e9
+    roof_plain = {"kernel": "cg1_band_kernel", "bound": "hbm", "achieved": round(ach64, 1), "peak": peak,
+                  "peak_kind": peak_kind, "unit": "GB/s", "frac": round(ach64 / peak, 3),
+                  "traffic": PCG_BAND_DRAM_BYTES_PER_SOLVE,
+                  "note": "112 B/DOF/iteration algorithmic over the solve; vectors live in shared memory, "
+                          "DRAM traffic is the inputs once (ncu); the iteration is bound by the grid reduction"}
+    # the learned solve's top kernel by time share: the blocked damped-Jacobi
+    # smoother (48 B per node and launch algorithmic, 4 sweeps per launch)
+    from twophaseflow_b200.kernel_cases import smoother_case
+    smo = smoother_case(N_PPE)
+    roof_learned = {"kernel": "smooth_block_kernel", "bound": "hbm", "achieved": smo["GBps"], "peak": peak,
+                    "peak_kind": peak_kind, "unit": "GB/s", "frac": round(smo["GBps"] / peak, 3),
+                    "us_per_launch": smo["us_per_launch"], "traffic": None,
+                    "note": "48 B/node per launch algorithmic (z, r, D^-1, couplings read, z written; 4 sweeps); "
+                            "the 513^2 operator is L2-resident"}
+    # launches of the learned solve (flexible GMRES): per Arnoldi column 33 for
+    # the preconditioner (6 input/restriction, 14 convolutions, 6 resampling,
+    # output, prolongation + first sweep, 4 blocked smoother launches, copy-out),
+    # 1 operator and 4 Gram-Schmidt; per restart cycle 6; 12 for the set-up
+    its_lr = dlr["ppe_learned_iterations"]
+    launches_lr = its_lr * 38 + 6 * ((its_lr + 79) // 80) + 12
 
     # CCD line kernels (2-D 1024^2 and 3-D 256^3, FP64 and FP32), graph-timed
     ccd = []
@@ -533,6 +569,7 @@ def main(argv=None):
         detail = {
             "bench_detail": True,
             "learned_heldout": heldout,
+            "learned_heldout_fgmres30": heldout30,
             "batched_32_cases": bat,
             "batched_64_cases_64x64": bat_small,
             "ccd": ccd,
@@ -558,7 +595,11 @@ def main(argv=None):
             "learned_fgmres30": {"ms": round(float(np.mean(tgm)), 3), "iterations": dgm["ppe_learned_iterations"],
                                  "fell_back": bool(dgm["ppe_learned_fell_back"]),
                                  "max_rel_diff_vs_fp64": float(f"{float(torch.max(torch.abs(pgm - p64))) / float(torch.max(torch.abs(p64))):.3g}")},
-            "learned_detail": {"fallback_iterations": dlr["ppe_learned_fallback_iterations"],
+            "learned_fcg8_smooth3": {"ms": round(float(np.mean(tfc)), 3), "iterations": dfc["ppe_learned_iterations"],
+                                     "fell_back": bool(dfc["ppe_learned_fell_back"]),
+                                     "max_rel_diff_vs_fp64": float(f"{float(torch.max(torch.abs(pfc - p64))) / float(torch.max(torch.abs(p64))):.3g}")},
+            "learned_detail": {"method": "flexible GMRES(80), U-Net two-level preconditioner, 16 Jacobi sweeps",
+                               "fallback_iterations": dlr["ppe_learned_fallback_iterations"],
                                "rel_residual": dlr["ppe_learned_relative_residual"],
                                "us_per_iteration": round(ms_lr * 1e3 / max(1, dlr["ppe_learned_iterations"]), 1)},
         }
@@ -566,12 +607,12 @@ def main(argv=None):
         line = {
             "metric": METRIC, "value": round(ms_best, 3), "unit": "ms", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_best, 3), "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if best == "fp64" else "f32 inner / f64 outer",
+            "scaling": "weak", "vs_baseline": None, "dtype": {"fp64": "f64", "mixed": "f32 inner / f64 outer", "learned": "bf16 preconditioner / f64 Krylov"}[best],
             "data": "synthetic (seeded droplets, seeded velocity divergence)",
             "config": {"workload": WORKLOAD, "grid": list(N_PPE), "tol": TOL,
                        "method": {"fp64": "FP64 Jacobi-PCG, persistent single-reduction kernel",
                                   "mixed": "mixed: band-resident FP32 Jacobi-PCG with FP64 residual replacement",
-                                  "learned": "two-level U-Net-preconditioned flexible CG"}[best],
+                                  "learned": "two-level U-Net-preconditioned flexible GMRES(80)"}[best],
                        "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{ws}"},
             "plain_fp64_pcg_ms": round(ms_64, 3), "plain_fp64_iterations": it64,
             "mixed_ms": round(ms_mx, 3), "mixed_max_rel_diff_vs_fp64": float(f"{err:.3g}"),
@@ -583,12 +624,9 @@ def main(argv=None):
             "ccd_frac_3d_f64": round(ccd3_gbps / peak, 3),
             "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": 2 * ndof * 8,
                     "d2h_bytes_per_step": ndof * 8, "wall_ms": round(e2e_wall, 3)},
-            "roofline": {"kernel": "cg1_band_kernel", "bound": "hbm", "achieved": round(ach64, 1), "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(ach64 / peak, 3),
-                         "traffic": PCG_BAND_DRAM_BYTES_PER_SOLVE,
-                         "note": "112 B/DOF/iteration algorithmic over the solve; vectors live in shared memory, "
-                                 "DRAM traffic is the inputs once (ncu); the iteration is bound by the grid reduction"},
-            "gpu_launches": 4 * args.steps,
+            "roofline": roof_learned if best == "learned" else roof_plain,
+            "roofline_plain_fp64": roof_plain,
+            "gpu_launches": (launches_lr if best == "learned" else 4) * args.steps,
             "clocks": clocks,
         }
         if cpu is not None:

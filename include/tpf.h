@@ -653,11 +653,13 @@ int tpf_unet_train_step_energy(tpf_unet* net, int B, const float* in2, const flo
 typedef struct tpf_learned_options {
   double tol;           /* relative residual tolerance of the weighted system   */
   int64_t maxiter;      /* flexible-CG iterations before the fallback           */
-  int smooth;           /* damped-Jacobi sweeps after the network (0..8)         */
+  int smooth;           /* damped-Jacobi sweeps after the network (0..32)        */
   double omega;         /* their damping                                         */
   int check_every;      /* iterations between host checks of the residual        */
   int stall_checks;     /* fallback when the best ||r|| has not fallen by         */
   double stall_factor;  /* stall_factor within stall_checks x check_every iters  */
+                        /* (flexible GMRES: judged after each restart cycle on   */
+                        /* the true residual, same window in Arnoldi columns)    */
   int fallback;         /* 1: finish with plain Jacobi PCG after a stall          */
   int use_graph;        /* 1: replay one iteration as a CUDA graph                */
   int window;           /* stored directions of the truncated flexible CG (1..8) */
@@ -687,11 +689,22 @@ int tpf_lppe_destroy(tpf_lppe* lp);
 /* tpf_ppe_prepare plus the density feature of the network input. */
 int tpf_lppe_prepare(tpf_lppe* lp, const double* rho, void* stream);
 /* Same contract as tpf_ppe_solve (p[pin] = 0, TPF_ENOCONV when the budget
- * ends), flexible CG preconditioned by the network. */
+ * ends), flexible CG (outer = 0) or flexible GMRES(restart) (outer = 1)
+ * preconditioned by the network; after a stall or at the end of the budget
+ * plain Jacobi PCG finishes from the current iterate when fallback = 1. */
 int tpf_lppe_solve(tpf_lppe* lp, const double* rhs, const double* rho, double* p, const double* p_init,
                    const tpf_learned_options* opts, void* stream, tpf_lppe_result* result);
 /* z = B(r), the preconditioner alone (r, z device vectors of the grid). */
 int tpf_lppe_precondition(tpf_lppe* lp, const double* r, double* z, int smooth, double omega, void* stream);
+/* Damped-Jacobi sweeps per smoother launch, 1..4 (default 4): the blocked
+ * smoother keeps a tile and a halo as wide as its sweeps in shared memory;
+ * every setting gives the same bits. */
+int tpf_lppe_set_smooth_block(tpf_lppe* lp, int sweeps);
+/* zout = J^sweeps(zin): damped-Jacobi sweeps z + omega D^-1 (r - S z) (pin
+ * 0) of the prepared operator, the preconditioner's smoother alone (zin, r,
+ * zout device vectors of the grid; zout may alias zin). */
+int tpf_lppe_smooth(tpf_lppe* lp, const double* zin, const double* r, double* zout, int sweeps, double omega,
+                    void* stream);
 /* Training pair from an error field e of the weighted system (pin 0), in the
  * form the network reads (in2, target: device FP32 on the network image).
  * coarsen = 1: in2 = (D^-1/2 S e / s, density feature, couplings of

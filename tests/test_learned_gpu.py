@@ -157,7 +157,7 @@ def test_flexible_cg_matches_direct_solution(cuda_device, smooth, coarsen):
     N = (64, 64)
     rho, rhs = _case(N, seed=3)
     cfg = _Cfg(pseudo_tol=1e-10, pseudo_maxiter=4000, ppe_learned_smooth=smooth, ppe_learned_fallback=False,
-               ppe_learned_coarsen=coarsen)
+               ppe_learned_coarsen=coarsen, ppe_learned_outer="fcg")
     s = PPESolverLearned(None, cfg, UniformGrid(N), params=np.zeros(num_params(), np.float32))
     p = s.solve(torch.from_numpy(rhs).to(cuda_device), torch.from_numpy(rho).to(cuda_device)).cpu().numpy()
     d = s.last_diagnostics
@@ -169,7 +169,8 @@ def test_flexible_cg_matches_direct_solution(cuda_device, smooth, coarsen):
     assert p.ravel()[pin] == 0.0
 
 
-def test_learned_solve_falls_back_to_pcg_on_stall(cuda_device):
+@pytest.mark.parametrize("outer", ["fcg", "fgmres"])
+def test_learned_solve_falls_back_to_pcg_on_stall(cuda_device, outer):
     import torch
     from twophaseflow_b200 import UniformGrid
     from twophaseflow_b200.learned import PPESolverLearned
@@ -178,7 +179,7 @@ def test_learned_solve_falls_back_to_pcg_on_stall(cuda_device):
     # an all-zero network without smoothing gives z = 0: no progress -> fallback
     from twophaseflow_b200.learned import num_params
     cfg = _Cfg(pseudo_tol=1e-9, pseudo_maxiter=400, ppe_learned_smooth=0, ppe_learned_maxiter=400,
-               ppe_learned_coarsen=1)
+               ppe_learned_coarsen=1, ppe_learned_outer=outer)
     s = PPESolverLearned(None, cfg, UniformGrid(N), params=np.zeros(num_params(), np.float32))
     p = s.solve(torch.from_numpy(rhs).to(cuda_device), torch.from_numpy(rho).to(cuda_device)).cpu().numpy()
     d = s.last_diagnostics
@@ -239,11 +240,14 @@ def test_energy_pairs_and_loss(cuda_device):
     assert np.isfinite(losses).all() and losses[-1] < min(1.0, losses[0]), (losses[0], losses[-1])
 
 
-def test_trained_network_gain(cuda_device):
+@pytest.mark.parametrize("outer,smooth,bar", [("fcg", 3, 2.5), ("fgmres", 16, 1.5)])
+def test_trained_network_gain(cuda_device, outer, smooth, bar):
     """The shipped network (trained on 512^2 solver pairs, energy loss) against
-    the same two-level flexible CG without it (all-zero network: the Jacobi
+    the same two-level method without it (all-zero network: the Jacobi
     two-grid cycle with no coarse correction) on a held-out 256^2 density at
-    ratio 1000: at least 2.5x fewer iterations (about 3x measured), same solution."""
+    ratio 1000: flexible CG with 3 sweeps needs at least 2.5x fewer iterations
+    with the network (about 3x measured), the default flexible GMRES(80) with
+    16 sweeps at least 1.5x; same solution."""
     import torch
     from twophaseflow_b200 import UniformGrid
     from twophaseflow_b200.learned import PPESolverLearned, load_params, num_params
@@ -251,7 +255,8 @@ def test_trained_network_gain(cuda_device):
     N = (256, 256)
     rho = torch.from_numpy(droplet_density(N, seed=101)).to(cuda_device)
     rhs = torch.from_numpy(divergence_rhs(N, seed=102)).to(cuda_device)
-    cfg = _Cfg(pseudo_tol=1e-8, pseudo_maxiter=5000, ppe_learned_maxiter=5000, ppe_learned_fallback=False)
+    cfg = _Cfg(pseudo_tol=1e-8, pseudo_maxiter=5000, ppe_learned_maxiter=5000, ppe_learned_fallback=False,
+               ppe_learned_outer=outer, ppe_learned_smooth=smooth)
     its = {}
     sol = {}
     for name, params in (("trained", load_params()), ("none", np.zeros(num_params(), np.float32))):
@@ -260,7 +265,8 @@ def test_trained_network_gain(cuda_device):
         d = s.last_diagnostics
         assert d["ppe_learned_info"] == 0 and not d["ppe_learned_fell_back"]
         its[name] = d["ppe_learned_iterations"]
-    assert its["trained"] * 2.5 <= its["none"], its
+    print(outer, smooth, its)
+    assert its["trained"] * bar <= its["none"], its
     scale = np.abs(sol["none"]).max()
     assert np.abs(sol["trained"] - sol["none"]).max() <= 1e-6 * scale
 
@@ -330,10 +336,57 @@ def test_flexible_gmres_with_trained_network(cuda_device):
     assert dg["ppe_learned_info"] == 0 and not dg["ppe_learned_fell_back"], dg
     pg2 = sg.solve(rhs, rho)
     assert torch.equal(pg, pg2) and sg.last_diagnostics["ppe_learned_iterations"] == dg["ppe_learned_iterations"]
-    sc = PPESolverLearned(None, _Cfg(**base), UniformGrid(N))
+    sc = PPESolverLearned(None, _Cfg(ppe_learned_outer="fcg", **base), UniformGrid(N))
     pc = sc.solve(rhs, rho)
     print("fgmres", dg["ppe_learned_iterations"], "fcg", sc.last_diagnostics["ppe_learned_iterations"])
     scale = float(torch.max(torch.abs(pc)))
     assert float(torch.max(torch.abs(pg - pc))) <= 1e-6 * scale
     with pytest.raises(ValueError, match="ppe_learned_outer"):
         PPESolverLearned(None, _Cfg(ppe_learned_outer="bicgstab", **base), UniformGrid(N))
+
+
+def test_flexible_gmres_stall_rule_hands_over_to_pcg(cuda_device):
+    """Restarted Jacobi-GMRES(7) (all-zero network, one sweep) at density ratio
+    1000 stalls: the stall rule (best true residual not halved within 128
+    Arnoldi columns, judged after each cycle) stops it long before the
+    iteration budget and plain PCG finishes the solve."""
+    import torch
+    from twophaseflow_b200 import UniformGrid
+    from twophaseflow_b200.learned import PPESolverLearned, num_params
+    N = (48, 48)
+    rho, rhs = _case(N, seed=5)
+    cfg = _Cfg(pseudo_tol=1e-9, pseudo_maxiter=4000, ppe_learned_smooth=1, ppe_learned_maxiter=4000,
+               ppe_learned_coarsen=1, ppe_learned_outer="fgmres", ppe_learned_restart=7)
+    s = PPESolverLearned(None, cfg, UniformGrid(N), params=np.zeros(num_params(), np.float32))
+    p = s.solve(torch.from_numpy(rhs).to(cuda_device), torch.from_numpy(rho).to(cuda_device)).cpu().numpy()
+    d = s.last_diagnostics
+    print(d)
+    assert d["ppe_learned_fell_back"] and d["ppe_learned_info"] == 0
+    assert d["ppe_learned_iterations"] < 2000
+    pd = oppe.spsolve_fvm(rhs, rho, oppe.uniform_coords(N, (1.0, 1.0)))
+    assert np.abs(p - pd).max() <= 1e-6 * np.abs(pd).max()
+
+
+@pytest.mark.parametrize("N,coarsen", [((64, 64), 1), ((100, 77), 4), ((256, 256), 4)])
+def test_blocked_smoother_equals_single_sweeps(cuda_device, N, coarsen):
+    """The preconditioner with 1, 3 or 4 damped-Jacobi sweeps per launch
+    (temporally blocked smoother) gives the same bits for 1, 5 and 16 sweeps,
+    on the fine-grid and the two-level form, with the pinned node inside."""
+    import torch
+    from twophaseflow_b200 import UniformGrid, _lib
+    from twophaseflow_b200.learned import PPESolverLearned
+    rho, rhs = _case(N, seed=7)
+    s = PPESolverLearned(None, _Cfg(pseudo_tol=1e-8, pseudo_maxiter=100, ppe_learned_coarsen=coarsen),
+                         UniformGrid(N))
+    s.prepare_operator(torch.from_numpy(rho).to(cuda_device))
+    r = torch.from_numpy(rhs).to(cuda_device)
+    for smooth in (1, 5, 16):
+        s.smooth = smooth
+        outs = []
+        for blk in (1, 3, 4):
+            _lib.check(s.lib.tpf_lppe_set_smooth_block(s._lp, blk))
+            outs.append(s.precondition(r).clone())
+        for o in outs[1:]:
+            assert torch.equal(outs[0], o), smooth
+    with pytest.raises(ValueError):
+        _lib.check(s.lib.tpf_lppe_set_smooth_block(s._lp, 5))

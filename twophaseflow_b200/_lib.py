@@ -216,6 +216,8 @@ SIGNATURES = {
     "tpf_lppe_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.POINTER(tpf_learned_options), C.c_void_p, C.POINTER(tpf_lppe_result)]),
     "tpf_lppe_precondition": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_void_p]),
+    "tpf_lppe_set_smooth_block": (C.c_int, [C.c_void_p, C.c_int]),
+    "tpf_lppe_smooth": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_void_p]),
     "tpf_lppe_pair": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]),
     "tpf_lppe_pair_energy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
                                        C.c_void_p]),

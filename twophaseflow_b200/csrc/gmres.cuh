@@ -156,11 +156,13 @@ __device__ void givens_rot(double f, double g, double& c, double& s, double& r) 
 }
 
 __global__ void gm_scale_kernel(int ndof, const double* w, double* vout, const GmState* st) {
+  tpf::chain_begin();
   if (st->done && st->scal == 0.0) return;
   // executed even when this column set done (the vector is then unused)
   const double sc = st->scal;
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ndof; idx += gridDim.x * blockDim.x)
     vout[idx] = w[idx] * sc;
+  tpf::chain_end();
 }
 
 // y = H(:ncols,:ncols)^-1 S (SciPy's trsv loop), then coef = y
@@ -324,6 +326,7 @@ __device__ void gm_column_step(double* H, int ldh, double* givens, double* S, Gm
 // h0 = ||w||, the re-orthogonalization decision, hcol2 = 0
 __global__ void gs1_kernel(int ndof, const double* __restrict__ V, int col, const double* __restrict__ w,
                            double* part, double* hcol, double* hcol2, GmState* st) {
+  tpf::chain_begin();
   if (st->done) return;
   __shared__ double sh[8 * 32];
   __shared__ double sums[kGmMaxCols + 2];
@@ -342,12 +345,14 @@ __global__ void gs1_kernel(int ndof, const double* __restrict__ V, int col, cons
     st->reorth = (sw - proj < 0.5 * sw) ? 1 : 0;
     st->arrive = 0u;
   }
+  tpf::chain_end();
 }
 
 // gs2: w -= sum_k hcol_k V_k; then either the second pass's dots
 // (re-orthogonalization: last block -> hcol2) or ||w|| and the column step
 __global__ void gs2_kernel(int ndof, const double* __restrict__ V, int col, double* w, const double* hcol,
                            double* part, double* H, int ldh, double* givens, double* S, double* hcol2, GmState* st) {
+  tpf::chain_begin();
   if (st->done) return;
   __shared__ double sh[8 * 32];
   __shared__ double sums[3 * kGmMaxCols + 4];
@@ -372,11 +377,13 @@ __global__ void gs2_kernel(int ndof, const double* __restrict__ V, int col, doub
   __syncthreads();
   gm_column_step(H, ldh, givens, S, st, col, h1, hcol2, sums);
   if (threadIdx.x == 0) st->arrive = 0u;
+  tpf::chain_end();
 }
 
 // gs3 (re-orthogonalization only): w -= sum_k hcol2_k V_k; ||w||; column step
 __global__ void gs3_kernel(int ndof, const double* __restrict__ V, int col, double* w, double* part, double* H,
                            int ldh, double* givens, double* S, const double* hcol2, GmState* st) {
+  tpf::chain_begin();
   if (st->done || !st->reorth) return;
   __shared__ double sh[8 * 32];
   __shared__ double sums[3 * kGmMaxCols + 4];
@@ -393,6 +400,7 @@ __global__ void gs3_kernel(int ndof, const double* __restrict__ V, int col, doub
   __syncthreads();
   gm_column_step(H, ldh, givens, S, st, col, h1, hcol2, sums);
   if (threadIdx.x == 0) st->arrive = 0u;
+  tpf::chain_end();
 }
 
 // Device GMRES workspace of one solver handle.  V holds restart_cap + 1
@@ -440,6 +448,7 @@ struct GmresOutcome {
   double bnrm2 = 0.0;
   double rnorm = 0.0;      // true residual norm at exit
   bool converged = false;
+  bool stalled = false;    // flexible GMRES: stopped by its stall rule
 };
 
 // SciPy gmres(A, b, x0, rtol=tol, atol=0, restart, maxiter, M) on the
@@ -501,10 +510,10 @@ int gmres_solve(GmresWork& W, int restart, double tol, long long maxiter, bool x
       if ((est = apply(vc, W.t, cs, done))) return est;
       if ((est = precond(W.t, W.w, cs, done))) return est;
       double* hc = H + (size_t)col * ldh;
-      gs1_kernel<<<nb_dot, 256, 0, cs>>>(n, W.V, col, W.w, W.part, hc, hcol2, W.gst);
-      gs2_kernel<<<nb_dot, 256, 0, cs>>>(n, W.V, col, W.w, hc, W.part, H, ldh, givens, S, hcol2, W.gst);
-      gs3_kernel<<<nb_dot, 256, 0, cs>>>(n, W.V, col, W.w, W.part, H, ldh, givens, S, hcol2, W.gst);
-      gm_scale_kernel<<<W.ew_blocks, 256, 0, cs>>>(n, W.w, W.V + (size_t)(col + 1) * n, W.gst);
+      tpf::launch_chained(gs1_kernel, nb_dot, 256, 0, cs, n, W.V, col, W.w, W.part, hc, hcol2, W.gst);
+      tpf::launch_chained(gs2_kernel, nb_dot, 256, 0, cs, n, W.V, col, W.w, hc, W.part, H, ldh, givens, S, hcol2, W.gst);
+      tpf::launch_chained(gs3_kernel, nb_dot, 256, 0, cs, n, W.V, col, W.w, W.part, H, ldh, givens, S, hcol2, W.gst);
+      tpf::launch_chained(gm_scale_kernel, W.ew_blocks, 256, 0, cs, n, W.w, W.V + (size_t)(col + 1) * n, W.gst);
       TPF_CUDA_TRY(cudaGetLastError());
     }
     return TPF_OK;
@@ -600,10 +609,14 @@ namespace {
 // unpreconditioned residual norm, so a cycle stops once it meets tol ||b||;
 // each restart starts from the true residual r = b - A x.
 // apply / resid / precond as for gmres_solve; Z: restart * n doubles.
+// Stall rule (stall_iters > 0): after a cycle, the best true ||r|| so far has
+// not fallen below stall_factor times the reference value within stall_iters
+// Arnoldi columns -> stop with out.stalled (the reference value is reset
+// whenever it does fall that far).
 template <class Apply, class Resid, class Precond>
 int fgmres_solve(GmresWork& W, double* Z, int restart, double tol, long long maxiter, bool x_nonzero,
                  long long key_a, long long key_b, Apply apply, Resid resid, Precond precond, cudaStream_t s,
-                 GmresOutcome& out) {
+                 GmresOutcome& out, double stall_factor = 0.5, long long stall_iters = 0) {
   const int n = W.n;
   int st;
   const int m = std::min(restart, n);
@@ -639,10 +652,10 @@ int fgmres_solve(GmresWork& W, double* Z, int restart, double tol, long long max
       if ((est = precond(vc, zc, cs, done))) return est;
       if ((est = apply(zc, W.w, cs, done))) return est;
       double* hc = H + (size_t)col * ldh;
-      gs1_kernel<<<nb_dot, 256, 0, cs>>>(n, W.V, col, W.w, W.part, hc, hcol2, W.gst);
-      gs2_kernel<<<nb_dot, 256, 0, cs>>>(n, W.V, col, W.w, hc, W.part, H, ldh, givens, S, hcol2, W.gst);
-      gs3_kernel<<<nb_dot, 256, 0, cs>>>(n, W.V, col, W.w, W.part, H, ldh, givens, S, hcol2, W.gst);
-      gm_scale_kernel<<<W.ew_blocks, 256, 0, cs>>>(n, W.w, W.V + (size_t)(col + 1) * n, W.gst);
+      tpf::launch_chained(gs1_kernel, nb_dot, 256, 0, cs, n, W.V, col, W.w, W.part, hc, hcol2, W.gst);
+      tpf::launch_chained(gs2_kernel, nb_dot, 256, 0, cs, n, W.V, col, W.w, hc, W.part, H, ldh, givens, S, hcol2, W.gst);
+      tpf::launch_chained(gs3_kernel, nb_dot, 256, 0, cs, n, W.V, col, W.w, W.part, H, ldh, givens, S, hcol2, W.gst);
+      tpf::launch_chained(gm_scale_kernel, W.ew_blocks, 256, 0, cs, n, W.w, W.V + (size_t)(col + 1) * n, W.gst);
       TPF_CUDA_TRY(cudaGetLastError());
     }
     return TPF_OK;
@@ -660,6 +673,8 @@ int fgmres_solve(GmresWork& W, double* Z, int restart, double tol, long long max
   }
   if ((st = gm_norm2(W, W.r, wnorm, s))) return st;
   if ((st = gm_read_scalar(wnorm, &rnorm, s))) return st;
+  double ref_rnorm = rnorm;
+  long long ref_inner = 0;
   for (long long iteration = 0; iteration < maxiter && !converged; ++iteration) {
     if (rnorm <= atol) { converged = true; break; }
     gm_start_kernel<<<W.ew_blocks, 256, 0, s>>>(n, W.r, W.V, S, m + 1, W.gst, rnorm, atol);
@@ -706,6 +721,15 @@ int fgmres_solve(GmresWork& W, double* Z, int restart, double tol, long long max
     if ((st = gm_read_scalar(wnorm, &rnorm, s))) return st;
     if (rnorm <= atol) converged = true;
     if (hs.breakdown) break;
+    if (!converged && stall_iters > 0) {
+      if (rnorm < stall_factor * ref_rnorm) {
+        ref_rnorm = rnorm;
+        ref_inner = inner;
+      } else if (inner - ref_inner >= stall_iters) {
+        out.stalled = true;
+        break;
+      }
+    }
   }
   out.inner = inner;
   out.applies = applies;

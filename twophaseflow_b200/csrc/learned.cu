@@ -183,6 +183,7 @@ __device__ __forceinline__ uint4 pack4bf(float c0, float c1, float c2, float c3)
 }
 
 __global__ void fcg_pack_kernel(LGrid g, const double* r, const float* feat, const FcgState* st, bf16* xin) {
+  tpf::chain_begin();
   tpf::tc::pdl_trigger();
   if (st->done) return;
   const int Wp = g.W + 2;
@@ -202,26 +203,133 @@ __global__ void fcg_pack_kernel(LGrid g, const double* r, const float* feat, con
     o[0] = pack4bf(c0, c1, c2, c3);
     o[1] = make_uint4(0, 0, 0, 0);
   }
+  tpf::chain_end();
 }
 
 // z = s D^-1/2 y (pin 0)
 __global__ void fcg_unpack_kernel(LGrid g, const float* y, const FcgState* st, double* z) {
+  tpf::chain_begin();
   if (st->done) return;
   const double s = st->s;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.ndof; i += gridDim.x * blockDim.x) {
     const int i0 = i / g.n1, i1 = i - i0 * g.n1;
     z[i] = (i == g.pin) ? 0.0 : s * sqrt(g.dinvS[i]) * (double)y[(size_t)i0 * g.W + i1];
   }
+  tpf::chain_end();
+}
+
+// one damped-Jacobi update of a node, z + omega D^-1 (r - S z), from its
+// value, its four neighbours' values and couplings (h*: whether the
+// neighbour exists); shared by the single-sweep and the blocked smoother so
+// that both round identically
+__device__ __forceinline__ double jacobi_node(double zc, double zm0, double zp0, double zm1, double zp1, double sm0,
+                                              double sp0, double sm1, double sp1, bool h0m, bool h0p, bool h1m,
+                                              bool h1p, double dinv, double rr, double omega) {
+  double off = 0.0;
+  if (h0m) off += sm0 * zm0;
+  if (h0p) off += sp0 * zp0;
+  if (h1m) off += sm1 * zm1;
+  if (h1p) off += sp1 * zp1;
+  const double sz = (sm0 + sp0 + sm1 + sp1) * zc - off;
+  return zc + omega * dinv * (rr - sz);
 }
 
 // zout = zin + omega D^-1 (r - S zin) (pin 0)
 __global__ void fcg_smooth_kernel(LGrid g, const double* zin, const double* r, double omega, const FcgState* st,
                                   double* zout) {
+  tpf::chain_begin();
   if (st->done) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.ndof; i += gridDim.x * blockDim.x) {
     const int i0 = i / g.n1, i1 = i - i0 * g.n1;
-    zout[i] = (i == g.pin) ? 0.0 : zin[i] + omega * g.dinvS[i] * (r[i] - s_apply(g, zin, i, i0, i1));
+    if (i == g.pin) {
+      zout[i] = 0.0;
+      continue;
+    }
+    const bool h0m = i0 > 0, h0p = i0 < g.n0 - 1, h1m = i1 > 0, h1p = i1 < g.n1 - 1;
+    zout[i] = jacobi_node(zin[i], h0m ? zin[i - g.n1] : 0.0, h0p ? zin[i + g.n1] : 0.0, h1m ? zin[i - 1] : 0.0,
+                          h1p ? zin[i + 1] : 0.0, h0m ? g.s0[i - g.n1] : 0.0, g.s0[i], h1m ? g.s1[i - 1] : 0.0,
+                          g.s1[i], h0m, h0p, h1m, h1p, g.dinvS[i], r[i], omega);
   }
+  tpf::chain_end();
+}
+
+// k <= kSmK damped-Jacobi sweeps in one pass (temporal blocking): a CTA loads
+// z, r, D^-1 and the couplings of its kSmTY x kSmTX tile plus a kSmK-node
+// halo into shared memory, sweeps k times over a region that shrinks by one
+// node per sweep, and writes the tile; each node's update is the single
+// sweep's (jacobi_node), so the result equals k single sweeps bit for bit
+constexpr int kSmTX = 32, kSmTY = 16, kSmK = 4;
+constexpr int kSmW = kSmTX + 2 * kSmK, kSmH = kSmTY + 2 * kSmK;
+
+__global__ void __launch_bounds__(256) smooth_block_kernel(LGrid g, const double* zin, const double* r,
+                                                           double omega, int k, const FcgState* st, double* zout) {
+  tpf::chain_begin();
+  if (st->done) return;
+  // only z goes through shared memory; each thread keeps r, D^-1 and the four
+  // couplings of its own kPer nodes (e = tid + 256 j of the tile with halo) in
+  // registers for all k sweeps and holds its last updates for the store
+  __shared__ double sz[2][kSmH][kSmW];
+  constexpr int kPer = (kSmH * kSmW + 255) / 256;
+  const int tiles1 = (g.n1 + kSmTX - 1) / kSmTX;
+  const int base0 = (int)(blockIdx.x / tiles1) * kSmTY - kSmK;
+  const int base1 = (int)(blockIdx.x % tiles1) * kSmTX - kSmK;
+  double lz[kPer], lr[kPer], ld[kPer], m0[kPer], p0[kPer], m1[kPer], p1[kPer];
+  unsigned flags[kPer];   // bit 0 in the domain, 1 pinned, 2..5 neighbours -0 +0 -1 +1 exist
+#pragma unroll
+  for (int j = 0; j < kPer; ++j) {
+    const int e = threadIdx.x + j * 256;
+    const int a = e / kSmW, c = e - (e / kSmW) * kSmW;
+    const int i0 = base0 + a, i1 = base1 + c;
+    const bool in = e < kSmH * kSmW && i0 >= 0 && i0 < g.n0 && i1 >= 0 && i1 < g.n1;
+    const int i = in ? i0 * g.n1 + i1 : 0;
+    const bool h0m = in && i0 > 0, h0p = in && i0 < g.n0 - 1, h1m = in && i1 > 0, h1p = in && i1 < g.n1 - 1;
+    flags[j] = (in ? 1u : 0u) | ((in && i == g.pin) ? 2u : 0u) | (h0m ? 4u : 0u) | (h0p ? 8u : 0u) |
+               (h1m ? 16u : 0u) | (h1p ? 32u : 0u);
+    lz[j] = in ? zin[i] : 0.0;
+    lr[j] = in ? r[i] : 0.0;
+    ld[j] = in ? g.dinvS[i] : 0.0;
+    m0[j] = h0m ? g.s0[i - g.n1] : 0.0;
+    p0[j] = in ? g.s0[i] : 0.0;
+    m1[j] = h1m ? g.s1[i - 1] : 0.0;
+    p1[j] = in ? g.s1[i] : 0.0;
+  }
+#pragma unroll
+  for (int j = 0; j < kPer; ++j) {
+    const int e = threadIdx.x + j * 256;
+    if (e < kSmH * kSmW) {
+      const int a = e / kSmW, c = e - (e / kSmW) * kSmW;
+      sz[0][a][c] = lz[j];
+      sz[1][a][c] = 0.0;
+    }
+  }
+  __syncthreads();
+  int cur = 0;
+  for (int sweep = 1; sweep <= k; ++sweep) {
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+      const int e = threadIdx.x + j * 256;
+      const int a = e / kSmW, c = e - (e / kSmW) * kSmW;
+      if (!(flags[j] & 1u) || a < sweep || a >= kSmH - sweep || c < sweep || c >= kSmW - sweep) continue;
+      const double v =
+          (flags[j] & 2u)
+              ? 0.0
+              : jacobi_node(sz[cur][a][c], sz[cur][a - 1][c], sz[cur][a + 1][c], sz[cur][a][c - 1],
+                            sz[cur][a][c + 1], m0[j], p0[j], m1[j], p1[j], (flags[j] & 4u) != 0,
+                            (flags[j] & 8u) != 0, (flags[j] & 16u) != 0, (flags[j] & 32u) != 0, ld[j], lr[j], omega);
+      sz[cur ^ 1][a][c] = v;
+      lz[j] = v;
+    }
+    cur ^= 1;
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < kPer; ++j) {
+    const int e = threadIdx.x + j * 256;
+    const int a = e / kSmW, c = e - (e / kSmW) * kSmW;
+    if (!(flags[j] & 1u) || a < kSmK || a >= kSmK + kSmTY || c < kSmK || c >= kSmK + kSmTX) continue;
+    zout[(base0 + a) * g.n1 + base1 + c] = lz[j];
+  }
+  tpf::chain_end();
 }
 
 // w = S z (pin 0); partials (z, Q_j) and (P_j, r) for the stored directions,
@@ -489,6 +597,7 @@ __global__ void coarse_setup_kernel(LGrid g, const double* dc, const float* feat
 
 // r1 = r - S (w D^-1 r), pin 0 (the pre-smoothing sweep from a zero start)
 __global__ void vc_pre_kernel(LGrid g, const double* r, double omega, const FcgState* st, double* r1) {
+  tpf::chain_begin();
   if (st && st->done) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.ndof; i += gridDim.x * blockDim.x) {
     const int i0 = i / g.n1, i1 = i - i0 * g.n1;
@@ -506,11 +615,13 @@ __global__ void vc_pre_kernel(LGrid g, const double* r, double omega, const FcgS
     }
     r1[i] = v;
   }
+  tpf::chain_end();
 }
 
 // rc = R r1 (block sums); partials of rc^2 / D_c
 __global__ void __launch_bounds__(kRedThreads) restrict_kernel(LGrid g, const double* r1, double* rc,
                                                                const FcgState* st, double* part) {
+  tpf::chain_begin();
   double v[1] = {0.0};
   if (!(st && st->done)) {
     const int nc = g.nc0 * g.nc1;
@@ -525,9 +636,11 @@ __global__ void __launch_bounds__(kRedThreads) restrict_kernel(LGrid g, const do
     }
   }
   block_partials<1>(v, part);
+  tpf::chain_end();
 }
 
 __global__ void coarse_scale_kernel(const double* part, int nb, int nc, FcgState* st) {
+  tpf::chain_begin();
   if (st->done) return;
   double v[1];
   reduce_partials<1>(part, nb, v);
@@ -536,6 +649,7 @@ __global__ void coarse_scale_kernel(const double* part, int nb, int nc, FcgState
     st->sc = sc;
     st->inv_sc = sc > 0.0 ? 1.0 / sc : 0.0;
   }
+  tpf::chain_end();
 }
 
 // scaled Galerkin couplings of aggregate I to the next row / column
@@ -548,6 +662,7 @@ __device__ __forceinline__ void coarse_coupl(const LGrid& g, const double* cc0, 
 // network input on the coarse image: (D_c^-1/2 rc / s_c, c~_c, coarse couplings)
 __global__ void pack_coarse_kernel(LGrid g, const double* rc, const double* cc0, const double* cc1,
                                    const FcgState* st, bf16* xin) {
+  tpf::chain_begin();
   tpf::tc::pdl_trigger();
   if (st->done) return;
   const int Wp = g.W + 2;
@@ -567,11 +682,13 @@ __global__ void pack_coarse_kernel(LGrid g, const double* rc, const double* cc0,
     o[0] = pack4bf(c0, c1, c2, c3);
     o[1] = make_uint4(0, 0, 0, 0);
   }
+  tpf::chain_end();
 }
 
 // z2 = w D^-1 r + P (s_c D_c^-1/2 y), pin 0
 __global__ void prolong_kernel(LGrid g, const float* y, const double* r, double omega, const FcgState* st,
                                double* z2) {
+  tpf::chain_begin();
   if (st->done) return;
   const double sc = st->sc;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.ndof; i += gridDim.x * blockDim.x) {
@@ -579,6 +696,7 @@ __global__ void prolong_kernel(LGrid g, const float* y, const double* r, double 
     const int I0 = i0 / g.b, I1 = i1 / g.b, I = I0 * g.nc1 + I1;
     z2[i] = (i == g.pin) ? 0.0 : omega * g.dinvS[i] * r[i] + sc * g.dcis[I] * (double)y[(size_t)I0 * g.W + I1];
   }
+  tpf::chain_end();
 }
 
 // prolongation fused with the first post-smoothing sweep:
@@ -586,6 +704,7 @@ __global__ void prolong_kernel(LGrid g, const float* y, const double* r, double 
 // neighbours, z = z2 + w D^-1 (r - S z2), pin 0
 __global__ void prolong_smooth_kernel(LGrid g, const float* y, const double* r, double omega, const FcgState* st,
                                       double* z) {
+  tpf::chain_begin();
   if (st->done) return;
   const double sc = st->sc;
   auto z2 = [&](int j, int j0, int j1) -> double {
@@ -610,6 +729,7 @@ __global__ void prolong_smooth_kernel(LGrid g, const float* y, const double* r, 
     const double sz = (sm0 + sp0 + sm1 + sp1) * zc - off;
     z[i] = zc + omega * g.dinvS[i] * (r[i] - sz);
   }
+  tpf::chain_end();
 }
 
 // training pair of the coarse problem: e1 = e - w D^-1 r (error after the
@@ -731,6 +851,7 @@ struct tpf_lppe {
   GmState* ggst = nullptr;
   cudaGraphExec_t gexec = nullptr;
   long long gkey[6] = {0, 0, 0, 0, 0, 0};
+  int smooth_block = 4;   // sweeps per smoother launch (1: one sweep per launch)
   std::vector<void*> allocs;
 };
 
@@ -773,14 +894,33 @@ int features(tpf_lppe* lp, const double* rho, cudaStream_t s) {
 }
 
 // z = B(r): network (+ smoothing); result in lp->z (smooth even) or lp->z2
+// n damped-Jacobi sweeps ping-ponging between cur and other (cur ends holding
+// the result): smooth_block sweeps per launch
+void enqueue_sweeps(tpf_lppe* lp, int n, double omega, cudaStream_t s, double*& cur, double*& other) {
+  const LGrid& g = lp->g;
+  if (lp->smooth_block <= 1) {
+    for (int k = 0; k < n; ++k) {
+      tpf::launch_chained(fcg_smooth_kernel, ew_blocks(g.ndof), 256, 0, s, g, cur, lp->r, omega, lp->st, other);
+      std::swap(cur, other);
+    }
+    return;
+  }
+  const int tiles = ((g.n0 + kSmTY - 1) / kSmTY) * ((g.n1 + kSmTX - 1) / kSmTX);
+  for (int k = 0; k < n; k += lp->smooth_block) {
+    const int kk = std::min(lp->smooth_block, n - k);
+    tpf::launch_chained(smooth_block_kernel, tiles, 256, 0, s, g, cur, lp->r, omega, kk, lp->st, other);
+    std::swap(cur, other);
+  }
+}
+
 int enqueue_precond(tpf_lppe* lp, int smooth, double omega, cudaStream_t s, double** zout) {
   const LGrid& g = lp->g;
   if (g.b > 1) {
     const int nc = g.nc0 * g.nc1;
-    vc_pre_kernel<<<ew_blocks(g.ndof), 256, 0, s>>>(g, lp->r, omega, lp->st, lp->r1);
-    restrict_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(g, lp->r1, lp->rc, lp->st, lp->part);
-    coarse_scale_kernel<<<1, 256, 0, s>>>(lp->part, kRedBlocks, nc, lp->st);
-    pack_coarse_kernel<<<ew_blocks((g.H + 2) * (g.W + 2)), 256, 0, s>>>(g, lp->rc, lp->cc0, lp->cc1, lp->st,
+    tpf::launch_chained(vc_pre_kernel, ew_blocks(g.ndof), 256, 0, s, g, lp->r, omega, lp->st, lp->r1);
+    tpf::launch_chained(restrict_kernel, kRedBlocks, kRedThreads, 0, s, g, lp->r1, lp->rc, lp->st, lp->part);
+    tpf::launch_chained(coarse_scale_kernel, 1, 256, 0, s, lp->part, kRedBlocks, nc, lp->st);
+    tpf::launch_chained(pack_coarse_kernel, ew_blocks((g.H + 2) * (g.W + 2)), 256, 0, s, g, lp->rc, lp->cc0, lp->cc1, lp->st,
                                                                          tpf::unet_input(lp->net));
     TPF_CUDA_TRY(cudaGetLastError());
     int st = tpf::unet_forward_packed(lp->net, 1, s);
@@ -788,31 +928,25 @@ int enqueue_precond(tpf_lppe* lp, int smooth, double omega, cudaStream_t s, doub
     double* cur = lp->z;
     double* other = lp->z2;
     if (smooth > 0) {
-      prolong_smooth_kernel<<<ew_blocks(g.ndof), 256, 0, s>>>(g, tpf::unet_output(lp->net), lp->r, omega, lp->st,
+      tpf::launch_chained(prolong_smooth_kernel, ew_blocks(g.ndof), 256, 0, s, g, tpf::unet_output(lp->net), lp->r, omega, lp->st,
                                                                lp->z);
     } else {
-      prolong_kernel<<<ew_blocks(g.ndof), 256, 0, s>>>(g, tpf::unet_output(lp->net), lp->r, omega, lp->st, lp->z);
+      tpf::launch_chained(prolong_kernel, ew_blocks(g.ndof), 256, 0, s, g, tpf::unet_output(lp->net), lp->r, omega, lp->st, lp->z);
     }
-    for (int k = 1; k < smooth; ++k) {
-      fcg_smooth_kernel<<<ew_blocks(g.ndof), 256, 0, s>>>(g, cur, lp->r, omega, lp->st, other);
-      std::swap(cur, other);
-    }
+    enqueue_sweeps(lp, smooth - 1, omega, s, cur, other);
     TPF_CUDA_TRY(cudaGetLastError());
     *zout = cur;
     return TPF_OK;
   }
-  fcg_pack_kernel<<<ew_blocks((g.H + 2) * (g.W + 2)), 256, 0, s>>>(g, lp->r, lp->feat, lp->st,
+  tpf::launch_chained(fcg_pack_kernel, ew_blocks((g.H + 2) * (g.W + 2)), 256, 0, s, g, lp->r, lp->feat, lp->st,
                                                                     tpf::unet_input(lp->net));
   TPF_CUDA_TRY(cudaGetLastError());
   int st = tpf::unet_forward_packed(lp->net, 1, s);
   if (st) return st;
-  fcg_unpack_kernel<<<ew_blocks(g.ndof), 256, 0, s>>>(g, tpf::unet_output(lp->net), lp->st, lp->z);
+  tpf::launch_chained(fcg_unpack_kernel, ew_blocks(g.ndof), 256, 0, s, g, tpf::unet_output(lp->net), lp->st, lp->z);
   double* cur = lp->z;
   double* other = lp->z2;
-  for (int k = 0; k < smooth; ++k) {
-    fcg_smooth_kernel<<<ew_blocks(g.ndof), 256, 0, s>>>(g, cur, lp->r, omega, lp->st, other);
-    std::swap(cur, other);
-  }
+  enqueue_sweeps(lp, smooth, omega, s, cur, other);
   TPF_CUDA_TRY(cudaGetLastError());
   *zout = cur;
   return TPF_OK;
@@ -824,6 +958,7 @@ int enqueue_precond(tpf_lppe* lp, int smooth, double omega, cudaStream_t s, doub
 // its D^-1-weighted norm (the network input scale); nothing once the cycle is done
 __global__ void __launch_bounds__(kRedThreads) fgm_in_kernel(LGrid g, const double* v, const int* gdone, double* r,
                                                              double* part) {
+  tpf::chain_begin();
   double acc[1] = {0.0};
   if (!*gdone) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.ndof; i += gridDim.x * blockDim.x) {
@@ -833,30 +968,37 @@ __global__ void __launch_bounds__(kRedThreads) fgm_in_kernel(LGrid g, const doub
     }
   }
   block_partials<1>(acc, part);
+  tpf::chain_end();
 }
 
 // the scale s of the network input and the preconditioner kernels' skip flag
 __global__ void fgm_scale_kernel(const double* part, int nb, int ndof, const int* gdone, FcgState* st) {
+  tpf::chain_begin();
   double v[1];
   reduce_partials<1>(part, nb, v);
   if (threadIdx.x == 0) {
     st->done = *gdone;
     set_scale(st, v[0], ndof);
   }
+  tpf::chain_end();
 }
 
 __global__ void fgm_out_kernel(int n, const double* z, const int* gdone, double* out) {
+  tpf::chain_begin();
   if (*gdone) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = z[i];
+  tpf::chain_end();
 }
 
 // w = S z with the pinned row w[pin] = z[pin] (z[pin] = 0 on this Krylov space)
 __global__ void fgm_apply_kernel(LGrid g, const double* z, const int* gdone, double* w) {
+  tpf::chain_begin();
   if (gdone && *gdone) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.ndof; i += gridDim.x * blockDim.x) {
     const int i0 = i / g.n1, i1 = i - i0 * g.n1;
     w[i] = (i == g.pin) ? z[i] : s_apply(g, z, i, i0, i1);
   }
+  tpf::chain_end();
 }
 
 // one flexible-CG step with M stored directions (the window length picks the instance)
@@ -966,7 +1108,7 @@ int solve_fgmres(tpf_lppe* lp, const tpf_learned_options& o, cudaStream_t s, boo
   W.cap = &lp->cap;
   W.key = lp->gkey;
   auto apply = [&](const double* in, double* outv, cudaStream_t cs, const int* done) -> int {
-    fgm_apply_kernel<<<ew_blocks(g.ndof), 256, 0, cs>>>(g, in, done, outv);
+    tpf::launch_chained(fgm_apply_kernel, ew_blocks(g.ndof), 256, 0, cs, g, in, done, outv);
     TPF_CUDA_TRY(cudaGetLastError());
     return TPF_OK;
   };
@@ -976,19 +1118,22 @@ int solve_fgmres(tpf_lppe* lp, const tpf_learned_options& o, cudaStream_t s, boo
     return TPF_OK;
   };
   auto precond = [&](const double* in, double* outv, cudaStream_t cs, const int* done) -> int {
-    fgm_in_kernel<<<kRedBlocks, kRedThreads, 0, cs>>>(g, in, done, lp->r, lp->part);
-    fgm_scale_kernel<<<1, 256, 0, cs>>>(lp->part, kRedBlocks, g.ndof, done, lp->st);
+    tpf::launch_chained(fgm_in_kernel, kRedBlocks, kRedThreads, 0, cs, g, in, done, lp->r, lp->part);
+    tpf::launch_chained(fgm_scale_kernel, 1, 256, 0, cs, lp->part, kRedBlocks, g.ndof, done, lp->st);
     double* z = nullptr;
     int est = enqueue_precond(lp, o.smooth, o.omega, cs, &z);
     if (est) return est;
-    fgm_out_kernel<<<ew_blocks(g.ndof), 256, 0, cs>>>(g.ndof, z, done, outv);
+    tpf::launch_chained(fgm_out_kernel, ew_blocks(g.ndof), 256, 0, cs, g.ndof, z, done, outv);
     TPF_CUDA_TRY(cudaGetLastError());
     return TPF_OK;
   };
   const long long cycles = std::max<long long>(1, (o.maxiter + o.restart - 1) / o.restart);
   const long long key_a = (long long)o.smooth * 1000003LL + (long long)(o.omega * 1e9);
+  // the flexible CG's stall rule, judged after each cycle on the true residual
+  const long long stall_iters =
+      (o.fallback && o.stall_checks > 0) ? (long long)o.stall_checks * o.check_every : 0;
   return fgmres_solve(W, lp->gZ, o.restart, o.tol, cycles, x_nonzero, key_a, (long long)(intptr_t)lp->st, apply,
-                      resid, precond, s, out);
+                      resid, precond, s, out, o.stall_factor, stall_iters);
 }
 
 int read_state(tpf_lppe* lp, cudaStream_t s) {
@@ -1012,7 +1157,7 @@ void tpf_lppe_default_options(tpf_learned_options* o) {
   if (!o) return;
   o->tol = 1e-8;
   o->maxiter = 2000;
-  o->smooth = 3;
+  o->smooth = 16;
   o->omega = 0.8;
   o->check_every = 8;
   o->stall_checks = 16;
@@ -1020,8 +1165,8 @@ void tpf_lppe_default_options(tpf_learned_options* o) {
   o->fallback = 1;
   o->use_graph = 1;
   o->window = 8;
-  o->outer = 0;
-  o->restart = 30;
+  o->outer = 1;
+  o->restart = 80;
 }
 
 int tpf_lppe_create(tpf_lppe** out, tpf_ppe* ppe, tpf_unet* net, int coarsen) {
@@ -1120,8 +1265,8 @@ int tpf_lppe_pair(tpf_lppe* lp, const double* e, float* in2, float* target, doub
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (lp->g.b > 1) {
     pair_residual_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(lp->g, e, lp->r, lp->part);
-    vc_pre_kernel<<<ew_blocks(lp->g.ndof), 256, 0, s>>>(lp->g, lp->r, omega, nullptr, lp->r1);
-    restrict_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(lp->g, lp->r1, lp->rc, nullptr, lp->part);
+    tpf::launch_chained(vc_pre_kernel, ew_blocks(lp->g.ndof), 256, 0, s, lp->g, lp->r, omega, nullptr, lp->r1);
+    tpf::launch_chained(restrict_kernel, kRedBlocks, kRedThreads, 0, s, lp->g, lp->r1, lp->rc, nullptr, lp->part);
     pair_coarse_write_kernel<<<ew_blocks(lp->g.H * lp->g.W), 256, 0, s>>>(lp->g, e, lp->r, lp->rc, lp->cc0, lp->cc1,
                                                                          omega, lp->part, kRedBlocks, in2, target);
     TPF_CUDA_TRY(cudaGetLastError());
@@ -1142,8 +1287,8 @@ int tpf_lppe_pair_energy(tpf_lppe* lp, const double* e, float* in2, float* coupl
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const LGrid& g = lp->g;
   pair_residual_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(g, e, lp->r, lp->part);
-  vc_pre_kernel<<<ew_blocks(g.ndof), 256, 0, s>>>(g, lp->r, omega, nullptr, lp->r1);
-  restrict_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(g, lp->r1, lp->rc, nullptr, lp->part);
+  tpf::launch_chained(vc_pre_kernel, ew_blocks(g.ndof), 256, 0, s, g, lp->r, omega, nullptr, lp->r1);
+  tpf::launch_chained(restrict_kernel, kRedBlocks, kRedThreads, 0, s, g, lp->r1, lp->rc, nullptr, lp->part);
   // in2 (channel 0 = scaled restricted residual, channel 1 = feature); the target is unused
   pair_coarse_write_kernel<<<ew_blocks(g.H * g.W), 256, 0, s>>>(g, e, lp->r, lp->rc, lp->cc0, lp->cc1, omega,
                                                                 lp->part, kRedBlocks, in2,
@@ -1155,10 +1300,41 @@ int tpf_lppe_pair_energy(tpf_lppe* lp, const double* e, float* in2, float* coupl
   return TPF_OK;
 }
 
+int tpf_lppe_set_smooth_block(tpf_lppe* lp, int sweeps) {
+  TPF_CHECK_ARG(lp, "NULL argument");
+  TPF_CHECK_ARG(sweeps >= 1 && sweeps <= kSmK, "sweeps per smoother launch must be in [1, 4]");
+  if (sweeps != lp->smooth_block) {
+    // the captured iteration / cycle graphs hold the old launches
+    if (lp->exec) { cudaGraphExecDestroy(lp->exec); lp->exec = nullptr; }
+    if (lp->gexec) { cudaGraphExecDestroy(lp->gexec); lp->gexec = nullptr; }
+    lp->graph_smooth = -1;
+    lp->smooth_block = sweeps;
+  }
+  return TPF_OK;
+}
+
+int tpf_lppe_smooth(tpf_lppe* lp, const double* zin, const double* r, double* zout, int sweeps, double omega,
+                    void* stream) {
+  TPF_CHECK_ARG(lp && zin && r && zout, "NULL argument");
+  TPF_CHECK_ARG(lp->have_feat, "call tpf_lppe_prepare first");
+  TPF_CHECK_ARG(sweeps >= 0 && sweeps <= 1024, "sweeps must be in [0, 1024]");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t bytes = sizeof(double) * lp->g.ndof;
+  TPF_CUDA_TRY(cudaMemsetAsync(&lp->st->done, 0, sizeof(int), s));
+  TPF_CUDA_TRY(cudaMemcpyAsync(lp->r, r, bytes, cudaMemcpyDeviceToDevice, s));
+  TPF_CUDA_TRY(cudaMemcpyAsync(lp->z, zin, bytes, cudaMemcpyDeviceToDevice, s));
+  double* cur = lp->z;
+  double* other = lp->z2;
+  enqueue_sweeps(lp, sweeps, omega, s, cur, other);
+  TPF_CUDA_TRY(cudaGetLastError());
+  TPF_CUDA_TRY(cudaMemcpyAsync(zout, cur, bytes, cudaMemcpyDeviceToDevice, s));
+  return TPF_OK;
+}
+
 int tpf_lppe_precondition(tpf_lppe* lp, const double* r, double* z, int smooth, double omega, void* stream) {
   TPF_CHECK_ARG(lp && r && z, "NULL argument");
   TPF_CHECK_ARG(lp->have_feat, "call tpf_lppe_prepare first");
-  TPF_CHECK_ARG(smooth >= 0 && smooth <= 8, "smooth must be in [0, 8]");
+  TPF_CHECK_ARG(smooth >= 0 && smooth <= 32, "smooth must be in [0, 32]");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int st = tpf::unet_prepare_weights(lp->net, s);
   if (st) return st;
@@ -1179,7 +1355,7 @@ int tpf_lppe_solve(tpf_lppe* lp, const double* rhs, const double* rho, double* p
   if (opt) o = *opt; else tpf_lppe_default_options(&o);
   TPF_CHECK_ARG(o.tol > 0.0 && std::isfinite(o.tol), "tolerance must be > 0");
   TPF_CHECK_ARG(o.maxiter >= 0, "maxiter must be >= 0");
-  TPF_CHECK_ARG(o.smooth >= 0 && o.smooth <= 8, "smooth must be in [0, 8]");
+  TPF_CHECK_ARG(o.smooth >= 0 && o.smooth <= 32, "smooth must be in [0, 32]");
   TPF_CHECK_ARG(o.check_every >= 1 && o.check_every <= 1024, "check_every must be in [1, 1024]");
   TPF_CHECK_ARG(o.window >= 1 && o.window <= kMaxWin, "window must be in [1, %d]", kMaxWin);
   TPF_CHECK_ARG(o.outer == 0 || o.outer == 1, "outer must be 0 (flexible CG) or 1 (flexible GMRES)");

@@ -59,6 +59,31 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long l
   return false;
 }
 
+// ---- bulk and tiled tensor copies (TMA engine), completion counted on an mbarrier ------
+// The arriving thread announces the bytes the copies will deliver; the phase
+// completes when they all have landed.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+// global -> shared, `bytes` contiguous (both addresses 16-byte aligned, bytes % 16 == 0)
+__device__ __forceinline__ void bulk_load(void* smem, const void* gmem, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_u32(smem)),
+               "l"(gmem), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+// global -> shared, the box of a 2-D tensor map at element coordinates
+// {x, y} (x * element size a multiple of 16 bytes; y may lie outside the
+// tensor: those rows are zero-filled)
+__device__ __forceinline__ void tensor_load_2d(void* smem, const void* tmap, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+      "[%4];\n" ::"r"(smem_u32(smem)),
+      "l"(tmap), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
 // ---- TMEM allocation (one warp) -----------------------------------------------------
 __device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
   asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(slot)),
@@ -89,6 +114,24 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
   d |= static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32;
   d |= static_cast<uint64_t>(1) << 46;  // descriptor version for sm_100
   // base offset 0, absolute LBO mode 0, layout type 0 = no swizzle
+  return d;
+}
+
+// K-major operand in the swizzled layout a tiled tensor copy writes: rows of
+// row_bytes (32, 64 or 128) contiguous bytes, one row per M (or N) index, the
+// 16-byte chunks of a row permuted by the 32/64/128-byte swizzle; 8-row
+// groups 8 * row_bytes apart (SBO; LBO is not used by these layouts).  The
+// swizzle is applied to the shared-memory address bits, so with the buffer
+// aligned to 1024 bytes a start address k rows in (or 32 bytes along K)
+// addresses the rows from k on (the next K step).
+__device__ __forceinline__ uint64_t smem_desc_swizzled(uint32_t saddr, uint32_t row_bytes) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((saddr >> 4) & 0x3FFFu);
+  d |= static_cast<uint64_t>(1) << 16;
+  d |= static_cast<uint64_t>(((8 * row_bytes) >> 4) & 0x3FFFu) << 32;
+  d |= static_cast<uint64_t>(1) << 46;  // descriptor version for sm_100
+  const uint64_t mode = row_bytes == 128 ? 2 : (row_bytes == 64 ? 4 : 6);   // 128B / 64B / 32B swizzle
+  d |= mode << 61;
   return d;
 }
 

@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstdarg>
 #include <string>
+#include <utility>
 
 #include "../../include/tpf.h"
 
@@ -65,6 +66,34 @@ inline int sm_count() {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
   return n > 0 ? n : 1;
+}
+
+// ---- programmatic dependent launch for chains of short dependent kernels ----
+// A kernel launched by launch_chained may be launched (its launch and block
+// scheduling overlapping the previous kernel's tail) before its predecessor in
+// the stream has finished; it must call chain_begin() before it touches any
+// memory: that waits until the predecessor has completed with its memory
+// visible.  chain_end(), the last statement of a chained kernel, lets the next
+// kernel launch once every block has reached it (blocks that return early
+// count when they exit).  Without the launch attribute (plain <<< >>>
+// launches) both return at once.
+__device__ __forceinline__ void chain_begin() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void chain_end() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_chained(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                  Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 template <typename T>

@@ -30,6 +30,7 @@
 #include "tc_sm100.cuh"
 #include "ppe_view.cuh"
 
+#include <cuda.h>   // CUtensorMap and its enums (the encoder is fetched through the runtime)
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -86,13 +87,6 @@ constexpr int kTile = 128;           // output pixels per CTA (MMA M)
 constexpr int kWin = kTile + 2;      // pixels per input window
 constexpr int kPlane = kWin * 16;    // bytes of one 8-channel plane of a window
 
-__host__ __device__ constexpr int taps_per_group(int cin, int cout) {
-  return (9 * cin * cout * 2 <= 80 * 1024) ? 9 : 3;
-}
-__host__ __device__ constexpr int conv_smem_bytes(int cin, int cout) {
-  return 3 * (cin / 8) * kPlane + taps_per_group(cin, cout) * cin * cout * 2;
-}
-
 struct ConvArgs {
   const bf16* in;     // [P][CIN]
   bf16* out;          // [P][COUT]
@@ -141,32 +135,62 @@ __device__ __forceinline__ void load_windows(const bf16* in, long long P, int Wp
   tpf::tc::cp_async_commit();
 }
 
-// One 128-pixel tile of a 3x3 convolution as an implicit GEMM on tcgen05:
-// D[pixel][co] = sum_{tap, ci} X[pixel + shift(tap)][ci] * W[tap][co][ci].
-// 4 warps; thread 0 issues the MMAs, all warps run the TMEM epilogue.
-template <int CIN, int COUT>
-__global__ void __launch_bounds__(128) conv3x3_tc_kernel(ConvArgs a) {
-  using namespace tpf::tc;
-  constexpr int KCH = CIN / 8;                 // 16-byte chunks per pixel
-  constexpr int WIN_BYTES = KCH * kPlane;
-  constexpr int TAP_W = CIN * COUT * 2;        // bytes of one tap's weights
-  constexpr int TG = taps_per_group(CIN, COUT);
-  constexpr int NCOLS = COUT < 32 ? 32 : COUT;
-  constexpr uint32_t IDESC = idesc_bf16_f32(kTile, COUT);
-  static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 256, "conv shape");
+// ---- tensor-copy-fed convolution (the layered forward and backward-data path) ---------------
+// The three input windows come straight from the pixel-major activations by
+// tiled tensor copies: a window block is [130 pixels][R bytes], R = 2 min(CIN,
+// 64) = 32, 64 or 128 (channels [64 kb, 64 kb + R/2) of each pixel), written
+// with the R-byte swizzle, which is the K-major swizzled operand layout of the
+// MMA with one pixel per row; tap dx is the same block read from row dx on.
+// Pixels outside the batch are zero-filled by the copy.  Weights are one
+// bulk copy per (tap, 8-channel plane) of the CTA's NS output channels
+// ([9][CIN/8][NS][8], K-major SWIZZLE_NONE core matrices), or a single copy
+// when NS = COUT.  The grid's y dimension splits COUT into NS-wide slices so
+// that the small deep-level images still occupy dozens of SMs.
+template <int CIN>
+struct WinGeom {
+  static constexpr int R = CIN < 64 ? CIN * 2 : 128;               // bytes of a block row
+  static constexpr int KB = CIN < 64 ? 1 : CIN / 64;               // blocks per window
+  static constexpr int BLOCK = ((kWin * R + 1023) / 1024) * 1024;  // 1024-byte aligned block
+  static constexpr int BYTES = 3 * KB * BLOCK;
+  static constexpr int TX = 3 * KB * kWin * R;                     // bytes the copies deliver
+};
 
-  extern __shared__ __align__(1024) unsigned char smem[];
-  unsigned char* sA = smem;
-  unsigned char* sB = smem + 3 * WIN_BYTES;
-  __shared__ uint64_t mbar;
+__host__ __device__ constexpr int conv_tma_smem_bytes(int cin, int ns) {
+  return 1024 + 3 * (cin < 64 ? 1 : cin / 64) * ((kWin * (cin < 64 ? cin * 2 : 128) + 1023) / 1024) * 1024 +
+         9 * cin * ns * 2;
+}
+constexpr int kConvSmemMax = 200 * 1024;
+// the widest output slice that fits (COUT itself when it does)
+__host__ __device__ constexpr int conv_ns_wide(int cin, int cout) {
+  return conv_tma_smem_bytes(cin, cout) <= kConvSmemMax ? cout : 32;
+}
+
+template <int CIN, int COUT, int NS>
+__global__ void __launch_bounds__(128) conv3x3_tma_kernel(const __grid_constant__ CUtensorMap tmap, ConvArgs a) {
+  using namespace tpf::tc;
+  using G = WinGeom<CIN>;
+  constexpr int KCH = CIN / 8;
+  constexpr int WBYTES = 9 * CIN * NS * 2;
+  constexpr int NCOLS = NS < 32 ? 32 : NS;
+  constexpr uint32_t IDESC = idesc_bf16_f32(kTile, NS);
+  static_assert(CIN % 16 == 0 && COUT % NS == 0 && NS % 16 == 0 && NS <= 256, "conv shape");
+  static_assert(conv_tma_smem_bytes(CIN, NS) <= kConvSmemMax, "conv shared memory");
+
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ uint64_t lbar, mbar;
   __shared__ uint32_t tmem_slot;
+  const uint32_t raw = smem_u32(smem_raw);
+  unsigned char* sA = smem_raw + (((raw + 1023u) & ~1023u) - raw);
+  unsigned char* sB = sA + G::BYTES;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const long long q0 = (long long)blockIdx.x * kTile;
+  const int n0 = blockIdx.y * NS;
 
   pdl_trigger();   // the next layer may start its prologue
   if (warp == 0) tmem_alloc(&tmem_slot, NCOLS);
   if (tid == 0) {
+    mbar_init(&lbar, 1);
     mbar_init(&mbar, 1);
     mbar_fence_init();
   }
@@ -175,66 +199,66 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(ConvArgs a) {
   fence_after_sync();
   const uint32_t tmem = tmem_slot;
 
-  // the first tap group's weights do not depend on the previous layer: load
-  // them before waiting for it
-  {
+  // the weights do not depend on the previous layer: request them before waiting for it
+  if (warp == 0) {
+    if (lane == 0) mbar_arrive_expect_tx(&lbar, WBYTES + G::TX);
+    __syncwarp();
     const unsigned char* wsrc = reinterpret_cast<const unsigned char*>(a.w);
-    for (int i = tid; i < TG * TAP_W / 16; i += 128) cp_async16(sB + i * 16, wsrc + i * 16, true);
-    cp_async_commit();
+    if (NS == COUT) {
+      if (lane == 0) bulk_load(sB, wsrc, WBYTES, &lbar);
+    } else {
+      for (int pl = lane; pl < 9 * KCH; pl += 32)
+        bulk_load(sB + pl * NS * 16, wsrc + ((size_t)pl * COUT + n0) * 16, NS * 16, &lbar);
+    }
   }
   pdl_wait();
-
-  load_windows<CIN>(a.in, a.P, a.Wp, q0, sA);
+  if (tid == 0) {
+#pragma unroll
+    for (int w = 0; w < 3; ++w) {
+      const int y = (int)(q0 - 1 + (long long)(w - 1) * a.Wp);
+#pragma unroll
+      for (int kb = 0; kb < G::KB; ++kb) tensor_load_2d(sA + (w * G::KB + kb) * G::BLOCK, &tmap, kb * 64, y, &lbar);
+    }
+  }
 
   bool ok = true;
-  uint32_t phase = 0;
-  for (int t0 = 0; t0 < 9; t0 += TG) {
-    if (t0 > 0) {
-      const unsigned char* wsrc = reinterpret_cast<const unsigned char*>(a.w) + (size_t)t0 * TAP_W;
-      for (int i = tid; i < TG * TAP_W / 16; i += 128) cp_async16(sB + i * 16, wsrc + i * 16, true);
-      cp_async_commit();
+  if (tid == 0) {
+    if (!mbar_wait(&lbar, 0, kSpin)) {
+      ok = false;
+      mbar_wait(&lbar, 0, kSpin);   // let copies still in flight land before going on
     }
-    cp_async_wait_all();
-    fence_proxy_async_smem();
-    __syncthreads();
-    if (tid == 0) {
-      fence_after_sync();
-      const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+    const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
 #pragma unroll 1
-      for (int tt = 0; tt < TG; ++tt) {
-        const int tap = t0 + tt;
-        const int dy = tap / 3, dx = tap - (tap / 3) * 3;   // 0..2
-        const uint32_t abase = a0 + dy * WIN_BYTES + dx * 16;
-        const uint32_t bbase = b0 + tt * TAP_W;
+    for (int tap = 0; tap < 9; ++tap) {
+      const int dy = tap / 3, dx = tap - (tap / 3) * 3;   // 0..2
 #pragma unroll
-        for (int kc = 0; kc < CIN / 16; ++kc) {
-          const uint64_t ad = smem_desc(abase + kc * 2 * kPlane, kPlane, 128);
-          const uint64_t bd = smem_desc(bbase + kc * 2 * (COUT * 16), COUT * 16, 128);
-          mma_bf16(tmem, ad, bd, IDESC, (tap > 0 || kc > 0) ? 1u : 0u);
-        }
+      for (int kc = 0; kc < CIN / 16; ++kc) {
+        const int kb = (kc * 32) / G::R, koff = (kc * 32) % G::R;
+        const uint64_t ad = smem_desc_swizzled(a0 + (dy * G::KB + kb) * G::BLOCK + dx * G::R + koff, G::R);
+        const uint64_t bd = smem_desc(b0 + (tap * KCH + 2 * kc) * (NS * 16), NS * 16, 128);
+        mma_bf16(tmem, ad, bd, IDESC, (tap > 0 || kc > 0) ? 1u : 0u);
       }
-      mma_commit(&mbar);
     }
-    __syncwarp();
-    if (!mbar_wait(&mbar, phase, kSpin)) ok = false;
-    phase ^= 1u;
-    fence_after_sync();
-    __syncthreads();
+    mma_commit(&mbar);
   }
-  if (!ok && lane == 0) atomicExch(a.err, 1);
+  __syncwarp();
+  if (!mbar_wait(&mbar, 0, kSpin)) ok = false;
+  fence_after_sync();
+  if (!ok) atomicExch(a.err, 1);
 
   // epilogue: warp w owns TMEM lanes / tile pixels [32w, 32w + 32)
   const long long q = q0 + warp * 32 + lane;
   const bool inb = q < a.P;
   const bool inner = inb && interior_pixel(q, a.Hp, a.Wp);
 #pragma unroll 1
-  for (int c0 = 0; c0 < COUT; c0 += 16) {
+  for (int c0 = 0; c0 < NS; c0 += 16) {
     float v[16];
     tmem_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + c0, v);
     if (inb) {
+      const int co = n0 + c0;
       float m[16];
       if (a.mask && inner) {
-        const uint4* mp = reinterpret_cast<const uint4*>(a.mask + q * COUT + c0);
+        const uint4* mp = reinterpret_cast<const uint4*>(a.mask + q * COUT + co);
         uint4 mv[2] = {mp[0], mp[1]};
         const bf16* mb = reinterpret_cast<const bf16*>(mv);
 #pragma unroll
@@ -248,14 +272,14 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(ConvArgs a) {
 #pragma unroll
       for (int i = 0; i < 16; i += 2) {
         float x0 = v[i], x1 = v[i + 1];
-        if (a.bias) { x0 += a.bias[c0 + i]; x1 += a.bias[c0 + i + 1]; }
+        if (a.bias) { x0 += a.bias[co + i]; x1 += a.bias[co + i + 1]; }
         if (a.relu) { x0 = fmaxf(x0, 0.f); x1 = fmaxf(x1, 0.f); }
         x0 *= m[i];
         x1 *= m[i + 1];
         if (!inner) { x0 = 0.f; x1 = 0.f; }
         o2[i / 2] = __floats2bfloat162_rn(x0, x1);
       }
-      uint4* op = reinterpret_cast<uint4*>(a.out + q * COUT + c0);
+      uint4* op = reinterpret_cast<uint4*>(a.out + q * COUT + co);
       op[0] = ov[0];
       op[1] = ov[1];
     }
@@ -357,18 +381,22 @@ __device__ __forceinline__ float out1x1_value(const uint4& lo, const uint4& hi, 
 
 template <int C>
 __global__ void pool_kernel(LevelGeom gi, LevelGeom go, const bf16* in, bf16* out) {
+  tpf::chain_begin();
   tpf::tc::pdl_trigger();
   const long long n = go.P() * (C / 8);
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     pool_item<C>(gi, go, in, out, i);
+  tpf::chain_end();
 }
 
 template <int C>
 __global__ void upadd_relu_kernel(LevelGeom gf, LevelGeom gc, const bf16* t, const bf16* skip, bf16* out) {
+  tpf::chain_begin();
   tpf::tc::pdl_trigger();
   const long long n = gf.P() * (C / 8);
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     upadd_item<C>(gf, gc, t, skip, out, i);
+  tpf::chain_end();
 }
 
 // backward of up(): out(level l+1) = 2x2 sum of in(level l)
@@ -441,6 +469,7 @@ __global__ void pack_input_kernel(LevelGeom g, const float* in, bf16* xin) {
 
 // y[B][H][W] = d0 . w_out + b_out
 __global__ void out1x1_kernel(LevelGeom g, const bf16* d0, const float* w, const float* bo, float* yout) {
+  tpf::chain_begin();
   const long long n = (long long)g.B * g.H * g.W;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const int x = (int)(i % g.W);
@@ -450,6 +479,7 @@ __global__ void out1x1_kernel(LevelGeom g, const bf16* d0, const float* w, const
     const uint4* p = reinterpret_cast<const uint4*>(d0 + g.q(b, y, x) * kOutC);
     yout[i] = out1x1_value(p[0], p[1], w, bo);
   }
+  tpf::chain_end();
 }
 
 // backward of the 1x1 output layer: g_d0 = dy * w * (d0 > 0); gw += sum dy*d0; gb += sum dy
@@ -988,20 +1018,65 @@ inline int grid_for(long long n, int threads = 256) {
 }
 
 // ---- conv dispatch ---------------------------------------------------------------------------
-template <int CIN, int COUT>
-int launch_conv_t(const ConvArgs& a, cudaStream_t s) {
-  constexpr int smem = conv_smem_bytes(CIN, COUT);
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+    else
+      cudaGetLastError();
+  }
+  return fn;
+}
+
+// Tensor map of the pixel-major [P][CIN] BF16 activations read by the
+// convolution: boxes of 130 pixels x min(CIN, 64) channels, swizzled to match
+// the MMA operand layout.
+int window_map(CUtensorMap* m, const bf16* in, int cin, long long P) {
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) {
+    tpf::set_error("cuTensorMapEncodeTiled is not available from the driver");
+    return TPF_ECUDA;
+  }
+  const int box_c = cin < 64 ? cin : 64;
+  const cuuint64_t dims[2] = {(cuuint64_t)cin, (cuuint64_t)P};
+  const cuuint64_t strides[1] = {(cuuint64_t)cin * sizeof(bf16)};
+  const cuuint32_t box[2] = {(cuuint32_t)box_c, (cuuint32_t)kWin};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUtensorMapSwizzle sw = box_c == 64 ? CU_TENSOR_MAP_SWIZZLE_128B
+                                            : (box_c == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B);
+  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16*>(in), dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    tpf::set_error("cuTensorMapEncodeTiled failed (%d) for %d channels x %lld pixels", (int)r, cin, P);
+    return TPF_ECUDA;
+  }
+  return TPF_OK;
+}
+
+template <int CIN, int COUT, int NS>
+int launch_conv_ns(const CUtensorMap& m, const ConvArgs& a, long long tiles, cudaStream_t s) {
+  constexpr int smem = conv_tma_smem_bytes(CIN, NS);
   static bool attr = false;
   if (!attr) {
-    TPF_CUDA_TRY(cudaFuncSetAttribute(conv3x3_tc_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      smem));
+    TPF_CUDA_TRY(cudaFuncSetAttribute(conv3x3_tma_kernel<CIN, COUT, NS>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     attr = true;
   }
-  const long long tiles = (a.P + kTile - 1) / kTile;
   // programmatic dependent launch: the prologue overlaps the previous kernel,
   // whose outputs are read only after griddepcontrol.wait
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)tiles);
+  cfg.gridDim = dim3((unsigned)tiles, COUT / NS);
   cfg.blockDim = dim3(128);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
@@ -1010,8 +1085,21 @@ int launch_conv_t(const ConvArgs& a, cudaStream_t s) {
   pdl[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = pdl;
   cfg.numAttrs = 1;
-  TPF_CUDA_TRY(cudaLaunchKernelEx(&cfg, conv3x3_tc_kernel<CIN, COUT>, a));
+  TPF_CUDA_TRY(cudaLaunchKernelEx(&cfg, conv3x3_tma_kernel<CIN, COUT, NS>, m, a));
   return TPF_OK;
+}
+
+// Output slices: the whole COUT per CTA when the pixel tiles alone fill the
+// GPU, else 16 channels per CTA (more CTAs, each with less weight traffic).
+template <int CIN, int COUT>
+int launch_conv_t(const ConvArgs& a, cudaStream_t s) {
+  CUtensorMap m;
+  int st = window_map(&m, a.in, CIN, a.P);
+  if (st) return st;
+  const long long tiles = (a.P + kTile - 1) / kTile;
+  constexpr int NW = conv_ns_wide(CIN, COUT);
+  if (tiles >= 128 || COUT == 16) return launch_conv_ns<CIN, COUT, NW>(m, a, tiles, s);
+  return launch_conv_ns<CIN, COUT, 16>(m, a, tiles, s);
 }
 
 #define TPF_CONV_CASES(X) \
@@ -1196,11 +1284,11 @@ int wgrad(tpf_unet* n, int l, int B, const bf16* X, const bf16* dz, cudaStream_t
 
 template <int C>
 void pool_t(const LevelGeom& gi, const LevelGeom& go, const bf16* in, bf16* out, cudaStream_t s) {
-  pool_kernel<C><<<grid_for(go.P() * (C / 8)), 256, 0, s>>>(gi, go, in, out);
+  tpf::launch_chained(pool_kernel<C>, grid_for(go.P() * (C / 8)), 256, 0, s, gi, go, in, out);
 }
 template <int C>
 void upadd_t(const LevelGeom& gf, const LevelGeom& gc, const bf16* t, const bf16* sk, bf16* out, cudaStream_t s) {
-  upadd_relu_kernel<C><<<grid_for(gf.P() * (C / 8)), 256, 0, s>>>(gf, gc, t, sk, out);
+  tpf::launch_chained(upadd_relu_kernel<C>, grid_for(gf.P() * (C / 8)), 256, 0, s, gf, gc, t, sk, out);
 }
 template <int C>
 void downsum_t(const LevelGeom& gf, const LevelGeom& gc, const bf16* in, bf16* out, cudaStream_t s) {
@@ -1350,7 +1438,7 @@ int forward(tpf_unet* n, int B, cudaStream_t s) {
   upadd_t<16>(g0, g1, n->t0, n->e0, n->d0a, s);
   if ((st = conv(n, 13, B, n->d0a, n->d0, s))) return st;
   const ParamLayout& L = layout();
-  out1x1_kernel<<<grid_for((long long)B * n->H * n->W), 256, 0, s>>>(g0, n->d0, n->params + L.wo, n->params + L.bo,
+  tpf::launch_chained(out1x1_kernel, grid_for((long long)B * n->H * n->W), 256, 0, s, g0, n->d0, n->params + L.wo, n->params + L.bo,
                                                                      n->out);
   TPF_CUDA_TRY(cudaGetLastError());
   n->last_batch = B;

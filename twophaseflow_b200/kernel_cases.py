@@ -451,10 +451,12 @@ def ppe_case(N, precision, reps, tol=1e-8):
             "us_per_iteration": round(ms * 1e3 / max(it, 1), 2)}
 
 
-def learned_case(N, reps, maxiter=None, tol=1e-8):
-    """Network-preconditioned flexible CG (shipped weights, two-level mode) on
-    the droplet PPE; ``maxiter`` bounds the iterations (no fallback) for
-    profiling a fixed amount of work."""
+def learned_case(N, reps, maxiter=None, tol=1e-8, outer="fgmres"):
+    """Network-preconditioned flexible GMRES (``outer='fgmres'``, the
+    solver's default restart and sweeps) or flexible CG (``outer='fcg'``;
+    shipped weights, two-level mode) on the droplet PPE; ``maxiter`` bounds
+    the iterations (no fallback; whole restart cycles for GMRES) for profiling
+    a fixed amount of work."""
     import torch
     from . import UniformGrid
     from .learned import PPESolverLearned
@@ -465,6 +467,7 @@ def learned_case(N, reps, maxiter=None, tol=1e-8):
         pseudo_maxiter = 20000
         ppe_learned_maxiter = maxiter if maxiter else 20000
         ppe_learned_fallback = False
+        ppe_learned_outer = outer
 
     rho = torch.from_numpy(droplet_density(N, seed=0)).cuda()
     rhs = torch.from_numpy(divergence_rhs(N, seed=1)).cuda()
@@ -490,8 +493,40 @@ def learned_case(N, reps, maxiter=None, tol=1e-8):
         ts.append(e0.elapsed_time(e1))
     it = s.last_diagnostics["ppe_learned_iterations"]
     ms = min(ts)
-    return {"case": "learned", "N": list(N), "ms": round(ms, 3), "iterations": it,
+    return {"case": "learned", "outer": outer, "N": list(N), "ms": round(ms, 3), "iterations": it,
             "us_per_iteration": round(ms * 1e3 / max(it, 1), 2)}
+
+
+def smoother_case(N, sweeps=256, block=4):
+    """The learned preconditioner's damped-Jacobi smoother alone on the droplet
+    operator: ``sweeps`` sweeps, ``block`` per launch (temporally blocked
+    kernel), timed from a CUDA graph.  Algorithmic bytes per launch: z, r,
+    D^-1 and the two couplings read once, z written once (48 B per node)."""
+    import torch
+    from . import UniformGrid, _lib
+    from .learned import PPESolverLearned
+    from .workloads import divergence_rhs, droplet_density
+
+    class Cfg:
+        pseudo_tol = 1e-8
+        pseudo_maxiter = 20000
+
+    s = PPESolverLearned(None, Cfg(), UniformGrid(N))
+    s.prepare_operator(torch.from_numpy(droplet_density(N, seed=0)).cuda())
+    r = torch.from_numpy(divergence_rhs(N, seed=1)).cuda()
+    z = torch.zeros_like(r)
+    _lib.check(s.lib.tpf_lppe_set_smooth_block(s._lp, block))
+
+    def call():
+        _lib.check(s.lib.tpf_lppe_smooth(s._lp, _lib.dptr(z), _lib.dptr(r), _lib.dptr(z), sweeps, 0.8,
+                                         _lib.current_stream_handle()))
+
+    ms = _graph_time(call, 1)
+    launches = (sweeps + block - 1) // block
+    us = ms * 1e3 / launches
+    ndof = r.numel()
+    return {"case": "smoother", "N": list(N), "block": block, "launches": launches, "us_per_launch": round(us, 3),
+            "GBps": round(48.0 * ndof / (us * 1e-6) / 1e9, 1)}
 
 
 def batched_case(n_cases=32, nmin=128, nmax=512, reps=3, seed=0, tol=1e-8):
@@ -587,7 +622,7 @@ def gmres_case(N, line, reps, maxiter=None, tol=1e-8):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["ccd", "ppe", "learned", "batched", "gmres", "corrector", "curvature", "rhiechow", "advect", "reinit", "viscous", "step"])
+    ap.add_argument("case", choices=["ccd", "ppe", "learned", "smoother", "batched", "gmres", "corrector", "curvature", "rhiechow", "advect", "reinit", "viscous", "step"])
     ap.add_argument("--line", default="thomas", choices=["thomas", "pcr"], help="gmres: line solver")
     ap.add_argument("--N", type=int, nargs="+", required=True)
     ap.add_argument("--axis", type=int, default=0)
@@ -597,6 +632,7 @@ def main(argv=None):
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--nmin", type=int, default=128, help="batched: smallest nodes per axis")
     ap.add_argument("--nmax", type=int, default=512, help="batched: largest nodes per axis")
+    ap.add_argument("--outer", default="fgmres", choices=["fcg", "fgmres"], help="learned: outer Krylov method")
     ap.add_argument("--maxiter", type=int, default=0,
                     help="learned: stop after this many iterations; gmres: after this many restart cycles")
     a = ap.parse_args(argv)
@@ -605,7 +641,9 @@ def main(argv=None):
     elif a.case == "ppe":
         r = ppe_case(tuple(a.N), a.precision, a.reps)
     elif a.case == "learned":
-        r = learned_case(tuple(a.N), a.reps, a.maxiter or None)
+        r = learned_case(tuple(a.N), a.reps, a.maxiter or None, outer=a.outer)
+    elif a.case == "smoother":
+        r = smoother_case(tuple(a.N))
     elif a.case == "gmres":
         r = gmres_case(tuple(a.N), a.line, a.reps, a.maxiter or None)
     elif a.case == "corrector":

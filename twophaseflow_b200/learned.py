@@ -1,4 +1,4 @@
-"""Learned PPE preconditioner: U-Net network, training, and the flexible-CG solver.
+"""Learned PPE preconditioner: U-Net network, training, and the flexible Krylov solver.
 
 The reference has no learned component (its PPE Krylov loops are SciPy's
 ``cg`` / ``gmres``, src/twophase/ppe/gmres_helpers.py:16-80).  This module is
@@ -14,9 +14,9 @@ the B200 addition built on top of the plain method:
   network sees (tpf_lppe_pair).
 * ``train`` -- Adam on the relative squared error of the scaled correction.
 * ``PPESolverLearned`` -- an ``IPPESolver`` with the reference's
-  ``solve(rhs, rho, dt, p_init)`` contract whose solve is flexible CG
-  preconditioned by the network (tpf_lppe_solve), checked on the true residual,
-  falling back to plain Jacobi PCG when the residual stalls.
+  ``solve(rhs, rho, dt, p_init)`` contract whose solve is flexible GMRES (or
+  flexible CG) preconditioned by the network (tpf_lppe_solve), checked on the
+  true residual, falling back to plain Jacobi PCG when the residual stalls.
 
 All arithmetic runs on the GPU in the CUDA library; PyTorch only holds device
 memory.
@@ -175,7 +175,7 @@ def default_coarsen(shape, meta=None) -> int:
     shipped weights): 4, or 8 once the grid has more than ~5.7x that many
     cells per axis.  Both were validated on held-out fields (4 at 512^2, 8 at
     1024^2); with 4 at 1024^2 the coarse problem outgrows the network's
-    receptive field and flexible CG stalls."""
+    receptive field and the flexible iteration stalls."""
     meta = meta or {}
     c_train = float(meta.get("grid", 512)) / float(meta.get("coarsen", 4))
     cells = max(int(n) - 1 for n in shape)
@@ -194,7 +194,7 @@ def load_params(path: str = DEFAULT_WEIGHTS) -> np.ndarray:
 
 # ---------------------------------------------------------------------------------------------
 class PPESolverLearned(PPESolverFVMMatrixFree):
-    """IPPESolver: flexible CG preconditioned by the trained U-Net (2-D, wall).
+    """IPPESolver: flexible GMRES / CG preconditioned by the trained U-Net (2-D, wall).
 
     Options are read from the solver config like the reference's own
     (``pseudo_tol``, ``pseudo_maxiter``) plus ``ppe_learned_coarsen`` (b > 1:
@@ -202,14 +202,16 @@ class PPESolverLearned(PPESolverFVMMatrixFree):
     two-grid cycle; 1: the network reads the fine residual; default: 4 or 8,
     whichever puts the coarse grid nearest the training size, see
     ``default_coarsen``),
-    ``ppe_learned_smooth`` (damped Jacobi sweeps after the network, default 3),
+    ``ppe_learned_smooth`` (damped Jacobi sweeps after the network, default 16),
     ``ppe_learned_omega`` (0.8), ``ppe_learned_weights`` (path of the trained
     parameters), ``ppe_learned_fallback`` (finish with plain Jacobi PCG on a
-    stall, True) and ``ppe_learned_outer``: 'fcg' (truncated flexible CG with
-    ``ppe_learned_window`` stored directions, default) or 'fgmres' (flexible
-    GMRES with restart ``ppe_learned_restart``, 30: each basis vector
+    stall, True) and ``ppe_learned_outer``: 'fgmres' (flexible GMRES with
+    restart ``ppe_learned_restart``, default 80: each basis vector
     preconditioned by the network, the solution built from the preconditioned
-    basis).
+    basis; the default) or 'fcg' (truncated flexible CG with
+    ``ppe_learned_window`` stored directions).  The defaults (FGMRES(80), 16
+    sweeps, omega 0.8) were chosen on validation density fields (seeds 21-30
+    at 512^2, 21-24 at 1024^2) that neither training nor the benchmark use.
     """
 
     scheme_names = ("fvm_learned",)
@@ -224,16 +226,16 @@ class PPESolverLearned(PPESolverFVMMatrixFree):
         if self.ndim != 2:
             raise ValueError("the learned preconditioner is two-dimensional")
         solver_cfg = getattr(config, "solver", config)
-        self.smooth = int(getattr(solver_cfg, "ppe_learned_smooth", 3))
+        self.smooth = int(getattr(solver_cfg, "ppe_learned_smooth", 16))
         self.omega = float(getattr(solver_cfg, "ppe_learned_omega", 0.8))
         self.fallback = bool(getattr(solver_cfg, "ppe_learned_fallback", True))
         self.learned_maxiter = int(getattr(solver_cfg, "ppe_learned_maxiter", max(self.maxiter, 2000)))
         self.window = int(getattr(solver_cfg, "ppe_learned_window", 8))
-        outer = str(getattr(solver_cfg, "ppe_learned_outer", "fcg")).strip().lower()
+        outer = str(getattr(solver_cfg, "ppe_learned_outer", "fgmres")).strip().lower()
         if outer not in ("fcg", "fgmres"):
             raise ValueError("ppe_learned_outer must be 'fcg' (flexible CG) or 'fgmres' (flexible GMRES)")
         self.outer = outer
-        self.restart = int(getattr(solver_cfg, "ppe_learned_restart", 30))
+        self.restart = int(getattr(solver_cfg, "ppe_learned_restart", 80))
         meta = {}
         if params is None:
             wpath = str(getattr(solver_cfg, "ppe_learned_weights", DEFAULT_WEIGHTS))
