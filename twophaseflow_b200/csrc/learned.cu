@@ -261,30 +261,35 @@ __global__ void fcg_smooth_kernel(LGrid g, const double* zin, const double* r, d
 constexpr int kSmTX = 32, kSmTY = 16, kSmK = 4;
 constexpr int kSmW = kSmTX + 2 * kSmK, kSmH = kSmTY + 2 * kSmK;
 
-__global__ void __launch_bounds__(256) smooth_block_kernel(LGrid g, const double* zin, const double* r,
-                                                           double omega, int k, const FcgState* st, double* zout) {
+constexpr int kSmThreads = 512;
+
+__global__ void __launch_bounds__(kSmThreads, 2) smooth_block_kernel(LGrid g, const double* zin, const double* r,
+                                                                     double omega, int k, const FcgState* st,
+                                                                     double* zout) {
   tpf::chain_begin();
   if (st->done) return;
   // only z goes through shared memory; each thread keeps r, D^-1 and the four
-  // couplings of its own kPer nodes (e = tid + 256 j of the tile with halo) in
-  // registers for all k sweeps and holds its last updates for the store
+  // couplings of its own kPer nodes (e = tid + kSmThreads j of the tile with
+  // halo) in registers for all k sweeps and holds its last updates for the store
   __shared__ double sz[2][kSmH][kSmW];
-  constexpr int kPer = (kSmH * kSmW + 255) / 256;
+  constexpr int kPer = (kSmH * kSmW + kSmThreads - 1) / kSmThreads;
   const int tiles1 = (g.n1 + kSmTX - 1) / kSmTX;
   const int base0 = (int)(blockIdx.x / tiles1) * kSmTY - kSmK;
   const int base1 = (int)(blockIdx.x % tiles1) * kSmTX - kSmK;
   double lz[kPer], lr[kPer], ld[kPer], m0[kPer], p0[kPer], m1[kPer], p1[kPer];
-  unsigned flags[kPer];   // bit 0 in the domain, 1 pinned, 2..5 neighbours -0 +0 -1 +1 exist
+  // bit 0 in the domain, 1 pinned, 2..5 neighbours -0 +0 -1 +1 exist,
+  // bits 8..15 the tile column, 16..23 the tile row
+  unsigned flags[kPer];
 #pragma unroll
   for (int j = 0; j < kPer; ++j) {
-    const int e = threadIdx.x + j * 256;
+    const int e = threadIdx.x + j * kSmThreads;
     const int a = e / kSmW, c = e - (e / kSmW) * kSmW;
     const int i0 = base0 + a, i1 = base1 + c;
     const bool in = e < kSmH * kSmW && i0 >= 0 && i0 < g.n0 && i1 >= 0 && i1 < g.n1;
     const int i = in ? i0 * g.n1 + i1 : 0;
     const bool h0m = in && i0 > 0, h0p = in && i0 < g.n0 - 1, h1m = in && i1 > 0, h1p = in && i1 < g.n1 - 1;
     flags[j] = (in ? 1u : 0u) | ((in && i == g.pin) ? 2u : 0u) | (h0m ? 4u : 0u) | (h0p ? 8u : 0u) |
-               (h1m ? 16u : 0u) | (h1p ? 32u : 0u);
+               (h1m ? 16u : 0u) | (h1p ? 32u : 0u) | ((unsigned)c << 8) | ((unsigned)a << 16);
     lz[j] = in ? zin[i] : 0.0;
     lr[j] = in ? r[i] : 0.0;
     ld[j] = in ? g.dinvS[i] : 0.0;
@@ -295,9 +300,9 @@ __global__ void __launch_bounds__(256) smooth_block_kernel(LGrid g, const double
   }
 #pragma unroll
   for (int j = 0; j < kPer; ++j) {
-    const int e = threadIdx.x + j * 256;
+    const int e = threadIdx.x + j * kSmThreads;
     if (e < kSmH * kSmW) {
-      const int a = e / kSmW, c = e - (e / kSmW) * kSmW;
+      const int a = (int)((flags[j] >> 16) & 255u), c = (int)((flags[j] >> 8) & 255u);
       sz[0][a][c] = lz[j];
       sz[1][a][c] = 0.0;
     }
@@ -307,8 +312,7 @@ __global__ void __launch_bounds__(256) smooth_block_kernel(LGrid g, const double
   for (int sweep = 1; sweep <= k; ++sweep) {
 #pragma unroll
     for (int j = 0; j < kPer; ++j) {
-      const int e = threadIdx.x + j * 256;
-      const int a = e / kSmW, c = e - (e / kSmW) * kSmW;
+      const int a = (int)((flags[j] >> 16) & 255u), c = (int)((flags[j] >> 8) & 255u);
       if (!(flags[j] & 1u) || a < sweep || a >= kSmH - sweep || c < sweep || c >= kSmW - sweep) continue;
       const double v =
           (flags[j] & 2u)
@@ -324,8 +328,7 @@ __global__ void __launch_bounds__(256) smooth_block_kernel(LGrid g, const double
   }
 #pragma unroll
   for (int j = 0; j < kPer; ++j) {
-    const int e = threadIdx.x + j * 256;
-    const int a = e / kSmW, c = e - (e / kSmW) * kSmW;
+    const int a = (int)((flags[j] >> 16) & 255u), c = (int)((flags[j] >> 8) & 255u);
     if (!(flags[j] & 1u) || a < kSmK || a >= kSmK + kSmTY || c < kSmK || c >= kSmK + kSmTX) continue;
     zout[(base0 + a) * g.n1 + base1 + c] = lz[j];
   }
@@ -596,24 +599,30 @@ __global__ void coarse_setup_kernel(LGrid g, const double* dc, const float* feat
 }
 
 // r1 = r - S (w D^-1 r), pin 0 (the pre-smoothing sweep from a zero start)
+// residual after the pre-smoothing sweep z1 = omega D^-1 r: r1 = r - S z1 at
+// node i (pin 0)
+__device__ __forceinline__ double pre_residual(const LGrid& g, const double* r, double omega, int i, int i0, int i1) {
+  auto zf = [&](int j) -> double { return (j == g.pin) ? 0.0 : omega * g.dinvS[j] * r[j]; };
+  double v = 0.0;
+  if (i != g.pin) {
+    const double sm0 = (i0 > 0) ? g.s0[i - g.n1] : 0.0, sp0 = g.s0[i];
+    const double sm1 = (i1 > 0) ? g.s1[i - 1] : 0.0, sp1 = g.s1[i];
+    double off = 0.0;
+    if (i0 > 0) off += sm0 * zf(i - g.n1);
+    if (i0 < g.n0 - 1) off += sp0 * zf(i + g.n1);
+    if (i1 > 0) off += sm1 * zf(i - 1);
+    if (i1 < g.n1 - 1) off += sp1 * zf(i + 1);
+    v = r[i] - ((sm0 + sp0 + sm1 + sp1) * zf(i) - off);
+  }
+  return v;
+}
+
 __global__ void vc_pre_kernel(LGrid g, const double* r, double omega, const FcgState* st, double* r1) {
   tpf::chain_begin();
   if (st && st->done) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.ndof; i += gridDim.x * blockDim.x) {
     const int i0 = i / g.n1, i1 = i - i0 * g.n1;
-    auto zf = [&](int j) -> double { return (j == g.pin) ? 0.0 : omega * g.dinvS[j] * r[j]; };
-    double v = 0.0;
-    if (i != g.pin) {
-      const double sm0 = (i0 > 0) ? g.s0[i - g.n1] : 0.0, sp0 = g.s0[i];
-      const double sm1 = (i1 > 0) ? g.s1[i - 1] : 0.0, sp1 = g.s1[i];
-      double off = 0.0;
-      if (i0 > 0) off += sm0 * zf(i - g.n1);
-      if (i0 < g.n0 - 1) off += sp0 * zf(i + g.n1);
-      if (i1 > 0) off += sm1 * zf(i - 1);
-      if (i1 < g.n1 - 1) off += sp1 * zf(i + 1);
-      v = r[i] - ((sm0 + sp0 + sm1 + sp1) * zf(i) - off);
-    }
-    r1[i] = v;
+    r1[i] = pre_residual(g, r, omega, i, i0, i1);
   }
   tpf::chain_end();
 }
@@ -648,6 +657,54 @@ __global__ void coarse_scale_kernel(const double* part, int nb, int nc, FcgState
     const double sc = sqrt(v[0] / nc);
     st->sc = sc;
     st->inv_sc = sc > 0.0 ? 1.0 / sc : 0.0;
+  }
+  tpf::chain_end();
+}
+
+// vc_pre, restrict and coarse_scale in one launch: rc = R r1 with each fine
+// node's pre-smoothed residual r1 formed once on the fly and summed in the
+// same order as the separate kernels (same bits), partials of (rc D_c^-1/2)^2;
+// the last block to finish sums the partials in block order into the input
+// scale s_c and, inside the flexible GMRES cycle (gdone non-null), copies the
+// cycle's done flag into st->done for the kernels after it
+__global__ void __launch_bounds__(kRedThreads) restrict_pre_kernel(LGrid g, const double* r, double omega,
+                                                                   FcgState* st, const int* gdone, double* rc,
+                                                                   double* part, unsigned* arrive) {
+  tpf::chain_begin();
+  const bool skip = gdone ? (*gdone != 0) : (st->done != 0);
+  const int nc = g.nc0 * g.nc1;
+  double v[1] = {0.0};
+  if (!skip) {
+    for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += gridDim.x * blockDim.x) {
+      const int I0 = I / g.nc1, I1 = I - I0 * g.nc1;
+      double acc = 0.0;
+      for (int a0 = I0 * g.b; a0 < min(g.n0, (I0 + 1) * g.b); ++a0)
+        for (int a1 = I1 * g.b; a1 < min(g.n1, (I1 + 1) * g.b); ++a1)
+          acc += pre_residual(g, r, omega, a0 * g.n1 + a1, a0, a1);
+      rc[I] = acc;
+      const double q = acc * g.dcis[I];
+      v[0] += q * q;
+    }
+  }
+  block_partials<1>(v, part);
+  __shared__ int s_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = (atomicAdd(arrive, 1u) == gridDim.x - 1) ? 1 : 0;
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    double t[1];
+    reduce_partials<1>(part, gridDim.x, t);
+    if (threadIdx.x == 0) {
+      if (!skip) {
+        const double sc = sqrt(t[0] / nc);
+        st->sc = sc;
+        st->inv_sc = sc > 0.0 ? 1.0 / sc : 0.0;
+      }
+      if (gdone) st->done = *gdone;
+      *arrive = 0u;
+    }
   }
   tpf::chain_end();
 }
@@ -852,6 +909,7 @@ struct tpf_lppe {
   cudaGraphExec_t gexec = nullptr;
   long long gkey[6] = {0, 0, 0, 0, 0, 0};
   int smooth_block = 4;   // sweeps per smoother launch (1: one sweep per launch)
+  unsigned* arrive = nullptr;   // last-block counter of restrict_pre_kernel (zero between launches)
   std::vector<void*> allocs;
 };
 
@@ -896,44 +954,56 @@ int features(tpf_lppe* lp, const double* rho, cudaStream_t s) {
 // z = B(r): network (+ smoothing); result in lp->z (smooth even) or lp->z2
 // n damped-Jacobi sweeps ping-ponging between cur and other (cur ends holding
 // the result): smooth_block sweeps per launch
-void enqueue_sweeps(tpf_lppe* lp, int n, double omega, cudaStream_t s, double*& cur, double*& other) {
+// (the residual is rin; with last_out non-null the final launch writes there
+// and cur ends as last_out)
+void enqueue_sweeps(tpf_lppe* lp, int n, double omega, cudaStream_t s, const double* rin, double*& cur,
+                    double*& other, double* last_out = nullptr) {
   const LGrid& g = lp->g;
   if (lp->smooth_block <= 1) {
     for (int k = 0; k < n; ++k) {
-      tpf::launch_chained(fcg_smooth_kernel, ew_blocks(g.ndof), 256, 0, s, g, cur, lp->r, omega, lp->st, other);
-      std::swap(cur, other);
+      double* dst = (last_out && k == n - 1) ? last_out : other;
+      tpf::launch_chained(fcg_smooth_kernel, ew_blocks(g.ndof), 256, 0, s, g, cur, rin, omega, lp->st, dst);
+      other = cur;
+      cur = dst;
     }
     return;
   }
   const int tiles = ((g.n0 + kSmTY - 1) / kSmTY) * ((g.n1 + kSmTX - 1) / kSmTX);
   for (int k = 0; k < n; k += lp->smooth_block) {
     const int kk = std::min(lp->smooth_block, n - k);
-    tpf::launch_chained(smooth_block_kernel, tiles, 256, 0, s, g, cur, lp->r, omega, kk, lp->st, other);
-    std::swap(cur, other);
+    double* dst = (last_out && k + kk >= n) ? last_out : other;
+    tpf::launch_chained(smooth_block_kernel, tiles, kSmThreads, 0, s, g, cur, rin, omega, kk, lp->st, dst);
+    other = cur;
+    cur = dst;
   }
 }
 
-int enqueue_precond(tpf_lppe* lp, int smooth, double omega, cudaStream_t s, double** zout) {
+// z = B(r).  Two-level mode: rin (default lp->r) is read in place; with zfinal
+// non-null the last kernel writes z there; gdone: the flexible GMRES cycle's
+// done flag (the preconditioner's kernels skip once it is set).
+int enqueue_precond(tpf_lppe* lp, int smooth, double omega, cudaStream_t s, double** zout,
+                    const double* rin = nullptr, double* zfinal = nullptr, const int* gdone = nullptr) {
   const LGrid& g = lp->g;
   if (g.b > 1) {
-    const int nc = g.nc0 * g.nc1;
-    tpf::launch_chained(vc_pre_kernel, ew_blocks(g.ndof), 256, 0, s, g, lp->r, omega, lp->st, lp->r1);
-    tpf::launch_chained(restrict_kernel, kRedBlocks, kRedThreads, 0, s, g, lp->r1, lp->rc, lp->st, lp->part);
-    tpf::launch_chained(coarse_scale_kernel, 1, 256, 0, s, lp->part, kRedBlocks, nc, lp->st);
-    tpf::launch_chained(pack_coarse_kernel, ew_blocks((g.H + 2) * (g.W + 2)), 256, 0, s, g, lp->rc, lp->cc0, lp->cc1, lp->st,
-                                                                         tpf::unet_input(lp->net));
+    if (!rin) rin = lp->r;
+    tpf::launch_chained(restrict_pre_kernel, kRedBlocks, kRedThreads, 0, s, g, rin, omega, lp->st, gdone, lp->rc,
+                        lp->part, lp->arrive);
+    tpf::launch_chained(pack_coarse_kernel, ew_blocks((g.H + 2) * (g.W + 2)), 256, 0, s, g, lp->rc, lp->cc0,
+                        lp->cc1, lp->st, tpf::unet_input(lp->net));
     TPF_CUDA_TRY(cudaGetLastError());
     int st = tpf::unet_forward_packed(lp->net, 1, s);
     if (st) return st;
-    double* cur = lp->z;
-    double* other = lp->z2;
+    double* first = (zfinal && smooth <= 1) ? zfinal : lp->z;
     if (smooth > 0) {
-      tpf::launch_chained(prolong_smooth_kernel, ew_blocks(g.ndof), 256, 0, s, g, tpf::unet_output(lp->net), lp->r, omega, lp->st,
-                                                               lp->z);
+      tpf::launch_chained(prolong_smooth_kernel, ew_blocks(g.ndof), 256, 0, s, g, tpf::unet_output(lp->net), rin,
+                          omega, lp->st, first);
     } else {
-      tpf::launch_chained(prolong_kernel, ew_blocks(g.ndof), 256, 0, s, g, tpf::unet_output(lp->net), lp->r, omega, lp->st, lp->z);
+      tpf::launch_chained(prolong_kernel, ew_blocks(g.ndof), 256, 0, s, g, tpf::unet_output(lp->net), rin, omega,
+                          lp->st, first);
     }
-    enqueue_sweeps(lp, smooth - 1, omega, s, cur, other);
+    double* cur = first;
+    double* other = lp->z2;
+    enqueue_sweeps(lp, smooth - 1, omega, s, rin, cur, other, zfinal);
     TPF_CUDA_TRY(cudaGetLastError());
     *zout = cur;
     return TPF_OK;
@@ -946,7 +1016,7 @@ int enqueue_precond(tpf_lppe* lp, int smooth, double omega, cudaStream_t s, doub
   tpf::launch_chained(fcg_unpack_kernel, ew_blocks(g.ndof), 256, 0, s, g, tpf::unet_output(lp->net), lp->st, lp->z);
   double* cur = lp->z;
   double* other = lp->z2;
-  enqueue_sweeps(lp, smooth, omega, s, cur, other);
+  enqueue_sweeps(lp, smooth, omega, s, lp->r, cur, other);
   TPF_CUDA_TRY(cudaGetLastError());
   *zout = cur;
   return TPF_OK;
@@ -1118,6 +1188,12 @@ int solve_fgmres(tpf_lppe* lp, const tpf_learned_options& o, cudaStream_t s, boo
     return TPF_OK;
   };
   auto precond = [&](const double* in, double* outv, cudaStream_t cs, const int* done) -> int {
+    if (g.b > 1) {
+      // the basis vector is read in place and z lands in the Z column; the
+      // two-level path needs no fine-grid input scale
+      double* z = nullptr;
+      return enqueue_precond(lp, o.smooth, o.omega, cs, &z, in, outv, done);
+    }
     tpf::launch_chained(fgm_in_kernel, kRedBlocks, kRedThreads, 0, cs, g, in, done, lp->r, lp->part);
     tpf::launch_chained(fgm_scale_kernel, 1, 256, 0, cs, lp->part, kRedBlocks, g.ndof, done, lp->st);
     double* z = nullptr;
@@ -1217,8 +1293,14 @@ int tpf_lppe_create(tpf_lppe** out, tpf_ppe* ppe, tpf_unet* net, int coarsen) {
     const size_t nc = (size_t)nc0 * nc1;
     if ((st = lalloc(lp, &lp->r1, n)) || (st = lalloc(lp, &lp->rc, nc)) || (st = lalloc(lp, &lp->dc, nc)) ||
         (st = lalloc(lp, &lp->dcis, nc)) || (st = lalloc(lp, &lp->featc, nc)) || (st = lalloc(lp, &lp->cc0, nc)) ||
-        (st = lalloc(lp, &lp->cc1, nc)) || (st = lalloc(lp, &lp->part2, kRedBlocks)))
+        (st = lalloc(lp, &lp->cc1, nc)) || (st = lalloc(lp, &lp->part2, kRedBlocks)) ||
+        (st = lalloc(lp, &lp->arrive, 1)))
       return fail(st);
+    if (cudaMemset(lp->arrive, 0, sizeof(unsigned)) != cudaSuccess) {
+      cudaGetLastError();
+      tpf::set_error("cudaMemset failed");
+      return fail(TPF_ECUDA);
+    }
     lp->g.dcis = lp->dcis;
     lp->g.featc = lp->featc;
   }
@@ -1325,7 +1407,7 @@ int tpf_lppe_smooth(tpf_lppe* lp, const double* zin, const double* r, double* zo
   TPF_CUDA_TRY(cudaMemcpyAsync(lp->z, zin, bytes, cudaMemcpyDeviceToDevice, s));
   double* cur = lp->z;
   double* other = lp->z2;
-  enqueue_sweeps(lp, sweeps, omega, s, cur, other);
+  enqueue_sweeps(lp, sweeps, omega, s, lp->r, cur, other);
   TPF_CUDA_TRY(cudaGetLastError());
   TPF_CUDA_TRY(cudaMemcpyAsync(zout, cur, bytes, cudaMemcpyDeviceToDevice, s));
   return TPF_OK;
