@@ -202,11 +202,13 @@ def test_gmres_with_truncated_pcr_converges(cuda_device):
     np.testing.assert_allclose(p, pd, rtol=1e-5, atol=1e-6 * np.abs(pd).max())
 
 
-@pytest.mark.parametrize("kind", [0, 1, 2])
+@pytest.mark.parametrize("kind", [0, 1, 2, 3])
 def test_batched_solve_matches_individual_solves(cuda_device, kind):
-    """Uneven grids in one persistent launch: same solutions (and iteration
+    """Uneven grids in one batched solve: same solutions (and iteration
     counts within one) as solving each system on its own -- band-resident
-    (kind 0, the default here, and 2, forced) and all-global (kind 1)."""
+    (kind 0, the default here, and 2, forced), all-global persistent (kind 1)
+    and the batched streaming PCG (kind 3: every system's iterations in the
+    same two launches)."""
     import ctypes as C
     import torch
     from twophaseflow_b200 import PPESolverFVMMatrixFree, UniformGrid, _lib, solve_batched
@@ -227,6 +229,45 @@ def test_batched_solve_matches_individual_solves(cuda_device, kind):
         assert abs(it1 - its_b[k]) <= 1, (k, it1, its_b[k])
         scale = float(torch.max(torch.abs(p1)))
         assert float(torch.max(torch.abs(pb[k] - p1))) <= 1e-8 * scale
+
+
+def test_streaming_batch_2d_and_3d_systems(cuda_device):
+    """The batched streaming PCG over 2-D and 3-D systems of uneven sizes
+    (the default for FP64 batches whose bands do not all fit in shared
+    memory): every system converges to its tolerance, within 1e-8 of its own
+    single solve, with iteration counts within one; a forced streaming batch
+    refuses mixed precision and a conflicting kernel choice."""
+    import ctypes as C
+    import torch
+    from twophaseflow_b200 import PPESolverFVMMatrixFree, UniformGrid, _lib, solve_batched
+    shapes = [(300, 280), (40, 36, 44), (512, 512), (24, 30, 28), (96, 200)]
+    solvers, rhs, rho = [], [], []
+    for k, N in enumerate(shapes):
+        cfg = _Cfg(pseudo_tol=1e-9, pseudo_maxiter=100000, ppe_iteration_method="cg", ppe_preconditioner="jacobi")
+        solvers.append(PPESolverFVMMatrixFree(None, cfg, UniformGrid(N)))
+        rho.append(torch.from_numpy(droplet_density(N, n_drops=4, seed=700 + k)).to(cuda_device))
+        rhs.append(torch.from_numpy(divergence_rhs(N, seed=800 + k)).to(cuda_device))
+    pb = solve_batched(solvers, rhs, rho)
+    its_b = [s.last_diagnostics["ppe_low_order_cg_iterations"] for s in solvers]
+    for k, s in enumerate(solvers):
+        assert s.last_diagnostics["ppe_low_order_cg_relative_residual"] < 1e-9
+        _lib.check(s.lib.tpf_ppe_set_cg_kernel(s._handle, C.c_int(3)))
+        p1 = s.solve(rhs[k], rho[k])
+        it1 = s.last_diagnostics["ppe_low_order_cg_iterations"]
+        assert abs(it1 - its_b[k]) <= 1, (k, it1, its_b[k])
+        scale = float(torch.max(torch.abs(p1)))
+        assert float(torch.max(torch.abs(pb[k] - p1))) <= 1e-8 * scale
+    _lib.check(solvers[0].lib.tpf_ppe_set_cg_kernel(solvers[0]._handle, C.c_int(2)))
+    with pytest.raises(ValueError):
+        solve_batched(solvers, rhs, rho)
+    cfgm = _Cfg(pseudo_tol=1e-9, pseudo_maxiter=100000, ppe_iteration_method="cg", ppe_preconditioner="jacobi",
+                ppe_precision="mixed")
+    sm = [PPESolverFVMMatrixFree(None, cfgm, UniformGrid((64, 64))) for _ in range(2)]
+    _lib.check(sm[0].lib.tpf_ppe_set_cg_kernel(sm[0]._handle, C.c_int(3)))
+    r64 = [torch.from_numpy(divergence_rhs((64, 64), seed=900 + k)).to(cuda_device) for k in range(2)]
+    d64 = [torch.from_numpy(droplet_density((64, 64), seed=910 + k)).to(cuda_device) for k in range(2)]
+    with pytest.raises(ValueError):
+        solve_batched(sm, r64, d64)
 
 
 def test_band_batch_many_small_systems_and_mixed(cuda_device):

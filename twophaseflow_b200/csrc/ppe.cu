@@ -30,6 +30,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <memory>
 #include <vector>
 
 namespace {
@@ -1336,12 +1337,13 @@ __device__ __forceinline__ void cgs_update_node(int idx, int pin, double ri, dou
 
 // Two consecutive nodes per thread and trip (16-byte loads and stores; the
 // vectors come from cudaMalloc, so even node indices are 16-byte aligned).
+// (bid, nblk: this block's index among the nblk blocks working on the system)
 template <bool INIT>
-__global__ void __launch_bounds__(256) cgs_update_kernel(int ndof, int pin, const double* __restrict__ dinv,
-                                                         const double* __restrict__ w, double* __restrict__ sv,
-                                                         double* __restrict__ pv, double* __restrict__ x,
-                                                         double* __restrict__ r, double* __restrict__ u,
-                                                         double* part, const CgScal* sc) {
+__device__ __forceinline__ void cgs_update_body(int bid, int nblk, int ndof, int pin, const double* __restrict__ dinv,
+                                                const double* __restrict__ w, double* __restrict__ sv,
+                                                double* __restrict__ pv, double* __restrict__ x,
+                                                double* __restrict__ r, double* __restrict__ u, double* part,
+                                                const CgScal* sc) {
   if (sc->done) return;
   __shared__ double scratch[4 * 32];
   double alpha = 0.0, beta = 0.0;
@@ -1351,7 +1353,7 @@ __global__ void __launch_bounds__(256) cgs_update_kernel(int ndof, int pin, cons
   }
   double red[4] = {0.0, 0.0, 0.0, 0.0};
   const int npair = ndof >> 1;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < npair; k += gridDim.x * blockDim.x) {
+  for (int k = bid * blockDim.x + threadIdx.x; k < npair; k += nblk * blockDim.x) {
     const int i0 = 2 * k;
     const double2 r2 = reinterpret_cast<const double2*>(r)[k];
     const double2 d2 = reinterpret_cast<const double2*>(dinv)[k];
@@ -1381,7 +1383,7 @@ __global__ void __launch_bounds__(256) cgs_update_kernel(int ndof, int pin, cons
     red[2] += pi1 * si1;
     red[3] += rn1 * rn1;
   }
-  if ((ndof & 1) && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {   // odd node count: the last node
+  if ((ndof & 1) && bid == nblk - 1 && threadIdx.x == 0) {   // odd node count: the last node
     const int i = ndof - 1;
     double xi = INIT ? 0.0 : x[i];
     double rn, si, pi, un;
@@ -1401,11 +1403,20 @@ __global__ void __launch_bounds__(256) cgs_update_kernel(int ndof, int pin, cons
   }
   tpf::block_sum<4>(red, scratch);
   if (threadIdx.x == 0) {
-    part[(size_t)0 * gridDim.x + blockIdx.x] = red[0];
-    part[(size_t)2 * gridDim.x + blockIdx.x] = red[1];
-    part[(size_t)4 * gridDim.x + blockIdx.x] = red[2];
-    part[(size_t)5 * gridDim.x + blockIdx.x] = red[3];
+    part[(size_t)0 * nblk + bid] = red[0];
+    part[(size_t)2 * nblk + bid] = red[1];
+    part[(size_t)4 * nblk + bid] = red[2];
+    part[(size_t)5 * nblk + bid] = red[3];
   }
+}
+
+template <bool INIT>
+__global__ void __launch_bounds__(256) cgs_update_kernel(int ndof, int pin, const double* __restrict__ dinv,
+                                                         const double* __restrict__ w, double* __restrict__ sv,
+                                                         double* __restrict__ pv, double* __restrict__ x,
+                                                         double* __restrict__ r, double* __restrict__ u,
+                                                         double* part, const CgScal* sc) {
+  cgs_update_body<INIT>(blockIdx.x, gridDim.x, ndof, pin, dinv, w, sv, pv, x, r, u, part, sc);
 }
 
 // w = S u, marching along axis 0: thread j owns column j of the (axis 1,
@@ -1414,17 +1425,18 @@ __global__ void __launch_bounds__(256) cgs_update_kernel(int ndof, int pin, cons
 // from HBM once; the pin row is the identity (w = u).  Then (w, u), (p, w);
 // the last block to finish advances the scalars.  Same grid for every launch
 // (the partial sums are indexed by the flattened block id).
+// (bx, by: this block's column tile and plane chunk in the system's gx x gy grid)
 template <bool INIT>
-__global__ void __launch_bounds__(256) cgs_stencil_kernel(Grid3 g, int chunk, const double* __restrict__ s0,
-                                                          const double* __restrict__ s1,
-                                                          const double* __restrict__ s2,
-                                                          const double* __restrict__ u, const double* __restrict__ pv,
-                                                          double* __restrict__ w, double* part, CgScal* sc) {
+__device__ __forceinline__ void cgs_stencil_body(int bx, int by, int gx, int gy, const Grid3& g, int chunk,
+                                                 const double* __restrict__ s0, const double* __restrict__ s1,
+                                                 const double* __restrict__ s2, const double* __restrict__ u,
+                                                 const double* __restrict__ pv, double* __restrict__ w, double* part,
+                                                 CgScal* sc) {
   if (sc->done) return;
   __shared__ double scratch[6 * 32];
   const int nplane = g.st0;
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  const int c0 = blockIdx.y * chunk;
+  const int j = bx * blockDim.x + threadIdx.x;
+  const int c0 = by * chunk;
   const int c1 = min(c0 + chunk, g.n0);
   double red[2] = {0.0, 0.0};
   if (j < nplane && c0 < c1) {
@@ -1462,8 +1474,8 @@ __global__ void __launch_bounds__(256) cgs_stencil_kernel(Grid3 g, int chunk, co
     }
   }
   tpf::block_sum<2>(red, scratch);
-  const int nb = gridDim.x * gridDim.y;
-  const int bid = blockIdx.y * gridDim.x + blockIdx.x;
+  const int nb = gx * gy;
+  const int bid = by * gx + bx;
   if (threadIdx.x == 0) {
     part[(size_t)1 * nb + bid] = red[0];
     part[(size_t)3 * nb + bid] = red[1];
@@ -1497,6 +1509,65 @@ __global__ void __launch_bounds__(256) cgs_stencil_kernel(Grid3 g, int chunk, co
     if (t[5] < sc->atol2) { sc->conv = 1; sc->done = 1; }
     else if (sc->it >= sc->maxiter) sc->done = 1;
   }
+}
+
+template <bool INIT>
+__global__ void __launch_bounds__(256) cgs_stencil_kernel(Grid3 g, int chunk, const double* __restrict__ s0,
+                                                          const double* __restrict__ s1,
+                                                          const double* __restrict__ s2,
+                                                          const double* __restrict__ u, const double* __restrict__ pv,
+                                                          double* __restrict__ w, double* part, CgScal* sc) {
+  cgs_stencil_body<INIT>(blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, g, chunk, s0, s1, s2, u, pv, w, part, sc);
+}
+
+// ---- batched streaming PCG: many systems' iterations in the same two launches ----
+// Each system keeps its own vectors, partial sums and scalars (its own last
+// block advances them); system c owns the blocks [first[c], first[c + 1]) of
+// both launches (gx[c] x gy[c] of them, the same count for the update), and
+// its blocks return at once after its solve is done.
+struct CgsSys {
+  Grid3 g;
+  int chunk, gx, gy;
+  const double *s0, *s1, *s2, *dinv;
+  double *x, *r, *u, *w, *sv, *pv, *part;
+  CgScal* sc;
+};
+struct CgsBatch {
+  CgsSys c[kBatchMax];
+  int first[kBatchMax + 1];
+  int n;
+};
+
+__device__ __forceinline__ int cgs_batch_system(const CgsBatch& b, int blk) {
+  int lo = 0, hi = b.n - 1;   // the system whose block range holds blk
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (blk >= b.first[mid]) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(256) cgsb_update_kernel(const __grid_constant__ CgsBatch b) {
+  const int c = cgs_batch_system(b, blockIdx.x);
+  const CgsSys& y = b.c[c];
+  cgs_update_body<false>(blockIdx.x - b.first[c], b.first[c + 1] - b.first[c], y.g.ndof, y.g.pin, y.dinv, y.w,
+                         y.sv, y.pv, y.x, y.r, y.u, y.part, y.sc);
+}
+
+__global__ void __launch_bounds__(256) cgsb_stencil_kernel(const __grid_constant__ CgsBatch b) {
+  const int c = cgs_batch_system(b, blockIdx.x);
+  const CgsSys& y = b.c[c];
+  const int lid = blockIdx.x - b.first[c];
+  cgs_stencil_body<false>(lid % y.gx, lid / y.gx, y.gx, y.gy, y.g, y.chunk, y.s0, y.s1, y.s2, y.u, y.pv, y.w,
+                          y.part, y.sc);
+}
+
+// number of systems still iterating
+__global__ void cgsb_pending_kernel(const __grid_constant__ CgsBatch b, int* pending) {
+  int k = 0;
+  for (int c = threadIdx.x; c < b.n; c += blockDim.x) k += b.c[c].sc->done ? 0 : 1;
+  k = tpf::warp_sum(k);
+  if (threadIdx.x == 0) *pending = k;
 }
 
 __global__ void cgs_init_kernel(CgScal* sc, double tol, long long maxiter, int x_nonzero) {
@@ -1563,6 +1634,7 @@ struct tpf_ppe {
   cudaGraphExec_t cg_exec = nullptr;   // a chunk of streaming-PCG iterations, captured
   long long cg_key[6] = {};
   void* cgs = nullptr;                 // streaming-PCG device scalars (CgScal)
+  int* batch_pending = nullptr;        // systems still iterating in a batched streaming solve
   int pending = 0;                     // captured CG solve: 1 status in st, 2 in cgs
   cudaStream_t cap = nullptr;          // stream the cycle is captured on (never the caller's)
   long long gm_key[6] = {};
@@ -2448,6 +2520,133 @@ bool band_batch_plan(tpf_ppe* const* hs, int n, bool mixed, std::vector<int>& nb
   return true;
 }
 
+// Batched streaming PCG (FP64 systems too large to keep resident): per system
+// the right-hand side, the initial residual and the first iteration as the
+// single-system launches, then chunks of kCgsChunk iterations of ALL systems
+// in two launches each (cgsb_update_kernel / cgsb_stencil_kernel), captured
+// once as a CUDA graph and replayed until no system is iterating; each
+// system's blocks (threads in proportion to its nodes) return at once when
+// its solve is done.  Writes p[c] and results[c]; returns the batch status.
+int solve_cgs_batch(tpf_ppe* const* hs, int n, const double* const* rhs, double* const* p, cudaStream_t s,
+                    tpf_ppe_result* results) {
+  int st;
+  std::unique_ptr<CgsBatch> b(new CgsBatch());
+  b->n = n;
+  b->first[0] = 0;
+  long long tot = 0;
+  for (int c = 0; c < n; ++c) tot += hs[c]->g.ndof;
+  const long long target = 2048LL * tpf::sm_count();   // threads resident at once
+  for (int c = 0; c < n; ++c) {
+    tpf_ppe* h = hs[c];
+    const Grid3& g = h->g;
+    if (!h->cgs) {
+      CgScal* cs = nullptr;
+      if ((st = dalloc(h, &cs, 1))) return st;
+      h->cgs = cs;
+    }
+    CgScal* sc = static_cast<CgScal*>(h->cgs);
+    const int gx = (g.st0 + 255) / 256;
+    const long long want = std::max<long long>(256LL * gx, target * g.ndof / std::max<long long>(tot, 1));
+    int gy = (int)std::max<long long>(1, std::min<long long>(g.n0, want / (256LL * gx)));
+    while (gy > 1 && gx * gy * 6 > h->part_len) --gy;
+    const int chunk = (g.n0 + gy - 1) / gy;
+    gy = (g.n0 + chunk - 1) / chunk;
+    TPF_CHECK_ARG(6 * gx * gy <= h->part_len, "batched streaming PCG: partial-sum area of system %d too small", c);
+    CgsSys& y = b->c[c];
+    y.g = g;
+    y.chunk = chunk;
+    y.gx = gx;
+    y.gy = gy;
+    y.s0 = h->s[0];
+    y.s1 = h->s[1];
+    y.s2 = (g.N2 > 0) ? h->s[2] : h->s[1];
+    y.dinv = (h->o.precond == TPF_PRECOND_NONE) ? h->ones64 : h->dinvS;
+    y.x = h->x;
+    y.r = h->c64[0];
+    y.u = h->c64[1];
+    y.w = h->c64[2];
+    y.sv = h->c64[4];
+    y.pv = h->c64[6];
+    y.part = h->part;
+    y.sc = sc;
+    b->first[c + 1] = b->first[c] + gx * gy;
+    const Geo geo{{h->dv[0], h->dv[1], h->dv[2]}, {h->dface[0], h->dface[1], h->dface[2]}};
+    cg_rhs_kernel<<<ew_grid(h), 256, 0, s>>>(g, geo, rhs[c], h->b, nullptr, h->x);
+    cgs_init_kernel<<<1, 1, 0, s>>>(sc, h->o.tol, h->o.maxiter, 0);
+    const int nr = std::max(1, std::min(h->ew_blocks, h->part_len / 8));
+    cgs_resid_kernel<<<nr, 256, 0, s>>>(g, y.s0, y.s1, y.s2, h->b, h->x, y.r, y.part, sc);
+    cgs_update_kernel<true><<<gx * gy, 256, 0, s>>>(g.ndof, g.pin, y.dinv, y.w, y.sv, y.pv, y.x, y.r, y.u, y.part,
+                                                     sc);
+    cgs_stencil_kernel<true><<<dim3(gx, gy), 256, 0, s>>>(g, chunk, y.s0, y.s1, y.s2, y.u, y.pv, y.w, y.part, sc);
+    TPF_CUDA_TRY(cudaGetLastError());
+  }
+  tpf_ppe* h0 = hs[0];
+  if (!h0->batch_pending && (st = dalloc(h0, &h0->batch_pending, 1))) return st;
+  if (!h0->cap && cudaStreamCreateWithFlags(&h0->cap, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    h0->cap = nullptr;
+    tpf::set_error("cudaStreamCreate failed");
+    return TPF_ECUDA;
+  }
+  const int nblk = b->first[n];
+  TPF_CUDA_TRY(cudaStreamBeginCapture(h0->cap, cudaStreamCaptureModeThreadLocal));
+  for (int k = 0; k < kCgsChunk; ++k) {
+    cgsb_update_kernel<<<nblk, 256, 0, h0->cap>>>(*b);
+    cgsb_stencil_kernel<<<nblk, 256, 0, h0->cap>>>(*b);
+  }
+  cgsb_pending_kernel<<<1, 64, 0, h0->cap>>>(*b, h0->batch_pending);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(h0->cap, &graph);
+  if (ce != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    tpf::set_error("capturing the batched PCG chunk failed: %s", cudaGetErrorString(ce));
+    return TPF_ECUDA;
+  }
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ie != cudaSuccess) {
+    cudaGetLastError();
+    tpf::set_error("instantiating the batched PCG graph failed: %s", cudaGetErrorString(ie));
+    return TPF_ECUDA;
+  }
+  cgsb_pending_kernel<<<1, 64, 0, s>>>(*b, h0->batch_pending);
+  int pending = 0;
+  cudaError_t le = cudaMemcpyAsync(&pending, h0->batch_pending, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (le == cudaSuccess) le = cudaStreamSynchronize(s);
+  while (le == cudaSuccess && pending > 0) {
+    le = cudaGraphLaunch(exec, s);
+    if (le == cudaSuccess) le = cudaMemcpyAsync(&pending, h0->batch_pending, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (le == cudaSuccess) le = cudaStreamSynchronize(s);
+  }
+  cudaGraphExecDestroy(exec);
+  TPF_CUDA_TRY(le);
+  std::vector<CgScal> hsc(n);
+  for (int c = 0; c < n; ++c) {
+    tpf_ppe* h = hs[c];
+    cgs_finish_kernel<<<ew_grid(h), 256, 0, s>>>(h->g.ndof, h->g.pin, b->c[c].sc, h->x, p[c]);
+    TPF_CUDA_TRY(cudaMemcpyAsync(&hsc[c], b->c[c].sc, sizeof(CgScal), cudaMemcpyDeviceToHost, s));
+  }
+  TPF_CUDA_TRY(cudaGetLastError());
+  TPF_CUDA_TRY(cudaStreamSynchronize(s));
+  int status = TPF_OK;
+  for (int c = 0; c < n; ++c) {
+    tpf_ppe_result r{};
+    r.iterations = hsc[c].it;
+    r.applies = hsc[c].applies;
+    r.refinements = 0;
+    r.rel_residual = hsc[c].bb > 0.0 ? std::sqrt(hsc[c].rr / hsc[c].bb) : 0.0;
+    r.info = hsc[c].conv ? 0 : (int)std::min<long long>(hs[c]->o.maxiter, 0x7fffffff);
+    if (results) results[c] = r;
+    if (!hsc[c].conv && status == TPF_OK) {
+      tpf::set_error("batched PCG system %d did not converge (info=%d)", c, r.info);
+      status = TPF_ENOCONV;
+    }
+  }
+  return status;
+}
+
 int launch_band_batch(tpf_ppe* const* hs, int n, const double* const* rhs, bool mixed, const std::vector<int>& nb,
                       const std::vector<int>& nmax, size_t smem, cudaStream_t s) {
   auto* b = new BandBatch();
@@ -2521,11 +2720,21 @@ int tpf_ppe_solve_batched(tpf_ppe* const* hs, int n, const double* const* rhs, c
   size_t bsmem = 0;
   bool force_band = false;
   for (int c = 0; c < n; ++c) force_band = force_band || hs[c]->cg_kernel == 2;
+  bool force_global = false, force_stream = false;
+  for (int c = 0; c < n; ++c) {
+    force_global = force_global || hs[c]->cg_kernel == 1;
+    force_stream = force_stream || hs[c]->cg_kernel == 3;
+  }
+  TPF_CHECK_ARG(!(force_stream && (force_band || force_global)), "conflicting CG kernel choices in one batch");
+  TPF_CHECK_ARG(!(force_stream && mixed), "the batched streaming PCG runs FP64 systems");
+  if (force_stream) return solve_cgs_batch(hs, n, rhs, p, s, results);
   if (band_batch_plan(hs, n, mixed, bnb, bnmax, bsmem)) {
     if ((st = launch_band_batch(hs, n, rhs, mixed, bnb, bnmax, bsmem, s))) return st;
   } else if (force_band) {
     tpf::set_error("the band-resident batch needs 2-D systems whose bands all fit in shared memory at once");
     return TPF_EINVAL;
+  } else if (!mixed && !force_global) {
+    return solve_cgs_batch(hs, n, rhs, p, s, results);
   } else {
     double wsum = 0.0;
     for (int c = 0; c < n; ++c) wsum += std::pow((double)hs[c]->g.ndof, 1.5);
