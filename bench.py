@@ -184,7 +184,7 @@ def time_ppe(precision, rho_d, rhs_d, steps, warmup, flush, cg_kernel=0):
 
 def time_learned(rho_d, rhs_d, steps, warmup, flush, **opts):
     """Network-preconditioned solve (shipped weights, two-level mode; the
-    solver's defaults -- flexible GMRES(80), 16 sweeps -- unless ``opts`` give
+    solver's defaults -- flexible GMRES(60), 16 sweeps -- unless ``opts`` give
     ``ppe_learned_*`` settings), device-resident inputs."""
     import torch
     from twophaseflow_b200 import UniformGrid
@@ -281,6 +281,9 @@ def time_ccd(N, bc, axis, dtype="f64", reps=10):
 # DRAM bytes read + written by one cg1_band_kernel solve at 513^2 (ncu,
 # dram__bytes_read.sum + dram__bytes_write.sum of the launch)
 PCG_BAND_DRAM_BYTES_PER_SOLVE = 11.5e6
+# DRAM bytes of one smooth_block_kernel launch (4 sweeps) at 513^2 (ncu,
+# cold caches: the five inputs read once; the output stays in L2)
+SMOOTH_DRAM_BYTES_PER_LAUNCH = 10.5e6
 
 
 def time_c1(steps, warmup):
@@ -436,7 +439,7 @@ def main(argv=None):
         s64, p64, t64 = time_ppe("fp64", rho_d, rhs_d, args.steps, args.warmup, flush)
         torch.cuda.synchronize()
         _barrier(ws)
-        # the learned solve (flexible GMRES(80), U-Net two-level preconditioner),
+        # the learned solve (flexible GMRES(60), U-Net two-level preconditioner),
         # the same steps / warm-up and L2 flush
         slr, plr, tlr = time_learned(rho_d, rhs_d, args.steps, args.warmup, flush)
         torch.cuda.synchronize()
@@ -492,15 +495,16 @@ def main(argv=None):
     smo = smoother_case(N_PPE)
     roof_learned = {"kernel": "smooth_block_kernel", "bound": "hbm", "achieved": smo["GBps"], "peak": peak,
                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(smo["GBps"] / peak, 3),
-                    "us_per_launch": smo["us_per_launch"], "traffic": None,
+                    "us_per_launch": smo["us_per_launch"], "traffic": SMOOTH_DRAM_BYTES_PER_LAUNCH,
                     "note": "48 B/node per launch algorithmic (z, r, D^-1, couplings read, z written; 4 sweeps); "
                             "the 513^2 operator is L2-resident"}
-    # launches of the learned solve (flexible GMRES): per Arnoldi column 33 for
-    # the preconditioner (6 input/restriction, 14 convolutions, 6 resampling,
-    # output, prolongation + first sweep, 4 blocked smoother launches, copy-out),
+    # launches of the learned solve (flexible GMRES, two-level mode), counted
+    # from its launch sequence: per Arnoldi column 28 for the preconditioner
+    # (fused restriction, input packing, 14 convolutions, 6 resampling layers,
+    # output layer, prolongation + first sweep, 4 blocked smoother launches),
     # 1 operator and 4 Gram-Schmidt; per restart cycle 6; 12 for the set-up
     its_lr = dlr["ppe_learned_iterations"]
-    launches_lr = its_lr * 38 + 6 * ((its_lr + 79) // 80) + 12
+    launches_lr = its_lr * 33 + 6 * ((its_lr + 59) // 60) + 12
 
     # CCD line kernels (2-D 1024^2 and 3-D 256^3, FP64 and FP32), graph-timed
     ccd = []
@@ -598,7 +602,7 @@ def main(argv=None):
             "learned_fcg8_smooth3": {"ms": round(float(np.mean(tfc)), 3), "iterations": dfc["ppe_learned_iterations"],
                                      "fell_back": bool(dfc["ppe_learned_fell_back"]),
                                      "max_rel_diff_vs_fp64": float(f"{float(torch.max(torch.abs(pfc - p64))) / float(torch.max(torch.abs(p64))):.3g}")},
-            "learned_detail": {"method": "flexible GMRES(80), U-Net two-level preconditioner, 16 Jacobi sweeps",
+            "learned_detail": {"method": "flexible GMRES(60), U-Net two-level preconditioner, 16 Jacobi sweeps",
                                "fallback_iterations": dlr["ppe_learned_fallback_iterations"],
                                "rel_residual": dlr["ppe_learned_relative_residual"],
                                "us_per_iteration": round(ms_lr * 1e3 / max(1, dlr["ppe_learned_iterations"]), 1)},
@@ -612,7 +616,7 @@ def main(argv=None):
             "config": {"workload": WORKLOAD, "grid": list(N_PPE), "tol": TOL,
                        "method": {"fp64": "FP64 Jacobi-PCG, persistent single-reduction kernel",
                                   "mixed": "mixed: band-resident FP32 Jacobi-PCG with FP64 residual replacement",
-                                  "learned": "two-level U-Net-preconditioned flexible GMRES(80)"}[best],
+                                  "learned": "two-level U-Net-preconditioned flexible GMRES(60)"}[best],
                        "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{ws}"},
             "plain_fp64_pcg_ms": round(ms_64, 3), "plain_fp64_iterations": it64,
             "mixed_ms": round(ms_mx, 3), "mixed_max_rel_diff_vs_fp64": float(f"{err:.3g}"),

@@ -502,18 +502,23 @@ int tpf_ppe_solve(tpf_ppe* h, const double* rhs, const double* rho, double* p,
 
 /* Batched solve (no counterpart in the reference, which solves one system
  * per call): n independent systems (n <= 64, each its own handle and grid,
- * all with method TPF_PPE_CG and one precision) in ONE cooperative launch;
- * every system runs the persistent PCG of tpf_ppe_solve on its own share of
- * the SMs (proportional to ndof^1.5, its expected work), with its own grid
- * barrier.  When every system is 2-D and all their bands fit in shared
- * memory at once (the systems' nodes summing to at most ~340 000 in FP64,
- * ~640 000 mixed, on 148 SMs), each runs band-resident; otherwise each runs
- * the all-global body.  tpf_ppe_set_cg_kernel on any handle selects: 1 the
- * all-global body, 2 the band-resident batch (TPF_EINVAL if it does not
- * fit).  rho may be NULL (or hold NULL entries) for handles prepared
- * beforehand.  results[c] as tpf_ppe_solve; returns the first failure
- * (TPF_ENOCONV / TPF_EABORT) after all systems finished.  Synchronizes
- * `stream`. */
+ * all with method TPF_PPE_CG and one precision).  When every system is 2-D
+ * and all their bands fit in shared memory at once (the systems' nodes
+ * summing to at most ~340 000 in FP64, ~640 000 mixed, on 148 SMs): ONE
+ * cooperative launch in which every system runs the band-resident PCG on its
+ * own share of the SMs (proportional to ndof^1.5, its expected work) with its
+ * own grid barrier.  Otherwise, FP64: the batched streaming PCG -- every
+ * system's iterations in the same two launches (each system its own blocks,
+ * threads in proportion to its nodes, its own scalars; a system's blocks
+ * return once it is done), chunks of 32 iterations replayed from a CUDA
+ * graph; mixed precision: one cooperative launch of the all-global body.
+ * tpf_ppe_set_cg_kernel on any handle selects: 1 the all-global body, 2 the
+ * band-resident batch (TPF_EINVAL if it does not fit), 3 the batched
+ * streaming PCG (FP64 only; TPF_EINVAL for mixed precision or with another
+ * handle asking for 1 or 2).  rho may be NULL (or hold NULL entries) for
+ * handles prepared beforehand.  results[c] as tpf_ppe_solve; returns the
+ * first failure (TPF_ENOCONV / TPF_EABORT) after all systems finished.
+ * Synchronizes `stream`. */
 int tpf_ppe_solve_batched(tpf_ppe* const* handles, int n, const double* const* rhs, const double* const* rho,
                           double* const* p, void* stream, tpf_ppe_result* results);
 

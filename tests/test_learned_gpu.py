@@ -246,7 +246,7 @@ def test_trained_network_gain(cuda_device, outer, smooth, bar):
     the same two-level method without it (all-zero network: the Jacobi
     two-grid cycle with no coarse correction) on a held-out 256^2 density at
     ratio 1000: flexible CG with 3 sweeps needs at least 2.5x fewer iterations
-    with the network (about 3x measured), the default flexible GMRES(80) with
+    with the network (about 3x measured), the default flexible GMRES(60) with
     16 sweeps at least 1.5x; same solution."""
     import torch
     from twophaseflow_b200 import UniformGrid

@@ -675,15 +675,28 @@ __global__ void __launch_bounds__(kRedThreads) restrict_pre_kernel(LGrid g, cons
   const int nc = g.nc0 * g.nc1;
   double v[1] = {0.0};
   if (!skip) {
-    for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += gridDim.x * blockDim.x) {
+    // b consecutive lanes per aggregate (b = 2, 4 or 8 divides the warp), lane
+    // k summing fine row k of the aggregate; the row sums are added by a
+    // shuffle tree.  Whole warps iterate together (the shuffles need every lane).
+    const int b = g.b;
+    const long long total = (long long)nc * b;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long t0 = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); t0 < total; t0 += stride) {
+      const long long t = t0 + (threadIdx.x & 31);
+      const bool on = t < total;
+      const int I = on ? (int)(t / b) : 0, k = on ? (int)(t - (long long)I * b) : 0;
       const int I0 = I / g.nc1, I1 = I - I0 * g.nc1;
+      const int a0 = I0 * b + k;
       double acc = 0.0;
-      for (int a0 = I0 * g.b; a0 < min(g.n0, (I0 + 1) * g.b); ++a0)
-        for (int a1 = I1 * g.b; a1 < min(g.n1, (I1 + 1) * g.b); ++a1)
+      if (on && a0 < g.n0)
+        for (int a1 = I1 * b; a1 < min(g.n1, (I1 + 1) * b); ++a1)
           acc += pre_residual(g, r, omega, a0 * g.n1 + a1, a0, a1);
-      rc[I] = acc;
-      const double q = acc * g.dcis[I];
-      v[0] += q * q;
+      for (int off = b >> 1; off >= 1; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+      if (on && k == 0) {
+        rc[I] = acc;
+        const double q = acc * g.dcis[I];
+        v[0] += q * q;
+      }
     }
   }
   block_partials<1>(v, part);
@@ -1242,7 +1255,7 @@ void tpf_lppe_default_options(tpf_learned_options* o) {
   o->use_graph = 1;
   o->window = 8;
   o->outer = 1;
-  o->restart = 80;
+  o->restart = 60;
 }
 
 int tpf_lppe_create(tpf_lppe** out, tpf_ppe* ppe, tpf_unet* net, int coarsen) {

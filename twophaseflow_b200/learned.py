@@ -206,10 +206,10 @@ class PPESolverLearned(PPESolverFVMMatrixFree):
     ``ppe_learned_omega`` (0.8), ``ppe_learned_weights`` (path of the trained
     parameters), ``ppe_learned_fallback`` (finish with plain Jacobi PCG on a
     stall, True) and ``ppe_learned_outer``: 'fgmres' (flexible GMRES with
-    restart ``ppe_learned_restart``, default 80: each basis vector
+    restart ``ppe_learned_restart``, default 60: each basis vector
     preconditioned by the network, the solution built from the preconditioned
     basis; the default) or 'fcg' (truncated flexible CG with
-    ``ppe_learned_window`` stored directions).  The defaults (FGMRES(80), 16
+    ``ppe_learned_window`` stored directions).  The defaults (FGMRES(60), 16
     sweeps, omega 0.8) were chosen on validation density fields (seeds 21-30
     at 512^2, 21-24 at 1024^2) that neither training nor the benchmark use.
     """
@@ -235,7 +235,7 @@ class PPESolverLearned(PPESolverFVMMatrixFree):
         if outer not in ("fcg", "fgmres"):
             raise ValueError("ppe_learned_outer must be 'fcg' (flexible CG) or 'fgmres' (flexible GMRES)")
         self.outer = outer
-        self.restart = int(getattr(solver_cfg, "ppe_learned_restart", 80))
+        self.restart = int(getattr(solver_cfg, "ppe_learned_restart", 60))
         meta = {}
         if params is None:
             wpath = str(getattr(solver_cfg, "ppe_learned_weights", DEFAULT_WEIGHTS))
