@@ -655,9 +655,12 @@ int tpf_unet_train_step(tpf_unet* net, int B, const float* in2, const float* tar
 int tpf_unet_train_step_energy(tpf_unet* net, int B, const float* in2, const float* coupl, const double* escale,
                                int nc0, int nc1, float lr, float weight_decay, double* loss, void* stream);
 
+/* Defaults (tpf_lppe_default_options): tol 1e-8, maxiter 2000, smooth 16,
+ * omega 0.8, check_every 8, stall_checks 16, stall_factor 0.5, fallback 1,
+ * use_graph 1, window 8, outer 1 (flexible GMRES), restart 60. */
 typedef struct tpf_learned_options {
   double tol;           /* relative residual tolerance of the weighted system   */
-  int64_t maxiter;      /* flexible-CG iterations before the fallback           */
+  int64_t maxiter;      /* iterations (Arnoldi columns) before the fallback      */
   int smooth;           /* damped-Jacobi sweeps after the network (0..32)        */
   double omega;         /* their damping                                         */
   int check_every;      /* iterations between host checks of the residual        */

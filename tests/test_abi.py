@@ -53,6 +53,11 @@ def test_host_only_calls_without_gpu():
     # reference defaults (fvm_matrixfree.py:90-127)
     assert o.method == _lib.TPF_PPE_GMRES and o.precond == _lib.TPF_PRECOND_LINE
     assert o.tol == 1e-8 and o.maxiter == 500 and o.restart == 80 and o.c_tau == 2.0 and o.pcr_stages == 4
+    # the learned solver's defaults: flexible GMRES(60), 16 sweeps at 0.8, PCG fallback
+    lo = _lib.tpf_learned_options()
+    lib.tpf_lppe_default_options(ctypes.byref(lo))
+    assert lo.outer == 1 and lo.restart == 60 and lo.smooth == 16 and lo.omega == 0.8 and lo.fallback == 1
+    assert lo.tol == 1e-8 and lo.stall_checks == 16 and lo.check_every == 8 and lo.stall_factor == 0.5
 
 
 def test_invalid_arguments_fail_closed_on_host():
