@@ -511,7 +511,8 @@ int gmres_solve(GmresWork& W, int restart, double tol, long long maxiter, bool x
       if ((est = precond(W.t, W.w, cs, done))) return est;
       double* hc = H + (size_t)col * ldh;
       tpf::launch_chained(gs1_kernel, nb_dot, 256, 0, cs, n, W.V, col, W.w, W.part, hc, hcol2, W.gst);
-      tpf::launch_chained(gs2_kernel, nb_dot, 256, 0, cs, n, W.V, col, W.w, hc, W.part, H, ldh, givens, S, hcol2, W.gst);
+      tpf::launch_chained(gs2_kernel, nb_dot, 256, 0, cs, n, W.V, col, W.w, hc, W.part, H, ldh, givens, S, hcol2,
+                          W.gst);
       tpf::launch_chained(gs3_kernel, nb_dot, 256, 0, cs, n, W.V, col, W.w, W.part, H, ldh, givens, S, hcol2, W.gst);
       tpf::launch_chained(gm_scale_kernel, W.ew_blocks, 256, 0, cs, n, W.w, W.V + (size_t)(col + 1) * n, W.gst);
       TPF_CUDA_TRY(cudaGetLastError());
@@ -653,7 +654,8 @@ int fgmres_solve(GmresWork& W, double* Z, int restart, double tol, long long max
       if ((est = apply(zc, W.w, cs, done))) return est;
       double* hc = H + (size_t)col * ldh;
       tpf::launch_chained(gs1_kernel, nb_dot, 256, 0, cs, n, W.V, col, W.w, W.part, hc, hcol2, W.gst);
-      tpf::launch_chained(gs2_kernel, nb_dot, 256, 0, cs, n, W.V, col, W.w, hc, W.part, H, ldh, givens, S, hcol2, W.gst);
+      tpf::launch_chained(gs2_kernel, nb_dot, 256, 0, cs, n, W.V, col, W.w, hc, W.part, H, ldh, givens, S, hcol2,
+                          W.gst);
       tpf::launch_chained(gs3_kernel, nb_dot, 256, 0, cs, n, W.V, col, W.w, W.part, H, ldh, givens, S, hcol2, W.gst);
       tpf::launch_chained(gm_scale_kernel, W.ew_blocks, 256, 0, cs, n, W.w, W.V + (size_t)(col + 1) * n, W.gst);
       TPF_CUDA_TRY(cudaGetLastError());

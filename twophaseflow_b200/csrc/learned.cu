@@ -1022,7 +1022,7 @@ int enqueue_precond(tpf_lppe* lp, int smooth, double omega, cudaStream_t s, doub
     return TPF_OK;
   }
   tpf::launch_chained(fcg_pack_kernel, ew_blocks((g.H + 2) * (g.W + 2)), 256, 0, s, g, lp->r, lp->feat, lp->st,
-                                                                    tpf::unet_input(lp->net));
+                      tpf::unet_input(lp->net));
   TPF_CUDA_TRY(cudaGetLastError());
   int st = tpf::unet_forward_packed(lp->net, 1, s);
   if (st) return st;

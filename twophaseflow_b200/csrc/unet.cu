@@ -1438,8 +1438,8 @@ int forward(tpf_unet* n, int B, cudaStream_t s) {
   upadd_t<16>(g0, g1, n->t0, n->e0, n->d0a, s);
   if ((st = conv(n, 13, B, n->d0a, n->d0, s))) return st;
   const ParamLayout& L = layout();
-  tpf::launch_chained(out1x1_kernel, grid_for((long long)B * n->H * n->W), 256, 0, s, g0, n->d0, n->params + L.wo, n->params + L.bo,
-                                                                     n->out);
+  tpf::launch_chained(out1x1_kernel, grid_for((long long)B * n->H * n->W), 256, 0, s, g0, n->d0, n->params + L.wo,
+                      n->params + L.bo, n->out);
   TPF_CUDA_TRY(cudaGetLastError());
   n->last_batch = B;
   return TPF_OK;
