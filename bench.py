@@ -499,12 +499,13 @@ def main(argv=None):
                     "note": "48 B/node per launch algorithmic (z, r, D^-1, couplings read, z written; 4 sweeps); "
                             "the 513^2 operator is L2-resident"}
     # launches of the learned solve (flexible GMRES, two-level mode), counted
-    # from its launch sequence: per Arnoldi column 28 for the preconditioner
+    # from its launch sequence: per Arnoldi column 27 for the preconditioner
     # (fused restriction, input packing, 14 convolutions, 6 resampling layers,
-    # output layer, prolongation + first sweep, 4 blocked smoother launches),
-    # 1 operator and 4 Gram-Schmidt; per restart cycle 6; 12 for the set-up
+    # output layer, 4 blocked smoother launches, the first starting from the
+    # prolongation), 1 operator and 4 Gram-Schmidt; per restart cycle 6; 12
+    # for the set-up
     its_lr = dlr["ppe_learned_iterations"]
-    launches_lr = its_lr * 33 + 6 * ((its_lr + 59) // 60) + 12
+    launches_lr = its_lr * 32 + 6 * ((its_lr + 59) // 60) + 12
 
     # CCD line kernels (2-D 1024^2 and 3-D 256^3, FP64 and FP32), graph-timed
     ccd = []

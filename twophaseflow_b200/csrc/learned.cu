@@ -234,6 +234,15 @@ __device__ __forceinline__ double jacobi_node(double zc, double zm0, double zp0,
   return zc + omega * dinv * (rr - sz);
 }
 
+// the prolongated coarse correction plus the pre-smoothing term at node j:
+// z2 = omega D^-1 r + P (s_c D_c^-1/2 y) (pin 0); two-level mode
+__device__ __forceinline__ double prolong_value(const LGrid& g, const float* y, const double* r, double omega,
+                                                double sc, int j, int j0, int j1) {
+  if (j == g.pin) return 0.0;
+  const int J0 = j0 / g.b, J1 = j1 / g.b;
+  return omega * g.dinvS[j] * r[j] + sc * g.dcis[J0 * g.nc1 + J1] * (double)y[(size_t)J0 * g.W + J1];
+}
+
 // zout = zin + omega D^-1 (r - S zin) (pin 0)
 __global__ void fcg_smooth_kernel(LGrid g, const double* zin, const double* r, double omega, const FcgState* st,
                                   double* zout) {
@@ -263,11 +272,15 @@ constexpr int kSmW = kSmTX + 2 * kSmK, kSmH = kSmTY + 2 * kSmK;
 
 constexpr int kSmThreads = 512;
 
-__global__ void __launch_bounds__(kSmThreads, 2) smooth_block_kernel(LGrid g, const double* zin, const double* r,
-                                                                     double omega, int k, const FcgState* st,
-                                                                     double* zout) {
+// yprol non-null (two-level mode): the sweeps start from the prolongated
+// correction z2 = omega D^-1 r + P (s_c D_c^-1/2 yprol) instead of zin, so the
+// first sweep is the prolongation sweep of prolong_smooth_kernel
+__global__ void __launch_bounds__(kSmThreads, 2) smooth_block_kernel(LGrid g, const double* zin, const float* yprol,
+                                                                     const double* r, double omega, int k,
+                                                                     const FcgState* st, double* zout) {
   tpf::chain_begin();
   if (st->done) return;
+  const double sc = yprol ? st->sc : 0.0;
   // only z goes through shared memory; each thread keeps r, D^-1 and the four
   // couplings of its own kPer nodes (e = tid + kSmThreads j of the tile with
   // halo) in registers for all k sweeps and holds its last updates for the store
@@ -290,7 +303,7 @@ __global__ void __launch_bounds__(kSmThreads, 2) smooth_block_kernel(LGrid g, co
     const bool h0m = in && i0 > 0, h0p = in && i0 < g.n0 - 1, h1m = in && i1 > 0, h1p = in && i1 < g.n1 - 1;
     flags[j] = (in ? 1u : 0u) | ((in && i == g.pin) ? 2u : 0u) | (h0m ? 4u : 0u) | (h0p ? 8u : 0u) |
                (h1m ? 16u : 0u) | (h1p ? 32u : 0u) | ((unsigned)c << 8) | ((unsigned)a << 16);
-    lz[j] = in ? zin[i] : 0.0;
+    lz[j] = in ? (yprol ? prolong_value(g, yprol, r, omega, sc, i, i0, i1) : zin[i]) : 0.0;
     lr[j] = in ? r[i] : 0.0;
     ld[j] = in ? g.dinvS[i] : 0.0;
     m0[j] = h0m ? g.s0[i - g.n1] : 0.0;
@@ -549,8 +562,6 @@ __global__ void rscale_finish_kernel(const double* part, int nb, int ndof, FcgSt
 //   z1 = w D^-1 r,  r1 = r - S z1,  z2 = z1 + P (s_c D_c^-1/2 UNet(D_c^-1/2 R r1 / s_c, c~_c)),
 //   z  = z2 + w D^-1 (r - S z2)  (smooth times)
 
-__device__ __forceinline__ int agg_of(const LGrid& g, int i0, int i1) { return (i0 / g.b) * g.nc1 + i1 / g.b; }
-
 // D_c (sum of the fine couplings crossing the aggregate's boundary) and the
 // Galerkin couplings to the aggregate below / to the right, gathered per
 // aggregate in a fixed order (deterministic, no atomics)
@@ -648,25 +659,13 @@ __global__ void __launch_bounds__(kRedThreads) restrict_kernel(LGrid g, const do
   tpf::chain_end();
 }
 
-__global__ void coarse_scale_kernel(const double* part, int nb, int nc, FcgState* st) {
-  tpf::chain_begin();
-  if (st->done) return;
-  double v[1];
-  reduce_partials<1>(part, nb, v);
-  if (threadIdx.x == 0) {
-    const double sc = sqrt(v[0] / nc);
-    st->sc = sc;
-    st->inv_sc = sc > 0.0 ? 1.0 / sc : 0.0;
-  }
-  tpf::chain_end();
-}
-
-// vc_pre, restrict and coarse_scale in one launch: rc = R r1 with each fine
-// node's pre-smoothed residual r1 formed once on the fly and summed in the
-// same order as the separate kernels (same bits), partials of (rc D_c^-1/2)^2;
-// the last block to finish sums the partials in block order into the input
-// scale s_c and, inside the flexible GMRES cycle (gdone non-null), copies the
-// cycle's done flag into st->done for the kernels after it
+// pre-smoothing, restriction and the coarse input scale in one launch:
+// rc = R r1 with each fine node's pre-smoothed residual r1 formed once on the
+// fly (the vc_pre_kernel formula), b lanes per aggregate adding its rows by a
+// shuffle tree, partials of (rc D_c^-1/2)^2; the last block to finish sums
+// the partials in block order into the input scale s_c and, inside the
+// flexible GMRES cycle (gdone non-null), copies the cycle's done flag into
+// st->done for the kernels after it
 __global__ void __launch_bounds__(kRedThreads) restrict_pre_kernel(LGrid g, const double* r, double omega,
                                                                    FcgState* st, const int* gdone, double* rc,
                                                                    double* part, unsigned* arrive) {
@@ -763,8 +762,7 @@ __global__ void prolong_kernel(LGrid g, const float* y, const double* r, double 
   const double sc = st->sc;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.ndof; i += gridDim.x * blockDim.x) {
     const int i0 = i / g.n1, i1 = i - i0 * g.n1;
-    const int I0 = i0 / g.b, I1 = i1 / g.b, I = I0 * g.nc1 + I1;
-    z2[i] = (i == g.pin) ? 0.0 : omega * g.dinvS[i] * r[i] + sc * g.dcis[I] * (double)y[(size_t)I0 * g.W + I1];
+    z2[i] = prolong_value(g, y, r, omega, sc, i, i0, i1);
   }
   tpf::chain_end();
 }
@@ -777,27 +775,20 @@ __global__ void prolong_smooth_kernel(LGrid g, const float* y, const double* r, 
   tpf::chain_begin();
   if (st->done) return;
   const double sc = st->sc;
-  auto z2 = [&](int j, int j0, int j1) -> double {
-    if (j == g.pin) return 0.0;
-    const int J0 = j0 / g.b, J1 = j1 / g.b;
-    return omega * g.dinvS[j] * r[j] + sc * g.dcis[J0 * g.nc1 + J1] * (double)y[(size_t)J0 * g.W + J1];
-  };
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.ndof; i += gridDim.x * blockDim.x) {
     const int i0 = i / g.n1, i1 = i - i0 * g.n1;
     if (i == g.pin) {
       z[i] = 0.0;
       continue;
     }
-    const double sm0 = (i0 > 0) ? g.s0[i - g.n1] : 0.0, sp0 = g.s0[i];
-    const double sm1 = (i1 > 0) ? g.s1[i - 1] : 0.0, sp1 = g.s1[i];
-    const double zc = z2(i, i0, i1);
-    double off = 0.0;
-    if (i0 > 0) off += sm0 * z2(i - g.n1, i0 - 1, i1);
-    if (i0 < g.n0 - 1) off += sp0 * z2(i + g.n1, i0 + 1, i1);
-    if (i1 > 0) off += sm1 * z2(i - 1, i0, i1 - 1);
-    if (i1 < g.n1 - 1) off += sp1 * z2(i + 1, i0, i1 + 1);
-    const double sz = (sm0 + sp0 + sm1 + sp1) * zc - off;
-    z[i] = zc + omega * g.dinvS[i] * (r[i] - sz);
+    const bool h0m = i0 > 0, h0p = i0 < g.n0 - 1, h1m = i1 > 0, h1p = i1 < g.n1 - 1;
+    z[i] = jacobi_node(prolong_value(g, y, r, omega, sc, i, i0, i1),
+                       h0m ? prolong_value(g, y, r, omega, sc, i - g.n1, i0 - 1, i1) : 0.0,
+                       h0p ? prolong_value(g, y, r, omega, sc, i + g.n1, i0 + 1, i1) : 0.0,
+                       h1m ? prolong_value(g, y, r, omega, sc, i - 1, i0, i1 - 1) : 0.0,
+                       h1p ? prolong_value(g, y, r, omega, sc, i + 1, i0, i1 + 1) : 0.0,
+                       h0m ? g.s0[i - g.n1] : 0.0, g.s0[i], h1m ? g.s1[i - 1] : 0.0, g.s1[i], h0m, h0p, h1m, h1p,
+                       g.dinvS[i], r[i], omega);
   }
   tpf::chain_end();
 }
@@ -985,7 +976,8 @@ void enqueue_sweeps(tpf_lppe* lp, int n, double omega, cudaStream_t s, const dou
   for (int k = 0; k < n; k += lp->smooth_block) {
     const int kk = std::min(lp->smooth_block, n - k);
     double* dst = (last_out && k + kk >= n) ? last_out : other;
-    tpf::launch_chained(smooth_block_kernel, tiles, kSmThreads, 0, s, g, cur, rin, omega, kk, lp->st, dst);
+    tpf::launch_chained(smooth_block_kernel, tiles, kSmThreads, 0, s, g, cur, static_cast<const float*>(nullptr), rin,
+                        omega, kk, lp->st, dst);
     other = cur;
     cur = dst;
   }
@@ -1006,8 +998,17 @@ int enqueue_precond(tpf_lppe* lp, int smooth, double omega, cudaStream_t s, doub
     TPF_CUDA_TRY(cudaGetLastError());
     int st = tpf::unet_forward_packed(lp->net, 1, s);
     if (st) return st;
-    double* first = (zfinal && smooth <= 1) ? zfinal : lp->z;
-    if (smooth > 0) {
+    // the prolongation sweep and the next ones: with the blocked smoother the
+    // first launch starts from the prolongated correction itself
+    const int first_sweeps = (smooth > 0 && lp->smooth_block > 1) ? std::min(smooth, lp->smooth_block)
+                                                                   : std::min(smooth, 1);
+    double* first = (zfinal && smooth <= first_sweeps) ? zfinal : lp->z;
+    if (first_sweeps > 1) {
+      const int tiles = ((g.n0 + kSmTY - 1) / kSmTY) * ((g.n1 + kSmTX - 1) / kSmTX);
+      tpf::launch_chained(smooth_block_kernel, tiles, kSmThreads, 0, s, g, static_cast<const double*>(nullptr),
+                          static_cast<const float*>(tpf::unet_output(lp->net)), rin, omega, first_sweeps, lp->st,
+                          first);
+    } else if (smooth > 0) {
       tpf::launch_chained(prolong_smooth_kernel, ew_blocks(g.ndof), 256, 0, s, g, tpf::unet_output(lp->net), rin,
                           omega, lp->st, first);
     } else {
@@ -1016,7 +1017,7 @@ int enqueue_precond(tpf_lppe* lp, int smooth, double omega, cudaStream_t s, doub
     }
     double* cur = first;
     double* other = lp->z2;
-    enqueue_sweeps(lp, smooth - 1, omega, s, rin, cur, other, zfinal);
+    enqueue_sweeps(lp, smooth - first_sweeps, omega, s, rin, cur, other, zfinal);
     TPF_CUDA_TRY(cudaGetLastError());
     *zout = cur;
     return TPF_OK;
