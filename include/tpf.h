@@ -666,7 +666,7 @@ typedef struct tpf_learned_options {
   int check_every;      /* iterations between host checks of the residual        */
   int stall_checks;     /* fallback when the best ||r|| has not fallen by         */
   double stall_factor;  /* stall_factor within stall_checks x check_every iters  */
-                        /* (flexible GMRES: judged after each restart cycle on   */
+                        /* (flexible GMRES: checked after each restart cycle on  */
                         /* the true residual, same window in Arnoldi columns)    */
   int fallback;         /* 1: finish with plain Jacobi PCG after a stall          */
   int use_graph;        /* 1: replay one iteration as a CUDA graph                */

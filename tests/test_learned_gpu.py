@@ -348,7 +348,7 @@ def test_flexible_gmres_with_trained_network(cuda_device):
 def test_flexible_gmres_stall_rule_hands_over_to_pcg(cuda_device):
     """Restarted Jacobi-GMRES(7) (all-zero network, one sweep) at density ratio
     1000 stalls: the stall rule (best true residual not halved within 128
-    Arnoldi columns, judged after each cycle) stops it long before the
+    Arnoldi columns, checked after each cycle) stops it long before the
     iteration budget and plain PCG finishes the solve."""
     import torch
     from twophaseflow_b200 import UniformGrid

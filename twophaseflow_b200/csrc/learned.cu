@@ -1219,7 +1219,7 @@ int solve_fgmres(tpf_lppe* lp, const tpf_learned_options& o, cudaStream_t s, boo
   };
   const long long cycles = std::max<long long>(1, (o.maxiter + o.restart - 1) / o.restart);
   const long long key_a = (long long)o.smooth * 1000003LL + (long long)(o.omega * 1e9);
-  // the flexible CG's stall rule, judged after each cycle on the true residual
+  // the flexible CG's stall rule, checked after each cycle on the true residual
   const long long stall_iters =
       (o.fallback && o.stall_checks > 0) ? (long long)o.stall_checks * o.check_every : 0;
   return fgmres_solve(W, lp->gZ, o.restart, o.tol, cycles, x_nonzero, key_a, (long long)(intptr_t)lp->st, apply,
