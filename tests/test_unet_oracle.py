@@ -65,3 +65,17 @@ def test_default_aggregation_matches_training_coarse_size():
     assert default_coarsen((1025, 257), meta) == 8          # the longest axis decides
     assert default_coarsen((1025, 1025), {"grid": 1024, "coarsen": 4}) == 4   # other training sizes
     assert default_coarsen((513, 513), {}) == 4              # no metadata: the shipped training size
+
+
+def test_shipped_weights_metadata():
+    """The shipped parameters come from the project's own GPU training: 20 000
+    (residual, correction) pairs of plain-PCG runs on 2 500 seeded 512^2
+    droplet / bubble densities, energy loss, two-level mode (4x4 aggregates)."""
+    from twophaseflow_b200.learned import load_meta, load_params, num_params
+    meta = load_meta()
+    assert meta["pairs"] == 20000 and meta["cases"] == 2500 and meta["grid"] == 512
+    assert meta["loss"] == "energy" and meta["coarsen"] == 4
+    hist = meta["loss_history"]
+    assert len(hist) == meta["epochs"] and hist[-1] < hist[0]
+    p = load_params()
+    assert p.shape == (num_params(),) and np.all(np.isfinite(p))
