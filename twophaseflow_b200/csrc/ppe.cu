@@ -2527,6 +2527,8 @@ bool band_batch_plan(tpf_ppe* const* hs, int n, bool mixed, std::vector<int>& nb
 // once as a CUDA graph and replayed until no system is iterating; each
 // system's blocks (threads in proportion to its nodes) return at once when
 // its solve is done.  Writes p[c] and results[c]; returns the batch status.
+constexpr int kBatchStencilThreads = 128;
+
 int solve_cgs_batch(tpf_ppe* const* hs, int n, const double* const* rhs, double* const* p, cudaStream_t s,
                     tpf_ppe_result* results) {
   int st;
@@ -2545,9 +2547,12 @@ int solve_cgs_batch(tpf_ppe* const* hs, int n, const double* const* rhs, double*
       h->cgs = cs;
     }
     CgScal* sc = static_cast<CgScal*>(h->cgs);
-    const int gx = (g.st0 + 255) / 256;
-    const long long want = std::max<long long>(256LL * gx, target * g.ndof / std::max<long long>(tot, 1));
-    int gy = (int)std::max<long long>(1, std::min<long long>(g.n0, want / (256LL * gx)));
+    // stencil blocks of kBatchStencilThreads columns (fewer idle lanes on the
+    // short rows of the smaller systems than 256-column blocks)
+    const int gx = (g.st0 + kBatchStencilThreads - 1) / kBatchStencilThreads;
+    const long long want =
+        std::max<long long>((long long)kBatchStencilThreads * gx, target * g.ndof / std::max<long long>(tot, 1));
+    int gy = (int)std::max<long long>(1, std::min<long long>(g.n0, want / ((long long)kBatchStencilThreads * gx)));
     while (gy > 1 && gx * gy * 6 > h->part_len) --gy;
     const int chunk = (g.n0 + gy - 1) / gy;
     gy = (g.n0 + chunk - 1) / chunk;
@@ -2577,7 +2582,8 @@ int solve_cgs_batch(tpf_ppe* const* hs, int n, const double* const* rhs, double*
     cgs_resid_kernel<<<nr, 256, 0, s>>>(g, y.s0, y.s1, y.s2, h->b, h->x, y.r, y.part, sc);
     cgs_update_kernel<true><<<gx * gy, 256, 0, s>>>(g.ndof, g.pin, y.dinv, y.w, y.sv, y.pv, y.x, y.r, y.u, y.part,
                                                      sc);
-    cgs_stencil_kernel<true><<<dim3(gx, gy), 256, 0, s>>>(g, chunk, y.s0, y.s1, y.s2, y.u, y.pv, y.w, y.part, sc);
+    cgs_stencil_kernel<true><<<dim3(gx, gy), kBatchStencilThreads, 0, s>>>(g, chunk, y.s0, y.s1, y.s2, y.u, y.pv,
+                                                                            y.w, y.part, sc);
     TPF_CUDA_TRY(cudaGetLastError());
   }
   tpf_ppe* h0 = hs[0];
@@ -2592,7 +2598,7 @@ int solve_cgs_batch(tpf_ppe* const* hs, int n, const double* const* rhs, double*
   TPF_CUDA_TRY(cudaStreamBeginCapture(h0->cap, cudaStreamCaptureModeThreadLocal));
   for (int k = 0; k < kCgsChunk; ++k) {
     cgsb_update_kernel<<<nblk, 256, 0, h0->cap>>>(*b);
-    cgsb_stencil_kernel<<<nblk, 256, 0, h0->cap>>>(*b);
+    cgsb_stencil_kernel<<<nblk, kBatchStencilThreads, 0, h0->cap>>>(*b);
   }
   cgsb_pending_kernel<<<1, 64, 0, h0->cap>>>(*b, h0->batch_pending);
   cudaGraph_t graph = nullptr;
