@@ -166,19 +166,34 @@ __global__ void gm_scale_kernel(int ndof, const double* w, double* vout, const G
 }
 
 // y = H(:ncols,:ncols)^-1 S (SciPy's trsv loop), then coef = y
+// Column-oriented back substitution R y = S (SciPy's order): y lives in
+// shared memory and the updates y[q] -= y[k] R[k][q] of one column k run on
+// the block's threads, one q each; every y[q] receives the same updates in
+// the same order as a single thread would apply them (same bits).
 __global__ void gm_backsolve_kernel(const double* H, int ldh, double* S, double* y, const GmState* st) {
-  int col = st->ncols - 1;
+  __shared__ double ys[kGmMaxCols + 1];
+  const int col = st->ncols - 1;
   if (col < 0) return;
-  if (H[(size_t)col * ldh + col] == 0.0) S[col] = 0.0;
-  for (int k = 0; k <= col; ++k) y[k] = S[k];
-  for (int k = col; k > 0; --k) {
-    if (y[k] != 0.0) {
-      y[k] /= H[(size_t)k * ldh + k];
-      double t = y[k];
-      for (int q = 0; q < k; ++q) y[q] -= t * H[(size_t)k * ldh + q];
-    }
+  for (int k = threadIdx.x; k <= col; k += blockDim.x) ys[k] = S[k];
+  __syncthreads();
+  if (threadIdx.x == 0 && H[(size_t)col * ldh + col] == 0.0) {
+    S[col] = 0.0;
+    ys[col] = 0.0;
   }
-  if (y[0] != 0.0) y[0] /= H[0];
+  __syncthreads();
+  for (int k = col; k > 0; --k) {
+    if (ys[k] != 0.0) {   // the same value in every thread: a uniform branch
+      __syncthreads();
+      if (threadIdx.x == 0) ys[k] /= H[(size_t)k * ldh + k];
+      __syncthreads();
+      const double t = ys[k];
+      for (int q = threadIdx.x; q < k; q += blockDim.x) ys[q] -= t * H[(size_t)k * ldh + q];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && ys[0] != 0.0) ys[0] /= H[0];
+  __syncthreads();
+  for (int k = threadIdx.x; k <= col; k += blockDim.x) y[k] = ys[k];
 }
 
 __global__ void gm_update_x_kernel(int ndof, const double* __restrict__ V, const double* y, double* x,
@@ -578,7 +593,7 @@ int gmres_solve(GmresWork& W, int restart, double tol, long long maxiter, bool x
     inner += hs.ncols;
     applies += hs.ncols;
     presid = hs.presid;
-    gm_backsolve_kernel<<<1, 1, 0, s>>>(H, ldh, S, y, W.gst);
+    gm_backsolve_kernel<<<1, 128, 0, s>>>(H, ldh, S, y, W.gst);
     gm_update_x_kernel<<<W.ew_blocks, 256, 0, s>>>(n, W.V, y, W.x, W.gst);
     if ((st = resid(W.x, W.r, s))) return st;
     ++applies;
@@ -715,7 +730,7 @@ int fgmres_solve(GmresWork& W, double* Z, int restart, double tol, long long max
     TPF_CUDA_TRY(cudaStreamSynchronize(s));
     inner += hs.ncols;
     applies += hs.ncols;
-    gm_backsolve_kernel<<<1, 1, 0, s>>>(H, ldh, S, y, W.gst);
+    gm_backsolve_kernel<<<1, 128, 0, s>>>(H, ldh, S, y, W.gst);
     gm_update_x_kernel<<<W.ew_blocks, 256, 0, s>>>(n, Z, y, W.x, W.gst);
     if ((st = resid(W.x, W.r, s))) return st;
     ++applies;
